@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""bench.py -- phi-ASE throughput of libhase_b200 on B200.
+
+Workload (default ``disc_poly``, the polychromatic disc with reflections): a
+step is one full adaptive phi-ASE solve (importance weights, ray->prism map,
+ray passes until every sample's relative error <= threshold or maxRays) over a
+batch of sample points of the seeded synthetic medium; consecutive steps (and
+ranks) take consecutive sample batches.  Metric: rays/s over the whole job;
+the step time is the time to reach the threshold for that batch.
+
+``value`` is device-timed (CUDA events recorded by the library on the stream
+its kernels run on), inputs resident; ``e2e`` goes through the public API with
+host buffers: each step uploads the step's beta field (H2D) and reads the
+per-sample results back (D2H).  Under torchrun each rank runs its own sample
+batches (weak scaling, no collective on the data path); timing is the max over
+ranks.
+
+``--impl reference`` times the CPU restatement of the same method (the oracle,
+FP64, OpenMP over all host threads) on a bounded sample of the same workload:
+the reference's own CPU backend cannot be built here (alpaka3 / openPMD-api
+are not available), and its serial backend throws for this path.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+FP32_INSTR_PER_CROSSING = 24   # stated per-crossing FP32 instruction count
+BYTES_PER_CROSSING = 52        # triangle record 48 B + prism beta 4 B
+SMS = 148
+LANES_PER_SM = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="disc_poly")
+    ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def cpu_baseline(workload, seconds, steps_hint=None):
+    """Oracle (FP64 port of the method) on all host threads, bounded in time."""
+    import numpy as np
+
+    from oracle import oracle
+
+    w = workload
+    sa, se = w.spectra.resampled(w.monochromatic)
+    cores = os.cpu_count() or 1
+    S = w.mesh.numberOfSamples
+    rng = np.random.default_rng(1)
+    rays = 0
+    n_samples = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        first = int(rng.integers(0, S - cores))
+        r = oracle.phi_ase(w.mesh, (sa, se), minRays=w.minRays, maxRays=w.minRays, useReflections=w.useReflections,
+                           seed=7, minSample=first, maxSample=first + cores - 1, threads=cores)
+        rays += int(r["totalRays"].astype(np.int64).sum())
+        n_samples += cores
+    dt = time.perf_counter() - t0
+    return {"value": rays / dt, "unit": "rays/s", "cores": cores, "kind": "port",
+            "sample": f"{n_samples} samples x {w.minRays} rays (first adaptive pass, importance included), "
+                      f"{dt:.1f} s on {cores} threads"}
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def l2_read_bandwidth(torch, dev):
+    """Live L2-resident read bandwidth (GB/s): repeated reduction of a 32 MiB buffer."""
+    x = torch.ones(8 << 20, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        x.sum()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record()
+    for _ in range(reps):
+        x.sum()
+    e1.record()
+    torch.cuda.synchronize()
+    return reps * x.numel() * 4 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from haseongpu_b200 import DeviceMesh, build as _build
+    from haseongpu_b200.configs import WORKLOADS
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    _build.build_library()
+    w = WORKLOADS[args.workload]()
+    mesh = w.mesh
+    sa, se = w.spectra.resampled(w.monochromatic)
+    S = mesh.numberOfSamples
+    B = min(args.samples, S)
+    ctx = DeviceMesh(mesh, sa, se, device=local)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MiB > 126 MB L2
+
+    def run_step(step, beta=None):
+        first = ((step * world + rank) * B) % (S - B + 1)
+        if beta is not None:
+            ctx.update_beta(beta)
+        return ctx.calc_phi_ase(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold,
+                                useReflections=w.useReflections, monochromatic=w.monochromatic,
+                                adaptiveSteps=w.adaptiveSteps, rngSeed=1000 + step, minSample=first,
+                                maxSample=first + B - 1)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for s in range(args.warmup):
+        run_step(s)
+    barrier()
+    dev_ms, ray_ms, rays, crossings, launches, unconverged, steps_ms = 0.0, 0.0, 0, 0, 0, 0, []
+    with ClockSampler(local) as clk:
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = run_step(args.warmup + s)
+            dev_ms += r.totalMilliseconds
+            ray_ms += r.rayMilliseconds
+            rays += r.raysTraced
+            crossings += r.crossings
+            launches += r.kernelLaunches + 1
+            unconverged += r.unconvergedSamples
+            steps_ms.append(r.totalMilliseconds)
+        barrier()
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+
+    # e2e: public API with host buffers (beta upload + results read back every step)
+    beta_host = [np.ascontiguousarray(mesh.betaVolume * (1.0 + 0.01 * k)) for k in range(args.steps)]
+    barrier()
+    t1 = time.perf_counter()
+    e2e_rays = 0
+    for s in range(args.steps):
+        r = run_step(args.warmup + s, beta=beta_host[s])
+        e2e_rays += r.raysTraced
+    barrier()
+    e2e_s = time.perf_counter() - t1
+    ctx.update_beta(mesh.betaVolume)
+
+    stats = torch.tensor([dev_ms, float(rays), float(e2e_s), float(e2e_rays), float(crossings), ray_ms],
+                         dtype=torch.float64, device=dev)
+    if world > 1:
+        mx = stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = stats.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        dev_ms_max, e2e_max = float(mx[0]), float(mx[2])
+        rays_all, e2e_rays_all, cross_all = float(sm[1]), float(sm[3]), float(sm[4])
+    else:
+        dev_ms_max, e2e_max, rays_all, e2e_rays_all, cross_all = dev_ms, e2e_s, float(rays), float(e2e_rays), float(crossings)
+
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+        r_fp32 = SMS * LANES_PER_SM * f_clk / FP32_INSTR_PER_CROSSING
+        l2 = l2_read_bandwidth(torch, dev)
+        r_l2 = l2 * 1e9 / BYTES_PER_CROSSING
+        achieved = crossings / (ray_ms * 1e-3)
+        roof = min(r_fp32, r_l2)
+        cpu = cpu_baseline(w, args.cpu_seconds) if world == 1 else None
+        h2d = mesh.numberOfPrisms * 8
+        d2h = B * (4 + 8 + 8 + 4 + 8 + 4)
+        line = {
+            "metric": "phi-ASE rays/s to per-sample relative error <= threshold (plain importance sampling, 1 B200)",
+            "value": rays_all / (dev_ms_max * 1e-3),
+            "unit": "rays/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": dev_ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 geometry, f64 sums",
+            "data": "synthetic (seeded gain medium, no dataset)",
+            "config": {"workload": w.name, "samples_per_step_per_gpu": B, "triangles": mesh.numberOfTriangles,
+                       "levels": mesh.numberOfLevels, "prisms": mesh.numberOfPrisms,
+                       "wavelengths": int(len(sa)), "reflections": w.useReflections,
+                       "rays_per_sample": [w.minRays, w.maxRays], "threshold": w.threshold,
+                       "adaptive_steps": w.adaptiveSteps, "parallelism": f"sample batches x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step; per-step weights > L2"},
+            "time_to_threshold_ms": statistics.median(steps_ms),
+            "crossings_per_s": cross_all / (dev_ms_max * 1e-3),
+            "unconverged_samples": unconverged,
+            "e2e": {"value": e2e_rays_all / e2e_max, "unit": "rays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel",
+                         "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
+                         "traffic": None, "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
+                         "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
+            "clocks": clocks,
+            "wall_s": wall,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    from haseongpu_b200.configs import WORKLOADS
+
+    w = WORKLOADS[args.workload]()
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+    for _ in range(args.warmup):
+        cpu_baseline(w, 0.5)
+    vals = [cpu_baseline(w, per_step) for _ in range(args.steps)]
+    value = statistics.median(v["value"] for v in vals)
+    cores = vals[0]["cores"]
+    line = {
+        "metric": "phi-ASE rays/s to per-sample relative error <= threshold (plain importance sampling, 1 B200)",
+        "value": value, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded gain medium, no dataset)", "impl": "reference",
+        "config": {"workload": w.name, "threshold": w.threshold, "reflections": w.useReflections},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": cores, "kind": "port",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

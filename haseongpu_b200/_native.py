@@ -1,0 +1,187 @@
+"""ctypes binding of libhase_b200.so (the C ABI declared in include/hase_b200.h).
+
+The shared library is built in-tree (``haseongpu_b200/libhase_b200.so``) by
+``haseongpu_b200.build.build_library()``.  There is no CPU fallback: every
+entry point runs on a CUDA device and reports ``HASE_NO_DEVICE`` otherwise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PACKAGE_DIR = Path(__file__).resolve().parent
+LIB_PATH = PACKAGE_DIR / "libhase_b200.so"
+
+HASE_OK = 0
+HASE_INVALID_ARGUMENT = 1
+HASE_CUDA_ERROR = 2
+HASE_OUT_OF_MEMORY = 3
+HASE_DEVICE_TIMEOUT = 4
+HASE_DROPPED_RAYS = 5
+HASE_NOT_CONVERGED = 6
+HASE_NO_DEVICE = 7
+WARNINGS = (HASE_DROPPED_RAYS, HASE_NOT_CONVERGED)
+
+# Every symbol include/hase_b200.h declares.
+EXPORTED_SYMBOLS = (
+    "hase_last_error_message",
+    "hase_status_string",
+    "hase_abi_version",
+    "hase_context_create",
+    "hase_context_update_beta",
+    "hase_calc_phi_ase",
+    "hase_context_destroy",
+    "hase_importance_weights",
+    "hase_ray_map",
+    "hase_trace_rays",
+    "hase_philox",
+)
+
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("numberOfPoints", C.c_uint32),
+        ("numberOfTriangles", C.c_uint32),
+        ("numberOfLevels", C.c_uint32),
+        ("points", _f64p),
+        ("triangles", _u32p),
+        ("thickness", C.c_double),
+        ("betaVolume", _f64p),
+        ("betaCells", _f64p),
+        ("claddingCellTypes", _u32p),
+        ("claddingNumber", C.c_uint32),
+        ("claddingAbsorption", C.c_double),
+        ("nTot", C.c_double),
+        ("crystalTFluo", C.c_double),
+        ("reflectivities", _f64p),
+        ("refractiveIndices", _f64p),
+    ]
+
+
+class SpectrumDesc(C.Structure):
+    _fields_ = [("numberOfWavelengths", C.c_uint32), ("sigmaA", _f64p), ("sigmaE", _f64p)]
+
+
+class ExperimentDesc(C.Structure):
+    _fields_ = [
+        ("minRays", C.c_uint32),
+        ("maxRays", C.c_uint32),
+        ("mseThreshold", C.c_double),
+        ("useReflections", C.c_uint32),
+        ("monochromatic", C.c_uint32),
+    ]
+
+
+class ComputeDesc(C.Structure):
+    _fields_ = [
+        ("adaptiveSteps", C.c_uint32),
+        ("repetitions", C.c_uint32),
+        ("rngSeed", C.c_uint32),
+        ("minSample", C.c_uint32),
+        ("maxSample", C.c_uint32),
+        ("raysPerThread", C.c_uint32),
+        ("blockSize", C.c_uint32),
+        ("workspaceBytes", C.c_uint64),
+    ]
+
+
+class ResultDesc(C.Structure):
+    _fields_ = [
+        ("phiAse", _f32p),
+        ("standardError", _f64p),
+        ("relativeStandardError", _f64p),
+        ("totalRays", _u32p),
+        ("dndtAse", _f64p),
+        ("droppedRays", _u32p),
+        ("raysTraced", C.c_uint64),
+        ("crossings", C.c_uint64),
+        ("importanceMilliseconds", C.c_double),
+        ("rayMilliseconds", C.c_double),
+        ("totalMilliseconds", C.c_double),
+        ("passes", C.c_uint32),
+        ("unconvergedSamples", C.c_uint32),
+        ("kernelLaunches", C.c_uint32),
+    ]
+
+
+class HaseError(RuntimeError):
+    """A libhase_b200 call failed; ``status`` is the hase_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing; build it with haseongpu_b200.build.build_library()")
+        L = C.CDLL(str(LIB_PATH))
+        L.hase_last_error_message.restype = C.c_char_p
+        L.hase_status_string.restype = C.c_char_p
+        L.hase_status_string.argtypes = [C.c_int]
+        L.hase_abi_version.restype = C.c_int
+        L.hase_context_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(SpectrumDesc), C.c_int,
+                                          C.POINTER(C.c_void_p)]
+        L.hase_context_update_beta.argtypes = [C.c_void_p, _f64p, _f64p]
+        L.hase_calc_phi_ase.argtypes = [C.c_void_p, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc),
+                                        C.POINTER(ResultDesc)]
+        L.hase_context_destroy.argtypes = [C.c_void_p]
+        L.hase_importance_weights.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
+        L.hase_ray_map.argtypes = [C.c_uint32, C.c_uint32, _f32p, C.c_uint32, _u32p, _u32p, _u32p, _u64p]
+        L.hase_trace_rays.argtypes = [C.c_void_p, C.c_uint32, _f32p, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
+                                      _f32p, _f32p, _u32p]
+        L.hase_philox.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
+        for name in EXPORTED_SYMBOLS:
+            if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version"):
+                getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(status: int, *, allow_warnings: bool = False) -> int:
+    if status == HASE_OK or (allow_warnings and status in WARNINGS):
+        return status
+    msg = lib().hase_last_error_message().decode(errors="replace")
+    name = lib().hase_status_string(status).decode()
+    raise HaseError(status, f"libhase_b200: {name}: {msg}")
+
+
+def ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def philox(ctr, key):
+    """Device Philox4x32-10 of counters ``ctr`` [n, 4] under ``key`` (2 words)."""
+    c = np.ascontiguousarray(np.asarray(ctr, np.uint32).reshape(-1, 4))
+    k = np.ascontiguousarray(np.asarray(key, np.uint32).reshape(2))
+    out = np.empty_like(c)
+    check(lib().hase_philox(c.shape[0], ptr(c, _u32p), ptr(k, _u32p), ptr(out, _u32p)))
+    return out
+
+
+def ray_map(weights, rays, phases):
+    """Device ray->prism map of weight rows ``weights`` [rows, n] (float32)."""
+    w = np.ascontiguousarray(np.atleast_2d(np.asarray(weights, np.float32)))
+    rows, n = w.shape
+    ph = np.ascontiguousarray(np.asarray(phases, np.uint32).reshape(rows))
+    q = np.empty((rows, n), np.uint32)
+    off = np.empty((rows, n + 1), np.uint32)
+    Q = np.empty(rows, np.uint64)
+    check(lib().hase_ray_map(rows, n, ptr(w, _f32p), int(rays), ptr(ph, _u32p), ptr(q, _u32p), ptr(off, _u32p),
+                             ptr(Q, _u64p)))
+    return Q, q, off

@@ -1,0 +1,82 @@
+"""Seeded synthetic gain media for the benchmark workloads.
+
+No public dataset is involved: every medium is generated here from a fixed
+master seed (20261203) with one ``numpy.random.SeedSequence`` child per
+workload.
+
+disc_small   ~550 points on 13 jittered concentric rings of a 1 cm disc,
+             Delaunay (~1,000 triangles), 10 levels over 0.7 cm (9 prism
+             layers); beta = 0.05 + 0.25 exp(-r^2/(0.4 cm)^2) exp(-z/0.5 cm)
+             at each prism centre; N_tot = 1.38e20 cm^-3; one wavelength,
+             sigma_e = 2.2e-20, sigma_a = 1.1e-21 cm^2; no reflections;
+             rays 1e5 -> 1e6 per sample, relative-error threshold 0.005.
+disc_poly    ~2,600 points on 29 rings (~5,100 triangles) x 20 levels, the
+             same beta profile x (1 + U(-0.05, 0.05)) noise, 16 wavelength
+             pairs from two Lorentzians (peaks 1030 / 940 nm) scaled to
+             1e-21..3e-20 cm^2, reflectivity 0.3 bottom / 0.9 top with
+             refractive index 1.83 inside / 1.0 outside (total internal
+             reflection above the critical angle), order <= 2; rays
+             1e5 -> 1e7, threshold 0.001.
+The fluorescence lifetime is 9.41e-4 s (the reference example media,
+example/laserPumpCladdingApi.py:241); it only scales phi.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mesh import PrismMesh, delaunay_triangles, disc_points, gaussian_pump_beta, point_beta
+from .spectra import CrossSectionData, two_lorentzian_spectrum
+
+MASTER_SEED = 20261203
+TAU = 9.41e-4
+
+
+@dataclass
+class Workload:
+    name: str
+    mesh: PrismMesh
+    spectra: CrossSectionData
+    minRays: int
+    maxRays: int
+    threshold: float
+    useReflections: bool
+    monochromatic: bool
+    adaptiveSteps: int = 4
+
+
+def _rng(index: int) -> np.random.Generator:
+    return np.random.default_rng(np.random.SeedSequence(MASTER_SEED).spawn(8)[index])
+
+
+def disc_small() -> Workload:
+    rng = _rng(0)
+    pts = disc_points(1.0, 13, rng)
+    tri = delaunay_triangles(pts)
+    levels, thickness = 10, 0.7 / 9
+    mesh = PrismMesh(points=pts, triangles=tri, numberOfLevels=levels, thickness=thickness,
+                     betaVolume=gaussian_pump_beta(pts, tri, levels, thickness), nTot=1.38e20, crystalTFluo=TAU,
+                     betaCells=point_beta(pts, levels, thickness), name="disc_small")
+    spectra = CrossSectionData.monochromatic(wavelength=1030e-9, crossSectionAbsorption=1.1e-21,
+                                             crossSectionEmission=2.2e-20)
+    return Workload("disc_small", mesh, spectra, 100_000, 1_000_000, 0.005, False, True)
+
+
+def disc_poly() -> Workload:
+    rng = _rng(1)
+    pts = disc_points(1.0, 29, rng)
+    tri = delaunay_triangles(pts)
+    levels, thickness = 20, 0.7 / 19
+    beta = gaussian_pump_beta(pts, tri, levels, thickness)
+    beta *= 1.0 + rng.uniform(-0.05, 0.05, beta.size)
+    T = tri.shape[0]
+    mesh = PrismMesh(points=pts, triangles=tri, numberOfLevels=levels, thickness=thickness, betaVolume=beta,
+                     nTot=1.38e20, crystalTFluo=TAU, betaCells=point_beta(pts, levels, thickness),
+                     reflectivities=np.tile([0.3, 0.9], (T, 1)), refractiveIndices=[1.83, 1.0, 1.83, 1.0],
+                     name="disc_poly")
+    return Workload("disc_poly", mesh, two_lorentzian_spectrum(16), 100_000, 10_000_000, 0.001, True, False)
+
+
+WORKLOADS = {"disc_small": disc_small, "disc_poly": disc_poly}

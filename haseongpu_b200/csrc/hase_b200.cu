@@ -1,0 +1,1126 @@
+// hase_b200.cu -- libhase_b200.so: sm_100a kernels of the backward,
+// importance-sampled phi-ASE method and the C ABI around them.
+//
+// Per batch of sample points (prism mesh, FP32 geometry, FP64 sums):
+//   (a1) importanceKernel  one thread per (sample, reflection slice, prism):
+//        straight-line walk from the prism centre to the (image) sample point,
+//        ln w = ln(beta V / d^2) + Int g dl.
+//   (a2) mapKernel         one CTA per sample: w = exp(ln w - max), integer
+//        quantisation q = ceil(w 2^24 / max w), block-wide warp-shuffle scan of
+//        q and the systematic-sampling ray offsets
+//        offsets[b] = floor((C_b M + floor(phase Q / 2^32)) / Q).
+//   (b)  rayKernel         CTAs over (ray chunk, active sample): Philox4x32-10
+//        start points, prism walk (neighbour + level crossings, top/bottom
+//        reflections), per-ray X = N_tot/(4 pi tau) beta V (Q/q) exp(G)/d^2,
+//        warp-shuffle FP64 reduction of sum X and sum X^2 per chunk.
+//   (c/d) finalizeKernel   one warp per active sample: deterministic reduction
+//        of the chunk partials, phi = sum/N, relative error, and compaction of
+//        the samples still above the threshold for the next adaptive pass.
+// Reference anchors (HASEonGPU v2.2.0 tree): result/experiment types
+// include/core/types.hpp:201-354; dndt include/core/forwardPhiAseUtilities.hpp:16-25;
+// entry point include/core/simulation.hpp:42-47.
+#include "hase_b200.h"
+#include "hase_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+using namespace hase;
+
+namespace {
+
+thread_local std::string g_lastError;
+
+hase_status fail(hase_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+    return st;
+}
+
+#define HASE_CUDA(call)                                                                                  \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            return fail(e_ == cudaErrorMemoryAllocation ? HASE_OUT_OF_MEMORY : HASE_CUDA_ERROR, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
+        }                                                                                                \
+    } while (0)
+
+#define HASE_TRY(expr)               \
+    do {                             \
+        hase_status s_ = (expr);     \
+        if (s_ != HASE_OK) return s_; \
+    } while (0)
+
+constexpr uint32_t kRayBlock = 256;
+constexpr uint32_t kRaysPerThread = 8;
+constexpr uint32_t kMaxChunks = 256;
+constexpr uint32_t kMapBlock = 1024;
+constexpr uint32_t kOffCap = 4096;
+constexpr double kPi = 3.14159265358979323846;
+
+// ------------------------------------------------------------ reductions ----
+template <typename T>
+__device__ __forceinline__ T warpSum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warpMax(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide inclusive scan of 64-bit values (warp shuffles + one shared pass).
+template <int BLOCK>
+__device__ __forceinline__ unsigned long long blockInclusiveScan(unsigned long long v, unsigned long long* warpTot,
+                                                                 unsigned long long& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    if (lane == 31) warpTot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = lane < BLOCK / 32 ? warpTot[lane] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long n = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += n;
+        }
+        if (lane < BLOCK / 32) warpTot[lane] = t;
+    }
+    __syncthreads();
+    if (warp > 0) v += warpTot[warp - 1];
+    total = warpTot[BLOCK / 32 - 1];
+    __syncthreads();
+    return v;
+}
+
+// --------------------------------------------------------- (a1) weights ----
+struct ImportanceLaunch {
+    MeshView m;
+    uint32_t firstSample, slices, nW;
+    float A, B;   // spectrally averaged gain coefficients
+    float* lnw;   // [rows][nW]
+};
+
+__global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= L.nW) return;
+    const uint32_t row = blockIdx.y;
+    const MeshView& m = L.m;
+    const uint32_t sample = L.firstSample + row;
+    const uint32_t j = b / m.P, p = b - j * m.P;
+    const uint32_t t = p % m.T, l = p / m.T;
+    float* out = L.lnw + size_t(row) * L.nW + b;
+    const float beta = __ldg(m.srcBeta + p);
+    if (!(beta > 0.0f)) {
+        *out = -INFINITY;
+        return;
+    }
+    const float2 S = __ldg(m.points + sample % m.Np);
+    const int ls = int(sample / m.Np);
+    const int kImg = imageLevel(ls, int(m.layers), j);
+    const float2 c = __ldg(m.centroid + t);
+    const float area = __ldg(&m.geo[2 * t + 1].z);
+    Ray r;
+    const float D2 = initRay(r, t, int(l), c.x, c.y, (float(int(l) - kImg) + 0.5f) * m.h, S.x, S.y, kImg, j, L.A,
+                             L.B, m.h);
+    GlobalLoader load{m.tri};
+    int st;
+    do {
+        st = stepRay(m, r, load);
+    } while (st == kContinue);
+    if (st == kDropped || !(D2 > 0.0f)) {
+        *out = -INFINITY;
+        return;
+    }
+    finishReflections(m, r);
+    *out = __logf(beta * area * m.h / D2) + r.G;
+}
+
+// ------------------------------------------------------- (a2) ray map ----
+struct MapLaunch {
+    const float* in;            // [rows][nW]: ln w (isLog) or w
+    int isLog;
+    int full;                   // 1: quantise + Q; 0: reuse q, Q
+    const uint32_t* rowList;    // nullptr: row = blockIdx.x
+    uint32_t nW;
+    uint32_t M;                 // rays to map this pass
+    const uint32_t* phases;     // nullptr: Philox(0, sample, pass, map tag)
+    uint32_t firstSample, pass, seedLo, seedHi;
+    float* wOut;                // optional [rows][nW] normalised weights
+    uint32_t* q;                // [rows][nW]
+    unsigned long long* Q;      // [rows]
+    uint32_t* offsets;          // [rows][nW+1]
+};
+
+__global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
+    __shared__ unsigned long long sWarp[kMapBlock / 32];
+    __shared__ float sMax;
+    __shared__ unsigned long long sQ;
+    const uint32_t row = L.rowList ? L.rowList[blockIdx.x] : blockIdx.x;
+    const uint32_t nW = L.nW;
+    const float* in = L.in + size_t(row) * nW;
+    uint32_t* q = L.q + size_t(row) * nW;
+    uint32_t* off = L.offsets + size_t(row) * (nW + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long Q;
+    if (L.full) {
+        float mx = -INFINITY;
+        for (uint32_t b = threadIdx.x; b < nW; b += kMapBlock) mx = fmaxf(mx, in[b]);
+        mx = warpMax(mx);
+        __shared__ float sRed[kMapBlock / 32];
+        if (lane == 0) sRed[warp] = mx;
+        __syncthreads();
+        if (warp == 0) {
+            float v = lane < kMapBlock / 32 ? sRed[lane] : -INFINITY;
+            v = warpMax(v);
+            if (lane == 0) sMax = v;
+        }
+        __syncthreads();
+        mx = sMax;
+        // Normalised weights: exp(ln w - max) has maximum exactly 1.
+        const float wmax = L.isLog ? (mx == -INFINITY ? 0.0f : 1.0f) : mx;
+        const double scale = wmax > 0.0f ? 16777216.0 / double(wmax) : 0.0;
+        unsigned long long part = 0;
+        for (uint32_t b = threadIdx.x; b < nW; b += kMapBlock) {
+            const float v = in[b];
+            const float w = L.isLog ? (v == -INFINITY || wmax == 0.0f ? 0.0f : expf(v - mx)) : v;
+            const uint32_t qi = (w > 0.0f && wmax > 0.0f) ? uint32_t(ceil(double(w) * scale)) : 0u;
+            q[b] = qi;
+            if (L.wOut) L.wOut[size_t(row) * nW + b] = w;
+            part += qi;
+        }
+        part = warpSum(part);
+        if (lane == 0) sWarp[warp] = part;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long v = lane < kMapBlock / 32 ? sWarp[lane] : 0ull;
+            v = warpSum(v);
+            if (lane == 0) {
+                sQ = v;
+                L.Q[row] = v;
+            }
+        }
+        __syncthreads();
+        Q = sQ;
+    } else {
+        Q = L.Q[row];
+    }
+    const uint32_t M = L.M;
+    if (Q == 0) {
+        for (uint32_t b = threadIdx.x; b <= nW; b += kMapBlock) off[b] = 0u;
+        return;
+    }
+    uint32_t phase;
+    if (L.phases) {
+        phase = L.phases[row];
+    } else {
+        phase = philox4x32_10(0u, L.firstSample + row, L.pass, kTagMap, L.seedLo, L.seedHi).x;
+    }
+    using u128 = unsigned __int128;
+    const unsigned long long phiQ = (unsigned long long)((u128(phase) * Q) >> 32);
+    unsigned long long carry = 0;
+    for (uint32_t base = 0; base < nW; base += kMapBlock) {
+        const uint32_t b = base + threadIdx.x;
+        const unsigned long long v = b < nW ? q[b] : 0u;
+        unsigned long long total;
+        const unsigned long long incl = blockInclusiveScan<kMapBlock>(v, sWarp, total);
+        if (b < nW) {
+            const unsigned long long C = carry + incl - v;
+            off[b] = uint32_t((u128(C) * M + phiQ) / Q);
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) off[nW] = M;
+}
+
+// --------------------------------------------------------- (b) rays ----
+struct RayLaunch {
+    MeshView m;
+    const uint32_t* active;       // active row ids
+    uint32_t firstSample, pass, M, raysPerChunk, nW;
+    const uint32_t* q;            // [rows][nW]
+    const unsigned long long* Q;  // [rows]
+    const uint32_t* offsets;      // [rows][nW+1]
+    uint32_t seedLo, seedHi;
+    const float2* spec;           // per wavelength (A, B)
+    uint32_t nLambda;
+    double C;                     // N_tot / (4 pi tau)
+    double* pSum;                 // [rows][kMaxChunks]
+    double* pSum2;
+    uint32_t* pDrop;
+    unsigned long long* pCross;
+};
+
+__device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int BLOCK, int RPT>
+__global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
+    __shared__ uint32_t sOff[kOffCap + 1];
+    __shared__ uint32_t sRange[2];
+    __shared__ double sRedD[2][BLOCK / 32];
+    __shared__ uint32_t sRedU[BLOCK / 32];
+    __shared__ unsigned long long sRedL[BLOCK / 32];
+
+    const MeshView& m = L.m;
+    const uint32_t row = L.active[blockIdx.y];
+    const uint32_t sample = L.firstSample + row;
+    const uint32_t chunk = blockIdx.x;
+    const uint32_t r0 = chunk * L.raysPerChunk;
+    const uint32_t r1 = min(r0 + L.raysPerChunk, L.M);
+    const uint32_t nW = L.nW;
+    const uint32_t* off = L.offsets + size_t(row) * (nW + 1);
+    const uint32_t* q = L.q + size_t(row) * nW;
+    const unsigned long long Qrow = L.Q[row];
+    if (Qrow == 0ull) {  // no source prism: every ray contributes 0
+        if (threadIdx.x == 0) {
+            const size_t k = size_t(row) * kMaxChunks + chunk;
+            L.pSum[k] = 0.0;
+            L.pSum2[k] = 0.0;
+            L.pDrop[k] = 0u;
+            L.pCross[k] = 0ull;
+        }
+        return;
+    }
+    const double CQ = L.C * double(Qrow);
+    const float2 S = __ldg(m.points + sample % m.Np);
+    const int ls = int(sample / m.Np);
+    const uint32_t lambdaPhase =
+        L.nLambda > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, L.seedLo, L.seedHi).y % L.nLambda : 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned laneLt = (1u << lane) - 1u;
+    GlobalLoader load{m.tri};
+
+    double sum = 0.0, sum2 = 0.0;
+    uint32_t dropped = 0;
+    unsigned long long crossings = 0;
+
+    for (uint32_t sub = r0; sub < r1; sub += BLOCK * RPT) {
+        const uint32_t subEnd = min(sub + BLOCK * RPT, r1);
+        if (threadIdx.x == 0) sRange[0] = upperBound(off, nW + 1, sub) - 1u;
+        if (threadIdx.x == 32) sRange[1] = upperBound(off, nW + 1, subEnd - 1u) - 1u;
+        __syncthreads();
+        const uint32_t pb = sRange[0], pe = sRange[1];
+        const uint32_t count = pe - pb + 2u;  // offsets pb .. pe+1
+        const bool staged = count <= kOffCap + 1;
+        if (staged)
+            for (uint32_t i = threadIdx.x; i < count; i += BLOCK) sOff[i] = off[pb + i];
+        __syncthreads();
+
+        const uint32_t wBegin = sub + uint32_t(warp) * 32u * RPT;
+        const uint32_t wEnd = min(wBegin + 32u * RPT, subEnd);
+        uint32_t fetch = wBegin;
+        bool active = false;
+        Ray ray;
+        float wf = 0.0f;
+        while (true) {
+            const unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (need && fetch < wEnd) {
+                const uint32_t r = fetch + __popc(need & laneLt);
+                if (!active && r < wEnd) {
+                    const uint32_t b = staged ? pb + upperBound(sOff, count, r) - 1u
+                                              : pb + upperBound(off + pb, count, r) - 1u;
+                    const uint32_t j = b / m.P, p = b - j * m.P;
+                    const uint32_t t = p % m.T, l = p / m.T;
+                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
+                    uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
+                    if (k1 + k2 + 1u > (1u << 24)) {
+                        k1 = (1u << 24) - 1u - k1;
+                        k2 = (1u << 24) - 1u - k2;
+                    }
+                    const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
+                    const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
+                    const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
+                    const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
+                    const int kImg = imageLevel(ls, int(m.layers), j);
+                    const uint32_t lam =
+                        L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
+                    const float2 ab = __ldg(L.spec + lam);
+                    const float D2 = initRay(ray, t, int(l), x, y, (float(int(l) - kImg) + u3) * m.h, S.x, S.y, kImg,
+                                             j, ab.x, ab.y, m.h);
+                    wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
+                    active = D2 > 0.0f;
+                    if (!active) ++dropped;  // start point on the sample point itself
+                }
+                fetch += __popc(need);
+            }
+            if (__ballot_sync(0xffffffffu, active) == 0u) break;
+            if (active) {
+                const int st = stepRay(m, ray, load);
+                ++crossings;
+                if (st != kContinue) {
+                    if (st == kDone) {
+                        finishReflections(m, ray);
+                        const double X = CQ * double(wf) * exp(double(ray.G));
+                        sum += X;
+                        sum2 += X * X;
+                    } else {
+                        ++dropped;
+                    }
+                    active = false;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    sum = warpSum(sum);
+    sum2 = warpSum(sum2);
+    dropped = warpSum(dropped);
+    crossings = warpSum(crossings);
+    if (lane == 0) {
+        sRedD[0][warp] = sum;
+        sRedD[1][warp] = sum2;
+        sRedU[warp] = dropped;
+        sRedL[warp] = crossings;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double a = lane < BLOCK / 32 ? sRedD[0][lane] : 0.0;
+        double b2 = lane < BLOCK / 32 ? sRedD[1][lane] : 0.0;
+        uint32_t d = lane < BLOCK / 32 ? sRedU[lane] : 0u;
+        unsigned long long c = lane < BLOCK / 32 ? sRedL[lane] : 0ull;
+        a = warpSum(a);
+        b2 = warpSum(b2);
+        d = warpSum(d);
+        c = warpSum(c);
+        if (lane == 0) {
+            const size_t k = size_t(row) * kMaxChunks + chunk;
+            L.pSum[k] = a;
+            L.pSum2[k] = b2;
+            L.pDrop[k] = d;
+            L.pCross[k] = c;
+        }
+    }
+}
+
+// ------------------------------------------------ (c)+(d) finalise ----
+struct FinalizeLaunch {
+    const uint32_t* active;
+    uint32_t nActive, chunks, M;
+    int last;                     // no further pass follows
+    double threshold;
+    const double* pSum;
+    const double* pSum2;
+    const uint32_t* pDrop;
+    const unsigned long long* pCross;
+    double* accSum;               // [rows]
+    double* accSum2;
+    uint32_t* accTotal;
+    uint32_t* accDrop;
+    unsigned long long* accCross;
+    float* phi;                   // [rows]
+    double* mse;
+    uint32_t* nextActive;
+    uint32_t* nextCount;
+};
+
+__global__ void __launch_bounds__(128) finalizeKernel(FinalizeLaunch L) {
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= L.nActive) return;
+    const uint32_t row = L.active[wid];
+    double s = 0.0, s2 = 0.0;
+    uint32_t d = 0;
+    unsigned long long c = 0;
+    for (uint32_t k = lane; k < L.chunks; k += 32) {
+        const size_t i = size_t(row) * kMaxChunks + k;
+        s += L.pSum[i];
+        s2 += L.pSum2[i];
+        d += L.pDrop[i];
+        c += L.pCross[i];
+    }
+    s = warpSum(s);
+    s2 = warpSum(s2);
+    d = warpSum(d);
+    c = warpSum(c);
+    if (lane == 0) {
+        const double sum = L.accSum[row] + s, sum2 = L.accSum2[row] + s2;
+        const uint32_t N = L.accTotal[row] + L.M;
+        L.accSum[row] = sum;
+        L.accSum2[row] = sum2;
+        L.accTotal[row] = N;
+        L.accDrop[row] += d;
+        L.accCross[row] += c;
+        const double mean = sum / double(N);
+        const double rse = mean > 0.0 ? sqrt(fabs(sum2 / double(N) - mean * mean) / double(N)) / mean : 0.0;
+        L.phi[row] = float(mean);
+        L.mse[row] = rse;
+        const bool again = !(rse <= L.threshold);
+        if (again && !L.last) L.nextActive[atomicAdd(L.nextCount, 1u)] = row;
+    }
+}
+
+__global__ void iotaKernel(uint32_t* a, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+// ------------------------------------------------------ diagnostics ----
+struct TraceLaunch {
+    MeshView m;
+    uint32_t n;
+    const float* start;
+    const uint32_t* tri;
+    const uint32_t* level;
+    const uint32_t* sample;
+    const uint32_t* slice;
+    float A, B;
+    float* lnGain;
+    float* dist;
+    uint32_t* dropped;
+};
+
+__global__ void traceKernel(TraceLaunch L) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    const MeshView& m = L.m;
+    const uint32_t sample = L.sample[i];
+    const float2 S = __ldg(m.points + sample % m.Np);
+    const int ls = int(sample / m.Np);
+    const uint32_t j = L.slice[i];
+    const int kImg = imageLevel(ls, int(m.layers), j);
+    const float zImgOffset = float(kImg) * m.h;
+    Ray r;
+    const float D2 = initRay(r, L.tri[i], int(L.level[i]), L.start[3 * i], L.start[3 * i + 1],
+                             L.start[3 * i + 2] - zImgOffset, S.x, S.y, kImg, j, L.A, L.B, m.h);
+    GlobalLoader load{m.tri};
+    int st;
+    do {
+        st = stepRay(m, r, load);
+    } while (st == kContinue);
+    if (st == kDone) finishReflections(m, r);
+    L.lnGain[i] = r.G;
+    L.dist[i] = sqrtf(D2);
+    L.dropped[i] = st == kDone ? 0u : 1u;
+}
+
+__global__ void philoxKernel(uint32_t n, const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Philox4 r = philox4x32_10(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3], k0, k1);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
+}
+
+// -------------------------------------------------------- host side ----
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(size_t count) {
+        if (count <= n) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
+
+struct HostTables {
+    std::vector<float4> tri, geo;
+    std::vector<float2> centroid, points;
+};
+
+hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& extent) {
+    const uint32_t T = d->numberOfTriangles, Np = d->numberOfPoints;
+    h.tri.assign(3 * size_t(T), make_float4(0, 0, 0, 0));
+    h.geo.assign(2 * size_t(T), make_float4(0, 0, 0, 0));
+    h.centroid.resize(T);
+    h.points.resize(Np);
+    extent = 0.0;
+    for (uint32_t i = 0; i < Np; ++i) {
+        h.points[i] = make_float2(float(d->points[2 * i]), float(d->points[2 * i + 1]));
+        extent = std::max(extent, std::max(std::fabs(d->points[2 * i]), std::fabs(d->points[2 * i + 1])));
+    }
+    std::vector<int32_t> nbr(3 * size_t(T), -1);
+    std::unordered_map<uint64_t, uint32_t> open;  // edge key -> 3*t + e
+    open.reserve(3 * size_t(T));
+    for (uint32_t t = 0; t < T; ++t) {
+        const uint32_t* v = d->triangles + 3 * size_t(t);
+        for (int e = 0; e < 3; ++e)
+            if (v[e] >= Np) return fail(HASE_INVALID_ARGUMENT, "triangle %u references point %u >= %u", t, v[e], Np);
+        const double x0 = d->points[2 * v[0]], y0 = d->points[2 * v[0] + 1];
+        const double x1 = d->points[2 * v[1]], y1 = d->points[2 * v[1] + 1];
+        const double x2 = d->points[2 * v[2]], y2 = d->points[2 * v[2] + 1];
+        const double cross = (x1 - x0) * (y2 - y0) - (y1 - y0) * (x2 - x0);
+        if (!(std::fabs(cross) > 0.0)) return fail(HASE_INVALID_ARGUMENT, "triangle %u is degenerate", t);
+        const double orient = cross > 0.0 ? 1.0 : -1.0;
+        double nx[3], ny[3], c[3];
+        for (int e = 0; e < 3; ++e) {
+            const uint32_t a = v[e], b = v[(e + 1) % 3];
+            const double ex = d->points[2 * b] - d->points[2 * a], ey = d->points[2 * b + 1] - d->points[2 * a + 1];
+            const double inv = 1.0 / std::sqrt(ex * ex + ey * ey);
+            nx[e] = orient * ey * inv;
+            ny[e] = -orient * ex * inv;
+            c[e] = nx[e] * d->points[2 * a] + ny[e] * d->points[2 * a + 1];
+            const uint64_t key = (uint64_t(std::min(a, b)) << 32) | std::max(a, b);
+            auto it = open.find(key);
+            if (it == open.end()) {
+                open.emplace(key, 3 * t + e);
+            } else {
+                const uint32_t other = it->second;
+                if (nbr[other] != -1) return fail(HASE_INVALID_ARGUMENT, "edge shared by more than two triangles");
+                nbr[3 * t + e] = int32_t(other);
+                nbr[other] = int32_t(3 * t + e);
+                open.erase(it);
+            }
+        }
+        h.tri[3 * t + 0] = make_float4(float(nx[0]), float(ny[0]), float(c[0]), float(nx[1]));
+        h.tri[3 * t + 1] = make_float4(float(ny[1]), float(c[1]), float(nx[2]), float(ny[2]));
+        h.tri[3 * t + 2].x = float(c[2]);
+        h.geo[2 * t] = make_float4(float(x0), float(y0), float(x1 - x0), float(y1 - y0));
+        h.geo[2 * t + 1] = make_float4(float(x2 - x0), float(y2 - y0), float(0.5 * std::fabs(cross)), 0.0f);
+        h.centroid[t] = make_float2(float((x0 + x1 + x2) / 3.0), float((y0 + y1 + y2) / 3.0));
+    }
+    for (uint32_t t = 0; t < T; ++t) {
+        int32_t w[3];
+        for (int e = 0; e < 3; ++e) {
+            const int32_t o = nbr[3 * t + e];
+            w[e] = o < 0 ? -1 : int32_t((uint32_t(o / 3) << 2) | uint32_t(o % 3));
+        }
+        float* rec = &h.tri[3 * t + 2].y;
+        std::memcpy(rec, w, sizeof(w));
+    }
+    return HASE_OK;
+}
+
+}  // namespace
+
+struct hase_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint32_t Np = 0, T = 0, L = 0, layers = 0, P = 0;
+    double h = 0, nTot = 0, tau = 0, cladAbs = 0, extent = 0;
+    uint32_t cladNumber = 0;
+    std::vector<uint32_t> cladTypes;
+    std::vector<double> betaCells, sigmaA, sigmaE;
+    bool hasReflect = false;
+    float tirCos2[2] = {-1.0f, -1.0f};
+    DevBuf<float4> tri, geo;
+    DevBuf<float2> centroid, points, spec;
+    DevBuf<float> gainBeta, srcBeta, reflect;
+    // workspace
+    DevBuf<float> lnw;
+    DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
+    DevBuf<unsigned long long> Q, accCross, pCross;
+    DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
+    DevBuf<float> phi;
+
+    MeshView view() const {
+        MeshView v{};
+        v.tri = tri.p;
+        v.geo = geo.p;
+        v.centroid = centroid.p;
+        v.gainBeta = gainBeta.p;
+        v.srcBeta = srcBeta.p;
+        v.points = points.p;
+        v.reflect = hasReflect ? reflect.p : nullptr;
+        v.T = T;
+        v.layers = layers;
+        v.P = P;
+        v.Np = Np;
+        v.h = float(h);
+        v.cladAbs = float(cladAbs);
+        v.tolEnd = float(4e-6 * extent);
+        v.tolBoundary = float(1e-4 * extent);
+        v.tirCos2[0] = tirCos2[0];
+        v.tirCos2[1] = tirCos2[1];
+        return v;
+    }
+};
+
+namespace {
+
+hase_status uploadBeta(hase_context* c, const double* betaVolume) {
+    std::vector<float> gain(c->P), src(c->P);
+    for (uint32_t p = 0; p < c->P; ++p) {
+        const double b = betaVolume[p];
+        if (!std::isfinite(b)) return fail(HASE_INVALID_ARGUMENT, "betaVolume[%u] is not finite", p);
+        const uint32_t t = p % c->T;
+        const bool clad = !c->cladTypes.empty() && c->cladTypes[t] == c->cladNumber;
+        src[p] = float(b);
+        gain[p] = clad ? NAN : float(b);
+    }
+    HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(c->srcBeta.p, src.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+uint32_t adaptiveTarget(uint32_t minRays, uint32_t maxRays, uint32_t steps, uint32_t k) {
+    // include/core/types.hpp:333-354: geometric growth minRays -> maxRays in `steps` increases.
+    if (maxRays <= minRays || steps == 0) return minRays;
+    if (k >= steps) return maxRays;
+    const double growth = std::pow(double(maxRays) / double(minRays), 1.0 / double(steps));
+    const double target = double(minRays) * std::pow(growth, double(k));
+    const uint32_t r = uint32_t(std::ceil(target));
+    return std::min(std::max(r, minRays), maxRays);
+}
+
+hase_status setDevice(hase_context* c) {
+    HASE_CUDA(cudaSetDevice(c->device));
+    return HASE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hase_last_error_message(void) { return g_lastError.c_str(); }
+
+int hase_abi_version(void) { return HASE_B200_ABI_VERSION; }
+
+const char* hase_status_string(hase_status s) {
+    switch (s) {
+        case HASE_OK: return "ok";
+        case HASE_INVALID_ARGUMENT: return "invalid argument";
+        case HASE_CUDA_ERROR: return "CUDA error";
+        case HASE_OUT_OF_MEMORY: return "out of device memory";
+        case HASE_DEVICE_TIMEOUT: return "device timeout";
+        case HASE_DROPPED_RAYS: return "dropped rays";
+        case HASE_NOT_CONVERGED: return "not converged";
+        case HASE_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_desc* sp, int device,
+                                hase_context** out) {
+    if (!d || !sp || !out) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (d->numberOfLevels < 2) return fail(HASE_INVALID_ARGUMENT, "numberOfLevels must be >= 2");
+    if (d->numberOfTriangles == 0 || d->numberOfPoints < 3) return fail(HASE_INVALID_ARGUMENT, "empty mesh");
+    if (!d->points || !d->triangles || !d->betaVolume) return fail(HASE_INVALID_ARGUMENT, "mesh arrays missing");
+    if (!(d->thickness > 0.0)) return fail(HASE_INVALID_ARGUMENT, "thickness must be positive");
+    if (!(d->nTot > 0.0) || !(d->crystalTFluo > 0.0)) return fail(HASE_INVALID_ARGUMENT, "nTot and crystalTFluo must be positive");
+    if (sp->numberOfWavelengths == 0 || !sp->sigmaA || !sp->sigmaE) return fail(HASE_INVALID_ARGUMENT, "empty spectrum");
+    if (uint64_t(d->numberOfTriangles) * (d->numberOfLevels - 1) * 5ull >= (1ull << 31))
+        return fail(HASE_INVALID_ARGUMENT, "mesh too large");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return fail(HASE_INVALID_ARGUMENT, "device %d out of range", device);
+
+    hase_context* c = new (std::nothrow) hase_context();
+    if (!c) return fail(HASE_OUT_OF_MEMORY, "host allocation failed");
+    auto cleanup = [&](hase_status s) {
+        hase_context_destroy(c);
+        return s;
+    };
+    c->device = device;
+    c->Np = d->numberOfPoints;
+    c->T = d->numberOfTriangles;
+    c->L = d->numberOfLevels;
+    c->layers = c->L - 1;
+    c->P = c->T * c->layers;
+    c->h = d->thickness;
+    c->nTot = d->nTot;
+    c->tau = d->crystalTFluo;
+    c->cladAbs = d->claddingAbsorption;
+    c->cladNumber = d->claddingNumber;
+    if (d->claddingCellTypes) c->cladTypes.assign(d->claddingCellTypes, d->claddingCellTypes + c->T);
+    if (d->betaCells) c->betaCells.assign(d->betaCells, d->betaCells + size_t(c->Np) * c->L);
+    c->sigmaA.assign(sp->sigmaA, sp->sigmaA + sp->numberOfWavelengths);
+    c->sigmaE.assign(sp->sigmaE, sp->sigmaE + sp->numberOfWavelengths);
+    for (uint32_t l = 0; l < sp->numberOfWavelengths; ++l)
+        if (!std::isfinite(sp->sigmaA[l]) || !std::isfinite(sp->sigmaE[l]) || sp->sigmaA[l] < 0 || sp->sigmaE[l] < 0)
+            return cleanup(fail(HASE_INVALID_ARGUMENT, "cross sections must be finite and non-negative"));
+    if (d->refractiveIndices) {
+        for (int s = 0; s < 2; ++s) {
+            const double nin = d->refractiveIndices[2 * s], nout = d->refractiveIndices[2 * s + 1];
+            if (nout < nin && nin > 0) {
+                const double r = nout / nin;
+                c->tirCos2[s] = float(1.0 - r * r);
+            }
+        }
+    }
+    HostTables ht;
+    hase_status st = buildHostTables(d, ht, c->extent);
+    if (st != HASE_OK) return cleanup(st);
+    c->extent = std::max(c->extent, c->h * c->layers);
+
+    if (cudaSetDevice(device) != cudaSuccess) return cleanup(fail(HASE_CUDA_ERROR, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(HASE_CUDA_ERROR, "cudaStreamCreate failed"));
+    for (auto& e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return cleanup(fail(HASE_CUDA_ERROR, "cudaEventCreate failed"));
+    auto up = [&](auto& buf, const auto& vec) -> hase_status {
+        using T = typename std::decay_t<decltype(vec)>::value_type;
+        HASE_CUDA(buf.ensure(vec.size()));
+        HASE_CUDA(cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        return HASE_OK;
+    };
+    if ((st = up(c->tri, ht.tri)) != HASE_OK) return cleanup(st);
+    if ((st = up(c->geo, ht.geo)) != HASE_OK) return cleanup(st);
+    if ((st = up(c->centroid, ht.centroid)) != HASE_OK) return cleanup(st);
+    if ((st = up(c->points, ht.points)) != HASE_OK) return cleanup(st);
+    if (c->gainBeta.ensure(c->P) != cudaSuccess || c->srcBeta.ensure(c->P) != cudaSuccess)
+        return cleanup(fail(HASE_OUT_OF_MEMORY, "beta tables"));
+    if (d->reflectivities) {
+        std::vector<float> r(2 * size_t(c->T));
+        for (size_t i = 0; i < r.size(); ++i) r[i] = float(d->reflectivities[i]);
+        c->hasReflect = true;
+        if ((st = up(c->reflect, r)) != HASE_OK) return cleanup(st);
+    }
+    if ((st = uploadBeta(c, d->betaVolume)) != HASE_OK) return cleanup(st);
+    *out = c;
+    return HASE_OK;
+}
+
+hase_status hase_context_update_beta(hase_context* c, const double* betaVolume, const double* betaCells) {
+    if (!c || !betaVolume) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    HASE_TRY(setDevice(c));
+    HASE_TRY(uploadBeta(c, betaVolume));
+    if (betaCells) c->betaCells.assign(betaCells, betaCells + size_t(c->Np) * c->L);
+    return HASE_OK;
+}
+
+hase_status hase_context_destroy(hase_context* c) {
+    if (!c) return HASE_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return HASE_OK;
+}
+
+hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                              hase_result* res) {
+    if (!c || !ex || !cp || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    HASE_TRY(setDevice(c));
+    const uint32_t nSamplesTotal = c->Np * c->L;
+    const uint32_t first = cp->minSample;
+    const uint32_t last = cp->maxSample == UINT32_MAX ? nSamplesTotal - 1 : cp->maxSample;
+    if (first > last || last >= nSamplesTotal)
+        return fail(HASE_INVALID_ARGUMENT, "sample range [%u, %u] outside [0, %u)", first, last, nSamplesTotal);
+    if (ex->minRays == 0) return fail(HASE_INVALID_ARGUMENT, "minRays must be positive");
+    if (ex->maxRays != 0 && ex->maxRays < ex->minRays) return fail(HASE_INVALID_ARGUMENT, "maxRays < minRays");
+    if (!(ex->mseThreshold >= 0.0)) return fail(HASE_INVALID_ARGUMENT, "mseThreshold must be >= 0");
+    const uint32_t maxRays = std::max(ex->maxRays, ex->minRays);
+    const uint32_t nS = last - first + 1;
+    const uint32_t slices = ex->useReflections ? 5u : 1u;
+    const uint32_t nW = slices * c->P;
+
+    // spectrum: (A, B) per wavelength, g = beta*A - B
+    const uint32_t nLambda = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    std::vector<float2> spec(nLambda);
+    double meanA = 0, meanB = 0, maxSA = 0, maxSE = 0;
+    for (uint32_t l = 0; l < nLambda; ++l) {
+        const double A = c->nTot * (c->sigmaE[l] + c->sigmaA[l]), B = c->nTot * c->sigmaA[l];
+        spec[l] = make_float2(float(A), float(B));
+        meanA += A / nLambda;
+        meanB += B / nLambda;
+        maxSA = std::max(maxSA, c->sigmaA[l]);
+        maxSE = std::max(maxSE, c->sigmaE[l]);
+    }
+    HASE_CUDA(c->spec.ensure(nLambda));
+    HASE_CUDA(cudaMemcpyAsync(c->spec.p, spec.data(), nLambda * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+
+    // batch rows by the workspace budget
+    const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
+    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxChunks * 28ull + 64;
+    uint32_t rows = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nS, budget / perRow)));
+    HASE_CUDA(c->lnw.ensure(size_t(rows) * nW));
+    HASE_CUDA(c->q.ensure(size_t(rows) * nW));
+    HASE_CUDA(c->offsets.ensure(size_t(rows) * (nW + 1)));
+    HASE_CUDA(c->Q.ensure(rows));
+    HASE_CUDA(c->activeA.ensure(rows));
+    HASE_CUDA(c->activeB.ensure(rows));
+    HASE_CUDA(c->counter.ensure(1));
+    HASE_CUDA(c->accSum.ensure(rows));
+    HASE_CUDA(c->accSum2.ensure(rows));
+    HASE_CUDA(c->accTotal.ensure(rows));
+    HASE_CUDA(c->accDrop.ensure(rows));
+    HASE_CUDA(c->accCross.ensure(rows));
+    HASE_CUDA(c->phi.ensure(rows));
+    HASE_CUDA(c->mse.ensure(rows));
+    HASE_CUDA(c->pSum.ensure(size_t(rows) * kMaxChunks));
+    HASE_CUDA(c->pSum2.ensure(size_t(rows) * kMaxChunks));
+    HASE_CUDA(c->pDrop.ensure(size_t(rows) * kMaxChunks));
+    HASE_CUDA(c->pCross.ensure(size_t(rows) * kMaxChunks));
+
+    const MeshView mv = c->view();
+    const double C = c->nTot / (4.0 * kPi * c->tau);
+    std::vector<float> hPhi(rows);
+    std::vector<double> hMse(rows);
+    std::vector<uint32_t> hTotal(rows), hDrop(rows);
+    std::vector<unsigned long long> hCross(rows);
+    res->raysTraced = 0;
+    res->crossings = 0;
+    res->importanceMilliseconds = 0;
+    res->rayMilliseconds = 0;
+    res->totalMilliseconds = 0;
+    res->passes = 0;
+    res->unconvergedSamples = 0;
+    res->kernelLaunches = 0;
+    uint64_t droppedTotal = 0;
+
+    for (uint32_t b0 = 0; b0 < nS; b0 += rows) {
+        const uint32_t nRows = std::min(rows, nS - b0);
+        const uint32_t firstSample = first + b0;
+        HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
+        ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p};
+        importanceKernel<<<dim3((nW + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+        HASE_CUDA(cudaGetLastError());
+        HASE_CUDA(cudaEventRecord(c->ev[1], c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->accSum.p, 0, nRows * sizeof(double), c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->accSum2.p, 0, nRows * sizeof(double), c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->accTotal.p, 0, nRows * sizeof(uint32_t), c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->accDrop.p, 0, nRows * sizeof(uint32_t), c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->accCross.p, 0, nRows * sizeof(unsigned long long), c->stream));
+        iotaKernel<<<(nRows + 255) / 256, 256, 0, c->stream>>>(c->activeA.p, nRows);
+        HASE_CUDA(cudaGetLastError());
+        res->kernelLaunches += 2;  // importance + iota
+        uint32_t* cur = c->activeA.p;
+        uint32_t* nxt = c->activeB.p;
+        uint32_t nActive = nRows;
+        uint32_t prevTarget = 0;
+        float impMs = 0;
+        for (uint32_t pass = 0;; ++pass) {
+            const uint32_t target = adaptiveTarget(ex->minRays, maxRays, cp->adaptiveSteps, pass);
+            const bool lastPass = target >= maxRays || pass >= cp->adaptiveSteps;
+            const uint32_t M = target - prevTarget;
+            MapLaunch ml{c->lnw.p, 1, pass == 0 ? 1 : 0, cur, nW, M, nullptr, firstSample, pass, cp->rngSeed, 0u,
+                         nullptr, c->q.p, c->Q.p, c->offsets.p};
+            mapKernel<<<nActive, kMapBlock, 0, c->stream>>>(ml);
+            HASE_CUDA(cudaGetLastError());
+            const uint32_t chunks = std::min<uint32_t>(kMaxChunks, (M + kRayBlock * kRaysPerThread - 1) / (kRayBlock * kRaysPerThread));
+            const uint32_t perChunk = (M + chunks - 1) / chunks;
+            HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
+            RayLaunch rl{mv, cur, firstSample, pass, M, perChunk, nW, c->q.p, c->Q.p, c->offsets.p, cp->rngSeed, 0u,
+                         c->spec.p, nLambda, C, c->pSum.p, c->pSum2.p, c->pDrop.p, c->pCross.p};
+            rayKernel<kRayBlock, kRaysPerThread><<<dim3(chunks, nActive), kRayBlock, 0, c->stream>>>(rl);
+            HASE_CUDA(cudaGetLastError());
+            HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
+            HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
+            FinalizeLaunch fl{cur, nActive, chunks, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,
+                              c->pDrop.p, c->pCross.p, c->accSum.p, c->accSum2.p, c->accTotal.p, c->accDrop.p,
+                              c->accCross.p, c->phi.p, c->mse.p, nxt, c->counter.p};
+            finalizeKernel<<<(nActive * 32 + 127) / 128, 128, 0, c->stream>>>(fl);
+            HASE_CUDA(cudaGetLastError());
+            res->kernelLaunches += 3;  // map + rays + finalize
+            uint32_t next = 0;
+            HASE_CUDA(cudaMemcpyAsync(&next, c->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+            HASE_CUDA(cudaStreamSynchronize(c->stream));
+            float ms = 0;
+            if (pass == 0) {
+                HASE_CUDA(cudaEventElapsedTime(&impMs, c->ev[0], c->ev[1]));
+                res->importanceMilliseconds += impMs;
+            }
+            HASE_CUDA(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+            res->rayMilliseconds += ms;
+            res->passes = std::max(res->passes, pass + 1);
+            prevTarget = target;
+            if (lastPass) {
+                res->unconvergedSamples += next;  // samples still above threshold at the cap
+                break;
+            }
+            if (next == 0) break;
+            std::swap(cur, nxt);
+            nActive = next;
+        }
+        HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
+        HASE_CUDA(cudaMemcpyAsync(hPhi.data(), c->phi.p, nRows * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaMemcpyAsync(hMse.data(), c->mse.p, nRows * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaMemcpyAsync(hTotal.data(), c->accTotal.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaMemcpyAsync(hDrop.data(), c->accDrop.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaMemcpyAsync(hCross.data(), c->accCross.p, nRows * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaStreamSynchronize(c->stream));
+        float total = 0;
+        HASE_CUDA(cudaEventElapsedTime(&total, c->ev[0], c->ev[3]));
+        res->totalMilliseconds += total;
+        for (uint32_t i = 0; i < nRows; ++i) {
+            const uint32_t o = b0 + i, s = firstSample + i;
+            if (res->phiAse) res->phiAse[o] = hPhi[i];
+            if (res->relativeStandardError) res->relativeStandardError[o] = hMse[i];
+            if (res->standardError) res->standardError[o] = hMse[i] * double(hPhi[i]);
+            if (res->totalRays) res->totalRays[o] = hTotal[i];
+            if (res->droppedRays) res->droppedRays[o] = hDrop[i];
+            if (res->dndtAse) {
+                const double sA = nLambda == 1 ? c->sigmaA[0] : maxSA, sE = nLambda == 1 ? c->sigmaE[0] : maxSE;
+                const double bc = c->betaCells.empty() ? 0.0 : c->betaCells[s];
+                res->dndtAse[o] = (bc * (sE + sA) - sA) * double(hPhi[i]);
+            }
+            res->raysTraced += hTotal[i];
+            res->crossings += hCross[i];
+            droppedTotal += hDrop[i];
+        }
+    }
+    if (droppedTotal) {
+        fail(HASE_DROPPED_RAYS, "%llu rays could not be walked", (unsigned long long)droppedTotal);
+        return HASE_DROPPED_RAYS;
+    }
+    if (res->unconvergedSamples) {
+        fail(HASE_NOT_CONVERGED, "%u samples above the threshold at maxRays", res->unconvergedSamples);
+        return HASE_NOT_CONVERGED;
+    }
+    return HASE_OK;
+}
+
+hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                                    float* weights) {
+    if (!c || !weights || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
+    HASE_TRY(setDevice(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    double meanA = 0, meanB = 0;
+    const uint32_t n = uint32_t(c->sigmaA.size());
+    for (uint32_t l = 0; l < n; ++l) {
+        meanA += c->nTot * (c->sigmaE[l] + c->sigmaA[l]) / n;
+        meanB += c->nTot * c->sigmaA[l] / n;
+    }
+    DevBuf<float> lnw, w;
+    DevBuf<uint32_t> q, off;
+    DevBuf<unsigned long long> Q;
+    HASE_CUDA(lnw.ensure(size_t(count) * nW));
+    HASE_CUDA(w.ensure(size_t(count) * nW));
+    HASE_CUDA(q.ensure(size_t(count) * nW));
+    HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
+    HASE_CUDA(Q.ensure(count));
+    ImportanceLaunch il{c->view(), firstSample, slices, nW, float(meanA), float(meanB), lnw.p};
+    importanceKernel<<<dim3((nW + 255) / 256, count), 256, 0, c->stream>>>(il);
+    HASE_CUDA(cudaGetLastError());
+    MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
+    mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(weights, w.p, size_t(count) * nW * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+hase_status hase_ray_map(uint32_t rows, uint32_t n, const float* weights, uint32_t rays, const uint32_t* phases,
+                         uint32_t* q, uint32_t* offsets, uint64_t* Qout) {
+    if (!weights || !phases || !q || !offsets || !Qout || rows == 0 || n == 0)
+        return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    for (size_t i = 0; i < size_t(rows) * n; ++i)
+        if (!(weights[i] >= 0.0f) || std::isinf(weights[i]))
+            return fail(HASE_INVALID_ARGUMENT, "weights must be finite and non-negative");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    DevBuf<float> w;
+    DevBuf<uint32_t> dq, doff, dph;
+    DevBuf<unsigned long long> dQ;
+    HASE_CUDA(w.ensure(size_t(rows) * n));
+    HASE_CUDA(dq.ensure(size_t(rows) * n));
+    HASE_CUDA(doff.ensure(size_t(rows) * (n + 1)));
+    HASE_CUDA(dph.ensure(rows));
+    HASE_CUDA(dQ.ensure(rows));
+    HASE_CUDA(cudaMemcpy(w.p, weights, size_t(rows) * n * sizeof(float), cudaMemcpyHostToDevice));
+    HASE_CUDA(cudaMemcpy(dph.p, phases, rows * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    MapLaunch ml{w.p, 0, 1, nullptr, n, rays, dph.p, 0u, 0u, 0u, 0u, nullptr, dq.p, dQ.p, doff.p};
+    mapKernel<<<rows, kMapBlock>>>(ml);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaDeviceSynchronize());
+    HASE_CUDA(cudaMemcpy(q, dq.p, size_t(rows) * n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    HASE_CUDA(cudaMemcpy(offsets, doff.p, size_t(rows) * (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> hQ(rows);
+    HASE_CUDA(cudaMemcpy(hQ.data(), dQ.p, rows * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < rows; ++i) Qout[i] = hQ[i];
+    return HASE_OK;
+}
+
+hase_status hase_trace_rays(hase_context* c, uint32_t n, const float* start, const uint32_t* tri,
+                            const uint32_t* level, const uint32_t* sample, const uint32_t* slice, uint32_t wavelength,
+                            float* lnGain, float* distance, uint32_t* dropped) {
+    if (!c || !start || !tri || !level || !sample || !slice || !lnGain || !distance || !dropped)
+        return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return HASE_OK;
+    if (wavelength >= c->sigmaA.size()) return fail(HASE_INVALID_ARGUMENT, "wavelength index out of range");
+    for (uint32_t i = 0; i < n; ++i) {
+        if (tri[i] >= c->T || level[i] >= c->layers || sample[i] >= c->Np * c->L || slice[i] > 4)
+            return fail(HASE_INVALID_ARGUMENT, "ray %u: index out of range", i);
+    }
+    HASE_TRY(setDevice(c));
+    DevBuf<float> dStart, dLn, dDist;
+    DevBuf<uint32_t> dTri, dLev, dSam, dSli, dDrop;
+    HASE_CUDA(dStart.ensure(3 * size_t(n)));
+    HASE_CUDA(dLn.ensure(n));
+    HASE_CUDA(dDist.ensure(n));
+    HASE_CUDA(dTri.ensure(n));
+    HASE_CUDA(dLev.ensure(n));
+    HASE_CUDA(dSam.ensure(n));
+    HASE_CUDA(dSli.ensure(n));
+    HASE_CUDA(dDrop.ensure(n));
+    HASE_CUDA(cudaMemcpyAsync(dStart.p, start, 3 * size_t(n) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dTri.p, tri, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dLev.p, level, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dSam.p, sample, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dSli.p, slice, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    const float A = float(c->nTot * (c->sigmaE[wavelength] + c->sigmaA[wavelength]));
+    const float B = float(c->nTot * c->sigmaA[wavelength]);
+    TraceLaunch tl{c->view(), n, dStart.p, dTri.p, dLev.p, dSam.p, dSli.p, A, B, dLn.p, dDist.p, dDrop.p};
+    traceKernel<<<(n + 127) / 128, 128, 0, c->stream>>>(tl);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(lnGain, dLn.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(distance, dDist.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dropped, dDrop.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+hase_status hase_philox(uint32_t n, const uint32_t* ctr, const uint32_t key[2], uint32_t* out) {
+    if (!ctr || !key || !out) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return HASE_OK;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    DevBuf<uint32_t> dc, dout;
+    HASE_CUDA(dc.ensure(4 * size_t(n)));
+    HASE_CUDA(dout.ensure(4 * size_t(n)));
+    HASE_CUDA(cudaMemcpy(dc.p, ctr, 4 * size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    philoxKernel<<<(n + 127) / 128, 128>>>(n, dc.p, key[0], key[1], dout.p);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaDeviceSynchronize());
+    HASE_CUDA(cudaMemcpy(out, dout.p, 4 * size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return HASE_OK;
+}
+
+}  // extern "C"

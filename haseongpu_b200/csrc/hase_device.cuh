@@ -1,0 +1,255 @@
+// hase_device.cuh -- device-side building blocks of the phi-ASE hot path:
+// Philox4x32-10, the packed prism-mesh view, and the FP32 prism walk.
+//
+// The walk follows the legacy HASEonGPU backward method (rays from a start
+// point in a prism to the sample point, crossing triangle edges through the
+// neighbour table and z levels), here parametrised by the remaining distance s
+// to the (image) sample point, p(s) = S + s*u, walked from s = |start - S|
+// down to 0.  The exits of a prism are the largest crossing parameters below
+// s: edges (2-D lines n.x = c whose outward normal points against the motion)
+// and the level planes z = k*h, all relative to the sample so that the last
+// prism (the one touching the sample point) ends the walk at s = 0 exactly.
+// Gain anchor: g = N_tot (beta (sigmaE + sigmaA) - sigmaA), cladding
+// g = -claddingAbsorption (include/kernels/forward/rayWalk.hpp:170-182).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hase {
+
+constexpr uint32_t kTagRay = 0u;
+constexpr uint32_t kTagMap = 1u;
+constexpr int kMaxSteps = 10000;  // bounded walk (include/kernels/forward/policyRay.hpp:386)
+
+// ---------------------------------------------------------------- Philox ----
+// Philox4x32-10, Salmon, Moraes, Dror, Shaw, "Parallel Random Numbers: As Easy
+// as 1, 2, 3", SC'11: 10 rounds of two 32x32->64 multiplies with a Weyl key
+// schedule.
+struct Philox4 {
+    uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                          uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        if (round > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+#ifdef __CUDA_ARCH__
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        const uint64_t p0 = uint64_t(0xD2511F53u) * c0, p1 = uint64_t(0xCD9E8D57u) * c2;
+        const uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0);
+        const uint32_t hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
+#endif
+        const uint32_t n0 = hi1 ^ c1 ^ k0;
+        const uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    return Philox4{c0, c1, c2, c3};
+}
+
+// 24-bit uniform in (0,1): (k + 1/2) 2^-24, exact in FP32.
+__device__ __forceinline__ float unit24(uint32_t k24) { return (float(k24) + 0.5f) * (1.0f / 16777216.0f); }
+
+// ------------------------------------------------------------ mesh view ----
+// Packed per-triangle walk record, 3 x float4 = 48 B:
+//   r0 = (nx0, ny0, c0, nx1), r1 = (ny1, c1, nx2, ny2), r2 = (c2, nb0, nb1, nb2)
+// with nb_e = (neighbour << 2 | entry edge in the neighbour) as int bits, -1 at
+// the mesh boundary.  Start-point record, 2 x float4 = 32 B:
+//   g0 = (ax, ay, bx-ax, by-ay), g1 = (cx-ax, cy-ay, area, 0); centroid separate.
+struct MeshView {
+    const float4* tri;       // [T][3]
+    const float4* geo;       // [T][2]
+    const float2* centroid;  // [T]
+    const float* gainBeta;   // [P] beta, NaN in cladding prisms (walk)
+    const float* srcBeta;    // [P] beta (source weight)
+    const float2* points;    // [Np]
+    const float* reflect;    // [T][2] or nullptr
+    uint32_t T, layers, P, Np;
+    float h;                 // level spacing
+    float cladAbs;           // claddingAbsorption
+    float tolEnd;            // |s| below which the target is reached
+    float tolBoundary;       // boundary exits closer than this to the target end the walk
+    float tirCos2[2];        // total internal reflection when uz^2 <= tirCos2[surface]
+};
+
+__device__ __forceinline__ int floorDivI(int a, int b) {
+    int q = a / b;
+    return (q * b != a && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+__device__ __forceinline__ uint32_t physLayer(int lu, uint32_t layers) {
+    const int twoL = int(2 * layers);
+    int m = lu % twoL;
+    if (m < 0) m += twoL;
+    return m < int(layers) ? uint32_t(m) : uint32_t(twoL - 1 - m);
+}
+
+// Unfolded integer level of the image of sample level ls for reflection slice.
+__device__ __forceinline__ int imageLevel(int ls, int layers, uint32_t slice) {
+    switch (slice) {
+        case 1: return -ls;                 // bottom
+        case 2: return 2 * layers - ls;     // top
+        case 3: return ls - 2 * layers;     // bottom, then top
+        case 4: return ls + 2 * layers;     // top, then bottom
+        default: return ls;
+    }
+}
+
+__device__ __forceinline__ int expectedReflections(uint32_t slice) { return slice == 0 ? 0 : (slice <= 2 ? 1 : 2); }
+
+// Legacy reflectivity index t*2 + surface (include/core/mesh.hpp:301-332), with
+// total internal reflection above the critical angle.
+__device__ __forceinline__ float reflectFactor(const MeshView& m, uint32_t t, int surf, float uz) {
+    if (uz * uz <= m.tirCos2[surf]) return 1.0f;
+    return m.reflect ? __ldg(m.reflect + 2 * t + surf) : 0.0f;
+}
+
+// One ray in flight.
+struct Ray {
+    uint32_t t;     // triangle
+    int lu;         // unfolded layer index
+    int forb;       // entry edge (excluded exit), -1 none
+    float s;        // remaining distance to the image point
+    float G;        // accumulated ln(gain) (incl. reflection factors)
+    int refl;       // reflections so far
+    int steps;
+    float ux, uy, uz, hOverUz;
+    float Sx, Sy;
+    int kImg;       // unfolded level of the image point
+    int expected;   // reflections the slice implies
+    float A, B;     // g = beta*A - B
+};
+
+enum StepResult { kContinue = 0, kDone = 1, kDropped = 2 };
+
+// Initialise a ray from start (x,y) + z offset above the image, toward the
+// image point (Sx, Sy, kImg*h).  dzImg = z_start - z_image.
+__device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float x, float y, float dzImg, float Sx,
+                                         float Sy, int kImg, uint32_t slice, float A, float B, float h) {
+    const float dx = x - Sx, dy = y - Sy;
+    const float D2 = fmaf(dx, dx, fmaf(dy, dy, dzImg * dzImg));
+    const float D = sqrtf(D2);
+    const float inv = 1.0f / D;
+    r.t = t;
+    r.lu = layer;
+    r.forb = -1;
+    r.s = D;
+    r.G = 0.0f;
+    r.refl = 0;
+    r.steps = 0;
+    r.ux = dx * inv;
+    r.uy = dy * inv;
+    r.uz = dzImg * inv;
+    r.hOverUz = r.uz != 0.0f ? h / r.uz : 0.0f;
+    r.Sx = Sx;
+    r.Sy = Sy;
+    r.kImg = kImg;
+    r.expected = expectedReflections(slice);
+    r.A = A;
+    r.B = B;
+    return D2;
+}
+
+template <typename Loader>
+__device__ __forceinline__ int stepRay(const MeshView& m, Ray& r, Loader&& load) {
+    float4 a, b, c;
+    load(r.t, a, b, c);
+    const float nx[3] = {a.x, a.w, b.z};
+    const float ny[3] = {a.y, b.x, b.w};
+    const float cc[3] = {a.z, b.y, c.x};
+    const int nb[3] = {__float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w)};
+    float best = -INFINITY;
+    int be = -1;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const float den = fmaf(nx[e], r.ux, ny[e] * r.uy);
+        if (e != r.forb && den < 0.0f) {
+            const float num = fmaf(nx[e], r.Sx, fmaf(ny[e], r.Sy, -cc[e]));
+            float se = __fdiv_rn(num, -den);
+            se = fminf(se, r.s);
+            if (se > best) {
+                best = se;
+                be = e;
+            }
+        }
+    }
+    float sz = -INFINITY;
+    int dl = 0;
+    if (r.uz > 0.0f) {
+        sz = float(r.lu - r.kImg) * r.hOverUz;
+        dl = -1;
+    } else if (r.uz < 0.0f) {
+        sz = float(r.lu + 1 - r.kImg) * r.hOverUz;
+        dl = 1;
+    }
+    sz = fminf(sz, r.s);
+    const uint32_t phys = physLayer(r.lu, m.layers);
+    const float gb = __ldg(m.gainBeta + phys * m.T + r.t);
+    const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
+    const float next = fmaxf(fmaxf(best, sz), 0.0f);
+    if (next <= m.tolEnd) {
+        r.G = fmaf(g, r.s, r.G);
+        r.s = 0.0f;
+        return kDone;
+    }
+    r.G = fmaf(g, r.s - next, r.G);
+    r.s = next;
+    if (++r.steps >= kMaxSteps) return kDropped;
+    if (sz >= best) {
+        const int k = dl < 0 ? r.lu : r.lu + 1;
+        const int L = int(m.layers);
+        const int kd = floorDivI(k, L);
+        if (kd * L == k) {  // a physical top/bottom surface
+            if (r.refl >= r.expected) return kDropped;
+            const float R = reflectFactor(m, r.t, kd & 1, r.uz);
+            r.G += __logf(R);
+            ++r.refl;
+        }
+        r.lu += dl;
+    } else {
+        const int w = be == 0 ? nb[0] : (be == 1 ? nb[1] : nb[2]);
+        if (w < 0) return r.s <= m.tolBoundary ? kDone : kDropped;
+        r.t = uint32_t(w) >> 2;
+        r.forb = w & 3;
+    }
+    return kContinue;
+}
+
+// After kDone: a reflection the slice implies but which happens at the target
+// itself (sample on the reflecting surface) is applied in the final triangle.
+__device__ __forceinline__ void finishReflections(const MeshView& m, Ray& r) {
+    if (r.refl < r.expected) {
+        const int kd = floorDivI(r.kImg, int(m.layers));
+        r.G += __logf(reflectFactor(m, r.t, kd & 1, r.uz));
+        r.refl = r.expected;
+    }
+}
+
+struct GlobalLoader {
+    const float4* tri;
+    __device__ __forceinline__ void operator()(uint32_t t, float4& a, float4& b, float4& c) const {
+        a = __ldg(tri + 3 * t);
+        b = __ldg(tri + 3 * t + 1);
+        c = __ldg(tri + 3 * t + 2);
+    }
+};
+
+struct SharedLoader {
+    const float4* tri;  // shared-memory copy
+    __device__ __forceinline__ void operator()(uint32_t t, float4& a, float4& b, float4& c) const {
+        a = tri[3 * t];
+        b = tri[3 * t + 1];
+        c = tri[3 * t + 2];
+    }
+};
+
+}  // namespace hase

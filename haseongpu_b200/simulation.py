@@ -1,0 +1,248 @@
+"""Host front end mirroring the reference's ``PhiASE`` call surface.
+
+``PhiASE`` keeps the field names, ``run(gainMedium, crossSections)`` ->
+``self`` and ``getResults()`` -> ``Result`` of pyInclude/simulation.py:110-489,
+and ``Result`` the fields of pyInclude/structures.py:7-18.  Where the reference
+hands the medium to the ``calcPhiASE`` executable through openPMD files
+(pyInclude/openpmd/transport.py:1696-1717), this front end calls
+libhase_b200.so directly through its C ABI (include/hase_b200.h).
+
+The propagation mode is the backward, importance-sampled prism method
+(``propagationMode="backward"``); the MSE threshold is the relative standard
+error of each sample's estimate, as the legacy ``mseThreshold`` and the
+reference's ``relativeStandardErrorThreshold``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .mesh import PrismMesh
+from .spectra import CrossSectionData
+
+
+@dataclass
+class Result:
+    phiAse: np.ndarray = field(default_factory=lambda: np.empty(0, np.float32))
+    standardError: np.ndarray = field(default_factory=lambda: np.empty(0))
+    relativeStandardError: np.ndarray = field(default_factory=lambda: np.empty(0))
+    totalRays: np.ndarray = field(default_factory=lambda: np.empty(0, np.uint32))
+    dndtAse: np.ndarray = field(default_factory=lambda: np.empty(0))
+    droppedRays: np.ndarray = field(default_factory=lambda: np.empty(0, np.uint32))
+    srmStatus: str = "disabled"
+    srmPasses: int = 0
+    srmRemainingFraction: float = 0.0
+    srmMaxIterations: int = 0
+    srmDivergenceStreak: int = 0
+    raysTraced: int = 0
+    crossings: int = 0
+    importanceMilliseconds: float = 0.0
+    rayMilliseconds: float = 0.0
+    totalMilliseconds: float = 0.0
+    passes: int = 0
+    unconvergedSamples: int = 0
+    kernelLaunches: int = 0
+    status: int = 0
+
+    @property
+    def mse(self) -> np.ndarray:
+        """Legacy name of the per-sample relative standard error."""
+        return self.relativeStandardError
+
+
+class DeviceMesh:
+    """A libhase_b200 context: the mesh tables resident on one device."""
+
+    def __init__(self, mesh: PrismMesh, sigmaA, sigmaE, device: int = 0):
+        self.mesh = mesh
+        self._keep = []
+        sa = self._hold(np.atleast_1d(np.asarray(sigmaA, np.float64)))
+        se = self._hold(np.atleast_1d(np.asarray(sigmaE, np.float64)))
+        if sa.size != se.size or sa.size == 0:
+            raise ValueError("sigmaA and sigmaE must be non-empty and of equal length")
+        desc = self._mesh_desc(mesh)
+        spec = N.SpectrumDesc(sa.size, N.ptr(sa, N._f64p), N.ptr(se, N._f64p))
+        handle = C.c_void_p()
+        N.check(N.lib().hase_context_create(C.byref(desc), C.byref(spec), int(device), C.byref(handle)))
+        self.handle = handle
+        self.numberOfWavelengths = sa.size
+
+    def _hold(self, a):
+        a = np.ascontiguousarray(a)
+        self._keep.append(a)
+        return a
+
+    def _mesh_desc(self, m: PrismMesh):
+        def opt(a, t, dtype):
+            return None if a is None else N.ptr(self._hold(np.asarray(a, dtype).ravel()), t)
+
+        return N.MeshDesc(
+            m.numberOfPoints, m.numberOfTriangles, m.numberOfLevels, N.ptr(self._hold(m.points), N._f64p),
+            N.ptr(self._hold(m.triangles), N._u32p), m.thickness, N.ptr(self._hold(m.betaVolume), N._f64p),
+            opt(m.betaCells, N._f64p, np.float64), opt(m.claddingCellTypes, N._u32p, np.uint32),
+            int(m.claddingNumber), float(m.claddingAbsorption), float(m.nTot), float(m.crystalTFluo),
+            opt(m.reflectivities, N._f64p, np.float64), opt(m.refractiveIndices, N._f64p, np.float64))
+
+    def update_beta(self, betaVolume, betaCells=None):
+        bv = np.ascontiguousarray(np.asarray(betaVolume, np.float64).ravel())
+        if bv.size != self.mesh.numberOfPrisms:
+            raise ValueError("betaVolume size mismatch")
+        bc = None if betaCells is None else np.ascontiguousarray(np.asarray(betaCells, np.float64).ravel())
+        if bc is not None and bc.size != self.mesh.numberOfSamples:
+            raise ValueError("betaCells size mismatch")
+        N.check(N.lib().hase_context_update_beta(self.handle, N.ptr(bv, N._f64p), N.ptr(bc, N._f64p)))
+
+    def calc_phi_ase(self, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
+                     adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
+                     blockSize=0, workspaceBytes=0) -> Result:
+        S = self.mesh.numberOfSamples
+        maxSample = S - 1 if maxSample is None else int(maxSample)
+        n = maxSample - int(minSample) + 1
+        if n <= 0:
+            raise ValueError("empty sample range")
+        out = Result(phiAse=np.empty(n, np.float32), standardError=np.empty(n), relativeStandardError=np.empty(n),
+                     totalRays=np.empty(n, np.uint32), dndtAse=np.empty(n), droppedRays=np.empty(n, np.uint32))
+        ex = N.ExperimentDesc(int(minRays), int(maxRays if maxRays is not None else minRays), float(mseThreshold),
+                              1 if useReflections else 0, 1 if monochromatic else 0)
+        cp = N.ComputeDesc(int(adaptiveSteps), int(repetitions), int(rngSeed) & 0xFFFFFFFF, int(minSample), maxSample,
+                           int(raysPerThread), int(blockSize), int(workspaceBytes))
+        r = N.ResultDesc(N.ptr(out.phiAse, N._f32p), N.ptr(out.standardError, N._f64p),
+                         N.ptr(out.relativeStandardError, N._f64p), N.ptr(out.totalRays, N._u32p),
+                         N.ptr(out.dndtAse, N._f64p), N.ptr(out.droppedRays, N._u32p))
+        status = N.check(N.lib().hase_calc_phi_ase(self.handle, C.byref(ex), C.byref(cp), C.byref(r)),
+                         allow_warnings=True)
+        out.status = status
+        out.raysTraced = int(r.raysTraced)
+        out.crossings = int(r.crossings)
+        out.importanceMilliseconds = float(r.importanceMilliseconds)
+        out.rayMilliseconds = float(r.rayMilliseconds)
+        out.totalMilliseconds = float(r.totalMilliseconds)
+        out.passes = int(r.passes)
+        out.unconvergedSamples = int(r.unconvergedSamples)
+        out.kernelLaunches = int(r.kernelLaunches)
+        return out
+
+    def importance_weights(self, firstSample, count, useReflections=False) -> np.ndarray:
+        slices = 5 if useReflections else 1
+        w = np.empty((count, slices * self.mesh.numberOfPrisms), np.float32)
+        N.check(N.lib().hase_importance_weights(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
+                                                N.ptr(w, N._f32p)))
+        return w
+
+    def trace(self, start, tri, level, sample, slice_=None, wavelength=0):
+        start = np.ascontiguousarray(np.asarray(start, np.float32).reshape(-1, 3))
+        n = start.shape[0]
+        arrs = [np.ascontiguousarray(np.asarray(a, np.uint32).reshape(n)) for a in
+                (tri, level, sample, np.zeros(n) if slice_ is None else slice_)]
+        ln = np.empty(n, np.float32)
+        dist = np.empty(n, np.float32)
+        dropped = np.empty(n, np.uint32)
+        N.check(N.lib().hase_trace_rays(self.handle, n, N.ptr(start, N._f32p), *[N.ptr(a, N._u32p) for a in arrs],
+                                        int(wavelength), N.ptr(ln, N._f32p), N.ptr(dist, N._f32p),
+                                        N.ptr(dropped, N._u32p)))
+        return ln, dist, dropped
+
+    def close(self):
+        if getattr(self, "handle", None):
+            N.lib().hase_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+@dataclass
+class PhiASE:
+    """Configure and run the phi-ASE calculation for one gain-medium state."""
+
+    config: object | None = None
+    crossSections: CrossSectionData | None = None
+    gainMedium: PrismMesh | None = None
+    propagationMode: str = "backward"
+    minRays: int = 100000
+    maxRays: int = 100000
+    forwardRayCount: int | None = None
+    relativeStandardErrorThreshold: float = 0.1
+    repetitions: int = 4
+    adaptiveSteps: int = 4
+    useReflections: bool = False
+    reflectionMaxIterations: int = 40
+    reflectionTolerance: float = 1e-4
+    surfaceReservoirSize: int = 32
+    monochromatic: bool = False
+    backend: str | None = "cuda_sm100a"
+    parallelMode: str = "single"
+    numDevices: int = 1
+    devices: list[int] = field(default_factory=list)
+    minSampleRange: int | None = None
+    maxSampleRange: int | None = None
+    rngSeed: int | None = None
+    writeVtk: bool = False
+
+    _result: Result | None = field(default=None, init=False, repr=False)
+    _context: DeviceMesh | None = field(default=None, init=False, repr=False)
+
+    def __post_init__(self):
+        if isinstance(self.config, dict):
+            for key, value in self.config.items():
+                if key == "mseThreshold":
+                    raise ValueError("mseThreshold is named relativeStandardErrorThreshold")
+                if not hasattr(self, key):
+                    raise ValueError(f"unknown PhiASE setting '{key}'")
+                setattr(self, key, value)
+        if self.propagationMode != "backward":
+            raise ValueError("only propagationMode='backward' (importance-sampled prism method) is implemented")
+        if self.parallelMode != "single":
+            raise ValueError("parallelMode must be 'single'; use one process per GPU for replicas")
+        if self.backend not in (None, "cuda_sm100a"):
+            raise ValueError(f"unknown backend '{self.backend}'; available: cuda_sm100a")
+        if self.minRays <= 0 or self.maxRays < self.minRays and self.maxRays != 0:
+            raise ValueError("need 0 < minRays <= maxRays")
+        if self.relativeStandardErrorThreshold < 0:
+            raise ValueError("relativeStandardErrorThreshold must be >= 0")
+
+    def _device(self) -> int:
+        return int(self.devices[0]) if self.devices else 0
+
+    def run(self, gainMedium: PrismMesh | None = None, crossSections: CrossSectionData | None = None) -> "PhiASE":
+        medium = gainMedium if gainMedium is not None else self.gainMedium
+        if medium is None:
+            raise ValueError("PhiASE.run requires gainMedium")
+        spectra = crossSections if crossSections is not None else self.crossSections
+        if spectra is None:
+            raise ValueError("PhiASE.run requires crossSections")
+        sigmaA, sigmaE = spectra.resampled(self.monochromatic)
+        ctx = self._context
+        if ctx is None or ctx.mesh is not medium or ctx.numberOfWavelengths != sigmaA.size:
+            if ctx is not None:
+                ctx.close()
+            ctx = DeviceMesh(medium, sigmaA, sigmaE, device=self._device())
+            self._context = ctx
+        rays = self.forwardRayCount
+        minRays = rays if rays else self.minRays
+        maxRays = rays if rays else max(self.maxRays, self.minRays)
+        self._result = ctx.calc_phi_ase(
+            minRays=minRays, maxRays=maxRays, mseThreshold=self.relativeStandardErrorThreshold,
+            useReflections=self.useReflections, monochromatic=self.monochromatic,
+            adaptiveSteps=0 if rays else self.adaptiveSteps, repetitions=self.repetitions,
+            rngSeed=5489 if self.rngSeed is None else self.rngSeed,
+            minSample=self.minSampleRange or 0, maxSample=self.maxSampleRange)
+        return self
+
+    def getResults(self) -> Result:
+        if self._result is None:
+            raise RuntimeError("simulation has not been run yet")
+        return self._result

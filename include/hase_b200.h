@@ -1,0 +1,160 @@
+/*
+ * hase_b200.h -- C ABI of libhase_b200.so, the B200 (sm_100a) implementation
+ * of HASEonGPU's adaptive Monte Carlo phi-ASE computation on extruded
+ * triangle-prism meshes (backward, importance-sampled method).
+ *
+ * Plain C types only; no exceptions cross this boundary.  Every entry point
+ * returns a hase_status; on failure hase_last_error_message() (thread-local)
+ * says why.  One context per host thread / stream; calls on one context must
+ * be serialised by the caller.
+ *
+ * What each entry point replaces in HASEonGPU v2.2.0 (paths inside the
+ * reference project):
+ *   hase_context_create       - HostMesh construction + device upload
+ *                               (include/core/mesh.hpp:509-768,
+ *                                include/core/forwardPhiAseEvaluator.hpp:184-204)
+ *   hase_context_update_beta  - dynamic beta update without re-sending topology
+ *                               (ForwardPhiAseDeviceContext::rebuildBetaVolumePrefix,
+ *                                include/core/calcForwardPhiAse.hpp:337-380)
+ *   hase_calc_phi_ase         - hase::core::startSimulation<false>(experiment,
+ *                               compute, result, mesh)
+ *                               (include/core/simulation.hpp:42-47), i.e. the
+ *                               calcPhiASE entry point behind PhiASE.run
+ *                               (pyInclude/simulation.py:452-483)
+ *   hase_result               - hase::core::Result (include/core/types.hpp:201-246)
+ *   hase_experiment_desc      - hase::core::ExperimentParameters
+ *                               (include/core/types.hpp:248-331)
+ *   hase_compute_desc         - hase::core::ComputeParameters (adaptiveSteps,
+ *                               repetitions, rngSeed, sample range)
+ */
+#ifndef HASE_B200_H
+#define HASE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HASE_B200_ABI_VERSION 1
+
+typedef enum {
+    HASE_OK = 0,
+    HASE_INVALID_ARGUMENT = 1, /* std::invalid_argument / std::out_of_range in the reference */
+    HASE_CUDA_ERROR = 2,       /* a CUDA runtime call failed */
+    HASE_OUT_OF_MEMORY = 3,
+    HASE_DEVICE_TIMEOUT = 4,   /* a bounded device wait gave up */
+    HASE_DROPPED_RAYS = 5,     /* warning: some rays could not be walked (counted in droppedRays) */
+    HASE_NOT_CONVERGED = 6,    /* warning: some samples stayed above the MSE threshold at maxRays */
+    HASE_NO_DEVICE = 7         /* no CUDA device (the reference returns non-zero when no backend matched) */
+} hase_status;
+
+typedef struct hase_context hase_context;
+
+/* Extruded triangle-prism gain medium (legacy HASEonGPU mesh layout).
+ * Prism (triangle t, layer l) has index t + l * numberOfTriangles; sample
+ * point (point p, level l) has index p + l * numberOfPoints. */
+typedef struct {
+    uint32_t numberOfPoints;            /* 2-D mesh points */
+    uint32_t numberOfTriangles;         /* T */
+    uint32_t numberOfLevels;            /* z levels (>= 2); layers = levels - 1 */
+    const double* points;               /* [numberOfPoints][2] x, y (cm) */
+    const uint32_t* triangles;          /* [T][3] point indices */
+    double thickness;                   /* level spacing (cm) */
+    const double* betaVolume;           /* [levels-1][T] excited fraction per prism */
+    const double* betaCells;            /* [levels][numberOfPoints] per sample point (dndt only); may be NULL */
+    const uint32_t* claddingCellTypes;  /* [T] or NULL */
+    uint32_t claddingNumber;            /* triangles with this type are cladding */
+    double claddingAbsorption;          /* cladding absorption coefficient (cm^-1) */
+    double nTot;                        /* doping density (cm^-3) */
+    double crystalTFluo;                /* fluorescence lifetime (s) */
+    const double* reflectivities;       /* [T][2]: t*2+0 bottom, t*2+1 top; NULL = 0 */
+    const double* refractiveIndices;    /* [4]: bottom inside, bottom outside, top inside, top outside; NULL = 1 */
+} hase_mesh_desc;
+
+typedef struct {
+    uint32_t numberOfWavelengths;       /* >= 1 */
+    const double* sigmaA;               /* absorption cross sections (cm^2) */
+    const double* sigmaE;               /* emission cross sections (cm^2) */
+} hase_spectrum_desc;
+
+typedef struct {
+    uint32_t minRays;                   /* rays per sample in the first pass */
+    uint32_t maxRays;                   /* cap of the adaptive schedule */
+    double mseThreshold;                /* stop when the relative standard error <= this */
+    uint32_t useReflections;            /* 0/1: top/bottom reflections of order <= 2 */
+    uint32_t monochromatic;             /* 1: use only the first (sigmaA, sigmaE) pair */
+} hase_experiment_desc;
+
+typedef struct {
+    uint32_t adaptiveSteps;             /* geometric ray-target increases minRays -> maxRays */
+    uint32_t repetitions;               /* accepted for interface compatibility (passes pool their rays) */
+    uint32_t rngSeed;
+    uint32_t minSample;                 /* inclusive */
+    uint32_t maxSample;                 /* inclusive; UINT32_MAX = last sample */
+    uint32_t raysPerThread;             /* 0 = default / autotuned */
+    uint32_t blockSize;                 /* 0 = default / autotuned */
+    uint64_t workspaceBytes;            /* 0 = default device workspace budget */
+} hase_compute_desc;
+
+/* Caller-allocated host arrays of (maxSample - minSample + 1) entries; any
+ * pointer may be NULL to skip that output. */
+typedef struct {
+    float* phiAse;
+    double* standardError;
+    double* relativeStandardError;      /* the legacy "mse" */
+    uint32_t* totalRays;
+    double* dndtAse;
+    uint32_t* droppedRays;
+    /* scalar outputs */
+    uint64_t raysTraced;
+    uint64_t crossings;                 /* prism crossings walked by the ray kernel */
+    double importanceMilliseconds;      /* device time, CUDA events */
+    double rayMilliseconds;
+    double totalMilliseconds;
+    uint32_t passes;
+    uint32_t unconvergedSamples;
+    uint32_t kernelLaunches;            /* kernels this call launched */
+} hase_result;
+
+const char* hase_last_error_message(void);
+const char* hase_status_string(hase_status status);
+int hase_abi_version(void);
+
+hase_status hase_context_create(const hase_mesh_desc* mesh, const hase_spectrum_desc* spectrum, int device,
+                                hase_context** out);
+hase_status hase_context_update_beta(hase_context* ctx, const double* betaVolume, const double* betaCells);
+hase_status hase_calc_phi_ase(hase_context* ctx, const hase_experiment_desc* experiment,
+                              const hase_compute_desc* compute, hase_result* result);
+hase_status hase_context_destroy(hase_context* ctx);
+
+/* ---- kernel-level entry points (the four hot-path kernels, one at a time) ----
+ * Used by the parity tests and the benchmark; no reference counterpart beyond
+ * the kernels they expose (importance weights, ray->prism map, ray walk). */
+
+/* Normalised importance weights (max 1) for samples [firstSample, firstSample+count):
+ * weights[i][j*P + p] for reflection slice j (slices = 5 with reflections, else 1). */
+hase_status hase_importance_weights(hase_context* ctx, uint32_t firstSample, uint32_t count,
+                                    uint32_t useReflections, float* weights);
+
+/* Ray->prism map of `rows` weight rows of length n: q[row][n] (quantised
+ * weights), offsets[row][n+1] (exclusive ray offsets), Q[row]. */
+hase_status hase_ray_map(uint32_t rows, uint32_t n, const float* weights, uint32_t rays, const uint32_t* phases,
+                         uint32_t* q, uint32_t* offsets, uint64_t* Q);
+
+/* ln(gain) and distance of explicit rays from start[i] (x,y,z) in prism
+ * (tri[i], level[i]) to sample[i] through reflection slice[i] at wavelength
+ * index `wavelength`. dropped[i] = 1 if the walk failed. */
+hase_status hase_trace_rays(hase_context* ctx, uint32_t n, const float* start, const uint32_t* tri,
+                            const uint32_t* level, const uint32_t* sample, const uint32_t* slice,
+                            uint32_t wavelength, float* lnGain, float* distance, uint32_t* dropped);
+
+/* Philox4x32-10 on the device: out[i] = philox(ctr[i], key). */
+hase_status hase_philox(uint32_t n, const uint32_t* ctr, const uint32_t key[2], uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HASE_B200_H */

@@ -1,0 +1,111 @@
+/*
+ * hase_oracle.h -- CPU (FP64, OpenMP) restatement of HASEonGPU's backward,
+ * importance-sampled prism phi-ASE method.  TEST INFRASTRUCTURE ONLY: the
+ * product library never links or calls this code; tests, smoke() and the CPU
+ * baseline leg of bench.py use it as the checker.
+ *
+ * The reference (HASEonGPU v2.2.0) retired the backward prism kernels; this
+ * restatement follows the method as published (Eckert et al., Comput. Phys.
+ * Commun. 207 (2016) 362) and the anchors that survive in the reference tree:
+ *   - prism tables:        pyInclude/geometry/core.py:670-774
+ *   - gain coefficient:    include/kernels/forward/rayWalk.hpp:170-182
+ *   - cladding segments:   tests/data/laserPumpCladding/true_cladding_no_reflection_phiase_reference/README.md:27-33
+ *   - legacy reflectivity index (cell*2 + face%2): include/core/mesh.hpp:301-332
+ *   - adaptive ray target: include/core/types.hpp:333-354
+ *   - dndt = (beta*(sigmaE+sigmaA) - sigmaA) * phi: include/core/forwardPhiAseUtilities.hpp:16-25
+ *   - golden outputs:      tests/data/compareSerial/phiase_reference.npz,
+ *                          tests/data/laserPumpCladding/true_cladding_no_reflection_phiase_reference/phiase_reference.npz
+ * Parity is pinned against those golden outputs by tests/test_oracle_golden.py.
+ */
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    uint32_t numberOfPoints;      /* 2-D mesh points */
+    uint32_t numberOfTriangles;   /* T */
+    uint32_t numberOfLevels;      /* z levels; prisms = T * (levels - 1) */
+    const double* points;         /* [numberOfPoints][2] x, y */
+    const uint32_t* triangles;    /* [T][3] */
+    double thickness;             /* level spacing h */
+    const double* betaVolume;     /* [levels-1][T]: prism = t + level * T */
+    const double* betaCells;      /* [levels][numberOfPoints] (dndt only), may be NULL */
+    const uint32_t* claddingCellTypes; /* [T] or NULL */
+    uint32_t claddingNumber;
+    double claddingAbsorption;
+    double nTot;
+    double crystalTFluo;
+    const double* reflectivities; /* [T][2]: t*2 + 0 bottom, t*2 + 1 top; NULL = 0 */
+    const double* refractiveIndices; /* [4]: bottom in/out, top in/out; NULL = 1 */
+} oracle_mesh;
+
+typedef struct {
+    uint32_t numberOfWavelengths;
+    const double* sigmaA;
+    const double* sigmaE;
+} oracle_spectrum;
+
+typedef struct {
+    uint32_t minRays;
+    uint32_t maxRays;
+    uint32_t adaptiveSteps;
+    double mseThreshold;
+    uint32_t useReflections;      /* 0/1: top/bottom reflections of order <= 2 */
+    uint32_t seed;
+    uint32_t minSample;           /* inclusive */
+    uint32_t maxSample;           /* inclusive */
+} oracle_experiment;
+
+typedef struct {
+    double* phiAse;       /* [nSamples] */
+    double* mse;          /* relative standard error of phiAse */
+    uint32_t* totalRays;
+    double* dndtAse;
+    uint32_t* droppedRays;
+    double* gainSum;      /* sum of per-ray contributions (FP64) */
+    double* gainSumSquare;
+} oracle_result;
+
+/* Philox4x32-10 (Salmon et al., SC'11): out = philox(ctr, key). */
+void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Per-triangle tables (row-major [t][e]); edge e runs from vertex e to e+1.
+ * normals are outward unit normals, c = n . (edge start point). */
+int oracle_build_tables(uint32_t numberOfPoints, const double* points, uint32_t numberOfTriangles,
+                        const uint32_t* triangles, int32_t* neighbors, int32_t* forbiddenEdge,
+                        double* normalX, double* normalY, double* edgeC, double* centerX,
+                        double* centerY, double* area);
+
+/* ln(gain) of straight rays from start (x,y,z) in prism (tri, level) to sample
+ * point `sample` (index point + level * numberOfPoints) through reflection
+ * slice `slice` (0 direct, 1 bottom, 2 top, 3 bottom+top, 4 top+bottom),
+ * for wavelength `wavelength`.  Reflection factors are included; a zero
+ * reflectivity yields -inf.  dropped[i] = 1 when the walk failed. */
+int oracle_trace(const oracle_mesh* mesh, const oracle_spectrum* spectrum, uint32_t wavelength,
+                 uint32_t n, const double* start, const uint32_t* tri, const uint32_t* level,
+                 const uint32_t* sample, const uint32_t* slice, double* lnGain, double* distance,
+                 uint32_t* dropped);
+
+/* Importance weights w[slice*P + prism] for one sample. */
+int oracle_importance(const oracle_mesh* mesh, const oracle_spectrum* spectrum, uint32_t sample,
+                      uint32_t slices, double* weights);
+
+/* Integer ray->prism map from weights: q = ceil(w * 2^24 / max w) (0 for w <= 0),
+ * Q = sum q, offsets[b] = floor((C_b * N * 2^32 + phase * Q) / (Q * 2^32)),
+ * C_b the exclusive prefix sum of q.  Returns Q (0 if all weights vanish). */
+uint64_t oracle_ray_map(uint32_t n, const float* weights, uint32_t rays, uint32_t phase,
+                        uint32_t* q, uint32_t* offsets);
+
+/* Full adaptive method over samples [minSample, maxSample].
+ * weightsOverride: NULL, or [nSamples][slices*P] FP32 importance weights
+ * (lets tests replay the GPU's weights so both walk identical rays). */
+int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum,
+                   const oracle_experiment* experiment, const float* weightsOverride,
+                   int threads, oracle_result* result);
+
+#ifdef __cplusplus
+}
+#endif
