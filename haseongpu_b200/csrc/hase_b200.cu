@@ -474,8 +474,11 @@ __global__ void __launch_bounds__(128) finalizeKernel(FinalizeLaunch L) {
         const double rse = mean > 0.0 ? sqrt(fabs(sum2 / double(N) - mean * mean) / double(N)) / mean : 0.0;
         L.phi[row] = float(mean);
         L.mse[row] = rse;
-        const bool again = !(rse <= L.threshold);
-        if (again && !L.last) L.nextActive[atomicAdd(L.nextCount, 1u)] = row;
+        // Above the threshold: queue for the next pass, or (last pass) just count.
+        if (!(rse <= L.threshold)) {
+            const uint32_t slot = atomicAdd(L.nextCount, 1u);
+            if (!L.last) L.nextActive[slot] = row;
+        }
     }
 }
 
@@ -661,7 +664,6 @@ struct hase_context {
         v.h = float(h);
         v.cladAbs = float(cladAbs);
         v.tolEnd = float(4e-6 * extent);
-        v.tolBoundary = float(1e-4 * extent);
         v.tirCos2[0] = tirCos2[0];
         v.tirCos2[1] = tirCos2[1];
         return v;

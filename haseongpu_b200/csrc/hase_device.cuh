@@ -77,7 +77,6 @@ struct MeshView {
     float h;                 // level spacing
     float cladAbs;           // claddingAbsorption
     float tolEnd;            // |s| below which the target is reached
-    float tolBoundary;       // boundary exits closer than this to the target end the walk
     float tirCos2[2];        // total internal reflection when uz^2 <= tirCos2[surface]
 };
 
@@ -172,7 +171,9 @@ __device__ __forceinline__ int stepRay(const MeshView& m, Ray& r, Loader&& load)
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
         const float den = fmaf(nx[e], r.ux, ny[e] * r.uy);
-        if (e != r.forb && den < 0.0f) {
+        // Boundary edges are never exits: the 2-D mesh is convex and the
+        // target lies in it, so only rounding could route a ray across one.
+        if (e != r.forb && den < 0.0f && nb[e] >= 0) {
             const float num = fmaf(nx[e], r.Sx, fmaf(ny[e], r.Sy, -cc[e]));
             float se = __fdiv_rn(num, -den);
             se = fminf(se, r.s);
@@ -217,7 +218,6 @@ __device__ __forceinline__ int stepRay(const MeshView& m, Ray& r, Loader&& load)
         r.lu += dl;
     } else {
         const int w = be == 0 ? nb[0] : (be == 1 ? nb[1] : nb[2]);
-        if (w < 0) return r.s <= m.tolBoundary ? kDone : kDropped;
         r.t = uint32_t(w) >> 2;
         r.forb = w & 3;
     }

@@ -224,6 +224,7 @@ Walk walk(const Model& md, double x0, double y0, double z0, uint32_t t, uint32_t
             if (e == forbidden) continue;
             const double den = tb.nx[3 * t + e] * ux + tb.ny[3 * t + e] * uy;
             if (!(den < 0.0)) continue;
+            if (tb.nbr[3 * t + e] < 0) continue;  // convex mesh: boundary edges are never exits
             double se = (tb.nx[3 * t + e] * Sx + tb.ny[3 * t + e] * Sy - tb.c[3 * t + e]) / (-den);
             if (se > s) se = s;
             if (se > best) { best = se; bestEdge = e; }
@@ -256,10 +257,6 @@ Walk walk(const Model& md, double x0, double y0, double z0, uint32_t t, uint32_t
             lu += dl;
         } else {
             const int32_t n = tb.nbr[3 * t + bestEdge];
-            if (n < 0) {  // left the (convex) mesh before reaching the target
-                w.dropped = true;
-                break;
-            }
             forbidden = tb.forb[3 * t + bestEdge];
             t = uint32_t(n);
         }
