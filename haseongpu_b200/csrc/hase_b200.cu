@@ -67,6 +67,7 @@ hase_status fail(hase_status st, const char* fmt, ...) {
 
 constexpr uint32_t kRayBlock = 256;
 constexpr uint32_t kRaysPerThread = 8;
+constexpr int kRefill = 8;  // idle lanes that trigger a batched refill
 constexpr uint32_t kMaxChunks = 256;
 constexpr uint32_t kMapBlock = 1024;
 constexpr uint32_t kOffCap = 4096;
@@ -142,12 +143,12 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     const float2 c = __ldg(m.centroid + t);
     const float area = __ldg(&m.geo[2 * t + 1].z);
     Ray r;
-    const float D2 = initRay(r, t, int(l), c.x, c.y, (float(int(l) - kImg) + 0.5f) * m.h, S.x, S.y, kImg, j, L.A,
+    const float D2 = initRay(r, t, int(l), c.x - S.x, c.y - S.y, (float(int(l) - kImg) + 0.5f) * m.h, kImg, j, L.A,
                              L.B, m.h);
     GlobalLoader load{m.tri};
     int st;
     do {
-        st = stepRay(m, r, load);
+        st = stepRay(m, S.x, S.y, r, load);
     } while (st == kContinue);
     if (st == kDropped || !(D2 > 0.0f)) {
         *out = -INFINITY;
@@ -282,7 +283,7 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
     return lo;
 }
 
-template <int BLOCK, int RPT>
+template <int BLOCK, int RPT, int REFILL>
 __global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
     __shared__ uint32_t sOff[kOffCap + 1];
     __shared__ uint32_t sRange[2];
@@ -342,9 +343,14 @@ __global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
         Ray ray;
         float wf = 0.0f;
         while (true) {
-            const unsigned need = __ballot_sync(0xffffffffu, !active);
-            if (need && fetch < wEnd) {
-                const uint32_t r = fetch + __popc(need & laneLt);
+            // Lanes whose ray finished take new rays together, once enough of
+            // them are idle (or no ray is left in flight), so the start-point
+            // code runs with most of the warp.
+            const unsigned idle = __ballot_sync(0xffffffffu, !active);
+            const int nIdle = __popc(idle);
+            if (fetch >= wEnd && nIdle == 32) break;
+            if (fetch < wEnd && (nIdle >= REFILL || nIdle == 32)) {
+                const uint32_t r = fetch + __popc(idle & laneLt);
                 if (!active && r < wEnd) {
                     const uint32_t b = staged ? pb + upperBound(sOff, count, r) - 1u
                                               : pb + upperBound(off + pb, count, r) - 1u;
@@ -364,19 +370,18 @@ __global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
                     const uint32_t lam =
                         L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
                     const float2 ab = __ldg(L.spec + lam);
-                    const float D2 = initRay(ray, t, int(l), x, y, (float(int(l) - kImg) + u3) * m.h, S.x, S.y, kImg,
+                    const float D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg,
                                              j, ab.x, ab.y, m.h);
                     wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
                     active = D2 > 0.0f;
                     if (!active) ++dropped;  // start point on the sample point itself
                 }
-                fetch += __popc(need);
+                fetch += uint32_t(nIdle);
             }
-            if (__ballot_sync(0xffffffffu, active) == 0u) break;
             if (active) {
-                const int st = stepRay(m, ray, load);
-                ++crossings;
+                const int st = stepRay(m, S.x, S.y, ray, load);
                 if (st != kContinue) {
+                    crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {
                         finishReflections(m, ray);
                         const double X = CQ * double(wf) * exp(double(ray.G));
@@ -513,12 +518,12 @@ __global__ void traceKernel(TraceLaunch L) {
     const int kImg = imageLevel(ls, int(m.layers), j);
     const float zImgOffset = float(kImg) * m.h;
     Ray r;
-    const float D2 = initRay(r, L.tri[i], int(L.level[i]), L.start[3 * i], L.start[3 * i + 1],
-                             L.start[3 * i + 2] - zImgOffset, S.x, S.y, kImg, j, L.A, L.B, m.h);
+    const float D2 = initRay(r, L.tri[i], int(L.level[i]), L.start[3 * i] - S.x, L.start[3 * i + 1] - S.y,
+                             L.start[3 * i + 2] - zImgOffset, kImg, j, L.A, L.B, m.h);
     GlobalLoader load{m.tri};
     int st;
     do {
-        st = stepRay(m, r, load);
+        st = stepRay(m, S.x, S.y, r, load);
     } while (st == kContinue);
     if (st == kDone) finishReflections(m, r);
     L.lnGain[i] = r.G;
@@ -934,7 +939,7 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
             HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
             RayLaunch rl{mv, cur, firstSample, pass, M, perChunk, nW, c->q.p, c->Q.p, c->offsets.p, cp->rngSeed, 0u,
                          c->spec.p, nLambda, C, c->pSum.p, c->pSum2.p, c->pDrop.p, c->pCross.p};
-            rayKernel<kRayBlock, kRaysPerThread><<<dim3(chunks, nActive), kRayBlock, 0, c->stream>>>(rl);
+            rayKernel<kRayBlock, kRaysPerThread, kRefill><<<dim3(chunks, nActive), kRayBlock, 0, c->stream>>>(rl);
             HASE_CUDA(cudaGetLastError());
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));

@@ -80,18 +80,6 @@ struct MeshView {
     float tirCos2[2];        // total internal reflection when uz^2 <= tirCos2[surface]
 };
 
-__device__ __forceinline__ int floorDivI(int a, int b) {
-    int q = a / b;
-    return (q * b != a && ((a < 0) != (b < 0))) ? q - 1 : q;
-}
-
-__device__ __forceinline__ uint32_t physLayer(int lu, uint32_t layers) {
-    const int twoL = int(2 * layers);
-    int m = lu % twoL;
-    if (m < 0) m += twoL;
-    return m < int(layers) ? uint32_t(m) : uint32_t(twoL - 1 - m);
-}
-
 // Unfolded integer level of the image of sample level ls for reflection slice.
 __device__ __forceinline__ int imageLevel(int ls, int layers, uint32_t slice) {
     switch (slice) {
@@ -112,91 +100,85 @@ __device__ __forceinline__ float reflectFactor(const MeshView& m, uint32_t t, in
     return m.reflect ? __ldg(m.reflect + 2 * t + surf) : 0.0f;
 }
 
-// One ray in flight.
+// One ray in flight.  The walk runs in the unfolded z coordinate (reflection
+// images); `phys` is the physical layer of the current unfolded layer and
+// `pdir` the sign mapping unfolded to physical layer steps (it flips at every
+// reflection), so no division or modulo is needed per crossing.
 struct Ray {
     uint32_t t;     // triangle
     int lu;         // unfolded layer index
+    int phys;       // physical layer of `lu`
+    int pdir;       // +1 / -1
     int forb;       // entry edge (excluded exit), -1 none
-    float s;        // remaining distance to the image point
-    float G;        // accumulated ln(gain) (incl. reflection factors)
-    int refl;       // reflections so far
+    int reflLeft;   // reflections the slice still implies
+    int zoff;       // level-plane offset: exit plane of layer lu is (lu + zoff) h above the image
     int steps;
-    float ux, uy, uz, hOverUz;
-    float Sx, Sy;
-    int kImg;       // unfolded level of the image point
-    int expected;   // reflections the slice implies
+    float s;        // remaining distance to the image point
+    float G;        // accumulated ln(gain), including reflection factors
+    float ux, uy, uz;
+    float hOverUz;  // h / uz
     float A, B;     // g = beta*A - B
 };
 
 enum StepResult { kContinue = 0, kDone = 1, kDropped = 2 };
 
-// Initialise a ray from start (x,y) + z offset above the image, toward the
-// image point (Sx, Sy, kImg*h).  dzImg = z_start - z_image.
-__device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float x, float y, float dzImg, float Sx,
-                                         float Sy, int kImg, uint32_t slice, float A, float B, float h) {
-    const float dx = x - Sx, dy = y - Sy;
-    const float D2 = fmaf(dx, dx, fmaf(dy, dy, dzImg * dzImg));
+// Initialise a ray from the start point, given as its offset (dx, dy, dz)
+// from the image point (Sx, Sy, kImg*h), in physical layer `layer`.
+// Returns |start - image|^2.
+__device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx, float dy, float dz, int kImg,
+                                         uint32_t slice, float A, float B, float h) {
+    if (dz == 0.0f) dz = 1e-6f * h;  // a ray inside a level plane: nudge it off the plane
+    const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const float D = sqrtf(D2);
     const float inv = 1.0f / D;
     r.t = t;
     r.lu = layer;
+    r.phys = layer;
+    r.pdir = 1;
     r.forb = -1;
+    r.reflLeft = expectedReflections(slice);
+    r.steps = 0;
     r.s = D;
     r.G = 0.0f;
-    r.refl = 0;
-    r.steps = 0;
     r.ux = dx * inv;
     r.uy = dy * inv;
-    r.uz = dzImg * inv;
-    r.hOverUz = r.uz != 0.0f ? h / r.uz : 0.0f;
-    r.Sx = Sx;
-    r.Sy = Sy;
-    r.kImg = kImg;
-    r.expected = expectedReflections(slice);
+    r.uz = dz * inv;
+    r.hOverUz = h / r.uz;
+    // moving toward the image: down (dl = -1) when uz > 0, up (dl = +1) otherwise
+    r.zoff = (r.uz > 0.0f ? 0 : 1) - kImg;
     r.A = A;
     r.B = B;
     return D2;
 }
 
+// One crossing.  Edge exits are compared as fractions num/den by cross
+// multiplication; one approximate division gives the chosen exit parameter.
 template <typename Loader>
-__device__ __forceinline__ int stepRay(const MeshView& m, Ray& r, Loader&& load) {
+__device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
     float4 a, b, c;
     load(r.t, a, b, c);
-    const float nx[3] = {a.x, a.w, b.z};
-    const float ny[3] = {a.y, b.x, b.w};
-    const float cc[3] = {a.z, b.y, c.x};
-    const int nb[3] = {__float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w)};
-    float best = -INFINITY;
-    int be = -1;
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-        const float den = fmaf(nx[e], r.ux, ny[e] * r.uy);
+    float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
+    int bw = -1;
+    const auto edge = [&](float nx, float ny, float cc, int nbw, int e) {
+        const float dd = -fmaf(nx, r.ux, ny * r.uy);       // > 0: moving out through e
+        const float nm = fmaf(nx, Sx, fmaf(ny, Sy, -cc));  // signed distance of the sample from the edge line
         // Boundary edges are never exits: the 2-D mesh is convex and the
         // target lies in it, so only rounding could route a ray across one.
-        if (e != r.forb && den < 0.0f && nb[e] >= 0) {
-            const float num = fmaf(nx[e], r.Sx, fmaf(ny[e], r.Sy, -cc[e]));
-            float se = __fdiv_rn(num, -den);
-            se = fminf(se, r.s);
-            if (se > best) {
-                best = se;
-                be = e;
-            }
+        const bool ok = (e != r.forb) & (dd > 0.0f) & (nbw >= 0);
+        if (ok && nm * bd > bn * dd) {
+            bn = nm;
+            bd = dd;
+            bw = nbw;
         }
-    }
-    float sz = -INFINITY;
-    int dl = 0;
-    if (r.uz > 0.0f) {
-        sz = float(r.lu - r.kImg) * r.hOverUz;
-        dl = -1;
-    } else if (r.uz < 0.0f) {
-        sz = float(r.lu + 1 - r.kImg) * r.hOverUz;
-        dl = 1;
-    }
-    sz = fminf(sz, r.s);
-    const uint32_t phys = physLayer(r.lu, m.layers);
-    const float gb = __ldg(m.gainBeta + phys * m.T + r.t);
+    };
+    edge(a.x, a.y, a.z, __float_as_int(c.y), 0);
+    edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
+    edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
+    const float sEdge = fminf(__fdividef(bn, bd), r.s);
+    const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
+    const float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
     const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
-    const float next = fmaxf(fmaxf(best, sz), 0.0f);
+    const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
     if (next <= m.tolEnd) {
         r.G = fmaf(g, r.s, r.G);
         r.s = 0.0f;
@@ -205,32 +187,32 @@ __device__ __forceinline__ int stepRay(const MeshView& m, Ray& r, Loader&& load)
     r.G = fmaf(g, r.s - next, r.G);
     r.s = next;
     if (++r.steps >= kMaxSteps) return kDropped;
-    if (sz >= best) {
-        const int k = dl < 0 ? r.lu : r.lu + 1;
-        const int L = int(m.layers);
-        const int kd = floorDivI(k, L);
-        if (kd * L == k) {  // a physical top/bottom surface
-            if (r.refl >= r.expected) return kDropped;
-            const float R = reflectFactor(m, r.t, kd & 1, r.uz);
-            r.G += __logf(R);
-            ++r.refl;
+    if (sz >= sEdge) {
+        const int dl = r.uz > 0.0f ? -1 : 1;
+        const int cand = r.phys + r.pdir * dl;
+        if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+            if (r.reflLeft <= 0) return kDropped;
+            r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
+            --r.reflLeft;
+            r.pdir = -r.pdir;
+        } else {
+            r.phys = cand;
         }
         r.lu += dl;
     } else {
-        const int w = be == 0 ? nb[0] : (be == 1 ? nb[1] : nb[2]);
-        r.t = uint32_t(w) >> 2;
-        r.forb = w & 3;
+        r.t = uint32_t(bw) >> 2;
+        r.forb = bw & 3;
     }
     return kContinue;
 }
 
 // After kDone: a reflection the slice implies but which happens at the target
-// itself (sample on the reflecting surface) is applied in the final triangle.
+// itself (a sample on the reflecting surface) is applied in the final triangle.
 __device__ __forceinline__ void finishReflections(const MeshView& m, Ray& r) {
-    if (r.refl < r.expected) {
-        const int kd = floorDivI(r.kImg, int(m.layers));
-        r.G += __logf(reflectFactor(m, r.t, kd & 1, r.uz));
-        r.refl = r.expected;
+    if (r.reflLeft > 0) {
+        const int cand = r.phys + r.pdir * (r.uz > 0.0f ? -1 : 1);
+        r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
+        r.reflLeft = 0;
     }
 }
 
