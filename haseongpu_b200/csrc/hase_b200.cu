@@ -70,7 +70,6 @@ constexpr uint32_t kRaysPerThread = 8;
 constexpr int kRefill = 8;  // idle lanes that trigger a batched refill
 constexpr uint32_t kMaxChunks = 256;
 constexpr uint32_t kMapBlock = 1024;
-constexpr uint32_t kOffCap = 4096;
 constexpr double kPi = 3.14159265358979323846;
 
 // ------------------------------------------------------------ reductions ----
@@ -284,9 +283,8 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 }
 
 template <int BLOCK, int RPT, int REFILL>
-__global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
-    __shared__ uint32_t sOff[kOffCap + 1];
-    __shared__ uint32_t sRange[2];
+__global__ void __launch_bounds__(BLOCK, 5) rayKernel(RayLaunch L) {
+    __shared__ uint32_t sNextBatch;
     __shared__ double sRedD[2][BLOCK / 32];
     __shared__ uint32_t sRedU[BLOCK / 32];
     __shared__ unsigned long long sRedL[BLOCK / 32];
@@ -324,77 +322,82 @@ __global__ void __launch_bounds__(BLOCK) rayKernel(RayLaunch L) {
     uint32_t dropped = 0;
     unsigned long long crossings = 0;
 
-    for (uint32_t sub = r0; sub < r1; sub += BLOCK * RPT) {
-        const uint32_t subEnd = min(sub + BLOCK * RPT, r1);
-        if (threadIdx.x == 0) sRange[0] = upperBound(off, nW + 1, sub) - 1u;
-        if (threadIdx.x == 32) sRange[1] = upperBound(off, nW + 1, subEnd - 1u) - 1u;
-        __syncthreads();
-        const uint32_t pb = sRange[0], pe = sRange[1];
-        const uint32_t count = pe - pb + 2u;  // offsets pb .. pe+1
-        const bool staged = count <= kOffCap + 1;
-        if (staged)
-            for (uint32_t i = threadIdx.x; i < count; i += BLOCK) sOff[i] = off[pb + i];
-        __syncthreads();
-
-        const uint32_t wBegin = sub + uint32_t(warp) * 32u * RPT;
-        const uint32_t wEnd = min(wBegin + 32u * RPT, subEnd);
-        uint32_t fetch = wBegin;
-        bool active = false;
-        Ray ray;
-        float wf = 0.0f;
-        while (true) {
-            // Lanes whose ray finished take new rays together, once enough of
-            // them are idle (or no ray is left in flight), so the start-point
-            // code runs with most of the warp.
-            const unsigned idle = __ballot_sync(0xffffffffu, !active);
-            const int nIdle = __popc(idle);
-            if (fetch >= wEnd && nIdle == 32) break;
-            if (fetch < wEnd && (nIdle >= REFILL || nIdle == 32)) {
-                const uint32_t r = fetch + __popc(idle & laneLt);
-                if (!active && r < wEnd) {
-                    const uint32_t b = staged ? pb + upperBound(sOff, count, r) - 1u
-                                              : pb + upperBound(off + pb, count, r) - 1u;
-                    const uint32_t j = b / m.P, p = b - j * m.P;
-                    const uint32_t t = p % m.T, l = p / m.T;
-                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
-                    uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
-                    if (k1 + k2 + 1u > (1u << 24)) {
-                        k1 = (1u << 24) - 1u - k1;
-                        k2 = (1u << 24) - 1u - k2;
-                    }
-                    const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
-                    const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
-                    const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
-                    const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
-                    const int kImg = imageLevel(ls, int(m.layers), j);
-                    const uint32_t lam =
-                        L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
-                    const float2 ab = __ldg(L.spec + lam);
-                    const float D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg,
-                                             j, ab.x, ab.y, m.h);
-                    wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
-                    active = D2 > 0.0f;
-                    if (!active) ++dropped;  // start point on the sample point itself
-                }
-                fetch += uint32_t(nIdle);
-            }
-            if (active) {
-                const int st = stepRay(m, S.x, S.y, ray, load);
-                if (st != kContinue) {
-                    crossings += uint32_t(ray.steps) + 1u;
-                    if (st == kDone) {
-                        finishReflections(m, ray);
-                        const double X = CQ * double(wf) * exp(double(ray.G));
-                        sum += X;
-                        sum2 += X * X;
-                    } else {
-                        ++dropped;
-                    }
-                    active = false;
-                }
+    // Warps pull batches of 32*RPT consecutive rays of this chunk from a
+    // shared counter and chain them without block barriers: a lane whose ray
+    // ends takes the next ray of the current batch, and a new batch is
+    // fetched as soon as the current one is handed out.
+    if (threadIdx.x == 0) sNextBatch = 0u;
+    __syncthreads();
+    constexpr uint32_t kBatch = 32u * RPT;
+    const uint32_t nBatches = r1 > r0 ? (r1 - r0 + kBatch - 1) / kBatch : 0u;
+    uint32_t fetch = 0, wEnd = 0;  // rays [fetch, wEnd) of the current batch are still to hand out
+    uint32_t pb = 0, count = 0;    // the batch's rays lie in prisms [pb, pb + count - 1)
+    bool more = true, active = false;
+    Ray ray;
+    float wf = 0.0f;
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, !active);
+        const int nIdle = __popc(idle);
+        if (fetch >= wEnd && more && (nIdle >= REFILL || nIdle == 32)) {
+            uint32_t batch = 0;
+            if (lane == 0) batch = atomicAdd(&sNextBatch, 1u);
+            batch = __shfl_sync(0xffffffffu, batch, 0);
+            if (batch >= nBatches) {
+                more = false;
+            } else {
+                fetch = r0 + batch * kBatch;
+                wEnd = min(fetch + kBatch, r1);
+                uint32_t bound = 0;
+                if (lane == 0) bound = upperBound(off, nW + 1, fetch) - 1u;
+                if (lane == 1) bound = upperBound(off, nW + 1, wEnd - 1u) - 1u;
+                pb = __shfl_sync(0xffffffffu, bound, 0);
+                count = __shfl_sync(0xffffffffu, bound, 1) - pb + 2u;  // offsets pb .. pe+1
             }
         }
-        __syncthreads();
+        if (!more && nIdle == 32) break;
+        if (fetch < wEnd && (nIdle >= REFILL || nIdle == 32)) {
+            const uint32_t r = fetch + __popc(idle & laneLt);
+            if (!active && r < wEnd) {
+                const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
+                const uint32_t j = b / m.P, p = b - j * m.P;
+                const uint32_t t = p % m.T, l = p / m.T;
+                const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
+                uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
+                if (k1 + k2 + 1u > (1u << 24)) {
+                    k1 = (1u << 24) - 1u - k1;
+                    k2 = (1u << 24) - 1u - k2;
+                }
+                const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
+                const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
+                const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
+                const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
+                const int kImg = imageLevel(ls, int(m.layers), j);
+                const uint32_t lam =
+                    L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
+                const float2 ab = __ldg(L.spec + lam);
+                const float D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg,
+                                         j, ab.x, ab.y, m.h);
+                wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
+                active = D2 > 0.0f;
+                if (!active) ++dropped;  // start point on the sample point itself
+            }
+            fetch += uint32_t(nIdle);
+        }
+        if (active) {
+            const int st = stepRay(m, S.x, S.y, ray, load);
+            if (st != kContinue) {
+                crossings += uint32_t(ray.steps) + 1u;
+                if (st == kDone) {
+                    finishReflections(m, ray);
+                    const double X = CQ * double(wf) * exp(double(ray.G));
+                    sum += X;
+                    sum2 += X * X;
+                } else {
+                    ++dropped;
+                }
+                active = false;
+            }
+        }
     }
 
     sum = warpSum(sum);
