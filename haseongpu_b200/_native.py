@@ -77,6 +77,7 @@ class ExperimentDesc(C.Structure):
         ("mseThreshold", C.c_double),
         ("useReflections", C.c_uint32),
         ("monochromatic", C.c_uint32),
+        ("nearFieldSampling", C.c_uint32),
     ]
 
 

@@ -66,9 +66,10 @@ hase_status fail(hase_status st, const char* fmt, ...) {
     } while (0)
 
 constexpr uint32_t kRayBlock = 256;
-constexpr uint32_t kRaysPerThread = 8;
+constexpr int kRayMinBlocks = 5;
 constexpr int kRefill = 8;  // idle lanes that trigger a batched refill
-constexpr uint32_t kMaxChunks = 256;
+constexpr uint32_t kMaxItems = 1024;  // work items per sample and pass
+constexpr uint32_t kMinItemRays = 1024;
 constexpr uint32_t kMapBlock = 1024;
 constexpr double kPi = 3.14159265358979323846;
 
@@ -258,15 +259,20 @@ __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
 struct RayLaunch {
     MeshView m;
     const uint32_t* active;       // active row ids
-    uint32_t firstSample, pass, M, raysPerChunk, nW;
+    uint32_t nActive;
+    uint32_t firstSample, pass, M, nW;
+    uint32_t itemRays;            // rays per work item
+    uint32_t itemsPerRow;         // ceil(M / itemRays) <= kMaxItems
+    unsigned int* itemCounter;    // zeroed before the launch
     const uint32_t* q;            // [rows][nW]
     const unsigned long long* Q;  // [rows]
     const uint32_t* offsets;      // [rows][nW+1]
     uint32_t seedLo, seedHi;
     const float2* spec;           // per wavelength (A, B)
     uint32_t nLambda;
+    uint32_t nearField;           // solid-angle start points in prisms touching the sample
     double C;                     // N_tot / (4 pi tau)
-    double* pSum;                 // [rows][kMaxChunks]
+    double* pSum;                 // [rows][kMaxItems]
     double* pSum2;
     uint32_t* pDrop;
     unsigned long long* pCross;
@@ -282,150 +288,126 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
     return lo;
 }
 
-template <int BLOCK, int RPT, int REFILL>
-__global__ void __launch_bounds__(BLOCK, 5) rayKernel(RayLaunch L) {
-    __shared__ uint32_t sNextBatch;
-    __shared__ double sRedD[2][BLOCK / 32];
-    __shared__ uint32_t sRedU[BLOCK / 32];
-    __shared__ unsigned long long sRedL[BLOCK / 32];
-
+// Persistent ray kernel: every warp repeatedly takes a work item -- itemRays
+// consecutive rays of one active sample -- from a global counter, walks them
+// (lanes whose ray ends take the next ray of the item, in groups of at least
+// REFILL idle lanes so start-point code runs convergent), and writes the
+// item's FP64 sums.  No block barrier; per-item partials keep the result
+// independent of which warp ran which item.
+template <int BLOCK, int REFILL, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     const MeshView& m = L.m;
-    const uint32_t row = L.active[blockIdx.y];
-    const uint32_t sample = L.firstSample + row;
-    const uint32_t chunk = blockIdx.x;
-    const uint32_t r0 = chunk * L.raysPerChunk;
-    const uint32_t r1 = min(r0 + L.raysPerChunk, L.M);
-    const uint32_t nW = L.nW;
-    const uint32_t* off = L.offsets + size_t(row) * (nW + 1);
-    const uint32_t* q = L.q + size_t(row) * nW;
-    const unsigned long long Qrow = L.Q[row];
-    if (Qrow == 0ull) {  // no source prism: every ray contributes 0
-        if (threadIdx.x == 0) {
-            const size_t k = size_t(row) * kMaxChunks + chunk;
-            L.pSum[k] = 0.0;
-            L.pSum2[k] = 0.0;
-            L.pDrop[k] = 0u;
-            L.pCross[k] = 0ull;
-        }
-        return;
-    }
-    const double CQ = L.C * double(Qrow);
-    const float2 S = __ldg(m.points + sample % m.Np);
-    const int ls = int(sample / m.Np);
-    const uint32_t lambdaPhase =
-        L.nLambda > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, L.seedLo, L.seedHi).y % L.nLambda : 0u;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const unsigned laneLt = (1u << lane) - 1u;
+    const uint32_t nItems = L.nActive * L.itemsPerRow;
     GlobalLoader load{m.tri};
-
-    double sum = 0.0, sum2 = 0.0;
-    uint32_t dropped = 0;
-    unsigned long long crossings = 0;
-
-    // Warps pull batches of 32*RPT consecutive rays of this chunk from a
-    // shared counter and chain them without block barriers: a lane whose ray
-    // ends takes the next ray of the current batch, and a new batch is
-    // fetched as soon as the current one is handed out.
-    if (threadIdx.x == 0) sNextBatch = 0u;
-    __syncthreads();
-    constexpr uint32_t kBatch = 32u * RPT;
-    const uint32_t nBatches = r1 > r0 ? (r1 - r0 + kBatch - 1) / kBatch : 0u;
-    uint32_t fetch = 0, wEnd = 0;  // rays [fetch, wEnd) of the current batch are still to hand out
-    uint32_t pb = 0, count = 0;    // the batch's rays lie in prisms [pb, pb + count - 1)
-    bool more = true, active = false;
-    Ray ray;
-    float wf = 0.0f;
     while (true) {
-        const unsigned idle = __ballot_sync(0xffffffffu, !active);
-        const int nIdle = __popc(idle);
-        if (fetch >= wEnd && more && (nIdle >= REFILL || nIdle == 32)) {
-            uint32_t batch = 0;
-            if (lane == 0) batch = atomicAdd(&sNextBatch, 1u);
-            batch = __shfl_sync(0xffffffffu, batch, 0);
-            if (batch >= nBatches) {
-                more = false;
-            } else {
-                fetch = r0 + batch * kBatch;
-                wEnd = min(fetch + kBatch, r1);
-                uint32_t bound = 0;
-                if (lane == 0) bound = upperBound(off, nW + 1, fetch) - 1u;
-                if (lane == 1) bound = upperBound(off, nW + 1, wEnd - 1u) - 1u;
-                pb = __shfl_sync(0xffffffffu, bound, 0);
-                count = __shfl_sync(0xffffffffu, bound, 1) - pb + 2u;  // offsets pb .. pe+1
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(L.itemCounter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= nItems) break;
+        const uint32_t row = L.active[item / L.itemsPerRow];
+        const uint32_t k = item % L.itemsPerRow;
+        const size_t slot = size_t(row) * kMaxItems + k;
+        const unsigned long long Qrow = L.Q[row];
+        if (Qrow == 0ull) {  // no source prism: every ray contributes 0
+            if (lane == 0) {
+                L.pSum[slot] = 0.0;
+                L.pSum2[slot] = 0.0;
+                L.pDrop[slot] = 0u;
+                L.pCross[slot] = 0ull;
             }
+            continue;
         }
-        if (!more && nIdle == 32) break;
-        if (fetch < wEnd && (nIdle >= REFILL || nIdle == 32)) {
-            const uint32_t r = fetch + __popc(idle & laneLt);
-            if (!active && r < wEnd) {
-                const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
-                const uint32_t j = b / m.P, p = b - j * m.P;
-                const uint32_t t = p % m.T, l = p / m.T;
-                const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
-                uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
-                if (k1 + k2 + 1u > (1u << 24)) {
-                    k1 = (1u << 24) - 1u - k1;
-                    k2 = (1u << 24) - 1u - k2;
-                }
-                const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
-                const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
-                const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
-                const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
-                const int kImg = imageLevel(ls, int(m.layers), j);
-                const uint32_t lam =
-                    L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
-                const float2 ab = __ldg(L.spec + lam);
-                const float D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg,
-                                         j, ab.x, ab.y, m.h);
-                wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
-                active = D2 > 0.0f;
-                if (!active) ++dropped;  // start point on the sample point itself
-            }
-            fetch += uint32_t(nIdle);
-        }
-        if (active) {
-            const int st = stepRay(m, S.x, S.y, ray, load);
-            if (st != kContinue) {
-                crossings += uint32_t(ray.steps) + 1u;
-                if (st == kDone) {
-                    finishReflections(m, ray);
-                    const double X = CQ * double(wf) * exp(double(ray.G));
-                    sum += X;
-                    sum2 += X * X;
-                } else {
-                    ++dropped;
-                }
-                active = false;
-            }
-        }
-    }
+        const uint32_t sample = L.firstSample + row;
+        const uint32_t r0 = k * L.itemRays;
+        const uint32_t r1 = min(r0 + L.itemRays, L.M);
+        const uint32_t nW = L.nW;
+        const uint32_t* off = L.offsets + size_t(row) * (nW + 1);
+        const uint32_t* q = L.q + size_t(row) * nW;
+        const double CQ = L.C * double(Qrow);
+        const float2 S = __ldg(m.points + sample % m.Np);
+        const int ls = int(sample / m.Np);
+        const uint32_t lambdaPhase =
+            L.nLambda > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, L.seedLo, L.seedHi).y % L.nLambda : 0u;
+        // prisms holding the item's rays: [pb, pb + count - 1)
+        uint32_t bound = 0;
+        if (lane == 0) bound = upperBound(off, nW + 1, r0) - 1u;
+        if (lane == 1) bound = upperBound(off, nW + 1, r1 - 1u) - 1u;
+        const uint32_t pb = __shfl_sync(0xffffffffu, bound, 0);
+        const uint32_t count = __shfl_sync(0xffffffffu, bound, 1) - pb + 2u;
 
-    sum = warpSum(sum);
-    sum2 = warpSum(sum2);
-    dropped = warpSum(dropped);
-    crossings = warpSum(crossings);
-    if (lane == 0) {
-        sRedD[0][warp] = sum;
-        sRedD[1][warp] = sum2;
-        sRedU[warp] = dropped;
-        sRedL[warp] = crossings;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        double a = lane < BLOCK / 32 ? sRedD[0][lane] : 0.0;
-        double b2 = lane < BLOCK / 32 ? sRedD[1][lane] : 0.0;
-        uint32_t d = lane < BLOCK / 32 ? sRedU[lane] : 0u;
-        unsigned long long c = lane < BLOCK / 32 ? sRedL[lane] : 0ull;
-        a = warpSum(a);
-        b2 = warpSum(b2);
-        d = warpSum(d);
-        c = warpSum(c);
+        double sum = 0.0, sum2 = 0.0;
+        uint32_t dropped = 0, crossings = 0;
+        uint32_t fetch = r0;
+        bool active = false;
+        Ray ray;
+        float wf = 0.0f;
+        while (true) {
+            const unsigned idle = __ballot_sync(0xffffffffu, !active);
+            const int nIdle = __popc(idle);
+            if (fetch >= r1 && nIdle == 32) break;
+            if (fetch < r1 && (nIdle >= REFILL || nIdle == 32)) {
+                const uint32_t r = fetch + __popc(idle & laneLt);
+                if (!active && r < r1) {
+                    const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
+                    const uint32_t j = b / m.P, p = b - j * m.P;
+                    const uint32_t t = p % m.T, l = p / m.T;
+                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
+                    uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
+                    if (k1 + k2 + 1u > (1u << 24)) {
+                        k1 = (1u << 24) - 1u - k1;
+                        k2 = (1u << 24) - 1u - k2;
+                    }
+                    const int kImg = imageLevel(ls, int(m.layers), j);
+                    const uint32_t lam =
+                        L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
+                    const float2 ab = __ldg(L.spec + lam);
+                    float dx, dy, dz, alphaL, D2;
+                    if (L.nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
+                        nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
+                                       unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
+                        D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
+                        wf = __ldg(m.srcBeta + p) * alphaL / float(__ldg(q + b));
+                    } else {
+                        const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
+                        const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
+                        const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
+                        const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
+                        D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j,
+                                     ab.x, ab.y, m.h);
+                        wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
+                    }
+                    active = D2 > 0.0f;
+                    if (!active) ++dropped;  // start point on the sample point itself
+                }
+                fetch += uint32_t(nIdle);
+            }
+            if (active) {
+                const int st = stepRay(m, S.x, S.y, ray, load);
+                if (st != kContinue) {
+                    crossings += uint32_t(ray.steps) + 1u;
+                    if (st == kDone) {
+                        finishReflections(m, ray);
+                        const double X = CQ * double(wf) * exp(double(ray.G));
+                        sum += X;
+                        sum2 += X * X;
+                    } else {
+                        ++dropped;
+                    }
+                    active = false;
+                }
+            }
+        }
+        sum = warpSum(sum);
+        sum2 = warpSum(sum2);
+        dropped = warpSum(dropped);
+        crossings = warpSum(crossings);
         if (lane == 0) {
-            const size_t k = size_t(row) * kMaxChunks + chunk;
-            L.pSum[k] = a;
-            L.pSum2[k] = b2;
-            L.pDrop[k] = d;
-            L.pCross[k] = c;
+            L.pSum[slot] = sum;
+            L.pSum2[slot] = sum2;
+            L.pDrop[slot] = dropped;
+            L.pCross[slot] = crossings;
         }
     }
 }
@@ -433,7 +415,7 @@ __global__ void __launch_bounds__(BLOCK, 5) rayKernel(RayLaunch L) {
 // ------------------------------------------------ (c)+(d) finalise ----
 struct FinalizeLaunch {
     const uint32_t* active;
-    uint32_t nActive, chunks, M;
+    uint32_t nActive, items, M;
     int last;                     // no further pass follows
     double threshold;
     const double* pSum;
@@ -459,8 +441,8 @@ __global__ void __launch_bounds__(128) finalizeKernel(FinalizeLaunch L) {
     double s = 0.0, s2 = 0.0;
     uint32_t d = 0;
     unsigned long long c = 0;
-    for (uint32_t k = lane; k < L.chunks; k += 32) {
-        const size_t i = size_t(row) * kMaxChunks + k;
+    for (uint32_t k = lane; k < L.items; k += 32) {
+        const size_t i = size_t(row) * kMaxItems + k;
         s += L.pSum[i];
         s2 += L.pSum2[i];
         d += L.pDrop[i];
@@ -566,6 +548,7 @@ struct DevBuf {
 };
 
 struct HostTables {
+    std::vector<int4> verts;
     std::vector<float4> tri, geo;
     std::vector<float2> centroid, points;
 };
@@ -576,6 +559,7 @@ hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& exte
     h.geo.assign(2 * size_t(T), make_float4(0, 0, 0, 0));
     h.centroid.resize(T);
     h.points.resize(Np);
+    h.verts.resize(T);
     extent = 0.0;
     for (uint32_t i = 0; i < Np; ++i) {
         h.points[i] = make_float2(float(d->points[2 * i]), float(d->points[2 * i + 1]));
@@ -620,6 +604,7 @@ hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& exte
         h.geo[2 * t] = make_float4(float(x0), float(y0), float(x1 - x0), float(y1 - y0));
         h.geo[2 * t + 1] = make_float4(float(x2 - x0), float(y2 - y0), float(0.5 * std::fabs(cross)), 0.0f);
         h.centroid[t] = make_float2(float((x0 + x1 + x2) / 3.0), float((y0 + y1 + y2) / 3.0));
+        h.verts[t] = make_int4(int(v[0]), int(v[1]), int(v[2]), 0);
     }
     for (uint32_t t = 0; t < T; ++t) {
         int32_t w[3];
@@ -647,11 +632,14 @@ struct hase_context {
     bool hasReflect = false;
     float tirCos2[2] = {-1.0f, -1.0f};
     DevBuf<float4> tri, geo;
+    DevBuf<int4> verts;
     DevBuf<float2> centroid, points, spec;
     DevBuf<float> gainBeta, srcBeta, reflect;
     // workspace
     DevBuf<float> lnw;
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
+    DevBuf<unsigned int> itemCounter;
+    uint32_t persistentBlocks = 0;  // resident rayKernel blocks on the device
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
@@ -660,6 +648,7 @@ struct hase_context {
         MeshView v{};
         v.tri = tri.p;
         v.geo = geo.p;
+        v.verts = verts.p;
         v.centroid = centroid.p;
         v.gainBeta = gainBeta.p;
         v.srcBeta = srcBeta.p;
@@ -803,6 +792,7 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
     };
     if ((st = up(c->tri, ht.tri)) != HASE_OK) return cleanup(st);
     if ((st = up(c->geo, ht.geo)) != HASE_OK) return cleanup(st);
+    if ((st = up(c->verts, ht.verts)) != HASE_OK) return cleanup(st);
     if ((st = up(c->centroid, ht.centroid)) != HASE_OK) return cleanup(st);
     if ((st = up(c->points, ht.points)) != HASE_OK) return cleanup(st);
     if (c->gainBeta.ensure(c->P) != cudaSuccess || c->srcBeta.ensure(c->P) != cudaSuccess)
@@ -871,7 +861,7 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
 
     // batch rows by the workspace budget
     const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
-    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxChunks * 28ull + 64;
+    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxItems * 28ull + 64;
     uint32_t rows = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nS, budget / perRow)));
     HASE_CUDA(c->lnw.ensure(size_t(rows) * nW));
     HASE_CUDA(c->q.ensure(size_t(rows) * nW));
@@ -880,6 +870,13 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     HASE_CUDA(c->activeA.ensure(rows));
     HASE_CUDA(c->activeB.ensure(rows));
     HASE_CUDA(c->counter.ensure(1));
+    HASE_CUDA(c->itemCounter.ensure(1));
+    if (c->persistentBlocks == 0) {
+        int perSM = 0, sms = 0;
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, rayKernel<kRayBlock, kRefill, kRayMinBlocks>, kRayBlock, 0));
+        HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        c->persistentBlocks = uint32_t(std::max(1, perSM) * std::max(1, sms));
+    }
     HASE_CUDA(c->accSum.ensure(rows));
     HASE_CUDA(c->accSum2.ensure(rows));
     HASE_CUDA(c->accTotal.ensure(rows));
@@ -887,10 +884,10 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     HASE_CUDA(c->accCross.ensure(rows));
     HASE_CUDA(c->phi.ensure(rows));
     HASE_CUDA(c->mse.ensure(rows));
-    HASE_CUDA(c->pSum.ensure(size_t(rows) * kMaxChunks));
-    HASE_CUDA(c->pSum2.ensure(size_t(rows) * kMaxChunks));
-    HASE_CUDA(c->pDrop.ensure(size_t(rows) * kMaxChunks));
-    HASE_CUDA(c->pCross.ensure(size_t(rows) * kMaxChunks));
+    HASE_CUDA(c->pSum.ensure(size_t(rows) * kMaxItems));
+    HASE_CUDA(c->pSum2.ensure(size_t(rows) * kMaxItems));
+    HASE_CUDA(c->pDrop.ensure(size_t(rows) * kMaxItems));
+    HASE_CUDA(c->pCross.ensure(size_t(rows) * kMaxItems));
 
     const MeshView mv = c->view();
     const double C = c->nTot / (4.0 * kPi * c->tau);
@@ -937,16 +934,21 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
                          nullptr, c->q.p, c->Q.p, c->offsets.p};
             mapKernel<<<nActive, kMapBlock, 0, c->stream>>>(ml);
             HASE_CUDA(cudaGetLastError());
-            const uint32_t chunks = std::min<uint32_t>(kMaxChunks, (M + kRayBlock * kRaysPerThread - 1) / (kRayBlock * kRaysPerThread));
-            const uint32_t perChunk = (M + chunks - 1) / chunks;
+            const uint32_t itemRays = std::max<uint32_t>(kMinItemRays, (M + kMaxItems - 1) / kMaxItems);
+            const uint32_t items = (M + itemRays - 1) / itemRays;
+            HASE_CUDA(cudaMemsetAsync(c->itemCounter.p, 0, sizeof(unsigned int), c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
-            RayLaunch rl{mv, cur, firstSample, pass, M, perChunk, nW, c->q.p, c->Q.p, c->offsets.p, cp->rngSeed, 0u,
-                         c->spec.p, nLambda, C, c->pSum.p, c->pSum2.p, c->pDrop.p, c->pCross.p};
-            rayKernel<kRayBlock, kRaysPerThread, kRefill><<<dim3(chunks, nActive), kRayBlock, 0, c->stream>>>(rl);
+            RayLaunch rl{mv, cur, nActive, firstSample, pass, M, nW, itemRays, items, c->itemCounter.p, c->q.p,
+                         c->Q.p, c->offsets.p, cp->rngSeed, 0u, c->spec.p, nLambda, ex->nearFieldSampling, C, c->pSum.p, c->pSum2.p,
+                         c->pDrop.p, c->pCross.p};
+            const uint64_t totalItems = uint64_t(nActive) * items;
+            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (kRayBlock / 32) + 1,
+                                                               uint64_t(c->persistentBlocks)));
+            rayKernel<kRayBlock, kRefill, kRayMinBlocks><<<grid, kRayBlock, 0, c->stream>>>(rl);
             HASE_CUDA(cudaGetLastError());
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
-            FinalizeLaunch fl{cur, nActive, chunks, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,
+            FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,
                               c->pDrop.p, c->pCross.p, c->accSum.p, c->accSum2.p, c->accTotal.p, c->accDrop.p,
                               c->accCross.p, c->phi.p, c->mse.p, nxt, c->counter.p};
             finalizeKernel<<<(nActive * 32 + 127) / 128, 128, 0, c->stream>>>(fl);

@@ -68,6 +68,7 @@ __device__ __forceinline__ float unit24(uint32_t k24) { return (float(k24) + 0.5
 struct MeshView {
     const float4* tri;       // [T][3]
     const float4* geo;       // [T][2]
+    const int4* verts;       // [T] point ids of the triangle's vertices (w unused)
     const float2* centroid;  // [T]
     const float* gainBeta;   // [P] beta, NaN in cladding prisms (walk)
     const float* srcBeta;    // [P] beta (source weight)
@@ -214,6 +215,57 @@ __device__ __forceinline__ void finishReflections(const MeshView& m, Ray& r) {
         r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
         r.reflLeft = 0;
     }
+}
+
+// Near-field start point for a prism (t, l) that touches the image point of
+// sample point `pS` (a vertex of triangle t at image level kImg = l or l+1).
+// Uniform start points give such prisms an infinite-variance 1/d^2 weight;
+// here the direction from the image point is uniform in the prism's solid
+// angle (azimuth uniform between the two triangle edges at the vertex,
+// sin(elevation) uniform: the prism seen from its vertex is that lune
+// segment, solid angle alpha) and the distance is uniform up to the prism
+// exit L(Omega).  The density is 1/(alpha L d^2), so the ray weight
+// beta G / d^2 / density = beta G alpha L stays bounded.
+// Returns false when t does not have pS as a vertex.
+__device__ __forceinline__ bool nearFieldStart(const MeshView& m, uint32_t t, int l, int kImg, uint32_t pS,
+                                               float2 S, float uAz, float uEl, float uR, float& dx, float& dy,
+                                               float& dz, float& alphaL) {
+    const int4 v = __ldg(m.verts + t);
+    const int iv = v.x == int(pS) ? 0 : (v.y == int(pS) ? 1 : (v.z == int(pS) ? 2 : -1));
+    if (iv < 0) return false;
+    const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
+    const float px[3] = {g0.x, g0.x + g0.z, g0.x + g1.x};
+    const float py[3] = {g0.y, g0.y + g0.w, g0.y + g1.y};
+    float e1x = (iv == 0 ? px[1] : (iv == 1 ? px[2] : px[0])) - S.x;
+    float e1y = (iv == 0 ? py[1] : (iv == 1 ? py[2] : py[0])) - S.y;
+    float e2x = (iv == 0 ? px[2] : (iv == 1 ? px[0] : px[1])) - S.x;
+    float e2y = (iv == 0 ? py[2] : (iv == 1 ? py[0] : py[1])) - S.y;
+    const float i1 = rsqrtf(e1x * e1x + e1y * e1y), i2 = rsqrtf(e2x * e2x + e2y * e2y);
+    e1x *= i1;
+    e1y *= i1;
+    e2x *= i2;
+    e2y *= i2;
+    const float cosA = fminf(fmaxf(fmaf(e1x, e2x, e1y * e2y), -1.0f), 1.0f);
+    const float alpha = acosf(cosA);
+    const float sinA = sinf(alpha);
+    const float w1 = sinf((1.0f - uAz) * alpha) / sinA, w2 = sinf(uAz * alpha) / sinA;
+    const float cx = fmaf(w1, e1x, w2 * e2x), cy = fmaf(w1, e1y, w2 * e2y);
+    const float se = uEl, ce = sqrtf(fmaxf(0.0f, 1.0f - se * se));
+    // edge opposite the vertex: edge (iv + 1) % 3 of the walk record
+    const int eo = iv == 2 ? 0 : iv + 1;
+    const float4 r0 = __ldg(m.tri + 3 * t), r1 = __ldg(m.tri + 3 * t + 1), r2 = __ldg(m.tri + 3 * t + 2);
+    const float nx = eo == 0 ? r0.x : (eo == 1 ? r0.w : r1.z);
+    const float ny = eo == 0 ? r0.y : (eo == 1 ? r1.x : r1.w);
+    const float cc = eo == 0 ? r0.z : (eo == 1 ? r1.y : r2.x);
+    const float lxy = (cc - fmaf(nx, S.x, ny * S.y)) / fmaf(nx, cx, ny * cy);
+    const float L = fminf(lxy / ce, m.h / se);
+    const float r = uR * L;
+    const float zs = l == kImg ? 1.0f : -1.0f;
+    dx = r * ce * cx;
+    dy = r * ce * cy;
+    dz = zs * r * se;
+    alphaL = alpha * L;
+    return true;
 }
 
 struct GlobalLoader {

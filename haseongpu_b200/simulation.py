@@ -97,7 +97,7 @@ class DeviceMesh:
         N.check(N.lib().hase_context_update_beta(self.handle, N.ptr(bv, N._f64p), N.ptr(bc, N._f64p)))
 
     def calc_phi_ase(self, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
-                     adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
+                     nearFieldSampling=True, adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
                      blockSize=0, workspaceBytes=0) -> Result:
         S = self.mesh.numberOfSamples
         maxSample = S - 1 if maxSample is None else int(maxSample)
@@ -107,7 +107,7 @@ class DeviceMesh:
         out = Result(phiAse=np.empty(n, np.float32), standardError=np.empty(n), relativeStandardError=np.empty(n),
                      totalRays=np.empty(n, np.uint32), dndtAse=np.empty(n), droppedRays=np.empty(n, np.uint32))
         ex = N.ExperimentDesc(int(minRays), int(maxRays if maxRays is not None else minRays), float(mseThreshold),
-                              1 if useReflections else 0, 1 if monochromatic else 0)
+                              1 if useReflections else 0, 1 if monochromatic else 0, 1 if nearFieldSampling else 0)
         cp = N.ComputeDesc(int(adaptiveSteps), int(repetitions), int(rngSeed) & 0xFFFFFFFF, int(minSample), maxSample,
                            int(raysPerThread), int(blockSize), int(workspaceBytes))
         r = N.ResultDesc(N.ptr(out.phiAse, N._f32p), N.ptr(out.standardError, N._f64p),
@@ -183,6 +183,7 @@ class PhiASE:
     reflectionTolerance: float = 1e-4
     surfaceReservoirSize: int = 32
     monochromatic: bool = False
+    nearFieldSampling: bool = True
     backend: str | None = "cuda_sm100a"
     parallelMode: str = "single"
     numDevices: int = 1
@@ -237,7 +238,7 @@ class PhiASE:
         self._result = ctx.calc_phi_ase(
             minRays=minRays, maxRays=maxRays, mseThreshold=self.relativeStandardErrorThreshold,
             useReflections=self.useReflections, monochromatic=self.monochromatic,
-            adaptiveSteps=0 if rays else self.adaptiveSteps, repetitions=self.repetitions,
+            nearFieldSampling=self.nearFieldSampling, adaptiveSteps=0 if rays else self.adaptiveSteps, repetitions=self.repetitions,
             rngSeed=5489 if self.rngSeed is None else self.rngSeed,
             minSample=self.minSampleRange or 0, maxSample=self.maxSampleRange)
         return self

@@ -85,6 +85,9 @@ typedef struct {
     double mseThreshold;                /* stop when the relative standard error <= this */
     uint32_t useReflections;            /* 0/1: top/bottom reflections of order <= 2 */
     uint32_t monochromatic;             /* 1: use only the first (sigmaA, sigmaE) pair */
+    uint32_t nearFieldSampling;         /* 1: solid-angle start points in the prisms touching the sample
+                                           (bounded weights); 0: uniform start points in every prism, as
+                                           the legacy method */
 } hase_experiment_desc;
 
 typedef struct {

@@ -443,19 +443,49 @@ int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum, con
                             uint32_t((uint64_t(r) * nLambda / M + po[1] % nLambda) % nLambda);
                         uint32_t rc4[4] = {r, s, pass, kTagRay}, ro[4];
                         philox(rc4, key, ro);
-                        uint32_t k1 = ro[0] >> 8, k2 = ro[1] >> 8;
-                        if (uint64_t(k1) + k2 + 1u > (1u << 24)) { k1 = (1u << 24) - 1u - k1; k2 = (1u << 24) - 1u - k2; }
-                        const double u1 = (double(k1) + 0.5) / 16777216.0, u2 = (double(k2) + 0.5) / 16777216.0;
                         const uint32_t* v = mesh->triangles + 3 * t;
-                        const double ax = mesh->points[2 * v[0]], ay = mesh->points[2 * v[0] + 1];
-                        const double x = ax + u1 * (mesh->points[2 * v[1]] - ax) + u2 * (mesh->points[2 * v[2]] - ax);
-                        const double y = ay + u1 * (mesh->points[2 * v[1] + 1] - ay) + u2 * (mesh->points[2 * v[2] + 1] - ay);
-                        const double z = (double(l) + unit(ro[2])) * md.h;
-                        const Walk wk = walk(md, x, y, z, t, l, Sx, Sy, imageZ(Sz, md.H, j), j, md.gainA[lambda],
-                                             md.gainB[lambda]);
+                        const double Iz = imageZ(Sz, md.H, j);
+                        const int kImg = int(std::lround(Iz / md.h));
+                        const uint32_t pS = s % md.Np;
+                        const int iv = v[0] == pS ? 0 : (v[1] == pS ? 1 : (v[2] == pS ? 2 : -1));
+                        double x, y, z, factor;  // factor: the start density's volume term
+                        if (ex->nearField && (int(l) == kImg || int(l) + 1 == kImg) && iv >= 0) {
+                            // solid angle of the prism at the (image) sample point: see nearFieldStart
+                            const uint32_t va = v[(iv + 1) % 3], vb = v[(iv + 2) % 3];
+                            double e1x = mesh->points[2 * va] - Sx, e1y = mesh->points[2 * va + 1] - Sy;
+                            double e2x = mesh->points[2 * vb] - Sx, e2y = mesh->points[2 * vb + 1] - Sy;
+                            const double i1 = 1.0 / std::sqrt(e1x * e1x + e1y * e1y), i2 = 1.0 / std::sqrt(e2x * e2x + e2y * e2y);
+                            e1x *= i1; e1y *= i1; e2x *= i2; e2y *= i2;
+                            const double alpha = std::acos(std::min(1.0, std::max(-1.0, e1x * e2x + e1y * e2y)));
+                            const double uAz = unit(ro[0]), se = unit(ro[2]), uR = unit(ro[3]);
+                            const double w1 = std::sin((1.0 - uAz) * alpha) / std::sin(alpha);
+                            const double w2 = std::sin(uAz * alpha) / std::sin(alpha);
+                            const double cx = w1 * e1x + w2 * e2x, cy = w1 * e1y + w2 * e2y;
+                            const double ce = std::sqrt(std::max(0.0, 1.0 - se * se));
+                            const int eo = (iv + 1) % 3;
+                            const double nx = md.tab.nx[3 * t + eo], ny = md.tab.ny[3 * t + eo], cc = md.tab.c[3 * t + eo];
+                            const double lxy = (cc - (nx * Sx + ny * Sy)) / (nx * cx + ny * cy);
+                            const double L = std::min(lxy / ce, md.h / se);
+                            const double rr = uR * L;
+                            const double zs = int(l) == kImg ? 1.0 : -1.0;
+                            x = Sx + rr * ce * cx;
+                            y = Sy + rr * ce * cy;
+                            z = double(kImg) * md.h + zs * rr * se;
+                            factor = alpha * L;  // start density 1/(alpha L d^2)
+                        } else {
+                            uint32_t k1 = ro[0] >> 8, k2 = ro[1] >> 8;
+                            if (uint64_t(k1) + k2 + 1u > (1u << 24)) { k1 = (1u << 24) - 1u - k1; k2 = (1u << 24) - 1u - k2; }
+                            const double u1 = (double(k1) + 0.5) / 16777216.0, u2 = (double(k2) + 0.5) / 16777216.0;
+                            const double ax = mesh->points[2 * v[0]], ay = mesh->points[2 * v[0] + 1];
+                            x = ax + u1 * (mesh->points[2 * v[1]] - ax) + u2 * (mesh->points[2 * v[2]] - ax);
+                            y = ay + u1 * (mesh->points[2 * v[1] + 1] - ay) + u2 * (mesh->points[2 * v[2] + 1] - ay);
+                            z = (double(l) + unit(ro[2])) * md.h;
+                            factor = -1.0;  // uniform in the prism: density 1/V
+                        }
+                        const Walk wk = walk(md, x, y, z, t, l, Sx, Sy, Iz, j, md.gainA[lambda], md.gainB[lambda]);
                         if (wk.dropped || wk.dist == 0.0) { ++dropped; continue; }
-                        const double X = C * mesh->betaVolume[p] * md.tab.area[t] * md.h * (double(Q) / double(q[b])) *
-                                         std::exp(wk.lnGain) / (wk.dist * wk.dist);
+                        const double vol = factor > 0.0 ? factor : md.tab.area[t] * md.h / (wk.dist * wk.dist);
+                        const double X = C * mesh->betaVolume[p] * vol * (double(Q) / double(q[b])) * std::exp(wk.lnGain);
                         sum += X;
                         sum2 += X * X;
                     }

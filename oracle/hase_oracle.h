@@ -57,6 +57,7 @@ typedef struct {
     uint32_t seed;
     uint32_t minSample;           /* inclusive */
     uint32_t maxSample;           /* inclusive */
+    uint32_t nearField;           /* solid-angle start points in prisms touching the (image) sample */
 } oracle_experiment;
 
 typedef struct {

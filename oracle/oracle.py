@@ -63,6 +63,7 @@ class _Experiment(C.Structure):
         ("seed", C.c_uint32),
         ("minSample", C.c_uint32),
         ("maxSample", C.c_uint32),
+        ("nearField", C.c_uint32),
     ]
 
 
@@ -210,7 +211,7 @@ def ray_map(weights, rays, phase):
 
 
 def phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, mseThreshold=0.0, useReflections=False,
-            seed=5489, minSample=0, maxSample=None, weights=None, threads=0):
+            seed=5489, minSample=0, maxSample=None, weights=None, threads=0, nearField=True):
     """Adaptive backward phi-ASE over samples [minSample, maxSample] (FP64)."""
     keep = _Keep()
     m = _mesh_struct(mesh, keep)
@@ -219,7 +220,7 @@ def phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, mseThresh
     maxSample = n_samples_total - 1 if maxSample is None else int(maxSample)
     e = _Experiment(int(minRays), int(maxRays if maxRays is not None else minRays), int(adaptiveSteps),
                     float(mseThreshold), 1 if useReflections else 0, int(seed) & 0xFFFFFFFF, int(minSample),
-                    maxSample)
+                    maxSample, 1 if nearField else 0)
     n = maxSample - int(minSample) + 1
     out = {
         "phiAse": np.empty(n), "mse": np.empty(n), "totalRays": np.empty(n, np.uint32),

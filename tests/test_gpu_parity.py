@@ -162,23 +162,30 @@ def test_estimator_replay_matches_oracle(oracle, workload):
 
 @pytest.mark.parametrize("name", ["cuboid", "cylindrical"])
 def test_gpu_matches_legacy_serial_reference(name):
+    """Per-sample agreement with the legacy serial buffers (1e6 rays/sample).
+
+    The legacy estimate's own error is that of the plain method (uniform
+    start points), measured here with nearFieldSampling off and scaled to
+    1e6 rays; its 1/d^2 tail is heavy, so the bar is 95 % within 3 sigma plus
+    mean and median ratios within 0.3 % / 0.5 %."""
     d = np.load(GOLDEN / f"legacy_{name}.npz")
     mesh = legacy_mesh(name)
     sa, se = legacy_spectrum(name)
     with _ctx(mesh, sa, se) as ctx:
         r = ctx.calc_phi_ase(minRays=200000, rngSeed=5489)
+        plain = ctx.calc_phi_ase(minRays=200000, rngSeed=77, nearFieldSampling=False)
     assert r.droppedRays.sum() <= 1e-7 * r.raysTraced
     legacy = d["phiASE"]
     ratio = r.phiAse / legacy
     assert abs(ratio.mean() - 1.0) < 0.003, ratio.mean()
     assert abs(np.median(ratio) - 1.0) < 0.005, np.median(ratio)
-    # 3 sigma of the combined error: ours (RSE) and the legacy 1e6-ray buffers.
-    # Uniform start points make the 1/d^2 weight of the prisms touching the
-    # sample heavy-tailed (infinite variance) in both implementations, so the
-    # sample RSE understates the error of a minority of samples.
-    sigma = np.sqrt((r.relativeStandardError * r.phiAse) ** 2 + (r.relativeStandardError * r.phiAse * 0.45) ** 2)
+    assert abs((plain.phiAse / legacy).mean() - 1.0) < 0.003
+    sigma_legacy = plain.relativeStandardError * plain.phiAse * np.sqrt(200000 / 1e6)
+    sigma = np.sqrt((r.relativeStandardError * r.phiAse) ** 2 + sigma_legacy ** 2)
     z = (r.phiAse - legacy) / sigma
-    assert np.mean(np.abs(z) < 3) > 0.9, np.mean(np.abs(z) < 3)
+    assert np.mean(np.abs(z) < 3) > 0.95, np.mean(np.abs(z) < 3)
+    # near-field sampling bounds the weights: far lower error at equal rays
+    assert np.median(r.relativeStandardError) < 0.5 * np.median(plain.relativeStandardError)
     np.testing.assert_allclose(r.dndtAse, (d["betaCells"] * (se[0] + sa[0]) - sa[0]) * r.phiAse.astype(np.float64),
                                rtol=1e-12)
 
