@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "hase_ray_map",
     "hase_trace_rays",
     "hase_philox",
+    "hase_probe_l2_bandwidth",
 )
 
 _u32p = C.POINTER(C.c_uint32)
@@ -147,6 +148,7 @@ def lib():
         L.hase_trace_rays.argtypes = [C.c_void_p, C.c_uint32, _f32p, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                       _f32p, _f32p, _u32p]
         L.hase_philox.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
+        L.hase_probe_l2_bandwidth.argtypes = [C.c_int, C.c_uint64, C.c_uint32, _f64p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version"):
                 getattr(L, name).restype = C.c_int
@@ -173,6 +175,13 @@ def philox(ctr, key):
     out = np.empty_like(c)
     check(lib().hase_philox(c.shape[0], ptr(c, _u32p), ptr(k, _u32p), ptr(out, _u32p)))
     return out
+
+
+def l2_bandwidth(device=0, bytes_=48 << 20, reps=40) -> float:
+    """Measured L2 read bandwidth (GB/s) of `device`."""
+    out = C.c_double(0.0)
+    check(lib().hase_probe_l2_bandwidth(int(device), int(bytes_), int(reps), C.byref(out)))
+    return out.value
 
 
 def ray_map(weights, rays, phases):

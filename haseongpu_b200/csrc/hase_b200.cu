@@ -526,6 +526,21 @@ __global__ void philoxKernel(uint32_t n, const uint32_t* ctr, uint32_t k0, uint3
     out[4 * i + 3] = r.w;
 }
 
+// ---------------------------------------------------------- L2 probe ----
+// Reads an L2-resident buffer `reps` times with 16-byte loads from every SM;
+// the bench uses it as the measured L2 read bandwidth of the gather roofline.
+__global__ void __launch_bounds__(512) l2ProbeKernel(const float4* __restrict__ buf, size_t n, uint32_t reps,
+                                                     float* sink) {
+    float acc = 0.0f;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (uint32_t r = 0; r < reps; ++r)
+        for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            acc += v.x + v.y + v.z + v.w;
+        }
+    if (acc == 1234.5f) *sink = acc;  // keeps the loads; never true for a zeroed buffer
+}
+
 // -------------------------------------------------------- host side ----
 template <typename T>
 struct DevBuf {
@@ -1132,6 +1147,40 @@ hase_status hase_philox(uint32_t n, const uint32_t* ctr, const uint32_t key[2], 
     HASE_CUDA(cudaGetLastError());
     HASE_CUDA(cudaDeviceSynchronize());
     HASE_CUDA(cudaMemcpy(out, dout.p, 4 * size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return HASE_OK;
+}
+
+hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, double* gbPerSecond) {
+    if (!gbPerSecond || bytes < 1024 || reps == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return fail(HASE_INVALID_ARGUMENT, "device out of range");
+    HASE_CUDA(cudaSetDevice(device));
+    const size_t n = size_t(bytes / 16);
+    DevBuf<float4> buf;
+    DevBuf<float> sink;
+    HASE_CUDA(buf.ensure(n));
+    HASE_CUDA(sink.ensure(1));
+    HASE_CUDA(cudaMemset(buf.p, 0, n * sizeof(float4)));
+    int sms = 0;
+    HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    cudaEvent_t e0, e1;
+    HASE_CUDA(cudaEventCreate(&e0));
+    HASE_CUDA(cudaEventCreate(&e1));
+    l2ProbeKernel<<<sms * 4, 512>>>(buf.p, n, 1, sink.p);  // warm the L2
+    HASE_CUDA(cudaEventRecord(e0));
+    l2ProbeKernel<<<sms * 4, 512>>>(buf.p, n, reps, sink.p);
+    HASE_CUDA(cudaEventRecord(e1));
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    HASE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *gbPerSecond = double(n) * 16.0 * reps / (double(ms) * 1e-3) / 1e9;
     return HASE_OK;
 }
 

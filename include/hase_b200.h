@@ -153,6 +153,10 @@ hase_status hase_trace_rays(hase_context* ctx, uint32_t n, const float* start, c
                             const uint32_t* level, const uint32_t* sample, const uint32_t* slice,
                             uint32_t wavelength, float* lnGain, float* distance, uint32_t* dropped);
 
+/* Measurement support (no reference counterpart): L2 read bandwidth of
+ * `device` in GB/s, from `reps` passes over an L2-resident buffer of `bytes`. */
+hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, double* gbPerSecond);
+
 /* Philox4x32-10 on the device: out[i] = philox(ctr[i], key). */
 hase_status hase_philox(uint32_t n, const uint32_t* ctr, const uint32_t key[2], uint32_t* out);
 
