@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "hase_trace_rays",
     "hase_philox",
     "hase_probe_l2_bandwidth",
+    "hase_estimate_sample_noalloc",
 )
 
 _u32p = C.POINTER(C.c_uint32)
@@ -149,6 +150,8 @@ def lib():
                                       _f32p, _f32p, _u32p]
         L.hase_philox.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
         L.hase_probe_l2_bandwidth.argtypes = [C.c_int, C.c_uint64, C.c_uint32, _f64p]
+        L.hase_estimate_sample_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                                   C.c_uint32, C.c_uint32, C.c_void_p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version"):
                 getattr(L, name).restype = C.c_int

@@ -29,6 +29,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <unordered_map>
@@ -541,6 +542,29 @@ __global__ void __launch_bounds__(512) l2ProbeKernel(const float4* __restrict__ 
     if (acc == 1234.5f) *sink = acc;  // keeps the loads; never true for a zeroed buffer
 }
 
+// ------------------------------------------- allocation-free estimate ----
+// Scratch of hase_estimate_sample_noalloc: a file-scope device array, so that
+// entry point never allocates.  Every GPU that loads this library holds it
+// (about 4.2 MiB) until the process exits; all calls on one GPU share it.
+constexpr uint32_t kNoAllocMaxPrismSlices = 1u << 19;  // reflection slices x prisms per sample
+constexpr size_t kNoAllocQ = 0;                                              // u32 [max]
+constexpr size_t kNoAllocOffsets = kNoAllocQ + 4ull * kNoAllocMaxPrismSlices;  // u32 [max + 1]
+constexpr size_t kNoAllocSmall = kNoAllocOffsets + 4ull * kNoAllocMaxPrismSlices + 256;
+// small block: Q u64, active u32, itemCounter u32, nextActive u32, nextCount u32,
+// accSum f64, accSum2 f64, accTotal u32, accDrop u32, accCross u64, phi f32, mse f64
+constexpr size_t kNoAllocPartials = kNoAllocSmall + 256;  // f64, f64, u32, u64 [kMaxItems] each
+constexpr size_t kNoAllocBytes = kNoAllocPartials + size_t(kMaxItems) * (8 + 8 + 4 + 8);
+
+static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocBytes];
+
+__global__ void noAllocEmitKernel(const float* phi, const double* mse, const uint32_t* total, const uint32_t* drop,
+                                  double* out) {
+    out[0] = double(*phi);
+    out[1] = *mse;
+    out[2] = double(*total);
+    out[3] = double(*drop);
+}
+
 // -------------------------------------------------------- host side ----
 template <typename T>
 struct DevBuf {
@@ -819,6 +843,21 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
         if ((st = up(c->reflect, r)) != HASE_OK) return cleanup(st);
     }
     if ((st = uploadBeta(c, d->betaVolume)) != HASE_OK) return cleanup(st);
+    {  // resident spectrum and launch shape: hase_estimate_sample_noalloc allocates nothing
+        std::vector<float2> spec(c->sigmaA.size());
+        for (size_t l = 0; l < spec.size(); ++l)
+            spec[l] = make_float2(float(c->nTot * (c->sigmaE[l] + c->sigmaA[l])), float(c->nTot * c->sigmaA[l]));
+        if ((st = up(c->spec, spec)) != HASE_OK) return cleanup(st);
+    }
+    {
+        int perSM = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, rayKernel<kRayBlock, kRefill, kRayMinBlocks>,
+                                                          kRayBlock, 0) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+            return cleanup(fail(HASE_CUDA_ERROR, "occupancy query failed"));
+        c->persistentBlocks = uint32_t(std::max(1, perSM) * std::max(1, sms));
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(HASE_CUDA_ERROR, "upload failed"));
     *out = c;
     return HASE_OK;
 }
@@ -1181,6 +1220,88 @@ hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, d
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *gbPerSecond = double(n) * 16.0 * reps / (double(ms) * 1e-3) / 1e9;
+    return HASE_OK;
+}
+
+// hase_estimate_sample_noalloc: device address of g_noAllocScratch, looked up
+// once per device (with that device current) on the first call there.
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noAllocMutex;
+unsigned char* g_noAllocPtr[kMaxDevices] = {};
+}  // namespace
+
+hase_status hase_estimate_sample_noalloc(hase_context* c, uint32_t sample, const float* deviceWeights, uint32_t rays,
+                                         uint32_t rngSeed, uint32_t useReflections, uint32_t nearFieldSampling,
+                                         double* deviceResult) {
+    if (!c || !deviceWeights || !deviceResult) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (sample >= c->Np * c->L) return fail(HASE_INVALID_ARGUMENT, "sample %u out of range", sample);
+    if (rays == 0 || rays > (1u << 31)) return fail(HASE_INVALID_ARGUMENT, "rays must be in [1, 2^31]");
+    const uint32_t slices = useReflections ? 5u : 1u;
+    const uint64_t nW = uint64_t(slices) * c->P;
+    if (nW > kNoAllocMaxPrismSlices)
+        return fail(HASE_INVALID_ARGUMENT,
+                    "%llu prism slices exceed the allocation-free limit of %u (reflection slices x prisms)",
+                    (unsigned long long)nW, kNoAllocMaxPrismSlices);
+    if (c->device < 0 || c->device >= kMaxDevices) return fail(HASE_INVALID_ARGUMENT, "device index too large");
+    HASE_TRY(setDevice(c));
+    unsigned char* base;
+    {
+        std::lock_guard<std::mutex> lock(g_noAllocMutex);
+        if (!g_noAllocPtr[c->device]) {
+            void* ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noAllocScratch);
+            if (e != cudaSuccess || !ptr)
+                return fail(HASE_CUDA_ERROR, "cudaGetSymbolAddress(g_noAllocScratch): %s", cudaGetErrorString(e));
+            g_noAllocPtr[c->device] = static_cast<unsigned char*>(ptr);
+        }
+        base = g_noAllocPtr[c->device];
+    }
+    uint32_t* q = reinterpret_cast<uint32_t*>(base + kNoAllocQ);
+    uint32_t* offsets = reinterpret_cast<uint32_t*>(base + kNoAllocOffsets);
+    unsigned char* small = base + kNoAllocSmall;
+    unsigned long long* Q = reinterpret_cast<unsigned long long*>(small + 0);
+    uint32_t* active = reinterpret_cast<uint32_t*>(small + 8);
+    unsigned int* itemCounter = reinterpret_cast<unsigned int*>(small + 12);
+    uint32_t* nextActive = reinterpret_cast<uint32_t*>(small + 16);
+    uint32_t* nextCount = reinterpret_cast<uint32_t*>(small + 20);
+    double* accSum = reinterpret_cast<double*>(small + 24);
+    double* accSum2 = reinterpret_cast<double*>(small + 32);
+    uint32_t* accTotal = reinterpret_cast<uint32_t*>(small + 40);
+    uint32_t* accDrop = reinterpret_cast<uint32_t*>(small + 44);
+    unsigned long long* accCross = reinterpret_cast<unsigned long long*>(small + 48);
+    float* phi = reinterpret_cast<float*>(small + 56);
+    double* mse = reinterpret_cast<double*>(small + 64);
+    unsigned char* parts = base + kNoAllocPartials;
+    double* pSum = reinterpret_cast<double*>(parts);
+    double* pSum2 = reinterpret_cast<double*>(parts + 8ull * kMaxItems);
+    uint32_t* pDrop = reinterpret_cast<uint32_t*>(parts + 16ull * kMaxItems);
+    unsigned long long* pCross = reinterpret_cast<unsigned long long*>(parts + 20ull * kMaxItems);
+
+    // The scratch keeps the previous call's contents: clear what must start at zero.
+    HASE_CUDA(cudaMemsetAsync(small, 0, 256, c->stream));  // Q, active = {row 0}, counters, accumulators
+    const MeshView mv = c->view();
+    MapLaunch ml{deviceWeights, 0, 1, active, uint32_t(nW), rays, nullptr, sample, 0u, rngSeed, 0u,
+                 nullptr, q, Q, offsets};
+    mapKernel<<<1, kMapBlock, 0, c->stream>>>(ml);
+    HASE_CUDA(cudaGetLastError());
+    const uint32_t itemRays = std::max<uint32_t>(kMinItemRays, (rays + kMaxItems - 1) / kMaxItems);
+    const uint32_t items = (rays + itemRays - 1) / itemRays;
+    const double C = c->nTot / (4.0 * kPi * c->tau);
+    RayLaunch rl{mv, active, 1u, sample, 0u, rays, uint32_t(nW), itemRays, items, itemCounter, q, Q, offsets,
+                 rngSeed, 0u, c->spec.p, uint32_t(c->sigmaA.size()), nearFieldSampling, C, pSum, pSum2, pDrop,
+                 pCross};
+    // row 0 addresses sample `sample`: the kernels index rows relative to firstSample
+    const uint32_t grid = std::min<uint32_t>(items / (kRayBlock / 32) + 1, c->persistentBlocks);
+    rayKernel<kRayBlock, kRefill, kRayMinBlocks><<<grid, kRayBlock, 0, c->stream>>>(rl);
+    HASE_CUDA(cudaGetLastError());
+    FinalizeLaunch fl{active, 1u, items, rays, 1, 0.0, pSum, pSum2, pDrop, pCross, accSum, accSum2, accTotal,
+                      accDrop, accCross, phi, mse, nextActive, nextCount};
+    finalizeKernel<<<1, 128, 0, c->stream>>>(fl);
+    HASE_CUDA(cudaGetLastError());
+    noAllocEmitKernel<<<1, 1, 0, c->stream>>>(phi, mse, accTotal, accDrop, deviceResult);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
     return HASE_OK;
 }
 

@@ -153,6 +153,28 @@ hase_status hase_trace_rays(hase_context* ctx, uint32_t n, const float* start, c
                             const uint32_t* level, const uint32_t* sample, const uint32_t* slice,
                             uint32_t wavelength, float* lnGain, float* distance, uint32_t* dropped);
 
+/* Allocation-free estimate of one sample point (no counterpart in the
+ * reference).  For callers that must not allocate device memory -- code that
+ * runs while a CUDA stream is being captured into a graph, real-time loops
+ * whose memory is fixed up front, or hosts that hand out device memory through
+ * their own pool -- this entry point calls no cudaMalloc/cudaFree and no
+ * allocating library routine.  The caller passes device pointers:
+ * `deviceWeights` [slices * prisms] non-negative importance weights (slices =
+ * 5 with reflections, else 1; e.g. from hase_importance_weights) and
+ * `deviceResult` [4] doubles receiving phiAse, relative standard error, rays
+ * and dropped rays.  One pass of `rays` rays over all wavelengths of the
+ * context, like hase_calc_phi_ase with minRays = maxRays = rays for that
+ * single sample.  Scratch lives in a fixed ~4.2 MiB device array inside the
+ * library, so slices * prisms may be at most 524,288 (larger meshes are
+ * rejected with HASE_INVALID_ARGUMENT).  The first call on a device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  All calls on one device share the array: calls that overlap on
+ * the GPU (other host threads, other contexts on the same device) race and
+ * must be serialised by the caller.  Returns after the result is written. */
+hase_status hase_estimate_sample_noalloc(hase_context* ctx, uint32_t sample, const float* deviceWeights, uint32_t rays,
+                                         uint32_t rngSeed, uint32_t useReflections, uint32_t nearFieldSampling,
+                                         double* deviceResult);
+
 /* Measurement support (no reference counterpart): L2 read bandwidth of
  * `device` in GB/s, from `reps` passes over an L2-resident buffer of `bytes`. */
 hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, double* gbPerSecond);
