@@ -30,6 +30,8 @@ EXPORTED_SYMBOLS = (
     "hase_last_error_message",
     "hase_status_string",
     "hase_abi_version",
+    "hase_ray_kernel_variant_count",
+    "hase_ray_kernel_variant_name",
     "hase_context_create",
     "hase_context_update_beta",
     "hase_calc_phi_ase",
@@ -93,6 +95,7 @@ class ComputeDesc(C.Structure):
         ("raysPerThread", C.c_uint32),
         ("blockSize", C.c_uint32),
         ("workspaceBytes", C.c_uint64),
+        ("rayKernelVariant", C.c_uint32),
     ]
 
 
@@ -138,6 +141,9 @@ def lib():
         L.hase_status_string.restype = C.c_char_p
         L.hase_status_string.argtypes = [C.c_int]
         L.hase_abi_version.restype = C.c_int
+        L.hase_ray_kernel_variant_count.restype = C.c_int
+        L.hase_ray_kernel_variant_name.restype = C.c_char_p
+        L.hase_ray_kernel_variant_name.argtypes = [C.c_uint32]
         L.hase_context_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(SpectrumDesc), C.c_int,
                                           C.POINTER(C.c_void_p)]
         L.hase_context_update_beta.argtypes = [C.c_void_p, _f64p, _f64p]
@@ -153,7 +159,8 @@ def lib():
         L.hase_estimate_sample_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                                    C.c_uint32, C.c_uint32, C.c_void_p]
         for name in EXPORTED_SYMBOLS:
-            if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version"):
+            if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
+                            "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):
                 getattr(L, name).restype = C.c_int
         _lib = L
     return _lib

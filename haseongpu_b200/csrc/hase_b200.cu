@@ -413,6 +413,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     }
 }
 
+// Launch shapes of rayKernel the autotuner chooses from: block size, idle
+// lanes that trigger a refill, and the occupancy target (blocks per SM the
+// register budget is fitted to).  Entry 0 is the default.
+struct RayVariant {
+    void (*kernel)(RayLaunch);
+    int block;
+    const char* name;
+};
+const RayVariant kRayVariants[] = {
+    {rayKernel<256, 8, 5>, 256, "block256_refill8_occ5"},
+    {rayKernel<256, 4, 5>, 256, "block256_refill4_occ5"},
+    {rayKernel<256, 16, 5>, 256, "block256_refill16_occ5"},
+    {rayKernel<256, 8, 4>, 256, "block256_refill8_occ4"},
+    {rayKernel<256, 8, 6>, 256, "block256_refill8_occ6"},
+    {rayKernel<128, 8, 10>, 128, "block128_refill8_occ10"},
+    {rayKernel<128, 8, 12>, 128, "block128_refill8_occ12"},
+    {rayKernel<512, 8, 2>, 512, "block512_refill8_occ2"},
+};
+constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
+
 // ------------------------------------------------ (c)+(d) finalise ----
 struct FinalizeLaunch {
     const uint32_t* active;
@@ -679,6 +699,7 @@ struct hase_context {
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> itemCounter;
     uint32_t persistentBlocks = 0;  // resident rayKernel blocks on the device
+    uint32_t variantBlocks[16] = {};  // the same for every launch shape of kRayVariants
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
@@ -759,6 +780,12 @@ const char* hase_status_string(hase_status s) {
         case HASE_NO_DEVICE: return "no CUDA device";
     }
     return "unknown status";
+}
+
+int hase_ray_kernel_variant_count(void) { return int(kNumRayVariants); }
+
+const char* hase_ray_kernel_variant_name(uint32_t variant) {
+    return variant < kNumRayVariants ? kRayVariants[variant].name : "";
 }
 
 hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_desc* sp, int device,
@@ -925,6 +952,16 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     HASE_CUDA(c->activeB.ensure(rows));
     HASE_CUDA(c->counter.ensure(1));
     HASE_CUDA(c->itemCounter.ensure(1));
+    if (cp->rayKernelVariant >= kNumRayVariants)
+        return fail(HASE_INVALID_ARGUMENT, "rayKernelVariant %u >= %u", cp->rayKernelVariant, kNumRayVariants);
+    const uint32_t variant = cp->rayKernelVariant;
+    if (c->variantBlocks[variant] == 0) {
+        int perSM = 0, sms = 0;
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kRayVariants[variant].kernel,
+                                                                kRayVariants[variant].block, 0));
+        HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        c->variantBlocks[variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
+    }
     if (c->persistentBlocks == 0) {
         int perSM = 0, sms = 0;
         HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, rayKernel<kRayBlock, kRefill, kRayMinBlocks>, kRayBlock, 0));
@@ -988,18 +1025,21 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
                          nullptr, c->q.p, c->Q.p, c->offsets.p};
             mapKernel<<<nActive, kMapBlock, 0, c->stream>>>(ml);
             HASE_CUDA(cudaGetLastError());
-            const uint32_t itemRays = std::max<uint32_t>(kMinItemRays, (M + kMaxItems - 1) / kMaxItems);
+            const uint32_t itemRays = std::max<uint32_t>(cp->raysPerThread ? 32u * cp->raysPerThread : kMinItemRays,
+                                                         (M + kMaxItems - 1) / kMaxItems);
             const uint32_t items = (M + itemRays - 1) / itemRays;
             HASE_CUDA(cudaMemsetAsync(c->itemCounter.p, 0, sizeof(unsigned int), c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
             RayLaunch rl{mv, cur, nActive, firstSample, pass, M, nW, itemRays, items, c->itemCounter.p, c->q.p,
                          c->Q.p, c->offsets.p, cp->rngSeed, 0u, c->spec.p, nLambda, ex->nearFieldSampling, C, c->pSum.p, c->pSum2.p,
                          c->pDrop.p, c->pCross.p};
+            const RayVariant& rv = kRayVariants[variant];
             const uint64_t totalItems = uint64_t(nActive) * items;
-            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (kRayBlock / 32) + 1,
-                                                               uint64_t(c->persistentBlocks)));
-            rayKernel<kRayBlock, kRefill, kRayMinBlocks><<<grid, kRayBlock, 0, c->stream>>>(rl);
-            HASE_CUDA(cudaGetLastError());
+            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1,
+                                                               uint64_t(c->variantBlocks[variant])));
+            void* rayArgs[] = {&rl};
+            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(rv.kernel), dim3(grid), dim3(rv.block), rayArgs,
+                                       0, c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
             FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,

@@ -152,8 +152,10 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     return D2;
 }
 
-// One crossing.  Edge exits are compared as fractions num/den by cross
-// multiplication; one approximate division gives the chosen exit parameter.
+// One triangle column: the edge exit of the current triangle (edge exits are
+// compared as fractions num/den by cross multiplication; one approximate
+// division gives the chosen exit parameter), then every level plane crossed
+// before it.
 template <typename Loader>
 __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
     float4 a, b, c;
@@ -176,20 +178,23 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
     edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
     edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
     const float sEdge = fminf(__fdividef(bn, bd), r.s);
-    const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
-    const float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
-    const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
-    const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
-    if (next <= m.tolEnd) {
-        r.G = fmaf(g, r.s, r.G);
-        r.s = 0.0f;
-        return kDone;
-    }
-    r.G = fmaf(g, r.s - next, r.G);
-    r.s = next;
-    if (++r.steps >= kMaxSteps) return kDropped;
-    if (sz >= sEdge) {
-        const int dl = r.uz > 0.0f ? -1 : 1;
+    // Level planes crossed before the edge exit: the triangle, and with it
+    // sEdge, stays the same, so they cost no edge test.
+    const int dl = r.uz > 0.0f ? -1 : 1;
+    while (true) {
+        const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
+        const float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
+        const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
+        const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
+        if (next <= m.tolEnd) {
+            r.G = fmaf(g, r.s, r.G);
+            r.s = 0.0f;
+            return kDone;
+        }
+        r.G = fmaf(g, r.s - next, r.G);
+        r.s = next;
+        if (++r.steps >= kMaxSteps) return kDropped;
+        if (sz < sEdge) break;
         const int cand = r.phys + r.pdir * dl;
         if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
             if (r.reflLeft <= 0) return kDropped;
@@ -200,10 +205,9 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             r.phys = cand;
         }
         r.lu += dl;
-    } else {
-        r.t = uint32_t(bw) >> 2;
-        r.forb = bw & 3;
     }
+    r.t = uint32_t(bw) >> 2;
+    r.forb = bw & 3;
     return kContinue;
 }
 

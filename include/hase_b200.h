@@ -96,9 +96,12 @@ typedef struct {
     uint32_t rngSeed;
     uint32_t minSample;                 /* inclusive */
     uint32_t maxSample;                 /* inclusive; UINT32_MAX = last sample */
-    uint32_t raysPerThread;             /* 0 = default / autotuned */
+    uint32_t raysPerThread;             /* rays per lane of a ray-kernel work item (item = 32 x this);
+                                           0 = default (1024-ray items) */
     uint32_t blockSize;                 /* 0 = default / autotuned */
     uint64_t workspaceBytes;            /* 0 = default device workspace budget */
+    uint32_t rayKernelVariant;          /* launch shape of the ray kernel, 0 = default; see
+                                           hase_ray_kernel_variant_name (chosen by the autotuner) */
 } hase_compute_desc;
 
 /* Caller-allocated host arrays of (maxSample - minSample + 1) entries; any
@@ -124,6 +127,9 @@ typedef struct {
 const char* hase_last_error_message(void);
 const char* hase_status_string(hase_status status);
 int hase_abi_version(void);
+/* Launch shapes of the ray kernel (hase_compute_desc.rayKernelVariant). */
+int hase_ray_kernel_variant_count(void);
+const char* hase_ray_kernel_variant_name(uint32_t variant);
 
 hase_status hase_context_create(const hase_mesh_desc* mesh, const hase_spectrum_desc* spectrum, int device,
                                 hase_context** out);

@@ -296,3 +296,18 @@ def test_invalid_arguments_raise():
             ctx.calc_phi_ase(minRays=10, minSample=5, maxSample=mesh.numberOfSamples)
         with pytest.raises(HaseError):
             ctx.update_beta(np.full(mesh.numberOfPrisms, np.nan))
+
+
+def test_every_ray_kernel_variant_gives_the_same_estimate():
+    """The autotuner's launch shapes change scheduling only: identical results."""
+    from haseongpu_b200.autotune import RAYS_PER_LANE, variant_names
+
+    mesh = legacy_mesh("cylindrical")
+    sa, se = legacy_spectrum("cylindrical")
+    with _ctx(mesh, sa, se) as ctx:
+        ref = ctx.calc_phi_ase(minRays=20000, rngSeed=4, maxSample=63)
+        for v in range(len(variant_names())):
+            for rpt in (RAYS_PER_LANE[0], RAYS_PER_LANE[-1]):
+                r = ctx.calc_phi_ase(minRays=20000, rngSeed=4, maxSample=63, rayKernelVariant=v, raysPerThread=rpt)
+                np.testing.assert_allclose(r.phiAse, ref.phiAse, rtol=1e-6)
+                np.testing.assert_array_equal(r.totalRays, ref.totalRays)
