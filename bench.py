@@ -273,7 +273,9 @@ def run_ours(args):
                        "adaptive_steps": w.adaptiveSteps, "parallelism": f"sample batches x{world}",
                        "l2": "flushed (256 MiB write) before every timed step; per-step weights > L2",
                        "ray_kernel": {"variant": tuned.name, "rays_per_item": 32 * tuned.raysPerThread,
-                                      "autotuned_ms": tuned.milliseconds}},
+                                      "autotuned_ms": tuned.milliseconds},
+                       "importance_kernel": {"layers_per_thread": tuned.importanceLayers,
+                                             "autotuned_ms": tuned.importanceMilliseconds}},
             "time_to_threshold_ms": statistics.median(steps_ms),
             "breakdown_ms_per_step": {"importance": imp_ms / args.steps, "rays": ray_ms / args.steps,
                                       "map_finalize_copies": (dev_ms - imp_ms - ray_ms) / args.steps},

@@ -96,6 +96,7 @@ class ComputeDesc(C.Structure):
         ("blockSize", C.c_uint32),
         ("workspaceBytes", C.c_uint64),
         ("rayKernelVariant", C.c_uint32),
+        ("importanceLayers", C.c_uint32),
     ]
 
 

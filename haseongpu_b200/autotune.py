@@ -26,9 +26,12 @@ class TuneResult:
     name: str
     milliseconds: float
     table: list
+    importanceLayers: int = 0
+    importanceMilliseconds: float = 0.0
 
     def kwargs(self) -> dict:
-        return {"rayKernelVariant": self.rayKernelVariant, "raysPerThread": self.raysPerThread}
+        return {"rayKernelVariant": self.rayKernelVariant, "raysPerThread": self.raysPerThread,
+                "importanceLayers": self.importanceLayers}
 
 
 def variant_names() -> list[str]:
@@ -56,6 +59,14 @@ def autotune(ctx, *, firstSample: int, samples: int, rays: int, useReflections: 
             table.append({"variant": v, "name": name, "raysPerThread": rpt, "ray_ms": t})
             if best is None or t < best[2]:
                 best = (v, rpt, t)
-    result = TuneResult(best[0], best[1], names[best[0]], best[2], table)
+    imp = []
+    for layers in (4, 8):
+        t = min(ctx.calc_phi_ase(minRays=1, maxRays=1, useReflections=useReflections, monochromatic=monochromatic,
+                                 nearFieldSampling=nearFieldSampling, rngSeed=3, minSample=firstSample,
+                                 maxSample=firstSample + samples - 1, importanceLayers=layers).importanceMilliseconds
+                for _ in range(repeats))
+        imp.append((t, layers))
+        table.append({"importanceLayers": layers, "importance_ms": t})
+    result = TuneResult(best[0], best[1], names[best[0]], best[2], table, min(imp)[1], min(imp)[0])
     _cache[key] = result
     return result

@@ -124,40 +124,139 @@ struct ImportanceLaunch {
     float* lnw;   // [rows][nW]
 };
 
+// One thread per (sample, reflection slice, triangle, group of G layers): the
+// straight lines from the centres of the G prisms (t, l) to the (image)
+// sample point all project onto the same 2-D segment, centroid -> sample
+// point, so they cross the same triangles at the same 2-D distances sigma.
+// The thread walks that 2-D segment once (edge tests shared by the G lines)
+// and, per line, the level planes and top/bottom reflections inside each
+// triangle: plane k of line l lies at sigma = D2 (k - kImg) / (l + 1/2 - kImg).
+// ln w = ln(beta V / d^2) + Int g dl, Int g dl = (D3 / D2) Int g dsigma.
+template <int G>
 __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= L.nW) return;
-    const uint32_t row = blockIdx.y;
     const MeshView& m = L.m;
+    const uint32_t groups = (m.layers + G - 1) / G;
+    const uint32_t perSlice = groups * m.T;
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L.slices * perSlice) return;
+    const uint32_t row = blockIdx.y;
+    const uint32_t j = idx / perSlice;
+    const uint32_t rem = idx - j * perSlice;
+    const uint32_t grp = rem / m.T, t = rem - grp * m.T;
+    const int l0 = int(grp * G);
     const uint32_t sample = L.firstSample + row;
-    const uint32_t j = b / m.P, p = b - j * m.P;
-    const uint32_t t = p % m.T, l = p / m.T;
-    float* out = L.lnw + size_t(row) * L.nW + b;
-    const float beta = __ldg(m.srcBeta + p);
-    if (!(beta > 0.0f)) {
-        *out = -INFINITY;
-        return;
-    }
     const float2 S = __ldg(m.points + sample % m.Np);
     const int ls = int(sample / m.Np);
     const int kImg = imageLevel(ls, int(m.layers), j);
     const float2 c = __ldg(m.centroid + t);
     const float area = __ldg(&m.geo[2 * t + 1].z);
-    Ray r;
-    const float D2 = initRay(r, t, int(l), c.x - S.x, c.y - S.y, (float(int(l) - kImg) + 0.5f) * m.h, kImg, j, L.A,
-                             L.B, m.h);
-    GlobalLoader load{m.tri};
-    int st;
-    do {
-        st = stepRay(m, S.x, S.y, r, load);
-    } while (st == kContinue);
-    if (st == kDropped || !(D2 > 0.0f)) {
-        *out = -INFINITY;
-        return;
+    const float dx = c.x - S.x, dy = c.y - S.y;
+    const float D2 = sqrtf(fmaf(dx, dx, dy * dy));
+    const float inv2 = 1.0f / D2;
+    const float ux = dx * inv2, uy = dy * inv2;
+    float* out = L.lnw + size_t(row) * L.nW + size_t(j) * m.P + t;
+
+    float J[G], lnR[G], invc[G];
+    int ka[G], phys[G], pdir[G], left[G];
+    bool ok[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int l = l0 + g;
+        ok[g] = l < int(m.layers) && __ldg(m.srcBeta + size_t(min(l, int(m.layers) - 1)) * m.T + t) > 0.0f;
+        J[g] = 0.0f;
+        lnR[g] = 0.0f;
+        ka[g] = l;
+        phys[g] = l;
+        pdir[g] = 1;
+        left[g] = expectedReflections(j);
+        invc[g] = D2 / (float(l - kImg) + 0.5f);
     }
-    finishReflections(m, r);
-    *out = __logf(beta * area * m.h / D2) + r.G;
+    GlobalLoader load{m.tri};
+    uint32_t tk = t;
+    int forb = -1;
+    float sc = D2;
+    bool done = false;
+    for (int step = 0; step < kMaxSteps && !done; ++step) {
+        float4 a, b, cc;
+        load(tk, a, b, cc);
+        float bn = -1.0f, bd = 0.0f;
+        int bw = -1;
+        const auto edge = [&](float nx, float ny, float ce, int nbw, int e) {
+            const float dd = -fmaf(nx, ux, ny * uy);
+            const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
+            const bool okE = (e != forb) & (dd > 0.0f) & (nbw >= 0);
+            if (okE && nm * bd > bn * dd) {
+                bn = nm;
+                bd = dd;
+                bw = nbw;
+            }
+        };
+        edge(a.x, a.y, a.z, __float_as_int(cc.y), 0);
+        edge(a.w, b.x, b.y, __float_as_int(cc.z), 1);
+        edge(b.z, b.w, cc.x, __float_as_int(cc.w), 2);
+        float sOut = fmaxf(fminf(__fdividef(bn, bd), sc), 0.0f);
+        if (sOut <= m.tolEnd) {
+            sOut = 0.0f;
+            done = true;
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            if (!ok[g]) continue;
+            const int dl = kImg > l0 + g ? 1 : -1;  // layer step toward the image level
+            float s = sc;
+            while (true) {
+                const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg) * invc[g];
+                if (!(sb > sOut)) break;
+                const float gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
+                J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sb, J[g]);
+                s = sb;
+                const int cand = phys[g] + pdir[g] * dl;
+                if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+                    if (left[g] <= 0) {
+                        ok[g] = false;
+                        break;
+                    }
+                    const float dz = (float(l0 + g - kImg) + 0.5f) * m.h;
+                    const float uz = dz * rsqrtf(fmaf(D2, D2, dz * dz));
+                    lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, uz));
+                    --left[g];
+                    pdir[g] = -pdir[g];
+                } else {
+                    phys[g] = cand;
+                }
+                ka[g] += dl;
+            }
+            if (!ok[g]) continue;
+            const float gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
+            J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sOut, J[g]);
+        }
+        if (!done) {
+            tk = uint32_t(bw) >> 2;
+            forb = bw & 3;
+            sc = sOut;
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int l = l0 + g;
+        if (l >= int(m.layers)) continue;
+        float v = -INFINITY;
+        if (ok[g] && done) {
+            const float dz = (float(l - kImg) + 0.5f) * m.h;
+            const float D3sq = fmaf(D2, D2, dz * dz);
+            if (left[g] > 0) {  // the bounce happens at the target itself, in the final triangle
+                const int dl = kImg > l ? 1 : -1;
+                const int cand = phys[g] + pdir[g] * dl;
+                lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
+            }
+            const float beta = __ldg(m.srcBeta + size_t(l) * m.T + t);
+            v = __logf(beta * area * m.h / D3sq) + J[g] * (sqrtf(D3sq) * inv2) + lnR[g];
+        }
+        out[size_t(l) * m.T] = v;
+    }
 }
+
+constexpr int kImportanceLayers = 8;  // layers per importance thread
 
 // ------------------------------------------------------- (a2) ray map ----
 struct MapLaunch {
@@ -952,6 +1051,8 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     HASE_CUDA(c->activeB.ensure(rows));
     HASE_CUDA(c->counter.ensure(1));
     HASE_CUDA(c->itemCounter.ensure(1));
+    if (cp->importanceLayers != 0 && cp->importanceLayers != 4 && cp->importanceLayers != kImportanceLayers)
+        return fail(HASE_INVALID_ARGUMENT, "importanceLayers must be 0, 4 or %d", kImportanceLayers);
     if (cp->rayKernelVariant >= kNumRayVariants)
         return fail(HASE_INVALID_ARGUMENT, "rayKernelVariant %u >= %u", cp->rayKernelVariant, kNumRayVariants);
     const uint32_t variant = cp->rayKernelVariant;
@@ -1001,7 +1102,13 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
         const uint32_t firstSample = first + b0;
         HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
         ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p};
-        importanceKernel<<<dim3((nW + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+        if (cp->importanceLayers == 4) {
+            const uint32_t impThreads = slices * ((c->layers + 3) / 4) * c->T;
+            importanceKernel<4><<<dim3((impThreads + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+        } else {
+            const uint32_t impThreads = slices * ((c->layers + kImportanceLayers - 1) / kImportanceLayers) * c->T;
+            importanceKernel<kImportanceLayers><<<dim3((impThreads + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+        }
         HASE_CUDA(cudaGetLastError());
         HASE_CUDA(cudaEventRecord(c->ev[1], c->stream));
         HASE_CUDA(cudaMemsetAsync(c->accSum.p, 0, nRows * sizeof(double), c->stream));
@@ -1127,7 +1234,8 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
     HASE_CUDA(Q.ensure(count));
     ImportanceLaunch il{c->view(), firstSample, slices, nW, float(meanA), float(meanB), lnw.p};
-    importanceKernel<<<dim3((nW + 255) / 256, count), 256, 0, c->stream>>>(il);
+    const uint32_t impThreads = slices * ((c->layers + kImportanceLayers - 1) / kImportanceLayers) * c->T;
+    importanceKernel<kImportanceLayers><<<dim3((impThreads + 255) / 256, count), 256, 0, c->stream>>>(il);
     HASE_CUDA(cudaGetLastError());
     MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
     mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);

@@ -137,8 +137,29 @@ def disc_points(radius: float, rings: int, rng: np.random.Generator, jitter: flo
     return np.vstack(pts)
 
 
-def delaunay_triangles(points: np.ndarray) -> np.ndarray:
-    """Delaunay triangulation (scipy/Qhull), counter-clockwise, slivers removed."""
+def morton_order(xy: np.ndarray, bits: int = 16) -> np.ndarray:
+    """Permutation sorting 2-D positions along a Z-order (Morton) curve."""
+    xy = np.asarray(xy, np.float64)
+    lo, hi = xy.min(axis=0), xy.max(axis=0)
+    q = ((xy - lo) / np.maximum(hi - lo, 1e-300) * ((1 << bits) - 1)).astype(np.uint64)
+
+    def spread(v):
+        v = v & np.uint64(0xFFFF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
+        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
+        return v
+
+    return np.argsort(spread(q[:, 0]) | (spread(q[:, 1]) << np.uint64(1)), kind="stable")
+
+
+def delaunay_triangles(points: np.ndarray, spatial_order: bool = True) -> np.ndarray:
+    """Delaunay triangulation (scipy/Qhull), counter-clockwise, slivers removed.
+
+    With ``spatial_order`` the triangles are numbered along a Morton curve of
+    their centroids, so neighbouring prism indices are neighbouring prisms
+    (warps then walk nearby rays)."""
     from scipy.spatial import Delaunay
 
     tri = Delaunay(points).simplices.astype(np.int64)
@@ -146,7 +167,10 @@ def delaunay_triangles(points: np.ndarray) -> np.ndarray:
     cross = (p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1]) - (p[:, 1, 1] - p[:, 0, 1]) * (p[:, 2, 0] - p[:, 0, 0])
     tri[cross < 0] = tri[cross < 0][:, [0, 2, 1]]
     keep = np.abs(cross) > 1e-12 * np.max(np.abs(cross))
-    return tri[keep].astype(np.uint32)
+    tri = tri[keep]
+    if spatial_order:
+        tri = tri[morton_order(points[tri].mean(axis=1))]
+    return tri.astype(np.uint32)
 
 
 def gaussian_pump_beta(mesh_points, triangles, levels, thickness, waist=0.4, depth=0.5, base=0.05, peak=0.25):

@@ -98,7 +98,7 @@ class DeviceMesh:
 
     def calc_phi_ase(self, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
                      nearFieldSampling=True, adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
-                     blockSize=0, workspaceBytes=0, rayKernelVariant=0) -> Result:
+                     blockSize=0, workspaceBytes=0, rayKernelVariant=0, importanceLayers=0) -> Result:
         S = self.mesh.numberOfSamples
         maxSample = S - 1 if maxSample is None else int(maxSample)
         n = maxSample - int(minSample) + 1
@@ -109,7 +109,8 @@ class DeviceMesh:
         ex = N.ExperimentDesc(int(minRays), int(maxRays if maxRays is not None else minRays), float(mseThreshold),
                               1 if useReflections else 0, 1 if monochromatic else 0, 1 if nearFieldSampling else 0)
         cp = N.ComputeDesc(int(adaptiveSteps), int(repetitions), int(rngSeed) & 0xFFFFFFFF, int(minSample), maxSample,
-                           int(raysPerThread), int(blockSize), int(workspaceBytes), int(rayKernelVariant))
+                           int(raysPerThread), int(blockSize), int(workspaceBytes), int(rayKernelVariant),
+                           int(importanceLayers))
         r = N.ResultDesc(N.ptr(out.phiAse, N._f32p), N.ptr(out.standardError, N._f64p),
                          N.ptr(out.relativeStandardError, N._f64p), N.ptr(out.totalRays, N._u32p),
                          N.ptr(out.dndtAse, N._f64p), N.ptr(out.droppedRays, N._u32p))

@@ -88,6 +88,19 @@ def test_trace_with_reflections_matches_oracle(oracle):
     assert np.quantile(err, 0.999) < 1e-5 and err.max() < 5e-4, (err.max(), np.quantile(err, 0.999))
 
 
+def test_importance_layer_groups_agree():
+    from haseongpu_b200.configs import disc_poly
+
+    w = disc_poly()
+    sa, se = w.spectra.resampled()
+    with _ctx(w.mesh, sa, se) as ctx:
+        a = ctx.calc_phi_ase(minRays=3000, useReflections=True, rngSeed=5, minSample=100, maxSample=131,
+                             importanceLayers=4)
+        b = ctx.calc_phi_ase(minRays=3000, useReflections=True, rngSeed=5, minSample=100, maxSample=131,
+                             importanceLayers=8)
+    np.testing.assert_allclose(a.phiAse, b.phiAse, rtol=1e-5)
+
+
 @pytest.mark.parametrize("reflections", [False, True])
 def test_importance_weights_match_oracle(oracle, reflections):
     from haseongpu_b200.configs import disc_poly, disc_small
