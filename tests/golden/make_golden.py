@@ -23,6 +23,13 @@ What it extracts (all citations are paths inside the reference project):
   N_tot and the fluorescence lifetime are not stored in that archive; the
   medium it was generated from (``example/laserPumpCladdingApi.py:240-241``)
   uses N_tot = 2 * 1.388e20 cm^-3 and tau = 9.41e-4 s.
+* ``tet4_true_cladding.npz`` -- the Tet4 twin of that disc
+  (``example/data/ptTet4.vtk``, three tetrahedra per wedge) with the cladding
+  tags and beta of the true-cladding run, and the reference's own forward
+  Tet4 volume integrals (total / gain / cladding for absorption 0, 5.5,
+  55 cm^-1) parsed from the table in that fixture's README.md.
+* ``tet4_cylindrical.npz`` -- ``example/data/cylindrical.vtk`` as Tet4 cells
+  with its per-cell betaVolume and material attributes.
 * ``mesh_tables.npz`` -- the reference's own per-triangle tables
   (``pyInclude/geometry/core.py:_derived_topology``: centres, surfaces, edge
   normals, normal points, neighbours, forbidden edges) for the three meshes
@@ -175,6 +182,72 @@ def _legacy_true_cladding(ref: Path, out: Path):
     return points3[:n_points, :2].copy(), triangles
 
 
+def _readme_integrals(readme: Path):
+    """Rows '| absorption | partition | legacy | current Tet4 | bias |' of the README table."""
+    import re
+
+    rows = []
+    for line in readme.read_text(encoding="utf-8").splitlines():
+        m = re.match(r"\|\s*([0-9.]+)\s*\|\s*(total|gain|cladding)\s*\|\s*([0-9.eE+-]+)\s*\|\s*([0-9.eE+-]+)\s*\|", line)
+        if m:
+            rows.append((float(m.group(1)), m.group(2), float(m.group(3)), float(m.group(4))))
+    return rows
+
+
+def _tet4_true_cladding(ref: Path, out: Path):
+    vtk = _load_module(ref / "pyInclude" / "geometry" / "vtk.py", "_ref_vtk")
+    points, cells, cell_types, point_data, cell_data, fields = vtk._parseVtk(ref / "example" / "data" / "ptTet4.vtk")
+    tets = np.asarray(cells, dtype=np.uint32)
+    base = ref / "tests" / "data" / "laserPumpCladding" / "true_cladding_no_reflection_phiase_reference"
+    d = np.load(base / "phiase_reference.npz")
+    meta = json.loads(str(d["metadata"]))
+    wedge_types = d["wedgeCladdingCellTypes"].astype(np.uint32)
+    tet_types = np.repeat(wedge_types, 3)
+    assert tets.shape == (3 * wedge_types.size, 4)
+    for wedge, children in zip(d["cells"], tets.reshape(-1, 3, 4)):
+        assert np.array_equal(np.unique(children), np.sort(wedge))
+    mat = meta["material"]
+    beta = np.where(tet_types == mat["claddingNumber"], 0.0, mat["gainBetaVolume"])
+    rows = _readme_integrals(base / "README.md")
+    absorptions = np.asarray(mat["claddingAbsorptions"], np.float64)
+    parts = ("total", "gain", "cladding")
+    current = np.zeros((absorptions.size, 3))
+    legacy = np.zeros((absorptions.size, 3))
+    for a, part, leg, cur in rows:
+        i = int(np.argmin(np.abs(absorptions - a)))
+        current[i, parts.index(part)] = cur
+        legacy[i, parts.index(part)] = leg
+    assert np.all(current > 0)
+    np.savez_compressed(
+        out, points=np.asarray(points, np.float64), cells=tets, betaVolume=beta, claddingCellTypes=tet_types,
+        claddingNumber=np.uint32(mat["claddingNumber"]), claddingAbsorptions=absorptions,
+        nTot=np.float64(2 * 1.388e20), crystalTFluo=np.float64(9.41e-4),
+        sigmaA=np.float64(mat["crossSectionAbsorption"]), sigmaE=np.float64(mat["crossSectionEmission"]),
+        currentIntegrals=current, legacyIntegrals=legacy, partitions=np.asarray(parts),
+        provenance=np.asarray(json.dumps({
+            "geometry": "example/data/ptTet4.vtk",
+            "integrals": str((base / "README.md").relative_to(ref)),
+            "note": "current Tet4 = the reference's forward estimator, no reflections, monochromatic",
+        })))
+
+
+def _tet4_from_vtk(ref: Path, name: str, out: Path):
+    vtk = _load_module(ref / "pyInclude" / "geometry" / "vtk.py", "_ref_vtk")
+    points, cells, cell_types, point_data, cell_data, fields = vtk._parseVtk(ref / "example" / "data" / f"{name}.vtk")
+    sigma_a = np.loadtxt(ref / "example" / "input" / "sigma_a.txt")
+    sigma_e = np.loadtxt(ref / "example" / "input" / "sigma_e.txt")
+    np.savez_compressed(
+        out, points=np.asarray(points, np.float64), cells=np.asarray(cells, np.uint32),
+        betaVolume=np.asarray(cell_data["betaVolume"], np.float64),
+        claddingCellTypes=np.asarray(fields["claddingCellTypes"], np.uint32),
+        claddingNumber=np.uint32(np.asarray(fields["claddingNumber"]).ravel()[0]),
+        claddingAbsorption=np.float64(np.asarray(fields["claddingAbsorption"]).ravel()[0]),
+        nTot=np.float64(np.asarray(fields["nTot"]).ravel()[0]),
+        crystalTFluo=np.float64(np.asarray(fields["crystalTFluo"]).ravel()[0]),
+        sigmaA=np.float64(sigma_a.ravel()[0]), sigmaE=np.float64(sigma_e.ravel()[0]),
+        provenance=np.asarray(json.dumps({"geometry": f"example/data/{name}.vtk"})))
+
+
 def _mesh_tables(ref: Path, meshes, out: Path):
     sys.path.insert(0, str(ref))
     from pyInclude.geometry import core  # noqa: PLC0415  (reference frontend, importable here)
@@ -206,6 +279,8 @@ def main(argv=None):
     for name in ("cuboid", "cylindrical"):
         meshes[name] = _legacy_compare_serial(ref, name, HERE / f"legacy_{name}.npz")
     meshes["true_cladding"] = _legacy_true_cladding(ref, HERE / "legacy_true_cladding.npz")
+    _tet4_true_cladding(ref, HERE / "tet4_true_cladding.npz")
+    _tet4_from_vtk(ref, "cylindrical", HERE / "tet4_cylindrical.npz")
     _mesh_tables(ref, meshes, HERE / "mesh_tables.npz")
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
