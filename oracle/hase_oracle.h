@@ -107,6 +107,68 @@ int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum,
                    const oracle_experiment* experiment, const float* weightsOverride,
                    int threads, oracle_result* result);
 
+
+/* ---- forward Tet4 estimator (the reference's current calcPhiASE) ----
+ * Restates include/kernels/forward/accumulation.hpp:369-453 (source rays by
+ * stratified beta*V CDF, uniform point in the tet, isotropic direction,
+ * stratified wavelength bin; walk out of the mesh; per crossed cell the
+ * track-length tally weight * G * (exp(g l) - 1)/g split to the cell's four
+ * material vertices by the segment-midpoint barycentric weights) and the
+ * finaliser include/kernels/forwardPhiAseMapping.hpp:51-150 (vertex -> cell
+ * density through lumped vertex volumes, estimate S B / (N V) * N_tot/tau,
+ * relative error of the batch means). */
+typedef struct {
+    uint32_t numberOfPoints;
+    uint32_t numberOfCells;
+    const double* points;              /* [Np][3] */
+    const uint32_t* cells;             /* [C][4] */
+    const double* betaVolume;          /* [C] */
+    const uint32_t* claddingCellTypes; /* [C] or NULL */
+    uint32_t claddingNumber;
+    double claddingAbsorption;
+    double nTot;
+    double crystalTFluo;
+} oracle_tet_mesh;
+
+typedef struct {
+    uint32_t minRays;
+    uint32_t maxRays;
+    uint32_t adaptiveSteps;
+    double rseThreshold;
+    uint32_t seed;
+    uint32_t batches;          /* statistical batches (reference default 8) */
+} oracle_forward_experiment;
+
+typedef struct {
+    double* phiAse;            /* [C] */
+    double* relativeStandardError;
+    double* dndtAse;
+    uint32_t* droppedRays;     /* [C] */
+    uint32_t* rayVisits;       /* [C] segments tallied per cell (the reference's forward totalRays), or NULL */
+    uint64_t totalRays;
+    uint32_t launches;
+} oracle_forward_result;
+
+/* Tet tables: neighbours [C][4] (-1 boundary), neighbour local face [C][4],
+ * barycentric gradients [C][4][3] (lambda_f(x) = delta_f0 + grad_f.(x - v0)),
+ * volumes [C]. */
+int oracle_tet_tables(const oracle_tet_mesh* mesh, int32_t* neighbors, int32_t* neighborFace, double* gradients,
+                      double* volumes);
+
+int oracle_forward_phi_ase(const oracle_tet_mesh* mesh, const oracle_spectrum* spectrum,
+                           const oracle_forward_experiment* experiment, int threads, oracle_forward_result* result);
+
+/* Single rays through the Tet4 mesh (no tally): ray i starts at origin[i] in
+ * startCell[i] along the unit direction[i].  segments[i] = cells crossed (a
+ * zero-length step counts), cells/lengths [n][maxSegments] the first
+ * maxSegments of them (either may be NULL), lnGain[i] = sum g l at
+ * `wavelength`, endPoint[i] where the walk stopped, status[i] 0 = left the
+ * mesh, 1 = walk failed. */
+int oracle_tet_trace(const oracle_tet_mesh* mesh, const oracle_spectrum* spectrum, uint32_t wavelength, uint32_t n,
+                     const uint32_t* startCell, const double* origin, const double* direction, uint32_t maxSegments,
+                     uint32_t* segments, uint32_t* cells, double* lengths, double* lnGain, double* endPoint,
+                     int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,421 @@
+// hase_oracle_forward.cpp -- FP64 CPU restatement of HASEonGPU's forward
+// Tet4 phi-ASE estimator (the reference's current calcPhiASE).
+//
+// TEST INFRASTRUCTURE ONLY (the checker): the product library never links
+// this file.  Method (reference paths):
+//   source rays   include/kernels/forward/accumulation.hpp:369-453,
+//                 include/kernels/forward/volumeSampling.hpp:19-161
+//                 (stratified beta*V CDF per statistical batch, uniform point
+//                 in the tet from four exponentials, isotropic direction,
+//                 stratified wavelength bin)
+//   walk + tally  include/kernels/forward/rayWalk.hpp:106-208,
+//                 include/kernels/forward/accumulation.hpp:300-352
+//                 (barycentric face planes; per crossed cell the tally
+//                 weight * G * (exp(g l) - 1)/g split to the four material
+//                 vertices by the segment-midpoint barycentric weights,
+//                 then G *= exp(g l); rays escape at the mesh boundary)
+//   finalise      include/kernels/forwardPhiAseMapping.hpp:51-150,
+//                 include/kernels/vertexAccumulation.hpp:17-68
+//                 (vertex -> cell density through lumped material vertex
+//                 volumes, estimate S B / (N V) * N_tot/tau, relative error
+//                 of the batch means, cells with dropped rays never converge)
+//   adaptive loop include/core/forwardPhiAseEvaluator.hpp:114-178 (rays of a
+//                 launch are added to the previous launches).
+// The random streams are this project's own Philox4x32-10 counters (the
+// reference's alpaka generator layout is not pinned bit for bit).
+#include "hase_oracle.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr uint32_t kTagFwdBatch = 2u;
+constexpr uint32_t kTagFwdRay = 3u;
+constexpr uint32_t kFwdKeyHi = 1u;
+constexpr int kMaxSteps = 10000;
+constexpr double kPi = 3.14159265358979323846;
+
+inline double unit(uint32_t x) { return (double(x >> 8) + 0.5) * (1.0 / 16777216.0); }
+
+struct TetTables {
+    uint32_t C = 0, Np = 0;
+    std::vector<int32_t> nbr, nbrFace;  // [C][4]
+    std::vector<double> grad;           // [C][4][3]
+    std::vector<double> plane;          // [C][4][4]: lambda_f(x) = a.x + d
+    std::vector<double> vol;            // [C]
+};
+
+int buildTetTables(const oracle_tet_mesh* m, TetTables& t) {
+    t.C = m->numberOfCells;
+    t.Np = m->numberOfPoints;
+    t.nbr.assign(4 * size_t(t.C), -1);
+    t.nbrFace.assign(4 * size_t(t.C), -1);
+    t.grad.assign(12 * size_t(t.C), 0.0);
+    t.plane.assign(16 * size_t(t.C), 0.0);
+    t.vol.assign(t.C, 0.0);
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, std::pair<uint32_t, int>> open;
+    for (uint32_t c = 0; c < t.C; ++c) {
+        const uint32_t* v = m->cells + 4 * size_t(c);
+        for (int k = 0; k < 4; ++k)
+            if (v[k] >= t.Np) return -1;
+        const double* p0 = m->points + 3 * size_t(v[0]);
+        double E[3][3];  // columns e_k = v_k - v0
+        for (int k = 1; k < 4; ++k)
+            for (int d = 0; d < 3; ++d) E[d][k - 1] = m->points[3 * size_t(v[k]) + d] - p0[d];
+        const double det = E[0][0] * (E[1][1] * E[2][2] - E[1][2] * E[2][1]) -
+                           E[0][1] * (E[1][0] * E[2][2] - E[1][2] * E[2][0]) +
+                           E[0][2] * (E[1][0] * E[2][1] - E[1][1] * E[2][0]);
+        if (!(std::fabs(det) > 0.0)) return -2;
+        t.vol[c] = std::fabs(det) / 6.0;
+        // rows of E^-1 are the gradients of lambda_1..3
+        double inv[3][3];
+        inv[0][0] = (E[1][1] * E[2][2] - E[1][2] * E[2][1]) / det;
+        inv[0][1] = (E[0][2] * E[2][1] - E[0][1] * E[2][2]) / det;
+        inv[0][2] = (E[0][1] * E[1][2] - E[0][2] * E[1][1]) / det;
+        inv[1][0] = (E[1][2] * E[2][0] - E[1][0] * E[2][2]) / det;
+        inv[1][1] = (E[0][0] * E[2][2] - E[0][2] * E[2][0]) / det;
+        inv[1][2] = (E[0][2] * E[1][0] - E[0][0] * E[1][2]) / det;
+        inv[2][0] = (E[1][0] * E[2][1] - E[1][1] * E[2][0]) / det;
+        inv[2][1] = (E[0][1] * E[2][0] - E[0][0] * E[2][1]) / det;
+        inv[2][2] = (E[0][0] * E[1][1] - E[0][1] * E[1][0]) / det;
+        double* g = &t.grad[12 * size_t(c)];
+        for (int d = 0; d < 3; ++d) {
+            g[3 + d] = inv[0][d];
+            g[6 + d] = inv[1][d];
+            g[9 + d] = inv[2][d];
+            g[d] = -(inv[0][d] + inv[1][d] + inv[2][d]);
+        }
+        // plane form (include/core/mesh.hpp:657-727): d_f = delta_f0 - grad_f . v0
+        double* pl = &t.plane[16 * size_t(c)];
+        for (int f = 0; f < 4; ++f) {
+            pl[4 * f] = g[3 * f];
+            pl[4 * f + 1] = g[3 * f + 1];
+            pl[4 * f + 2] = g[3 * f + 2];
+            pl[4 * f + 3] = (f == 0 ? 1.0 : 0.0) - (g[3 * f] * p0[0] + g[3 * f + 1] * p0[1] + g[3 * f + 2] * p0[2]);
+        }
+        // face f is opposite vertex f
+        for (int f = 0; f < 4; ++f) {
+            uint32_t a[3], n = 0;
+            for (int k = 0; k < 4; ++k)
+                if (k != f) a[n++] = v[k];
+            std::sort(a, a + 3);
+            const auto key = std::make_tuple(a[0], a[1], a[2]);
+            auto it = open.find(key);
+            if (it == open.end()) {
+                open.emplace(key, std::make_pair(c, f));
+            } else {
+                const uint32_t o = it->second.first;
+                const int of = it->second.second;
+                if (t.nbr[4 * o + of] != -1) return -3;  // face shared by more than two cells
+                t.nbr[4 * c + f] = int32_t(o);
+                t.nbrFace[4 * c + f] = of;
+                t.nbr[4 * o + of] = int32_t(c);
+                t.nbrFace[4 * o + of] = f;
+                open.erase(it);
+            }
+        }
+    }
+    return 0;
+}
+
+struct FwdModel {
+    const oracle_tet_mesh* m;
+    TetTables tab;
+    std::vector<double> prefix;  // inclusive beta*V prefix
+    double Btot = 0.0;
+    std::vector<uint32_t> matVertex;  // [C][4]
+    std::vector<double> lumped;       // [2 Np]
+};
+
+inline bool isClad(const oracle_tet_mesh* m, uint32_t c) {
+    return m->claddingCellTypes && m->claddingCellTypes[c] == m->claddingNumber;
+}
+
+inline double gainCoeff(const oracle_tet_mesh* m, uint32_t c, double sA, double sE) {
+    if (isClad(m, c)) return -m->claddingAbsorption;
+    return m->nTot * (m->betaVolume[c] * (sE + sA) - sA);
+}
+
+// Walk one source ray from x in cell c along unit direction u.  With score
+// != NULL, adds the tally of every crossed cell to score[c*4 + k] (vertex k of
+// cell c) and counts the visit in visits[c]; with path != NULL, records every
+// segment (cell, length, g l).  Returns -1 when the ray escaped through the
+// mesh boundary, else the cell in which the walk failed.
+//
+// Exit face: among the faces whose coordinate decreases along u (the entry
+// face excluded), the one reached first, length max(-lambda/dlambda, 0); the
+// lowest face index wins a tie.  A ray through an edge or a vertex therefore
+// takes zero-length steps through the cells around it until it is in a cell
+// that it enters with positive length.
+struct Segment {
+    uint32_t cell;
+    double length, gl;
+};
+
+int64_t walkForward(const FwdModel& md, uint32_t c, double x[3], const double u[3], double sA, double sE,
+                    double* score, uint32_t* visits, std::vector<Segment>* path) {
+    const oracle_tet_mesh* m = md.m;
+    int ff = -1;
+    double G = 1.0;
+    for (int step = 0; step < kMaxSteps; ++step) {
+        const double* pl = &md.tab.plane[16 * size_t(c)];
+        double lam[4], dl[4];
+        double best = DBL_MAX;
+        int bf = -1;
+        for (int f = 0; f < 4; ++f) {
+            lam[f] = pl[4 * f] * x[0] + pl[4 * f + 1] * x[1] + pl[4 * f + 2] * x[2] + pl[4 * f + 3];
+            dl[f] = pl[4 * f] * u[0] + pl[4 * f + 1] * u[1] + pl[4 * f + 2] * u[2];
+            if (f == ff || !(dl[f] < 0.0)) continue;
+            const double len = std::max(-lam[f] / dl[f], 0.0);
+            if (len < best) {
+                best = len;
+                bf = f;
+            }
+        }
+        if (bf < 0) return int64_t(c);
+        const double gc = gainCoeff(m, c, sA, sE);
+        const double gl = gc * best;
+        if (path) path->push_back(Segment{c, best, gl});
+        if (score) {
+            const double T = std::fabs(gl) < 1e-8 ? best : std::expm1(gl) / gc;
+            const double contribution = G * T;
+            if (!std::isfinite(contribution)) return int64_t(c);
+            double w[4], wsum = 0.0;
+            for (int f = 0; f < 4; ++f) {
+                w[f] = std::max(0.0, lam[f] + 0.5 * best * dl[f]);
+                wsum += w[f];
+            }
+            for (int f = 0; f < 4; ++f)
+                score[4 * size_t(c) + f] += contribution * (wsum > DBL_EPSILON ? w[f] / wsum : 0.25);
+            ++visits[c];
+            G *= std::exp(gl);
+        }
+        for (int d = 0; d < 3; ++d) x[d] += u[d] * best;
+        const int32_t n = md.tab.nbr[4 * size_t(c) + bf];
+        if (n < 0) return -1;  // escaped through the boundary
+        ff = md.tab.nbrFace[4 * size_t(c) + bf];
+        c = uint32_t(n);
+    }
+    return int64_t(c);
+}
+
+}  // namespace
+
+namespace {
+
+void philoxFwd(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t seed, uint32_t out[4]) {
+    const uint32_t ctr[4] = {c0, c1, c2, c3}, key[2] = {seed, kFwdKeyHi};
+    oracle_philox4x32_10(ctr, key, out);
+}
+
+uint32_t fwdTarget(const oracle_forward_experiment* e, uint32_t k) {
+    if (e->maxRays <= e->minRays || e->adaptiveSteps == 0) return e->minRays;
+    if (k >= e->adaptiveSteps) return e->maxRays;
+    const double growth = std::pow(double(e->maxRays) / double(e->minRays), 1.0 / double(e->adaptiveSteps));
+    const uint32_t r = uint32_t(std::ceil(double(e->minRays) * std::pow(growth, double(k))));
+    return std::min(std::max(r, e->minRays), e->maxRays);
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_tet_tables(const oracle_tet_mesh* mesh, int32_t* neighbors, int32_t* neighborFace, double* gradients,
+                      double* volumes) {
+    TetTables t;
+    const int rc = buildTetTables(mesh, t);
+    if (rc) return rc;
+    std::memcpy(neighbors, t.nbr.data(), t.nbr.size() * sizeof(int32_t));
+    std::memcpy(neighborFace, t.nbrFace.data(), t.nbrFace.size() * sizeof(int32_t));
+    std::memcpy(gradients, t.grad.data(), t.grad.size() * sizeof(double));
+    std::memcpy(volumes, t.vol.data(), t.vol.size() * sizeof(double));
+    return 0;
+}
+
+int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, const oracle_forward_experiment* ex,
+                           int threads, oracle_forward_result* res) {
+    FwdModel md;
+    md.m = m;
+    int rc = buildTetTables(m, md.tab);
+    if (rc) return rc;
+    if (ex->minRays == 0 || ex->batches < 2 || sp->numberOfWavelengths == 0) return -10;
+    const uint32_t C = m->numberOfCells, Np = m->numberOfPoints, B = ex->batches;
+    const uint32_t nL = sp->numberOfWavelengths;
+    md.prefix.resize(C);
+    double acc = 0.0;
+    for (uint32_t c = 0; c < C; ++c) {
+        acc += m->betaVolume[c] * md.tab.vol[c];
+        md.prefix[c] = acc;
+    }
+    md.Btot = acc;
+    md.matVertex.resize(4 * size_t(C));
+    md.lumped.assign(2 * size_t(Np), 0.0);
+    for (uint32_t c = 0; c < C; ++c)
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t mv = m->cells[4 * size_t(c) + k] + (isClad(m, c) ? Np : 0u);
+            md.matVertex[4 * size_t(c) + k] = mv;
+            md.lumped[mv] += md.tab.vol[c] / 4.0;
+        }
+    uint32_t lastSource = 0;
+    for (uint32_t c = 0; c < C; ++c)
+        if (m->betaVolume[c] * md.tab.vol[c] > 0.0) lastSource = c;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+    std::vector<double> score(size_t(B) * 4 * C, 0.0);  // [batch][cell][vertex]
+    std::vector<uint32_t> dropped(C, 0), visits(C, 0), raysInBatch(B, 0);
+    uint64_t total = 0;
+    double sA = sp->sigmaA[0], sE = sp->sigmaE[0];
+    for (uint32_t l = 1; l < nL; ++l) { sA = std::max(sA, sp->sigmaA[l]); sE = std::max(sE, sp->sigmaE[l]); }
+    uint32_t launch = 0;
+    for (;; ++launch) {
+        const uint32_t target = fwdTarget(ex, launch);
+        const uint32_t M = uint32_t(target - total);
+        std::vector<double> shift(B);
+        std::vector<uint32_t> phase(B), nb(B);
+        for (uint32_t b = 0; b < B; ++b) {
+            uint32_t o[4];
+            philoxFwd(b, launch, 0u, kTagFwdBatch, ex->seed, o);
+            shift[b] = double(o[0]) / 4294967296.0;
+            phase[b] = o[1] % nL;
+            nb[b] = b < M ? (M - b + B - 1) / B : 0u;
+            raysInBatch[b] += nb[b];
+        }
+        if (md.Btot > 0.0) {
+#pragma omp parallel
+            {
+                std::vector<double> local(size_t(B) * 4 * C, 0.0);
+                std::vector<uint32_t> ldrop(C, 0), lvisit(C, 0);
+#pragma omp for schedule(dynamic, 4096)
+                for (uint32_t r = 0; r < M; ++r) {
+                    const uint32_t b = r % B, i = r / B;
+                    const double t = (double(i) + shift[b]) / double(nb[b]) * md.Btot;
+                    uint32_t c = uint32_t(std::upper_bound(md.prefix.begin(), md.prefix.end(), t) - md.prefix.begin());
+                    if (c >= C) c = lastSource;
+                    uint32_t o[4], o2[4];
+                    philoxFwd(r, launch, 0u, kTagFwdRay, ex->seed, o);
+                    philoxFwd(r, launch, 1u, kTagFwdRay, ex->seed, o2);
+                    double e[4], esum = 0.0;
+                    for (int k = 0; k < 4; ++k) { e[k] = -std::log(unit(o[k])); esum += e[k]; }
+                    double x[3] = {0.0, 0.0, 0.0};
+                    for (int k = 0; k < 4; ++k) {
+                        const double* p = m->points + 3 * size_t(m->cells[4 * size_t(c) + k]);
+                        for (int d = 0; d < 3; ++d) x[d] += e[k] / esum * p[d];
+                    }
+                    const double z = 2.0 * unit(o2[0]) - 1.0, phi = 2.0 * kPi * unit(o2[1]);
+                    const double rr = std::sqrt(std::max(0.0, 1.0 - z * z));
+                    const double u[3] = {rr * std::cos(phi), rr * std::sin(phi), z};
+                    const uint32_t lam = uint32_t((uint64_t(i) * nL / nb[b] + phase[b]) % nL);
+                    const int64_t fail = walkForward(md, c, x, u, sp->sigmaA[lam], sp->sigmaE[lam],
+                                                     &local[size_t(b) * 4 * C], lvisit.data(), nullptr);
+                    if (fail >= 0) ++ldrop[size_t(fail)];
+                }
+#pragma omp critical
+                {
+                    for (size_t k = 0; k < local.size(); ++k) score[k] += local[k];
+                    for (uint32_t c = 0; c < C; ++c) {
+                        dropped[c] += ldrop[c];
+                        visits[c] += lvisit[c];
+                    }
+                }
+            }
+        }
+        total = target;
+        // finalise
+        std::vector<double> vscore(size_t(B) * 2 * Np, 0.0);
+        for (uint32_t b = 0; b < B; ++b)
+            for (size_t k = 0; k < 4 * size_t(C); ++k)
+                vscore[size_t(b) * 2 * Np + md.matVertex[k]] += score[size_t(b) * 4 * C + k];
+        bool converged = true;
+        for (uint32_t c = 0; c < C; ++c) {
+            const double V = md.tab.vol[c];
+            double sum = 0.0, mSum = 0.0, m2Sum = 0.0;
+            uint32_t active = 0;
+            for (uint32_t b = 0; b < B; ++b) {
+                double dens = 0.0;
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t mv = md.matVertex[4 * size_t(c) + k];
+                    dens += md.lumped[mv] > 0.0 ? vscore[size_t(b) * 2 * Np + mv] / md.lumped[mv] : 0.0;
+                }
+                const double bs = dens / 4.0 * V;
+                sum += bs;
+                if (raysInBatch[b] == 0) continue;
+                const double mean = bs / double(raysInBatch[b]);
+                mSum += mean;
+                m2Sum += mean * mean;
+                ++active;
+            }
+            const double estimate = sum * md.Btot / (double(total) * V);
+            double rse = DBL_MAX;
+            if (dropped[c] == 0 && active >= 2) {
+                const double mean = mSum / active;
+                if (mean == 0.0) {
+                    rse = NAN;
+                } else {
+                    const double var = std::max(0.0, (m2Sum - mSum * mSum / active) / (active - 1.0));
+                    rse = std::sqrt(var / active) / std::fabs(mean);
+                }
+            }
+            const double phi = double(float(estimate * m->nTot / m->crystalTFluo));
+            res->phiAse[c] = phi;
+            res->relativeStandardError[c] = rse;
+            if (res->dndtAse) {
+                const double a = nL == 1 ? sp->sigmaA[0] : sA, e = nL == 1 ? sp->sigmaE[0] : sE;
+                res->dndtAse[c] = (m->betaVolume[c] * (e + a) - a) * phi;
+            }
+            if (res->droppedRays) res->droppedRays[c] = dropped[c];
+            if (res->rayVisits) res->rayVisits[c] = visits[c];
+            if (!(std::isfinite(rse) && rse <= ex->rseThreshold)) converged = false;
+        }
+        if (target >= ex->maxRays || ex->maxRays <= ex->minRays || ex->adaptiveSteps == 0 || converged) break;
+    }
+    res->totalRays = total;
+    res->launches = launch + 1;
+    return 0;
+}
+
+int oracle_tet_trace(const oracle_tet_mesh* m, const oracle_spectrum* sp, uint32_t wavelength, uint32_t n,
+                     const uint32_t* startCell, const double* origin, const double* direction, uint32_t maxSegments,
+                     uint32_t* segments, uint32_t* cells, double* lengths, double* lnGain, double* endPoint,
+                     int32_t* status) {
+    FwdModel md;
+    md.m = m;
+    const int rc = buildTetTables(m, md.tab);
+    if (rc) return rc;
+    if (wavelength >= sp->numberOfWavelengths) return -10;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (startCell[i] >= m->numberOfCells) return -11;
+        double x[3] = {origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]};
+        std::vector<Segment> path;
+        const int64_t fail = walkForward(md, startCell[i], x, direction + 3 * size_t(i), sp->sigmaA[wavelength],
+                                         sp->sigmaE[wavelength], nullptr, nullptr, &path);
+        segments[i] = uint32_t(path.size());
+        double lg = 0.0;
+        for (size_t k = 0; k < path.size(); ++k) {
+            lg += path[k].gl;
+            if (k < maxSegments) {
+                if (cells) cells[size_t(i) * maxSegments + k] = path[k].cell;
+                if (lengths) lengths[size_t(i) * maxSegments + k] = path[k].length;
+            }
+        }
+        if (lnGain) lnGain[i] = lg;
+        if (endPoint)
+            for (int d = 0; d < 3; ++d) endPoint[3 * size_t(i) + d] = x[d];
+        status[i] = fail < 0 ? 0 : 1;
+    }
+    return 0;
+}
+
+}  // extern "C"

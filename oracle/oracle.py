@@ -238,3 +238,112 @@ def phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, mseThresh
     if rc:
         raise ValueError(f"oracle_phi_ase failed ({rc})")
     return out
+
+
+# ---- forward Tet4 estimator -------------------------------------------------
+
+class _TetMesh(C.Structure):
+    _fields_ = [
+        ("numberOfPoints", C.c_uint32),
+        ("numberOfCells", C.c_uint32),
+        ("points", _f64p),
+        ("cells", _u32p),
+        ("betaVolume", _f64p),
+        ("claddingCellTypes", _u32p),
+        ("claddingNumber", C.c_uint32),
+        ("claddingAbsorption", C.c_double),
+        ("nTot", C.c_double),
+        ("crystalTFluo", C.c_double),
+    ]
+
+
+class _FwdExperiment(C.Structure):
+    _fields_ = [
+        ("minRays", C.c_uint32),
+        ("maxRays", C.c_uint32),
+        ("adaptiveSteps", C.c_uint32),
+        ("rseThreshold", C.c_double),
+        ("seed", C.c_uint32),
+        ("batches", C.c_uint32),
+    ]
+
+
+class _FwdResult(C.Structure):
+    _fields_ = [
+        ("phiAse", _f64p),
+        ("relativeStandardError", _f64p),
+        ("dndtAse", _f64p),
+        ("droppedRays", _u32p),
+        ("rayVisits", _u32p),
+        ("totalRays", C.c_uint64),
+        ("launches", C.c_uint32),
+    ]
+
+
+def _tet_struct(mesh, keep):
+    pts = keep(np.ascontiguousarray(np.asarray(mesh.points, np.float64).reshape(-1, 3)))
+    cells = keep(np.ascontiguousarray(np.asarray(mesh.cells, np.uint32).reshape(-1, 4)))
+    beta = keep(np.ascontiguousarray(np.asarray(mesh.betaVolume, np.float64).ravel()))
+    clad = None if getattr(mesh, "claddingCellTypes", None) is None else keep(
+        np.ascontiguousarray(np.asarray(mesh.claddingCellTypes, np.uint32).ravel()))
+    return _TetMesh(pts.shape[0], cells.shape[0], _ptr(pts, _f64p), _ptr(cells, _u32p), _ptr(beta, _f64p),
+                    _ptr(clad, _u32p), int(getattr(mesh, "claddingNumber", 1)),
+                    float(getattr(mesh, "claddingAbsorption", 0.0)), float(mesh.nTot), float(mesh.crystalTFluo))
+
+
+def tet_tables(mesh):
+    keep = _Keep()
+    m = _tet_struct(mesh, keep)
+    Cn = m.numberOfCells
+    out = {"neighbors": np.empty((Cn, 4), np.int32), "neighborFace": np.empty((Cn, 4), np.int32),
+           "gradients": np.empty((Cn, 4, 3)), "volumes": np.empty(Cn)}
+    rc = lib().oracle_tet_tables(C.byref(m), _ptr(out["neighbors"], _i32p), _ptr(out["neighborFace"], _i32p),
+                                 _ptr(out["gradients"], _f64p), _ptr(out["volumes"], _f64p))
+    if rc:
+        raise ValueError(f"oracle_tet_tables failed ({rc})")
+    return out
+
+
+def forward_phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, rseThreshold=0.0, seed=5489,
+                    batches=8, threads=0):
+    """Forward Tet4 phi-ASE per cell (FP64)."""
+    keep = _Keep()
+    m = _tet_struct(mesh, keep)
+    s = _spectrum_struct(spectrum, keep)
+    n = m.numberOfCells
+    out = {"phiAse": np.empty(n), "relativeStandardError": np.empty(n), "dndtAse": np.empty(n),
+           "droppedRays": np.empty(n, np.uint32), "rayVisits": np.empty(n, np.uint32)}
+    r = _FwdResult(_ptr(out["phiAse"], _f64p), _ptr(out["relativeStandardError"], _f64p),
+                   _ptr(out["dndtAse"], _f64p), _ptr(out["droppedRays"], _u32p), _ptr(out["rayVisits"], _u32p), 0, 0)
+    e = _FwdExperiment(int(minRays), int(maxRays if maxRays is not None else minRays), int(adaptiveSteps),
+                       float(rseThreshold), int(seed) & 0xFFFFFFFF, int(batches))
+    rc = lib().oracle_forward_phi_ase(C.byref(m), C.byref(s), C.byref(e), int(threads or os.cpu_count() or 1),
+                                      C.byref(r))
+    if rc:
+        raise ValueError(f"oracle_forward_phi_ase failed ({rc})")
+    out["totalRays"] = int(r.totalRays)
+    out["launches"] = int(r.launches)
+    return out
+
+
+def tet_trace(mesh, spectrum, start_cell, origin, direction, *, wavelength=0, max_segments=64):
+    """Single rays through a Tet4 mesh: segments, cells, lengths, lnGain, endPoint, status."""
+    keep = _Keep()
+    m = _tet_struct(mesh, keep)
+    s = _spectrum_struct(spectrum, keep)
+    sc = keep(np.ascontiguousarray(np.atleast_1d(np.asarray(start_cell, np.uint32))))
+    o = keep(np.ascontiguousarray(np.asarray(origin, np.float64).reshape(-1, 3)))
+    d = keep(np.ascontiguousarray(np.asarray(direction, np.float64).reshape(-1, 3)))
+    n = sc.size
+    if o.shape[0] != n or d.shape[0] != n:
+        raise ValueError("start_cell, origin and direction must describe the same rays")
+    out = {"segments": np.empty(n, np.uint32), "cells": np.zeros((n, max_segments), np.uint32),
+           "lengths": np.zeros((n, max_segments)), "lnGain": np.empty(n), "endPoint": np.empty((n, 3)),
+           "status": np.empty(n, np.int32)}
+    rc = lib().oracle_tet_trace(C.byref(m), C.byref(s), int(wavelength), n, _ptr(sc, _u32p), _ptr(o, _f64p),
+                                _ptr(d, _f64p), int(max_segments), _ptr(out["segments"], _u32p),
+                                _ptr(out["cells"], _u32p), _ptr(out["lengths"], _f64p), _ptr(out["lnGain"], _f64p),
+                                _ptr(out["endPoint"], _f64p), _ptr(out["status"], _i32p))
+    if rc:
+        raise ValueError(f"oracle_tet_trace failed ({rc})")
+    return out

@@ -30,6 +30,10 @@ What it extracts (all citations are paths inside the reference project):
   55 cm^-1) parsed from the table in that fixture's README.md.
 * ``tet4_cylindrical.npz`` -- ``example/data/cylindrical.vtk`` as Tet4 cells
   with its per-cell betaVolume and material attributes.
+* ``tet4_tables.npz`` -- the reference's own Tet4 topology
+  (``pyInclude/geometry/volume.py:_deriveTet4Topology``: neighbour cells,
+  neighbour local faces and cell volumes, with its local-face table
+  ``TET4_FACE_VERTICES``) for the two Tet4 fixtures above.
 * ``mesh_tables.npz`` -- the reference's own per-triangle tables
   (``pyInclude/geometry/core.py:_derived_topology``: centres, surfaces, edge
   normals, normal points, neighbours, forbidden edges) for the three meshes
@@ -248,6 +252,20 @@ def _tet4_from_vtk(ref: Path, name: str, out: Path):
         provenance=np.asarray(json.dumps({"geometry": f"example/data/{name}.vtk"})))
 
 
+def _tet4_tables(ref: Path, fixtures, out: Path):
+    sys.path.insert(0, str(ref))
+    from pyInclude.geometry import volume  # noqa: PLC0415  (reference frontend, importable here)
+
+    payload = {"faceVertices": np.asarray(volume.TET4_FACE_VERTICES, np.int32)}
+    for name, path in fixtures.items():
+        d = np.load(path)
+        topo = volume._deriveTet4Topology(np.asarray(d["points"], np.float64), np.asarray(d["cells"], np.int64), None)
+        payload[f"{name}_neighborCells"] = np.asarray(topo["neighborCells"], np.int32)
+        payload[f"{name}_neighborLocalFaces"] = np.asarray(topo["neighborLocalFaces"], np.int32)
+        payload[f"{name}_cellVolumes"] = np.asarray(topo["cellVolumes"], np.float32)
+    np.savez_compressed(out, **payload)
+
+
 def _mesh_tables(ref: Path, meshes, out: Path):
     sys.path.insert(0, str(ref))
     from pyInclude.geometry import core  # noqa: PLC0415  (reference frontend, importable here)
@@ -281,6 +299,8 @@ def main(argv=None):
     meshes["true_cladding"] = _legacy_true_cladding(ref, HERE / "legacy_true_cladding.npz")
     _tet4_true_cladding(ref, HERE / "tet4_true_cladding.npz")
     _tet4_from_vtk(ref, "cylindrical", HERE / "tet4_cylindrical.npz")
+    _tet4_tables(ref, {"true_cladding": HERE / "tet4_true_cladding.npz",
+                       "cylindrical": HERE / "tet4_cylindrical.npz"}, HERE / "tet4_tables.npz")
     _mesh_tables(ref, meshes, HERE / "mesh_tables.npz")
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
