@@ -1,4 +1,5 @@
-"""ctypes binding of libhase_b200.so (the C ABI declared in include/hase_b200.h).
+"""ctypes binding of libhase_b200.so (the C ABI declared in include/hase_b200.h
+and include/hase_b200_forward.h).
 
 The shared library is built in-tree (``haseongpu_b200/libhase_b200.so``) by
 ``haseongpu_b200.build.build_library()``.  There is no CPU fallback: every
@@ -42,6 +43,13 @@ EXPORTED_SYMBOLS = (
     "hase_philox",
     "hase_probe_l2_bandwidth",
     "hase_estimate_sample_noalloc",
+    # include/hase_b200_forward.h
+    "hase_tet_context_create",
+    "hase_tet_context_update_beta",
+    "hase_tet_calc_phi_ase",
+    "hase_tet_context_destroy",
+    "hase_tet_tables",
+    "hase_tet_trace",
 )
 
 _u32p = C.POINTER(C.c_uint32)
@@ -119,6 +127,53 @@ class ResultDesc(C.Structure):
     ]
 
 
+class TetMeshDesc(C.Structure):
+    _fields_ = [
+        ("numberOfPoints", C.c_uint32),
+        ("numberOfCells", C.c_uint32),
+        ("points", _f64p),
+        ("cells", _u32p),
+        ("betaVolume", _f64p),
+        ("claddingCellTypes", _u32p),
+        ("claddingNumber", C.c_uint32),
+        ("claddingAbsorption", C.c_double),
+        ("nTot", C.c_double),
+        ("crystalTFluo", C.c_double),
+    ]
+
+
+class ForwardDesc(C.Structure):
+    _fields_ = [
+        ("forwardRayCount", C.c_uint32),
+        ("maxRays", C.c_uint32),
+        ("adaptiveSteps", C.c_uint32),
+        ("relativeStandardErrorThreshold", C.c_double),
+        ("monochromatic", C.c_uint32),
+        ("rngSeed", C.c_uint32),
+        ("batches", C.c_uint32),
+        ("blockSize", C.c_uint32),
+        ("tallyMode", C.c_uint32),
+    ]
+
+
+class ForwardResultDesc(C.Structure):
+    _fields_ = [
+        ("phiAse", _f32p),
+        ("relativeStandardError", _f64p),
+        ("dndtAse", _f64p),
+        ("totalRays", _u32p),
+        ("droppedRays", _u32p),
+        ("raysTraced", C.c_uint64),
+        ("crossings", C.c_uint64),
+        ("rayMilliseconds", C.c_double),
+        ("totalMilliseconds", C.c_double),
+        ("launches", C.c_uint32),
+        ("unconvergedCells", C.c_uint32),
+        ("kernelLaunches", C.c_uint32),
+        ("tallyMode", C.c_uint32),
+    ]
+
+
 class HaseError(RuntimeError):
     """A libhase_b200 call failed; ``status`` is the hase_status code."""
 
@@ -159,6 +214,15 @@ def lib():
         L.hase_probe_l2_bandwidth.argtypes = [C.c_int, C.c_uint64, C.c_uint32, _f64p]
         L.hase_estimate_sample_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                                    C.c_uint32, C.c_uint32, C.c_void_p]
+        _i32p = C.POINTER(C.c_int32)
+        L.hase_tet_context_create.argtypes = [C.POINTER(TetMeshDesc), C.POINTER(SpectrumDesc), C.c_int,
+                                              C.POINTER(C.c_void_p)]
+        L.hase_tet_context_update_beta.argtypes = [C.c_void_p, _f64p]
+        L.hase_tet_calc_phi_ase.argtypes = [C.c_void_p, C.POINTER(ForwardDesc), C.POINTER(ForwardResultDesc)]
+        L.hase_tet_context_destroy.argtypes = [C.c_void_p]
+        L.hase_tet_tables.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _f64p]
+        L.hase_tet_trace.argtypes = [C.c_void_p, C.c_uint32, _u32p, _f64p, _f64p, C.c_uint32, C.c_uint32, _u32p,
+                                     _u32p, _f64p, _f64p, _f64p, _i32p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

@@ -21,6 +21,7 @@
 // entry point include/core/simulation.hpp:42-47.
 #include "hase_b200.h"
 #include "hase_device.cuh"
+#include "hase_host.cuh"
 
 #include <cuda_runtime.h>
 
@@ -37,7 +38,7 @@
 
 using namespace hase;
 
-namespace {
+namespace hase {
 
 thread_local std::string g_lastError;
 
@@ -51,20 +52,9 @@ hase_status fail(hase_status st, const char* fmt, ...) {
     return st;
 }
 
-#define HASE_CUDA(call)                                                                                  \
-    do {                                                                                                 \
-        cudaError_t e_ = (call);                                                                         \
-        if (e_ != cudaSuccess) {                                                                         \
-            return fail(e_ == cudaErrorMemoryAllocation ? HASE_OUT_OF_MEMORY : HASE_CUDA_ERROR, "%s: %s (%s:%d)", \
-                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
-        }                                                                                                \
-    } while (0)
+}  // namespace hase
 
-#define HASE_TRY(expr)               \
-    do {                             \
-        hase_status s_ = (expr);     \
-        if (s_ != HASE_OK) return s_; \
-    } while (0)
+namespace {
 
 constexpr uint32_t kRayBlock = 256;
 constexpr int kRayMinBlocks = 5;
@@ -685,26 +675,6 @@ __global__ void noAllocEmitKernel(const float* phi, const double* mse, const uin
 }
 
 // -------------------------------------------------------- host side ----
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t ensure(size_t count) {
-        if (count <= n) return cudaSuccess;
-        release();
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        else p = nullptr;
-        return e;
-    }
-};
-
 struct HostTables {
     std::vector<int4> verts;
     std::vector<float4> tri, geo;

@@ -1,0 +1,918 @@
+// hase_forward.cu -- the forward Tet4 phi-ASE path of libhase_b200.so
+// (HASEonGPU v2.2.0's current calcPhiASE), FP64 on sm_100a.
+//
+// Per adaptive launch of M source rays, split round-robin over B statistical
+// batches (ray r -> batch r % B, index r / B inside it):
+//   fwdRayKernel   each block serves one batch; each lane owns a sequence of
+//                  rays and starts the next one as soon as its current ray has
+//                  left the mesh, so a warp stays full until the tail.  Source:
+//                  stratified beta*V CDF target (i + shift_b)/N_b * B_tot and a
+//                  binary search of the inclusive prefix, a uniform point in
+//                  the tet from four exponentials, an isotropic direction, a
+//                  stratified wavelength bin.  Walk: per cell the four
+//                  barycentric face coordinates lambda_f = a.x + d and their
+//                  rates along the ray; the exit is the decreasing coordinate
+//                  that reaches zero first (cross-multiplied comparisons, one
+//                  division per crossing).  Tally: weight G (e^{gl} - 1)/g split
+//                  to the cell's four material vertices by the segment-midpoint
+//                  barycentric weights, into a per-block shared-memory vertex
+//                  histogram of the block's batch (flushed once per block) or,
+//                  for meshes whose histogram does not fit, straight into
+//                  device memory.
+//   fwdFinalizeKernel  one thread per cell: vertex -> cell density through
+//                  the lumped material-vertex volumes, estimate
+//                  S B_tot / (N V) N_tot / tau, batch-mean relative error,
+//                  dndt, and the count of cells above the threshold.
+// Reference anchors (paths inside the HASEonGPU tree):
+//   include/kernels/forward/accumulation.hpp:300-453 (kernel, tally),
+//   include/kernels/forward/volumeSampling.hpp:19-161 (source sampling),
+//   include/kernels/forward/rayWalk.hpp:106-208 (exit face, segment gain),
+//   include/kernels/forwardPhiAseMapping.hpp:51-150 and
+//   include/kernels/vertexAccumulation.hpp:17-68 (finaliser),
+//   include/core/forwardPhiAseEvaluator.hpp:114-178 (adaptive launches),
+//   include/core/mesh.hpp:657-727 (barycentric face planes).
+#include "hase_b200_forward.h"
+#include "hase_device.cuh"
+#include "hase_host.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+using namespace hase;
+
+namespace {
+
+constexpr uint32_t kTagFwdBatch = 2u;  // Philox counter tags of the forward streams
+constexpr uint32_t kTagFwdRay = 3u;
+constexpr uint32_t kFwdKeyHi = 1u;     // key = {seed, 1}
+constexpr uint32_t kMaxBatches = 64u;
+constexpr uint32_t kFwdBlock = 256u;
+constexpr int kFwdMaxSteps = 10000;    // bounded walk: a ray still inside after this many cells is dropped
+constexpr size_t kMaxHistogramBytes = 200u * 1024u;
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+struct TetView {
+    const double4* plane;   // [C][4]: lambda_f(x) = a.x + b.y + c.z + d
+    const int* nbr;         // [C][4]: (neighbour << 2) | neighbour's local face, -1 at the boundary
+    const uint4* matv;      // [C]: material vertex of each corner (cladding cells offset by Np)
+    const uint4* cellv;     // [C]: point indices
+    const double* gainBeta; // [C]: beta, NaN for cladding cells
+    const double* points;   // [Np][3]
+    const double* prefix;   // [C]: inclusive prefix of beta * V
+    uint32_t C, Np, lastSource;
+    double cladAbs, nTot, Btot;
+};
+
+__device__ __forceinline__ double unit53(uint32_t x) { return (double(x >> 8) + 0.5) * (1.0 / 16777216.0); }
+
+// Exit face of the cell whose planes are pl for a ray at (x, y, z) moving
+// along u, the entry face ff excluded: among the faces with dlambda < 0, the
+// smallest max(lambda, 0) / -dlambda (lowest index on a tie).  Fills lam and
+// dl for all four faces; returns -1 when no face decreases.
+__device__ __forceinline__ int exitFace(const double4* __restrict__ pl, double x, double y, double z, double ux,
+                                        double uy, double uz, int ff, double lam[4], double dl[4], double& len) {
+    int bf = -1;
+    double bl = 0.0, bd = -1.0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const double2 ab = __ldg(reinterpret_cast<const double2*>(pl + f));
+        const double2 cd = __ldg(reinterpret_cast<const double2*>(pl + f) + 1);
+        lam[f] = fma(ab.x, x, fma(ab.y, y, fma(cd.x, z, cd.y)));
+        dl[f] = fma(ab.x, ux, fma(ab.y, uy, cd.x * uz));
+        if (f == ff || !(dl[f] < 0.0)) continue;
+        const double lc = fmax(lam[f], 0.0);
+        // lc / -dl[f] < bl / -bd  <=>  lc * bd > bl * dl[f]   (both rates negative)
+        if (bf < 0 || lc * bd > bl * dl[f]) {
+            bf = f;
+            bl = lc;
+            bd = dl[f];
+        }
+    }
+    len = bf < 0 ? 0.0 : -bl / bd;
+    return bf;
+}
+
+__device__ __forceinline__ double gainCoefficient(const TetView& m, uint32_t c, double sA, double sE) {
+    const double beta = __ldg(m.gainBeta + c);
+    return isnan(beta) ? -m.cladAbs : m.nTot * (beta * (sE + sA) - sA);
+}
+
+struct FwdRay {
+    double x, y, z, ux, uy, uz, G, sA, sE;
+    uint32_t c;
+    int ff, steps;
+};
+
+// Track-length tally of one segment: weight G (e^{gl} - 1)/g split to the
+// four corners by the midpoint barycentric weights.  Returns false (ray
+// dropped) when the contribution is not finite.
+template <typename Tally>
+__device__ __forceinline__ bool tallySegment(const TetView& m, FwdRay& r, double len, const double lam[4],
+                                             const double dl[4], Tally&& add) {
+    const double gc = gainCoefficient(m, r.c, r.sA, r.sE);
+    const double gl = gc * len;
+    const double E = expm1(gl);
+    const double T = fabs(gl) < 1e-8 ? len : E / gc;
+    const double contribution = r.G * T;
+    if (!isfinite(contribution)) return false;
+    double w[4], wsum = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        w[f] = fmax(0.0, fma(0.5 * len, dl[f], lam[f]));
+        wsum += w[f];
+    }
+    const uint4 mv = __ldg(m.matv + r.c);
+    if (wsum > DBL_EPSILON) {
+        const double s = contribution / wsum;
+        add(mv.x, w[0] * s);
+        add(mv.y, w[1] * s);
+        add(mv.z, w[2] * s);
+        add(mv.w, w[3] * s);
+    } else {
+        const double q = 0.25 * contribution;
+        add(mv.x, q);
+        add(mv.y, q);
+        add(mv.z, q);
+        add(mv.w, q);
+    }
+    r.G = fma(r.G, E, r.G);
+    return true;
+}
+
+struct FwdLaunch {
+    TetView m;
+    const double* sigmaA;
+    const double* sigmaE;
+    uint32_t nL, seed, launch, B, blocksPerBatch;
+    double* score;                 // [B][2 Np]
+    uint32_t* visits;              // [C]
+    uint32_t* dropped;             // [C]
+    unsigned long long* crossings; // [1]
+    double shift[kMaxBatches];
+    uint32_t nb[kMaxBatches];
+    uint32_t phase[kMaxBatches];
+};
+
+// Source ray i of batch b (ray r = i B + b of this launch).
+__device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, uint64_t i, FwdRay& r) {
+    const TetView& m = L.m;
+    const uint32_t nb = L.nb[b];
+    const double t = (double(i) + L.shift[b]) / double(nb) * m.Btot;
+    // upper_bound: first cell whose inclusive prefix exceeds t
+    uint32_t lo = 0, hi = m.C;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(m.prefix + mid) > t) hi = mid;
+        else lo = mid + 1;
+    }
+    const uint32_t c = lo >= m.C ? m.lastSource : lo;
+    const uint32_t ray = uint32_t(i * L.B + b);
+    const Philox4 o = philox4x32_10(ray, L.launch, 0u, kTagFwdRay, L.seed, kFwdKeyHi);
+    const Philox4 o2 = philox4x32_10(ray, L.launch, 1u, kTagFwdRay, L.seed, kFwdKeyHi);
+    const double e0 = -log(unit53(o.x)), e1 = -log(unit53(o.y)), e2 = -log(unit53(o.z)), e3 = -log(unit53(o.w));
+    const double esum = e0 + e1 + e2 + e3;
+    const uint4 cv = __ldg(m.cellv + c);
+    const double* P = m.points;
+    const double w0 = e0 / esum, w1 = e1 / esum, w2 = e2 / esum, w3 = e3 / esum;
+    r.x = w0 * P[3 * cv.x] + w1 * P[3 * cv.y] + w2 * P[3 * cv.z] + w3 * P[3 * cv.w];
+    r.y = w0 * P[3 * cv.x + 1] + w1 * P[3 * cv.y + 1] + w2 * P[3 * cv.z + 1] + w3 * P[3 * cv.w + 1];
+    r.z = w0 * P[3 * cv.x + 2] + w1 * P[3 * cv.y + 2] + w2 * P[3 * cv.z + 2] + w3 * P[3 * cv.w + 2];
+    const double z = 2.0 * unit53(o2.x) - 1.0;
+    double sphi, cphi;
+    sincos(kTwoPi * unit53(o2.y), &sphi, &cphi);
+    const double rr = sqrt(fmax(0.0, 1.0 - z * z));
+    r.ux = rr * cphi;
+    r.uy = rr * sphi;
+    r.uz = z;
+    const uint32_t lamIdx = uint32_t((i * L.nL / nb + L.phase[b]) % L.nL);
+    r.sA = __ldg(L.sigmaA + lamIdx);
+    r.sE = __ldg(L.sigmaE + lamIdx);
+    r.G = 1.0;
+    r.c = c;
+    r.ff = -1;
+    r.steps = 0;
+}
+
+}  // namespace
+
+namespace {
+
+// Block j serves batch j % B; the blocksPerBatch blocks of a batch stride its
+// rays.  SMEM: the block's vertex tallies go to a shared-memory histogram of
+// 2 Np doubles, added to the batch's device-memory tallies once at the end.
+template <bool SMEM>
+__global__ void __launch_bounds__(kFwdBlock) fwdRayKernel(const FwdLaunch L) {
+    extern __shared__ double hist[];
+    const TetView& m = L.m;
+    const uint32_t b = blockIdx.x % L.B;
+    const uint32_t nV = 2u * m.Np;
+    double* gscore = L.score + size_t(b) * nV;
+    if (SMEM) {
+        for (uint32_t k = threadIdx.x; k < nV; k += blockDim.x) hist[k] = 0.0;
+        __syncthreads();
+    }
+    const uint64_t nb = L.nb[b];
+    const uint64_t stride = uint64_t(L.blocksPerBatch) * blockDim.x;
+    uint64_t i = uint64_t(blockIdx.x / L.B) * blockDim.x + threadIdx.x;
+    auto add = [&](uint32_t v, double val) {
+        if (SMEM) atomicAdd(hist + v, val);
+        else atomicAdd(gscore + v, val);
+    };
+    FwdRay r;
+    bool live = false;
+    unsigned long long crossings = 0;
+    for (;;) {
+        if (!live) {
+            if (i >= nb) break;
+            initSourceRay(L, b, i, r);
+            i += stride;
+            live = true;
+        }
+        double lam[4], dl[4], len;
+        const int bf = exitFace(m.plane + 4 * size_t(r.c), r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
+        bool drop = bf < 0 || ++r.steps > kFwdMaxSteps;
+        if (!drop) {
+            drop = !tallySegment(m, r, len, lam, dl, add);
+            if (!drop) {
+                atomicAdd(L.visits + r.c, 1u);
+                ++crossings;
+            }
+        }
+        if (drop) {
+            atomicAdd(L.dropped + r.c, 1u);
+            live = false;
+            continue;
+        }
+        r.x = fma(r.ux, len, r.x);
+        r.y = fma(r.uy, len, r.y);
+        r.z = fma(r.uz, len, r.z);
+        const int n = __ldg(m.nbr + 4 * size_t(r.c) + bf);
+        if (n < 0) {
+            live = false;  // left the mesh
+        } else {
+            r.c = uint32_t(n) >> 2;
+            r.ff = n & 3;
+        }
+    }
+    // crossings: warp sum, one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) crossings += __shfl_xor_sync(0xffffffffu, crossings, o);
+    if ((threadIdx.x & 31) == 0 && crossings) atomicAdd(L.crossings, crossings);
+    if (SMEM) {
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < nV; k += blockDim.x) {
+            const double v = hist[k];
+            if (v != 0.0) atomicAdd(gscore + k, v);
+        }
+    }
+}
+
+struct FinLaunch {
+    const double* score;   // [B][2 Np]
+    const double* lumped;  // [2 Np]
+    const double* vol;     // [C]
+    const double* beta;    // [C] (dndt)
+    const uint4* matv;     // [C]
+    const uint32_t* dropped;
+    float* phi;
+    double* rse;
+    double* dndt;
+    uint32_t* unconverged;
+    uint32_t C, Np, B;
+    double Btot, totalRays, nTot, tau, threshold, dndtA, dndtE;
+    double raysInBatch[kMaxBatches];
+};
+
+// Vertex -> cell density through lumped material-vertex volumes, estimate,
+// batch-mean relative error (include/kernels/forwardPhiAseMapping.hpp:51-150).
+__global__ void __launch_bounds__(256) fwdFinalizeKernel(const FinLaunch F) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= F.C) return;
+    const uint4 mv = F.matv[c];
+    const uint32_t v[4] = {mv.x, mv.y, mv.z, mv.w};
+    double lumped[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) lumped[k] = F.lumped[v[k]];
+    const double V = F.vol[c];
+    const size_t nV = 2u * size_t(F.Np);
+    double sum = 0.0, mSum = 0.0, m2Sum = 0.0;
+    uint32_t active = 0;
+    for (uint32_t b = 0; b < F.B; ++b) {
+        double dens = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dens += lumped[k] > 0.0 ? F.score[b * nV + v[k]] / lumped[k] : 0.0;
+        const double bs = dens / 4.0 * V;
+        sum += bs;
+        if (F.raysInBatch[b] == 0.0) continue;
+        const double mean = bs / F.raysInBatch[b];
+        mSum += mean;
+        m2Sum += mean * mean;
+        ++active;
+    }
+    const double estimate = sum * F.Btot / (F.totalRays * V);
+    double rse = DBL_MAX;
+    if (F.dropped[c] == 0 && active >= 2) {
+        const double mean = mSum / active;
+        if (mean == 0.0) {
+            rse = nan("");
+        } else {
+            const double var = fmax(0.0, (m2Sum - mSum * mSum / active) / (active - 1.0));
+            rse = sqrt(var / active) / fabs(mean);
+        }
+    }
+    const float phi = __double2float_rn(estimate * F.nTot / F.tau);
+    F.phi[c] = phi;
+    F.rse[c] = rse;
+    F.dndt[c] = (F.beta[c] * (F.dndtE + F.dndtA) - F.dndtA) * double(phi);
+    if (!(isfinite(rse) && rse <= F.threshold)) atomicAdd(F.unconverged, 1u);
+}
+
+struct TraceLaunch {
+    TetView m;
+    uint32_t n, maxSegments;
+    const uint32_t* startCell;
+    const double* origin;
+    const double* direction;
+    double sA, sE;
+    uint32_t* segments;
+    uint32_t* cells;
+    double* lengths;
+    double* lnGain;
+    double* endPoint;
+    int32_t* status;
+};
+
+__global__ void __launch_bounds__(128) fwdTraceKernel(const TraceLaunch T) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.n) return;
+    const TetView& m = T.m;
+    FwdRay r;
+    r.x = T.origin[3 * size_t(i)];
+    r.y = T.origin[3 * size_t(i) + 1];
+    r.z = T.origin[3 * size_t(i) + 2];
+    r.ux = T.direction[3 * size_t(i)];
+    r.uy = T.direction[3 * size_t(i) + 1];
+    r.uz = T.direction[3 * size_t(i) + 2];
+    r.c = T.startCell[i];
+    r.ff = -1;
+    r.steps = 0;
+    double lg = 0.0;
+    int32_t st = 1;
+    uint32_t seg = 0;
+    while (seg < uint32_t(kFwdMaxSteps)) {
+        double lam[4], dl[4], len;
+        const int bf = exitFace(m.plane + 4 * size_t(r.c), r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
+        if (bf < 0) break;
+        lg += gainCoefficient(m, r.c, T.sA, T.sE) * len;
+        if (seg < T.maxSegments) {
+            if (T.cells) T.cells[size_t(i) * T.maxSegments + seg] = r.c;
+            if (T.lengths) T.lengths[size_t(i) * T.maxSegments + seg] = len;
+        }
+        ++seg;
+        r.x = fma(r.ux, len, r.x);
+        r.y = fma(r.uy, len, r.y);
+        r.z = fma(r.uz, len, r.z);
+        const int n = m.nbr[4 * size_t(r.c) + bf];
+        if (n < 0) {
+            st = 0;
+            break;
+        }
+        r.c = uint32_t(n) >> 2;
+        r.ff = n & 3;
+    }
+    T.segments[i] = seg;
+    T.lnGain[i] = lg;
+    T.endPoint[3 * size_t(i)] = r.x;
+    T.endPoint[3 * size_t(i) + 1] = r.y;
+    T.endPoint[3 * size_t(i) + 2] = r.z;
+    T.status[i] = st;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host side ----
+namespace {
+
+struct TetHost {
+    std::vector<double4> plane;
+    std::vector<int> nbr;
+    std::vector<uint4> matv, cellv;
+    std::vector<double> vol, lumped;
+};
+
+// Barycentric face planes, volumes and face neighbours of a Tet4 mesh.  Face f
+// of a cell is opposite its vertex f; lambda_f = delta_f0 + grad_f . (x - v0)
+// with grad_1..3 the rows of E^-1 (E = [v1-v0, v2-v0, v3-v0]) and grad_0 =
+// -(grad_1 + grad_2 + grad_3), stored as planes a.x + d.
+hase_status buildTetHost(const hase_tet_mesh_desc* d, TetHost& h) {
+    const uint32_t C = d->numberOfCells, Np = d->numberOfPoints;
+    h.plane.resize(4 * size_t(C));
+    h.nbr.assign(4 * size_t(C), -1);
+    h.matv.resize(C);
+    h.cellv.resize(C);
+    h.vol.resize(C);
+    h.lumped.assign(2 * size_t(Np), 0.0);
+    struct FaceKey {
+        uint32_t a, b, c, id;
+    };
+    std::vector<FaceKey> faces(4 * size_t(C));
+    for (uint32_t c = 0; c < C; ++c) {
+        const uint32_t* v = d->cells + 4 * size_t(c);
+        for (int k = 0; k < 4; ++k)
+            if (v[k] >= Np) return fail(HASE_INVALID_ARGUMENT, "cell %u references point %u >= %u", c, v[k], Np);
+        const double* p0 = d->points + 3 * size_t(v[0]);
+        double E[3][3];
+        for (int k = 1; k < 4; ++k)
+            for (int a = 0; a < 3; ++a) E[a][k - 1] = d->points[3 * size_t(v[k]) + a] - p0[a];
+        const double det = E[0][0] * (E[1][1] * E[2][2] - E[1][2] * E[2][1]) -
+                           E[0][1] * (E[1][0] * E[2][2] - E[1][2] * E[2][0]) +
+                           E[0][2] * (E[1][0] * E[2][1] - E[1][1] * E[2][0]);
+        if (!(std::fabs(det) > 0.0) || !std::isfinite(det))
+            return fail(HASE_INVALID_ARGUMENT, "cell %u is degenerate", c);
+        h.vol[c] = std::fabs(det) / 6.0;
+        double inv[3][3];
+        inv[0][0] = (E[1][1] * E[2][2] - E[1][2] * E[2][1]) / det;
+        inv[0][1] = (E[0][2] * E[2][1] - E[0][1] * E[2][2]) / det;
+        inv[0][2] = (E[0][1] * E[1][2] - E[0][2] * E[1][1]) / det;
+        inv[1][0] = (E[1][2] * E[2][0] - E[1][0] * E[2][2]) / det;
+        inv[1][1] = (E[0][0] * E[2][2] - E[0][2] * E[2][0]) / det;
+        inv[1][2] = (E[0][2] * E[1][0] - E[0][0] * E[1][2]) / det;
+        inv[2][0] = (E[1][0] * E[2][1] - E[1][1] * E[2][0]) / det;
+        inv[2][1] = (E[0][1] * E[2][0] - E[0][0] * E[2][1]) / det;
+        inv[2][2] = (E[0][0] * E[1][1] - E[0][1] * E[1][0]) / det;
+        double g[4][3];
+        for (int a = 0; a < 3; ++a) {
+            g[1][a] = inv[0][a];
+            g[2][a] = inv[1][a];
+            g[3][a] = inv[2][a];
+            g[0][a] = -(inv[0][a] + inv[1][a] + inv[2][a]);
+        }
+        for (int f = 0; f < 4; ++f) {
+            const double dd = (f == 0 ? 1.0 : 0.0) - (g[f][0] * p0[0] + g[f][1] * p0[1] + g[f][2] * p0[2]);
+            h.plane[4 * size_t(c) + f] = make_double4(g[f][0], g[f][1], g[f][2], dd);
+        }
+        const bool clad = d->claddingCellTypes && d->claddingCellTypes[c] == d->claddingNumber;
+        const uint32_t off = clad ? Np : 0u;
+        h.cellv[c] = make_uint4(v[0], v[1], v[2], v[3]);
+        h.matv[c] = make_uint4(v[0] + off, v[1] + off, v[2] + off, v[3] + off);
+        for (int k = 0; k < 4; ++k) h.lumped[v[k] + off] += h.vol[c] / 4.0;
+        for (int f = 0; f < 4; ++f) {
+            uint32_t a[3], n = 0;
+            for (int k = 0; k < 4; ++k)
+                if (k != f) a[n++] = v[k];
+            std::sort(a, a + 3);
+            faces[4 * size_t(c) + f] = FaceKey{a[0], a[1], a[2], uint32_t(4 * c + f)};
+        }
+    }
+    std::sort(faces.begin(), faces.end(), [](const FaceKey& x, const FaceKey& y) {
+        return std::tie(x.a, x.b, x.c, x.id) < std::tie(y.a, y.b, y.c, y.id);
+    });
+    auto same = [](const FaceKey& x, const FaceKey& y) { return x.a == y.a && x.b == y.b && x.c == y.c; };
+    for (size_t k = 0; k < faces.size();) {
+        size_t e = k + 1;
+        while (e < faces.size() && same(faces[k], faces[e])) ++e;
+        if (e - k > 2) return fail(HASE_INVALID_ARGUMENT, "a face is shared by more than two cells");
+        if (e - k == 2) {
+            const uint32_t x = faces[k].id, y = faces[k + 1].id;
+            h.nbr[x] = int(y);  // ids are 4 * cell + face = the packed (cell << 2) | face
+            h.nbr[y] = int(x);
+        }
+        k = e;
+    }
+    return HASE_OK;
+}
+
+uint32_t forwardTarget(uint32_t minRays, uint32_t maxRays, uint32_t steps, uint32_t k) {
+    // include/core/types.hpp:333-354: geometric growth minRays -> maxRays in `steps` increases.
+    if (maxRays <= minRays || steps == 0) return minRays;
+    if (k >= steps) return maxRays;
+    const double growth = std::pow(double(maxRays) / double(minRays), 1.0 / double(steps));
+    const uint32_t r = uint32_t(std::ceil(double(minRays) * std::pow(growth, double(k))));
+    return std::min(std::max(r, minRays), maxRays);
+}
+
+}  // namespace
+
+struct hase_tet_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    uint32_t C = 0, Np = 0, lastSource = 0, numSMs = 0;
+    double nTot = 0, tau = 0, cladAbs = 0, Btot = 0;
+    uint32_t cladNumber = 0;
+    std::vector<uint32_t> cladTypes;
+    std::vector<double> vol, sigmaA, sigmaE;
+    DevBuf<double4> plane;
+    DevBuf<int> nbr;
+    DevBuf<uint4> matv, cellv;
+    DevBuf<double> gainBeta, beta, points, prefix, lumped, dvol, sigA, sigE;
+    // accumulators and outputs
+    DevBuf<double> score, rse, dndt;
+    DevBuf<uint32_t> visits, dropped, unconverged;
+    DevBuf<unsigned long long> crossings;
+    DevBuf<float> phi;
+
+    TetView view() const {
+        TetView v{};
+        v.plane = plane.p;
+        v.nbr = nbr.p;
+        v.matv = matv.p;
+        v.cellv = cellv.p;
+        v.gainBeta = gainBeta.p;
+        v.points = points.p;
+        v.prefix = prefix.p;
+        v.C = C;
+        v.Np = Np;
+        v.lastSource = lastSource;
+        v.cladAbs = cladAbs;
+        v.nTot = nTot;
+        v.Btot = Btot;
+        return v;
+    }
+};
+
+namespace {
+
+hase_status uploadTetBeta(hase_tet_context* c, const double* betaVolume) {
+    std::vector<double> gain(c->C), pre(c->C);
+    double acc = 0.0;
+    uint32_t last = 0;
+    for (uint32_t k = 0; k < c->C; ++k) {
+        const double b = betaVolume[k];
+        if (!std::isfinite(b)) return fail(HASE_INVALID_ARGUMENT, "betaVolume[%u] is not finite", k);
+        const bool clad = !c->cladTypes.empty() && c->cladTypes[k] == c->cladNumber;
+        gain[k] = clad ? NAN : b;
+        const double w = b * c->vol[k];
+        if (w < 0.0) return fail(HASE_INVALID_ARGUMENT, "betaVolume[%u] is negative", k);
+        acc += w;
+        pre[k] = acc;
+        if (w > 0.0) last = k;
+    }
+    c->Btot = acc;
+    c->lastSource = last;
+    HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(c->beta.p, betaVolume, c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(c->prefix.p, pre.data(), c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+template <typename T>
+hase_status upload(DevBuf<T>& buf, const T* src, size_t n, cudaStream_t s) {
+    HASE_CUDA(buf.ensure(n));
+    HASE_CUDA(cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return HASE_OK;
+}
+
+hase_status requireDevice(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return fail(HASE_INVALID_ARGUMENT, "device %d out of range", device);
+    return HASE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spectrum_desc* sp, int device,
+                                    hase_tet_context** out) {
+    if (!d || !sp || !out) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (d->numberOfCells == 0 || d->numberOfPoints < 4) return fail(HASE_INVALID_ARGUMENT, "empty mesh");
+    if (d->numberOfCells >= (1u << 29)) return fail(HASE_INVALID_ARGUMENT, "mesh too large (at most 2^29 cells)");
+    if (d->numberOfPoints >= (1u << 30)) return fail(HASE_INVALID_ARGUMENT, "mesh too large (at most 2^30 points)");
+    if (!d->points || !d->cells || !d->betaVolume) return fail(HASE_INVALID_ARGUMENT, "mesh arrays missing");
+    if (!(d->nTot > 0.0) || !(d->crystalTFluo > 0.0))
+        return fail(HASE_INVALID_ARGUMENT, "nTot and crystalTFluo must be positive");
+    if (!std::isfinite(d->claddingAbsorption)) return fail(HASE_INVALID_ARGUMENT, "claddingAbsorption is not finite");
+    if (sp->numberOfWavelengths == 0 || !sp->sigmaA || !sp->sigmaE) return fail(HASE_INVALID_ARGUMENT, "empty spectrum");
+    for (uint32_t l = 0; l < sp->numberOfWavelengths; ++l)
+        if (!std::isfinite(sp->sigmaA[l]) || !std::isfinite(sp->sigmaE[l]))
+            return fail(HASE_INVALID_ARGUMENT, "cross section %u is not finite", l);
+    for (size_t k = 0; k < 3 * size_t(d->numberOfPoints); ++k)
+        if (!std::isfinite(d->points[k])) return fail(HASE_INVALID_ARGUMENT, "point coordinates must be finite");
+    HASE_TRY(requireDevice(device));
+
+    TetHost h;
+    HASE_TRY(buildTetHost(d, h));
+    hase_tet_context* c = new (std::nothrow) hase_tet_context();
+    if (!c) return fail(HASE_OUT_OF_MEMORY, "host allocation failed");
+    auto cleanup = [&](hase_status s) {
+        hase_tet_context_destroy(c);
+        return s;
+    };
+    c->device = device;
+    c->C = d->numberOfCells;
+    c->Np = d->numberOfPoints;
+    c->nTot = d->nTot;
+    c->tau = d->crystalTFluo;
+    c->cladAbs = d->claddingAbsorption;
+    c->cladNumber = d->claddingNumber;
+    if (d->claddingCellTypes) c->cladTypes.assign(d->claddingCellTypes, d->claddingCellTypes + c->C);
+    c->vol = h.vol;
+    c->sigmaA.assign(sp->sigmaA, sp->sigmaA + sp->numberOfWavelengths);
+    c->sigmaE.assign(sp->sigmaE, sp->sigmaE + sp->numberOfWavelengths);
+    if (cudaSetDevice(device) != cudaSuccess) return cleanup(fail(HASE_CUDA_ERROR, "cudaSetDevice failed"));
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return cleanup(fail(HASE_CUDA_ERROR, "cannot query the SM count"));
+    c->numSMs = uint32_t(sms);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev[0]) != cudaSuccess || cudaEventCreate(&c->ev[1]) != cudaSuccess)
+        return cleanup(fail(HASE_CUDA_ERROR, "stream/event creation failed"));
+    const size_t C = c->C, Np = c->Np;
+    hase_status st = HASE_OK;
+    if ((st = upload(c->plane, h.plane.data(), 4 * C, c->stream)) != HASE_OK ||
+        (st = upload(c->nbr, h.nbr.data(), 4 * C, c->stream)) != HASE_OK ||
+        (st = upload(c->matv, h.matv.data(), C, c->stream)) != HASE_OK ||
+        (st = upload(c->cellv, h.cellv.data(), C, c->stream)) != HASE_OK ||
+        (st = upload(c->points, d->points, 3 * Np, c->stream)) != HASE_OK ||
+        (st = upload(c->lumped, h.lumped.data(), 2 * Np, c->stream)) != HASE_OK ||
+        (st = upload(c->dvol, h.vol.data(), C, c->stream)) != HASE_OK ||
+        (st = upload(c->sigA, c->sigmaA.data(), c->sigmaA.size(), c->stream)) != HASE_OK ||
+        (st = upload(c->sigE, c->sigmaE.data(), c->sigmaE.size(), c->stream)) != HASE_OK)
+        return cleanup(st);
+    if (c->gainBeta.ensure(C) != cudaSuccess || c->beta.ensure(C) != cudaSuccess || c->prefix.ensure(C) != cudaSuccess)
+        return cleanup(fail(HASE_OUT_OF_MEMORY, "device allocation failed"));
+    if ((st = uploadTetBeta(c, d->betaVolume)) != HASE_OK) return cleanup(st);
+    *out = c;
+    return HASE_OK;
+}
+
+hase_status hase_tet_context_update_beta(hase_tet_context* c, const double* betaVolume) {
+    if (!c || !betaVolume) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    HASE_CUDA(cudaSetDevice(c->device));
+    return uploadTetBeta(c, betaVolume);
+}
+
+hase_status hase_tet_context_destroy(hase_tet_context* c) {
+    if (!c) return HASE_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return HASE_OK;
+}
+
+hase_status hase_tet_tables(hase_tet_context* c, int32_t* neighbors, int32_t* neighborFace, double* planes,
+                            double* volumes) {
+    if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
+    HASE_CUDA(cudaSetDevice(c->device));
+    const size_t C = c->C;
+    if (neighbors || neighborFace) {
+        std::vector<int> packed(4 * C);
+        HASE_CUDA(cudaMemcpyAsync(packed.data(), c->nbr.p, 4 * C * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaStreamSynchronize(c->stream));
+        for (size_t k = 0; k < 4 * C; ++k) {
+            if (neighbors) neighbors[k] = packed[k] < 0 ? -1 : packed[k] >> 2;
+            if (neighborFace) neighborFace[k] = packed[k] < 0 ? -1 : packed[k] & 3;
+        }
+    }
+    if (planes) HASE_CUDA(cudaMemcpyAsync(planes, c->plane.p, 4 * C * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+    if (volumes) HASE_CUDA(cudaMemcpyAsync(volumes, c->dvol.p, C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+hase_status hase_tet_trace(hase_tet_context* c, uint32_t n, const uint32_t* startCell, const double* origin,
+                           const double* direction, uint32_t wavelength, uint32_t maxSegments, uint32_t* segments,
+                           uint32_t* cells, double* lengths, double* lnGain, double* endPoint, int32_t* status) {
+    if (!c || !startCell || !origin || !direction || !segments || !lnGain || !endPoint || !status)
+        return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (wavelength >= c->sigmaA.size()) return fail(HASE_INVALID_ARGUMENT, "wavelength index out of range");
+    if (n == 0) return HASE_OK;
+    for (uint32_t i = 0; i < n; ++i)
+        if (startCell[i] >= c->C) return fail(HASE_INVALID_ARGUMENT, "startCell[%u] out of range", i);
+    HASE_CUDA(cudaSetDevice(c->device));
+    const size_t N = n, S = size_t(n) * maxSegments;
+    DevBuf<uint32_t> dStart, dSeg, dCells;
+    DevBuf<double> dOrigin, dDir, dLen, dLn, dEnd;
+    DevBuf<int32_t> dStatus;
+    HASE_TRY(upload(dStart, startCell, N, c->stream));
+    HASE_TRY(upload(dOrigin, origin, 3 * N, c->stream));
+    HASE_TRY(upload(dDir, direction, 3 * N, c->stream));
+    HASE_CUDA(dSeg.ensure(N));
+    HASE_CUDA(dLn.ensure(N));
+    HASE_CUDA(dEnd.ensure(3 * N));
+    HASE_CUDA(dStatus.ensure(N));
+    if (cells && S) HASE_CUDA(dCells.ensure(S));
+    if (lengths && S) HASE_CUDA(dLen.ensure(S));
+    TraceLaunch T{};
+    T.m = c->view();
+    T.n = n;
+    T.maxSegments = maxSegments;
+    T.startCell = dStart.p;
+    T.origin = dOrigin.p;
+    T.direction = dDir.p;
+    T.sA = c->sigmaA[wavelength];
+    T.sE = c->sigmaE[wavelength];
+    T.segments = dSeg.p;
+    T.cells = dCells.p;
+    T.lengths = dLen.p;
+    T.lnGain = dLn.p;
+    T.endPoint = dEnd.p;
+    T.status = dStatus.p;
+    fwdTraceKernel<<<(n + 127) / 128, 128, 0, c->stream>>>(T);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(segments, dSeg.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(lnGain, dLn.p, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(endPoint, dEnd.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(status, dStatus.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (cells && S) HASE_CUDA(cudaMemcpyAsync(cells, dCells.p, S * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (lengths && S) HASE_CUDA(cudaMemcpyAsync(lengths, dLen.p, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+}  // extern "C"
+
+extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_forward_desc* fw,
+                                             hase_forward_result* res) {
+    if (!c || !fw || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (fw->forwardRayCount == 0) return fail(HASE_INVALID_ARGUMENT, "forwardRayCount must be positive");
+    const uint32_t B = fw->batches ? fw->batches : 8u;
+    if (B < 2 || B > kMaxBatches) return fail(HASE_INVALID_ARGUMENT, "batches must be in [2, %u]", kMaxBatches);
+    if (!(fw->relativeStandardErrorThreshold >= 0.0))
+        return fail(HASE_INVALID_ARGUMENT, "relativeStandardErrorThreshold must be >= 0");
+    if (fw->tallyMode > 2) return fail(HASE_INVALID_ARGUMENT, "tallyMode must be 0, 1 or 2");
+    const uint32_t block = fw->blockSize ? fw->blockSize : kFwdBlock;
+    if (block != kFwdBlock) return fail(HASE_INVALID_ARGUMENT, "blockSize must be 0 or %u", kFwdBlock);
+    const uint32_t minRays = fw->forwardRayCount;
+    const uint32_t maxRays = std::max(fw->maxRays, minRays);
+    const bool adaptive = maxRays > minRays && fw->adaptiveSteps > 0;
+    HASE_CUDA(cudaSetDevice(c->device));
+
+    const uint32_t C = c->C, Np = c->Np;
+    const size_t nV = 2 * size_t(Np);
+    const size_t histBytes = nV * sizeof(double);
+    bool smem = fw->tallyMode == 2 || (fw->tallyMode == 0 && histBytes <= kMaxHistogramBytes);
+    if (smem && histBytes > kMaxHistogramBytes)
+        return fail(HASE_INVALID_ARGUMENT, "shared-memory tallies need 2 * numberOfPoints * 8 <= %zu bytes",
+                    kMaxHistogramBytes);
+    int perSM = 0;
+    if (smem) {
+        HASE_CUDA(cudaFuncSetAttribute(fwdRayKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(histBytes)));
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<true>, block, histBytes));
+    } else {
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<false>, block, 0));
+    }
+    if (perSM < 1) return fail(HASE_CUDA_ERROR, "the ray kernel does not fit on an SM");
+    const uint32_t resident = uint32_t(perSM) * c->numSMs;
+
+    HASE_CUDA(c->score.ensure(size_t(B) * nV));
+    HASE_CUDA(c->visits.ensure(C));
+    HASE_CUDA(c->dropped.ensure(C));
+    HASE_CUDA(c->unconverged.ensure(1));
+    HASE_CUDA(c->crossings.ensure(1));
+    HASE_CUDA(c->phi.ensure(C));
+    HASE_CUDA(c->rse.ensure(C));
+    HASE_CUDA(c->dndt.ensure(C));
+    HASE_CUDA(cudaMemsetAsync(c->score.p, 0, size_t(B) * nV * sizeof(double), c->stream));
+    HASE_CUDA(cudaMemsetAsync(c->visits.p, 0, C * sizeof(uint32_t), c->stream));
+    HASE_CUDA(cudaMemsetAsync(c->dropped.p, 0, C * sizeof(uint32_t), c->stream));
+    HASE_CUDA(cudaMemsetAsync(c->crossings.p, 0, sizeof(unsigned long long), c->stream));
+
+    const uint32_t nL = fw->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double dA = c->sigmaA[0], dE = c->sigmaE[0];
+    if (nL > 1)
+        for (uint32_t l = 1; l < nL; ++l) {
+            dA = std::max(dA, c->sigmaA[l]);
+            dE = std::max(dE, c->sigmaE[l]);
+        }
+
+    FwdLaunch L{};
+    L.m = c->view();
+    L.sigmaA = c->sigA.p;
+    L.sigmaE = c->sigE.p;
+    L.nL = nL;
+    L.seed = fw->rngSeed;
+    L.B = B;
+    L.score = c->score.p;
+    L.visits = c->visits.p;
+    L.dropped = c->dropped.p;
+    L.crossings = c->crossings.p;
+
+    FinLaunch F{};
+    F.score = c->score.p;
+    F.lumped = c->lumped.p;
+    F.vol = c->dvol.p;
+    F.beta = c->beta.p;
+    F.matv = c->matv.p;
+    F.dropped = c->dropped.p;
+    F.phi = c->phi.p;
+    F.rse = c->rse.p;
+    F.dndt = c->dndt.p;
+    F.unconverged = c->unconverged.p;
+    F.C = C;
+    F.Np = Np;
+    F.B = B;
+    F.Btot = c->Btot;
+    F.nTot = c->nTot;
+    F.tau = c->tau;
+    F.threshold = fw->relativeStandardErrorThreshold;
+    F.dndtA = dA;
+    F.dndtE = dE;
+
+    res->raysTraced = 0;
+    res->crossings = 0;
+    res->rayMilliseconds = 0.0;
+    res->totalMilliseconds = 0.0;
+    res->launches = 0;
+    res->unconvergedCells = 0;
+    res->kernelLaunches = 0;
+    res->tallyMode = smem ? 2u : 1u;
+
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    HASE_CUDA(cudaEventCreate(&t0));
+    if (cudaEventCreate(&t1) != cudaSuccess) {
+        cudaEventDestroy(t0);
+        return fail(HASE_CUDA_ERROR, "event creation failed");
+    }
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } guard{t0, t1};
+    HASE_CUDA(cudaEventRecord(t0, c->stream));
+
+    uint64_t total = 0;
+    uint32_t unconverged = 0;
+    for (uint32_t launch = 0;; ++launch) {
+        const uint32_t target = forwardTarget(minRays, maxRays, adaptive ? fw->adaptiveSteps : 0u, launch);
+        const uint32_t M = uint32_t(target - total);
+        uint32_t maxNb = 0;
+        for (uint32_t b = 0; b < B; ++b) {
+            const Philox4 o = philox4x32_10(b, launch, 0u, kTagFwdBatch, fw->rngSeed, kFwdKeyHi);
+            L.shift[b] = double(o.x) / 4294967296.0;
+            L.phase[b] = o.y % nL;
+            L.nb[b] = b < M ? (M - b + B - 1) / B : 0u;
+            F.raysInBatch[b] += double(L.nb[b]);
+            maxNb = std::max(maxNb, L.nb[b]);
+        }
+        L.launch = launch;
+        if (c->Btot > 0.0 && M > 0) {
+            // enough blocks to fill the device, no more than the rays of a batch need
+            uint32_t perBatch = std::max(1u, resident / B);
+            perBatch = std::min(perBatch, std::max(1u, (maxNb + block - 1) / block));
+            L.blocksPerBatch = perBatch;
+            HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
+            if (smem) fwdRayKernel<true><<<perBatch * B, block, histBytes, c->stream>>>(L);
+            else fwdRayKernel<false><<<perBatch * B, block, 0, c->stream>>>(L);
+            HASE_CUDA(cudaGetLastError());
+            HASE_CUDA(cudaEventRecord(c->ev[1], c->stream));
+            res->kernelLaunches += 1;
+        }
+        total = target;
+        F.totalRays = double(total);
+        HASE_CUDA(cudaMemsetAsync(c->unconverged.p, 0, sizeof(uint32_t), c->stream));
+        fwdFinalizeKernel<<<(C + 255) / 256, 256, 0, c->stream>>>(F);
+        HASE_CUDA(cudaGetLastError());
+        res->kernelLaunches += 1;
+        HASE_CUDA(cudaMemcpyAsync(&unconverged, c->unconverged.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->Btot > 0.0 && M > 0) {
+            float ms = 0.0f;
+            HASE_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+            res->rayMilliseconds += ms;
+        }
+        res->launches = launch + 1;
+        if (target >= maxRays || !adaptive || unconverged == 0) break;
+    }
+    HASE_CUDA(cudaEventRecord(t1, c->stream));
+    unsigned long long cross = 0;
+    HASE_CUDA(cudaMemcpyAsync(&cross, c->crossings.p, sizeof(cross), cudaMemcpyDeviceToHost, c->stream));
+    if (res->phiAse) HASE_CUDA(cudaMemcpyAsync(res->phiAse, c->phi.p, C * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    if (res->relativeStandardError)
+        HASE_CUDA(cudaMemcpyAsync(res->relativeStandardError, c->rse.p, C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (res->dndtAse) HASE_CUDA(cudaMemcpyAsync(res->dndtAse, c->dndt.p, C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (res->totalRays) HASE_CUDA(cudaMemcpyAsync(res->totalRays, c->visits.p, C * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<uint32_t> drop(C);
+    HASE_CUDA(cudaMemcpyAsync(drop.data(), c->dropped.p, C * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    float totalMs = 0.0f;
+    HASE_CUDA(cudaEventElapsedTime(&totalMs, t0, t1));
+    res->totalMilliseconds = totalMs;
+    res->crossings = cross;
+    res->raysTraced = total;
+    res->unconvergedCells = unconverged;
+    uint64_t droppedTotal = 0;
+    for (uint32_t k = 0; k < C; ++k) droppedTotal += drop[k];
+    if (res->droppedRays) std::copy(drop.begin(), drop.end(), res->droppedRays);
+    if (droppedTotal) return fail(HASE_DROPPED_RAYS, "%llu rays could not be walked", (unsigned long long)droppedTotal);
+    if (unconverged) return fail(HASE_NOT_CONVERGED, "%u cells above the threshold at maxRays", unconverged);
+    return HASE_OK;
+}

@@ -7,10 +7,16 @@ hands the medium to the ``calcPhiASE`` executable through openPMD files
 (pyInclude/openpmd/transport.py:1696-1717), this front end calls
 libhase_b200.so directly through its C ABI (include/hase_b200.h).
 
-The propagation mode is the backward, importance-sampled prism method
-(``propagationMode="backward"``); the MSE threshold is the relative standard
-error of each sample's estimate, as the legacy ``mseThreshold`` and the
-reference's ``relativeStandardErrorThreshold``.
+Two propagation modes:
+
+* ``"forward"`` (the default, as in the reference): the reference's current
+  method on a Tet4 medium (``TetMesh``; a ``PrismMesh`` is split into its
+  Tet4 twin), results per cell (include/hase_b200_forward.h).
+* ``"backward"``: the importance-sampled prism method on a ``PrismMesh``,
+  results per sample point (include/hase_b200.h).
+
+The threshold is the relative standard error of each estimate, as the legacy
+``mseThreshold`` and the reference's ``relativeStandardErrorThreshold``.
 """
 
 from __future__ import annotations
@@ -46,6 +52,7 @@ class Result:
     passes: int = 0
     unconvergedSamples: int = 0
     kernelLaunches: int = 0
+    tallyMode: int = 0
     status: int = 0
 
     @property
@@ -171,8 +178,8 @@ class PhiASE:
 
     config: object | None = None
     crossSections: CrossSectionData | None = None
-    gainMedium: PrismMesh | None = None
-    propagationMode: str = "backward"
+    gainMedium: object | None = None       # TetMesh (forward) or PrismMesh
+    propagationMode: str = "forward"
     minRays: int = 100000
     maxRays: int = 100000
     forwardRayCount: int | None = None
@@ -195,7 +202,8 @@ class PhiASE:
     writeVtk: bool = False
 
     _result: Result | None = field(default=None, init=False, repr=False)
-    _context: DeviceMesh | None = field(default=None, init=False, repr=False)
+    _context: object | None = field(default=None, init=False, repr=False)
+    _tetTwin: tuple | None = field(default=None, init=False, repr=False)
 
     def __post_init__(self):
         if isinstance(self.config, dict):
@@ -205,8 +213,9 @@ class PhiASE:
                 if not hasattr(self, key):
                     raise ValueError(f"unknown PhiASE setting '{key}'")
                 setattr(self, key, value)
-        if self.propagationMode != "backward":
-            raise ValueError("only propagationMode='backward' (importance-sampled prism method) is implemented")
+        if self.propagationMode not in ("forward", "backward"):
+            raise ValueError("propagationMode must be 'forward' (Tet4 source rays) or 'backward' "
+                             "(importance-sampled prism method)")
         if self.parallelMode != "single":
             raise ValueError("parallelMode must be 'single'; use one process per GPU for replicas")
         if self.backend not in (None, "cuda_sm100a"):
@@ -219,7 +228,7 @@ class PhiASE:
     def _device(self) -> int:
         return int(self.devices[0]) if self.devices else 0
 
-    def run(self, gainMedium: PrismMesh | None = None, crossSections: CrossSectionData | None = None) -> "PhiASE":
+    def run(self, gainMedium=None, crossSections: CrossSectionData | None = None) -> "PhiASE":
         medium = gainMedium if gainMedium is not None else self.gainMedium
         if medium is None:
             raise ValueError("PhiASE.run requires gainMedium")
@@ -227,6 +236,10 @@ class PhiASE:
         if spectra is None:
             raise ValueError("PhiASE.run requires crossSections")
         sigmaA, sigmaE = spectra.resampled(self.monochromatic)
+        if self.propagationMode == "forward":
+            return self._run_forward(medium, sigmaA, sigmaE)
+        if not isinstance(medium, PrismMesh):
+            raise ValueError("propagationMode='backward' needs a PrismMesh gain medium")
         ctx = self._context
         if ctx is None or ctx.mesh is not medium or ctx.numberOfWavelengths != sigmaA.size:
             if ctx is not None:
@@ -242,6 +255,40 @@ class PhiASE:
             nearFieldSampling=self.nearFieldSampling, adaptiveSteps=0 if rays else self.adaptiveSteps, repetitions=self.repetitions,
             rngSeed=5489 if self.rngSeed is None else self.rngSeed,
             minSample=self.minSampleRange or 0, maxSample=self.maxSampleRange)
+        return self
+
+    def _run_forward(self, medium, sigmaA, sigmaE) -> "PhiASE":
+        from .forward import TetDeviceMesh
+        from .tetmesh import TetMesh
+
+        if self.useReflections:
+            raise ValueError("useReflections with propagationMode='forward' (surface reflections of the forward "
+                             "method) is not provided; use propagationMode='backward'")
+        if isinstance(medium, PrismMesh):
+            key = medium
+            if self._tetTwin is None or self._tetTwin[0] is not medium:
+                self._tetTwin = (medium, TetMesh.fromPrismMesh(medium))
+            medium = self._tetTwin[1]
+        elif not isinstance(medium, TetMesh):
+            raise ValueError("propagationMode='forward' needs a TetMesh or PrismMesh gain medium")
+        else:
+            key = medium
+        ctx = self._context
+        if (not isinstance(ctx, TetDeviceMesh) or ctx.source is not key
+                or ctx.numberOfWavelengths != sigmaA.size):
+            if ctx is not None:
+                ctx.close()
+            ctx = TetDeviceMesh(medium, sigmaA, sigmaE, device=self._device())
+            ctx.source = key
+            self._context = ctx
+        rays = self.forwardRayCount
+        minRays = rays if rays else self.minRays
+        maxRays = rays if rays else max(self.maxRays, self.minRays)
+        self._result = ctx.calc_phi_ase(
+            forwardRayCount=minRays, maxRays=maxRays, adaptiveSteps=0 if rays else self.adaptiveSteps,
+            relativeStandardErrorThreshold=self.relativeStandardErrorThreshold, monochromatic=self.monochromatic,
+            rngSeed=5489 if self.rngSeed is None else self.rngSeed)
+        self._result.standardError = self._result.relativeStandardError * self._result.phiAse
         return self
 
     def getResults(self) -> Result:

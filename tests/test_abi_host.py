@@ -20,8 +20,12 @@ import pytest
 from conftest import REPO
 
 
+def _header_text():
+    return "\n".join(p.read_text() for p in sorted((REPO / "include").glob("*.h")))
+
+
 def _header_functions():
-    text = (REPO / "include" / "hase_b200.h").read_text()
+    text = _header_text()
     return sorted(set(re.findall(r"^(?:const char\*|int|hase_status)\s+(hase_\w+)\(", text, re.M)))
 
 
@@ -36,10 +40,11 @@ def test_library_exports_every_declared_symbol(native):
 
 
 def test_structures_match_header(native):
-    text = (REPO / "include" / "hase_b200.h").read_text()
+    text = _header_text()
     for cname, pyt in [("hase_mesh_desc", native.MeshDesc), ("hase_spectrum_desc", native.SpectrumDesc),
                        ("hase_experiment_desc", native.ExperimentDesc), ("hase_compute_desc", native.ComputeDesc),
-                       ("hase_result", native.ResultDesc)]:
+                       ("hase_result", native.ResultDesc), ("hase_tet_mesh_desc", native.TetMeshDesc),
+                       ("hase_forward_desc", native.ForwardDesc), ("hase_forward_result", native.ForwardResultDesc)]:
         body = re.search(r"typedef struct \{([^{}]*)\}\s*" + cname + ";", text).group(1)
         fields = re.findall(r"\b(\w+);", re.sub(r"/\*.*?\*/", "", body, flags=re.S))
         assert fields == [f for f, _ in pyt._fields_], cname
@@ -71,6 +76,29 @@ def test_no_device_fails_loudly(native):
     with pytest.raises(native.HaseError) as err:
         DeviceMesh(legacy_mesh("cuboid"), *legacy_spectrum("cuboid"))
     assert err.value.status == native.HASE_NO_DEVICE
+    from haseongpu_b200 import TetDeviceMesh, TetMesh
+
+    with pytest.raises(native.HaseError) as err:
+        TetDeviceMesh(TetMesh.fromPrismMesh(legacy_mesh("cuboid")), *legacy_spectrum("cuboid"))
+    assert err.value.status == native.HASE_NO_DEVICE
+
+
+def test_tet_context_rejects_bad_meshes_before_touching_a_device(native):
+    """Argument checks run before the device query (HASE_INVALID_ARGUMENT, not a fallback)."""
+    from haseongpu_b200 import TetDeviceMesh, TetMesh
+
+    pts = np.array([(0.0, 0, 0), (1.0, 0, 0), (0.0, 1, 0), (0.0, 0, 1)])
+    flat = TetMesh(pts, np.array([(0, 1, 2, 3)]), [0.1], 1e20, 1e-3)
+    flat.nTot = -1.0
+    with pytest.raises(native.HaseError) as err:
+        TetDeviceMesh(flat, [1e-21], [2e-20])
+    assert err.value.status == native.HASE_INVALID_ARGUMENT
+    bad = TetMesh(pts, np.array([(0, 1, 2, 3)]), [0.1], 1e20, 1e-3)
+    bad.points = np.ascontiguousarray(np.where(np.isfinite(bad.points), bad.points, 0.0))
+    bad.points[0, 0] = np.nan
+    with pytest.raises(native.HaseError) as err:
+        TetDeviceMesh(bad, [1e-21], [2e-20])
+    assert err.value.status == native.HASE_INVALID_ARGUMENT
 
 
 def test_interpolate_linear_exact_on_linear_data():
@@ -122,7 +150,7 @@ def test_phiase_validation():
     from haseongpu_b200 import PhiASE
 
     with pytest.raises(ValueError):
-        PhiASE(propagationMode="forward")
+        PhiASE(propagationMode="sideways")
     with pytest.raises(ValueError):
         PhiASE(parallelMode="mpi")
     with pytest.raises(ValueError):

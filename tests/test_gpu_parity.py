@@ -274,7 +274,8 @@ def test_phiase_front_end_runs_and_validates():
     sa, se = legacy_spectrum("cylindrical")
     spectra = CrossSectionData.monochromatic(wavelength=905e-9, crossSectionAbsorption=sa[0],
                                              crossSectionEmission=se[0])
-    p = PhiASE(minRays=4000, maxRays=4000, adaptiveSteps=1, relativeStandardErrorThreshold=0.1,
+    p = PhiASE(propagationMode="backward", minRays=4000, maxRays=4000, adaptiveSteps=1,
+               relativeStandardErrorThreshold=0.1,
                monochromatic=True, rngSeed=7, minSampleRange=10, maxSampleRange=59)
     res = p.run(gainMedium=mesh, crossSections=spectra).getResults()
     assert res.phiAse.shape == (50,) and np.all(res.phiAse > 0)
