@@ -43,6 +43,10 @@ FP32_INSTR_PER_CROSSING = 24   # stated per-crossing FP32 instruction count
 BYTES_PER_CROSSING = 52        # triangle record 48 B + prism beta 4 B
 SMS = 148
 LANES_PER_SM = 128
+FWD_METRIC = "forward Tet4 phi-ASE source rays traced and tallied per second on 1 B200 (crossings/s alongside)"
+FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count of the forward walk
+BYTES_PER_TET_CROSSING = 192       # gathered 156 B (planes 128, neighbour 4, corners 16, beta 8) + tallies 36 B
+FP64_LANES_PER_SM = 64
 
 
 def parse():
@@ -54,6 +58,11 @@ def parse():
     ap.add_argument("--workload", default="disc_poly")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
+    ap.add_argument("--path", default="backward", choices=["backward", "forward"],
+                    help="backward: importance-sampled prism method (headline); forward: Tet4 source-ray method")
+    ap.add_argument("--forward-rays", type=int, default=16_000_000, help="source rays per forward step")
+    ap.add_argument("--tally", default="auto", choices=["auto", "global", "shared"],
+                    help="vertex tallies of the forward kernel")
     return ap.parse_args()
 
 
@@ -226,6 +235,14 @@ def run_ours(args):
                              useReflections=w.useReflections, monochromatic=w.monochromatic,
                              adaptiveSteps=w.adaptiveSteps, rngSeed=1000, minSample=0, maxSample=B - 1,
                              nearFieldSampling=False, **tuned.kwargs())
+    # the forward Tet4 path on the twin of the same medium (1 GPU runs only; fewer steps)
+    fwd = None
+    if world == 1:
+        import argparse as _ap
+
+        fargs = _ap.Namespace(**vars(args))
+        fargs.steps, fargs.warmup = max(2, min(args.steps, 3)), max(args.warmup, 3)
+        fwd = measure_forward(fargs, local, cpu_seconds=min(args.cpu_seconds, 6.0))
     stats = torch.tensor([dev_ms, float(rays), float(e2e_s), float(e2e_rays), float(crossings), ray_ms,
                           float(solved), float(e2e_solved)], dtype=torch.float64, device=dev)
     if world > 1:
@@ -297,8 +314,152 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if fwd is not None:
+            line["forward_tet4"] = fwd
         print(json.dumps(line), flush=True)
     ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def forward_cpu_baseline(tet, sa, se, seconds):
+    """Forward oracle (FP64, OpenMP over all host threads) on a bounded number
+    of source rays of the same Tet4 medium, sized to about `seconds`."""
+    from oracle import oracle
+
+    cores = os.cpu_count() or 1
+    rays = 200_000
+    while True:
+        t0 = time.perf_counter()
+        r = oracle.forward_phi_ase(tet, (sa, se), minRays=rays, seed=4, threads=cores)
+        dt = time.perf_counter() - t0
+        if dt >= seconds / 3 or rays >= 50_000_000:
+            break
+        rays = int(min(rays * max(2.0, min(8.0, seconds / max(dt, 1e-3) / 2)), 50_000_000))
+    return {"value": rays / dt, "unit": "rays/s", "cores": cores, "kind": "port",
+            "sample": f"{rays} source rays of one launch on the Tet4 medium ({tet.numberOfCells} cells, table build "
+                      f"included), "
+                      f"{dt:.1f} s on {cores} threads", "launches": int(r["launches"])}
+
+
+def measure_forward(args, local, rank=0, world=1, cpu_seconds=None):
+    """Forward Tet4 path: steps of `--forward-rays` source rays on the Tet4
+    twin of the workload medium; device time (CUDA events in the library),
+    L2 flushed before every timed step; e2e through the public API with the
+    step's beta uploaded from the host and the per-cell results read back."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from haseongpu_b200 import TetDeviceMesh, TetMesh, _native
+    from haseongpu_b200.configs import WORKLOADS
+
+    w = WORKLOADS[args.workload]()
+    tet = TetMesh.fromPrismMesh(w.mesh)
+    sa, se = w.spectra.resampled(w.monochromatic)
+    dev = torch.device("cuda", local)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)
+    ctx = TetDeviceMesh(tet, sa, se, device=local)
+    rays = int(args.forward_rays)
+
+    def step(k, beta=None):
+        if beta is not None:
+            ctx.update_beta(beta)
+        return ctx.calc_phi_ase(forwardRayCount=rays, rngSeed=1000 + k * world + rank, monochromatic=w.monochromatic,
+                                tallyMode=args.tally)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        step(k)
+    barrier()
+    dev_ms = ray_ms = 0.0
+    cross = traced = launches = 0
+    tally = 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = step(args.warmup + k)
+            dev_ms += r.totalMilliseconds
+            ray_ms += r.rayMilliseconds
+            cross += r.crossings
+            traced += r.raysTraced
+            launches += r.kernelLaunches + 1
+            tally = r.tallyMode
+        barrier()
+    clocks = clk.summary()
+    betas = [np.ascontiguousarray(tet.betaVolume * (1.0 + 0.01 * k)) for k in range(args.steps)]
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(args.warmup + k, beta=betas[k])
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    ctx.update_beta(tet.betaVolume)
+    ctx.close()
+    stats = torch.tensor([dev_ms, e2e_s, float(traced), float(cross), ray_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        mx, sm = stats.clone(), stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        dev_ms_max, e2e_max, traced_all, cross_all = float(mx[0]), float(mx[1]), float(sm[2]), float(sm[3])
+    else:
+        dev_ms_max, e2e_max, traced_all, cross_all = dev_ms, e2e_s, float(traced), float(cross)
+    peaks, peak_kind = measured_peaks()
+    f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    r_fp64 = SMS * FP64_LANES_PER_SM * f_clk / FP64_INSTR_PER_TET_CROSSING
+    l2 = _native.l2_bandwidth(local)
+    r_l2 = l2 * 1e9 / BYTES_PER_TET_CROSSING
+    achieved = cross / (ray_ms * 1e-3)
+    roof = min(r_fp64, r_l2)
+    out = {
+        "value": traced_all / (dev_ms_max * 1e-3), "unit": "rays/s", "ms_per_step": dev_ms_max / args.steps,
+        "crossings_per_s": cross_all / (dev_ms_max * 1e-3), "crossings_per_ray": cross / max(traced, 1),
+        "config": {"workload": f"{w.name} Tet4 twin", "cells": tet.numberOfCells, "points": tet.numberOfPoints,
+                   "wavelengths": int(len(sa)), "rays_per_step_per_gpu": rays, "batches": 8,
+                   "tally": {1: "device-memory atomics", 2: "shared-memory vertex histogram"}.get(tally),
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "e2e": {"value": traced_all / e2e_max, "unit": "rays/s", "h2d_bytes_per_step": tet.numberOfCells * 8,
+                "d2h_bytes_per_step": tet.numberOfCells * (4 + 8 + 8 + 4 + 4)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64_issue" if r_fp64 <= r_l2 else "l2_gather", "kernel": "fwdRayKernel",
+                     "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
+                     "traffic": None, "fp64_issue_peak": r_fp64, "l2_gather_peak": r_l2, "l2_read_gbs_live": l2,
+                     "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
+        "clocks": clocks,
+    }
+    if cpu_seconds and world == 1:
+        out["cpu_baseline"] = forward_cpu_baseline(tet, sa, se, cpu_seconds)
+    return out
+
+
+def run_forward(args):
+    import torch
+    import torch.distributed as dist
+
+    from haseongpu_b200 import build as _build
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    _build.build_library()
+    f = measure_forward(args, local, rank, world, cpu_seconds=args.cpu_seconds)
+    if rank == 0:
+        line = {"metric": FWD_METRIC, "value": f["value"], "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": f["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded gain medium, no dataset)"}
+        line.update({k: v for k, v in f.items() if k not in line})
+        line["config"]["parallelism"] = f"independent ray launches x{world}"
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
@@ -333,6 +494,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.path == "forward":
+        run_forward(args)
     else:
         run_ours(args)
 

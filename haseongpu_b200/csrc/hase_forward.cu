@@ -54,23 +54,53 @@ constexpr uint32_t kTagFwdRay = 3u;
 constexpr uint32_t kFwdKeyHi = 1u;     // key = {seed, 1}
 constexpr uint32_t kMaxBatches = 64u;
 constexpr uint32_t kFwdBlock = 256u;
+constexpr int kFwdRefill = 8;          // idle lanes that trigger a batched start of new rays
+constexpr int kFwdMinBlocks = 3;       // resident ray-kernel blocks per SM the register budget is cut for
 constexpr int kFwdMaxSteps = 10000;    // bounded walk: a ray still inside after this many cells is dropped
 constexpr size_t kMaxHistogramBytes = 200u * 1024u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
+// One cell's walk record: 160 B on a 32-byte boundary, so every record lies
+// in exactly two 128-byte lines and a crossing fetches all of it at once.
+struct __align__(32) TetCell {
+    double4 plane[4];  // lambda_f(x) = a.x + b.y + c.z + d
+    int4 nbr;          // per face (neighbour << 2) | neighbour's local face, -1 at the boundary
+    uint4 matv;        // material vertex of each corner (cladding cells offset by Np)
+};
+static_assert(sizeof(TetCell) == 160, "TetCell must be 160 bytes");
+
 struct TetView {
-    const double4* plane;   // [C][4]: lambda_f(x) = a.x + b.y + c.z + d
-    const int* nbr;         // [C][4]: (neighbour << 2) | neighbour's local face, -1 at the boundary
-    const uint4* matv;      // [C]: material vertex of each corner (cladding cells offset by Np)
-    const uint4* cellv;     // [C]: point indices
+    const TetCell* cell;    // [C]
     const double* gainBeta; // [C]: beta, NaN for cladding cells
     const double* points;   // [Np][3]
     const double* prefix;   // [C]: inclusive prefix of beta * V
-    uint32_t C, Np, lastSource;
-    double cladAbs, nTot, Btot;
+    const uint32_t* guide;  // [K + 1]: guide[j] = first cell whose prefix exceeds j Btot / K; guide[K] = C
+    uint32_t C, Np, lastSource, K;
+    double cladAbs, nTot, Btot, guideScale;  // guideScale = K / Btot
 };
 
 __device__ __forceinline__ double unit53(uint32_t x) { return (double(x >> 8) + 0.5) * (1.0 / 16777216.0); }
+
+// 256-bit read-only loads (sm_100): one 32-byte sector per lane and instruction.
+__device__ __forceinline__ double4 ldPlane(const double4* p) {
+    double4 v;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
+}
+
+struct CellLinks {
+    int4 nbr;
+    uint4 matv;
+};
+
+__device__ __forceinline__ CellLinks ldLinks(const int4* p) {
+    CellLinks l;
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(l.nbr.x), "=r"(l.nbr.y), "=r"(l.nbr.z), "=r"(l.nbr.w), "=r"(l.matv.x), "=r"(l.matv.y),
+          "=r"(l.matv.z), "=r"(l.matv.w)
+        : "l"(p));
+    return l;
+}
 
 // Exit face of the cell whose planes are pl for a ray at (x, y, z) moving
 // along u, the entry face ff excluded: among the faces with dlambda < 0, the
@@ -82,10 +112,9 @@ __device__ __forceinline__ int exitFace(const double4* __restrict__ pl, double x
     double bl = 0.0, bd = -1.0;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        const double2 ab = __ldg(reinterpret_cast<const double2*>(pl + f));
-        const double2 cd = __ldg(reinterpret_cast<const double2*>(pl + f) + 1);
-        lam[f] = fma(ab.x, x, fma(ab.y, y, fma(cd.x, z, cd.y)));
-        dl[f] = fma(ab.x, ux, fma(ab.y, uy, cd.x * uz));
+        const double4 p = ldPlane(pl + f);
+        lam[f] = fma(p.x, x, fma(p.y, y, fma(p.z, z, p.w)));
+        dl[f] = fma(p.x, ux, fma(p.y, uy, p.z * uz));
         if (f == ff || !(dl[f] < 0.0)) continue;
         const double lc = fmax(lam[f], 0.0);
         // lc / -dl[f] < bl / -bd  <=>  lc * bd > bl * dl[f]   (both rates negative)
@@ -106,16 +135,19 @@ __device__ __forceinline__ double gainCoefficient(const TetView& m, uint32_t c, 
 
 struct FwdRay {
     double x, y, z, ux, uy, uz, G, sA, sE;
+    double pv[4];  // tallies not yet added to device memory, per corner of the current cell
+    uint4 pid;     // the current cell's material vertices (owners of pv)
+    int4 nbr;      // the current cell's neighbours
     uint32_t c;
     int ff, steps;
 };
 
 // Track-length tally of one segment: weight G (e^{gl} - 1)/g split to the
-// four corners by the midpoint barycentric weights.  Returns false (ray
-// dropped) when the contribution is not finite.
-template <typename Tally>
+// four corners by the midpoint barycentric weights, added to the ray's
+// pending corner tallies.  Returns false (ray dropped) when the contribution
+// is not finite.
 __device__ __forceinline__ bool tallySegment(const TetView& m, FwdRay& r, double len, const double lam[4],
-                                             const double dl[4], Tally&& add) {
+                                             const double dl[4]) {
     const double gc = gainCoefficient(m, r.c, r.sA, r.sE);
     const double gl = gc * len;
     const double E = expm1(gl);
@@ -128,22 +160,57 @@ __device__ __forceinline__ bool tallySegment(const TetView& m, FwdRay& r, double
         w[f] = fmax(0.0, fma(0.5 * len, dl[f], lam[f]));
         wsum += w[f];
     }
-    const uint4 mv = __ldg(m.matv + r.c);
-    if (wsum > DBL_EPSILON) {
-        const double s = contribution / wsum;
-        add(mv.x, w[0] * s);
-        add(mv.y, w[1] * s);
-        add(mv.z, w[2] * s);
-        add(mv.w, w[3] * s);
-    } else {
-        const double q = 0.25 * contribution;
-        add(mv.x, q);
-        add(mv.y, q);
-        add(mv.z, q);
-        add(mv.w, q);
-    }
+    const bool split = wsum > DBL_EPSILON;
+    const double s = split ? contribution / wsum : 0.25 * contribution;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) r.pv[f] = fma(split ? w[f] : 1.0, s, r.pv[f]);
     r.G = fma(r.G, E, r.G);
     return true;
+}
+
+// Moving into a cell with material vertices mn: pending tallies of vertices the
+// new cell shares carry over (a face crossing keeps three of the four), the
+// others are added to device memory through `flush`.
+template <typename Flush>
+__device__ __forceinline__ void carryPending(FwdRay& r, uint4 mn, Flush&& flush) {
+    const uint32_t o[4] = {r.pid.x, r.pid.y, r.pid.z, r.pid.w};
+    const uint32_t nn[4] = {mn.x, mn.y, mn.z, mn.w};
+    double nv[4] = {0.0, 0.0, 0.0, 0.0};
+    uint32_t gone = 0;  // old corners the new cell does not have
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        bool kept = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (o[j] == nn[k]) {
+                nv[k] = r.pv[j];
+                kept = true;
+            }
+        gone |= kept ? 0u : 1u << j;
+    }
+    // a crossing inside one material drops exactly one corner: one flush site
+    // for all lanes; a change of material (gain <-> cladding) drops all four
+    const int j0 = __ffs(gone) - 1;
+    const double v0 = j0 == 0 ? r.pv[0] : j0 == 1 ? r.pv[1] : j0 == 2 ? r.pv[2] : r.pv[3];
+    const uint32_t id0 = j0 == 0 ? o[0] : j0 == 1 ? o[1] : j0 == 2 ? o[2] : o[3];
+    if (v0 != 0.0) flush(id0, v0);
+    const uint32_t rest = gone & (gone - 1);
+    if (rest) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (((rest >> j) & 1u) && r.pv[j] != 0.0) flush(o[j], r.pv[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r.pv[k] = nv[k];
+    r.pid = mn;
+}
+
+template <typename Flush>
+__device__ __forceinline__ void flushPending(FwdRay& r, Flush&& flush) {
+    const uint32_t o[4] = {r.pid.x, r.pid.y, r.pid.z, r.pid.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (r.pv[j] != 0.0) flush(o[j], r.pv[j]);
 }
 
 struct FwdLaunch {
@@ -154,31 +221,38 @@ struct FwdLaunch {
     double* score;                 // [B][2 Np]
     uint32_t* visits;              // [C]
     uint32_t* dropped;             // [C]
-    unsigned long long* crossings; // [1]
     double shift[kMaxBatches];
     uint32_t nb[kMaxBatches];
     uint32_t phase[kMaxBatches];
 };
 
 // Source ray i of batch b (ray r = i B + b of this launch).
-__device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, uint64_t i, FwdRay& r) {
+__device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, uint32_t i, FwdRay& r) {
     const TetView& m = L.m;
     const uint32_t nb = L.nb[b];
     const double t = (double(i) + L.shift[b]) / double(nb) * m.Btot;
-    // upper_bound: first cell whose inclusive prefix exceeds t
-    uint32_t lo = 0, hi = m.C;
+    // upper_bound (first cell whose inclusive prefix exceeds t) inside the
+    // guide-table bracket of t, widened by one slot on each side for the
+    // rounding of j (indexed search, Chen and Asau 1974)
+    const double jf = fmin(fmax(t * m.guideScale, 0.0), double(m.K - 1));
+    const uint32_t j = uint32_t(jf);
+    uint32_t lo = __ldg(m.guide + (j > 0 ? j - 1 : 0));
+    uint32_t hi = __ldg(m.guide + min(j + 2, m.K));
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         if (__ldg(m.prefix + mid) > t) hi = mid;
         else lo = mid + 1;
     }
     const uint32_t c = lo >= m.C ? m.lastSource : lo;
-    const uint32_t ray = uint32_t(i * L.B + b);
+    const uint32_t ray = i * L.B + b;
     const Philox4 o = philox4x32_10(ray, L.launch, 0u, kTagFwdRay, L.seed, kFwdKeyHi);
     const Philox4 o2 = philox4x32_10(ray, L.launch, 1u, kTagFwdRay, L.seed, kFwdKeyHi);
     const double e0 = -log(unit53(o.x)), e1 = -log(unit53(o.y)), e2 = -log(unit53(o.z)), e3 = -log(unit53(o.w));
     const double esum = e0 + e1 + e2 + e3;
-    const uint4 cv = __ldg(m.cellv + c);
+    const CellLinks lk = ldLinks(&m.cell[c].nbr);
+    const uint4 mv = lk.matv;
+    const uint32_t off = mv.x >= m.Np ? m.Np : 0u;
+    const uint4 cv = make_uint4(mv.x - off, mv.y - off, mv.z - off, mv.w - off);
     const double* P = m.points;
     const double w0 = e0 / esum, w1 = e1 / esum, w2 = e2 / esum, w3 = e3 / esum;
     r.x = w0 * P[3 * cv.x] + w1 * P[3 * cv.y] + w2 * P[3 * cv.z] + w3 * P[3 * cv.w];
@@ -191,13 +265,17 @@ __device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, ui
     r.ux = rr * cphi;
     r.uy = rr * sphi;
     r.uz = z;
-    const uint32_t lamIdx = uint32_t((i * L.nL / nb + L.phase[b]) % L.nL);
+    const uint32_t lamIdx = uint32_t((uint64_t(i) * L.nL / nb + L.phase[b]) % L.nL);
     r.sA = __ldg(L.sigmaA + lamIdx);
     r.sE = __ldg(L.sigmaE + lamIdx);
     r.G = 1.0;
     r.c = c;
     r.ff = -1;
     r.steps = 0;
+    r.pid = mv;
+    r.nbr = lk.nbr;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r.pv[k] = 0.0;
 }
 
 }  // namespace
@@ -208,7 +286,7 @@ namespace {
 // rays.  SMEM: the block's vertex tallies go to a shared-memory histogram of
 // 2 Np doubles, added to the batch's device-memory tallies once at the end.
 template <bool SMEM>
-__global__ void __launch_bounds__(kFwdBlock) fwdRayKernel(const FwdLaunch L) {
+__global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const FwdLaunch L) {
     extern __shared__ double hist[];
     const TetView& m = L.m;
     const uint32_t b = blockIdx.x % L.B;
@@ -218,52 +296,58 @@ __global__ void __launch_bounds__(kFwdBlock) fwdRayKernel(const FwdLaunch L) {
         for (uint32_t k = threadIdx.x; k < nV; k += blockDim.x) hist[k] = 0.0;
         __syncthreads();
     }
-    const uint64_t nb = L.nb[b];
-    const uint64_t stride = uint64_t(L.blocksPerBatch) * blockDim.x;
-    uint64_t i = uint64_t(blockIdx.x / L.B) * blockDim.x + threadIdx.x;
+    // 32-bit ray indices: a batch holds at most 2^31 rays, so i + stride cannot wrap
+    const uint32_t nb = L.nb[b];
+    const uint32_t stride = L.blocksPerBatch * blockDim.x;
+    uint32_t i = (blockIdx.x / L.B) * blockDim.x + threadIdx.x;
     auto add = [&](uint32_t v, double val) {
         if (SMEM) atomicAdd(hist + v, val);
         else atomicAdd(gscore + v, val);
     };
     FwdRay r;
     bool live = false;
-    unsigned long long crossings = 0;
     for (;;) {
-        if (!live) {
-            if (i >= nb) break;
+        // idle lanes start their next rays together, once kFwdRefill of them
+        // wait (or no lane of the warp is walking), so the warp runs the
+        // source sampling once for several lanes instead of once per lane
+        const bool canStart = !live && i < nb;
+        const unsigned starters = __ballot_sync(0xffffffffu, canStart);
+        const unsigned walking = __ballot_sync(0xffffffffu, live);
+        if (starters == 0 && walking == 0) break;
+        if (starters != 0 && (__popc(starters) >= kFwdRefill || walking == 0) && canStart) {
             initSourceRay(L, b, i, r);
             i += stride;
             live = true;
         }
+        if (!live) continue;
         double lam[4], dl[4], len;
-        const int bf = exitFace(m.plane + 4 * size_t(r.c), r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
+        const int bf = exitFace(m.cell[r.c].plane, r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
         bool drop = bf < 0 || ++r.steps > kFwdMaxSteps;
         if (!drop) {
-            drop = !tallySegment(m, r, len, lam, dl, add);
-            if (!drop) {
-                atomicAdd(L.visits + r.c, 1u);
-                ++crossings;
-            }
+            drop = !tallySegment(m, r, len, lam, dl);
+            if (!drop) atomicAdd(L.visits + r.c, 1u);
         }
         if (drop) {
             atomicAdd(L.dropped + r.c, 1u);
+            flushPending(r, add);
             live = false;
             continue;
         }
         r.x = fma(r.ux, len, r.x);
         r.y = fma(r.uy, len, r.y);
         r.z = fma(r.uz, len, r.z);
-        const int n = __ldg(m.nbr + 4 * size_t(r.c) + bf);
+        const int n = bf == 0 ? r.nbr.x : bf == 1 ? r.nbr.y : bf == 2 ? r.nbr.z : r.nbr.w;
         if (n < 0) {
+            flushPending(r, add);
             live = false;  // left the mesh
         } else {
             r.c = uint32_t(n) >> 2;
             r.ff = n & 3;
+            const CellLinks lk = ldLinks(&m.cell[r.c].nbr);
+            r.nbr = lk.nbr;
+            carryPending(r, lk.matv, add);
         }
     }
-    // crossings: warp sum, one atomic per warp
-    for (int o = 16; o > 0; o >>= 1) crossings += __shfl_xor_sync(0xffffffffu, crossings, o);
-    if ((threadIdx.x & 31) == 0 && crossings) atomicAdd(L.crossings, crossings);
     if (SMEM) {
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < nV; k += blockDim.x) {
@@ -278,8 +362,10 @@ struct FinLaunch {
     const double* lumped;  // [2 Np]
     const double* vol;     // [C]
     const double* beta;    // [C] (dndt)
-    const uint4* matv;     // [C]
+    const TetCell* cell;   // [C] (material vertices)
     const uint32_t* dropped;
+    const uint32_t* visits;
+    unsigned long long* crossings;  // sum of visits (zeroed before the launch)
     float* phi;
     double* rse;
     double* dndt;
@@ -293,8 +379,11 @@ struct FinLaunch {
 // batch-mean relative error (include/kernels/forwardPhiAseMapping.hpp:51-150).
 __global__ void __launch_bounds__(256) fwdFinalizeKernel(const FinLaunch F) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long nvis = c < F.C ? F.visits[c] : 0ull;
+    for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
+    if ((threadIdx.x & 31) == 0 && nvis) atomicAdd(F.crossings, nvis);
     if (c >= F.C) return;
-    const uint4 mv = F.matv[c];
+    const uint4 mv = F.cell[c].matv;
     const uint32_t v[4] = {mv.x, mv.y, mv.z, mv.w};
     double lumped[4];
 #pragma unroll
@@ -367,7 +456,8 @@ __global__ void __launch_bounds__(128) fwdTraceKernel(const TraceLaunch T) {
     uint32_t seg = 0;
     while (seg < uint32_t(kFwdMaxSteps)) {
         double lam[4], dl[4], len;
-        const int bf = exitFace(m.plane + 4 * size_t(r.c), r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
+        const TetCell* rec = m.cell + r.c;
+        const int bf = exitFace(rec->plane, r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
         if (bf < 0) break;
         lg += gainCoefficient(m, r.c, T.sA, T.sE) * len;
         if (seg < T.maxSegments) {
@@ -378,7 +468,7 @@ __global__ void __launch_bounds__(128) fwdTraceKernel(const TraceLaunch T) {
         r.x = fma(r.ux, len, r.x);
         r.y = fma(r.uy, len, r.y);
         r.z = fma(r.uz, len, r.z);
-        const int n = m.nbr[4 * size_t(r.c) + bf];
+        const int n = (&rec->nbr.x)[bf];
         if (n < 0) {
             st = 0;
             break;
@@ -402,7 +492,7 @@ namespace {
 struct TetHost {
     std::vector<double4> plane;
     std::vector<int> nbr;
-    std::vector<uint4> matv, cellv;
+    std::vector<uint4> matv;
     std::vector<double> vol, lumped;
 };
 
@@ -415,7 +505,6 @@ hase_status buildTetHost(const hase_tet_mesh_desc* d, TetHost& h) {
     h.plane.resize(4 * size_t(C));
     h.nbr.assign(4 * size_t(C), -1);
     h.matv.resize(C);
-    h.cellv.resize(C);
     h.vol.resize(C);
     h.lumped.assign(2 * size_t(Np), 0.0);
     struct FaceKey {
@@ -459,7 +548,6 @@ hase_status buildTetHost(const hase_tet_mesh_desc* d, TetHost& h) {
         }
         const bool clad = d->claddingCellTypes && d->claddingCellTypes[c] == d->claddingNumber;
         const uint32_t off = clad ? Np : 0u;
-        h.cellv[c] = make_uint4(v[0], v[1], v[2], v[3]);
         h.matv[c] = make_uint4(v[0] + off, v[1] + off, v[2] + off, v[3] + off);
         for (int k = 0; k < 4; ++k) h.lumped[v[k] + off] += h.vol[c] / 4.0;
         for (int f = 0; f < 4; ++f) {
@@ -508,9 +596,10 @@ struct hase_tet_context {
     uint32_t cladNumber = 0;
     std::vector<uint32_t> cladTypes;
     std::vector<double> vol, sigmaA, sigmaE;
-    DevBuf<double4> plane;
-    DevBuf<int> nbr;
-    DevBuf<uint4> matv, cellv;
+    DevBuf<TetCell> cell;
+    DevBuf<uint32_t> guide;
+    uint32_t K = 1;
+    double guideScale = 0.0;
     DevBuf<double> gainBeta, beta, points, prefix, lumped, dvol, sigA, sigE;
     // accumulators and outputs
     DevBuf<double> score, rse, dndt;
@@ -520,16 +609,16 @@ struct hase_tet_context {
 
     TetView view() const {
         TetView v{};
-        v.plane = plane.p;
-        v.nbr = nbr.p;
-        v.matv = matv.p;
-        v.cellv = cellv.p;
+        v.cell = cell.p;
         v.gainBeta = gainBeta.p;
         v.points = points.p;
         v.prefix = prefix.p;
+        v.guide = guide.p;
         v.C = C;
         v.Np = Np;
         v.lastSource = lastSource;
+        v.K = K;
+        v.guideScale = guideScale;
         v.cladAbs = cladAbs;
         v.nTot = nTot;
         v.Btot = Btot;
@@ -556,6 +645,20 @@ hase_status uploadTetBeta(hase_tet_context* c, const double* betaVolume) {
     }
     c->Btot = acc;
     c->lastSource = last;
+    // guide table of the source CDF: guide[j] = upper_bound(prefix, j Btot / K)
+    const uint32_t K = c->C;
+    std::vector<uint32_t> guide(size_t(K) + 1);
+    uint32_t at = 0;
+    for (uint32_t j = 0; j < K; ++j) {
+        const double bj = double(j) * (acc / double(K));
+        while (at < c->C && !(pre[at] > bj)) ++at;
+        guide[j] = at;
+    }
+    guide[K] = c->C;
+    c->K = K;
+    c->guideScale = acc > 0.0 ? double(K) / acc : 0.0;
+    HASE_CUDA(cudaMemcpyAsync(c->guide.p, guide.data(), guide.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->beta.p, betaVolume, c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->prefix.p, pre.data(), c->C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -632,17 +735,21 @@ hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spec
         return cleanup(fail(HASE_CUDA_ERROR, "stream/event creation failed"));
     const size_t C = c->C, Np = c->Np;
     hase_status st = HASE_OK;
-    if ((st = upload(c->plane, h.plane.data(), 4 * C, c->stream)) != HASE_OK ||
-        (st = upload(c->nbr, h.nbr.data(), 4 * C, c->stream)) != HASE_OK ||
-        (st = upload(c->matv, h.matv.data(), C, c->stream)) != HASE_OK ||
-        (st = upload(c->cellv, h.cellv.data(), C, c->stream)) != HASE_OK ||
+    std::vector<TetCell> rec(C);
+    for (size_t k = 0; k < C; ++k) {
+        for (int f = 0; f < 4; ++f) rec[k].plane[f] = h.plane[4 * k + f];
+        rec[k].nbr = make_int4(h.nbr[4 * k], h.nbr[4 * k + 1], h.nbr[4 * k + 2], h.nbr[4 * k + 3]);
+        rec[k].matv = h.matv[k];
+    }
+    if ((st = upload(c->cell, rec.data(), C, c->stream)) != HASE_OK ||
         (st = upload(c->points, d->points, 3 * Np, c->stream)) != HASE_OK ||
         (st = upload(c->lumped, h.lumped.data(), 2 * Np, c->stream)) != HASE_OK ||
         (st = upload(c->dvol, h.vol.data(), C, c->stream)) != HASE_OK ||
         (st = upload(c->sigA, c->sigmaA.data(), c->sigmaA.size(), c->stream)) != HASE_OK ||
         (st = upload(c->sigE, c->sigmaE.data(), c->sigmaE.size(), c->stream)) != HASE_OK)
         return cleanup(st);
-    if (c->gainBeta.ensure(C) != cudaSuccess || c->beta.ensure(C) != cudaSuccess || c->prefix.ensure(C) != cudaSuccess)
+    if (c->gainBeta.ensure(C) != cudaSuccess || c->beta.ensure(C) != cudaSuccess || c->prefix.ensure(C) != cudaSuccess ||
+        c->guide.ensure(C + 1) != cudaSuccess)
         return cleanup(fail(HASE_OUT_OF_MEMORY, "device allocation failed"));
     if ((st = uploadTetBeta(c, d->betaVolume)) != HASE_OK) return cleanup(st);
     *out = c;
@@ -671,16 +778,23 @@ hase_status hase_tet_tables(hase_tet_context* c, int32_t* neighbors, int32_t* ne
     if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
     HASE_CUDA(cudaSetDevice(c->device));
     const size_t C = c->C;
-    if (neighbors || neighborFace) {
-        std::vector<int> packed(4 * C);
-        HASE_CUDA(cudaMemcpyAsync(packed.data(), c->nbr.p, 4 * C * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        HASE_CUDA(cudaStreamSynchronize(c->stream));
-        for (size_t k = 0; k < 4 * C; ++k) {
-            if (neighbors) neighbors[k] = packed[k] < 0 ? -1 : packed[k] >> 2;
-            if (neighborFace) neighborFace[k] = packed[k] < 0 ? -1 : packed[k] & 3;
+    std::vector<TetCell> rec(C);
+    HASE_CUDA(cudaMemcpyAsync(rec.data(), c->cell.p, C * sizeof(TetCell), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < C; ++k) {
+        const int n4[4] = {rec[k].nbr.x, rec[k].nbr.y, rec[k].nbr.z, rec[k].nbr.w};
+        for (int f = 0; f < 4; ++f) {
+            if (neighbors) neighbors[4 * k + f] = n4[f] < 0 ? -1 : n4[f] >> 2;
+            if (neighborFace) neighborFace[4 * k + f] = n4[f] < 0 ? -1 : n4[f] & 3;
+            if (planes) {
+                const double4 p = rec[k].plane[f];
+                planes[16 * k + 4 * f] = p.x;
+                planes[16 * k + 4 * f + 1] = p.y;
+                planes[16 * k + 4 * f + 2] = p.z;
+                planes[16 * k + 4 * f + 3] = p.w;
+            }
         }
     }
-    if (planes) HASE_CUDA(cudaMemcpyAsync(planes, c->plane.p, 4 * C * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
     if (volumes) HASE_CUDA(cudaMemcpyAsync(volumes, c->dvol.p, C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
     return HASE_OK;
@@ -802,15 +916,16 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
     L.score = c->score.p;
     L.visits = c->visits.p;
     L.dropped = c->dropped.p;
-    L.crossings = c->crossings.p;
 
     FinLaunch F{};
     F.score = c->score.p;
     F.lumped = c->lumped.p;
     F.vol = c->dvol.p;
     F.beta = c->beta.p;
-    F.matv = c->matv.p;
+    F.cell = c->cell.p;
     F.dropped = c->dropped.p;
+    F.visits = c->visits.p;
+    F.crossings = c->crossings.p;
     F.phi = c->phi.p;
     F.rse = c->rse.p;
     F.dndt = c->dndt.p;
@@ -879,6 +994,7 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
         total = target;
         F.totalRays = double(total);
         HASE_CUDA(cudaMemsetAsync(c->unconverged.p, 0, sizeof(uint32_t), c->stream));
+        HASE_CUDA(cudaMemsetAsync(c->crossings.p, 0, sizeof(unsigned long long), c->stream));
         fwdFinalizeKernel<<<(C + 255) / 256, 256, 0, c->stream>>>(F);
         HASE_CUDA(cudaGetLastError());
         res->kernelLaunches += 1;
