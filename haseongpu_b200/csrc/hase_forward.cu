@@ -60,14 +60,15 @@ constexpr int kFwdMaxSteps = 10000;    // bounded walk: a ray still inside after
 constexpr size_t kMaxHistogramBytes = 200u * 1024u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
-// One cell's walk record: 160 B on a 32-byte boundary, so every record lies
-// in exactly two 128-byte lines and a crossing fetches all of it at once.
-struct __align__(32) TetCell {
-    double4 plane[4];  // lambda_f(x) = a.x + b.y + c.z + d
+// One cell's walk record: one 128-byte line.  Only the planes of faces 1..3
+// are stored; lambda_0 = 1 - (lambda_1 + lambda_2 + lambda_3) and its rate
+// along the ray is minus the sum of theirs.
+struct __align__(128) TetCell {
+    double4 plane[3];  // faces 1..3: lambda_f(x) = a.x + b.y + c.z + d
     int4 nbr;          // per face (neighbour << 2) | neighbour's local face, -1 at the boundary
     uint4 matv;        // material vertex of each corner (cladding cells offset by Np)
 };
-static_assert(sizeof(TetCell) == 160, "TetCell must be 160 bytes");
+static_assert(sizeof(TetCell) == 128, "TetCell must be one 128-byte line");
 
 struct TetView {
     const TetCell* cell;    // [C]
@@ -102,7 +103,7 @@ __device__ __forceinline__ CellLinks ldLinks(const int4* p) {
     return l;
 }
 
-// Exit face of the cell whose planes are pl for a ray at (x, y, z) moving
+// Exit face of the cell whose planes of faces 1..3 are pl for a ray at (x, y, z) moving
 // along u, the entry face ff excluded: among the faces with dlambda < 0, the
 // smallest max(lambda, 0) / -dlambda (lowest index on a tie).  Fills lam and
 // dl for all four faces; returns -1 when no face decreases.
@@ -111,10 +112,15 @@ __device__ __forceinline__ int exitFace(const double4* __restrict__ pl, double x
     int bf = -1;
     double bl = 0.0, bd = -1.0;
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        const double4 p = ldPlane(pl + f);
+    for (int f = 1; f < 4; ++f) {
+        const double4 p = ldPlane(pl + f - 1);
         lam[f] = fma(p.x, x, fma(p.y, y, fma(p.z, z, p.w)));
         dl[f] = fma(p.x, ux, fma(p.y, uy, p.z * uz));
+    }
+    lam[0] = 1.0 - (lam[1] + lam[2] + lam[3]);
+    dl[0] = -(dl[1] + dl[2] + dl[3]);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
         if (f == ff || !(dl[f] < 0.0)) continue;
         const double lc = fmax(lam[f], 0.0);
         // lc / -dl[f] < bl / -bd  <=>  lc * bd > bl * dl[f]   (both rates negative)
@@ -221,6 +227,7 @@ struct FwdLaunch {
     double* score;                 // [B][2 Np]
     uint32_t* visits;              // [C]
     uint32_t* dropped;             // [C]
+    uint32_t* next;                // [B]: next unclaimed ray index of each batch (zeroed per launch)
     double shift[kMaxBatches];
     uint32_t nb[kMaxBatches];
     uint32_t phase[kMaxBatches];
@@ -296,28 +303,38 @@ __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const F
         for (uint32_t k = threadIdx.x; k < nV; k += blockDim.x) hist[k] = 0.0;
         __syncthreads();
     }
-    // 32-bit ray indices: a batch holds at most 2^31 rays, so i + stride cannot wrap
+    // Rays of the batch are claimed dynamically: a warp whose idle lanes
+    // reach kFwdRefill (or that has no lane walking) takes the next
+    // popc(idle) ray indices of its batch with one atomic and starts them
+    // together, so every lane of every warp of the batch stays busy until the
+    // batch runs dry.
     const uint32_t nb = L.nb[b];
-    const uint32_t stride = L.blocksPerBatch * blockDim.x;
-    uint32_t i = (blockIdx.x / L.B) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     auto add = [&](uint32_t v, double val) {
         if (SMEM) atomicAdd(hist + v, val);
         else atomicAdd(gscore + v, val);
     };
     FwdRay r;
     bool live = false;
+    bool exhausted = nb == 0;  // warp-uniform
     for (;;) {
-        // idle lanes start their next rays together, once kFwdRefill of them
-        // wait (or no lane of the warp is walking), so the warp runs the
-        // source sampling once for several lanes instead of once per lane
-        const bool canStart = !live && i < nb;
-        const unsigned starters = __ballot_sync(0xffffffffu, canStart);
         const unsigned walking = __ballot_sync(0xffffffffu, live);
-        if (starters == 0 && walking == 0) break;
-        if (starters != 0 && (__popc(starters) >= kFwdRefill || walking == 0) && canStart) {
-            initSourceRay(L, b, i, r);
-            i += stride;
-            live = true;
+        if (walking == 0 && exhausted) break;
+        const unsigned idle = ~walking;
+        if (!exhausted && idle != 0 && (__popc(idle) >= kFwdRefill || walking == 0)) {
+            const int leader = __ffs(idle) - 1;
+            const uint32_t want = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(L.next + b, want);
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + want >= nb) exhausted = true;
+            if (!live) {
+                const uint32_t i = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+                if (i < nb) {
+                    initSourceRay(L, b, i, r);
+                    live = true;
+                }
+            }
         }
         if (!live) continue;
         double lam[4], dl[4], len;
@@ -603,7 +620,7 @@ struct hase_tet_context {
     DevBuf<double> gainBeta, beta, points, prefix, lumped, dvol, sigA, sigE;
     // accumulators and outputs
     DevBuf<double> score, rse, dndt;
-    DevBuf<uint32_t> visits, dropped, unconverged;
+    DevBuf<uint32_t> visits, dropped, unconverged, next;
     DevBuf<unsigned long long> crossings;
     DevBuf<float> phi;
 
@@ -737,7 +754,7 @@ hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spec
     hase_status st = HASE_OK;
     std::vector<TetCell> rec(C);
     for (size_t k = 0; k < C; ++k) {
-        for (int f = 0; f < 4; ++f) rec[k].plane[f] = h.plane[4 * k + f];
+        for (int f = 1; f < 4; ++f) rec[k].plane[f - 1] = h.plane[4 * k + f];
         rec[k].nbr = make_int4(h.nbr[4 * k], h.nbr[4 * k + 1], h.nbr[4 * k + 2], h.nbr[4 * k + 3]);
         rec[k].matv = h.matv[k];
     }
@@ -783,11 +800,15 @@ hase_status hase_tet_tables(hase_tet_context* c, int32_t* neighbors, int32_t* ne
     HASE_CUDA(cudaStreamSynchronize(c->stream));
     for (size_t k = 0; k < C; ++k) {
         const int n4[4] = {rec[k].nbr.x, rec[k].nbr.y, rec[k].nbr.z, rec[k].nbr.w};
+        const double4 q1 = rec[k].plane[0], q2 = rec[k].plane[1], q3 = rec[k].plane[2];
+        const double4 q0 = make_double4(-(q1.x + q2.x + q3.x), -(q1.y + q2.y + q3.y), -(q1.z + q2.z + q3.z),
+                                        1.0 - (q1.w + q2.w + q3.w));
+        const double4 q[4] = {q0, q1, q2, q3};
         for (int f = 0; f < 4; ++f) {
             if (neighbors) neighbors[4 * k + f] = n4[f] < 0 ? -1 : n4[f] >> 2;
             if (neighborFace) neighborFace[4 * k + f] = n4[f] < 0 ? -1 : n4[f] & 3;
             if (planes) {
-                const double4 p = rec[k].plane[f];
+                const double4 p = q[f];
                 planes[16 * k + 4 * f] = p.x;
                 planes[16 * k + 4 * f + 1] = p.y;
                 planes[16 * k + 4 * f + 2] = p.z;
@@ -889,6 +910,7 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
     HASE_CUDA(c->visits.ensure(C));
     HASE_CUDA(c->dropped.ensure(C));
     HASE_CUDA(c->unconverged.ensure(1));
+    HASE_CUDA(c->next.ensure(kMaxBatches));
     HASE_CUDA(c->crossings.ensure(1));
     HASE_CUDA(c->phi.ensure(C));
     HASE_CUDA(c->rse.ensure(C));
@@ -916,6 +938,7 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
     L.score = c->score.p;
     L.visits = c->visits.p;
     L.dropped = c->dropped.p;
+    L.next = c->next.p;
 
     FinLaunch F{};
     F.score = c->score.p;
@@ -984,6 +1007,7 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
             uint32_t perBatch = std::max(1u, resident / B);
             perBatch = std::min(perBatch, std::max(1u, (maxNb + block - 1) / block));
             L.blocksPerBatch = perBatch;
+            HASE_CUDA(cudaMemsetAsync(c->next.p, 0, B * sizeof(uint32_t), c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
             if (smem) fwdRayKernel<true><<<perBatch * B, block, histBytes, c->stream>>>(L);
             else fwdRayKernel<false><<<perBatch * B, block, 0, c->stream>>>(L);

@@ -100,7 +100,9 @@ hase_status hase_tet_context_destroy(hase_tet_context* ctx);
 
 /* Device tables of the context: neighbours [C][4] (-1 at the boundary),
  * neighbour local face [C][4], face planes [C][4][4] (lambda_f(x) =
- * a.x + b.y + c.z + d), volumes [C].  Any pointer may be NULL. */
+ * a.x + b.y + c.z + d; the device keeps faces 1..3, face 0 is returned as
+ * lambda_0 = 1 - lambda_1 - lambda_2 - lambda_3), volumes [C].  Any pointer
+ * may be NULL. */
 hase_status hase_tet_tables(hase_tet_context* ctx, int32_t* neighbors, int32_t* neighborFace, double* planes,
                             double* volumes);
 
