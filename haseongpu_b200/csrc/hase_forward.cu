@@ -8,7 +8,8 @@
 //                  left the mesh, so a warp stays full until the tail.  Source:
 //                  stratified beta*V CDF target (i + shift_b)/N_b * B_tot and a
 //                  binary search of the inclusive prefix, a uniform point in
-//                  the tet from four exponentials, an isotropic direction, a
+//                  the tet from four exponentials (paired with the corners in
+//                  ascending point index), an isotropic direction, a
 //                  stratified wavelength bin.  Walk: per cell the four
 //                  barycentric face coordinates lambda_f = a.x + d and their
 //                  rates along the ray; the exit is the decreasing coordinate
@@ -60,7 +61,11 @@ constexpr int kFwdMaxSteps = 10000;    // bounded walk: a ray still inside after
 constexpr size_t kMaxHistogramBytes = 200u * 1024u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
-// One cell's walk record: one 128-byte line.  Only the planes of faces 1..3
+// One cell's walk record: one 128-byte line.  Corners are stored sorted by
+// global point index (face k opposite corner k), so that when a ray crosses
+// from one cell into its neighbour the three shared corners keep their
+// relative order: the old corners other than the exit face map, in order, to
+// the new corners other than the entry face.  Only the planes of faces 1..3
 // are stored; lambda_0 = 1 - (lambda_1 + lambda_2 + lambda_3) and its rate
 // along the ray is minus the sum of theirs.
 struct __align__(128) TetCell {
@@ -174,40 +179,33 @@ __device__ __forceinline__ bool tallySegment(const TetView& m, FwdRay& r, double
     return true;
 }
 
-// Moving into a cell with material vertices mn: pending tallies of vertices the
-// new cell shares carry over (a face crossing keeps three of the four), the
-// others are added to device memory through `flush`.
+// Moving from the current cell through its face bf into the neighbour entered
+// through its face fe (corner-sorted records, material vertices mn): inside
+// one material the neighbour's corners other than fe are the old corners
+// other than bf, in the same order, so their pending tallies move over and
+// only the old corner bf is added to device memory; a change of material
+// (gain <-> cladding, other material vertices) adds all four.
 template <typename Flush>
-__device__ __forceinline__ void carryPending(FwdRay& r, uint4 mn, Flush&& flush) {
-    const uint32_t o[4] = {r.pid.x, r.pid.y, r.pid.z, r.pid.w};
-    const uint32_t nn[4] = {mn.x, mn.y, mn.z, mn.w};
-    double nv[4] = {0.0, 0.0, 0.0, 0.0};
-    uint32_t gone = 0;  // old corners the new cell does not have
+__device__ __forceinline__ void carryPending(FwdRay& r, int bf, int fe, uint4 mn, uint32_t Np, Flush&& flush) {
+    if ((r.pid.x >= Np) == (mn.x >= Np)) {
+        const double s0 = bf == 0 ? r.pv[1] : r.pv[0];
+        const double s1 = bf <= 1 ? r.pv[2] : r.pv[1];
+        const double s2 = bf <= 2 ? r.pv[3] : r.pv[2];
+        const double v = bf == 0 ? r.pv[0] : bf == 1 ? r.pv[1] : bf == 2 ? r.pv[2] : r.pv[3];
+        const uint32_t id = bf == 0 ? r.pid.x : bf == 1 ? r.pid.y : bf == 2 ? r.pid.z : r.pid.w;
+        r.pv[0] = fe == 0 ? 0.0 : s0;
+        r.pv[1] = fe == 1 ? 0.0 : fe == 0 ? s0 : s1;
+        r.pv[2] = fe == 2 ? 0.0 : fe < 2 ? s1 : s2;
+        r.pv[3] = fe == 3 ? 0.0 : s2;
+        if (v != 0.0) flush(id, v);
+    } else {
+        const uint32_t o[4] = {r.pid.x, r.pid.y, r.pid.z, r.pid.w};
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        bool kept = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (o[j] == nn[k]) {
-                nv[k] = r.pv[j];
-                kept = true;
-            }
-        gone |= kept ? 0u : 1u << j;
+        for (int j = 0; j < 4; ++j) {
+            if (r.pv[j] != 0.0) flush(o[j], r.pv[j]);
+            r.pv[j] = 0.0;
+        }
     }
-    // a crossing inside one material drops exactly one corner: one flush site
-    // for all lanes; a change of material (gain <-> cladding) drops all four
-    const int j0 = __ffs(gone) - 1;
-    const double v0 = j0 == 0 ? r.pv[0] : j0 == 1 ? r.pv[1] : j0 == 2 ? r.pv[2] : r.pv[3];
-    const uint32_t id0 = j0 == 0 ? o[0] : j0 == 1 ? o[1] : j0 == 2 ? o[2] : o[3];
-    if (v0 != 0.0) flush(id0, v0);
-    const uint32_t rest = gone & (gone - 1);
-    if (rest) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (((rest >> j) & 1u) && r.pv[j] != 0.0) flush(o[j], r.pv[j]);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) r.pv[k] = nv[k];
     r.pid = mn;
 }
 
@@ -256,6 +254,7 @@ __device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, ui
     const Philox4 o2 = philox4x32_10(ray, L.launch, 1u, kTagFwdRay, L.seed, kFwdKeyHi);
     const double e0 = -log(unit53(o.x)), e1 = -log(unit53(o.y)), e2 = -log(unit53(o.z)), e3 = -log(unit53(o.w));
     const double esum = e0 + e1 + e2 + e3;
+    // exponential k goes to sorted corner k (ascending point index)
     const CellLinks lk = ldLinks(&m.cell[c].nbr);
     const uint4 mv = lk.matv;
     const uint32_t off = mv.x >= m.Np ? m.Np : 0u;
@@ -362,7 +361,7 @@ __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const F
             r.ff = n & 3;
             const CellLinks lk = ldLinks(&m.cell[r.c].nbr);
             r.nbr = lk.nbr;
-            carryPending(r, lk.matv, add);
+            carryPending(r, bf, r.ff, lk.matv, m.Np, add);
         }
     }
     if (SMEM) {
@@ -614,6 +613,7 @@ struct hase_tet_context {
     std::vector<uint32_t> cladTypes;
     std::vector<double> vol, sigmaA, sigmaE;
     DevBuf<TetCell> cell;
+    std::vector<uint8_t> sortedCorner;  // [C][4]: caller's corner index of sorted corner k
     DevBuf<uint32_t> guide;
     uint32_t K = 1;
     double guideScale = 0.0;
@@ -752,11 +752,34 @@ hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spec
         return cleanup(fail(HASE_CUDA_ERROR, "stream/event creation failed"));
     const size_t C = c->C, Np = c->Np;
     hase_status st = HASE_OK;
+    // corner-sorted records: sorted corner k is the caller's corner srt[k];
+    // the face opposite it keeps its plane, its neighbour gets the
+    // neighbour's sorted face index
+    c->sortedCorner.resize(4 * C);
+    std::vector<uint8_t> inv(4 * C);
+    for (size_t k = 0; k < C; ++k) {
+        uint8_t srt[4] = {0, 1, 2, 3};
+        const uint32_t* v = d->cells + 4 * k;
+        std::sort(srt, srt + 4, [&](uint8_t a, uint8_t b) { return v[a] < v[b]; });
+        for (int j = 0; j < 4; ++j) {
+            c->sortedCorner[4 * k + j] = srt[j];
+            inv[4 * k + srt[j]] = uint8_t(j);
+        }
+    }
     std::vector<TetCell> rec(C);
     for (size_t k = 0; k < C; ++k) {
-        for (int f = 1; f < 4; ++f) rec[k].plane[f - 1] = h.plane[4 * k + f];
-        rec[k].nbr = make_int4(h.nbr[4 * k], h.nbr[4 * k + 1], h.nbr[4 * k + 2], h.nbr[4 * k + 3]);
-        rec[k].matv = h.matv[k];
+        const uint8_t* srt = &c->sortedCorner[4 * k];
+        for (int j = 1; j < 4; ++j) rec[k].plane[j - 1] = h.plane[4 * k + srt[j]];
+        int n4[4];
+        uint32_t mv[4];
+        const uint32_t hm[4] = {h.matv[k].x, h.matv[k].y, h.matv[k].z, h.matv[k].w};
+        for (int j = 0; j < 4; ++j) {
+            const int id = h.nbr[4 * k + srt[j]];
+            n4[j] = id < 0 ? -1 : int((uint32_t(id) >> 2) << 2 | inv[4 * (size_t(id) >> 2) + (id & 3)]);
+            mv[j] = hm[srt[j]];
+        }
+        rec[k].nbr = make_int4(n4[0], n4[1], n4[2], n4[3]);
+        rec[k].matv = make_uint4(mv[0], mv[1], mv[2], mv[3]);
     }
     if ((st = upload(c->cell, rec.data(), C, c->stream)) != HASE_OK ||
         (st = upload(c->points, d->points, 3 * Np, c->stream)) != HASE_OK ||
@@ -804,11 +827,13 @@ hase_status hase_tet_tables(hase_tet_context* c, int32_t* neighbors, int32_t* ne
         const double4 q0 = make_double4(-(q1.x + q2.x + q3.x), -(q1.y + q2.y + q3.y), -(q1.z + q2.z + q3.z),
                                         1.0 - (q1.w + q2.w + q3.w));
         const double4 q[4] = {q0, q1, q2, q3};
-        for (int f = 0; f < 4; ++f) {
-            if (neighbors) neighbors[4 * k + f] = n4[f] < 0 ? -1 : n4[f] >> 2;
-            if (neighborFace) neighborFace[4 * k + f] = n4[f] < 0 ? -1 : n4[f] & 3;
+        for (int j = 0; j < 4; ++j) {
+            const int f = c->sortedCorner[4 * k + j];  // the caller's face index of sorted face j
+            const int n = n4[j] < 0 ? -1 : n4[j] >> 2;
+            if (neighbors) neighbors[4 * k + f] = n;
+            if (neighborFace) neighborFace[4 * k + f] = n < 0 ? -1 : c->sortedCorner[4 * size_t(n) + (n4[j] & 3)];
             if (planes) {
-                const double4 p = q[f];
+                const double4 p = q[j];
                 planes[16 * k + 4 * f] = p.x;
                 planes[16 * k + 4 * f + 1] = p.y;
                 planes[16 * k + 4 * f + 2] = p.z;

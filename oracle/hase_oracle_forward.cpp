@@ -6,7 +6,8 @@
 //   source rays   include/kernels/forward/accumulation.hpp:369-453,
 //                 include/kernels/forward/volumeSampling.hpp:19-161
 //                 (stratified beta*V CDF per statistical batch, uniform point
-//                 in the tet from four exponentials, isotropic direction,
+//                 in the tet from four exponentials paired with the corners
+//                 in ascending point index, isotropic direction,
 //                 stratified wavelength bin)
 //   walk + tally  include/kernels/forward/rayWalk.hpp:106-208,
 //                 include/kernels/forward/accumulation.hpp:300-352
@@ -309,9 +310,13 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
                     philoxFwd(r, launch, 1u, kTagFwdRay, ex->seed, o2);
                     double e[4], esum = 0.0;
                     for (int k = 0; k < 4; ++k) { e[k] = -std::log(unit(o[k])); esum += e[k]; }
+                    // exponential k goes to the corner of k-th smallest point index
+                    uint32_t v[4];
+                    for (int k = 0; k < 4; ++k) v[k] = m->cells[4 * size_t(c) + k];
+                    std::sort(v, v + 4);
                     double x[3] = {0.0, 0.0, 0.0};
                     for (int k = 0; k < 4; ++k) {
-                        const double* p = m->points + 3 * size_t(m->cells[4 * size_t(c) + k]);
+                        const double* p = m->points + 3 * size_t(v[k]);
                         for (int d = 0; d < 3; ++d) x[d] += e[k] / esum * p[d];
                     }
                     const double z = 2.0 * unit(o2[0]) - 1.0, phi = 2.0 * kPi * unit(o2[1]);

@@ -56,7 +56,10 @@ def test_device_tables_equal_oracle_tables(oracle, name):
         dev = ctx.tables()
     np.testing.assert_array_equal(dev["neighbors"], ref["neighbors"])
     np.testing.assert_array_equal(dev["neighborFace"], ref["neighborFace"])
-    np.testing.assert_array_equal(dev["planes"][:, :, :3], ref["gradients"])
+    # the device keeps three planes per cell and rebuilds the fourth as
+    # 1 - (sum of the others): equal to rounding
+    scale = np.abs(ref["gradients"]).max()
+    np.testing.assert_allclose(dev["planes"][:, :, :3], ref["gradients"], rtol=1e-12, atol=1e-12 * scale)
     np.testing.assert_array_equal(dev["volumes"], ref["volumes"])
 
 
