@@ -45,7 +45,8 @@ SMS = 148
 LANES_PER_SM = 128
 FWD_METRIC = "forward Tet4 phi-ASE source rays traced and tallied per second on 1 B200 (crossings/s alongside)"
 FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count of the forward walk
-BYTES_PER_TET_CROSSING = 192       # gathered 156 B (planes 128, neighbour 4, corners 16, beta 8) + tallies 36 B
+BYTES_PER_TET_CROSSING = 148       # cell record 128 B + beta 8 B + one vertex tally 8 B + one visit count 4 B
+FWD_TRAFFIC_DISC_POLY = 49128192   # DRAM bytes of one fwdRayKernel launch on the disc_poly Tet4 twin (ncu)
 FP64_LANES_PER_SM = 64
 
 
@@ -428,7 +429,9 @@ def measure_forward(args, local, rank=0, world=1, cpu_seconds=None):
         "gpu_launches": launches,
         "roofline": {"bound": "fp64_issue" if r_fp64 <= r_l2 else "l2_gather", "kernel": "fwdRayKernel",
                      "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
-                     "traffic": None, "fp64_issue_peak": r_fp64, "l2_gather_peak": r_l2, "l2_read_gbs_live": l2,
+                     "traffic": FWD_TRAFFIC_DISC_POLY if w.name == "disc_poly" else None,
+                     "traffic_note": "resident tables read once per launch; independent of the ray count",
+                     "fp64_issue_peak": r_fp64, "l2_gather_peak": r_l2, "l2_read_gbs_live": l2,
                      "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
         "clocks": clocks,
     }
