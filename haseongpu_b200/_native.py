@@ -1,5 +1,5 @@
-"""ctypes binding of libhase_b200.so (the C ABI declared in include/hase_b200.h
-and include/hase_b200_forward.h).
+"""ctypes binding of libhase_b200.so (the C ABI declared in include/hase_b200.h,
+include/hase_b200_forward.h and include/hase_b200_proposal.h).
 
 The shared library is built in-tree (``haseongpu_b200/libhase_b200.so``) by
 ``haseongpu_b200.build.build_library()``.  There is no CPU fallback: every
@@ -50,7 +50,15 @@ EXPORTED_SYMBOLS = (
     "hase_tet_context_destroy",
     "hase_tet_tables",
     "hase_tet_trace",
+    # include/hase_b200_proposal.h
+    "hase_proposal_create",
+    "hase_proposal_destroy",
+    "hase_proposal_get_params",
+    "hase_proposal_set_params",
+    "hase_proposal_forward",
 )
+PROPOSAL_FEATURES = 12
+PROPOSAL_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 
 _u32p = C.POINTER(C.c_uint32)
 _u64p = C.POINTER(C.c_uint64)
@@ -223,6 +231,11 @@ def lib():
         L.hase_tet_tables.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _f64p]
         L.hase_tet_trace.argtypes = [C.c_void_p, C.c_uint32, _u32p, _f64p, _f64p, C.c_uint32, C.c_uint32, _u32p,
                                      _u32p, _f64p, _f64p, _f64p, _i32p]
+        L.hase_proposal_create.argtypes = [C.c_int, C.c_uint32, C.POINTER(C.c_void_p)]
+        L.hase_proposal_destroy.argtypes = [C.c_void_p]
+        L.hase_proposal_get_params.argtypes = [C.c_void_p, _f32p]
+        L.hase_proposal_set_params.argtypes = [C.c_void_p, _f32p]
+        L.hase_proposal_forward.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

@@ -8,9 +8,11 @@ from pathlib import Path
 
 PACKAGE_DIR = Path(__file__).resolve().parent
 REPO_ROOT = PACKAGE_DIR.parent
-SOURCES = [PACKAGE_DIR / "csrc" / "hase_b200.cu", PACKAGE_DIR / "csrc" / "hase_forward.cu"]
+SOURCES = [PACKAGE_DIR / "csrc" / "hase_b200.cu", PACKAGE_DIR / "csrc" / "hase_forward.cu",
+           PACKAGE_DIR / "csrc" / "hase_proposal.cu"]
 HEADERS = [PACKAGE_DIR / "csrc" / "hase_device.cuh", PACKAGE_DIR / "csrc" / "hase_host.cuh",
-           REPO_ROOT / "include" / "hase_b200.h", REPO_ROOT / "include" / "hase_b200_forward.h"]
+           REPO_ROOT / "include" / "hase_b200.h", REPO_ROOT / "include" / "hase_b200_forward.h",
+           REPO_ROOT / "include" / "hase_b200_proposal.h"]
 LIB_PATH = PACKAGE_DIR / "libhase_b200.so"
 
 NVCC_FLAGS = [

@@ -1,0 +1,61 @@
+/*
+ * hase_b200_proposal.h -- the learned importance proposal of libhase_b200.so:
+ * a small MLP that scores every (sample point, reflection slice, prism) pair,
+ * trained on the GPU from the per-prism gain contributions that the
+ * importance-sampled method logs, and used as the ray->prism proposal of
+ * hase_calc_phi_ase_learned.  No counterpart in the reference (HASEonGPU's
+ * importance distribution is the straight-line gain estimate of
+ * hase_importance_weights); the estimator stays unbiased because every prism
+ * with beta > 0 keeps a positive probability (a defensive mixture with the
+ * beta V / d^2 prior) and each ray is weighted by the inverse probability of
+ * the proposal actually used.
+ *
+ * Network: 12 inputs -> 64 -> 64 -> 64 (SiLU) -> 1 logit; BF16 weights and
+ * activations on the tensor cores (tcgen05, FP32 accumulation in tensor
+ * memory), FP32 biases and output layer.  Per sample point the logits of all
+ * (slice, prism) pairs go through a softmax.
+ *
+ * Parameters (FP32 master copy, HASE_PROPOSAL_PARAMS floats, row-major):
+ *   W1[12][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4[1]
+ * (W[in][out]; the device rounds W1..W3 and w4 to BF16).
+ *
+ * Features of a pair (sample s, image point s_j of slice j, prism p with
+ * centre c, volume V, excited fraction beta), R = radius of the mesh,
+ * H = height of the medium:
+ *   0..2  s / (R, R, H)            3..5  (c - s_j) / (R, R, H)
+ *   6     ln(|c - s_j| / R)        7     beta
+ *   8     estimated ln gain along c -> s_j (a coarse column-averaged gain
+ *         field sampled at 8 points, reflections folded)
+ *   9     ln(beta V / |c - s_j|^2) - ln(V_mean / R^2)   (0 when beta = 0)
+ *   10    slice index / 4          11    ln(sigma_e / sigma_a) of the
+ *                                        spectrally averaged gain
+ */
+#ifndef HASE_B200_PROPOSAL_H
+#define HASE_B200_PROPOSAL_H
+
+#include "hase_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HASE_PROPOSAL_FEATURES 12
+#define HASE_PROPOSAL_HIDDEN 64
+#define HASE_PROPOSAL_PARAMS (12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
+
+typedef struct hase_proposal hase_proposal;
+
+/* A network on `device` with seeded uniform fan-in initialisation. */
+hase_status hase_proposal_create(int device, uint32_t seed, hase_proposal** out);
+hase_status hase_proposal_destroy(hase_proposal* net);
+hase_status hase_proposal_get_params(hase_proposal* net, float* params);
+hase_status hase_proposal_set_params(hase_proposal* net, const float* params);
+
+/* Logits of `rows` explicit feature rows (host arrays [rows][12] -> [rows]). */
+hase_status hase_proposal_forward(hase_proposal* net, uint32_t rows, const float* features, float* logits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HASE_B200_PROPOSAL_H */
