@@ -56,6 +56,8 @@ EXPORTED_SYMBOLS = (
     "hase_proposal_get_params",
     "hase_proposal_set_params",
     "hase_proposal_forward",
+    "hase_proposal_loss_grad",
+    "hase_proposal_train",
 )
 PROPOSAL_FEATURES = 12
 PROPOSAL_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -182,6 +184,27 @@ class ForwardResultDesc(C.Structure):
     ]
 
 
+class ProposalBatch(C.Structure):
+    _fields_ = [
+        ("groups", C.c_uint32),
+        ("offsets", _u32p),
+        ("features", _f32p),
+        ("targets", _f32p),
+        ("groupWeights", _f32p),
+    ]
+
+
+class ProposalTrainDesc(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint32),
+        ("groupsPerStep", C.c_uint32),
+        ("learningRate", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("epsilon", C.c_float),
+    ]
+
+
 class HaseError(RuntimeError):
     """A libhase_b200 call failed; ``status`` is the hase_status code."""
 
@@ -236,6 +259,8 @@ def lib():
         L.hase_proposal_get_params.argtypes = [C.c_void_p, _f32p]
         L.hase_proposal_set_params.argtypes = [C.c_void_p, _f32p]
         L.hase_proposal_forward.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
+        L.hase_proposal_loss_grad.argtypes = [C.c_void_p, C.POINTER(ProposalBatch), _f32p, _f32p]
+        L.hase_proposal_train.argtypes = [C.c_void_p, C.POINTER(ProposalBatch), C.POINTER(ProposalTrainDesc), _f32p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

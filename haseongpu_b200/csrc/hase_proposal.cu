@@ -51,12 +51,17 @@ static_assert(kOffB4 + 1 == HASE_PROPOSAL_PARAMS, "parameter layout");
 // shared-memory images (bytes)
 constexpr uint32_t kW1Bytes = kHid * kIn * 2;    // [64 n][16 k]
 constexpr uint32_t kW2Bytes = kHid * kHid * 2;   // [64 n][64 k]
-constexpr uint32_t kWBlobBytes = kW1Bytes + 2 * kW2Bytes;
+constexpr uint32_t kWFwdBytes = kW1Bytes + 2 * kW2Bytes;   // W1^T W2^T W3^T (forward)
+constexpr uint32_t kWBlobBytes = kWFwdBytes + 2 * kW2Bytes;  // + W2, W3 untransposed (backward)
 constexpr uint32_t kA0Bytes = kTile * kIn * 2;
 constexpr uint32_t kA1Bytes = kTile * kHid * 2;
 constexpr int kVecFloats = 4 * kHid + 1;          // b1 b2 b3 w4 b4
 
+// Inference: forward weight images, one activation buffer per layer input,
+// 64 TMEM columns (one accumulator reused by the three layers).
 struct SmemMap {
+    static constexpr uint32_t wBytes = kWFwdBytes;
+    static constexpr uint32_t tmemCols = 64;
     static constexpr uint32_t w1 = 0;
     static constexpr uint32_t w2 = w1 + kW1Bytes;
     static constexpr uint32_t w3 = w2 + kW2Bytes;
@@ -69,6 +74,32 @@ struct SmemMap {
     static constexpr uint32_t bytes = tslot + 8;
 };
 constexpr uint32_t kSmemBytes = SmemMap::bytes + 1024;  // + alignment slack
+
+// Training: also the backward weight images (W2, W3 as [in][out]: the B
+// operands of dz2 W2^T and dz3 W3^T), dz as the bf16 A operand and in f32 for
+// the weight-gradient reductions, and 256 TMEM columns: the three layer
+// accumulators side by side (0, 64, 128) and the backward products (192).
+struct TrainSmem {
+    static constexpr uint32_t wBytes = kWBlobBytes;
+    static constexpr uint32_t tmemCols = 256;
+    static constexpr uint32_t w1 = 0;
+    static constexpr uint32_t w2 = w1 + kW1Bytes;
+    static constexpr uint32_t w3 = w2 + kW2Bytes;
+    static constexpr uint32_t w2b = w3 + kW2Bytes;
+    static constexpr uint32_t w3b = w2b + kW2Bytes;
+    static constexpr uint32_t a0 = w3b + kW2Bytes;
+    static constexpr uint32_t a1 = a0 + kA0Bytes;
+    static constexpr uint32_t a2 = a1 + kA1Bytes;
+    static constexpr uint32_t dzb = a2 + kA1Bytes;
+    static constexpr uint32_t dzf = dzb + kA1Bytes;
+    static constexpr uint32_t dls = dzf + kTile * kHid * 4;
+    static constexpr uint32_t vec = dls + kTile * 4;
+    static constexpr uint32_t bar = (vec + kVecFloats * 4 + 15) & ~15u;
+    static constexpr uint32_t tslot = bar + 8;
+    static constexpr uint32_t bytes = tslot + 8;
+};
+constexpr uint32_t kTrainSmemBytes = TrainSmem::bytes + 1024;
+static_assert(SmemMap::w3 == TrainSmem::w3, "the forward images lead the weight blob in both maps");
 
 __host__ __device__ constexpr uint32_t canonOffset(uint32_t r, uint32_t k, uint32_t K) {
     return (r >> 3) * (K * 16u) + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
@@ -146,40 +177,51 @@ struct Tile {
     bool ok;            // false after a timed-out wait
 };
 
-// Reads this thread's row of the accumulator (64 f32 columns).
-__device__ __forceinline__ void loadRow(const Tile& T, float (&acc)[kHid]) {
+// Reads this thread's row of the accumulator at TMEM column `col` (64 f32 columns).
+__device__ __forceinline__ void loadRow(const Tile& T, uint32_t col, float (&acc)[kHid]) {
     const uint32_t lane0 = (threadIdx.x & ~31u) << 16;
 #pragma unroll
     for (int q = 0; q < kHid / 16; ++q) {
         uint32_t r[16];
-        tmemLd16(T.tmem + lane0 + uint32_t(16 * q), r);
+        tmemLd16(T.tmem + lane0 + col + uint32_t(16 * q), r);
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[16 * q + j] = __uint_as_float(r[j]);
     }
 }
 
-// Issues the MMAs of one layer (K = kIn or kHid) from thread 0 and waits for them.
-__device__ __forceinline__ void runLayer(Tile& T, uint32_t aOff, uint32_t wOff, uint32_t K) {
+// Issues the MMAs of one product [128 x K] x [64 x K]^T (K = kIn or kHid)
+// into TMEM column `col` from thread 0 and commits them to the mbarrier.
+__device__ __forceinline__ void issueLayer(Tile& T, uint32_t aOff, uint32_t wOff, uint32_t K, uint32_t col,
+                                           uint32_t barOff) {
     if (threadIdx.x == 0) {
         fenceAfterSync();
         const uint32_t sbo = K * 16u;
         for (uint32_t kk = 0; kk < K / 16u; ++kk) {
             const uint64_t a = smemDesc(T.sbase + aOff + kk * 256u, 128u, sbo);
             const uint64_t b = smemDesc(T.sbase + wOff + kk * 256u, 128u, sbo);
-            mmaBf16(T.tmem, a, b, kk > 0 ? 1u : 0u);
+            mmaBf16(T.tmem + col, a, b, kk > 0 ? 1u : 0u);
         }
-        mmaCommit(T.sbase + SmemMap::bar);
+        mmaCommit(T.sbase + barOff);
     }
-    if (!mbarWait(T.sbase + SmemMap::bar, T.parity)) T.ok = false;
+}
+
+__device__ __forceinline__ void waitLayer(Tile& T, uint32_t barOff) {
+    if (!mbarWait(T.sbase + barOff, T.parity)) T.ok = false;
     T.parity ^= 1u;
     fenceAfterSync();
 }
 
+__device__ __forceinline__ void runLayer(Tile& T, uint32_t aOff, uint32_t wOff, uint32_t K, uint32_t col,
+                                         uint32_t barOff) {
+    issueLayer(T, aOff, wOff, K, col, barOff);
+    waitLayer(T, barOff);
+}
+
 // Bias + SiLU of the accumulator row, stored as bf16 row `threadIdx.x` of the
 // next layer's A operand (K = 64).
-__device__ __forceinline__ void epilogueToSmem(Tile& T, const float* bias, uint32_t outOff) {
+__device__ __forceinline__ void epilogueToSmem(Tile& T, uint32_t col, const float* bias, uint32_t outOff) {
     float acc[kHid];
-    loadRow(T, acc);
+    loadRow(T, col, acc);
     const uint32_t t = threadIdx.x;
     uint8_t* out = T.base + outOff + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
 #pragma unroll
@@ -197,9 +239,9 @@ __device__ __forceinline__ void epilogueToSmem(Tile& T, const float* bias, uint3
 }
 
 // Writes this thread's feature row (kFeat floats, padded to 16) into A0.
-__device__ __forceinline__ void storeFeatures(Tile& T, const float (&f)[kFeat]) {
+__device__ __forceinline__ void storeFeatures(Tile& T, uint32_t a0Off, const float (&f)[kFeat]) {
     const uint32_t t = threadIdx.x;
-    uint8_t* out = T.base + SmemMap::a0 + (t >> 3) * (kIn * 16u) + (t & 7u) * 16u;
+    uint8_t* out = T.base + a0Off + (t >> 3) * (kIn * 16u) + (t & 7u) * 16u;
     uint4 v0, v1;
     v0.x = packBf16(f[0], f[1]);
     v0.y = packBf16(f[2], f[3]);
@@ -218,13 +260,13 @@ __device__ __forceinline__ void storeFeatures(Tile& T, const float (&f)[kFeat]) 
 // The three tensor-core layers and the output layer for the rows in A0.
 __device__ __forceinline__ float mlpTile(Tile& T) {
     const float* vec = reinterpret_cast<const float*>(T.base + SmemMap::vec);
-    runLayer(T, SmemMap::a0, SmemMap::w1, kIn);
-    epilogueToSmem(T, vec, SmemMap::a1);
-    runLayer(T, SmemMap::a1, SmemMap::w2, kHid);
-    epilogueToSmem(T, vec + kHid, SmemMap::a2);
-    runLayer(T, SmemMap::a2, SmemMap::w3, kHid);
+    runLayer(T, SmemMap::a0, SmemMap::w1, kIn, 0, SmemMap::bar);
+    epilogueToSmem(T, 0, vec, SmemMap::a1);
+    runLayer(T, SmemMap::a1, SmemMap::w2, kHid, 0, SmemMap::bar);
+    epilogueToSmem(T, 0, vec + kHid, SmemMap::a2);
+    runLayer(T, SmemMap::a2, SmemMap::w3, kHid, 0, SmemMap::bar);
     float acc[kHid];
-    loadRow(T, acc);
+    loadRow(T, 0, acc);
     const float* b3 = vec + 2 * kHid;
     const float* w4 = vec + 3 * kHid;
     float logit = vec[4 * kHid];
@@ -236,6 +278,7 @@ __device__ __forceinline__ float mlpTile(Tile& T) {
 }
 
 // CTA prologue: smem map, weight images, TMEM and the mbarrier.
+template <typename Map>
 __device__ __forceinline__ bool tileBegin(Tile& T, uint8_t* dyn, const uint4* wimg, const float* vec) {
     const uint32_t raw = smemU32(dyn);
     const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
@@ -244,32 +287,33 @@ __device__ __forceinline__ bool tileBegin(Tile& T, uint8_t* dyn, const uint4* wi
     T.parity = 0;
     T.ok = true;
     uint4* w = reinterpret_cast<uint4*>(T.base + SmemMap::w1);
-    for (uint32_t k = threadIdx.x; k < kWBlobBytes / 16u; k += blockDim.x) w[k] = wimg[k];
-    float* v = reinterpret_cast<float*>(T.base + SmemMap::vec);
+    for (uint32_t k = threadIdx.x; k < Map::wBytes / 16u; k += blockDim.x) w[k] = wimg[k];
+    float* v = reinterpret_cast<float*>(T.base + Map::vec);
     for (uint32_t k = threadIdx.x; k < uint32_t(kVecFloats); k += blockDim.x) v[k] = vec[k];
     if (threadIdx.x < 32) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(T.sbase + SmemMap::tslot),
-                     "r"(uint32_t(kHid)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(T.sbase + Map::tslot),
+                     "r"(Map::tmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(T.sbase + SmemMap::bar), "r"(1u));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(T.sbase + Map::bar), "r"(1u));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fenceProxyAsync();
     fenceBeforeSync();
     __syncthreads();
     fenceAfterSync();
-    T.tmem = *reinterpret_cast<volatile uint32_t*>(T.base + SmemMap::tslot);
+    T.tmem = *reinterpret_cast<volatile uint32_t*>(T.base + Map::tslot);
     return true;
 }
 
+template <typename Map>
 __device__ __forceinline__ void tileEnd(Tile& T, int* error) {
     fenceBeforeSync();
     __syncthreads();
     if (threadIdx.x < 32) {
         fenceAfterSync();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(T.tmem), "r"(uint32_t(kHid)));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(T.tmem), "r"(Map::tmemCols));
     }
     if (!T.ok && threadIdx.x == 0) atomicExch(error, 1);
 }
@@ -287,20 +331,312 @@ struct ForwardLaunch {
 __global__ void __launch_bounds__(kTile, 1) mlpForwardKernel(const ForwardLaunch P) {
     extern __shared__ uint8_t dynSmem[];
     Tile T;
-    tileBegin(T, dynSmem, P.wimg, P.vec);
+    tileBegin<SmemMap>(T, dynSmem, P.wimg, P.vec);
     const uint32_t tiles = (P.rows + kTile - 1) / kTile;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t row = tile * kTile + threadIdx.x;
         float f[kFeat];
 #pragma unroll
         for (int j = 0; j < kFeat; ++j) f[j] = row < P.rows ? P.features[size_t(row) * kFeat + j] : 0.0f;
-        storeFeatures(T, f);
+        storeFeatures(T, SmemMap::a0, f);
         const float logit = mlpTile(T);
         if (row < P.rows) P.logits[row] = logit;
         if (!__syncthreads_and(T.ok)) break;
     }
-    tileEnd(T, P.error);
+    tileEnd<SmemMap>(T, P.error);
 }
+
+}  // namespace
+
+// ------------------------------------------------------------- training ----
+namespace {
+
+__device__ __forceinline__ float dsilu(float z) {
+    const float sg = 1.0f / (1.0f + __expf(-z));
+    return sg * (1.0f + z * (1.0f - sg));
+}
+
+// g[j] += sum over the tile's rows r of h[r][i0 + j] * dz[r][o] (j < 32) and
+// gb += sum_r dz[r][o]: h bf16 in the canonical layout (K = 64) at hOff, dz
+// f32 [128][64] at dzOff.  Every lane of a warp reads the same h (broadcast).
+__device__ __forceinline__ void accumulateGrad64(const Tile& T, uint32_t hOff, uint32_t dzOff, uint32_t o,
+                                                 uint32_t ih, float (&g)[32], float& gb) {
+    const float* dz = reinterpret_cast<const float*>(T.base + dzOff);
+    for (uint32_t r = 0; r < uint32_t(kTile); ++r) {
+        const float d = dz[r * kHid + o];
+        const uint8_t* hp = T.base + hOff + (r >> 3) * (kHid * 16u) + (r & 7u) * 16u;
+#pragma unroll
+        for (uint32_t cc = 0; cc < 4; ++cc) {
+            const uint4 v = *reinterpret_cast<const uint4*>(hp + (4u * ih + cc) * 128u);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                g[8 * cc + 2 * e] = fmaf(__uint_as_float(w[e] << 16), d, g[8 * cc + 2 * e]);
+                g[8 * cc + 2 * e + 1] = fmaf(__uint_as_float(w[e] & 0xFFFF0000u), d, g[8 * cc + 2 * e + 1]);
+            }
+        }
+        gb += d;
+    }
+}
+
+struct TrainLaunch {
+    const uint4* wimg;      // forward + backward images
+    const float* vec;
+    const float* features;  // [rows][kFeat]
+    const float* dl;        // [rows]: dLoss / dlogit
+    uint32_t rows;
+    float* grad;            // [HASE_PROPOSAL_PARAMS], accumulated
+    int* error;
+};
+
+// Recomputes the forward pass of each tile (layer accumulators kept in TMEM
+// columns 0 / 64 / 128) and back-propagates dL/dlogit: the products
+// dz3 W3^T and dz2 W2^T on the tensor cores (TMEM column 192), the weight
+// and bias gradients as FP32 reductions over the tile's rows on the CUDA
+// cores, per-thread across tiles, added to `grad` once per CTA.
+__global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch P) {
+    extern __shared__ uint8_t dynSmem[];
+    Tile T;
+    tileBegin<TrainSmem>(T, dynSmem, P.wimg, P.vec);
+    const uint32_t t = threadIdx.x, o = t & 63u, ih = t >> 6;
+    const float* vec = reinterpret_cast<const float*>(T.base + TrainSmem::vec);
+    const float *b1 = vec, *b2 = vec + kHid, *b3 = vec + 2 * kHid, *w4 = vec + 3 * kHid;
+    float* dzf = reinterpret_cast<float*>(T.base + TrainSmem::dzf);
+    float* dls = reinterpret_cast<float*>(T.base + TrainSmem::dls);
+    float gW3[32], gW2[32], gW1[6];
+    for (int j = 0; j < 32; ++j) gW3[j] = gW2[j] = 0.0f;
+    for (int j = 0; j < 6; ++j) gW1[j] = 0.0f;
+    float gb1 = 0.0f, gb2 = 0.0f, gb3 = 0.0f, gw4 = 0.0f, gb4 = 0.0f;
+    const uint32_t tiles = (P.rows + kTile - 1) / kTile;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t row = tile * kTile + t;
+        float f[kFeat];
+#pragma unroll
+        for (int j = 0; j < kFeat; ++j) f[j] = row < P.rows ? P.features[size_t(row) * kFeat + j] : 0.0f;
+        const float dl = row < P.rows ? P.dl[row] : 0.0f;
+        storeFeatures(T, TrainSmem::a0, f);
+        runLayer(T, TrainSmem::a0, TrainSmem::w1, kIn, 0, TrainSmem::bar);
+        epilogueToSmem(T, 0, b1, TrainSmem::a1);
+        runLayer(T, TrainSmem::a1, TrainSmem::w2, kHid, 64, TrainSmem::bar);
+        epilogueToSmem(T, 64, b2, TrainSmem::a2);
+        runLayer(T, TrainSmem::a2, TrainSmem::w3, kHid, 128, TrainSmem::bar);
+        // output layer: g_w4 = sum_r h3 dl, g_b4 = sum_r dl
+        {
+            float z[kHid];
+            loadRow(T, 128, z);
+            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = silu(z[n] + b3[n]) * dl;
+            dls[t] = dl;
+        }
+        __syncthreads();
+        if (ih == 0) {
+            float sum = 0.0f;
+            for (uint32_t r = 0; r < uint32_t(kTile); ++r) sum += dzf[r * kHid + o];
+            gw4 += sum;
+        }
+        if (t == 0)
+            for (uint32_t r = 0; r < uint32_t(kTile); ++r) gb4 += dls[r];
+        __syncthreads();
+        // dz3 = dl w4 * silu'(z3)
+        {
+            float z[kHid];
+            loadRow(T, 128, z);
+            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
+#pragma unroll
+            for (int c = 0; c < kHid / 8; ++c) {
+                float d[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const int n = 8 * c + e;
+                    d[e] = dl * w4[n] * dsilu(z[n] + b3[n]);
+                    dzf[t * kHid + n] = d[e];
+                }
+                uint4 v;
+                v.x = packBf16(d[0], d[1]);
+                v.y = packBf16(d[2], d[3]);
+                v.z = packBf16(d[4], d[5]);
+                v.w = packBf16(d[6], d[7]);
+                *reinterpret_cast<uint4*>(out + c * 128u) = v;
+            }
+        }
+        fenceBeforeSync();
+        fenceProxyAsync();
+        __syncthreads();
+        // dh2 = dz3 W3^T on the tensor cores while the CUDA cores reduce g_W3
+        issueLayer(T, TrainSmem::dzb, TrainSmem::w3b, kHid, 192, TrainSmem::bar);
+        {
+            float gb = 0.0f;
+            accumulateGrad64(T, TrainSmem::a2, TrainSmem::dzf, o, ih, gW3, gb);
+            if (ih == 0) gb3 += gb;
+        }
+        waitLayer(T, TrainSmem::bar);
+        float dh[kHid];
+        loadRow(T, 192, dh);
+        {
+            float z[kHid];
+            loadRow(T, 64, z);
+            for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b2[n]);
+        }
+        fenceBeforeSync();
+        __syncthreads();  // g_W3 reads of dzf done; TMEM column 192 read
+        {
+            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
+#pragma unroll
+            for (int c = 0; c < kHid / 8; ++c) {
+                uint4 v;
+                v.x = packBf16(dh[8 * c + 0], dh[8 * c + 1]);
+                v.y = packBf16(dh[8 * c + 2], dh[8 * c + 3]);
+                v.z = packBf16(dh[8 * c + 4], dh[8 * c + 5]);
+                v.w = packBf16(dh[8 * c + 6], dh[8 * c + 7]);
+                *reinterpret_cast<uint4*>(out + c * 128u) = v;
+            }
+            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
+        }
+        fenceProxyAsync();
+        __syncthreads();
+        // dh1 = dz2 W2^T while the CUDA cores reduce g_W2
+        issueLayer(T, TrainSmem::dzb, TrainSmem::w2b, kHid, 192, TrainSmem::bar);
+        {
+            float gb = 0.0f;
+            accumulateGrad64(T, TrainSmem::a1, TrainSmem::dzf, o, ih, gW2, gb);
+            if (ih == 0) gb2 += gb;
+        }
+        waitLayer(T, TrainSmem::bar);
+        loadRow(T, 192, dh);
+        {
+            float z[kHid];
+            loadRow(T, 0, z);
+            for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b1[n]);
+        }
+        fenceBeforeSync();
+        __syncthreads();
+        for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
+        __syncthreads();
+        // g_W1 from the bf16 features in A0 (inputs 6 ih .. 6 ih + 5), g_b1
+        for (uint32_t r = 0; r < uint32_t(kTile); ++r) {
+            const float d = dzf[r * kHid + o];
+            const uint8_t* xp = T.base + TrainSmem::a0 + (r >> 3) * (kIn * 16u) + (r & 7u) * 16u;
+            const uint4 v0 = *reinterpret_cast<const uint4*>(xp);
+            const uint4 v1 = *reinterpret_cast<const uint4*>(xp + 128u);
+            const uint32_t w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const int i = int(6 * ih) + j;
+                const uint32_t bits = (i & 1) ? (w[i >> 1] & 0xFFFF0000u) : (w[i >> 1] << 16);
+                gW1[j] = fmaf(__uint_as_float(bits), d, gW1[j]);
+            }
+            if (ih == 0) gb1 += d;
+        }
+        fenceBeforeSync();
+        if (!__syncthreads_and(T.ok)) break;
+    }
+    for (int j = 0; j < 32; ++j) {
+        atomicAdd(P.grad + kOffW3 + (32 * ih + j) * kHid + o, gW3[j]);
+        atomicAdd(P.grad + kOffW2 + (32 * ih + j) * kHid + o, gW2[j]);
+    }
+    for (int j = 0; j < 6; ++j) atomicAdd(P.grad + kOffW1 + (6 * ih + j) * kHid + o, gW1[j]);
+    if (ih == 0) {
+        atomicAdd(P.grad + kOffB1 + o, gb1);
+        atomicAdd(P.grad + kOffB2 + o, gb2);
+        atomicAdd(P.grad + kOffB3 + o, gb3);
+        atomicAdd(P.grad + kOffW4 + o, gw4);
+    }
+    if (t == 0) atomicAdd(P.grad + kOffB4, gb4);
+    tileEnd<TrainSmem>(T, P.error);
+}
+
+// Softmax statistics of group g (rows off[g] .. off[g+1] of the step, minus
+// rowBase): lse, and dl_r = w_g / G (exp(l_r - lse) - t_r / sum t); the group's
+// cross entropy w_g (lse - sum t l / sum t) / G is added to *loss.
+struct StatsLaunch {
+    const float* logits;
+    const float* targets;
+    const float* groupWeights;  // or null
+    const uint32_t* offsets;
+    uint32_t g0, rowBase;
+    float invGroups;
+    float* dl;
+    float* loss;
+};
+
+__device__ __forceinline__ float blockReduce(float v, float* red, bool isMax) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const float w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = isMax ? fmaxf(v, w) : v + w;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    v = red[0];
+    for (int k = 1; k < int(blockDim.x >> 5); ++k) v = isMax ? fmaxf(v, red[k]) : v + red[k];
+    return v;
+}
+
+__global__ void __launch_bounds__(256) groupStatsKernel(const StatsLaunch S) {
+    __shared__ float red[8];
+    const uint32_t g = S.g0 + blockIdx.x;
+    const uint32_t a = S.offsets[g] - S.rowBase, b = S.offsets[g + 1] - S.rowBase;
+    float m = -INFINITY;
+    for (uint32_t r = a + threadIdx.x; r < b; r += blockDim.x) m = fmaxf(m, S.logits[r]);
+    m = blockReduce(m, red, true);
+    float se = 0.0f, st = 0.0f, stl = 0.0f;
+    for (uint32_t r = a + threadIdx.x; r < b; r += blockDim.x) {
+        const float l = S.logits[r], tt = S.targets[r];
+        se += __expf(l - m);
+        st += tt;
+        stl += tt * (l - m);
+    }
+    se = blockReduce(se, red, false);
+    st = blockReduce(st, red, false);
+    stl = blockReduce(stl, red, false);
+    const float w = (S.groupWeights ? S.groupWeights[g] : 1.0f) * S.invGroups;
+    const float lse = logf(se);  // relative to m
+    for (uint32_t r = a + threadIdx.x; r < b; r += blockDim.x)
+        S.dl[r] = st > 0.0f ? w * (__expf(S.logits[r] - m - lse) - S.targets[r] / st) : 0.0f;
+    if (threadIdx.x == 0 && st > 0.0f) atomicAdd(S.loss, w * (lse - stl / st));
+}
+
+__global__ void adamKernel(float* p, float* m, float* v, const float* g, int n, float lr, float b1, float b2,
+                           float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// BF16 weight images and the f32 vector from the f32 master parameters
+// (the device copy of packImages).
+__global__ void packKernel(const float* p, uint8_t* img, float* vec) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr uint32_t n1 = kHid * kIn, n2 = kHid * kHid;
+    auto put = [&](uint32_t base, uint32_t n, uint32_t k, uint32_t K, float val) {
+        *reinterpret_cast<__nv_bfloat16*>(img + base + canonOffset(n, k, K)) = __float2bfloat16_rn(val);
+    };
+    if (i < n1) {
+        const uint32_t n = i / kIn, k = i % kIn;
+        put(TrainSmem::w1, n, k, kIn, k < uint32_t(kFeat) ? p[kOffW1 + k * kHid + n] : 0.0f);
+    } else if (i < n1 + 4 * n2) {
+        const uint32_t j = i - n1, which = j / n2, n = (j % n2) / kHid, k = j % kHid;
+        if (which == 0) put(TrainSmem::w2, n, k, kHid, p[kOffW2 + k * kHid + n]);
+        else if (which == 1) put(TrainSmem::w3, n, k, kHid, p[kOffW3 + k * kHid + n]);
+        else if (which == 2) put(TrainSmem::w2b, n, k, kHid, p[kOffW2 + n * kHid + k]);
+        else put(TrainSmem::w3b, n, k, kHid, p[kOffW3 + n * kHid + k]);
+    } else if (i < n1 + 4 * n2 + uint32_t(kVecFloats)) {
+        const uint32_t j = i - n1 - 4 * n2;
+        float val;
+        if (j < uint32_t(kHid)) val = p[kOffB1 + j];
+        else if (j < 2u * kHid) val = p[kOffB2 + j - kHid];
+        else if (j < 3u * kHid) val = p[kOffB3 + j - 2 * kHid];
+        else if (j < 4u * kHid) val = __bfloat162float(__float2bfloat16_rn(p[kOffW4 + j - 3 * kHid]));
+        else val = p[kOffB4];
+        vec[j] = val;
+    }
+}
+constexpr uint32_t kPackThreads = kHid * kIn + 4 * kHid * kHid + kVecFloats;
 
 }  // namespace
 
@@ -335,6 +671,8 @@ void packImages(const std::vector<float>& p, std::vector<uint8_t>& img, std::vec
         for (uint32_t k = 0; k < uint32_t(kHid); ++k) {
             put(SmemMap::w2, n, k, kHid, p[kOffW2 + k * kHid + n]);
             put(SmemMap::w3, n, k, kHid, p[kOffW3 + k * kHid + n]);
+            put(TrainSmem::w2b, n, k, kHid, p[kOffW2 + n * kHid + k]);
+            put(TrainSmem::w3b, n, k, kHid, p[kOffW3 + n * kHid + k]);
         }
     }
     vec.assign(kVecFloats, 0.0f);
@@ -357,6 +695,8 @@ struct hase_proposal {
     DevBuf<uint4> wimg;
     DevBuf<float> vec;
     DevBuf<int> error;
+    // training state
+    DevBuf<float> dparams, adamM, adamV, grad, loss;
 };
 
 namespace {
@@ -474,6 +814,145 @@ hase_status hase_proposal_forward(hase_proposal* net, uint32_t rows, const float
     mlpForwardKernel<<<grid, kTile, kSmemBytes, net->stream>>>(P);
     HASE_CUDA(cudaGetLastError());
     HASE_CUDA(cudaMemcpyAsync(logits, l.p, rows * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+    HASE_CUDA(cudaStreamSynchronize(net->stream));
+    return checkError(net);
+}
+
+}  // extern "C"
+
+namespace {
+
+struct DeviceBatch {
+    uint32_t groups = 0, rows = 0;
+    std::vector<uint32_t> offsets;
+    DevBuf<uint32_t> doffsets;
+    DevBuf<float> features, targets, weights, logits, dl;
+    bool hasWeights = false;
+};
+
+hase_status uploadBatch(hase_proposal* net, const hase_proposal_batch* b, DeviceBatch& d) {
+    if (!b || !b->offsets || b->groups == 0) return fail(HASE_INVALID_ARGUMENT, "empty training batch");
+    if (b->offsets[0] != 0) return fail(HASE_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (uint32_t g = 0; g < b->groups; ++g)
+        if (b->offsets[g + 1] < b->offsets[g]) return fail(HASE_INVALID_ARGUMENT, "offsets must not decrease");
+    d.groups = b->groups;
+    d.rows = b->offsets[b->groups];
+    if (d.rows == 0) return fail(HASE_INVALID_ARGUMENT, "the batch has no rows");
+    if (!b->features || !b->targets) return fail(HASE_INVALID_ARGUMENT, "features and targets are required");
+    for (uint32_t r = 0; r < d.rows; ++r)
+        if (!(b->targets[r] >= 0.0f) || !std::isfinite(b->targets[r]))
+            return fail(HASE_INVALID_ARGUMENT, "targets must be finite and >= 0");
+    d.offsets.assign(b->offsets, b->offsets + b->groups + 1);
+    d.hasWeights = b->groupWeights != nullptr;
+    HASE_CUDA(d.doffsets.ensure(b->groups + 1));
+    HASE_CUDA(d.features.ensure(size_t(d.rows) * kFeat));
+    HASE_CUDA(d.targets.ensure(d.rows));
+    HASE_CUDA(d.logits.ensure(d.rows));
+    HASE_CUDA(d.dl.ensure(d.rows));
+    HASE_CUDA(cudaMemcpyAsync(d.doffsets.p, b->offsets, (b->groups + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              net->stream));
+    HASE_CUDA(cudaMemcpyAsync(d.features.p, b->features, size_t(d.rows) * kFeat * sizeof(float),
+                              cudaMemcpyHostToDevice, net->stream));
+    HASE_CUDA(cudaMemcpyAsync(d.targets.p, b->targets, d.rows * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+    if (d.hasWeights) {
+        HASE_CUDA(d.weights.ensure(b->groups));
+        HASE_CUDA(cudaMemcpyAsync(d.weights.p, b->groupWeights, b->groups * sizeof(float), cudaMemcpyHostToDevice,
+                                  net->stream));
+    }
+    return HASE_OK;
+}
+
+// Loss (added to *dLoss) and gradient (added to dGrad) of groups [g0, g1).
+hase_status lossGrad(hase_proposal* net, DeviceBatch& d, uint32_t g0, uint32_t g1, float* dLoss, float* dGrad) {
+    const uint32_t r0 = d.offsets[g0], r1 = d.offsets[g1];
+    const uint32_t rows = r1 - r0;
+    if (rows == 0) return HASE_OK;
+    const uint32_t tiles = (rows + kTile - 1) / kTile;
+    const uint32_t grid = std::min(tiles, net->numSMs);
+    ForwardLaunch F{net->wimg.p, net->vec.p, d.features.p + size_t(r0) * kFeat, d.logits.p + r0, rows, net->error.p};
+    mlpForwardKernel<<<grid, kTile, kSmemBytes, net->stream>>>(F);
+    HASE_CUDA(cudaGetLastError());
+    StatsLaunch S{d.logits.p, d.targets.p, d.hasWeights ? d.weights.p : nullptr, d.doffsets.p, g0, 0u,
+                  1.0f / float(g1 - g0), d.dl.p, dLoss};
+    groupStatsKernel<<<g1 - g0, 256, 0, net->stream>>>(S);
+    HASE_CUDA(cudaGetLastError());
+    TrainLaunch T{net->wimg.p, net->vec.p, d.features.p + size_t(r0) * kFeat, d.dl.p + r0, rows, dGrad,
+                  net->error.p};
+    mlpBackwardKernel<<<grid, kTile, kTrainSmemBytes, net->stream>>>(T);
+    HASE_CUDA(cudaGetLastError());
+    return HASE_OK;
+}
+
+hase_status prepareTraining(hase_proposal* net) {
+    HASE_CUDA(cudaSetDevice(net->device));
+    HASE_CUDA(cudaFuncSetAttribute(mlpForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
+    HASE_CUDA(
+        cudaFuncSetAttribute(mlpBackwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmemBytes)));
+    HASE_CUDA(net->grad.ensure(HASE_PROPOSAL_PARAMS));
+    HASE_CUDA(net->loss.ensure(1));
+    return HASE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_proposal_loss_grad(hase_proposal* net, const hase_proposal_batch* batch, float* loss, float* grad) {
+    if (!net || !loss || !grad) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    HASE_TRY(prepareTraining(net));
+    DeviceBatch d;
+    HASE_TRY(uploadBatch(net, batch, d));
+    HASE_CUDA(cudaMemsetAsync(net->grad.p, 0, HASE_PROPOSAL_PARAMS * sizeof(float), net->stream));
+    HASE_CUDA(cudaMemsetAsync(net->loss.p, 0, sizeof(float), net->stream));
+    HASE_TRY(lossGrad(net, d, 0, d.groups, net->loss.p, net->grad.p));
+    HASE_CUDA(cudaMemcpyAsync(grad, net->grad.p, HASE_PROPOSAL_PARAMS * sizeof(float), cudaMemcpyDeviceToHost,
+                              net->stream));
+    HASE_CUDA(cudaMemcpyAsync(loss, net->loss.p, sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+    HASE_CUDA(cudaStreamSynchronize(net->stream));
+    return checkError(net);
+}
+
+hase_status hase_proposal_train(hase_proposal* net, const hase_proposal_batch* batch,
+                                const hase_proposal_train_desc* tr, float* lossHistory) {
+    if (!net || !tr) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (tr->steps == 0) return HASE_OK;
+    if (tr->groupsPerStep == 0) return fail(HASE_INVALID_ARGUMENT, "groupsPerStep must be positive");
+    if (!(tr->learningRate > 0.0f)) return fail(HASE_INVALID_ARGUMENT, "learningRate must be positive");
+    HASE_TRY(prepareTraining(net));
+    DeviceBatch d;
+    HASE_TRY(uploadBatch(net, batch, d));
+    if (tr->groupsPerStep > d.groups) return fail(HASE_INVALID_ARGUMENT, "groupsPerStep exceeds the groups");
+    const float b1 = tr->beta1 > 0.0f ? tr->beta1 : 0.9f, b2 = tr->beta2 > 0.0f ? tr->beta2 : 0.999f;
+    const float eps = tr->epsilon > 0.0f ? tr->epsilon : 1e-8f;
+    DevBuf<float> hist;
+    HASE_CUDA(hist.ensure(tr->steps));
+    HASE_CUDA(cudaMemsetAsync(hist.p, 0, tr->steps * sizeof(float), net->stream));
+    HASE_CUDA(net->dparams.ensure(HASE_PROPOSAL_PARAMS));
+    HASE_CUDA(net->adamM.ensure(HASE_PROPOSAL_PARAMS));
+    HASE_CUDA(net->adamV.ensure(HASE_PROPOSAL_PARAMS));
+    HASE_CUDA(cudaMemcpyAsync(net->dparams.p, net->params.data(), HASE_PROPOSAL_PARAMS * sizeof(float),
+                              cudaMemcpyHostToDevice, net->stream));
+    HASE_CUDA(cudaMemsetAsync(net->adamM.p, 0, HASE_PROPOSAL_PARAMS * sizeof(float), net->stream));
+    HASE_CUDA(cudaMemsetAsync(net->adamV.p, 0, HASE_PROPOSAL_PARAMS * sizeof(float), net->stream));
+    const uint32_t blocks = d.groups / tr->groupsPerStep;
+    double p1 = 1.0, p2 = 1.0;
+    for (uint32_t step = 0; step < tr->steps; ++step) {
+        const uint32_t g0 = (step % blocks) * tr->groupsPerStep, g1 = g0 + tr->groupsPerStep;
+        HASE_CUDA(cudaMemsetAsync(net->grad.p, 0, HASE_PROPOSAL_PARAMS * sizeof(float), net->stream));
+        HASE_TRY(lossGrad(net, d, g0, g1, hist.p + step, net->grad.p));
+        p1 *= b1;
+        p2 *= b2;
+        adamKernel<<<(HASE_PROPOSAL_PARAMS + 255) / 256, 256, 0, net->stream>>>(
+            net->dparams.p, net->adamM.p, net->adamV.p, net->grad.p, HASE_PROPOSAL_PARAMS, tr->learningRate, b1, b2,
+            eps, float(1.0 - p1), float(1.0 - p2));
+        packKernel<<<(kPackThreads + 255) / 256, 256, 0, net->stream>>>(
+            net->dparams.p, reinterpret_cast<uint8_t*>(net->wimg.p), net->vec.p);
+        HASE_CUDA(cudaGetLastError());
+    }
+    HASE_CUDA(cudaMemcpyAsync(net->params.data(), net->dparams.p, HASE_PROPOSAL_PARAMS * sizeof(float),
+                              cudaMemcpyDeviceToHost, net->stream));
+    if (lossHistory)
+        HASE_CUDA(cudaMemcpyAsync(lossHistory, hist.p, tr->steps * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
     HASE_CUDA(cudaStreamSynchronize(net->stream));
     return checkError(net);
 }

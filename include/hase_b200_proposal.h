@@ -54,6 +54,37 @@ hase_status hase_proposal_set_params(hase_proposal* net, const float* params);
 /* Logits of `rows` explicit feature rows (host arrays [rows][12] -> [rows]). */
 hase_status hase_proposal_forward(hase_proposal* net, uint32_t rows, const float* features, float* logits);
 
+/* A training set: `groups` sample points, group g owning rows
+ * offsets[g] .. offsets[g+1]-1 (offsets[0] = 0), each row a feature vector and
+ * a non-negative target score (the logged gain contribution of that prism).
+ * Loss of a group: w_g times the cross entropy between the normalised targets
+ * and the softmax of the group's logits; a batch's loss is the mean over its
+ * groups. */
+typedef struct {
+    uint32_t groups;
+    const uint32_t* offsets;     /* [groups + 1] */
+    const float* features;       /* [rows][HASE_PROPOSAL_FEATURES] */
+    const float* targets;        /* [rows] */
+    const float* groupWeights;   /* [groups] or NULL (all 1) */
+} hase_proposal_batch;
+
+typedef struct {
+    uint32_t steps;              /* Adam steps */
+    uint32_t groupsPerStep;      /* step s uses groups [k G', (k+1) G'), k = s mod (groups / G') */
+    float learningRate;
+    float beta1, beta2, epsilon; /* 0 = 0.9, 0.999, 1e-8 */
+} hase_proposal_train_desc;
+
+/* Loss and gradient (HASE_PROPOSAL_PARAMS floats, master-vector order) of the
+ * whole batch: tensor-core forward and backward products, FP32 reductions. */
+hase_status hase_proposal_loss_grad(hase_proposal* net, const hase_proposal_batch* batch, float* loss, float* grad);
+
+/* Trains the network in place (Adam on the FP32 master parameters, BF16
+ * images repacked on the device after every step); lossHistory [steps] may be
+ * NULL. */
+hase_status hase_proposal_train(hase_proposal* net, const hase_proposal_batch* batch,
+                                const hase_proposal_train_desc* train, float* lossHistory);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,9 +13,12 @@ The network and its numerics follow include/hase_b200_proposal.h:
 Loss of one sample point (group of rows): cross entropy between the softmax
 of its logits and the normalised target weights t (>= 0), scaled by the
 group weight,  L_g = -w_g * sum_i (t_i / sum t) * log softmax(l)_i.
-``backward`` returns dL/dparams in the master-vector order
+``loss_and_grad`` returns the loss and dL/dparams in the master-vector order
 W1[12][64] b1 W2[64][64] b2 W3[64][64] b3 w4 b4.  It is computed in FP64 on
-the same BF16-rounded operands (straight-through for the roundings).
+the same BF16-rounded operands as the device (straight-through for the
+roundings): the backward products dz3 W3^T and dz2 W2^T take dz rounded to
+BF16 (they run on the tensor cores), the weight and bias gradients take the
+unrounded dz (FP32 reductions on the device).
 """
 
 from __future__ import annotations
@@ -118,13 +121,16 @@ def loss_and_grad(params, features, offsets, targets, group_weights=None):
     W2r, W3r, w4r, W1r = (np.asarray(bf16(np.asarray(w, np.float32)), np.float64) for w in (W2, W3, w4, W1))
     g_w4 = h3.T @ dl
     g_b4 = dl.sum()
+    def r(a):
+        return np.asarray(bf16(np.asarray(a, np.float32)), np.float64)
+
     dz3 = np.outer(dl, w4r) * _dsilu(z3)
     g_W3 = h2.T @ dz3
     g_b3 = dz3.sum(0)
-    dz2 = (dz3 @ W3r.T) * _dsilu(z2)
+    dz2 = (r(dz3) @ W3r.T) * _dsilu(z2)
     g_W2 = h1.T @ dz2
     g_b2 = dz2.sum(0)
-    dz1 = (dz2 @ W2r.T) * _dsilu(z1)
+    dz1 = (r(dz2) @ W2r.T) * _dsilu(z1)
     g_W1 = x.T @ dz1
     g_b1 = dz1.sum(0)
     grad = np.concatenate([g_W1.ravel(), g_b1, g_W2.ravel(), g_b2, g_W3.ravel(), g_b3, g_w4, [g_b4]])
