@@ -58,6 +58,9 @@ EXPORTED_SYMBOLS = (
     "hase_proposal_forward",
     "hase_proposal_loss_grad",
     "hase_proposal_train",
+    "hase_calc_phi_ase_learned",
+    "hase_log_contributions",
+    "hase_proposal_features",
 )
 PROPOSAL_FEATURES = 12
 PROPOSAL_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -205,6 +208,14 @@ class ProposalTrainDesc(C.Structure):
     ]
 
 
+class LearnedDesc(C.Structure):
+    _fields_ = [
+        ("mixture", C.c_float),
+        ("fallbackVariance", C.c_float),
+        ("fallbackSamples", C.c_uint32),
+    ]
+
+
 class HaseError(RuntimeError):
     """A libhase_b200 call failed; ``status`` is the hase_status code."""
 
@@ -261,6 +272,11 @@ def lib():
         L.hase_proposal_forward.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
         L.hase_proposal_loss_grad.argtypes = [C.c_void_p, C.POINTER(ProposalBatch), _f32p, _f32p]
         L.hase_proposal_train.argtypes = [C.c_void_p, C.POINTER(ProposalBatch), C.POINTER(ProposalTrainDesc), _f32p]
+        L.hase_calc_phi_ase_learned.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(ExperimentDesc),
+                                                C.POINTER(ComputeDesc), C.POINTER(LearnedDesc), C.POINTER(ResultDesc)]
+        L.hase_log_contributions.argtypes = [C.c_void_p, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), _f32p,
+                                             C.POINTER(ResultDesc)]
+        L.hase_proposal_features.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

@@ -20,8 +20,10 @@
 // include/core/types.hpp:201-354; dndt include/core/forwardPhiAseUtilities.hpp:16-25;
 // entry point include/core/simulation.hpp:42-47.
 #include "hase_b200.h"
+#include "hase_b200_proposal.h"
 #include "hase_device.cuh"
 #include "hase_host.cuh"
+#include "hase_mlp.cuh"
 
 #include <cuda_runtime.h>
 
@@ -112,6 +114,7 @@ struct ImportanceLaunch {
     uint32_t firstSample, slices, nW;
     float A, B;   // spectrally averaged gain coefficients
     float* lnw;   // [rows][nW]
+    const uint32_t* rowList;  // rows to compute (blockIdx.y indexes it), or null: rows 0 .. gridDim.y - 1
 };
 
 // One thread per (sample, reflection slice, triangle, group of G layers): the
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     const uint32_t perSlice = groups * m.T;
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= L.slices * perSlice) return;
-    const uint32_t row = blockIdx.y;
+    const uint32_t row = L.rowList ? L.rowList[blockIdx.y] : blockIdx.y;
     const uint32_t j = idx / perSlice;
     const uint32_t rem = idx - j * perSlice;
     const uint32_t grp = rem / m.T, t = rem - grp * m.T;
@@ -366,6 +369,7 @@ struct RayLaunch {
     double* pSum2;
     uint32_t* pDrop;
     unsigned long long* pCross;
+    float* logBuf;                // [rows][nW]: per-(slice, prism) sum of contributions (LOG kernels only)
 };
 
 __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, uint32_t x) {
@@ -384,7 +388,7 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 // REFILL idle lanes so start-point code runs convergent), and writes the
 // item's FP64 sums.  No block barrier; per-item partials keep the result
 // independent of which warp ran which item.
-template <int BLOCK, int REFILL, int MINB>
+template <int BLOCK, int REFILL, int MINB, bool LOG = false>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     const MeshView& m = L.m;
     const int lane = threadIdx.x & 31;
@@ -433,6 +437,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
         bool active = false;
         Ray ray;
         float wf = 0.0f;
+        uint32_t bsel = 0;  // (slice, prism) of the lane's ray, for the contribution log
         while (true) {
             const unsigned idle = __ballot_sync(0xffffffffu, !active);
             const int nIdle = __popc(idle);
@@ -441,6 +446,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 const uint32_t r = fetch + __popc(idle & laneLt);
                 if (!active && r < r1) {
                     const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
+                    if (LOG) bsel = b;
                     const uint32_t j = b / m.P, p = b - j * m.P;
                     const uint32_t t = p % m.T, l = p / m.T;
                     const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
@@ -482,6 +488,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         const double X = CQ * double(wf) * exp(double(ray.G));
                         sum += X;
                         sum2 += X * X;
+                        if (LOG) atomicAdd(L.logBuf + size_t(row) * nW + bsel, float(X));
                     } else {
                         ++dropped;
                     }
@@ -674,6 +681,175 @@ __global__ void noAllocEmitKernel(const float* phi, const double* mse, const uin
     out[3] = double(*drop);
 }
 
+// ------------------------------------------------- learned proposal ----
+// Features of a (sample, slice, prism) pair (include/hase_b200_proposal.h)
+// and the defensive-mixture weights that replace the importance weights.
+struct ProposalView {
+    MeshView m;
+    const float* grid;      // [layers][gy][gx] mean gain coefficient per cell (1/cm)
+    uint32_t gx, gy;
+    float x0, y0, invCell;  // grid origin and 1 / cell size
+    float lnRb, lnRt;       // mean ln reflectivity of the bottom and top surfaces
+    float R, H;             // mesh radius and height
+    float lnVref;           // ln(mean prism volume / R^2)
+    float lnSigmaRatio;     // ln(sigma_e / sigma_a) of the averaged spectrum
+    uint32_t firstSample, nW;
+};
+
+__device__ __forceinline__ float sliceLnReflect(const ProposalView& V, uint32_t j) {
+    return j == 0 ? 0.0f : j == 1 ? V.lnRb : j == 2 ? V.lnRt : V.lnRb + V.lnRt;
+}
+
+// Returns the prior beta V R_j / d^2 (0 without a source) and fills f.
+__device__ __forceinline__ float pairFeatures(const ProposalView& V, uint32_t sample, uint32_t jp, float (&f)[kFeat]) {
+    const MeshView& m = V.m;
+    const uint32_t j = jp / m.P, p = jp - j * m.P;
+    const uint32_t t = p % m.T, l = p / m.T;
+    const float2 S = __ldg(m.points + sample % m.Np);
+    const int ls = int(sample / m.Np);
+    const float zs = float(ls) * m.h;
+    const float zi = float(imageLevel(ls, int(m.layers), j)) * m.h;
+    const float2 c = __ldg(m.centroid + t);
+    const float zc = (float(l) + 0.5f) * m.h;
+    const float dx = c.x - S.x, dy = c.y - S.y, dz = zc - zi;
+    const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float beta = __ldg(m.srcBeta + p);
+    const float vol = __ldg(m.geo + 2 * t + 1).z * m.h;
+    // straight-line ln gain estimated on the coarse grid, 8 points, z folded
+    float lng = 0.0f;
+    const float twoH = 2.0f * V.H;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float a = (float(k) + 0.5f) * 0.125f;
+        const float x = S.x + a * dx, y = S.y + a * dy;
+        // fold the unfolded height into [0, H]: period 2H, mirrored halves
+        float z = zi + a * dz;
+        z -= twoH * floorf(z / twoH);
+        if (z > V.H) z = twoH - z;
+        const int ly = min(max(int(z / m.h), 0), int(m.layers) - 1);
+        const int ix = min(max(int((x - V.x0) * V.invCell), 0), int(V.gx) - 1);
+        const int iy = min(max(int((y - V.y0) * V.invCell), 0), int(V.gy) - 1);
+        lng += __ldg(V.grid + (size_t(ly) * V.gy + iy) * V.gx + ix);
+    }
+    const float lnR = sliceLnReflect(V, j);
+    lng = lng * 0.125f * d + lnR;
+    f[0] = S.x / V.R;
+    f[1] = S.y / V.R;
+    f[2] = zs / V.H;
+    f[3] = dx / V.R;
+    f[4] = dy / V.R;
+    f[5] = dz / V.H;
+    f[6] = logf(d / V.R);
+    f[7] = beta;
+    f[8] = lng;
+    f[9] = beta > 0.0f ? logf(beta * vol / (d * d)) - V.lnVref : 0.0f;
+    f[10] = float(j) * 0.25f;
+    f[11] = V.lnSigmaRatio;
+    return beta > 0.0f ? beta * vol * __expf(lnR) / (d * d) : 0.0f;
+}
+
+struct ProposalLaunch {
+    ProposalView V;
+    const uint4* wimg;
+    const float* vec;
+    float* out;             // [rows][nW]: logits
+    float* prior;           // [rows][nW]: beta V R_j / d^2 (0 without a source)
+    float* features;        // [rows][nW][kFeat] (featureKernel) or null
+    uint32_t rows;          // sample rows from V.firstSample
+    int* error;
+};
+
+// Network logits of every (slice, prism) of `rows` sample rows (tensor cores).
+__global__ void __launch_bounds__(kTile, kMlpBlocksPerSM) proposalKernel(const ProposalLaunch P) {
+    extern __shared__ uint8_t dynSmem[];
+    Tile T;
+    tileBegin<SmemMap>(T, dynSmem, P.wimg, P.vec);
+    const uint64_t total = uint64_t(P.rows) * P.V.nW;
+    const uint64_t tiles = (total + kTile - 1) / kTile;
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint64_t gr = tile * kTile + threadIdx.x;
+        float f[kFeat];
+        if (gr < total) {
+            P.prior[gr] = pairFeatures(P.V, P.V.firstSample + uint32_t(gr / P.V.nW), uint32_t(gr % P.V.nW), f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kFeat; ++k) f[k] = 0.0f;
+        }
+        storeFeatures(T, SmemMap::a0, f);
+        const float logit = mlpTile(T);
+        if (gr < total) P.out[gr] = logit;
+        if (!__syncthreads_and(T.ok)) break;
+    }
+    tileEnd<SmemMap>(T, P.error);
+}
+
+// Feature rows only (training sets): one thread per pair.
+__global__ void featureKernel(const ProposalLaunch P) {
+    const uint64_t gr = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gr >= uint64_t(P.rows) * P.V.nW) return;
+    float f[kFeat];
+    pairFeatures(P.V, P.V.firstSample + uint32_t(gr / P.V.nW), uint32_t(gr % P.V.nW), f);
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) P.features[gr * kFeat + k] = f[k];
+}
+
+template <bool MAX>
+__device__ __forceinline__ float blockReduce1024(float v, float* red) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const float w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = MAX ? fmaxf(v, w) : v + w;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    v = red[0];
+    for (int k = 1; k < int(blockDim.x >> 5); ++k) v = MAX ? fmaxf(v, red[k]) : v + red[k];
+    return v;
+}
+
+// One block per sample row: lnw = ln((1 - alpha) softmax(logits) + alpha
+// prior / sum prior) over the pairs with a source (prior > 0), -inf elsewhere.
+__global__ void __launch_bounds__(1024) mixtureKernel(uint32_t nW, float* lnw, const float* priorBuf, float alpha) {
+    __shared__ float red[32];
+    const uint32_t row = blockIdx.x;
+    float* w = lnw + size_t(row) * nW;
+    const float* pr = priorBuf + size_t(row) * nW;
+    float mx = -INFINITY, ps = 0.0f;
+    for (uint32_t jp = threadIdx.x; jp < nW; jp += blockDim.x) {
+        const float prior = pr[jp];
+        if (prior > 0.0f) {
+            mx = fmaxf(mx, w[jp]);
+            ps += prior;
+        }
+    }
+    mx = blockReduce1024<true>(mx, red);
+    ps = blockReduce1024<false>(ps, red);
+    float se = 0.0f;
+    for (uint32_t jp = threadIdx.x; jp < nW; jp += blockDim.x)
+        if (pr[jp] > 0.0f) se += __expf(w[jp] - mx);
+    se = blockReduce1024<false>(se, red);
+    const float a = ps > 0.0f ? alpha / ps : 0.0f, b = se > 0.0f ? (1.0f - alpha) / se : 0.0f;
+    for (uint32_t jp = threadIdx.x; jp < nW; jp += blockDim.x) {
+        const float prior = pr[jp];
+        const float q = prior > 0.0f ? b * __expf(w[jp] - mx) + a * prior : 0.0f;
+        w[jp] = q > 0.0f ? logf(q) : -INFINITY;
+    }
+}
+
+// Zeroes the accumulators of the listed rows (samples restarted with the
+// exact importance weights).
+__global__ void resetRowsKernel(const uint32_t* rows, uint32_t n, double* sum, double* sum2, uint32_t* total,
+                                uint32_t* drop, unsigned long long* cross) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t r = rows[i];
+    sum[r] = 0.0;
+    sum2[r] = 0.0;
+    total[r] = 0u;
+    drop[r] = 0u;
+    cross[r] = 0ull;
+}
+
 // -------------------------------------------------------- host side ----
 struct HostTables {
     std::vector<int4> verts;
@@ -772,6 +948,12 @@ struct hase_context {
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
+    // host copies used by the learned proposal's features
+    std::vector<float2> hCentroid, hPoints;
+    std::vector<float> hArea, hGainBeta, hReflect;
+    // learned proposal: coarse gain grid, fallback rows, contribution log
+    DevBuf<float> featGrid, logBuf, priorBuf;
+    DevBuf<uint32_t> rowList;
 
     MeshView view() const {
         MeshView v{};
@@ -808,6 +990,7 @@ hase_status uploadBeta(hase_context* c, const double* betaVolume) {
         src[p] = float(b);
         gain[p] = clad ? NAN : float(b);
     }
+    c->hGainBeta = gain;
     HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->srcBeta.p, src.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
@@ -826,6 +1009,100 @@ uint32_t adaptiveTarget(uint32_t minRays, uint32_t maxRays, uint32_t steps, uint
 
 hase_status setDevice(hase_context* c) {
     HASE_CUDA(cudaSetDevice(c->device));
+    return HASE_OK;
+}
+
+struct LearnedArgs {
+    hase_proposal* net;
+    float alpha;             // weight of the beta V / d^2 prior in the mixture
+    float fallbackVariance;  // per-ray relative variance that sends a sample to the exact weights (0: never)
+    uint32_t fallbackSamples;
+};
+
+constexpr uint32_t kGridCells = 48;  // feature grid cells along the longer side
+
+// Feature view of the context: the coarse gain grid (mean g = A beta - B of
+// the prisms whose centre falls in a cell, empty cells filled from their
+// neighbours), scales, and mean reflectivities.
+hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V) {
+    float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY, R = 0.0f;
+    for (const float2& q : c->hPoints) {
+        x0 = std::min(x0, q.x);
+        y0 = std::min(y0, q.y);
+        x1 = std::max(x1, q.x);
+        y1 = std::max(y1, q.y);
+        R = std::max(R, std::sqrt(q.x * q.x + q.y * q.y));
+    }
+    const float cell = std::max(x1 - x0, y1 - y0) / float(kGridCells) * 1.0001f;
+    const uint32_t gx = uint32_t(std::ceil((x1 - x0) / cell)) + 1, gy = uint32_t(std::ceil((y1 - y0) / cell)) + 1;
+    const uint32_t L = c->layers;
+    std::vector<float> sum(size_t(L) * gx * gy, 0.0f), cnt(sum.size(), 0.0f);
+    for (uint32_t l = 0; l < L; ++l)
+        for (uint32_t t = 0; t < c->T; ++t) {
+            const float b = c->hGainBeta[t + size_t(l) * c->T];
+            const float g = std::isnan(b) ? -float(c->cladAbs) : float(A * b - B);
+            const uint32_t ix = std::min(gx - 1, uint32_t((c->hCentroid[t].x - x0) / cell));
+            const uint32_t iy = std::min(gy - 1, uint32_t((c->hCentroid[t].y - y0) / cell));
+            const size_t k = (size_t(l) * gy + iy) * gx + ix;
+            sum[k] += g;
+            cnt[k] += 1.0f;
+        }
+    for (size_t k = 0; k < sum.size(); ++k)
+        if (cnt[k] > 0.0f) sum[k] /= cnt[k];
+    for (uint32_t l = 0; l < L; ++l)  // fill empty cells from filled 4-neighbours
+        for (uint32_t sweep = 0; sweep < gx + gy; ++sweep) {
+            bool changed = false;
+            std::vector<float> add(size_t(gx) * gy, 0.0f), n(size_t(gx) * gy, 0.0f);
+            for (uint32_t iy = 0; iy < gy; ++iy)
+                for (uint32_t ix = 0; ix < gx; ++ix) {
+                    const size_t k = (size_t(l) * gy + iy) * gx + ix;
+                    if (cnt[k] > 0.0f) continue;
+                    const int dxy[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+                    for (auto& o : dxy) {
+                        const int jx = int(ix) + o[0], jy = int(iy) + o[1];
+                        if (jx < 0 || jy < 0 || jx >= int(gx) || jy >= int(gy)) continue;
+                        const size_t kk = (size_t(l) * gy + jy) * gx + jx;
+                        if (cnt[kk] > 0.0f) {
+                            add[iy * gx + ix] += sum[kk];
+                            n[iy * gx + ix] += 1.0f;
+                        }
+                    }
+                }
+            for (uint32_t i = 0; i < gx * gy; ++i)
+                if (n[i] > 0.0f) {
+                    const size_t k = size_t(l) * gx * gy + i;
+                    sum[k] = add[i] / n[i];
+                    cnt[k] = 1.0f;
+                    changed = true;
+                }
+            if (!changed) break;
+        }
+    HASE_CUDA(c->featGrid.ensure(sum.size()));
+    HASE_CUDA(cudaMemcpyAsync(c->featGrid.p, sum.data(), sum.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              c->stream));
+    double lnRb = 0.0, lnRt = 0.0, vmean = 0.0;
+    if (!c->hReflect.empty()) {
+        for (uint32_t t = 0; t < c->T; ++t) {
+            lnRb += std::log(std::max(1e-6, double(c->hReflect[2 * t]))) / c->T;
+            lnRt += std::log(std::max(1e-6, double(c->hReflect[2 * t + 1]))) / c->T;
+        }
+    }
+    for (float a : c->hArea) vmean += double(a) * c->h / c->T;
+    V = ProposalView{};
+    V.m = c->view();
+    V.grid = c->featGrid.p;
+    V.gx = gx;
+    V.gy = gy;
+    V.x0 = x0;
+    V.y0 = y0;
+    V.invCell = 1.0f / cell;
+    V.lnRb = float(lnRb);
+    V.lnRt = float(lnRt);
+    V.R = std::max(R, 1e-6f);
+    V.H = float(c->h * L);
+    V.lnVref = float(std::log(std::max(vmean, 1e-30) / (double(V.R) * V.R)));
+    const double se = (A - B), sa = B;
+    V.lnSigmaRatio = float(std::log(std::max(se, 1e-30) / std::max(sa, 1e-30)));
     return HASE_OK;
 }
 
@@ -913,6 +1190,12 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
     hase_status st = buildHostTables(d, ht, c->extent);
     if (st != HASE_OK) return cleanup(st);
     c->extent = std::max(c->extent, c->h * c->layers);
+    c->hCentroid = ht.centroid;
+    c->hPoints = ht.points;
+    c->hArea.resize(c->T);
+    for (uint32_t t = 0; t < c->T; ++t) c->hArea[t] = ht.geo[2 * t + 1].z;
+    if (d->reflectivities)
+        for (size_t k = 0; k < 2 * size_t(c->T); ++k) c->hReflect.push_back(float(d->reflectivities[k]));
 
     if (cudaSetDevice(device) != cudaSuccess) return cleanup(fail(HASE_CUDA_ERROR, "cudaSetDevice failed"));
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -977,8 +1260,13 @@ hase_status hase_context_destroy(hase_context* c) {
     return HASE_OK;
 }
 
-hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
-                              hase_result* res) {
+// The adaptive solve of hase_calc_phi_ase.  la != null: the learned
+// proposal replaces the importance weights (samples whose first-pass per-ray
+// relative variance exceeds la->fallbackVariance restart with the importance
+// weights).  logOut != null: the rays' contributions are summed per
+// (sample, slice, prism) into logOut [samples][slices * P].
+static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                            hase_result* res, LearnedArgs* la, float* logOut) {
     if (!c || !ex || !cp || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
     HASE_TRY(setDevice(c));
     const uint32_t nSamplesTotal = c->Np * c->L;
@@ -1008,6 +1296,18 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     }
     HASE_CUDA(c->spec.ensure(nLambda));
     HASE_CUDA(cudaMemcpyAsync(c->spec.p, spec.data(), nLambda * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    ProposalView pv{};
+    uint32_t proposalGrid = 0;
+    if (la) {
+        if (la->net->device != c->device)
+            return fail(HASE_INVALID_ARGUMENT, "the proposal network and the context are on different devices");
+        HASE_TRY(buildProposalView(c, meanA, meanB, pv));
+        HASE_CUDA(cudaFuncSetAttribute(proposalKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
+        int sms = 0;
+        HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        proposalGrid = uint32_t(std::max(1, sms) * kMlpBlocksPerSM);
+        la->fallbackSamples = 0;
+    }
 
     // batch rows by the workspace budget
     const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
@@ -1050,6 +1350,14 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     HASE_CUDA(c->pSum2.ensure(size_t(rows) * kMaxItems));
     HASE_CUDA(c->pDrop.ensure(size_t(rows) * kMaxItems));
     HASE_CUDA(c->pCross.ensure(size_t(rows) * kMaxItems));
+    if (logOut) HASE_CUDA(c->logBuf.ensure(size_t(rows) * nW));
+    if (la) {
+        HASE_CUDA(c->rowList.ensure(rows));
+        HASE_CUDA(c->priorBuf.ensure(size_t(rows) * nW));
+    }
+    std::vector<uint32_t> hList;
+    std::vector<double> hRse;
+    std::vector<uint32_t> hTot;
 
     const MeshView mv = c->view();
     const double C = c->nTot / (4.0 * kPi * c->tau);
@@ -1071,15 +1379,32 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
         const uint32_t nRows = std::min(rows, nS - b0);
         const uint32_t firstSample = first + b0;
         HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
-        ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p};
-        if (cp->importanceLayers == 4) {
-            const uint32_t impThreads = slices * ((c->layers + 3) / 4) * c->T;
-            importanceKernel<4><<<dim3((impThreads + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+        ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p, nullptr};
+        auto launchImportance = [&](uint32_t nLaunchRows) {
+            if (cp->importanceLayers == 4) {
+                const uint32_t impThreads = slices * ((c->layers + 3) / 4) * c->T;
+                importanceKernel<4><<<dim3((impThreads + 255) / 256, nLaunchRows), 256, 0, c->stream>>>(il);
+            } else {
+                const uint32_t impThreads = slices * ((c->layers + kImportanceLayers - 1) / kImportanceLayers) * c->T;
+                importanceKernel<kImportanceLayers>
+                    <<<dim3((impThreads + 255) / 256, nLaunchRows), 256, 0, c->stream>>>(il);
+            }
+        };
+        if (la) {
+            pv.firstSample = firstSample;
+            pv.nW = nW;
+            ProposalLaunch pl{pv, la->net->wimg.p, la->net->vec.p, c->lnw.p, c->priorBuf.p, nullptr, nRows,
+                              la->net->error.p};
+            const uint64_t tiles = (uint64_t(nRows) * nW + kTile - 1) / kTile;
+            proposalKernel<<<uint32_t(std::min<uint64_t>(tiles, proposalGrid)), kTile, kSmemBytes, c->stream>>>(pl);
+            HASE_CUDA(cudaGetLastError());
+            mixtureKernel<<<nRows, 1024, 0, c->stream>>>(nW, c->lnw.p, c->priorBuf.p, la->alpha);
+            res->kernelLaunches += 1;
         } else {
-            const uint32_t impThreads = slices * ((c->layers + kImportanceLayers - 1) / kImportanceLayers) * c->T;
-            importanceKernel<kImportanceLayers><<<dim3((impThreads + 255) / 256, nRows), 256, 0, c->stream>>>(il);
+            launchImportance(nRows);
         }
         HASE_CUDA(cudaGetLastError());
+        if (logOut) HASE_CUDA(cudaMemsetAsync(c->logBuf.p, 0, size_t(nRows) * nW * sizeof(float), c->stream));
         HASE_CUDA(cudaEventRecord(c->ev[1], c->stream));
         HASE_CUDA(cudaMemsetAsync(c->accSum.p, 0, nRows * sizeof(double), c->stream));
         HASE_CUDA(cudaMemsetAsync(c->accSum2.p, 0, nRows * sizeof(double), c->stream));
@@ -1109,8 +1434,9 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
             HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
             RayLaunch rl{mv, cur, nActive, firstSample, pass, M, nW, itemRays, items, c->itemCounter.p, c->q.p,
                          c->Q.p, c->offsets.p, cp->rngSeed, 0u, c->spec.p, nLambda, ex->nearFieldSampling, C, c->pSum.p, c->pSum2.p,
-                         c->pDrop.p, c->pCross.p};
-            const RayVariant& rv = kRayVariants[variant];
+                         c->pDrop.p, c->pCross.p, logOut ? c->logBuf.p : nullptr};
+            const RayVariant logVariant{rayKernel<kRayBlock, kRefill, kRayMinBlocks, true>, int(kRayBlock), "log"};
+            const RayVariant& rv = logOut ? logVariant : kRayVariants[variant];
             const uint64_t totalItems = uint64_t(nActive) * items;
             const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1,
                                                                uint64_t(c->variantBlocks[variant])));
@@ -1142,6 +1468,49 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
                 break;
             }
             if (next == 0) break;
+            if (la && pass == 0 && la->fallbackVariance > 0.0f) {
+                // the plain method judges: samples whose per-ray relative
+                // variance under the learned proposal exceeds the plain
+                // method's restart with the importance weights
+                hList.resize(next);
+                hRse.resize(nRows);
+                hTot.resize(nRows);
+                HASE_CUDA(cudaMemcpyAsync(hList.data(), nxt, next * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+                HASE_CUDA(cudaMemcpyAsync(hRse.data(), c->mse.p, nRows * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+                HASE_CUDA(cudaMemcpyAsync(hTot.data(), c->accTotal.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                          c->stream));
+                HASE_CUDA(cudaStreamSynchronize(c->stream));
+                std::vector<uint32_t> fb;
+                for (uint32_t i = 0; i < next; ++i) {
+                    const uint32_t r = hList[i];
+                    const double v = double(hTot[r]) * hRse[r] * hRse[r];
+                    if (!std::isfinite(hRse[r]) || v > double(la->fallbackVariance)) fb.push_back(r);
+                }
+                if (!fb.empty()) {
+                    const uint32_t nf = uint32_t(fb.size());
+                    HASE_CUDA(cudaMemcpyAsync(c->rowList.p, fb.data(), nf * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                              c->stream));
+                    HASE_CUDA(cudaEventRecord(c->ev[2], c->stream));
+                    il.rowList = c->rowList.p;
+                    launchImportance(nf);
+                    il.rowList = nullptr;
+                    HASE_CUDA(cudaGetLastError());
+                    HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
+                    MapLaunch rq{c->lnw.p, 1, 1, c->rowList.p, nW, 1u, nullptr, firstSample, 0u, cp->rngSeed, 0u,
+                                 nullptr, c->q.p, c->Q.p, c->offsets.p};
+                    mapKernel<<<nf, kMapBlock, 0, c->stream>>>(rq);
+                    resetRowsKernel<<<(nf + 255) / 256, 256, 0, c->stream>>>(c->rowList.p, nf, c->accSum.p,
+                                                                             c->accSum2.p, c->accTotal.p,
+                                                                             c->accDrop.p, c->accCross.p);
+                    HASE_CUDA(cudaGetLastError());
+                    res->kernelLaunches += 3;
+                    HASE_CUDA(cudaStreamSynchronize(c->stream));
+                    float fbMs = 0.0f;
+                    HASE_CUDA(cudaEventElapsedTime(&fbMs, c->ev[2], c->ev[3]));
+                    res->importanceMilliseconds += fbMs;
+                    la->fallbackSamples += nf;
+                }
+            }
             std::swap(cur, nxt);
             nActive = next;
         }
@@ -1151,6 +1520,9 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
         HASE_CUDA(cudaMemcpyAsync(hTotal.data(), c->accTotal.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
         HASE_CUDA(cudaMemcpyAsync(hDrop.data(), c->accDrop.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
         HASE_CUDA(cudaMemcpyAsync(hCross.data(), c->accCross.p, nRows * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        if (logOut)
+            HASE_CUDA(cudaMemcpyAsync(logOut + size_t(b0) * nW, c->logBuf.p, size_t(nRows) * nW * sizeof(float),
+                                      cudaMemcpyDeviceToHost, c->stream));
         HASE_CUDA(cudaStreamSynchronize(c->stream));
         float total = 0;
         HASE_CUDA(cudaEventElapsedTime(&total, c->ev[0], c->ev[3]));
@@ -1180,6 +1552,64 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
         fail(HASE_NOT_CONVERGED, "%u samples above the threshold at maxRays", res->unconvergedSamples);
         return HASE_NOT_CONVERGED;
     }
+    return HASE_OK;
+}
+
+
+hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                              hase_result* res) {
+    return calcCore(c, ex, cp, res, nullptr, nullptr);
+}
+
+hase_status hase_calc_phi_ase_learned(hase_context* c, hase_proposal* net, const hase_experiment_desc* ex,
+                                      const hase_compute_desc* cp, hase_learned_desc* learned, hase_result* res) {
+    if (!net || !learned) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (!(learned->mixture >= 0.0f) || learned->mixture >= 1.0f)
+        return fail(HASE_INVALID_ARGUMENT, "mixture must be in [0, 1)");
+    if (!(learned->fallbackVariance >= 0.0f)) return fail(HASE_INVALID_ARGUMENT, "fallbackVariance must be >= 0");
+    LearnedArgs la{net, learned->mixture > 0.0f ? learned->mixture : 0.1f, learned->fallbackVariance, 0u};
+    const hase_status st = calcCore(c, ex, cp, res, &la, nullptr);
+    learned->fallbackSamples = la.fallbackSamples;
+    int err = 0;
+    if (cudaMemcpy(&err, net->error.p, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && err)
+        return fail(HASE_DEVICE_TIMEOUT, "a tensor-core wait of the proposal network timed out");
+    return st;
+}
+
+hase_status hase_log_contributions(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                                   float* contributions, hase_result* res) {
+    if (!contributions) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    hase_result local{};
+    return calcCore(c, ex, cp, res ? res : &local, nullptr, contributions);
+}
+
+hase_status hase_proposal_features(hase_context* c, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                                   uint32_t monochromatic, float* features) {
+    if (!c || !features) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (count == 0) return HASE_OK;
+    if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L)
+        return fail(HASE_INVALID_ARGUMENT, "sample range outside the mesh");
+    HASE_TRY(setDevice(c));
+    const uint32_t nW = (useReflections ? 5u : 1u) * c->P;
+    const uint32_t nL = monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double A = 0.0, B = 0.0;
+    for (uint32_t l = 0; l < nL; ++l) {
+        A += c->nTot * (c->sigmaE[l] + c->sigmaA[l]) / nL;
+        B += c->nTot * c->sigmaA[l] / nL;
+    }
+    ProposalView pv{};
+    HASE_TRY(buildProposalView(c, A, B, pv));
+    pv.firstSample = firstSample;
+    pv.nW = nW;
+    const size_t n = size_t(count) * nW * kFeat;
+    DevBuf<float> out;
+    HASE_CUDA(out.ensure(n));
+    ProposalLaunch pl{pv, nullptr, nullptr, nullptr, nullptr, out.p, count, nullptr};
+    const uint64_t pairs = uint64_t(count) * nW;
+    featureKernel<<<uint32_t((pairs + 255) / 256), 256, 0, c->stream>>>(pl);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(features, out.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
     return HASE_OK;
 }
 

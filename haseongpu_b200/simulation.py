@@ -53,6 +53,7 @@ class Result:
     unconvergedSamples: int = 0
     kernelLaunches: int = 0
     tallyMode: int = 0
+    fallbackSamples: int = 0
     status: int = 0
 
     @property
@@ -103,9 +104,9 @@ class DeviceMesh:
             raise ValueError("betaCells size mismatch")
         N.check(N.lib().hase_context_update_beta(self.handle, N.ptr(bv, N._f64p), N.ptr(bc, N._f64p)))
 
-    def calc_phi_ase(self, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
-                     nearFieldSampling=True, adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
-                     blockSize=0, workspaceBytes=0, rayKernelVariant=0, importanceLayers=0) -> Result:
+    def _descs(self, minRays, maxRays, mseThreshold, useReflections, monochromatic, nearFieldSampling, adaptiveSteps,
+               repetitions, rngSeed, minSample, maxSample, raysPerThread, blockSize, workspaceBytes, rayKernelVariant,
+               importanceLayers):
         S = self.mesh.numberOfSamples
         maxSample = S - 1 if maxSample is None else int(maxSample)
         n = maxSample - int(minSample) + 1
@@ -121,6 +122,62 @@ class DeviceMesh:
         r = N.ResultDesc(N.ptr(out.phiAse, N._f32p), N.ptr(out.standardError, N._f64p),
                          N.ptr(out.relativeStandardError, N._f64p), N.ptr(out.totalRays, N._u32p),
                          N.ptr(out.dndtAse, N._f64p), N.ptr(out.droppedRays, N._u32p))
+        return out, ex, cp, r, n
+
+    @staticmethod
+    def _fill(out, r, status):
+        out.status = status
+        out.raysTraced = int(r.raysTraced)
+        out.crossings = int(r.crossings)
+        out.importanceMilliseconds = float(r.importanceMilliseconds)
+        out.rayMilliseconds = float(r.rayMilliseconds)
+        out.totalMilliseconds = float(r.totalMilliseconds)
+        out.passes = int(r.passes)
+        out.unconvergedSamples = int(r.unconvergedSamples)
+        out.kernelLaunches = int(r.kernelLaunches)
+        return out
+
+    def calc_phi_ase_learned(self, net, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False,
+                             monochromatic=False, nearFieldSampling=True, adaptiveSteps=0, rngSeed=5489, minSample=0,
+                             maxSample=None, mixture=0.0, fallbackVariance=0.0, workspaceBytes=0, rayKernelVariant=0,
+                             raysPerThread=0) -> Result:
+        """The solve with the learned proposal ``net`` (a ProposalNet on the same device)."""
+        out, ex, cp, r, _ = self._descs(minRays, maxRays, mseThreshold, useReflections, monochromatic,
+                                        nearFieldSampling, adaptiveSteps, 1, rngSeed, minSample, maxSample,
+                                        raysPerThread, 0, workspaceBytes, rayKernelVariant, 0)
+        ld = N.LearnedDesc(float(mixture), float(fallbackVariance), 0)
+        status = N.check(N.lib().hase_calc_phi_ase_learned(self.handle, net.handle, C.byref(ex), C.byref(cp),
+                                                           C.byref(ld), C.byref(r)), allow_warnings=True)
+        self._fill(out, r, status)
+        out.fallbackSamples = int(ld.fallbackSamples)
+        return out
+
+    def log_contributions(self, *, minRays, useReflections=False, monochromatic=False, nearFieldSampling=True,
+                          rngSeed=5489, minSample=0, maxSample=None):
+        """One pass of `minRays` rays per sample with the importance weights;
+        returns (Result, contributions [samples][slices * P]) -- the summed ray
+        contributions per (slice, prism), the proposal's training targets."""
+        out, ex, cp, r, n = self._descs(minRays, minRays, 0.0, useReflections, monochromatic, nearFieldSampling, 0, 1,
+                                        rngSeed, minSample, maxSample, 0, 0, 0, 0, 0)
+        slices = 5 if useReflections else 1
+        contrib = np.empty((n, slices * self.mesh.numberOfPrisms), np.float32)
+        status = N.check(N.lib().hase_log_contributions(self.handle, C.byref(ex), C.byref(cp),
+                                                        N.ptr(contrib, N._f32p), C.byref(r)), allow_warnings=True)
+        return self._fill(out, r, status), contrib
+
+    def proposal_features(self, firstSample, count, useReflections=False, monochromatic=False) -> np.ndarray:
+        slices = 5 if useReflections else 1
+        f = np.empty((int(count), slices * self.mesh.numberOfPrisms, N.PROPOSAL_FEATURES), np.float32)
+        N.check(N.lib().hase_proposal_features(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
+                                               1 if monochromatic else 0, N.ptr(f, N._f32p)))
+        return f
+
+    def calc_phi_ase(self, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
+                     nearFieldSampling=True, adaptiveSteps=0, repetitions=1, rngSeed=5489, minSample=0, maxSample=None, raysPerThread=0,
+                     blockSize=0, workspaceBytes=0, rayKernelVariant=0, importanceLayers=0) -> Result:
+        out, ex, cp, r, _ = self._descs(minRays, maxRays, mseThreshold, useReflections, monochromatic,
+                                        nearFieldSampling, adaptiveSteps, repetitions, rngSeed, minSample, maxSample,
+                                        raysPerThread, blockSize, workspaceBytes, rayKernelVariant, importanceLayers)
         status = N.check(N.lib().hase_calc_phi_ase(self.handle, C.byref(ex), C.byref(cp), C.byref(r)),
                          allow_warnings=True)
         out.status = status

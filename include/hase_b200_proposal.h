@@ -85,6 +85,38 @@ hase_status hase_proposal_loss_grad(hase_proposal* net, const hase_proposal_batc
 hase_status hase_proposal_train(hase_proposal* net, const hase_proposal_batch* batch,
                                 const hase_proposal_train_desc* train, float* lossHistory);
 
+/* ---- the learned proposal in the phi-ASE solve ---- */
+
+typedef struct {
+    float mixture;               /* weight alpha of the beta V / d^2 prior in
+                                    q = (1 - alpha) softmax + alpha prior; 0 = 0.1 */
+    float fallbackVariance;      /* a sample whose first-pass per-ray relative variance
+                                    (rays x relative error^2) under the learned proposal
+                                    exceeds this restarts with the importance weights of
+                                    hase_importance_weights; 0 = never */
+    uint32_t fallbackSamples;    /* out: samples that restarted */
+} hase_learned_desc;
+
+/* hase_calc_phi_ase with the learned proposal in place of the importance
+ * weights (same experiment / compute / result conventions).  Every ray is
+ * weighted by the inverse probability of the quantised proposal it was drawn
+ * from, so the estimate stays unbiased. */
+hase_status hase_calc_phi_ase_learned(hase_context* ctx, hase_proposal* net, const hase_experiment_desc* experiment,
+                                      const hase_compute_desc* compute, hase_learned_desc* learned,
+                                      hase_result* result);
+
+/* hase_calc_phi_ase that also sums every ray's contribution X per (sample,
+ * slice, prism): contributions [samples][slices * P] (slices = 5 with
+ * reflections, else 1), the training targets of the proposal.  result may be
+ * NULL. */
+hase_status hase_log_contributions(hase_context* ctx, const hase_experiment_desc* experiment,
+                                   const hase_compute_desc* compute, float* contributions, hase_result* result);
+
+/* Network features of every (slice, prism) pair of samples
+ * [firstSample, firstSample + count): features [count][slices * P][12]. */
+hase_status hase_proposal_features(hase_context* ctx, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                                   uint32_t monochromatic, float* features);
+
 #ifdef __cplusplus
 }
 #endif
