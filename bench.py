@@ -1,13 +1,19 @@
 #!/usr/bin/env python3
 """bench.py -- phi-ASE throughput of libhase_b200 on B200.
 
-Workload (default ``disc_poly``, the polychromatic disc with reflections): a
-step is one full adaptive phi-ASE solve (importance weights, ray->prism map,
-ray passes until every sample's relative error <= threshold or maxRays) over a
-batch of sample points of the seeded synthetic medium; consecutive steps (and
-ranks) take consecutive sample batches.  Metric: time to threshold, reported
-as its throughput form -- sample points brought to the threshold per second
-over the whole job -- with rays/s and the per-step time beside it.
+Default workload ``learned`` (the headline: time to threshold with the
+learned proposal against plain importance sampling): the network is trained
+(untimed) on contributions logged on 32 seeded pump fields of the disc_small
+geometry; a step is one full adaptive phi-ASE solve of every sample point of
+one unseen pump field (learned proposal, ray->prism map, ray passes until
+every sample's relative error <= threshold or maxRays).  The same fields are
+also solved with the reference's plain importance sampling and with the
+importance weights + near-field start points.  Metric: time to threshold,
+reported as its throughput form -- sample points brought to the threshold per
+second over the whole job -- with rays/s and the per-step time beside it.
+The line nests the importance-sampled solve of ``disc_poly`` (polychromatic
+disc with reflections; ``--workload disc_poly`` prints it as the line) and the
+forward Tet4 path (``--path forward``).
 
 ``value`` is device-timed (CUDA events recorded by the library on the stream
 its kernels run on), inputs resident; ``e2e`` goes through the public API with
@@ -43,6 +49,7 @@ FP32_INSTR_PER_CROSSING = 24   # stated per-crossing FP32 instruction count
 BYTES_PER_CROSSING = 52        # triangle record 48 B + prism beta 4 B
 SMS = 148
 LANES_PER_SM = 128
+MLP_FLOP_PER_PAIR = 2 * (12 * 64 + 64 * 64 + 64 * 64 + 64 * 1)  # 18,048 FLOP per (sample, prism) inference
 FWD_METRIC = "forward Tet4 phi-ASE source rays traced and tallied per second on 1 B200 (crossings/s alongside)"
 FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count of the forward walk
 BYTES_PER_TET_CROSSING = 148       # cell record 128 B + beta 8 B + one vertex tally 8 B + one visit count 4 B
@@ -56,7 +63,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="disc_poly")
+    ap.add_argument("--workload", default="learned",
+                    help="learned (config 4, the headline), disc_poly or disc_small (importance-sampled solve)")
+    ap.add_argument("--no-nested", action="store_true", help="learned workload only: skip the disc_poly and forward lines")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--path", default="backward", choices=["backward", "forward"],
@@ -148,23 +157,52 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def run_ours(args):
-    import numpy as np
+def setup_ranks():
+    """rank, world, local; one process per GPU, NCCL process group for N > 1."""
     import torch
     import torch.distributed as dist
 
-    from haseongpu_b200 import DeviceMesh, build as _build
-    from haseongpu_b200.configs import WORKLOADS
+    from haseongpu_b200 import build as _build
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     _build.build_library()
+    return rank, world, local
+
+
+def teardown_ranks(world):
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    rank, world, local = setup_ranks()
+    line = measure_importance(args, local, rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    teardown_ranks(world)
+
+
+def measure_importance(args, local, rank=0, world=1, nested=False):
+    """The importance-sampled solve to the threshold on ``args.workload``
+    (default disc_poly), the plain method beside it; the contract line's
+    fields (rank 0; None elsewhere).  nested: no CPU baseline and no forward
+    measurement (the caller reports those)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from haseongpu_b200 import DeviceMesh
+    from haseongpu_b200.configs import WORKLOADS
+
+    dev = torch.device("cuda", local)
     w = WORKLOADS[args.workload]()
     mesh = w.mesh
     sa, se = w.spectra.resampled(w.monochromatic)
@@ -238,7 +276,7 @@ def run_ours(args):
                              nearFieldSampling=False, **tuned.kwargs())
     # the forward Tet4 path on the twin of the same medium (1 GPU runs only; fewer steps)
     fwd = None
-    if world == 1:
+    if world == 1 and not nested:
         import argparse as _ap
 
         fargs = _ap.Namespace(**vars(args))
@@ -268,7 +306,7 @@ def run_ours(args):
         r_l2 = l2 * 1e9 / BYTES_PER_CROSSING
         achieved = crossings / (ray_ms * 1e-3)
         roof = min(r_fp32, r_l2)
-        cpu = cpu_baseline(w, args.cpu_seconds) if world == 1 else None
+        cpu = cpu_baseline(w, args.cpu_seconds) if world == 1 and not nested else None
         h2d = mesh.numberOfPrisms * 8
         d2h = B * (4 + 8 + 8 + 4 + 8 + 4)
         line = {
@@ -317,10 +355,8 @@ def run_ours(args):
             line["cpu_baseline"] = cpu
         if fwd is not None:
             line["forward_tet4"] = fwd
-        print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    return line if rank == 0 else None
 
 
 def forward_cpu_baseline(tet, sa, se, seconds):
@@ -355,7 +391,7 @@ def measure_forward(args, local, rank=0, world=1, cpu_seconds=None):
     from haseongpu_b200 import TetDeviceMesh, TetMesh, _native
     from haseongpu_b200.configs import WORKLOADS
 
-    w = WORKLOADS[args.workload]()
+    w = WORKLOADS["disc_poly" if args.workload == "learned" else args.workload]()
     tet = TetMesh.fromPrismMesh(w.mesh)
     sa, se = w.spectra.resampled(w.monochromatic)
     dev = torch.device("cuda", local)
@@ -467,13 +503,192 @@ def run_forward(args):
         dist.destroy_process_group()
 
 
+LEARNED_METRIC = ("phi-ASE time to per-sample relative error <= threshold with the learned proposal, as sample points "
+                  "solved per second (plain importance sampling on the same fields beside it; rays/s alongside)")
+
+
+def run_learned(args):
+    """Config 4: the learned proposal on the disc_small geometry.  Untimed:
+    logging 32 seeded training fields with the importance weights and
+    training the network (Adam, device).  Timed: each step solves every
+    sample point of one unseen pump field to the threshold (rays 1e5 -> 1e6,
+    relative error 0.005) with the learned proposal; the same fields are then
+    solved with the reference's plain importance sampling (uniform start
+    points) and with the importance weights + near-field start points."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from haseongpu_b200 import DeviceMesh, _native
+    from haseongpu_b200 import learned as LP
+    from haseongpu_b200.configs import disc_small
+
+    rank, world, local = setup_ranks()
+    dev = torch.device("cuda", local)
+    w = disc_small()
+    mesh = w.mesh
+    sa, se = w.spectra.resampled(True)
+    S = mesh.numberOfSamples
+    ctx = DeviceMesh(mesh, sa, se, device=local)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MiB > 126 MB L2
+
+    t0 = time.perf_counter()
+    data = LP.training_set(ctx, LP.pump_fields(mesh, 32, LP.TRAIN_SEED))
+    t1 = time.perf_counter()
+    net, hist = LP.train_proposal(data, steps=3000, device=local)
+    t2 = time.perf_counter()
+    fields = LP.pump_fields(mesh, args.warmup + args.steps, LP.EVAL_SEED + 7919 * rank)
+    kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
+              monochromatic=True, minSample=0, maxSample=S - 1)
+
+    def solve(kind, k):
+        ctx.update_beta(fields[k])
+        if kind == "learned":
+            return ctx.calc_phi_ase_learned(net, rngSeed=3000 + k, **kw)
+        return ctx.calc_phi_ase(rngSeed=3000 + k, nearFieldSampling=(kind == "nearfield"), **kw)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        solve("learned", k)
+    barrier()
+    acc = {"learned": [], "plain": [], "nearfield": []}
+    with ClockSampler(local) as clk:
+        for kind in ("learned", "plain", "nearfield"):
+            for s_ in range(args.steps):
+                ctx.update_beta(fields[args.warmup + s_])
+                flush.zero_()
+                torch.cuda.synchronize()
+                acc[kind].append(solve(kind, args.warmup + s_))
+        barrier()
+    clocks = clk.summary()
+    # e2e: the public API with host buffers (beta upload and per-sample results read back every step)
+    barrier()
+    te = time.perf_counter()
+    for s_ in range(args.steps):
+        solve("learned", args.warmup + s_)
+    barrier()
+    e2e_s = time.perf_counter() - te
+
+    def agg(rs):
+        ms = sum(r.totalMilliseconds for r in rs)
+        return {"ms": ms, "rays": sum(r.raysTraced for r in rs), "crossings": sum(r.crossings for r in rs),
+                "ray_ms": sum(r.rayMilliseconds for r in rs), "proposal_ms": sum(r.importanceMilliseconds for r in rs),
+                "unconverged": sum(r.unconvergedSamples for r in rs), "launches": sum(r.kernelLaunches + 1 for r in rs)}
+
+    a = {k: agg(v) for k, v in acc.items()}
+    stats = torch.tensor([a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s,
+                          float(a["learned"]["rays"]), float(args.steps * S)], dtype=torch.float64, device=dev)
+    if world > 1:
+        mx, sm = stats.clone(), stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_l, ms_p, ms_n, e2e_max = float(mx[0]), float(mx[1]), float(mx[2]), float(mx[3])
+        rays_all, solved_all = float(sm[4]), float(sm[5])
+    else:
+        ms_l, ms_p, ms_n, e2e_max = a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s
+        rays_all, solved_all = float(a["learned"]["rays"]), float(args.steps * S)
+    disc_poly = fwd = None
+    if world == 1 and not args.no_nested:
+        import argparse as _ap
+
+        nargs = _ap.Namespace(**vars(args))
+        nargs.workload, nargs.samples = "disc_poly", 1024
+        nargs.steps, nargs.warmup = max(2, min(args.steps, 3)), max(args.warmup, 3)
+        disc_poly = measure_importance(nargs, local, rank, world, nested=True)
+        fwd = measure_forward(nargs, local, cpu_seconds=min(args.cpu_seconds, 6.0))
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+        r_fp32 = SMS * LANES_PER_SM * f_clk / FP32_INSTR_PER_CROSSING
+        l2 = _native.l2_bandwidth(local)
+        r_l2 = l2 * 1e9 / BYTES_PER_CROSSING
+        roof = min(r_fp32, r_l2)
+        achieved = a["learned"]["crossings"] / (a["learned"]["ray_ms"] * 1e-3)
+        rows = args.steps * S * mesh.numberOfPrisms
+        prop_tflops = rows * MLP_FLOP_PER_PAIR / (a["learned"]["proposal_ms"] * 1e-3) / 1e12
+        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        lv = np.concatenate([LP.per_ray_variance(r) for r in acc["learned"]])
+        pv = np.concatenate([LP.per_ray_variance(r) for r in acc["plain"]])
+        nv = np.concatenate([LP.per_ray_variance(r) for r in acc["nearfield"]])
+        cpu = cpu_baseline(w, args.cpu_seconds) if world == 1 else None
+        line = {
+            "metric": LEARNED_METRIC,
+            "value": solved_all / (ms_l * 1e-3),
+            "unit": "samples/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_l / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 geometry, f64 sums, bf16 proposal network (f32 accumulation)",
+            "data": "synthetic (seeded gain media and pump fields, no dataset)",
+            "config": {"workload": "learned proposal (config 4): disc_small geometry, 32 training pump fields, "
+                                   "unseen evaluation pump fields",
+                       "samples_per_step_per_gpu": S, "triangles": mesh.numberOfTriangles,
+                       "levels": mesh.numberOfLevels, "prisms": mesh.numberOfPrisms, "wavelengths": 1,
+                       "rays_per_sample": [w.minRays, w.maxRays], "threshold": w.threshold,
+                       "adaptive_steps": w.adaptiveSteps, "parallelism": f"independent fields x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "time_to_threshold_ms": ms_l / args.steps,
+            "plain_is": {"value": solved_all / (ms_p * 1e-3), "unit": "samples/s", "ms_per_step": ms_p / args.steps,
+                         "rays": a["plain"]["rays"], "unconverged_samples": a["plain"]["unconverged"],
+                         "median_per_ray_variance": float(np.median(pv)), "max_per_ray_variance": float(pv.max()),
+                         "note": "the reference's importance weights with uniform start points (legacy estimator)"},
+            "importance_nearfield": {"value": solved_all / (ms_n * 1e-3), "unit": "samples/s",
+                                     "ms_per_step": ms_n / args.steps, "rays": a["nearfield"]["rays"],
+                                     "unconverged_samples": a["nearfield"]["unconverged"],
+                                     "median_per_ray_variance": float(np.median(nv))},
+            "learned": {"rays": a["learned"]["rays"], "unconverged_samples": a["learned"]["unconverged"],
+                        "median_per_ray_variance": float(np.median(lv)), "max_per_ray_variance": float(lv.max()),
+                        "proposal_ms_per_step": a["learned"]["proposal_ms"] / args.steps,
+                        "ray_ms_per_step": a["learned"]["ray_ms"] / args.steps,
+                        "training": {"groups": data.groups, "rows": int(data.offsets[-1]),
+                                     "rays_logged": data.groups * data.rays, "log_s": t1 - t0, "train_s": t2 - t1,
+                                     "adam_steps": 3000, "loss_first_50": float(hist[:50].mean()),
+                                     "loss_last_200": float(hist[-200:].mean())},
+                        "speedup_vs_plain_is": ms_p / ms_l, "speedup_vs_importance_nearfield": ms_n / ms_l},
+            "rays_per_s": rays_all / (ms_l * 1e-3),
+            "e2e": {"value": solved_all / e2e_max, "unit": "samples/s", "h2d_bytes_per_step": mesh.numberOfPrisms * 8,
+                    "d2h_bytes_per_step": S * (4 + 8 + 8 + 4 + 8 + 4)},
+            "gpu_launches": a["learned"]["launches"],
+            "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel",
+                         "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
+                         "traffic": None, "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
+                         "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
+            "proposal_roofline": {"bound": "tensor", "kernel": "proposalKernel", "achieved": prop_tflops,
+                                  "peak": bf16, "unit": "TFLOP/s", "frac": prop_tflops / bf16,
+                                  "flop_per_pair": MLP_FLOP_PER_PAIR, "pairs": rows, "peak_source": peak_kind},
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if disc_poly is not None:
+            line["importance_disc_poly"] = {k: disc_poly[k] for k in (
+                "value", "unit", "ms_per_step", "config", "time_to_threshold_ms", "breakdown_ms_per_step",
+                "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline")}
+        if fwd is not None:
+            line["forward_tet4"] = fwd
+        print(json.dumps(line), flush=True)
+    net.close()
+    ctx.close()
+    teardown_ranks(world)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
     from haseongpu_b200.configs import WORKLOADS
 
-    w = WORKLOADS[args.workload]()
+    # the learned workload's reference: the reference's method (importance
+    # weights, uniform start points) on its geometry
+    w = WORKLOADS["disc_small" if args.workload == "learned" else args.workload]()
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
     for _ in range(args.warmup):
         cpu_baseline(w, 0.0)
@@ -481,7 +696,8 @@ def run_reference(args):
     value = statistics.median(v["value"] for v in vals)
     cores = vals[0]["cores"]
     line = {
-        "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus, "steps": args.steps,
+        "metric": LEARNED_METRIC if args.workload == "learned" else METRIC, "value": value, "unit": "samples/s",
+        "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded gain medium, no dataset)", "impl": "reference",
         "config": {"workload": w.name, "threshold": w.threshold, "reflections": w.useReflections},
@@ -499,6 +715,8 @@ def main():
         run_reference(args)
     elif args.path == "forward":
         run_forward(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 
