@@ -50,6 +50,8 @@ BYTES_PER_CROSSING = 52        # triangle record 48 B + prism beta 4 B
 SMS = 148
 LANES_PER_SM = 128
 MLP_FLOP_PER_PAIR = 2 * (12 * 64 + 64 * 64 + 64 * 64 + 64 * 1)  # 18,048 FLOP per (sample, prism) inference
+XU_INSTR_PER_PAIR = 430  # special-function (MUFU + conversion) instructions per pair: 192 SiLUs x 2 + features
+XU_LANES_PER_SM = 16
 FWD_METRIC = "forward Tet4 phi-ASE source rays traced and tallied per second on 1 B200 (crossings/s alongside)"
 FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count of the forward walk
 BYTES_PER_TET_CROSSING = 148       # cell record 128 B + beta 8 B + one vertex tally 8 B + one visit count 4 B
@@ -661,9 +663,14 @@ def run_learned(args):
                          "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
                          "traffic": None, "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
                          "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
-            "proposal_roofline": {"bound": "tensor", "kernel": "proposalKernel", "achieved": prop_tflops,
-                                  "peak": bf16, "unit": "TFLOP/s", "frac": prop_tflops / bf16,
-                                  "flop_per_pair": MLP_FLOP_PER_PAIR, "pairs": rows, "peak_source": peak_kind},
+            "proposal_roofline": {"bound": "xu", "kernel": "proposalKernel",
+                                  "achieved": rows / (a["learned"]["proposal_ms"] * 1e-3),
+                                  "peak": SMS * XU_LANES_PER_SM * f_clk / XU_INSTR_PER_PAIR, "unit": "pairs/s",
+                                  "frac": rows / (a["learned"]["proposal_ms"] * 1e-3)
+                                  / (SMS * XU_LANES_PER_SM * f_clk / XU_INSTR_PER_PAIR),
+                                  "tensor_tflops": prop_tflops, "tensor_frac_of_bf16": prop_tflops / bf16,
+                                  "flop_per_pair": MLP_FLOP_PER_PAIR, "xu_instr_per_pair": XU_INSTR_PER_PAIR,
+                                  "pairs": rows, "peak_source": peak_kind},
             "clocks": clocks,
         }
         if cpu:
