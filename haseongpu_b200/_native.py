@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "hase_philox",
     "hase_probe_l2_bandwidth",
     "hase_estimate_sample_noalloc",
+    "hase_simulate",
     # include/hase_b200_forward.h
     "hase_tet_context_create",
     "hase_tet_context_update_beta",
@@ -216,6 +217,45 @@ class LearnedDesc(C.Structure):
     ]
 
 
+class PumpDesc(C.Structure):
+    _fields_ = [
+        ("peakIntensity", C.c_double),
+        ("radius", C.c_double),
+        ("exponent", C.c_double),
+        ("centerX", C.c_double),
+        ("centerY", C.c_double),
+        ("wavelength", C.c_double),
+        ("sigmaA", C.c_double),
+        ("sigmaE", C.c_double),
+        ("retroreflect", C.c_uint32),
+    ]
+
+
+class TimeDesc(C.Structure):
+    _fields_ = [
+        ("timeStep", C.c_double),
+        ("steps", C.c_uint32),
+        ("pumpSteps", C.c_uint32),
+        ("aseSteps", C.c_uint32),
+        ("integrator", C.c_uint32),
+    ]
+
+
+class TimeResultDesc(C.Structure):
+    _fields_ = [
+        ("betaVolume", _f64p),
+        ("meanBeta", _f64p),
+        ("meanPhi", _f64p),
+        ("pumpAbsorbed", _f64p),
+        ("phiHistory", _f32p),
+        ("aseMilliseconds", C.c_double),
+        ("pumpMilliseconds", C.c_double),
+        ("totalMilliseconds", C.c_double),
+        ("raysTraced", C.c_uint64),
+        ("fallbackSamples", C.c_uint32),
+    ]
+
+
 class HaseError(RuntimeError):
     """A libhase_b200 call failed; ``status`` is the hase_status code."""
 
@@ -277,6 +317,8 @@ def lib():
         L.hase_log_contributions.argtypes = [C.c_void_p, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), _f32p,
                                              C.POINTER(ResultDesc)]
         L.hase_proposal_features.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
+        L.hase_simulate.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc),
+                                    C.POINTER(PumpDesc), C.POINTER(TimeDesc), C.POINTER(TimeResultDesc)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

@@ -850,6 +850,88 @@ __global__ void resetRowsKernel(const uint32_t* rows, uint32_t n, double* sum, d
     cross[r] = 0ull;
 }
 
+// ------------------------------------------------ time stepping ----
+// Rate equations of the excited fraction per prism (hase_simulate).
+struct PumpLaunch {
+    const float2* centroid;       // [T]
+    const double* beta;           // [P] stage beta
+    const uint8_t* clad;          // [P] 1 = cladding prism, or null
+    double* rate;                 // [P] out: d beta / dt from the pump
+    double* absorbed;             // [1] absorbed photon flux x area (first stage diagnostics), or null
+    const float* area;            // [T]
+    uint32_t T, layers;
+    double h, nTot, sA, sE, cladAbs;
+    double flux0, radius, expo, cx, cy;  // peak photon flux (1/(cm^2 s)), profile
+    int retro;
+};
+
+// One thread per triangle column: Beer-Lambert up the column (and back down
+// with retro-reflection); each layer's absorbed photons / (N_tot h).
+__global__ void pumpColumnKernel(const PumpLaunch L) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.T) return;
+    const float2 c = L.centroid[t];
+    const double r = sqrt(double(c.x - L.cx) * double(c.x - L.cx) + double(c.y - L.cy) * double(c.y - L.cy));
+    double phi = L.flux0 * exp(-pow(r / L.radius, L.expo));
+    const double phi0 = phi;
+    for (int pass = 0; pass < (L.retro ? 2 : 1); ++pass) {
+        for (uint32_t k = 0; k < L.layers; ++k) {
+            const uint32_t l = pass == 0 ? k : L.layers - 1 - k;
+            const size_t p = t + size_t(l) * L.T;
+            const bool cl = L.clad && L.clad[p];
+            const double g = cl ? -L.cladAbs : L.nTot * (L.beta[p] * (L.sA + L.sE) - L.sA);
+            const double out = phi * exp(g * L.h);
+            if (!cl) L.rate[p] += (phi - out) / (L.nTot * L.h);
+            phi = out;
+        }
+    }
+    if (L.absorbed) atomicAdd(L.absorbed, (phi0 - phi) * double(L.area[t]));
+}
+
+// Mean phi-ASE of each prism's six vertices (levels l and l + 1).
+__global__ void phiPrismKernel(const int4* verts, const float* phiSample, float* phiPrism, uint32_t T,
+                               uint32_t layers, uint32_t Np) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= T * layers) return;
+    const uint32_t t = p % T, l = p / T;
+    const int4 v = verts[t];
+    const float* a = phiSample + size_t(l) * Np;
+    const float* b = a + Np;
+    phiPrism[p] = (a[v.x] + a[v.y] + a[v.z] + b[v.x] + b[v.y] + b[v.z]) * (1.0f / 6.0f);
+}
+
+// k = pump - [beta (sE + sA) - sA] Phi - beta / tau (0 in cladding); then the
+// stage update: next = beta0 + cStage dt k, acc += wStage k.
+__global__ void rateStageKernel(const double* beta0, const double* betaStage, const double* pumpRate,
+                                const float* phiPrism, const uint8_t* clad, double* next, double* acc, uint32_t P,
+                                double sA, double sE, double tau, double dt, double cStage, double wStage,
+                                int first) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    double k = 0.0;
+    if (!(clad && clad[p])) {
+        const double b = betaStage[p];
+        k = pumpRate[p] - (b * (sE + sA) - sA) * double(phiPrism ? phiPrism[p] : 0.0f) - b / tau;
+    }
+    next[p] = beta0[p] + cStage * dt * k;
+    acc[p] = first ? wStage * k : acc[p] + wStage * k;
+}
+
+__global__ void rateFinishKernel(double* beta, const double* acc, uint32_t P, double dt) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < P) beta[p] += dt * acc[p];
+}
+
+// The context's walk / source beta from the FP64 state (NaN marks cladding in the walk table).
+__global__ void betaToTablesKernel(const double* beta, const uint8_t* clad, float* gainBeta, float* srcBeta,
+                                   uint32_t P) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const float b = float(beta[p]);
+    srcBeta[p] = b;
+    gainBeta[p] = (clad && clad[p]) ? __int_as_float(0x7fc00000) : b;
+}
+
 // -------------------------------------------------------- host side ----
 struct HostTables {
     std::vector<int4> verts;
@@ -951,6 +1033,7 @@ struct hase_context {
     // host copies used by the learned proposal's features
     std::vector<float2> hCentroid, hPoints;
     std::vector<float> hArea, hGainBeta, hReflect;
+    std::vector<double> hBeta;  // betaVolume as given (FP64)
     // learned proposal: coarse gain grid, fallback rows, contribution log
     DevBuf<float> featGrid, logBuf, priorBuf;
     DevBuf<uint32_t> rowList;
@@ -991,6 +1074,7 @@ hase_status uploadBeta(hase_context* c, const double* betaVolume) {
         gain[p] = clad ? NAN : float(b);
     }
     c->hGainBeta = gain;
+    c->hBeta.assign(betaVolume, betaVolume + c->P);
     HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->srcBeta.p, src.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
@@ -1559,6 +1643,169 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
 hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, const hase_compute_desc* cp,
                               hase_result* res) {
     return calcCore(c, ex, cp, res, nullptr, nullptr);
+}
+
+hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVariance,
+                          const hase_experiment_desc* ex, const hase_compute_desc* cp, const hase_pump_desc* pd,
+                          const hase_time_desc* td, hase_time_result* res) {
+    if (!c || !ex || !cp || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (!(td->timeStep > 0.0) || td->steps == 0) return fail(HASE_INVALID_ARGUMENT, "timeStep and steps must be positive");
+    if (td->integrator > 1) return fail(HASE_INVALID_ARGUMENT, "integrator must be 0 (frozen-ASE RK4) or 1 (Euler)");
+    if (td->aseSteps > td->steps) return fail(HASE_INVALID_ARGUMENT, "aseSteps > steps");
+    if (!(pd->radius > 0.0) || !(pd->exponent > 0.0) || !(pd->wavelength > 0.0) || !(pd->peakIntensity >= 0.0) ||
+        !(pd->sigmaA >= 0.0) || !(pd->sigmaE >= 0.0))
+        return fail(HASE_INVALID_ARGUMENT, "pump parameters must be positive (intensity and cross sections >= 0)");
+    if (!(fallbackVariance >= 0.0f)) return fail(HASE_INVALID_ARGUMENT, "fallbackVariance must be >= 0");
+    HASE_TRY(setDevice(c));
+    const uint32_t P = c->P, T = c->T, S = c->Np * c->L;
+    std::vector<uint8_t> clad(P, 0);
+    if (!c->cladTypes.empty())
+        for (uint32_t p = 0; p < P; ++p) clad[p] = c->cladTypes[p % T] == c->cladNumber ? 1 : 0;
+    DevBuf<double> beta0, stage, nextB, acc, rate, absorbed;
+    DevBuf<float> phiS, phiP, area;
+    DevBuf<uint8_t> dclad;
+    HASE_CUDA(beta0.ensure(P));
+    HASE_CUDA(stage.ensure(P));
+    HASE_CUDA(nextB.ensure(P));
+    HASE_CUDA(acc.ensure(P));
+    HASE_CUDA(rate.ensure(P));
+    HASE_CUDA(absorbed.ensure(1));
+    HASE_CUDA(phiS.ensure(S));
+    HASE_CUDA(phiP.ensure(P));
+    HASE_CUDA(area.ensure(T));
+    HASE_CUDA(dclad.ensure(P));
+    HASE_CUDA(cudaMemcpyAsync(beta0.p, c->hBeta.data(), P * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(area.p, c->hArea.data(), T * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    HASE_CUDA(cudaMemcpyAsync(dclad.p, clad.data(), P, cudaMemcpyHostToDevice, c->stream));
+    const uint32_t nL = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double sA = c->sigmaA[0], sE = c->sigmaE[0];
+    if (nL > 1)
+        for (uint32_t l = 1; l < nL; ++l) {
+            sA = std::max(sA, c->sigmaA[l]);
+            sE = std::max(sE, c->sigmaE[l]);
+        }
+    const double photon = 6.62607015e-34 * 2.99792458e8 / pd->wavelength;  // J
+    PumpLaunch pl{};
+    pl.centroid = c->centroid.p;
+    pl.clad = dclad.p;
+    pl.rate = rate.p;
+    pl.area = area.p;
+    pl.T = T;
+    pl.layers = c->layers;
+    pl.h = c->h;
+    pl.nTot = c->nTot;
+    pl.sA = pd->sigmaA;
+    pl.sE = pd->sigmaE;
+    pl.cladAbs = c->cladAbs;
+    pl.flux0 = pd->peakIntensity / photon;
+    pl.radius = pd->radius;
+    pl.expo = pd->exponent;
+    pl.cx = pd->centerX;
+    pl.cy = pd->centerY;
+    pl.retro = pd->retroreflect ? 1 : 0;
+    double incident = 0.0;  // photons / s entering the bottom surface
+    for (uint32_t t = 0; t < T; ++t) {
+        const double dx = c->hCentroid[t].x - pd->centerX, dy = c->hCentroid[t].y - pd->centerY;
+        incident += pl.flux0 * std::exp(-std::pow(std::sqrt(dx * dx + dy * dy) / pd->radius, pd->exponent)) *
+                    c->hArea[t];
+    }
+    hase_compute_desc all = *cp;
+    all.minSample = 0;
+    all.maxSample = UINT32_MAX;
+    std::vector<float> phiHost(S);
+    std::vector<double> betaHost(P);
+    LearnedArgs la{net, 0.1f, fallbackVariance, 0u};
+    res->aseMilliseconds = res->pumpMilliseconds = res->totalMilliseconds = 0.0;
+    res->raysTraced = 0;
+    res->fallbackSamples = 0;
+    auto meanGain = [&](const std::vector<double>& b) {
+        double sum = 0.0;
+        uint32_t n = 0;
+        for (uint32_t p = 0; p < P; ++p)
+            if (!clad[p]) {
+                sum += b[p];
+                ++n;
+            }
+        return n ? sum / n : 0.0;
+    };
+    if (res->meanBeta) res->meanBeta[0] = meanGain(c->hBeta);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    HASE_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(HASE_CUDA_ERROR, "event creation failed");
+    }
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evs{e0, e1};
+    const uint32_t blocksP = (P + 255) / 256, blocksT = (T + 255) / 256;
+    const double dt = td->timeStep;
+    hase_status worst = HASE_OK;
+    for (uint32_t step = 0; step < td->steps; ++step) {
+        const bool ase = step < td->aseSteps, pumpOn = step < td->pumpSteps;
+        if (ase) {
+            hase_result r{};
+            r.phiAse = phiHost.data();
+            const hase_status st = calcCore(c, ex, &all, &r, net ? &la : nullptr, nullptr);
+            if (st != HASE_OK && st != HASE_NOT_CONVERGED && st != HASE_DROPPED_RAYS) return st;
+            if (st != HASE_OK && worst == HASE_OK) worst = st;
+            res->aseMilliseconds += r.totalMilliseconds;
+            res->totalMilliseconds += r.totalMilliseconds;
+            res->raysTraced += r.raysTraced;
+            if (net) res->fallbackSamples += la.fallbackSamples;
+            double mp = 0.0;
+            for (uint32_t k = 0; k < S; ++k) mp += phiHost[k];
+            if (res->meanPhi) res->meanPhi[step] = mp / S;
+            if (res->phiHistory) std::copy(phiHost.begin(), phiHost.end(), res->phiHistory + size_t(step) * S);
+            HASE_CUDA(cudaMemcpyAsync(phiS.p, phiHost.data(), S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+            phiPrismKernel<<<blocksP, 256, 0, c->stream>>>(c->verts.p, phiS.p, phiP.p, T, c->layers, c->Np);
+        } else if (res->meanPhi) {
+            res->meanPhi[step] = 0.0;
+        }
+        HASE_CUDA(cudaEventRecord(e0, c->stream));
+        HASE_CUDA(cudaMemsetAsync(absorbed.p, 0, sizeof(double), c->stream));
+        const int stages = td->integrator == 0 ? 4 : 1;
+        const double cNext[4] = {0.5, 0.5, 1.0, 0.0};
+        const double wStage[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+        const double* cur = beta0.p;
+        for (int sIdx = 0; sIdx < stages; ++sIdx) {
+            HASE_CUDA(cudaMemsetAsync(rate.p, 0, P * sizeof(double), c->stream));
+            if (pumpOn) {
+                pl.beta = cur;
+                pl.absorbed = sIdx == 0 ? absorbed.p : nullptr;
+                pumpColumnKernel<<<blocksT, 256, 0, c->stream>>>(pl);
+            }
+            double* out = (sIdx % 2 == 0) ? stage.p : nextB.p;
+            rateStageKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, cur, rate.p, ase ? phiP.p : nullptr, dclad.p, out,
+                                                         acc.p, P, sA, sE, c->tau, dt, cNext[sIdx],
+                                                         stages == 1 ? 1.0 : wStage[sIdx], sIdx == 0 ? 1 : 0);
+            cur = out;
+        }
+        rateFinishKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, acc.p, P, dt);
+        betaToTablesKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, dclad.p, c->gainBeta.p, c->srcBeta.p, P);
+        HASE_CUDA(cudaGetLastError());
+        HASE_CUDA(cudaEventRecord(e1, c->stream));
+        double abs = 0.0;
+        HASE_CUDA(cudaMemcpyAsync(&abs, absorbed.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaMemcpyAsync(betaHost.data(), beta0.p, P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaStreamSynchronize(c->stream));
+        float ms = 0.0f;
+        HASE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        res->pumpMilliseconds += ms;
+        res->totalMilliseconds += ms;
+        if (res->pumpAbsorbed) res->pumpAbsorbed[step] = pumpOn && incident > 0.0 ? abs / incident : 0.0;
+        // host copies the next solve's features read
+        c->hBeta = betaHost;
+        for (uint32_t p = 0; p < P; ++p) c->hGainBeta[p] = clad[p] ? NAN : float(betaHost[p]);
+        if (res->meanBeta) res->meanBeta[step + 1] = meanGain(betaHost);
+    }
+    if (res->betaVolume) std::copy(betaHost.begin(), betaHost.end(), res->betaVolume);
+    if (worst != HASE_OK) return fail(worst, "a phi-ASE solve of the time loop ended with a warning");
+    return HASE_OK;
 }
 
 hase_status hase_calc_phi_ase_learned(hase_context* c, hase_proposal* net, const hase_experiment_desc* ex,

@@ -165,6 +165,36 @@ class DeviceMesh:
                                                         N.ptr(contrib, N._f32p), C.byref(r)), allow_warnings=True)
         return self._fill(out, r, status), contrib
 
+    def simulate(self, *, pump, time, net=None, fallbackVariance=0.0, minRays, maxRays=None, mseThreshold=0.0,
+                 useReflections=False, monochromatic=False, nearFieldSampling=True, adaptiveSteps=0, rngSeed=5489,
+                 keepPhi=False) -> dict:
+        """Time-stepped rate equations (hase_simulate): `pump` and `time` are
+        dicts with the fields of hase_pump_desc / hase_time_desc.  The
+        context's beta is advanced in place."""
+        _, ex, cp, _, _ = self._descs(minRays, maxRays, mseThreshold, useReflections, monochromatic, nearFieldSampling,
+                                      adaptiveSteps, 1, rngSeed, 0, None, 0, 0, 0, 0, 0)
+        pd = N.PumpDesc(float(pump["peakIntensity"]), float(pump["radius"]), float(pump["exponent"]),
+                        float(pump.get("centerX", 0.0)), float(pump.get("centerY", 0.0)), float(pump["wavelength"]),
+                        float(pump["sigmaA"]), float(pump["sigmaE"]), 1 if pump.get("retroreflect", True) else 0)
+        steps = int(time["steps"])
+        td = N.TimeDesc(float(time["timeStep"]), steps, int(time.get("pumpSteps", steps)),
+                        int(time.get("aseSteps", steps)), int(time.get("integrator", 0)))
+        P, S = self.mesh.numberOfPrisms, self.mesh.numberOfSamples
+        out = {"betaVolume": np.empty(P), "meanBeta": np.empty(steps + 1), "meanPhi": np.empty(steps),
+               "pumpAbsorbed": np.empty(steps)}
+        if keepPhi:
+            out["phiHistory"] = np.empty((td.aseSteps, S), np.float32)
+        r = N.TimeResultDesc(N.ptr(out["betaVolume"], N._f64p), N.ptr(out["meanBeta"], N._f64p),
+                             N.ptr(out["meanPhi"], N._f64p), N.ptr(out["pumpAbsorbed"], N._f64p),
+                             N.ptr(out.get("phiHistory"), N._f32p))
+        out["status"] = N.check(N.lib().hase_simulate(self.handle, net.handle if net is not None else None,
+                                                      float(fallbackVariance), C.byref(ex), C.byref(cp), C.byref(pd),
+                                                      C.byref(td), C.byref(r)), allow_warnings=True)
+        out.update(aseMilliseconds=r.aseMilliseconds, pumpMilliseconds=r.pumpMilliseconds,
+                   totalMilliseconds=r.totalMilliseconds, raysTraced=int(r.raysTraced),
+                   fallbackSamples=int(r.fallbackSamples))
+        return out
+
     def proposal_features(self, firstSample, count, useReflections=False, monochromatic=False) -> np.ndarray:
         slices = 5 if useReflections else 1
         f = np.empty((int(count), slices * self.mesh.numberOfPrisms, N.PROPOSAL_FEATURES), np.float32)

@@ -182,6 +182,62 @@ hase_status hase_estimate_sample_noalloc(hase_context* ctx, uint32_t sample, con
                                          uint32_t rngSeed, uint32_t useReflections, uint32_t nearFieldSampling,
                                          double* deviceResult);
 
+/* ---- time-stepped rate equations (pump pulse, fluorescence, ASE) ----
+ * Replaces the reference's compiled time loop, hase::core time-stepped
+ * simulation (include/core/timeSteppedSimulation.hpp:132-617, stages
+ * include/kernels/timeIntegrationUpdateKernels.hpp:21-127, derivative
+ * include/kernels/derivativeComposition.hpp:27-93), on the prism mesh:
+ *   d beta/dt = pump(beta) - [beta (sigma_e + sigma_a) - sigma_a] Phi - beta / tau
+ * per gain prism (cladding prisms keep their beta), Phi the prism's mean
+ * phi-ASE over its six vertices, the ASE cross sections the first pair
+ * (monochromatic) or the largest pair.  The pump is a collimated
+ * super-Gaussian beam entering the bottom surface along +z (the reference
+ * example's SurfacePumpInjector with a collimated angular distribution),
+ * optionally retro-reflected at the top: per triangle column an exact
+ * Beer-Lambert integration with g_p = N_tot [beta (sigma_a + sigma_e) -
+ * sigma_a] at the pump wavelength, absorbed photons / (N_tot h) per layer
+ * (cladding prisms attenuate with claddingAbsorption). */
+typedef struct {
+    double peakIntensity;       /* W/cm^2 at the profile centre */
+    double radius;              /* super-Gaussian radius (cm) */
+    double exponent;            /* super-Gaussian exponent */
+    double centerX;             /* profile centre (cm) */
+    double centerY;
+    double wavelength;          /* pump wavelength (m): photon energy h c / lambda */
+    double sigmaA;              /* pump cross sections (cm^2) */
+    double sigmaE;
+    uint32_t retroreflect;      /* 1: the beam returns down from the top surface */
+} hase_pump_desc;
+
+typedef struct {
+    double timeStep;            /* s */
+    uint32_t steps;             /* simulation steps */
+    uint32_t pumpSteps;         /* steps with the pump on, from the first */
+    uint32_t aseSteps;          /* steps with a phi-ASE solve, from the first (0: pump and fluorescence only) */
+    uint32_t integrator;        /* 0: RK4 with the step's phi-ASE frozen (FrozenPhiAseRungeKutta4), 1: explicit Euler */
+} hase_time_desc;
+
+typedef struct {
+    double* betaVolume;         /* out [prisms] beta after the last step, or NULL */
+    double* meanBeta;           /* out [steps + 1] mean beta of the gain prisms, or NULL */
+    double* meanPhi;            /* out [steps] mean phi-ASE of the samples (0 without a solve), or NULL */
+    double* pumpAbsorbed;       /* out [steps] absorbed fraction of the pump power (first stage), or NULL */
+    float* phiHistory;          /* out [aseSteps][samples] phi-ASE of every solve, or NULL */
+    double aseMilliseconds;     /* device time of the phi-ASE solves */
+    double pumpMilliseconds;    /* device time of pump, derivative and stage kernels */
+    double totalMilliseconds;
+    uint64_t raysTraced;
+    uint32_t fallbackSamples;
+} hase_time_result;
+
+/* `proposal` (hase_b200_proposal.h): NULL solves with the importance
+ * weights; otherwise with the learned proposal (its fallback limit
+ * `fallbackVariance`).  The context's beta is advanced in place. */
+struct hase_proposal;
+hase_status hase_simulate(hase_context* ctx, struct hase_proposal* proposal, float fallbackVariance,
+                          const hase_experiment_desc* experiment, const hase_compute_desc* compute,
+                          const hase_pump_desc* pump, const hase_time_desc* time, hase_time_result* result);
+
 /* Measurement support (no reference counterpart): L2 read bandwidth of
  * `device` in GB/s, from `reps` passes over an L2-resident buffer of `bytes`. */
 hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, double* gbPerSecond);

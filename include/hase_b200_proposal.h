@@ -72,7 +72,9 @@ typedef struct {
     uint32_t steps;              /* Adam steps */
     uint32_t groupsPerStep;      /* step s uses groups [k G', (k+1) G'), k = s mod (groups / G') */
     float learningRate;
-    float beta1, beta2, epsilon; /* 0 = 0.9, 0.999, 1e-8 */
+    float beta1;                 /* Adam moments; 0 = 0.9 */
+    float beta2;                 /* 0 = 0.999 */
+    float epsilon;               /* 0 = 1e-8 */
 } hase_proposal_train_desc;
 
 /* Loss and gradient (HASE_PROPOSAL_PARAMS floats, master-vector order) of the

@@ -1,0 +1,100 @@
+"""CPU restatement of the time-stepped rate equations of hase_simulate
+(TEST INFRASTRUCTURE ONLY: the product never imports this file).
+
+Per gain prism (include/kernels/derivativeComposition.hpp:27-93):
+    d beta/dt = pump(beta) - [beta (sE + sA) - sA] Phi - beta / tau,
+cladding prisms keep their beta.  Phi of a prism is the mean phi-ASE of its
+six vertices (float32, as the device).  Pump: a collimated super-Gaussian
+beam entering the bottom along +z, optionally retro-reflected at the top;
+per triangle column Beer-Lambert with g_p = N_tot [beta (sA_p + sE_p) - sA_p]
+per layer, absorbed photons / (N_tot h) (cladding prisms attenuate with
+claddingAbsorption and gain nothing).  Integration: RK4 with the step's
+phi-ASE frozen (the reference's FrozenPhiAseRungeKutta4,
+include/kernels/timeIntegrationUpdateKernels.hpp:21-127) or explicit Euler.
+The phi-ASE of each solve comes from the caller (the device's phiHistory),
+so both integrate the same ASE term.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+PLANCK = 6.62607015e-34
+LIGHT = 2.99792458e8
+
+
+def pump_rate(mesh, beta, pump, clad):
+    """d beta / dt from the pump, [P]; and absorbed photons / s."""
+    T, L = mesh.numberOfTriangles, mesh.numberOfLevels - 1
+    cen = mesh.points[mesh.triangles].mean(axis=1)
+    a = mesh.points[mesh.triangles]
+    area = 0.5 * np.abs((a[:, 1, 0] - a[:, 0, 0]) * (a[:, 2, 1] - a[:, 0, 1])
+                        - (a[:, 1, 1] - a[:, 0, 1]) * (a[:, 2, 0] - a[:, 0, 0]))
+    area = area.astype(np.float32).astype(np.float64)
+    cen = cen.astype(np.float32).astype(np.float64)
+    flux0 = pump["peakIntensity"] / (PLANCK * LIGHT / pump["wavelength"])
+    r = np.hypot(cen[:, 0] - pump["centerX"], cen[:, 1] - pump["centerY"])
+    phi = flux0 * np.exp(-(r / pump["radius"]) ** pump["exponent"])
+    phi0 = phi.copy()
+    h, nTot = mesh.thickness, mesh.nTot
+    b = np.asarray(beta, np.float64).reshape(L, T)
+    cl = np.asarray(clad, bool).reshape(L, T)
+    rate = np.zeros((L, T))
+    order = list(range(L)) + (list(range(L - 1, -1, -1)) if pump["retroreflect"] else [])
+    for l in order:
+        g = np.where(cl[l], -mesh.claddingAbsorption, nTot * (b[l] * (pump["sigmaA"] + pump["sigmaE"]) - pump["sigmaA"]))
+        out = phi * np.exp(g * h)
+        rate[l] += np.where(cl[l], 0.0, (phi - out) / (nTot * h))
+        phi = out
+    return rate.ravel(), float(((phi0 - phi) * area).sum()), float((phi0 * area).sum())
+
+
+def prism_phi(mesh, phi_samples):
+    T, L, Np = mesh.numberOfTriangles, mesh.numberOfLevels - 1, mesh.numberOfPoints
+    ps = np.asarray(phi_samples, np.float32).reshape(mesh.numberOfLevels, Np)
+    tri = mesh.triangles.astype(np.int64)
+    out = np.empty((L, T), np.float32)
+    for l in range(L):
+        a, b = ps[l][tri], ps[l + 1][tri]
+        s = a[:, 0] + a[:, 1] + a[:, 2] + b[:, 0] + b[:, 1] + b[:, 2]
+        out[l] = s * np.float32(1.0 / 6.0)
+    return out.ravel()
+
+
+def simulate(mesh, beta0, *, pump, time, sigma_ase, phi_history=None):
+    """beta after every step ([steps + 1][P]) and the absorbed pump fraction per step."""
+    sA, sE = sigma_ase
+    P = mesh.numberOfPrisms
+    clad = np.zeros(P, bool)
+    if mesh.claddingCellTypes is not None:
+        clad = np.tile(mesh.claddingCellTypes == mesh.claddingNumber, mesh.numberOfLevels - 1)
+    beta = np.asarray(beta0, np.float64).copy()
+    hist = [beta.copy()]
+    absorbed = []
+    dt, tau = time["timeStep"], mesh.crystalTFluo
+    for step in range(time["steps"]):
+        ase = step < time["aseSteps"]
+        pump_on = step < time["pumpSteps"]
+        phi_p = prism_phi(mesh, phi_history[step]).astype(np.float64) if ase else np.zeros(P)
+
+        def deriv(b, first=False):
+            rate = np.zeros(P)
+            if pump_on:
+                rate, absd, inc = pump_rate(mesh, b, pump, clad)
+                if first:
+                    absorbed.append(absd / inc if inc > 0 else 0.0)
+            k = rate - (b * (sE + sA) - sA) * phi_p - b / tau
+            return np.where(clad, 0.0, k)
+
+        if not pump_on:
+            absorbed.append(0.0)
+        if time["integrator"] == 0:
+            k1 = deriv(beta, True)
+            k2 = deriv(beta + 0.5 * dt * k1)
+            k3 = deriv(beta + 0.5 * dt * k2)
+            k4 = deriv(beta + dt * k3)
+            beta = beta + dt * (k1 / 6 + k2 / 3 + k3 / 3 + k4 / 6)
+        else:
+            beta = beta + dt * deriv(beta, True)
+        hist.append(beta.copy())
+    return np.array(hist), np.array(absorbed)

@@ -44,7 +44,10 @@ def test_structures_match_header(native):
     for cname, pyt in [("hase_mesh_desc", native.MeshDesc), ("hase_spectrum_desc", native.SpectrumDesc),
                        ("hase_experiment_desc", native.ExperimentDesc), ("hase_compute_desc", native.ComputeDesc),
                        ("hase_result", native.ResultDesc), ("hase_tet_mesh_desc", native.TetMeshDesc),
-                       ("hase_forward_desc", native.ForwardDesc), ("hase_forward_result", native.ForwardResultDesc)]:
+                       ("hase_forward_desc", native.ForwardDesc), ("hase_forward_result", native.ForwardResultDesc),
+                       ("hase_pump_desc", native.PumpDesc), ("hase_time_desc", native.TimeDesc),
+                       ("hase_time_result", native.TimeResultDesc), ("hase_proposal_batch", native.ProposalBatch),
+                       ("hase_proposal_train_desc", native.ProposalTrainDesc), ("hase_learned_desc", native.LearnedDesc)]:
         body = re.search(r"typedef struct \{([^{}]*)\}\s*" + cname + ";", text).group(1)
         fields = re.findall(r"\b(\w+);", re.sub(r"/\*.*?\*/", "", body, flags=re.S))
         assert fields == [f for f, _ in pyt._fields_], cname

@@ -1,0 +1,87 @@
+"""GPU parity of the time-stepped rate equations (hase_simulate) against the
+CPU restatement oracle/time_oracle.py.
+
+The device integrates in FP64 like the oracle; they differ by the last bits
+of exp / pow on the two sides (pump) and by nothing else, so beta agrees to
+~1e-12 relative without ASE.  With ASE the oracle replays the device's phi-ASE
+of every solve (phiHistory), and beta agrees to ~1e-9.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import legacy_mesh
+
+pytestmark = pytest.mark.gpu
+
+PUMP = dict(peakIntensity=16e3, radius=2.5, exponent=40.0, centerX=0.0, centerY=0.0, wavelength=940e-9,
+            sigmaA=0.8e-20, sigmaE=0.16e-20, retroreflect=True)
+
+
+def _ctx(mesh, sa, se):
+    from haseongpu_b200 import DeviceMesh, build
+
+    build.build_library()
+    return DeviceMesh(mesh, sa, se, device=0)
+
+
+def _cladding_mesh():
+    """The true-cladding disc (cladding ring, absorption 5.5 / cm) at 1030 nm."""
+    return legacy_mesh("true_cladding", claddingAbsorption=5.5), [5e-21], [1e-20]
+
+
+def test_pump_and_fluorescence_match_oracle():
+    from oracle import time_oracle as to
+
+    mesh, sa, se = _cladding_mesh()
+    beta0 = mesh.betaVolume.copy()
+    time = dict(timeStep=2e-5, steps=12, pumpSteps=8, aseSteps=0, integrator=0)
+    with _ctx(mesh, sa, se) as ctx:
+        out = ctx.simulate(pump=PUMP, time=time, minRays=1000, monochromatic=True)
+    hist, absorbed = to.simulate(mesh, beta0, pump=PUMP, time=time, sigma_ase=(sa[0], se[0]))
+    np.testing.assert_allclose(out["betaVolume"], hist[-1], rtol=1e-11, atol=1e-14)
+    gain = ~np.tile(mesh.claddingCellTypes == mesh.claddingNumber, mesh.numberOfLevels - 1)
+    np.testing.assert_allclose(out["meanBeta"], hist[:, gain].mean(axis=1), rtol=1e-11)
+    np.testing.assert_allclose(out["pumpAbsorbed"], absorbed, rtol=1e-9, atol=1e-15)
+    assert out["meanBeta"][8] > out["meanBeta"][0]          # the pump excites
+    assert np.all(np.diff(out["meanBeta"][9:]) < 0)         # then the excitation decays
+    np.testing.assert_array_equal(out["betaVolume"][~gain], beta0[~gain])  # cladding keeps its beta
+
+
+def test_decay_without_pump_is_exponential():
+    mesh, sa, se = _cladding_mesh()
+    time = dict(timeStep=2e-5, steps=5, pumpSteps=0, aseSteps=0, integrator=0)
+    with _ctx(mesh, sa, se) as ctx:
+        out = ctx.simulate(pump=PUMP, time=time, minRays=1000, monochromatic=True)
+    ratio = out["meanBeta"][1:] / out["meanBeta"][:-1]
+    np.testing.assert_allclose(ratio, np.exp(-2e-5 / mesh.crystalTFluo), rtol=1e-10)
+
+
+@pytest.mark.parametrize("integrator", [0, 1])
+def test_ase_steps_replay_the_oracle(integrator):
+    from oracle import time_oracle as to
+
+    mesh, sa, se = _cladding_mesh()
+    beta0 = mesh.betaVolume.copy()
+    time = dict(timeStep=2e-5, steps=3, pumpSteps=3, aseSteps=2, integrator=integrator)
+    with _ctx(mesh, sa, se) as ctx:
+        out = ctx.simulate(pump=PUMP, time=time, minRays=4000, monochromatic=True, keepPhi=True)
+    assert out["phiHistory"].shape == (2, mesh.numberOfSamples) and np.all(out["phiHistory"] > 0)
+    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=time, sigma_ase=(sa[0], se[0]),
+                          phi_history=out["phiHistory"])
+    np.testing.assert_allclose(out["betaVolume"], hist[-1], rtol=1e-9, atol=1e-14)
+    assert out["raysTraced"] == 2 * 4000 * mesh.numberOfSamples
+    assert out["meanPhi"][2] == 0.0 and out["meanPhi"][0] > 0
+
+
+def test_learned_proposal_in_the_time_loop():
+    from haseongpu_b200.proposal import ProposalNet
+
+    mesh, sa, se = _cladding_mesh()
+    time = dict(timeStep=2e-5, steps=2, pumpSteps=2, aseSteps=2, integrator=0)
+    with _ctx(mesh, sa, se) as ctx, ProposalNet(seed=3) as net:
+        out = ctx.simulate(pump=PUMP, time=time, net=net, fallbackVariance=1e9, minRays=4000, monochromatic=True)
+    assert np.all(np.isfinite(out["betaVolume"])) and out["fallbackSamples"] == 0
+    assert out["meanPhi"][0] > 0 and out["meanBeta"][2] > out["meanBeta"][0]
