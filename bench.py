@@ -66,9 +66,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="learned",
-                    help="learned (config 4, the headline), disc_poly or disc_small (importance-sampled solve)")
+                    help="learned (config 4, the headline), media64 (config 3, batched media), disc_poly or "
+                         "disc_small (importance-sampled solve)")
     ap.add_argument("--no-nested", action="store_true", help="learned workload only: skip the disc_poly and forward lines")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
+    ap.add_argument("--media-samples", type=int, default=128,
+                    help="media64 workload: sample points per medium (64 media) per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--path", default="backward", choices=["backward", "forward"],
                     help="backward: importance-sampled prism method (headline); forward: Tet4 source-ray method")
@@ -505,6 +508,151 @@ def run_forward(args):
         dist.destroy_process_group()
 
 
+MEDIA_METRIC = ("batched phi-ASE over 64 independent gain media (config 3) to per-sample relative error <= threshold "
+                "on 1 B200, as sample points solved per second (rays/s alongside; the same media solved one after "
+                "another beside it)")
+
+
+def measure_media(args, local, steps, warmup):
+    """Config 3: 64 seeded media (triangles 200..20,000, levels 5..40, 1..8
+    wavelengths), a seeded block of ``--media-samples`` sample points per
+    medium, rays 1e4 -> 1e7, relative error 0.001, near-field start points.
+    Timed: the batched solve (one graph: pooled importance, one persistent ray
+    launch per pass over all media).  Beside it: the same media solved one
+    after another (identical rays and results, host-driven passes)."""
+    import numpy as np
+    import torch
+
+    from haseongpu_b200 import DeviceMesh, MediaBatch, _native
+    from haseongpu_b200.autotune import autotune_batch
+    from haseongpu_b200.batch import solve_sequential
+    from haseongpu_b200.configs import media64
+
+    w = media64()
+    ctxs = [DeviceMesh(m.mesh, *m.spectra.resampled(False), device=local) for m in w.media]
+    rng = np.random.default_rng(5)
+    K = args.media_samples
+    items = []
+    for c in ctxs:
+        S = c.mesh.numberOfSamples
+        lo = int(rng.integers(0, max(1, S - K)))
+        items.append((c, lo, min(S - 1, lo + K - 1)))
+    rows = sum(hi - lo + 1 for _, lo, hi in items)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=torch.device("cuda", local))
+    ws = 32 << 30
+    batch = MediaBatch(local)
+    tune = autotune_batch(batch, items, rays=20_000, workspaceBytes=ws)
+    kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
+              monochromatic=False, workspaceBytes=ws, rayKernelVariant=tune.rayKernelVariant,
+              raysPerThread=tune.raysPerThread)
+    for k in range(warmup):
+        batch.solve(items, rngSeed=100 + 64 * k, **kw)
+    torch.cuda.synchronize()
+    bt, st_all, wall_b = [], [], 0.0
+    with ClockSampler(local) as clk:
+        for s_ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res, st = batch.solve(items, rngSeed=1000 + 64 * s_, **kw)
+            wall_b += time.perf_counter() - t0
+            bt.append(res)
+            st_all.append(st)
+    clocks = clk.summary()
+    seq_ms, wall_s = 0.0, 0.0
+    for s_ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seq = solve_sequential(items, rngSeed=1000 + 64 * s_, **kw)
+        wall_s += time.perf_counter() - t0
+        seq_ms += sum(r.totalMilliseconds for r in seq)
+        same = all(np.array_equal(a.phiAse, b.phiAse) for a, b in zip(bt[s_], seq))
+    # e2e: beta of every medium uploaded from host and every result read back, each step
+    betas = [c.mesh.betaVolume for c in ctxs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s_ in range(steps):
+        for c, b in zip(ctxs, betas):
+            c.update_beta(b)
+        batch.solve(items, rngSeed=1000 + 64 * s_, **kw)
+    e2e_s = time.perf_counter() - t0
+    ms = sum(st.totalMilliseconds for st in st_all)
+    ray_ms = sum(st.rayMilliseconds for st in st_all)
+    rays = sum(st.raysTraced for st in st_all)
+    cross = sum(st.crossings for st in st_all)
+    peaks, peak_kind = measured_peaks()
+    f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    r_fp32 = SMS * LANES_PER_SM * f_clk / FP32_INSTR_PER_CROSSING
+    l2 = _native.l2_bandwidth(local)
+    r_l2 = l2 * 1e9 / BYTES_PER_CROSSING
+    roof = min(r_fp32, r_l2)
+    per_ray = np.concatenate([r.totalRays.astype(np.int64) for r in bt[-1]])
+    out = {
+        "value": steps * rows / (ms * 1e-3), "unit": "samples/s", "ms_per_step": ms / steps,
+        "rays_per_s": rays / (ms * 1e-3), "crossings_per_s": cross / (ray_ms * 1e-3),
+        "config": {"workload": "media64 (config 3): 64 seeded gain media in one batched solve",
+                   "media": len(ctxs), "samples_per_medium": K, "samples_per_step": rows,
+                   "triangles": [min(c.mesh.numberOfTriangles for c in ctxs),
+                                 max(c.mesh.numberOfTriangles for c in ctxs)],
+                   "levels": [min(c.mesh.numberOfLevels for c in ctxs), max(c.mesh.numberOfLevels for c in ctxs)],
+                   "prisms_total": sum(c.mesh.numberOfPrisms for c in ctxs),
+                   "wavelengths": [m.wavelengths for m in w.media], "rays_per_sample": [w.minRays, w.maxRays],
+                   "threshold": w.threshold, "adaptive_steps": w.adaptiveSteps,
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "ray_kernel": {"variant": tune.name, "rays_per_lane": tune.raysPerThread,
+                                  "autotuned_over": len(tune.table)}},
+        "breakdown_ms_per_step": {"importance": sum(st.importanceMilliseconds for st in st_all) / steps,
+                                  "map_ray_finalise_passes": ray_ms / steps,
+                                  "graph_capture_host": sum(st.captureMilliseconds for st in st_all) / steps},
+        "rays_per_sample": {"min": int(per_ray.min()), "median": float(np.median(per_ray)), "max": int(per_ray.max())},
+        "passes": max(st.passes for st in st_all),
+        "unconverged_samples": sum(st.unconvergedSamples for st in st_all),
+        "graph": {"kernels": st_all[-1].kernelLaunches, "nodes": st_all[-1].graphNodes, "chunks": st_all[-1].chunks},
+        "sequential": {"value": steps * rows / (seq_ms * 1e-3), "unit": "samples/s", "ms_per_step": seq_ms / steps,
+                       "wall_ms_per_step": wall_s * 1e3 / steps, "identical_results": bool(same),
+                       "note": "the same media, one calc_phi_ase per medium (host-synchronised passes)"},
+        "speedup_vs_sequential": seq_ms / ms,
+        "wall_ms_per_step": wall_b * 1e3 / steps,
+        "e2e": {"value": steps * rows / e2e_s, "unit": "samples/s",
+                "h2d_bytes_per_step": sum(c.mesh.numberOfPrisms * 8 for c in ctxs),
+                "d2h_bytes_per_step": rows * (4 + 8 + 8 + 4 + 8 + 4)},
+        "gpu_launches": sum(st.kernelLaunches for st in st_all),
+        "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel (pooled)",
+                     "achieved": cross / (ray_ms * 1e-3), "peak": roof, "unit": "crossings/s",
+                     "frac": cross / (ray_ms * 1e-3) / roof, "traffic": None, "peak_source": peak_kind,
+                     "note": "ray time includes the map and finalise launches of every pass"},
+        "clocks": clocks,
+    }
+    batch.close()
+    for c in ctxs:
+        c.close()
+    return out
+
+
+def run_media(args):
+    """Config 3 on its own line; with N ranks every rank solves its own copy
+    of the 64 media (replicas), timed as the maximum over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = setup_ranks()
+    m = measure_media(args, local, args.steps, args.warmup)
+    ms = torch.tensor([m["ms_per_step"]], dtype=torch.float64, device=torch.device("cuda", local))
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms[0])
+    if rank == 0:
+        rows = m["config"]["samples_per_step"]
+        line = {"metric": MEDIA_METRIC, "value": world * rows / (ms_max * 1e-3), "unit": "samples/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 geometry, f64 sums", "data": "synthetic (seeded gain media, no dataset)"}
+        line.update({k: v for k, v in m.items() if k not in ("value", "ms_per_step")})
+        print(json.dumps(line), flush=True)
+    teardown_ranks(world)
+
+
 LEARNED_METRIC = ("phi-ASE time to per-sample relative error <= threshold with the learned proposal, as sample points "
                   "solved per second (plain importance sampling on the same fields beside it; rays/s alongside)")
 
@@ -724,6 +872,8 @@ def main():
         run_forward(args)
     elif args.workload == "learned":
         run_learned(args)
+    elif args.workload == "media64":
+        run_media(args)
     else:
         run_ours(args)
 

@@ -7,12 +7,13 @@ include/hase_b200.h and include/hase_b200_forward.h); this package is its host
 front end, mirroring the reference's ``PhiASE`` / ``Result`` call surface.
 """
 
+from .batch import MediaBatch
 from .forward import TetDeviceMesh
 from .mesh import PrismMesh
 from .simulation import DeviceMesh, PhiASE, Result
 from .spectra import CrossSectionData, interpolate_linear
 from .tetmesh import TetMesh
 
-__all__ = ["PrismMesh", "TetMesh", "DeviceMesh", "TetDeviceMesh", "PhiASE", "Result", "CrossSectionData",
+__all__ = ["PrismMesh", "TetMesh", "DeviceMesh", "TetDeviceMesh", "MediaBatch", "PhiASE", "Result", "CrossSectionData",
            "interpolate_linear"]
 __version__ = "0.1.0"

@@ -62,6 +62,10 @@ EXPORTED_SYMBOLS = (
     "hase_calc_phi_ase_learned",
     "hase_log_contributions",
     "hase_proposal_features",
+    # include/hase_b200_batch.h
+    "hase_batch_create",
+    "hase_batch_destroy",
+    "hase_calc_phi_ase_batch",
 )
 PROPOSAL_FEATURES = 12
 PROPOSAL_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -256,6 +260,32 @@ class TimeResultDesc(C.Structure):
     ]
 
 
+class BatchInstance(C.Structure):
+    _fields_ = [
+        ("context", C.c_void_p),
+        ("minSample", C.c_uint32),
+        ("maxSample", C.c_uint32),
+        ("result", C.POINTER(ResultDesc)),
+    ]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("raysTraced", C.c_uint64),
+        ("crossings", C.c_uint64),
+        ("rows", C.c_uint32),
+        ("chunks", C.c_uint32),
+        ("passes", C.c_uint32),
+        ("unconvergedSamples", C.c_uint32),
+        ("kernelLaunches", C.c_uint32),
+        ("graphNodes", C.c_uint32),
+        ("importanceMilliseconds", C.c_double),
+        ("rayMilliseconds", C.c_double),
+        ("totalMilliseconds", C.c_double),
+        ("captureMilliseconds", C.c_double),
+    ]
+
+
 class HaseError(RuntimeError):
     """A libhase_b200 call failed; ``status`` is the hase_status code."""
 
@@ -319,6 +349,10 @@ def lib():
         L.hase_proposal_features.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
         L.hase_simulate.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc),
                                     C.POINTER(PumpDesc), C.POINTER(TimeDesc), C.POINTER(TimeResultDesc)]
+        L.hase_batch_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        L.hase_batch_destroy.argtypes = [C.c_void_p]
+        L.hase_calc_phi_ase_batch.argtypes = [C.c_void_p, C.POINTER(BatchInstance), C.c_uint32,
+                                              C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), C.POINTER(BatchStats)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

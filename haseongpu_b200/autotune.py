@@ -1,4 +1,4 @@
-"""Autotuner for the ray kernel's launch shape.
+"""Autotuner for the ray kernel's launch shape (single-medium and batched solves).
 
 Sweeps every launch shape libhase_b200 compiles (block size, idle lanes that
 trigger a batched refill, occupancy target; ``hase_ray_kernel_variant_name``)
@@ -70,3 +70,23 @@ def autotune(ctx, *, firstSample: int, samples: int, rays: int, useReflections: 
     result = TuneResult(best[0], best[1], names[best[0]], best[2], table, min(imp)[1], min(imp)[0])
     _cache[key] = result
     return result
+
+
+def autotune_batch(batch, media, *, rays: int, useReflections: bool = False, monochromatic: bool = False,
+                   nearFieldSampling: bool = True, repeats: int = 2, workspaceBytes: int = 0) -> TuneResult:
+    """The same sweep for the pooled ray kernel of a batched solve
+    (``MediaBatch.solve``): every launch shape x work-item size on a fixed-ray
+    solve of the caller's media, timed by the ray launches' device time."""
+    names = variant_names()
+    table = []
+    best = None
+    for v, name in enumerate(names):
+        for rpt in RAYS_PER_LANE:
+            t = min(batch.solve(media, minRays=rays, maxRays=rays, useReflections=useReflections,
+                                monochromatic=monochromatic, nearFieldSampling=nearFieldSampling, rngSeed=31 + k,
+                                rayKernelVariant=v, raysPerThread=rpt, workspaceBytes=workspaceBytes)[1].rayMilliseconds
+                    for k in range(repeats))
+            table.append({"variant": v, "name": name, "raysPerThread": rpt, "ray_ms": t})
+            if best is None or t < best[2]:
+                best = (v, rpt, t)
+    return TuneResult(best[0], best[1], names[best[0]], best[2], table)

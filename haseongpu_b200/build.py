@@ -12,7 +12,8 @@ SOURCES = [PACKAGE_DIR / "csrc" / "hase_b200.cu", PACKAGE_DIR / "csrc" / "hase_f
            PACKAGE_DIR / "csrc" / "hase_proposal.cu"]
 HEADERS = [PACKAGE_DIR / "csrc" / "hase_device.cuh", PACKAGE_DIR / "csrc" / "hase_host.cuh",
            REPO_ROOT / "include" / "hase_b200.h", REPO_ROOT / "include" / "hase_b200_forward.h",
-           REPO_ROOT / "include" / "hase_b200_proposal.h", PACKAGE_DIR / "csrc" / "hase_mlp.cuh"]
+           REPO_ROOT / "include" / "hase_b200_proposal.h", REPO_ROOT / "include" / "hase_b200_batch.h",
+           PACKAGE_DIR / "csrc" / "hase_mlp.cuh"]
 LIB_PATH = PACKAGE_DIR / "libhase_b200.so"
 
 NVCC_FLAGS = [

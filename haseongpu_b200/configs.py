@@ -17,6 +17,14 @@ disc_poly    ~2,600 points on 29 rings (~5,100 triangles) x 20 levels, the
              refractive index 1.83 inside / 1.0 outside (total internal
              reflection above the critical angle), order <= 2; rays
              1e5 -> 1e7, threshold 0.001.
+media64      64 independent gain media (config 3): per medium a seeded
+             triangle count log-uniform in 200..20,000 (ring count chosen
+             to match), levels uniform in 5..40, radius U(0.5, 3) cm,
+             thickness U(0.3, 2) cm, Gaussian-pump beta with seeded waist
+             U(0.3, 0.7) x radius, depth U(0.5, 1.5) x thickness and peak
+             U(0.15, 0.35), 1..8 wavelengths (one pair: the disc_small pair;
+             more: the two-Lorentzian spectrum); rays 1e4 -> 1e7 per sample,
+             threshold 0.001.
 The fluorescence lifetime is 9.41e-4 s (the reference example media,
 example/laserPumpCladdingApi.py:241); it only scales phi.
 """
@@ -77,6 +85,55 @@ def disc_poly() -> Workload:
                      reflectivities=np.tile([0.3, 0.9], (T, 1)), refractiveIndices=[1.83, 1.0, 1.83, 1.0],
                      name="disc_poly")
     return Workload("disc_poly", mesh, two_lorentzian_spectrum(16), 100_000, 10_000_000, 0.001, True, False)
+
+
+@dataclass
+class Medium:
+    mesh: PrismMesh
+    spectra: CrossSectionData
+    wavelengths: int
+
+
+@dataclass
+class MediaWorkload:
+    name: str
+    media: list
+    minRays: int
+    maxRays: int
+    threshold: float
+    adaptiveSteps: int = 6
+
+
+def batch_medium(rng: np.random.Generator, index: int) -> Medium:
+    """One seeded gain medium of the batched-media workload."""
+    target_t = float(np.exp(rng.uniform(np.log(200.0), np.log(20000.0))))
+    rings = max(3, int(round(np.sqrt(target_t / 6.3))))
+    levels = int(rng.integers(5, 41))
+    radius = float(rng.uniform(0.5, 3.0))
+    height = float(rng.uniform(0.3, 2.0))
+    waist = float(rng.uniform(0.3, 0.7)) * radius
+    depth = float(rng.uniform(0.5, 1.5)) * height
+    peak = float(rng.uniform(0.15, 0.35))
+    nl = int(rng.integers(1, 9))
+    pts = disc_points(radius, rings, rng)
+    tri = delaunay_triangles(pts)
+    h = height / (levels - 1)
+    mesh = PrismMesh(points=pts, triangles=tri, numberOfLevels=levels, thickness=h,
+                     betaVolume=gaussian_pump_beta(pts, tri, levels, h, waist=waist, depth=depth, peak=peak),
+                     nTot=1.38e20, crystalTFluo=TAU,
+                     betaCells=point_beta(pts, levels, h, waist=waist, depth=depth, peak=peak),
+                     name=f"medium{index}")
+    if nl == 1:
+        spectra = CrossSectionData.monochromatic(wavelength=1030e-9, crossSectionAbsorption=1.1e-21,
+                                                 crossSectionEmission=2.2e-20)
+    else:
+        spectra = two_lorentzian_spectrum(nl)
+    return Medium(mesh, spectra, nl)
+
+
+def media64(count: int = 64) -> MediaWorkload:
+    rng = _rng(2)
+    return MediaWorkload("media64", [batch_medium(rng, i) for i in range(count)], 10_000, 10_000_000, 0.001)
 
 
 WORKLOADS = {"disc_small": disc_small, "disc_poly": disc_poly}

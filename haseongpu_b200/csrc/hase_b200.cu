@@ -20,6 +20,7 @@
 // include/core/types.hpp:201-354; dndt include/core/forwardPhiAseUtilities.hpp:16-25;
 // entry point include/core/simulation.hpp:42-47.
 #include "hase_b200.h"
+#include "hase_b200_batch.h"
 #include "hase_b200_proposal.h"
 #include "hase_device.cuh"
 #include "hase_host.cuh"
@@ -28,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -251,12 +253,28 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
 
 constexpr int kImportanceLayers = 8;  // layers per importance thread
 
+// ------------------------------------------------- batched gain media ----
+// One medium of a batched solve (device array, one entry per instance).
+struct InstanceView {
+    MeshView m;
+    const float2* spec;           // per wavelength (A, B)
+    uint32_t nLambda, nW, seedLo, pad;
+    double C;                     // N_tot / (4 pi tau)
+};
+
+// One sample row of a batched solve: its [rows][nW] workspace arrays start at
+// element w (the [rows][nW + 1] offsets at w + row index).
+struct RowInfo {
+    unsigned long long w;
+    uint32_t inst, sample, nW, seedLo;
+};
+
 // ------------------------------------------------------- (a2) ray map ----
 struct MapLaunch {
     const float* in;            // [rows][nW]: ln w (isLog) or w
     int isLog;
     int full;                   // 1: quantise + Q; 0: reuse q, Q
-    const uint32_t* rowList;    // nullptr: row = blockIdx.x
+    const uint32_t* rowList;    // nullptr: row = block index
     uint32_t nW;
     uint32_t M;                 // rays to map this pass
     const uint32_t* phases;     // nullptr: Philox(0, sample, pass, map tag)
@@ -265,24 +283,34 @@ struct MapLaunch {
     uint32_t* q;                // [rows][nW]
     unsigned long long* Q;      // [rows]
     uint32_t* offsets;          // [rows][nW+1]
+    const RowInfo* rows;        // batched media: ragged rows (nW, workspace offset, sample, seed per row)
+    const unsigned int* count;  // batched media: rows of rowList to map (device), blocks stride over them
 };
 
-__global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
+__device__ void mapRow(const MapLaunch& L, uint32_t row) {
     __shared__ unsigned long long sWarp[kMapBlock / 32];
     __shared__ float sMax;
     __shared__ unsigned long long sQ;
-    const uint32_t row = L.rowList ? L.rowList[blockIdx.x] : blockIdx.x;
-    const uint32_t nW = L.nW;
-    const float* in = L.in + size_t(row) * nW;
-    uint32_t* q = L.q + size_t(row) * nW;
-    uint32_t* off = L.offsets + size_t(row) * (nW + 1);
+    __shared__ float sRed[kMapBlock / 32];
+    uint32_t nW = L.nW, sample = L.firstSample + row, seedLo = L.seedLo;
+    size_t wBase = size_t(row) * nW, oBase = size_t(row) * (nW + 1);
+    if (L.rows) {
+        const RowInfo ri = L.rows[row];
+        nW = ri.nW;
+        sample = ri.sample;
+        seedLo = ri.seedLo;
+        wBase = ri.w;
+        oBase = ri.w + row;
+    }
+    const float* in = L.in + wBase;
+    uint32_t* q = L.q + wBase;
+    uint32_t* off = L.offsets + oBase;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long Q;
     if (L.full) {
         float mx = -INFINITY;
         for (uint32_t b = threadIdx.x; b < nW; b += kMapBlock) mx = fmaxf(mx, in[b]);
         mx = warpMax(mx);
-        __shared__ float sRed[kMapBlock / 32];
         if (lane == 0) sRed[warp] = mx;
         __syncthreads();
         if (warp == 0) {
@@ -301,7 +329,7 @@ __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
             const float w = L.isLog ? (v == -INFINITY || wmax == 0.0f ? 0.0f : expf(v - mx)) : v;
             const uint32_t qi = (w > 0.0f && wmax > 0.0f) ? uint32_t(ceil(double(w) * scale)) : 0u;
             q[b] = qi;
-            if (L.wOut) L.wOut[size_t(row) * nW + b] = w;
+            if (L.wOut) L.wOut[wBase + b] = w;
             part += qi;
         }
         part = warpSum(part);
@@ -329,7 +357,7 @@ __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
     if (L.phases) {
         phase = L.phases[row];
     } else {
-        phase = philox4x32_10(0u, L.firstSample + row, L.pass, kTagMap, L.seedLo, L.seedHi).x;
+        phase = philox4x32_10(0u, sample, L.pass, kTagMap, seedLo, L.seedHi).x;
     }
     using u128 = unsigned __int128;
     const unsigned long long phiQ = (unsigned long long)((u128(phase) * Q) >> 32);
@@ -346,6 +374,16 @@ __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
         carry += total;
     }
     if (threadIdx.x == 0) off[nW] = M;
+}
+
+// One CTA per row (grid = rows), or, with L.count, CTAs striding over the
+// device-held number of rows.
+__global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
+    const uint32_t n = L.count ? *L.count : gridDim.x;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        mapRow(L, L.rowList ? L.rowList[i] : i);
+        __syncthreads();  // shared scratch is reused by the next row
+    }
 }
 
 // --------------------------------------------------------- (b) rays ----
@@ -370,6 +408,11 @@ struct RayLaunch {
     uint32_t* pDrop;
     unsigned long long* pCross;
     float* logBuf;                // [rows][nW]: per-(slice, prism) sum of contributions (LOG kernels only)
+    // batched media (POOL kernels): per-row medium, workspace offset, sample
+    // and seed; the medium's view; the number of active rows (device)
+    const InstanceView* inst;
+    const RowInfo* rows;
+    const unsigned int* count;
 };
 
 __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, uint32_t x) {
@@ -388,13 +431,16 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 // REFILL idle lanes so start-point code runs convergent), and writes the
 // item's FP64 sums.  No block barrier; per-item partials keep the result
 // independent of which warp ran which item.
-template <int BLOCK, int REFILL, int MINB, bool LOG = false>
+// POOL: the rows belong to many gain media; the warp copies the view of its
+// item's medium into its shared-memory slot (when the medium changes) and
+// walks from there, and the number of active rows is read on the device.
+template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
-    const MeshView& m = L.m;
+    __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
     const int lane = threadIdx.x & 31;
     const unsigned laneLt = (1u << lane) - 1u;
-    const uint32_t nItems = L.nActive * L.itemsPerRow;
-    GlobalLoader load{m.tri};
+    const uint32_t nItems = (POOL ? *L.count : L.nActive) * L.itemsPerRow;
+    uint32_t curInst = 0xffffffffu;
     while (true) {
         uint32_t item = 0;
         if (lane == 0) item = atomicAdd(L.itemCounter, 1u);
@@ -413,17 +459,46 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
             }
             continue;
         }
-        const uint32_t sample = L.firstSample + row;
+        uint32_t sample, nW;
+        size_t wBase, oBase;
+        if constexpr (POOL) {
+            const RowInfo ri = L.rows[row];
+            if (ri.inst != curInst) {
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(L.inst + ri.inst);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(sInst + (threadIdx.x >> 5));
+                for (uint32_t w = uint32_t(lane); w < sizeof(InstanceView) / 4; w += 32) dst[w] = __ldg(src + w);
+                __syncwarp();
+                curInst = ri.inst;
+            }
+            sample = ri.sample;
+            nW = ri.nW;
+            wBase = ri.w;
+            oBase = ri.w + row;
+        } else {
+            sample = L.firstSample + row;
+            nW = L.nW;
+            wBase = size_t(row) * nW;
+            oBase = size_t(row) * (nW + 1);
+        }
+        // per-medium constants: the kernel parameters, or the warp's shared
+        // slot, read (volatile) where they are used so that they do not hold
+        // registers across the walk
+        const volatile InstanceView& iv = sInst[threadIdx.x >> 5];
+#define HASE_SEED_LO (POOL ? uint32_t(iv.seedLo) : uint32_t(L.seedLo))
+#define HASE_N_LAMBDA (POOL ? uint32_t(iv.nLambda) : uint32_t(L.nLambda))
+#define HASE_SPEC (POOL ? (const float2*)iv.spec : L.spec)
+        const double Cm = POOL ? double(iv.C) : double(L.C);
+        const MeshView& m = POOL ? sInst[threadIdx.x >> 5].m : L.m;
+        const GlobalLoader load{m.tri};
         const uint32_t r0 = k * L.itemRays;
         const uint32_t r1 = min(r0 + L.itemRays, L.M);
-        const uint32_t nW = L.nW;
-        const uint32_t* off = L.offsets + size_t(row) * (nW + 1);
-        const uint32_t* q = L.q + size_t(row) * nW;
-        const double CQ = L.C * double(Qrow);
+        const uint32_t* off = L.offsets + oBase;
+        const uint32_t* q = L.q + wBase;
+        const double CQ = Cm * double(Qrow);
         const float2 S = __ldg(m.points + sample % m.Np);
         const int ls = int(sample / m.Np);
         const uint32_t lambdaPhase =
-            L.nLambda > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, L.seedLo, L.seedHi).y % L.nLambda : 0u;
+            HASE_N_LAMBDA > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, HASE_SEED_LO, L.seedHi).y % HASE_N_LAMBDA : 0u;
         // prisms holding the item's rays: [pb, pb + count - 1)
         uint32_t bound = 0;
         if (lane == 0) bound = upperBound(off, nW + 1, r0) - 1u;
@@ -449,7 +524,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                     if (LOG) bsel = b;
                     const uint32_t j = b / m.P, p = b - j * m.P;
                     const uint32_t t = p % m.T, l = p / m.T;
-                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, L.seedLo, L.seedHi);
+                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, HASE_SEED_LO, L.seedHi);
                     uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
                     if (k1 + k2 + 1u > (1u << 24)) {
                         k1 = (1u << 24) - 1u - k1;
@@ -457,8 +532,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                     }
                     const int kImg = imageLevel(ls, int(m.layers), j);
                     const uint32_t lam =
-                        L.nLambda > 1 ? uint32_t((uint64_t(r) * L.nLambda / L.M + lambdaPhase) % L.nLambda) : 0u;
-                    const float2 ab = __ldg(L.spec + lam);
+                        HASE_N_LAMBDA > 1 ? uint32_t((uint64_t(r) * HASE_N_LAMBDA / L.M + lambdaPhase) % HASE_N_LAMBDA)
+                                        : 0u;
+                    const float2 ab = __ldg(HASE_SPEC + lam);
                     float dx, dy, dz, alphaL, D2;
                     if (L.nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
                         nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
@@ -488,7 +564,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         const double X = CQ * double(wf) * exp(double(ray.G));
                         sum += X;
                         sum2 += X * X;
-                        if (LOG) atomicAdd(L.logBuf + size_t(row) * nW + bsel, float(X));
+                        if (LOG) atomicAdd(L.logBuf + wBase + bsel, float(X));
                     } else {
                         ++dropped;
                     }
@@ -496,6 +572,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 }
             }
         }
+#undef HASE_SEED_LO
+#undef HASE_N_LAMBDA
+#undef HASE_SPEC
         sum = warpSum(sum);
         sum2 = warpSum(sum2);
         dropped = warpSum(dropped);
@@ -528,6 +607,18 @@ const RayVariant kRayVariants[] = {
     {rayKernel<512, 8, 2>, 512, "block512_refill8_occ2"},
 };
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
+// The same launch shapes for batched media (same order and names).
+const RayVariant kPoolVariants[] = {
+    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5"},
+    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5"},
+    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5"},
+    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4"},
+    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6"},
+    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10"},
+    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12"},
+    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2"},
+};
+static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
 // ------------------------------------------------ (c)+(d) finalise ----
 struct FinalizeLaunch {
@@ -548,13 +639,19 @@ struct FinalizeLaunch {
     double* mse;
     uint32_t* nextActive;
     uint32_t* nextCount;
+    const unsigned int* count;    // batched media: the number of active rows (device); warps stride over them
 };
 
+__device__ void finalizeRow(const FinalizeLaunch& L, uint32_t row, int lane);
+
 __global__ void __launch_bounds__(128) finalizeKernel(FinalizeLaunch L) {
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= L.nActive) return;
-    const uint32_t row = L.active[wid];
+    const uint32_t n = L.count ? *L.count : L.nActive;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wid < n; wid += warps)
+        finalizeRow(L, L.active[wid], threadIdx.x & 31);
+}
+
+__device__ void finalizeRow(const FinalizeLaunch& L, uint32_t row, int lane) {
     double s = 0.0, s2 = 0.0;
     uint32_t d = 0;
     unsigned long long c = 0;
@@ -592,6 +689,13 @@ __global__ void __launch_bounds__(128) finalizeKernel(FinalizeLaunch L) {
 __global__ void iotaKernel(uint32_t* a, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = i;
+}
+
+// iota plus the device-held row count of a batched solve's first pass.
+__global__ void iotaCountKernel(uint32_t* a, uint32_t n, unsigned int* count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+    if (i == 0) *count = n;
 }
 
 // ------------------------------------------------------ diagnostics ----
@@ -2097,6 +2201,473 @@ hase_status hase_estimate_sample_noalloc(hase_context* c, uint32_t sample, const
     noAllocEmitKernel<<<1, 1, 0, c->stream>>>(phi, mse, accTotal, accDrop, deviceResult);
     HASE_CUDA(cudaGetLastError());
     HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- batched gain media ----
+// hase_calc_phi_ase_batch: the sample points of many contexts in one pooled
+// workspace, every adaptive pass one map, one persistent ray and one finalise
+// launch over the active rows of all media, the whole schedule of a
+// workspace chunk captured as one CUDA graph.
+
+struct hase_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> ev;  // timing events recorded inside the graphs
+    DevBuf<float> lnw, phi;
+    DevBuf<uint32_t> q, offsets, activeA, activeB, accTotal, accDrop, pDrop;
+    DevBuf<unsigned int> counts;  // [0], [1]: active rows (alternating), [2]: item counter, [3 ..]: per pass
+    DevBuf<unsigned long long> Q, accCross, pCross;
+    DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
+    DevBuf<float2> spec;
+    DevBuf<InstanceView> inst;
+    DevBuf<RowInfo> rows;
+    uint32_t variantBlocks[16] = {};
+    int sms = 0;
+};
+
+namespace {
+
+struct BatchMedium {
+    hase_context* c;
+    uint32_t first, nS, nW, nLambda;
+    double meanA, meanB, sA, sE;  // sA/sE: the pair of the dndt output
+};
+
+// Ends a stream capture that an error interrupted, so the stream stays usable.
+struct CaptureGuard {
+    cudaStream_t s;
+    bool active = false;
+    ~CaptureGuard() {
+        if (active) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+    }
+};
+
+struct GraphOwner {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    ~GraphOwner() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_batch_create(int device, hase_batch** out) {
+    if (!out) return fail(HASE_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(HASE_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n) return fail(HASE_INVALID_ARGUMENT, "device %d outside [0, %d)", device, n);
+    HASE_CUDA(cudaSetDevice(device));
+    hase_batch* b = new (std::nothrow) hase_batch;
+    if (!b) return fail(HASE_OUT_OF_MEMORY, "host allocation failed");
+    b->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(HASE_CUDA_ERROR, "batch stream: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return HASE_OK;
+}
+
+hase_status hase_batch_destroy(hase_batch* b) {
+    if (!b) return HASE_OK;
+    cudaSetDevice(b->device);
+    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return HASE_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Checks the instances and fills the per-medium table (spectrum, sizes).
+hase_status batchMedia(const hase_batch* b, const hase_batch_instance* in, uint32_t count,
+                       const hase_experiment_desc* ex, std::vector<BatchMedium>& media,
+                       std::vector<float2>& specPool, std::vector<uint32_t>& specBase) {
+    const uint32_t slices = ex->useReflections ? 5u : 1u;
+    media.resize(count);
+    specPool.clear();
+    specBase.resize(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        hase_context* c = in[i].context;
+        if (!c) return fail(HASE_INVALID_ARGUMENT, "instance %u has no context", i);
+        if (c->device != b->device)
+            return fail(HASE_INVALID_ARGUMENT, "instance %u is on device %d, the batch on %d", i, c->device, b->device);
+        if (!in[i].result) return fail(HASE_INVALID_ARGUMENT, "instance %u has no result", i);
+        const uint32_t nTot = c->Np * c->L;
+        const uint32_t first = in[i].minSample;
+        const uint32_t last = in[i].maxSample == UINT32_MAX ? nTot - 1 : in[i].maxSample;
+        if (first > last || last >= nTot)
+            return fail(HASE_INVALID_ARGUMENT, "instance %u: sample range [%u, %u] outside [0, %u)", i, first, last,
+                        nTot);
+        if (uint64_t(slices) * c->P > 0xffffffffull)
+            return fail(HASE_INVALID_ARGUMENT, "instance %u: too many prisms", i);
+        BatchMedium& m = media[i];
+        m.c = c;
+        m.first = first;
+        m.nS = last - first + 1;
+        m.nW = slices * c->P;
+        m.nLambda = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+        m.meanA = m.meanB = m.sA = m.sE = 0.0;
+        specBase[i] = uint32_t(specPool.size());
+        for (uint32_t l = 0; l < m.nLambda; ++l) {
+            const double A = c->nTot * (c->sigmaE[l] + c->sigmaA[l]), B = c->nTot * c->sigmaA[l];
+            specPool.push_back(make_float2(float(A), float(B)));
+            m.meanA += A / m.nLambda;
+            m.meanB += B / m.nLambda;
+            m.sA = std::max(m.sA, c->sigmaA[l]);
+            m.sE = std::max(m.sE, c->sigmaE[l]);
+        }
+        if (m.nLambda == 1) {
+            m.sA = c->sigmaA[0];
+            m.sE = c->sigmaE[0];
+        }
+    }
+    return HASE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in, uint32_t count,
+                                    const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                                    hase_batch_stats* stats) {
+    if (!b || !in || !ex || !cp || count == 0) return fail(HASE_INVALID_ARGUMENT, "null argument or no instances");
+    if (ex->minRays == 0) return fail(HASE_INVALID_ARGUMENT, "minRays must be positive");
+    if (ex->maxRays != 0 && ex->maxRays < ex->minRays) return fail(HASE_INVALID_ARGUMENT, "maxRays < minRays");
+    if (!(ex->mseThreshold >= 0.0)) return fail(HASE_INVALID_ARGUMENT, "mseThreshold must be >= 0");
+    if (cp->importanceLayers != 0 && cp->importanceLayers != 4 && cp->importanceLayers != kImportanceLayers)
+        return fail(HASE_INVALID_ARGUMENT, "importanceLayers must be 0, 4 or %d", kImportanceLayers);
+    if (cp->rayKernelVariant >= kNumRayVariants)
+        return fail(HASE_INVALID_ARGUMENT, "rayKernelVariant %u >= %u", cp->rayKernelVariant, kNumRayVariants);
+    HASE_CUDA(cudaSetDevice(b->device));
+    std::vector<BatchMedium> media;
+    std::vector<float2> specPool;
+    std::vector<uint32_t> specBase;
+    HASE_TRY(batchMedia(b, in, count, ex, media, specPool, specBase));
+    const uint32_t maxRays = std::max(ex->maxRays, ex->minRays);
+    const uint32_t slices = ex->useReflections ? 5u : 1u;
+    const uint32_t variant = cp->rayKernelVariant;
+    const RayVariant& rv = kPoolVariants[variant];
+    if (b->variantBlocks[variant] == 0) {
+        int perSM = 0;
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, rv.kernel, rv.block, 0));
+        b->variantBlocks[variant] = uint32_t(std::max(1, perSM) * std::max(1, b->sms));
+    }
+
+    // the pass schedule (shared by all media)
+    struct Pass {
+        uint32_t M, itemRays, items;
+        bool last;
+    };
+    std::vector<Pass> passes;
+    for (uint32_t pass = 0, prev = 0;; ++pass) {
+        const uint32_t target = adaptiveTarget(ex->minRays, maxRays, cp->adaptiveSteps, pass);
+        const bool last = target >= maxRays || pass >= cp->adaptiveSteps;
+        Pass ps;
+        ps.M = target - prev;
+        ps.itemRays = std::max<uint32_t>(cp->raysPerThread ? 32u * cp->raysPerThread : kMinItemRays,
+                                         (ps.M + kMaxItems - 1) / kMaxItems);
+        ps.items = (ps.M + ps.itemRays - 1) / ps.itemRays;
+        ps.last = last;
+        passes.push_back(ps);
+        prev = target;
+        if (last) break;
+    }
+    const uint32_t nPasses = uint32_t(passes.size());
+
+    // media views and spectra
+    HASE_CUDA(b->spec.ensure(specPool.size()));
+    HASE_CUDA(b->inst.ensure(count));
+    std::vector<InstanceView> views(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const hase_context* c = media[i].c;
+        InstanceView& v = views[i];
+        std::memset(&v, 0, sizeof(v));
+        v.m = c->view();
+        v.spec = b->spec.p + specBase[i];
+        v.nLambda = media[i].nLambda;
+        v.nW = media[i].nW;
+        v.seedLo = cp->rngSeed + i;
+        v.C = c->nTot / (4.0 * kPi * c->tau);
+    }
+    HASE_CUDA(cudaMemcpyAsync(b->spec.p, specPool.data(), specPool.size() * sizeof(float2), cudaMemcpyHostToDevice,
+                              b->stream));
+    HASE_CUDA(cudaMemcpyAsync(b->inst.p, views.data(), count * sizeof(InstanceView), cudaMemcpyHostToDevice,
+                              b->stream));
+
+    // rows of every medium, cut into workspace chunks
+    struct Chunk {
+        size_t r0, r1;            // global rows [r0, r1)
+        unsigned long long ws;    // workspace entries (sum of nW)
+    };
+    std::vector<RowInfo> all;
+    for (uint32_t i = 0; i < count; ++i) {
+        all.reserve(all.size() + media[i].nS);
+        for (uint32_t s = 0; s < media[i].nS; ++s) all.push_back(RowInfo{0ull, i, media[i].first + s, media[i].nW,
+                                                                           cp->rngSeed + i});
+    }
+    const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
+    std::vector<Chunk> chunks;
+    {
+        Chunk ch{0, 0, 0};
+        uint64_t bytes = 0;
+        for (size_t r = 0; r < all.size(); ++r) {
+            const uint64_t perRow = uint64_t(all[r].nW) * 12 + 16 + kMaxItems * 28ull + 64;
+            if (ch.r1 > ch.r0 && bytes + perRow > budget) {
+                chunks.push_back(ch);
+                ch = Chunk{r, r, 0};
+                bytes = 0;
+            }
+            all[r].w = ch.ws;
+            ch.ws += all[r].nW;
+            ch.r1 = r + 1;
+            bytes += perRow;
+        }
+        chunks.push_back(ch);
+    }
+    size_t maxRows = 0;
+    unsigned long long maxWs = 0;
+    for (const Chunk& ch : chunks) {
+        maxRows = std::max(maxRows, ch.r1 - ch.r0);
+        maxWs = std::max(maxWs, ch.ws);
+    }
+    if (maxRows > 0xffffffffull) return fail(HASE_INVALID_ARGUMENT, "too many sample points in one chunk");
+    HASE_CUDA(b->lnw.ensure(maxWs));
+    HASE_CUDA(b->q.ensure(maxWs));
+    HASE_CUDA(b->offsets.ensure(maxWs + maxRows));
+    HASE_CUDA(b->Q.ensure(maxRows));
+    HASE_CUDA(b->rows.ensure(maxRows));
+    HASE_CUDA(b->activeA.ensure(maxRows));
+    HASE_CUDA(b->activeB.ensure(maxRows));
+    HASE_CUDA(b->counts.ensure(3 + nPasses));
+    HASE_CUDA(b->accSum.ensure(maxRows));
+    HASE_CUDA(b->accSum2.ensure(maxRows));
+    HASE_CUDA(b->accTotal.ensure(maxRows));
+    HASE_CUDA(b->accDrop.ensure(maxRows));
+    HASE_CUDA(b->accCross.ensure(maxRows));
+    HASE_CUDA(b->phi.ensure(maxRows));
+    HASE_CUDA(b->mse.ensure(maxRows));
+    HASE_CUDA(b->pSum.ensure(maxRows * kMaxItems));
+    HASE_CUDA(b->pSum2.ensure(maxRows * kMaxItems));
+    HASE_CUDA(b->pDrop.ensure(maxRows * kMaxItems));
+    HASE_CUDA(b->pCross.ensure(maxRows * kMaxItems));
+    const size_t nEvents = 3 + 2 * size_t(nPasses);
+    while (b->ev.size() < nEvents) {
+        cudaEvent_t e = nullptr;
+        HASE_CUDA(cudaEventCreate(&e));
+        b->ev.push_back(e);
+    }
+
+    hase_batch_stats st{};
+    st.rows = uint32_t(all.size());
+    st.chunks = uint32_t(chunks.size());
+    std::vector<uint32_t> unconvergedOf(count, 0), passesOf(count, 0);
+    std::vector<uint64_t> raysOf(count, 0), crossOf(count, 0);
+    uint64_t droppedTotal = 0;
+    std::vector<float> hPhi(maxRows);
+    std::vector<double> hMse(maxRows);
+    std::vector<uint32_t> hTotal(maxRows), hDrop(maxRows), hCounts(3 + nPasses);
+    std::vector<unsigned long long> hCross(maxRows);
+    const double thr = ex->mseThreshold;
+
+    for (const Chunk& ch : chunks) {
+        const uint32_t nRows = uint32_t(ch.r1 - ch.r0);
+        HASE_CUDA(cudaMemcpyAsync(b->rows.p, all.data() + ch.r0, nRows * sizeof(RowInfo), cudaMemcpyHostToDevice,
+                                  b->stream));
+        HASE_CUDA(cudaStreamSynchronize(b->stream));
+        const auto tc0 = std::chrono::steady_clock::now();
+        GraphOwner graph;
+        uint32_t kernels = 0;
+        {
+            CaptureGuard guard{b->stream};
+            HASE_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            guard.active = true;
+            HASE_CUDA(cudaEventRecordWithFlags(b->ev[0], b->stream, cudaEventRecordExternal));
+            // (a1) importance weights, one launch per run of rows of one medium
+            for (size_t r = ch.r0; r < ch.r1;) {
+                const uint32_t i = all[r].inst;
+                size_t e = r;
+                while (e < ch.r1 && all[e].inst == i && e - r < 65535) ++e;
+                const BatchMedium& md = media[i];
+                const hase_context* c = md.c;
+                ImportanceLaunch il{views[i].m, all[r].sample, slices, md.nW, float(md.meanA), float(md.meanB),
+                                    b->lnw.p + all[r].w, nullptr};
+                const uint32_t G = cp->importanceLayers == 4 ? 4u : uint32_t(kImportanceLayers);
+                const uint32_t threads = slices * ((c->layers + G - 1) / G) * c->T;
+                if (G == 4)
+                    importanceKernel<4><<<dim3((threads + 255) / 256, uint32_t(e - r)), 256, 0, b->stream>>>(il);
+                else
+                    importanceKernel<kImportanceLayers>
+                        <<<dim3((threads + 255) / 256, uint32_t(e - r)), 256, 0, b->stream>>>(il);
+                HASE_CUDA(cudaGetLastError());
+                ++kernels;
+                r = e;
+            }
+            HASE_CUDA(cudaEventRecordWithFlags(b->ev[1], b->stream, cudaEventRecordExternal));
+            HASE_CUDA(cudaMemsetAsync(b->accSum.p, 0, nRows * sizeof(double), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->accSum2.p, 0, nRows * sizeof(double), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->accTotal.p, 0, nRows * sizeof(uint32_t), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->accDrop.p, 0, nRows * sizeof(uint32_t), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->accCross.p, 0, nRows * sizeof(unsigned long long), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->counts.p, 0, (3 + nPasses) * sizeof(unsigned int), b->stream));
+            iotaCountKernel<<<(nRows + 255) / 256, 256, 0, b->stream>>>(b->activeA.p, nRows, b->counts.p);
+            HASE_CUDA(cudaGetLastError());
+            ++kernels;
+            uint32_t* cur = b->activeA.p;
+            uint32_t* nxt = b->activeB.p;
+            unsigned int* cntCur = b->counts.p;
+            unsigned int* cntNxt = b->counts.p + 1;
+            unsigned int* itemCounter = b->counts.p + 2;
+            const uint32_t mapGrid = std::min<uint32_t>(nRows, uint32_t(2 * b->sms));
+            const uint32_t finGrid = std::min<uint32_t>((nRows * 32u + 127u) / 128u, uint32_t(16 * b->sms));
+            for (uint32_t k = 0; k < nPasses; ++k) {
+                const Pass& ps = passes[k];
+                HASE_CUDA(cudaMemcpyAsync(b->counts.p + 3 + k, cntCur, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                                          b->stream));
+                MapLaunch ml{b->lnw.p, 1, k == 0 ? 1 : 0, cur, 0u, ps.M, nullptr, 0u, k, 0u, 0u, nullptr, b->q.p,
+                             b->Q.p, b->offsets.p, b->rows.p, cntCur};
+                mapKernel<<<mapGrid, kMapBlock, 0, b->stream>>>(ml);
+                HASE_CUDA(cudaGetLastError());
+                HASE_CUDA(cudaMemsetAsync(itemCounter, 0, sizeof(unsigned int), b->stream));
+                HASE_CUDA(cudaEventRecordWithFlags(b->ev[3 + 2 * k], b->stream, cudaEventRecordExternal));
+                RayLaunch rl{};
+                rl.active = cur;
+                rl.pass = k;
+                rl.M = ps.M;
+                rl.itemRays = ps.itemRays;
+                rl.itemsPerRow = ps.items;
+                rl.itemCounter = itemCounter;
+                rl.q = b->q.p;
+                rl.Q = b->Q.p;
+                rl.offsets = b->offsets.p;
+                rl.nearField = ex->nearFieldSampling;
+                rl.pSum = b->pSum.p;
+                rl.pSum2 = b->pSum2.p;
+                rl.pDrop = b->pDrop.p;
+                rl.pCross = b->pCross.p;
+                rl.inst = b->inst.p;
+                rl.rows = b->rows.p;
+                rl.count = cntCur;
+                const uint32_t grid = uint32_t(std::min<uint64_t>(uint64_t(nRows) * ps.items / (rv.block / 32) + 1,
+                                                                   uint64_t(b->variantBlocks[variant])));
+                void* rayArgs[] = {&rl};
+                HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(rv.kernel), dim3(grid), dim3(rv.block),
+                                           rayArgs, 0, b->stream));
+                HASE_CUDA(cudaEventRecordWithFlags(b->ev[4 + 2 * k], b->stream, cudaEventRecordExternal));
+                HASE_CUDA(cudaMemsetAsync(cntNxt, 0, sizeof(unsigned int), b->stream));
+                FinalizeLaunch fl{cur, 0u, ps.items, ps.M, ps.last ? 1 : 0, thr, b->pSum.p, b->pSum2.p, b->pDrop.p,
+                                  b->pCross.p, b->accSum.p, b->accSum2.p, b->accTotal.p, b->accDrop.p, b->accCross.p,
+                                  b->phi.p, b->mse.p, nxt, cntNxt, cntCur};
+                finalizeKernel<<<finGrid, 128, 0, b->stream>>>(fl);
+                HASE_CUDA(cudaGetLastError());
+                kernels += 3;
+                std::swap(cur, nxt);
+                std::swap(cntCur, cntNxt);
+            }
+            // after the last pass cntCur holds the samples above the threshold at maxRays
+            if (cntCur != b->counts.p)
+                HASE_CUDA(cudaMemcpyAsync(b->counts.p, cntCur, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                                          b->stream));
+            HASE_CUDA(cudaEventRecordWithFlags(b->ev[2], b->stream, cudaEventRecordExternal));
+            guard.active = false;
+            HASE_CUDA(cudaStreamEndCapture(b->stream, &graph.g));
+        }
+        HASE_CUDA(cudaGraphInstantiate(&graph.x, graph.g, 0));
+        size_t nodes = 0;
+        HASE_CUDA(cudaGraphGetNodes(graph.g, nullptr, &nodes));
+        st.captureMilliseconds +=
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
+        HASE_CUDA(cudaGraphLaunch(graph.x, b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hPhi.data(), b->phi.p, nRows * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hMse.data(), b->mse.p, nRows * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hTotal.data(), b->accTotal.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hDrop.data(), b->accDrop.p, nRows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hCross.data(), b->accCross.p, nRows * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, b->stream));
+        HASE_CUDA(cudaMemcpyAsync(hCounts.data(), b->counts.p, (3 + nPasses) * sizeof(unsigned int),
+                                  cudaMemcpyDeviceToHost, b->stream));
+        HASE_CUDA(cudaStreamSynchronize(b->stream));
+        float ms = 0.0f;
+        HASE_CUDA(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+        st.importanceMilliseconds += ms;
+        HASE_CUDA(cudaEventElapsedTime(&ms, b->ev[0], b->ev[2]));
+        st.totalMilliseconds += ms;
+        for (uint32_t k = 0; k < nPasses; ++k) {
+            HASE_CUDA(cudaEventElapsedTime(&ms, b->ev[3 + 2 * k], b->ev[4 + 2 * k]));
+            st.rayMilliseconds += ms;
+            if (hCounts[3 + k] > 0) st.passes = std::max(st.passes, k + 1);
+        }
+        st.unconvergedSamples += hCounts[0];
+        st.kernelLaunches += kernels;
+        st.graphNodes += uint32_t(nodes);
+        // scatter the chunk's rows into the media's results
+        for (uint32_t j = 0; j < nRows; ++j) {
+            const RowInfo& ri = all[ch.r0 + j];
+            const BatchMedium& md = media[ri.inst];
+            hase_result* res = in[ri.inst].result;
+            const uint32_t o = ri.sample - md.first;
+            if (res->phiAse) res->phiAse[o] = hPhi[j];
+            if (res->relativeStandardError) res->relativeStandardError[o] = hMse[j];
+            if (res->standardError) res->standardError[o] = hMse[j] * double(hPhi[j]);
+            if (res->totalRays) res->totalRays[o] = hTotal[j];
+            if (res->droppedRays) res->droppedRays[o] = hDrop[j];
+            if (res->dndtAse) {
+                const double bc = md.c->betaCells.empty() ? 0.0 : md.c->betaCells[ri.sample];
+                res->dndtAse[o] = (bc * (md.sE + md.sA) - md.sA) * double(hPhi[j]);
+            }
+            if (!(hMse[j] <= thr)) ++unconvergedOf[ri.inst];
+            uint32_t np = 0;
+            for (uint32_t k = 0, cum = 0; k < nPasses && cum < hTotal[j]; ++k) {
+                cum += passes[k].M;
+                np = k + 1;
+            }
+            passesOf[ri.inst] = std::max(passesOf[ri.inst], np);
+            raysOf[ri.inst] += hTotal[j];
+            crossOf[ri.inst] += hCross[j];
+            droppedTotal += hDrop[j];
+            st.raysTraced += hTotal[j];
+            st.crossings += hCross[j];
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        hase_result* res = in[i].result;
+        res->raysTraced = raysOf[i];
+        res->crossings = crossOf[i];
+        res->unconvergedSamples = unconvergedOf[i];
+        res->passes = passesOf[i];
+        res->importanceMilliseconds = st.importanceMilliseconds;
+        res->rayMilliseconds = st.rayMilliseconds;
+        res->totalMilliseconds = st.totalMilliseconds;
+        res->kernelLaunches = st.kernelLaunches;
+    }
+    if (stats) *stats = st;
+    if (droppedTotal) {
+        fail(HASE_DROPPED_RAYS, "%llu rays could not be walked", (unsigned long long)droppedTotal);
+        return HASE_DROPPED_RAYS;
+    }
+    if (st.unconvergedSamples) {
+        fail(HASE_NOT_CONVERGED, "%u samples above the threshold at maxRays", st.unconvergedSamples);
+        return HASE_NOT_CONVERGED;
+    }
     return HASE_OK;
 }
 

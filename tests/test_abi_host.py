@@ -47,7 +47,8 @@ def test_structures_match_header(native):
                        ("hase_forward_desc", native.ForwardDesc), ("hase_forward_result", native.ForwardResultDesc),
                        ("hase_pump_desc", native.PumpDesc), ("hase_time_desc", native.TimeDesc),
                        ("hase_time_result", native.TimeResultDesc), ("hase_proposal_batch", native.ProposalBatch),
-                       ("hase_proposal_train_desc", native.ProposalTrainDesc), ("hase_learned_desc", native.LearnedDesc)]:
+                       ("hase_proposal_train_desc", native.ProposalTrainDesc), ("hase_learned_desc", native.LearnedDesc),
+                       ("hase_batch_instance", native.BatchInstance), ("hase_batch_stats", native.BatchStats)]:
         body = re.search(r"typedef struct \{([^{}]*)\}\s*" + cname + ";", text).group(1)
         fields = re.findall(r"\b(\w+);", re.sub(r"/\*.*?\*/", "", body, flags=re.S))
         assert fields == [f for f, _ in pyt._fields_], cname
@@ -83,6 +84,11 @@ def test_no_device_fails_loudly(native):
 
     with pytest.raises(native.HaseError) as err:
         TetDeviceMesh(TetMesh.fromPrismMesh(legacy_mesh("cuboid")), *legacy_spectrum("cuboid"))
+    assert err.value.status == native.HASE_NO_DEVICE
+    from haseongpu_b200 import MediaBatch
+
+    with pytest.raises(native.HaseError) as err:
+        MediaBatch(0)
     assert err.value.status == native.HASE_NO_DEVICE
 
 

@@ -1,0 +1,135 @@
+"""Batched gain media (include/hase_b200_batch.h): many media, one pooled
+workspace, one persistent ray launch per adaptive pass, one CUDA graph.
+
+Medium i of a batch uses the Philox key rngSeed + i, so its result must be
+bit-identical to the single-medium solve (hase_calc_phi_ase, itself checked
+against the oracle and the golden vectors) with that seed: per-sample phi,
+relative error, ray counts and dropped rays, across adaptive passes, with
+polychromatic spectra, reflections and workspace chunking; every launch
+shape of the pooled ray kernel walks the same rays (sums equal to rounding).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(minRays=2000, maxRays=64000, mseThreshold=0.004, adaptiveSteps=3, monochromatic=False, rngSeed=77)
+
+
+@pytest.fixture(scope="module")
+def media():
+    from haseongpu_b200 import DeviceMesh, build
+    from haseongpu_b200.configs import batch_medium
+    from haseongpu_b200.mesh import PrismMesh
+
+    build.build_library()
+    rng = np.random.default_rng(123)
+    picked = []
+    while len(picked) < 5:
+        m = batch_medium(rng, len(picked))
+        if m.mesh.numberOfPrisms <= 40000:
+            picked.append(m)
+    # one medium with reflecting surfaces and total internal reflection
+    m0 = picked[0].mesh
+    T = m0.numberOfTriangles
+    refl = PrismMesh(points=m0.points, triangles=m0.triangles, numberOfLevels=m0.numberOfLevels,
+                     thickness=m0.thickness, betaVolume=m0.betaVolume, nTot=m0.nTot, crystalTFluo=m0.crystalTFluo,
+                     betaCells=m0.betaCells, reflectivities=np.tile([0.3, 0.9], (T, 1)),
+                     refractiveIndices=[1.83, 1.0, 1.83, 1.0], name="reflecting")
+    ctxs = []
+    for m in picked:
+        ctxs.append(DeviceMesh(m.mesh, *m.spectra.resampled(False), device=0))
+    ctxs.append(DeviceMesh(refl, *picked[0].spectra.resampled(False), device=0))
+    yield ctxs
+    for c in ctxs:
+        c.close()
+
+
+def _ranges(ctxs, n=96):
+    out = []
+    for i, c in enumerate(ctxs):
+        S = c.mesh.numberOfSamples
+        lo = (37 * i) % max(1, S - n)
+        out.append((c, lo, min(S - 1, lo + n - 1)))
+    return out
+
+
+def _same(a, b):
+    np.testing.assert_array_equal(a.phiAse, b.phiAse)
+    np.testing.assert_array_equal(a.relativeStandardError, b.relativeStandardError)
+    np.testing.assert_array_equal(a.totalRays, b.totalRays)
+    np.testing.assert_array_equal(a.droppedRays, b.droppedRays)
+    np.testing.assert_array_equal(a.dndtAse, b.dndtAse)
+    assert a.raysTraced == b.raysTraced and a.crossings == b.crossings
+    assert a.unconvergedSamples == b.unconvergedSamples
+
+
+def test_batch_equals_single_medium_solves(media):
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.batch import solve_sequential
+
+    items = _ranges(media)
+    with MediaBatch(0) as b:
+        res, st = b.solve(items, **KW)
+    seq = solve_sequential(items, **KW)
+    for r, s in zip(res, seq):
+        _same(r, s)
+    assert st.rows == sum(hi - lo + 1 for _, lo, hi in items)
+    assert st.passes >= 2  # the adaptive schedule ran past its first pass
+    assert st.raysTraced == sum(r.raysTraced for r in res)
+    assert st.unconvergedSamples == sum(r.unconvergedSamples for r in res)
+    assert np.all(np.isfinite([r.phiAse for r in res][0])) and all(np.all(r.phiAse > 0) for r in res)
+    assert st.chunks == 1 and st.graphNodes > st.kernelLaunches > 0
+
+
+def test_batch_with_reflections_and_chunks(media):
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.batch import solve_sequential
+
+    items = _ranges(media, n=40)
+    kw = dict(KW, useReflections=True, maxRays=16000, adaptiveSteps=2)
+    with MediaBatch(0) as b:
+        whole, st1 = b.solve(items, **kw)
+        small, st2 = b.solve(items, workspaceBytes=6 << 20, **kw)  # forces chunks that split media
+    assert st1.chunks == 1 and st2.chunks >= 3
+    seq = solve_sequential(items, **kw)
+    for a, c, s in zip(whole, small, seq):
+        _same(a, s)
+        _same(c, s)
+
+
+def test_every_launch_shape_gives_the_same_result(media):
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.autotune import variant_names
+
+    items = _ranges(media[:3], n=32)
+    kw = dict(KW, maxRays=8000, adaptiveSteps=1)
+    with MediaBatch(0) as b:
+        ref, _ = b.solve(items, **kw)
+        # the same rays in every shape; lanes (refill policy) and work items
+        # group them differently, so the FP64 sums agree to rounding
+        for v in range(1, len(variant_names())):
+            for rpt in (0, 64):
+                got, _ = b.solve(items, rayKernelVariant=v, raysPerThread=rpt, **kw)
+                for a, g in zip(ref, got):
+                    np.testing.assert_array_equal(a.totalRays, g.totalRays)
+                    np.testing.assert_array_equal(a.droppedRays, g.droppedRays)
+                    np.testing.assert_allclose(a.phiAse, g.phiAse, rtol=1e-6)
+                    np.testing.assert_allclose(a.relativeStandardError, g.relativeStandardError, rtol=1e-9)
+
+
+def test_batch_rejects_bad_ranges(media):
+    from haseongpu_b200 import MediaBatch, _native as N
+
+    c = media[0]
+    with MediaBatch(0) as b:
+        with pytest.raises(N.HaseError) as err:
+            b.solve([(c, 0, c.mesh.numberOfSamples)], minRays=100)
+        assert err.value.status == N.HASE_INVALID_ARGUMENT
+        with pytest.raises(ValueError):
+            b.solve([], minRays=100)
+        res, st = b.solve([(c, 5, 5)], minRays=100)
+        assert res[0].phiAse.shape == (1,) and st.rows == 1
