@@ -70,7 +70,7 @@ def parse():
                          "disc_small (importance-sampled solve)")
     ap.add_argument("--no-nested", action="store_true", help="learned workload only: skip the disc_poly and forward lines")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
-    ap.add_argument("--media-samples", type=int, default=128,
+    ap.add_argument("--media-samples", type=int, default=64,
                     help="media64 workload: sample points per medium (64 media) per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--path", default="backward", choices=["backward", "forward"],
@@ -568,6 +568,18 @@ def measure_media(args, local, steps, warmup):
         wall_s += time.perf_counter() - t0
         seq_ms += sum(r.totalMilliseconds for r in seq)
         same = all(np.array_equal(a.phiAse, b.phiAse) for a, b in zip(bt[s_], seq))
+    # the reference's estimator (importance weights, uniform start points) on
+    # the same media, one medium after another: the plain importance-sampled
+    # GPU path the batched solve replaces
+    plain_ms, plain_rays, plain_unconv = 0.0, 0, 0
+    pkw = dict(kw, rayKernelVariant=0, raysPerThread=0, nearFieldSampling=False)
+    for s_ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        pr = solve_sequential(items, rngSeed=1000 + 64 * s_, **pkw)
+        plain_ms += sum(r.totalMilliseconds for r in pr)
+        plain_rays += sum(r.raysTraced for r in pr)
+        plain_unconv += sum(r.unconvergedSamples for r in pr)
     # e2e: beta of every medium uploaded from host and every result read back, each step
     betas = [c.mesh.betaVolume for c in ctxs]
     torch.cuda.synchronize()
@@ -613,6 +625,12 @@ def measure_media(args, local, steps, warmup):
                        "wall_ms_per_step": wall_s * 1e3 / steps, "identical_results": bool(same),
                        "note": "the same media, one calc_phi_ase per medium (host-synchronised passes)"},
         "speedup_vs_sequential": seq_ms / ms,
+        "plain_is_sequential": {"value": steps * rows / (plain_ms * 1e-3), "unit": "samples/s",
+                                "ms_per_step": plain_ms / steps, "rays": plain_rays,
+                                "unconverged_samples": plain_unconv,
+                                "note": "the reference's importance weights with uniform start points, one medium "
+                                        "after another"},
+        "speedup_vs_plain_is_sequential": plain_ms / ms,
         "wall_ms_per_step": wall_b * 1e3 / steps,
         "e2e": {"value": steps * rows / e2e_s, "unit": "samples/s",
                 "h2d_bytes_per_step": sum(c.mesh.numberOfPrisms * 8 for c in ctxs),
@@ -741,7 +759,7 @@ def run_learned(args):
     else:
         ms_l, ms_p, ms_n, e2e_max = a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s
         rays_all, solved_all = float(a["learned"]["rays"]), float(args.steps * S)
-    disc_poly = fwd = None
+    disc_poly = fwd = media = None
     if world == 1 and not args.no_nested:
         import argparse as _ap
 
@@ -749,6 +767,7 @@ def run_learned(args):
         nargs.workload, nargs.samples = "disc_poly", 1024
         nargs.steps, nargs.warmup = max(2, min(args.steps, 3)), max(args.warmup, 3)
         disc_poly = measure_importance(nargs, local, rank, world, nested=True)
+        media = measure_media(nargs, local, steps=2, warmup=3)
         fwd = measure_forward(nargs, local, cpu_seconds=min(args.cpu_seconds, 6.0))
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -829,6 +848,11 @@ def run_learned(args):
                 "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline")}
         if fwd is not None:
             line["forward_tet4"] = fwd
+        if media is not None:
+            line["batched_media"] = {k: media[k] for k in (
+                "value", "unit", "ms_per_step", "config", "rays_per_s", "crossings_per_s", "breakdown_ms_per_step",
+                "rays_per_sample", "unconverged_samples", "graph", "sequential", "speedup_vs_sequential",
+                "plain_is_sequential", "speedup_vs_plain_is_sequential", "e2e", "roofline")}
         print(json.dumps(line), flush=True)
     net.close()
     ctx.close()
