@@ -157,6 +157,13 @@ class TetMeshDesc(C.Structure):
         ("claddingAbsorption", C.c_double),
         ("nTot", C.c_double),
         ("crystalTFluo", C.c_double),
+        ("cellFaceBoundaries", C.POINTER(C.c_int32)),
+        ("numberOfSurfaces", C.c_uint32),
+        ("surfaceReflectivities", _f64p),
+        ("surfaceRefractiveIndexInside", _f64p),
+        ("surfaceRefractiveIndexOutside", _f64p),
+        ("reflectivities", _f64p),
+        ("refractiveIndices", _f64p),
     ]
 
 
@@ -171,6 +178,11 @@ class ForwardDesc(C.Structure):
         ("batches", C.c_uint32),
         ("blockSize", C.c_uint32),
         ("tallyMode", C.c_uint32),
+        ("useReflections", C.c_uint32),
+        ("reflectionMaxIterations", C.c_uint32),
+        ("reflectionTolerance", C.c_double),
+        ("surfaceReservoirSize", C.c_uint32),
+        ("divergenceStreak", C.c_uint32),
     ]
 
 
@@ -189,7 +201,16 @@ class ForwardResultDesc(C.Structure):
         ("unconvergedCells", C.c_uint32),
         ("kernelLaunches", C.c_uint32),
         ("tallyMode", C.c_uint32),
+        ("srmStatus", C.c_uint32),
+        ("srmPasses", C.c_uint32),
+        ("srmRemainingFraction", C.c_double),
+        ("srmMaxIterations", C.c_uint32),
+        ("srmDivergenceStreak", C.c_uint32),
+        ("reflectingFaces", C.c_uint32),
     ]
+
+
+SRM_STATUS = ("disabled", "converged", "stable", "diverged", "max_iterations")
 
 
 class ProposalBatch(C.Structure):

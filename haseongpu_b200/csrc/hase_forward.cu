@@ -148,9 +148,46 @@ struct FwdRay {
     double x, y, z, ux, uy, uz, G, sA, sE;
     double pv[4];  // tallies not yet added to device memory, per corner of the current cell
     uint4 pid;     // the current cell's material vertices (owners of pv)
-    int4 nbr;      // the current cell's neighbours
+    int4 nbr;      // the current cell's neighbours (-1: boundary, <= -2: reflecting boundary face -2 - n)
     uint32_t c;
     int ff, steps;
+    uint32_t id, lam;  // ray index of the launch, wavelength bin (reflection deposits)
+};
+
+// ---- surface-reservoir reflections ----
+// A boundary face with a reflecting surface: outward unit normal, centroid
+// (start point of the reflected rays), reflectivity, squared index ratio
+// n_in / n_out (-1: no total internal reflection), its cell and the cell
+// record's (corner-sorted) local face.
+struct __align__(16) BFace {
+    double n[3], cen[3], R, ratio2;
+    uint32_t c, f, pad[2];
+};
+static_assert(sizeof(BFace) == 80, "BFace layout");
+
+// One batch's reflection chain (include/core/forwardSrm.hpp:281-363).
+struct SrmChain {
+    double initial, prev, remaining;
+    uint32_t grow, status, passes, active;
+};
+
+enum : uint32_t { kSrmDisabled = 0, kSrmConverged = 1, kSrmStable = 2, kSrmDiverged = 3, kSrmMaxIterations = 4 };
+
+struct SrmLaunch {
+    const BFace* faces;  // [nF]
+    uint32_t nF, S, pass;
+    // reservoir the launch deposits into: [B][nF] counts and weights, [B][nF][S] slots
+    uint32_t* outCounts;
+    double* outFaceW;
+    double4* outSlot;    // reflected direction, weight
+    uint32_t* outLam;
+    uint32_t* outRay;    // ray index of the deposit (slot order; see srmSortKernel)
+    // reservoir the reflected rays are drawn from, and the inclusive CDF of its face weights per batch
+    const uint32_t* inCounts;
+    const double4* inSlot;
+    const uint32_t* inLam;
+    const double* cdf;
+    SrmChain* chain;     // [B]
 };
 
 // Track-length tally of one segment: weight G (e^{gl} - 1)/g split to the
@@ -226,6 +263,7 @@ struct FwdLaunch {
     uint32_t* visits;              // [C]
     uint32_t* dropped;             // [C]
     uint32_t* next;                // [B]: next unclaimed ray index of each batch (zeroed per launch)
+    SrmLaunch srm;                 // reflection passes (kernel modes 1 and 2)
     double shift[kMaxBatches];
     uint32_t nb[kMaxBatches];
     uint32_t phase[kMaxBatches];
@@ -280,8 +318,107 @@ __device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, ui
     r.steps = 0;
     r.pid = mv;
     r.nbr = lk.nbr;
+    r.id = ray;
+    r.lam = lamIdx;
 #pragma unroll
     for (int k = 0; k < 4; ++k) r.pv[k] = 0.0;
+}
+
+// Reflected ray i of batch b (ray r = i B + b) of a reflection pass
+// (include/kernels/forward/accumulation.hpp:714-810): its face by the
+// stratified target (i + shift_b)/N_b W_b in the input reservoir's face-weight
+// CDF, its slot by weight among the face's filled slots, started at the face
+// centroid along the stored reflected direction with the chain's previous
+// total weight / N_b.  Returns false when the face holds no weight.
+__device__ __forceinline__ bool initReflectedRay(const FwdLaunch& L, uint32_t b, uint32_t i, FwdRay& r) {
+    const SrmLaunch& S = L.srm;
+    const double* cb = S.cdf + size_t(b) * S.nF;
+    const double t = (double(i) + L.shift[b]) / double(L.nb[b]) * cb[S.nF - 1];
+    uint32_t lo = 0, hi = S.nF;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (cb[mid] > t) hi = mid;
+        else lo = mid + 1;
+    }
+    const uint32_t k = min(lo, S.nF - 1);
+    const size_t face = size_t(b) * S.nF + k;
+    const uint32_t filled = min(S.inCounts[face], S.S);
+    if (filled == 0) return false;
+    const double4* slots = S.inSlot + face * S.S;
+    double slotSum = 0.0;
+    for (uint32_t q = 0; q < filled; ++q) slotSum += slots[q].w;
+    if (!(slotSum > 0.0)) return false;
+    const uint32_t ray = i * L.B + b;
+    const Philox4 o = philox4x32_10(ray, L.launch, S.pass << 2, kTagFwdRay, L.seed, kFwdKeyHi);
+    const double target = unit53(o.x) * slotSum;
+    double cum = 0.0;
+    uint32_t slot = filled - 1;
+    for (uint32_t q = 0; q < filled; ++q) {
+        cum += slots[q].w;
+        if (cum >= target) {
+            slot = q;
+            break;
+        }
+    }
+    const double4 sd = slots[slot];
+    const double len = sqrt(sd.x * sd.x + sd.y * sd.y + sd.z * sd.z);
+    const double inv = len > DBL_EPSILON ? 1.0 / len : 0.0;
+    r.ux = sd.x * inv;
+    r.uy = sd.y * inv;
+    r.uz = sd.z * inv;
+    const uint32_t lam = S.inLam[face * S.S + slot];
+    const BFace& f = S.faces[k];
+    r.x = f.cen[0];
+    r.y = f.cen[1];
+    r.z = f.cen[2];
+    r.c = f.c;
+    r.ff = int(f.f);
+    r.G = S.chain[b].prev / double(L.nb[b]);
+    r.sA = __ldg(L.sigmaA + lam);
+    r.sE = __ldg(L.sigmaE + lam);
+    r.lam = lam;
+    r.id = ray;
+    r.steps = 0;
+    const CellLinks lk = ldLinks(&L.m.cell[r.c].nbr);
+    r.pid = lk.matv;
+    r.nbr = lk.nbr;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) r.pv[q] = 0.0;
+    return true;
+}
+
+// A ray of batch b that left the mesh through reflecting face k: weight x
+// gain x reflectance (include/kernels/reflection.hpp:21-47) into the face's
+// weighted reservoir of reflected directions
+// (include/kernels/forward/accumulation.hpp:455-506).  Slots fill in arrival
+// order; once full, a deposit replaces a random slot with probability
+// min(1, S w / (W_prior + w)).
+__device__ __forceinline__ void depositReflection(const FwdLaunch& L, uint32_t b, uint32_t k, const FwdRay& r) {
+    const SrmLaunch& S = L.srm;
+    if (S.S == 0 || !(r.G > 0.0) || !isfinite(r.G)) return;
+    const BFace& f = S.faces[k];
+    const double dn = r.ux * f.n[0] + r.uy * f.n[1] + r.uz * f.n[2];
+    const double cosI = fmin(1.0, fabs(dn));
+    const double sin2 = fmax(0.0, 1.0 - cosI * cosI);
+    const double refl = (f.ratio2 > 0.0 && f.ratio2 * sin2 > 1.0) ? 1.0 : fmax(0.0, f.R);
+    const double w = r.G * refl;
+    if (!(w > 0.0) || !isfinite(w)) return;
+    const size_t face = size_t(b) * S.nF + k;
+    const uint32_t seen = atomicAdd(S.outCounts + face, 1u);
+    const double prior = atomicAdd(S.outFaceW + face, w);
+    uint32_t slot = seen;
+    if (slot >= S.S) {
+        const Philox4 o = philox4x32_10(r.id, L.launch, (S.pass << 2) | 2u, kTagFwdRay, L.seed, kFwdKeyHi);
+        const double p = fmin(1.0, double(S.S) * w / (prior + w));
+        if (unit53(o.x) >= p) return;
+        slot = min(S.S - 1, uint32_t(unit53(o.y) * double(S.S)));
+    }
+    double rx = r.ux - f.n[0] * (2.0 * dn), ry = r.uy - f.n[1] * (2.0 * dn), rz = r.uz - f.n[2] * (2.0 * dn);
+    const double rl = sqrt(rx * rx + ry * ry + rz * rz);
+    const double inv = rl > DBL_EPSILON ? 1.0 / rl : 0.0;
+    S.outSlot[face * S.S + slot] = make_double4(rx * inv, ry * inv, rz * inv, w);
+    S.outLam[face * S.S + slot] = r.lam;
+    S.outRay[face * S.S + slot] = r.id;
 }
 
 }  // namespace
@@ -291,11 +428,16 @@ namespace {
 // Block j serves batch j % B; the blocksPerBatch blocks of a batch stride its
 // rays.  SMEM: the block's vertex tallies go to a shared-memory histogram of
 // 2 Np doubles, added to the batch's device-memory tallies once at the end.
-template <bool SMEM>
+// MODE 0: source rays; 1: source rays that deposit at reflecting faces (the
+// first pass of the surface-reservoir method); 2: reflected rays drawn from
+// the reservoir, depositing in turn (blocks of a batch whose chain has ended
+// return at once).
+template <bool SMEM, int MODE>
 __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const FwdLaunch L) {
     extern __shared__ double hist[];
     const TetView& m = L.m;
     const uint32_t b = blockIdx.x % L.B;
+    if (MODE == 2 && !L.srm.chain[b].active) return;
     const uint32_t nV = 2u * m.Np;
     double* gscore = L.score + size_t(b) * nV;
     if (SMEM) {
@@ -330,8 +472,12 @@ __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const F
             if (!live) {
                 const uint32_t i = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (i < nb) {
-                    initSourceRay(L, b, i, r);
-                    live = true;
+                    if (MODE == 2) {
+                        live = initReflectedRay(L, b, i, r);
+                    } else {
+                        initSourceRay(L, b, i, r);
+                        live = true;
+                    }
                 }
             }
         }
@@ -355,6 +501,7 @@ __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const F
         const int n = bf == 0 ? r.nbr.x : bf == 1 ? r.nbr.y : bf == 2 ? r.nbr.z : r.nbr.w;
         if (n < 0) {
             flushPending(r, add);
+            if (MODE != 0 && n <= -2) depositReflection(L, b, uint32_t(-2 - n), r);
             live = false;  // left the mesh
         } else {
             r.c = uint32_t(n) >> 2;
@@ -436,6 +583,123 @@ __global__ void __launch_bounds__(256) fwdFinalizeKernel(const FinLaunch F) {
     F.rse[c] = rse;
     F.dndt[c] = (F.beta[c] * (F.dndtE + F.dndtA) - F.dndtA) * double(phi);
     if (!(isfinite(rse) && rse <= F.threshold)) atomicAdd(F.unconverged, 1u);
+}
+
+// Inclusive CDF of one batch's reservoir face weights (one block per batch,
+// FP64 block scan in chunks of the block size).
+constexpr uint32_t kScanBlock = 1024u;
+__global__ void __launch_bounds__(kScanBlock) srmScanKernel(const double* faceW, double* cdf, uint32_t nF) {
+    __shared__ double warpTot[kScanBlock / 32];
+    const double* in = faceW + size_t(blockIdx.x) * nF;
+    double* out = cdf + size_t(blockIdx.x) * nF;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double carry = 0.0;
+    for (uint32_t base = 0; base < nF; base += kScanBlock) {
+        const uint32_t k = base + threadIdx.x;
+        double v = k < nF ? in[k] : 0.0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double n = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += n;
+        }
+        if (lane == 31) warpTot[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            double t = warpTot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double n = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += n;
+            }
+            warpTot[lane] = t;
+        }
+        __syncthreads();
+        if (warp > 0) v += warpTot[warp - 1];
+        if (k < nF) out[k] = carry + v;
+        carry += warpTot[kScanBlock / 32 - 1];
+        __syncthreads();
+    }
+}
+
+// Slots in ray order: a face that received no more deposits than it has
+// slots holds every deposit, in the order the atomics happened to assign;
+// sorting them by ray index makes the reservoir (and so the next pass's
+// reflected rays) independent of that order.  Faces that overflowed keep the
+// slots their random replacements chose.  One thread per (batch, face).
+__global__ void srmSortKernel(const uint32_t* counts, double4* slot, uint32_t* lam, uint32_t* ray, uint32_t S,
+                              size_t faces) {
+    const size_t face = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (face >= faces) return;
+    const uint32_t n = counts[face];
+    if (n < 2 || n > S) return;
+    double4* sl = slot + face * S;
+    uint32_t* la = lam + face * S;
+    uint32_t* ra = ray + face * S;
+    for (uint32_t i = 1; i < n; ++i) {
+        const double4 v = sl[i];
+        const uint32_t l = la[i], r = ra[i];
+        uint32_t j = i;
+        while (j > 0 && ra[j - 1] > r) {
+            sl[j] = sl[j - 1];
+            la[j] = la[j - 1];
+            ra[j] = ra[j - 1];
+            --j;
+        }
+        sl[j] = v;
+        la[j] = l;
+        ra[j] = r;
+    }
+}
+
+// Status of every batch's chain after a pass (include/core/forwardSrm.hpp:
+// 281-363): pass 0 opens the chain with the first reservoir's weight (none:
+// converged); later passes compare the new total weight with the previous
+// one: a growth streak of `streak` passes ends it as diverged, a relative
+// change below `tol` as stable, a weight below tol x the first as converged.
+__global__ void srmControlKernel(SrmChain* chain, const double* cdf, uint32_t nF, uint32_t B, uint32_t pass,
+                                 double tol, uint32_t streak) {
+    const uint32_t b = threadIdx.x;
+    if (b >= B) return;
+    const double cur = nF ? cdf[size_t(b) * nF + nF - 1] : 0.0;
+    SrmChain& ch = chain[b];
+    if (pass == 0) {
+        ch.grow = 0;
+        ch.passes = 0;
+        if (cur == 0.0) {
+            ch.initial = ch.prev = ch.remaining = 0.0;
+            ch.status = kSrmConverged;
+            ch.active = 0;
+        } else {
+            ch.initial = ch.prev = cur;
+            ch.remaining = 1.0;
+            ch.status = kSrmMaxIterations;
+            ch.active = 1;
+        }
+        return;
+    }
+    if (!ch.active) return;
+    ch.passes = pass;
+    ch.remaining = cur / ch.initial;
+    if (cur > ch.prev) {
+        if (++ch.grow >= streak) {
+            ch.status = kSrmDiverged;
+            ch.active = 0;
+            return;
+        }
+    } else {
+        ch.grow = 0;
+        if (fabs(cur - ch.prev) / fmax(cur, 1.0e-30) < tol) {
+            ch.status = kSrmStable;
+            ch.active = 0;
+            return;
+        }
+    }
+    if (ch.remaining < tol) {
+        ch.status = kSrmConverged;
+        ch.active = 0;
+        return;
+    }
+    ch.prev = cur;
 }
 
 struct TraceLaunch {
@@ -623,6 +887,13 @@ struct hase_tet_context {
     DevBuf<uint32_t> visits, dropped, unconverged, next;
     DevBuf<unsigned long long> crossings;
     DevBuf<float> phi;
+    // reflecting boundary faces and the surface-reservoir workspace (two reservoirs)
+    DevBuf<BFace> bfaces;
+    uint32_t nBF = 0;
+    DevBuf<uint32_t> resCounts[2], resLam[2], resRay[2];
+    DevBuf<double> resW[2], cdf;
+    DevBuf<double4> resSlot[2];
+    DevBuf<SrmChain> chain;
 
     TetView view() const {
         TetView v{};
@@ -781,6 +1052,59 @@ hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spec
         rec[k].nbr = make_int4(n4[0], n4[1], n4[2], n4[3]);
         rec[k].matv = make_uint4(mv[0], mv[1], mv[2], mv[3]);
     }
+    // reflecting boundary faces: outward normal of the face's points turned
+    // away from the cell centre (include/kernels/forward/rayWalk.hpp:60-84),
+    // centroid, reflectivity and index ratio resolved as
+    // include/core/mesh.hpp:301-332; the record's neighbour code -2 - k
+    std::vector<BFace> bf;
+    if (d->cellFaceBoundaries) {
+        for (size_t k = 0; k < C; ++k) {
+            const uint32_t* v = d->cells + 4 * k;
+            for (int f = 0; f < 4; ++f) {
+                const int32_t id = d->cellFaceBoundaries[4 * k + f];
+                if (h.nbr[4 * k + f] >= 0 || id <= 0) continue;
+                BFace b{};
+                const double* P[3];
+                int n = 0;
+                for (int j = 0; j < 4; ++j)
+                    if (j != f) P[n++] = d->points + 3 * size_t(v[j]);
+                double e1[3], e2[3], cc[3] = {0, 0, 0};
+                for (int a = 0; a < 3; ++a) {
+                    e1[a] = P[1][a] - P[0][a];
+                    e2[a] = P[2][a] - P[0][a];
+                    b.cen[a] = (P[0][a] + P[1][a] + P[2][a]) / 3.0;
+                    for (int j = 0; j < 4; ++j) cc[a] += d->points[3 * size_t(v[j]) + a] / 4.0;
+                }
+                double nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                e1[0] * e2[1] - e1[1] * e2[0]};
+                const double len = std::sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+                for (int a = 0; a < 3; ++a) nn[a] /= len;
+                if (nn[0] * (cc[0] - b.cen[0]) + nn[1] * (cc[1] - b.cen[1]) + nn[2] * (cc[2] - b.cen[2]) > 0.0)
+                    for (int a = 0; a < 3; ++a) nn[a] = -nn[a];
+                for (int a = 0; a < 3; ++a) b.n[a] = nn[a];
+                const uint32_t sid = uint32_t(id);
+                if (d->surfaceReflectivities && sid < d->numberOfSurfaces) b.R = d->surfaceReflectivities[sid];
+                else b.R = d->reflectivities ? d->reflectivities[2 * k + f % 2] : 0.0;
+                double nIn, nOut;
+                if (d->surfaceRefractiveIndexInside && sid < d->numberOfSurfaces)
+                    nIn = d->surfaceRefractiveIndexInside[sid];
+                else nIn = d->refractiveIndices ? d->refractiveIndices[2 * (f % 2)] : 1.0;
+                if (d->surfaceRefractiveIndexOutside && sid < d->numberOfSurfaces)
+                    nOut = d->surfaceRefractiveIndexOutside[sid];
+                else nOut = d->refractiveIndices ? d->refractiveIndices[2 * (f % 2) + 1] : 1.0;
+                if (!std::isfinite(b.R) || !std::isfinite(nIn) || !std::isfinite(nOut))
+                    return cleanup(fail(HASE_INVALID_ARGUMENT, "surface of cell %zu face %d is not finite", k, f));
+                b.ratio2 = (nIn > 0.0 && nOut > 0.0) ? (nIn / nOut) * (nIn / nOut) : -1.0;
+                b.c = uint32_t(k);
+                b.f = inv[4 * k + f];
+                (&rec[k].nbr.x)[inv[4 * k + f]] = -2 - int(bf.size());
+                bf.push_back(b);
+            }
+        }
+        if (bf.size() >= (size_t(1) << 30)) return cleanup(fail(HASE_INVALID_ARGUMENT, "too many reflecting faces"));
+    }
+    c->nBF = uint32_t(bf.size());
+    if (!bf.empty() && (st = upload(c->bfaces, bf.data(), bf.size(), c->stream)) != HASE_OK) return cleanup(st);
     if ((st = upload(c->cell, rec.data(), C, c->stream)) != HASE_OK ||
         (st = upload(c->points, d->points, 3 * Np, c->stream)) != HASE_OK ||
         (st = upload(c->lumped, h.lumped.data(), 2 * Np, c->stream)) != HASE_OK ||
@@ -922,11 +1246,38 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
         return fail(HASE_INVALID_ARGUMENT, "shared-memory tallies need 2 * numberOfPoints * 8 <= %zu bytes",
                     kMaxHistogramBytes);
     int perSM = 0;
+    const bool srm = fw->useReflections != 0;
     if (smem) {
-        HASE_CUDA(cudaFuncSetAttribute(fwdRayKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(histBytes)));
-        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<true>, block, histBytes));
+        HASE_CUDA(cudaFuncSetAttribute(fwdRayKernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(histBytes)));
+        HASE_CUDA(cudaFuncSetAttribute(fwdRayKernel<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(histBytes)));
+        HASE_CUDA(cudaFuncSetAttribute(fwdRayKernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(histBytes)));
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<true, 0>, block, histBytes));
     } else {
-        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<false>, block, 0));
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fwdRayKernel<false, 0>, block, 0));
+    }
+    // surface-reservoir controls (include/core/types.hpp:328-330, src/core/srm.cpp:36-41)
+    const uint32_t srmMaxIt = fw->reflectionMaxIterations ? fw->reflectionMaxIterations : 40u;
+    const double srmTol = fw->reflectionTolerance > 0.0 ? fw->reflectionTolerance : 1.0e-4;
+    const uint32_t srmSlots = fw->surfaceReservoirSize ? fw->surfaceReservoirSize : 32u;
+    const uint32_t srmStreak = fw->divergenceStreak ? fw->divergenceStreak : 3u;
+    if (srm && !(std::isfinite(fw->reflectionTolerance) && fw->reflectionTolerance >= 0.0))
+        return fail(HASE_INVALID_ARGUMENT, "reflectionTolerance must be >= 0");
+    if (srm && srmSlots > 4096) return fail(HASE_INVALID_ARGUMENT, "surfaceReservoirSize must be <= 4096");
+    const uint32_t nF = c->nBF;
+    if (srm && nF > 0) {
+        const size_t faces = size_t(B) * nF, slots = faces * srmSlots;
+        for (int k = 0; k < 2; ++k) {
+            HASE_CUDA(c->resCounts[k].ensure(faces));
+            HASE_CUDA(c->resW[k].ensure(faces));
+            HASE_CUDA(c->resSlot[k].ensure(slots));
+            HASE_CUDA(c->resLam[k].ensure(slots));
+            HASE_CUDA(c->resRay[k].ensure(slots));
+        }
+        HASE_CUDA(c->cdf.ensure(faces));
+        HASE_CUDA(c->chain.ensure(B));
     }
     if (perSM < 1) return fail(HASE_CUDA_ERROR, "the ray kernel does not fit on an SM");
     const uint32_t resident = uint32_t(perSM) * c->numSMs;
@@ -996,6 +1347,13 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
     res->unconvergedCells = 0;
     res->kernelLaunches = 0;
     res->tallyMode = smem ? 2u : 1u;
+    res->srmStatus = srm ? kSrmConverged : kSrmDisabled;
+    res->srmPasses = 0;
+    res->srmRemainingFraction = 0.0;
+    res->srmMaxIterations = srm ? srmMaxIt : 0u;
+    res->srmDivergenceStreak = srm ? srmStreak : 0u;
+    res->reflectingFaces = nF;
+    bool chainRan = false;
 
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     HASE_CUDA(cudaEventCreate(&t0));
@@ -1034,11 +1392,62 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
             L.blocksPerBatch = perBatch;
             HASE_CUDA(cudaMemsetAsync(c->next.p, 0, B * sizeof(uint32_t), c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
-            if (smem) fwdRayKernel<true><<<perBatch * B, block, histBytes, c->stream>>>(L);
-            else fwdRayKernel<false><<<perBatch * B, block, 0, c->stream>>>(L);
-            HASE_CUDA(cudaGetLastError());
+            const uint32_t grid = perBatch * B;
+            const size_t shm = smem ? histBytes : 0;
+            if (!srm || nF == 0) {
+                if (smem) fwdRayKernel<true, 0><<<grid, block, shm, c->stream>>>(L);
+                else fwdRayKernel<false, 0><<<grid, block, shm, c->stream>>>(L);
+                HASE_CUDA(cudaGetLastError());
+                res->kernelLaunches += 1;
+            } else {
+                // surface-reservoir chain: the source pass deposits into
+                // reservoir 0, reflected pass p reads reservoir (p - 1) % 2 and
+                // deposits into p % 2; every pass is queued, batches whose
+                // chain ended skip the rest on the device (no host sync)
+                const size_t faces = size_t(B) * nF;
+                SrmLaunch& S = L.srm;
+                S.faces = c->bfaces.p;
+                S.nF = nF;
+                S.S = srmSlots;
+                S.cdf = c->cdf.p;
+                S.chain = c->chain.p;
+                for (uint32_t pass = 0; pass <= srmMaxIt; ++pass) {
+                    const int out = int(pass & 1u), in = 1 - out;
+                    S.pass = pass;
+                    S.outCounts = c->resCounts[out].p;
+                    S.outFaceW = c->resW[out].p;
+                    S.outSlot = c->resSlot[out].p;
+                    S.outLam = c->resLam[out].p;
+                    S.outRay = c->resRay[out].p;
+                    S.inCounts = c->resCounts[in].p;
+                    S.inSlot = c->resSlot[in].p;
+                    S.inLam = c->resLam[in].p;
+                    HASE_CUDA(cudaMemsetAsync(S.outCounts, 0, faces * sizeof(uint32_t), c->stream));
+                    HASE_CUDA(cudaMemsetAsync(S.outFaceW, 0, faces * sizeof(double), c->stream));
+                    if (pass > 0) {
+                        HASE_CUDA(cudaMemsetAsync(c->next.p, 0, B * sizeof(uint32_t), c->stream));
+                        for (uint32_t b = 0; b < B; ++b) {
+                            const Philox4 o = philox4x32_10(b, launch, pass, kTagFwdBatch, fw->rngSeed, kFwdKeyHi);
+                            L.shift[b] = double(o.x) / 4294967296.0;
+                        }
+                        if (smem) fwdRayKernel<true, 2><<<grid, block, shm, c->stream>>>(L);
+                        else fwdRayKernel<false, 2><<<grid, block, shm, c->stream>>>(L);
+                    } else {
+                        if (smem) fwdRayKernel<true, 1><<<grid, block, shm, c->stream>>>(L);
+                        else fwdRayKernel<false, 1><<<grid, block, shm, c->stream>>>(L);
+                    }
+                    HASE_CUDA(cudaGetLastError());
+                    srmSortKernel<<<uint32_t((faces + 255) / 256), 256, 0, c->stream>>>(
+                        S.outCounts, S.outSlot, S.outLam, S.outRay, srmSlots, faces);
+                    srmScanKernel<<<B, kScanBlock, 0, c->stream>>>(S.outFaceW, c->cdf.p, nF);
+                    srmControlKernel<<<1, kMaxBatches, 0, c->stream>>>(c->chain.p, c->cdf.p, nF, B, pass, srmTol,
+                                                                      srmStreak);
+                    HASE_CUDA(cudaGetLastError());
+                    res->kernelLaunches += 4;
+                }
+                chainRan = true;
+            }
             HASE_CUDA(cudaEventRecord(c->ev[1], c->stream));
-            res->kernelLaunches += 1;
         }
         total = target;
         F.totalRays = double(total);
@@ -1055,6 +1464,23 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
             res->rayMilliseconds += ms;
         }
         res->launches = launch + 1;
+        if (chainRan) {  // the last launch's chains are the ones reported
+            std::vector<SrmChain> ch(B);
+            HASE_CUDA(cudaMemcpy(ch.data(), c->chain.p, B * sizeof(SrmChain), cudaMemcpyDeviceToHost));
+            auto priority = [](uint32_t st) {
+                return st == kSrmDiverged ? 4 : st == kSrmMaxIterations ? 3 : st == kSrmStable ? 2
+                                            : st == kSrmConverged ? 1 : 0;
+            };
+            res->srmStatus = kSrmDisabled;
+            res->srmPasses = 0;
+            res->srmRemainingFraction = 0.0;
+            for (const SrmChain& x : ch) {
+                if (priority(x.status) > priority(res->srmStatus)) res->srmStatus = x.status;
+                res->srmPasses = std::max(res->srmPasses, x.passes);
+                res->srmRemainingFraction = std::max(res->srmRemainingFraction, x.remaining);
+            }
+            chainRan = false;
+        }
         if (target >= maxRays || !adaptive || unconverged == 0) break;
     }
     HASE_CUDA(cudaEventRecord(t1, c->stream));

@@ -32,10 +32,17 @@ class TetDeviceMesh:
         if sa.size != se.size or sa.size == 0:
             raise ValueError("sigmaA and sigmaE must be non-empty and of equal length")
         clad = None if mesh.claddingCellTypes is None else N.ptr(self._hold(mesh.claddingCellTypes), N._u32p)
+
+        def opt(v, t):
+            return None if v is None else N.ptr(self._hold(v), t)
+
+        surf = mesh.surfaceArrays()
         desc = N.TetMeshDesc(mesh.numberOfPoints, mesh.numberOfCells, N.ptr(self._hold(mesh.points), N._f64p),
                              N.ptr(self._hold(mesh.cells), N._u32p), N.ptr(self._hold(mesh.betaVolume), N._f64p),
                              clad, int(mesh.claddingNumber), float(mesh.claddingAbsorption), float(mesh.nTot),
-                             float(mesh.crystalTFluo))
+                             float(mesh.crystalTFluo), opt(mesh.cellFaceBoundaries, C.POINTER(C.c_int32)),
+                             mesh.numberOfSurfaces, *[opt(v, N._f64p) for v in surf],
+                             opt(mesh.reflectivities, N._f64p), opt(mesh.refractiveIndices, N._f64p))
         spec = N.SpectrumDesc(sa.size, N.ptr(sa, N._f64p), N.ptr(se, N._f64p))
         handle = C.c_void_p()
         N.check(N.lib().hase_tet_context_create(C.byref(desc), C.byref(spec), int(device), C.byref(handle)))
@@ -54,7 +61,12 @@ class TetDeviceMesh:
         N.check(N.lib().hase_tet_context_update_beta(self.handle, N.ptr(bv, N._f64p)))
 
     def calc_phi_ase(self, *, forwardRayCount, maxRays=None, adaptiveSteps=0, relativeStandardErrorThreshold=0.0,
-                     monochromatic=False, rngSeed=5489, batches=8, blockSize=0, tallyMode="auto") -> Result:
+                     monochromatic=False, rngSeed=5489, batches=8, blockSize=0, tallyMode="auto",
+                     useReflections=False, reflectionMaxIterations=40, reflectionTolerance=1.0e-4,
+                     surfaceReservoirSize=32, divergenceStreak=3) -> Result:
+        """The forward solve; with ``useReflections`` the surface-reservoir
+        reflection passes run at the mesh's reflecting boundary faces and the
+        ``srm*`` fields of the result are filled."""
         n = self.mesh.numberOfCells
         out = Result(phiAse=np.empty(n, np.float32), relativeStandardError=np.empty(n),
                      totalRays=np.empty(n, np.uint32), dndtAse=np.empty(n), droppedRays=np.empty(n, np.uint32))
@@ -62,7 +74,9 @@ class TetDeviceMesh:
             raise ValueError(f"tallyMode must be one of {sorted(TALLY_MODES)}")
         fw = N.ForwardDesc(int(forwardRayCount), int(maxRays if maxRays is not None else forwardRayCount),
                            int(adaptiveSteps), float(relativeStandardErrorThreshold), 1 if monochromatic else 0,
-                           int(rngSeed) & 0xFFFFFFFF, int(batches), int(blockSize), TALLY_MODES[tallyMode])
+                           int(rngSeed) & 0xFFFFFFFF, int(batches), int(blockSize), TALLY_MODES[tallyMode],
+                           1 if useReflections else 0, int(reflectionMaxIterations), float(reflectionTolerance),
+                           int(surfaceReservoirSize), int(divergenceStreak))
         r = N.ForwardResultDesc(N.ptr(out.phiAse, N._f32p), N.ptr(out.relativeStandardError, N._f64p),
                                 N.ptr(out.dndtAse, N._f64p), N.ptr(out.totalRays, N._u32p),
                                 N.ptr(out.droppedRays, N._u32p))
@@ -76,6 +90,12 @@ class TetDeviceMesh:
         out.unconvergedSamples = int(r.unconvergedCells)
         out.kernelLaunches = int(r.kernelLaunches)
         out.tallyMode = int(r.tallyMode)
+        out.srmStatus = N.SRM_STATUS[r.srmStatus]
+        out.srmPasses = int(r.srmPasses)
+        out.srmRemainingFraction = float(r.srmRemainingFraction)
+        out.srmMaxIterations = int(r.srmMaxIterations)
+        out.srmDivergenceStreak = int(r.srmDivergenceStreak)
+        out.reflectingFaces = int(r.reflectingFaces)
         return out
 
     def tables(self):

@@ -44,6 +44,7 @@ class Result:
     srmRemainingFraction: float = 0.0
     srmMaxIterations: int = 0
     srmDivergenceStreak: int = 0
+    reflectingFaces: int = 0
     raysTraced: int = 0
     crossings: int = 0
     importanceMilliseconds: float = 0.0
@@ -348,9 +349,6 @@ class PhiASE:
         from .forward import TetDeviceMesh
         from .tetmesh import TetMesh
 
-        if self.useReflections:
-            raise ValueError("useReflections with propagationMode='forward' (surface reflections of the forward "
-                             "method) is not provided; use propagationMode='backward'")
         if isinstance(medium, PrismMesh):
             key = medium
             if self._tetTwin is None or self._tetTwin[0] is not medium:
@@ -374,7 +372,9 @@ class PhiASE:
         self._result = ctx.calc_phi_ase(
             forwardRayCount=minRays, maxRays=maxRays, adaptiveSteps=0 if rays else self.adaptiveSteps,
             relativeStandardErrorThreshold=self.relativeStandardErrorThreshold, monochromatic=self.monochromatic,
-            rngSeed=5489 if self.rngSeed is None else self.rngSeed)
+            rngSeed=5489 if self.rngSeed is None else self.rngSeed, useReflections=self.useReflections,
+            reflectionMaxIterations=self.reflectionMaxIterations, reflectionTolerance=self.reflectionTolerance,
+            surfaceReservoirSize=self.surfaceReservoirSize)
         self._result.standardError = self._result.relativeStandardError * self._result.phiAse
         return self
 

@@ -33,6 +33,18 @@ class TetMesh:
     claddingNumber: int = 1
     claddingAbsorption: float = 0.0        # cm^-1
     name: str = field(default="tet4-mesh", compare=False)
+    # Reflecting boundary surfaces (include/core/mesh.hpp:301-332): surface
+    # id per local face (> 0 on a boundary face: a reflecting surface), per
+    # surface reflectivity and refractive indices inside / outside; ids
+    # outside the per-surface arrays fall back to the legacy per-cell
+    # ``reflectivities`` [C, 2] (by local face % 2) and ``refractiveIndices``
+    # [4] (face % 2 = 0: inside, outside; face % 2 = 1: inside, outside).
+    cellFaceBoundaries: np.ndarray | None = None     # [C, 4] int32
+    surfaceReflectivities: np.ndarray | None = None  # [S]
+    surfaceRefractiveIndexInside: np.ndarray | None = None
+    surfaceRefractiveIndexOutside: np.ndarray | None = None
+    reflectivities: np.ndarray | None = None         # legacy [C, 2]
+    refractiveIndices: np.ndarray | None = None      # legacy [4]
 
     def __post_init__(self):
         self.points = np.ascontiguousarray(np.asarray(self.points, np.float64).reshape(-1, 3))
@@ -46,6 +58,19 @@ class TetMesh:
             self.claddingCellTypes = np.ascontiguousarray(np.asarray(self.claddingCellTypes, np.uint32).ravel())
             if self.claddingCellTypes.size != self.numberOfCells:
                 raise ValueError("claddingCellTypes must have one entry per cell")
+        if self.cellFaceBoundaries is not None:
+            self.cellFaceBoundaries = np.ascontiguousarray(np.asarray(self.cellFaceBoundaries, np.int32).reshape(-1, 4))
+            if self.cellFaceBoundaries.shape[0] != self.numberOfCells:
+                raise ValueError("cellFaceBoundaries must have one row of 4 surface ids per cell")
+        for name in ("surfaceReflectivities", "surfaceRefractiveIndexInside", "surfaceRefractiveIndexOutside",
+                     "refractiveIndices"):
+            v = getattr(self, name)
+            if v is not None:
+                setattr(self, name, np.ascontiguousarray(np.asarray(v, np.float64).ravel()))
+        if self.reflectivities is not None:
+            self.reflectivities = np.ascontiguousarray(np.asarray(self.reflectivities, np.float64).reshape(-1, 2))
+            if self.reflectivities.shape[0] != self.numberOfCells:
+                raise ValueError("reflectivities must have one row of 2 per cell")
         self.claddingNumber = int(self.claddingNumber)
         self.claddingAbsorption = float(self.claddingAbsorption)
         self.nTot = float(self.nTot)
@@ -72,9 +97,45 @@ class TetMesh:
             return np.zeros(self.numberOfCells, bool)
         return self.claddingCellTypes == self.claddingNumber
 
+    @property
+    def numberOfSurfaces(self) -> int:
+        return max(0 if v is None else int(v.size) for v in (self.surfaceReflectivities,
+                                                             self.surfaceRefractiveIndexInside,
+                                                             self.surfaceRefractiveIndexOutside))
+
+    def surfaceArrays(self) -> tuple:
+        """Per-surface arrays padded to numberOfSurfaces (None stays None)."""
+        n = self.numberOfSurfaces
+        out = []
+        for v, fill in ((self.surfaceReflectivities, 0.0), (self.surfaceRefractiveIndexInside, 1.0),
+                        (self.surfaceRefractiveIndexOutside, 1.0)):
+            out.append(None if v is None else np.concatenate([v, np.full(n - v.size, fill)]))
+        return tuple(out)
+
+    def boundaryFaces(self) -> np.ndarray:
+        """[C, 4] bool: local faces without a neighbour."""
+        from collections import Counter
+
+        faces = np.sort(np.stack([np.delete(self.cells, f, axis=1) for f in range(4)], axis=1), axis=2)
+        keys = [tuple(k) for k in faces.reshape(-1, 3)]
+        count = Counter(keys)
+        return np.array([count[k] == 1 for k in keys]).reshape(-1, 4)
+
     def withBeta(self, betaVolume) -> "TetMesh":
         return TetMesh(self.points, self.cells, betaVolume, self.nTot, self.crystalTFluo, self.claddingCellTypes,
-                       self.claddingNumber, self.claddingAbsorption, self.name)
+                       self.claddingNumber, self.claddingAbsorption, self.name, self.cellFaceBoundaries,
+                       self.surfaceReflectivities, self.surfaceRefractiveIndexInside,
+                       self.surfaceRefractiveIndexOutside, self.reflectivities, self.refractiveIndices)
+
+    def withReflectingBoundary(self, reflectivity: float, nInside: float = 1.0, nOutside: float = 1.0) -> "TetMesh":
+        """The same mesh with every boundary face on one reflecting surface (id 1)."""
+        ids = np.where(self.boundaryFaces(), 1, 0).astype(np.int32)
+        m = self.withBeta(self.betaVolume)
+        m.cellFaceBoundaries = ids
+        m.surfaceReflectivities = np.array([0.0, float(reflectivity)])
+        m.surfaceRefractiveIndexInside = np.array([1.0, float(nInside)])
+        m.surfaceRefractiveIndexOutside = np.array([1.0, float(nOutside)])
+        return m
 
     @classmethod
     def fromFixture(cls, path, claddingAbsorption=None) -> "TetMesh":
@@ -116,8 +177,26 @@ class TetMesh:
         clad = None
         if prism.claddingCellTypes is not None:
             clad = np.repeat(np.tile(prism.claddingCellTypes, L - 1), 3)
-        return cls(pts, cells.reshape(-1, 4), np.repeat(prism.betaVolume, 3), prism.nTot, prism.crystalTFluo, clad,
-                   prism.claddingNumber, prism.claddingAbsorption, name=f"{prism.name}-tet4")
+        out = cls(pts, cells.reshape(-1, 4), np.repeat(prism.betaVolume, 3), prism.nTot, prism.crystalTFluo, clad,
+                  prism.claddingNumber, prism.claddingAbsorption, name=f"{prism.name}-tet4")
+        if getattr(prism, "reflectivities", None) is not None:
+            # bottom face of cell 0 of layer 0 (opposite corner 3) and top face
+            # of cell 2 of the last layer (opposite corner 0): surface 1 + 2 t
+            # (bottom of triangle t) and 2 + 2 t (top), with the prism's
+            # reflectivities and refractive indices
+            C = out.numberOfCells
+            ids = np.zeros((C, 4), np.int32)
+            t = np.arange(T)
+            ids[3 * t, 3] = 1 + 2 * t
+            ids[3 * ((L - 2) * T + t) + 2, 0] = 2 + 2 * t
+            R = np.asarray(prism.reflectivities, np.float64).reshape(T, 2)
+            n = np.asarray(prism.refractiveIndices if getattr(prism, "refractiveIndices", None) is not None
+                           else [1.0, 1.0, 1.0, 1.0], np.float64)
+            out.cellFaceBoundaries = ids
+            out.surfaceReflectivities = np.concatenate([[0.0], R.ravel()])
+            out.surfaceRefractiveIndexInside = np.concatenate([[1.0], np.tile([n[0], n[2]], T)])
+            out.surfaceRefractiveIndexOutside = np.concatenate([[1.0], np.tile([n[1], n[3]], T)])
+        return out
 
     @classmethod
     def ball(cls, radius: float, divisions: int, beta: float, nTot: float, crystalTFluo: float) -> "TetMesh":

@@ -29,6 +29,11 @@
  *                                  totalRays (= cell ray visits,
  *                                  include/core/calcForwardPhiAse.hpp:258),
  *                                  droppedRays
+ *   useReflections (SRM)         - the surface-reservoir reflection passes
+ *                                  (include/core/forwardSrm.hpp:100-365,
+ *                                  include/kernels/forward/accumulation.hpp:455-833,
+ *                                  reflectance include/kernels/reflection.hpp:21-47,
+ *                                  surfaces include/core/mesh.hpp:301-332)
  *   hase_tet_trace               - one ray through the mesh, as the reference's
  *                                  traversal tests drive nextFaceIntersection /
  *                                  transitionAcrossIntersection
@@ -57,6 +62,21 @@ typedef struct {
     double claddingAbsorption;          /* cladding absorption coefficient (cm^-1) */
     double nTot;                        /* doping density (cm^-3) */
     double crystalTFluo;                /* fluorescence lifetime (s) */
+    /* Reflecting boundary surfaces (used with hase_forward_desc.useReflections).
+     * A boundary face whose surface id is > 0 reflects: its reflectivity is
+     * surfaceReflectivities[id] when id < numberOfSurfaces, else the legacy
+     * reflectivities[cell * 2 + face % 2] (0 when NULL); its refractive
+     * indices likewise come from the per-surface arrays or the legacy
+     * refractiveIndices[2 * (face % 2)] (inside) and [2 * (face % 2) + 1]
+     * (outside), 1 when NULL.  Total internal reflection (reflectance 1) when
+     * (n_in / n_out)^2 sin^2(incidence) > 1.  All pointers may be NULL. */
+    const int32_t* cellFaceBoundaries;             /* [numberOfCells][4] surface id per local face */
+    uint32_t numberOfSurfaces;
+    const double* surfaceReflectivities;           /* [numberOfSurfaces] */
+    const double* surfaceRefractiveIndexInside;    /* [numberOfSurfaces] */
+    const double* surfaceRefractiveIndexOutside;   /* [numberOfSurfaces] */
+    const double* reflectivities;                  /* legacy [numberOfCells][2] */
+    const double* refractiveIndices;               /* legacy [4] */
 } hase_tet_mesh_desc;
 
 typedef struct {
@@ -70,6 +90,17 @@ typedef struct {
     uint32_t blockSize;                 /* threads per block of the ray kernel; 0 = default */
     uint32_t tallyMode;                 /* 0 = automatic, 1 = device-memory atomics,
                                            2 = per-block shared-memory vertex tallies */
+    /* Surface-reservoir method (SRM): rays leaving through a reflecting face
+     * deposit weight x gain x reflectance into a per-face reservoir of
+     * reflected directions; every launch then runs reflected passes of the
+     * same ray count from the reservoir (start at the face centroid) until the
+     * reflected weight converges, stabilises, diverges or the pass limit is
+     * reached.  Every statistical batch runs its own chain. */
+    uint32_t useReflections;
+    uint32_t reflectionMaxIterations;   /* reflected passes per launch; 0 = 40 */
+    double reflectionTolerance;         /* 0 = 1e-4 */
+    uint32_t surfaceReservoirSize;      /* reservoir slots per reflecting face; 0 = 32 */
+    uint32_t divergenceStreak;          /* passes of growing weight that end a chain as diverged; 0 = 3 */
 } hase_forward_desc;
 
 /* Caller-allocated host arrays of numberOfCells entries; any pointer may be
@@ -89,6 +120,17 @@ typedef struct {
     uint32_t unconvergedCells;
     uint32_t kernelLaunches;            /* kernels this call launched */
     uint32_t tallyMode;                 /* tally mode used (1 or 2) */
+    /* SRM outputs of the last launch (include/core/types.hpp:174-246): the
+     * worst status over the batches (0 disabled, 1 converged, 2 stable,
+     * 3 diverged, 4 max_iterations; worst = diverged > max_iterations >
+     * stable > converged), the most passes, the largest remaining fraction
+     * of the first reflected weight */
+    uint32_t srmStatus;
+    uint32_t srmPasses;
+    double srmRemainingFraction;
+    uint32_t srmMaxIterations;
+    uint32_t srmDivergenceStreak;
+    uint32_t reflectingFaces;           /* boundary faces with a reflecting surface */
 } hase_forward_result;
 
 hase_status hase_tet_context_create(const hase_tet_mesh_desc* mesh, const hase_spectrum_desc* spectrum, int device,

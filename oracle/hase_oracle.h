@@ -128,6 +128,15 @@ typedef struct {
     double claddingAbsorption;
     double nTot;
     double crystalTFluo;
+    /* reflecting boundary surfaces (include/core/mesh.hpp:301-332,
+     * include/kernels/reflection.hpp:21-47); all may be NULL */
+    const int32_t* cellFaceBoundaries;             /* [C][4] surface id (> 0: a reflecting surface) */
+    uint32_t numberOfSurfaces;
+    const double* surfaceReflectivities;           /* [numberOfSurfaces] */
+    const double* surfaceRefractiveIndexInside;    /* [numberOfSurfaces] */
+    const double* surfaceRefractiveIndexOutside;   /* [numberOfSurfaces] */
+    const double* reflectivities;                  /* legacy [C][2], by local face % 2 */
+    const double* refractiveIndices;               /* legacy [4] */
 } oracle_tet_mesh;
 
 typedef struct {
@@ -137,6 +146,12 @@ typedef struct {
     double rseThreshold;
     uint32_t seed;
     uint32_t batches;          /* statistical batches (reference default 8) */
+    /* surface-reservoir reflections (include/core/forwardSrm.hpp:100-365) */
+    uint32_t useReflections;
+    uint32_t reflectionMaxIterations;
+    double reflectionTolerance;
+    uint32_t surfaceReservoirSize;
+    uint32_t divergenceStreak;
 } oracle_forward_experiment;
 
 typedef struct {
@@ -147,6 +162,12 @@ typedef struct {
     uint32_t* rayVisits;       /* [C] segments tallied per cell (the reference's forward totalRays), or NULL */
     uint64_t totalRays;
     uint32_t launches;
+    /* SRM outputs of the last launch: worst status over the batches
+     * (0 disabled, 1 converged, 2 stable, 3 diverged, 4 max_iterations), most
+     * passes, largest remaining weight fraction */
+    uint32_t srmStatus;
+    uint32_t srmPasses;
+    double srmRemainingFraction;
 } oracle_forward_result;
 
 /* Tet tables: neighbours [C][4] (-1 boundary), neighbour local face [C][4],

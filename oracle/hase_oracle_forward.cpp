@@ -27,6 +27,7 @@
 #include "hase_oracle.h"
 
 #include <algorithm>
+#include <numeric>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -163,11 +164,16 @@ struct Segment {
     double length, gl;
 };
 
+// G0: the ray's starting weight (1 for a source ray, the reservoir's source
+// weight for a reflected ray); ff0: its entry face (-1: none).  On escape,
+// exitCell / exitFace / Gout (when given) receive the boundary face and the
+// weight times the accumulated gain at it.
 int64_t walkForward(const FwdModel& md, uint32_t c, double x[3], const double u[3], double sA, double sE,
-                    double* score, uint32_t* visits, std::vector<Segment>* path) {
+                    double* score, uint32_t* visits, std::vector<Segment>* path, double G0 = 1.0, int ff0 = -1,
+                    uint32_t* exitCell = nullptr, int* exitFace = nullptr, double* Gout = nullptr) {
     const oracle_tet_mesh* m = md.m;
-    int ff = -1;
-    double G = 1.0;
+    int ff = ff0;
+    double G = G0;
     for (int step = 0; step < kMaxSteps; ++step) {
         const double* pl = &md.tab.plane[16 * size_t(c)];
         double lam[4], dl[4];
@@ -203,7 +209,12 @@ int64_t walkForward(const FwdModel& md, uint32_t c, double x[3], const double u[
         }
         for (int d = 0; d < 3; ++d) x[d] += u[d] * best;
         const int32_t n = md.tab.nbr[4 * size_t(c) + bf];
-        if (n < 0) return -1;  // escaped through the boundary
+        if (n < 0) {  // escaped through the boundary
+            if (exitCell) *exitCell = c;
+            if (exitFace) *exitFace = bf;
+            if (Gout) *Gout = G;
+            return -1;
+        }
         ff = md.tab.nbrFace[4 * size_t(c) + bf];
         c = uint32_t(n);
     }
@@ -225,6 +236,147 @@ uint32_t fwdTarget(const oracle_forward_experiment* e, uint32_t k) {
     const double growth = std::pow(double(e->maxRays) / double(e->minRays), 1.0 / double(e->adaptiveSteps));
     const uint32_t r = uint32_t(std::ceil(double(e->minRays) * std::pow(growth, double(k))));
     return std::min(std::max(r, e->minRays), e->maxRays);
+}
+
+// ---- surface-reservoir reflections (include/core/forwardSrm.hpp:100-365,
+// include/kernels/forward/accumulation.hpp:455-833) ----
+
+// A boundary face with a reflecting surface (surface id > 0): outward unit
+// normal normalize((b - a) x (c - a)) turned away from the cell centre
+// (include/kernels/forward/rayWalk.hpp:60-84), centroid (the reflected rays'
+// start point, rayWalk.hpp:44-58), reflectivity and squared index ratio
+// n_inside / n_outside (-1: no total internal reflection) as
+// include/core/mesh.hpp:301-332 resolve them.
+struct BFace {
+    uint32_t c;
+    int f;
+    double n[3], cen[3], R, ratio2;
+};
+
+void buildBoundaryFaces(const FwdModel& md, std::vector<BFace>& faces) {
+    const oracle_tet_mesh* m = md.m;
+    faces.clear();
+    if (!m->cellFaceBoundaries) return;
+    for (uint32_t c = 0; c < m->numberOfCells; ++c) {
+        const uint32_t* v = m->cells + 4 * size_t(c);
+        for (int f = 0; f < 4; ++f) {
+            const int32_t id = m->cellFaceBoundaries[4 * size_t(c) + f];
+            if (md.tab.nbr[4 * size_t(c) + f] >= 0 || id <= 0) continue;
+            BFace b{};
+            b.c = c;
+            b.f = f;
+            const double* P[3];
+            int n = 0;
+            for (int k = 0; k < 4; ++k)
+                if (k != f) P[n++] = m->points + 3 * size_t(v[k]);
+            double e1[3], e2[3], cc[3] = {0, 0, 0}, cen[3] = {0, 0, 0};
+            for (int d = 0; d < 3; ++d) {
+                e1[d] = P[1][d] - P[0][d];
+                e2[d] = P[2][d] - P[0][d];
+                b.cen[d] = (P[0][d] + P[1][d] + P[2][d]) / 3.0;
+                for (int k = 0; k < 4; ++k) cc[d] += m->points[3 * size_t(v[k]) + d] / 4.0;
+                cen[d] = b.cen[d];
+            }
+            double nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            const double len = std::sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+            for (int d = 0; d < 3; ++d) nn[d] /= len;
+            if (nn[0] * (cc[0] - cen[0]) + nn[1] * (cc[1] - cen[1]) + nn[2] * (cc[2] - cen[2]) > 0.0)
+                for (int d = 0; d < 3; ++d) nn[d] = -nn[d];
+            for (int d = 0; d < 3; ++d) b.n[d] = nn[d];
+            const uint32_t sid = uint32_t(id);
+            if (m->surfaceReflectivities && sid < m->numberOfSurfaces) b.R = m->surfaceReflectivities[sid];
+            else b.R = m->reflectivities ? m->reflectivities[2 * size_t(c) + f % 2] : 0.0;
+            double nIn, nOut;
+            if (m->surfaceRefractiveIndexInside && sid < m->numberOfSurfaces) nIn = m->surfaceRefractiveIndexInside[sid];
+            else nIn = m->refractiveIndices ? m->refractiveIndices[2 * (f % 2)] : 1.0;
+            if (m->surfaceRefractiveIndexOutside && sid < m->numberOfSurfaces)
+                nOut = m->surfaceRefractiveIndexOutside[sid];
+            else nOut = m->refractiveIndices ? m->refractiveIndices[2 * (f % 2) + 1] : 1.0;
+            b.ratio2 = (nIn > 0.0 && nOut > 0.0) ? (nIn / nOut) * (nIn / nOut) : -1.0;
+            faces.push_back(b);
+        }
+    }
+}
+
+// include/kernels/reflection.hpp:21-47
+double boundaryReflectance(const BFace& b, const double u[3]) {
+    const double un = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double cosI = std::min(1.0, std::fabs((u[0] * b.n[0] + u[1] * b.n[1] + u[2] * b.n[2]) / un));
+    const double sin2 = std::max(0.0, 1.0 - cosI * cosI);
+    if (b.ratio2 > 0.0 && b.ratio2 * sin2 > 1.0) return 1.0;
+    return std::max(0.0, b.R);
+}
+
+struct Reservoir {
+    uint32_t S = 0, nF = 0, B = 0;
+    std::vector<uint32_t> counts, lam;     // [B][nF], [B][nF][S]
+    std::vector<double> faceW, dir, w;     // [B][nF], [B][nF][S][3], [B][nF][S]
+    void init(uint32_t b, uint32_t f, uint32_t s) {
+        B = b;
+        nF = f;
+        S = s;
+        counts.assign(size_t(B) * nF, 0u);
+        faceW.assign(size_t(B) * nF, 0.0);
+        lam.assign(size_t(B) * nF * S, 0u);
+        w.assign(size_t(B) * nF * S, 0.0);
+        dir.assign(size_t(B) * nF * S * 3, 0.0);
+    }
+    void clear() {
+        std::fill(counts.begin(), counts.end(), 0u);
+        std::fill(faceW.begin(), faceW.end(), 0.0);
+    }
+};
+
+// A ray that left the mesh through reflecting face k of batch b.
+struct Deposit {
+    uint32_t ray, b, k, lam;
+    double G, u[3];
+};
+
+// include/kernels/forward/accumulation.hpp:455-506: weighted reservoir of
+// reflected directions per face; uA, uB decide a replacement once the face's
+// slots are full.
+void deposit(Reservoir& res, const BFace& bf, const Deposit& d, double uA, double uB) {
+    if (res.S == 0 || !(d.G > 0.0) || !std::isfinite(d.G)) return;
+    const double w = d.G * boundaryReflectance(bf, d.u);
+    if (!(w > 0.0) || !std::isfinite(w)) return;
+    const size_t face = size_t(d.b) * res.nF + d.k;
+    const uint32_t seen = res.counts[face]++;
+    const double prior = res.faceW[face];
+    res.faceW[face] += w;
+    uint32_t slot = seen;
+    if (slot >= res.S) {
+        const double p = std::min(1.0, double(res.S) * w / (prior + w));
+        if (uA >= p) return;
+        slot = std::min(res.S - 1, uint32_t(uB * double(res.S)));
+    }
+    const double dn = d.u[0] * bf.n[0] + d.u[1] * bf.n[1] + d.u[2] * bf.n[2];
+    double r[3];
+    for (int k = 0; k < 3; ++k) r[k] = d.u[k] - bf.n[k] * (2.0 * dn);
+    const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const size_t s = face * res.S + slot;
+    for (int k = 0; k < 3; ++k) res.dir[3 * s + k] = rl > DBL_EPSILON ? r[k] / rl : 0.0;
+    res.w[s] = w;
+    res.lam[s] = d.lam;
+}
+
+// Status of one batch's reflection chain (include/core/forwardSrm.hpp:281-363).
+struct SrmChain {
+    double initial = 0.0, prev = 0.0, remaining = 0.0;
+    uint32_t grow = 0, status = 0, passes = 0;
+    bool active = false;
+};
+
+enum : uint32_t { kSrmDisabled = 0, kSrmConverged = 1, kSrmStable = 2, kSrmDiverged = 3, kSrmMaxIterations = 4 };
+
+uint32_t srmPriority(uint32_t s) {
+    switch (s) {
+        case kSrmDisabled: return 0;
+        case kSrmConverged: return 1;
+        case kSrmStable: return 2;
+        case kSrmMaxIterations: return 3;
+        default: return 4;
+    }
 }
 
 }  // namespace
@@ -277,6 +429,175 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
 #endif
     std::vector<double> score(size_t(B) * 4 * C, 0.0);  // [batch][cell][vertex]
     std::vector<uint32_t> dropped(C, 0), visits(C, 0), raysInBatch(B, 0);
+    // reflections: reflecting boundary faces, face index per (cell, face), two reservoirs
+    const bool srm = ex->useReflections != 0;
+    std::vector<BFace> bfaces;
+    std::vector<int32_t> bidx;
+    Reservoir resA, resB;
+    if (srm) {
+        buildBoundaryFaces(md, bfaces);
+        bidx.assign(4 * size_t(C), -1);
+        for (size_t k = 0; k < bfaces.size(); ++k) bidx[4 * size_t(bfaces[k].c) + bfaces[k].f] = int32_t(k);
+        resA.init(B, uint32_t(bfaces.size()), ex->surfaceReservoirSize);
+        resB.init(B, uint32_t(bfaces.size()), ex->surfaceReservoirSize);
+    }
+    res->srmStatus = kSrmDisabled;
+    res->srmPasses = 0;
+    res->srmRemainingFraction = 0.0;
+    auto applyDeposits = [&](std::vector<Deposit>& deps, Reservoir& into, uint32_t launch, uint32_t pass) {
+        std::sort(deps.begin(), deps.end(), [](const Deposit& a, const Deposit& b) { return a.ray < b.ray; });
+        for (const Deposit& d : deps) {
+            uint32_t o[4];
+            philoxFwd(d.ray, launch, (pass << 2) | 2u, kTagFwdRay, ex->seed, o);
+            deposit(into, bfaces[d.k], d, unit(o[0]), unit(o[1]));
+        }
+        deps.clear();
+    };
+    // The reflected passes of one launch (include/core/forwardSrm.hpp:216-363):
+    // per batch, nb rays per pass drawn from the input reservoir (face by a
+    // stratified target in the face-weight CDF, slot by weight), started at
+    // the face centroid with the previous pass's total weight / nb, their
+    // own boundary hits deposited into the other reservoir.
+    auto reflectPasses = [&](uint32_t launch, const std::vector<uint32_t>& nb) {
+        const uint32_t nF = uint32_t(bfaces.size()), S = resA.S;
+        std::vector<SrmChain> chain(B);
+        Reservoir* in = &resA;
+        Reservoir* out = &resB;
+        std::vector<double> cdf(size_t(B) * nF);
+        auto scan = [&](const Reservoir& r) {
+            std::vector<double> tot(B, 0.0);
+            for (uint32_t b = 0; b < B; ++b) {
+                double acc = 0.0;
+                for (uint32_t k = 0; k < nF; ++k) {
+                    acc += r.faceW[size_t(b) * nF + k];
+                    cdf[size_t(b) * nF + k] = acc;
+                }
+                tot[b] = acc;
+            }
+            return tot;
+        };
+        std::vector<double> W = scan(*in);
+        for (uint32_t b = 0; b < B; ++b) {
+            if (W[b] == 0.0) {
+                chain[b].status = kSrmConverged;
+                continue;
+            }
+            chain[b].initial = chain[b].prev = W[b];
+            chain[b].status = kSrmMaxIterations;
+            chain[b].remaining = 1.0;
+            chain[b].active = true;
+        }
+        const uint32_t M = uint32_t(std::accumulate(nb.begin(), nb.end(), uint64_t(0)));
+        for (uint32_t pass = 1; pass <= ex->reflectionMaxIterations; ++pass) {
+            bool any = false;
+            for (uint32_t b = 0; b < B; ++b) any = any || chain[b].active;
+            if (!any) break;
+            out->clear();
+            std::vector<double> shift(B);
+            for (uint32_t b = 0; b < B; ++b) {
+                uint32_t o[4];
+                philoxFwd(b, launch, pass, kTagFwdBatch, ex->seed, o);
+                shift[b] = double(o[0]) / 4294967296.0;
+            }
+            std::vector<Deposit> deps;
+#pragma omp parallel
+            {
+                std::vector<double> local(size_t(B) * 4 * C, 0.0);
+                std::vector<uint32_t> ldrop(C, 0), lvisit(C, 0);
+                std::vector<Deposit> ldeps;
+#pragma omp for schedule(dynamic, 4096)
+                for (uint32_t r = 0; r < M; ++r) {
+                    const uint32_t b = r % B, i = r / B;
+                    if (!chain[b].active || S == 0 || nF == 0) continue;
+                    const double* cb = &cdf[size_t(b) * nF];
+                    const double t = (double(i) + shift[b]) / double(nb[b]) * cb[nF - 1];
+                    uint32_t k = uint32_t(std::upper_bound(cb, cb + nF, t) - cb);
+                    if (k >= nF) k = nF - 1;
+                    const size_t face = size_t(b) * nF + k;
+                    const uint32_t filled = std::min(in->counts[face], S);
+                    if (filled == 0) continue;
+                    double slotSum = 0.0;
+                    for (uint32_t q = 0; q < filled; ++q) slotSum += in->w[face * S + q];
+                    if (!(slotSum > 0.0)) continue;
+                    uint32_t o[4];
+                    philoxFwd(r, launch, pass << 2, kTagFwdRay, ex->seed, o);
+                    const double target = unit(o[0]) * slotSum;
+                    double cum = 0.0;
+                    uint32_t slot = filled - 1;
+                    for (uint32_t q = 0; q < filled; ++q) {
+                        cum += in->w[face * S + q];
+                        if (cum >= target) {
+                            slot = q;
+                            break;
+                        }
+                    }
+                    const size_t si = face * S + slot;
+                    double u[3] = {in->dir[3 * si], in->dir[3 * si + 1], in->dir[3 * si + 2]};
+                    const double ul = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                    for (int d = 0; d < 3; ++d) u[d] = ul > DBL_EPSILON ? u[d] / ul : 0.0;
+                    const BFace& bf = bfaces[k];
+                    double x[3] = {bf.cen[0], bf.cen[1], bf.cen[2]};
+                    const uint32_t lam = in->lam[si];
+                    uint32_t ec = 0;
+                    int ef = -1;
+                    double eg = 0.0;
+                    const int64_t fail = walkForward(md, bf.c, x, u, sp->sigmaA[lam], sp->sigmaE[lam],
+                                                     &local[size_t(b) * 4 * C], lvisit.data(), nullptr,
+                                                     chain[b].prev / double(nb[b]), bf.f, &ec, &ef, &eg);
+                    if (fail >= 0) ++ldrop[size_t(fail)];
+                    else if (bidx[4 * size_t(ec) + ef] >= 0)
+                        ldeps.push_back(Deposit{r, b, uint32_t(bidx[4 * size_t(ec) + ef]), lam, eg, {u[0], u[1], u[2]}});
+                }
+#pragma omp critical
+                {
+                    for (size_t k = 0; k < local.size(); ++k) score[k] += local[k];
+                    for (uint32_t c = 0; c < C; ++c) {
+                        dropped[c] += ldrop[c];
+                        visits[c] += lvisit[c];
+                    }
+                    deps.insert(deps.end(), ldeps.begin(), ldeps.end());
+                }
+            }
+            applyDeposits(deps, *out, launch, pass);
+            std::swap(in, out);
+            W = scan(*in);
+            for (uint32_t b = 0; b < B; ++b) {
+                SrmChain& ch = chain[b];
+                if (!ch.active) continue;
+                const double cur = W[b];
+                ch.passes = pass;
+                ch.remaining = cur / ch.initial;
+                if (cur > ch.prev) {
+                    if (++ch.grow >= ex->divergenceStreak) {
+                        ch.status = kSrmDiverged;
+                        ch.active = false;
+                        continue;
+                    }
+                } else {
+                    ch.grow = 0;
+                    if (std::fabs(cur - ch.prev) / std::max(cur, 1.0e-30) < ex->reflectionTolerance) {
+                        ch.status = kSrmStable;
+                        ch.active = false;
+                        continue;
+                    }
+                }
+                if (ch.remaining < ex->reflectionTolerance) {
+                    ch.status = kSrmConverged;
+                    ch.active = false;
+                    continue;
+                }
+                ch.prev = cur;
+            }
+        }
+        res->srmStatus = kSrmDisabled;
+        res->srmPasses = 0;
+        res->srmRemainingFraction = 0.0;
+        for (uint32_t b = 0; b < B; ++b) {
+            if (srmPriority(chain[b].status) > srmPriority(res->srmStatus)) res->srmStatus = chain[b].status;
+            res->srmPasses = std::max(res->srmPasses, chain[b].passes);
+            res->srmRemainingFraction = std::max(res->srmRemainingFraction, chain[b].remaining);
+        }
+    };
     uint64_t total = 0;
     double sA = sp->sigmaA[0], sE = sp->sigmaE[0];
     for (uint32_t l = 1; l < nL; ++l) { sA = std::max(sA, sp->sigmaA[l]); sE = std::max(sE, sp->sigmaE[l]); }
@@ -294,11 +615,14 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
             nb[b] = b < M ? (M - b + B - 1) / B : 0u;
             raysInBatch[b] += nb[b];
         }
+        std::vector<Deposit> deps;
+        if (srm) resA.clear();
         if (md.Btot > 0.0) {
 #pragma omp parallel
             {
                 std::vector<double> local(size_t(B) * 4 * C, 0.0);
                 std::vector<uint32_t> ldrop(C, 0), lvisit(C, 0);
+                std::vector<Deposit> ldeps;
 #pragma omp for schedule(dynamic, 4096)
                 for (uint32_t r = 0; r < M; ++r) {
                     const uint32_t b = r % B, i = r / B;
@@ -323,9 +647,15 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
                     const double rr = std::sqrt(std::max(0.0, 1.0 - z * z));
                     const double u[3] = {rr * std::cos(phi), rr * std::sin(phi), z};
                     const uint32_t lam = uint32_t((uint64_t(i) * nL / nb[b] + phase[b]) % nL);
+                    uint32_t ec = 0;
+                    int ef = -1;
+                    double eg = 0.0;
                     const int64_t fail = walkForward(md, c, x, u, sp->sigmaA[lam], sp->sigmaE[lam],
-                                                     &local[size_t(b) * 4 * C], lvisit.data(), nullptr);
+                                                     &local[size_t(b) * 4 * C], lvisit.data(), nullptr, 1.0, -1, &ec,
+                                                     &ef, &eg);
                     if (fail >= 0) ++ldrop[size_t(fail)];
+                    else if (srm && bidx[4 * size_t(ec) + ef] >= 0)
+                        ldeps.push_back(Deposit{r, b, uint32_t(bidx[4 * size_t(ec) + ef]), lam, eg, {u[0], u[1], u[2]}});
                 }
 #pragma omp critical
                 {
@@ -334,8 +664,13 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
                         dropped[c] += ldrop[c];
                         visits[c] += lvisit[c];
                     }
+                    deps.insert(deps.end(), ldeps.begin(), ldeps.end());
                 }
             }
+        }
+        if (srm) {
+            applyDeposits(deps, resA, launch, 0u);
+            reflectPasses(launch, nb);
         }
         total = target;
         // finalise

@@ -254,6 +254,13 @@ class _TetMesh(C.Structure):
         ("claddingAbsorption", C.c_double),
         ("nTot", C.c_double),
         ("crystalTFluo", C.c_double),
+        ("cellFaceBoundaries", _i32p),
+        ("numberOfSurfaces", C.c_uint32),
+        ("surfaceReflectivities", _f64p),
+        ("surfaceRefractiveIndexInside", _f64p),
+        ("surfaceRefractiveIndexOutside", _f64p),
+        ("reflectivities", _f64p),
+        ("refractiveIndices", _f64p),
     ]
 
 
@@ -265,6 +272,11 @@ class _FwdExperiment(C.Structure):
         ("rseThreshold", C.c_double),
         ("seed", C.c_uint32),
         ("batches", C.c_uint32),
+        ("useReflections", C.c_uint32),
+        ("reflectionMaxIterations", C.c_uint32),
+        ("reflectionTolerance", C.c_double),
+        ("surfaceReservoirSize", C.c_uint32),
+        ("divergenceStreak", C.c_uint32),
     ]
 
 
@@ -277,6 +289,9 @@ class _FwdResult(C.Structure):
         ("rayVisits", _u32p),
         ("totalRays", C.c_uint64),
         ("launches", C.c_uint32),
+        ("srmStatus", C.c_uint32),
+        ("srmPasses", C.c_uint32),
+        ("srmRemainingFraction", C.c_double),
     ]
 
 
@@ -286,9 +301,19 @@ def _tet_struct(mesh, keep):
     beta = keep(np.ascontiguousarray(np.asarray(mesh.betaVolume, np.float64).ravel()))
     clad = None if getattr(mesh, "claddingCellTypes", None) is None else keep(
         np.ascontiguousarray(np.asarray(mesh.claddingCellTypes, np.uint32).ravel()))
+    def opt(name, dtype):
+        v = getattr(mesh, name, None)
+        return None if v is None else keep(np.ascontiguousarray(np.asarray(v, dtype).ravel()))
+
+    bnd = opt("cellFaceBoundaries", np.int32)
+    surf = mesh.surfaceArrays() if hasattr(mesh, "surfaceArrays") else (None, None, None)
+    surf = [None if v is None else keep(np.ascontiguousarray(v, np.float64)) for v in surf]
+    nsurf = max([0] + [v.size for v in surf if v is not None])
     return _TetMesh(pts.shape[0], cells.shape[0], _ptr(pts, _f64p), _ptr(cells, _u32p), _ptr(beta, _f64p),
                     _ptr(clad, _u32p), int(getattr(mesh, "claddingNumber", 1)),
-                    float(getattr(mesh, "claddingAbsorption", 0.0)), float(mesh.nTot), float(mesh.crystalTFluo))
+                    float(getattr(mesh, "claddingAbsorption", 0.0)), float(mesh.nTot), float(mesh.crystalTFluo),
+                    _ptr(bnd, _i32p), nsurf, *[_ptr(v, _f64p) for v in surf],
+                    _ptr(opt("reflectivities", np.float64), _f64p), _ptr(opt("refractiveIndices", np.float64), _f64p))
 
 
 def tet_tables(mesh):
@@ -304,9 +329,14 @@ def tet_tables(mesh):
     return out
 
 
+SRM_STATUS = ("disabled", "converged", "stable", "diverged", "max_iterations")
+
+
 def forward_phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, rseThreshold=0.0, seed=5489,
-                    batches=8, threads=0):
-    """Forward Tet4 phi-ASE per cell (FP64)."""
+                    batches=8, threads=0, useReflections=False, reflectionMaxIterations=40, reflectionTolerance=1e-4,
+                    surfaceReservoirSize=32, divergenceStreak=3):
+    """Forward Tet4 phi-ASE per cell (FP64), with the surface-reservoir
+    reflection passes when ``useReflections``."""
     keep = _Keep()
     m = _tet_struct(mesh, keep)
     s = _spectrum_struct(spectrum, keep)
@@ -316,13 +346,18 @@ def forward_phi_ase(mesh, spectrum, *, minRays, maxRays=None, adaptiveSteps=0, r
     r = _FwdResult(_ptr(out["phiAse"], _f64p), _ptr(out["relativeStandardError"], _f64p),
                    _ptr(out["dndtAse"], _f64p), _ptr(out["droppedRays"], _u32p), _ptr(out["rayVisits"], _u32p), 0, 0)
     e = _FwdExperiment(int(minRays), int(maxRays if maxRays is not None else minRays), int(adaptiveSteps),
-                       float(rseThreshold), int(seed) & 0xFFFFFFFF, int(batches))
+                       float(rseThreshold), int(seed) & 0xFFFFFFFF, int(batches), 1 if useReflections else 0,
+                       int(reflectionMaxIterations), float(reflectionTolerance), int(surfaceReservoirSize),
+                       int(divergenceStreak))
     rc = lib().oracle_forward_phi_ase(C.byref(m), C.byref(s), C.byref(e), int(threads or os.cpu_count() or 1),
                                       C.byref(r))
     if rc:
         raise ValueError(f"oracle_forward_phi_ase failed ({rc})")
     out["totalRays"] = int(r.totalRays)
     out["launches"] = int(r.launches)
+    out["srmStatus"] = SRM_STATUS[r.srmStatus]
+    out["srmPasses"] = int(r.srmPasses)
+    out["srmRemainingFraction"] = float(r.srmRemainingFraction)
     return out
 
 
