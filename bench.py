@@ -442,6 +442,30 @@ def measure_forward(args, local, rank=0, world=1, cpu_seconds=None):
     barrier()
     e2e_s = time.perf_counter() - t0
     ctx.update_beta(tet.betaVolume)
+    srm = None
+    if w.useReflections and tet.cellFaceBoundaries is not None:
+        # surface-reservoir reflections: every reflected pass relaunches the
+        # launch's source-ray count, so a smaller launch keeps the step short
+        srm_rays = max(1, rays // 8)
+        kw = dict(forwardRayCount=srm_rays, monochromatic=w.monochromatic, tallyMode=args.tally, useReflections=True)
+        for k in range(2):
+            ctx.calc_phi_ase(rngSeed=50 + k, **kw)
+        torch.cuda.synchronize()
+        s_ms = s_ray = 0.0
+        s_cross = 0
+        res_s = None
+        for k in range(2):
+            flush.zero_()
+            torch.cuda.synchronize()
+            res_s = ctx.calc_phi_ase(rngSeed=60 + k, **kw)
+            s_ms += res_s.totalMilliseconds
+            s_ray += res_s.rayMilliseconds
+            s_cross += res_s.crossings
+        srm = {"source_rays_per_step": srm_rays, "ms_per_step": s_ms / 2, "status": res_s.srmStatus,
+               "passes": res_s.srmPasses, "remaining_fraction": res_s.srmRemainingFraction,
+               "reflecting_faces": res_s.reflectingFaces, "crossings_per_s": s_cross / (s_ray * 1e-3),
+               "kernel_launches_per_step": res_s.kernelLaunches,
+               "note": "source pass + reflected passes of the same ray count; crossings of all passes"}
     ctx.close()
     stats = torch.tensor([dev_ms, e2e_s, float(traced), float(cross), ray_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -476,6 +500,8 @@ def measure_forward(args, local, rank=0, world=1, cpu_seconds=None):
                      "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
         "clocks": clocks,
     }
+    if srm is not None:
+        out["srm_reflections"] = srm
     if cpu_seconds and world == 1:
         out["cpu_baseline"] = forward_cpu_baseline(tet, sa, se, cpu_seconds)
     return out
