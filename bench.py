@@ -534,25 +534,29 @@ def run_forward(args):
         dist.destroy_process_group()
 
 
-MEDIA_METRIC = ("batched phi-ASE over 64 independent gain media (config 3) to per-sample relative error <= threshold "
-                "on 1 B200, as sample points solved per second (rays/s alongside; the same media solved one after "
-                "another beside it)")
+MEDIA_METRIC = ("batched phi-ASE over 64 independent gain media (config 3) with the learned proposal to per-sample "
+                "relative error <= threshold on 1 B200, as sample points solved per second (rays/s alongside; "
+                "importance-weighted batched, sequential and plain importance sampling beside it)")
 
 
 def measure_media(args, local, steps, warmup):
     """Config 3: 64 seeded media (triangles 200..20,000, levels 5..40, 1..8
     wavelengths), a seeded block of ``--media-samples`` sample points per
-    medium, rays 1e4 -> 1e7, relative error 0.001, near-field start points.
-    Timed: the batched solve (one graph: pooled importance, one persistent ray
-    launch per pass over all media).  Beside it: the same media solved one
-    after another (identical rays and results, host-driven passes)."""
+    medium, rays 1e4 -> 1e7, relative error 0.001.  Untimed: a proposal
+    network trained on 24 other seeded media of the family.  Timed (one graph
+    per solve: pooled proposal or importance weights, one persistent ray
+    launch per pass over all media): the learned proposal + batching (the
+    value), the importance weights with near-field start points + batching,
+    the same media solved one after another (identical rays), and the
+    reference's plain importance sampling one medium after another."""
     import numpy as np
     import torch
 
     from haseongpu_b200 import DeviceMesh, MediaBatch, _native
+    from haseongpu_b200 import learned as LP
     from haseongpu_b200.autotune import autotune_batch
     from haseongpu_b200.batch import solve_sequential
-    from haseongpu_b200.configs import media64
+    from haseongpu_b200.configs import media64, media_training
 
     w = media64()
     ctxs = [DeviceMesh(m.mesh, *m.spectra.resampled(False), device=local) for m in w.media]
@@ -566,38 +570,51 @@ def measure_media(args, local, steps, warmup):
     rows = sum(hi - lo + 1 for _, lo, hi in items)
     flush = torch.empty(64 << 20, dtype=torch.int32, device=torch.device("cuda", local))
     ws = 32 << 30
+    t0 = time.perf_counter()
+    trainers = [DeviceMesh(m.mesh, *m.spectra.resampled(False), device=local) for m in media_training()]
+    data = LP.training_set_media(trainers, samples_per_medium=16, rays=100_000)
+    t1 = time.perf_counter()
+    net, hist = LP.train_proposal(data, steps=3000, device=local)
+    t2 = time.perf_counter()
+    for c in trainers:
+        c.close()
     batch = MediaBatch(local)
     tune = autotune_batch(batch, items, rays=20_000, workspaceBytes=ws)
     kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
               monochromatic=False, workspaceBytes=ws, rayKernelVariant=tune.rayKernelVariant,
               raysPerThread=tune.raysPerThread)
-    for k in range(warmup):
-        batch.solve(items, rngSeed=100 + 64 * k, **kw)
-    torch.cuda.synchronize()
-    bt, st_all, wall_b = [], [], 0.0
-    with ClockSampler(local) as clk:
+
+    def timed(fn):
+        out, st_all = [], []
         for s_ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            res, st = batch.solve(items, rngSeed=1000 + 64 * s_, **kw)
-            wall_b += time.perf_counter() - t0
-            bt.append(res)
+            res, st = fn(1000 + 64 * s_)
+            out.append(res)
             st_all.append(st)
+        return out, st_all
+
+    for k in range(warmup):
+        batch.solve(items, rngSeed=100 + 64 * k, net=net, **kw)
+        batch.solve(items, rngSeed=100 + 64 * k, **kw)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        lt, lst = timed(lambda seed: batch.solve(items, rngSeed=seed, net=net, **kw))
+        bt, bst = timed(lambda seed: batch.solve(items, rngSeed=seed, **kw))
     clocks = clk.summary()
-    seq_ms, wall_s = 0.0, 0.0
+    seq_ms, wall_s, same = 0.0, 0.0, True
     for s_ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        t_s = time.perf_counter()
         seq = solve_sequential(items, rngSeed=1000 + 64 * s_, **kw)
-        wall_s += time.perf_counter() - t0
+        wall_s += time.perf_counter() - t_s
         seq_ms += sum(r.totalMilliseconds for r in seq)
-        same = all(np.array_equal(a.phiAse, b.phiAse) for a, b in zip(bt[s_], seq))
+        same = same and all(np.array_equal(a.phiAse, b.phiAse) for a, b in zip(bt[s_], seq))
     # the reference's estimator (importance weights, uniform start points) on
     # the same media, one medium after another: the plain importance-sampled
-    # GPU path the batched solve replaces
-    plain_ms, plain_rays, plain_unconv = 0.0, 0, 0
+    # GPU path
+    plain_ms, plain_rays, plain_unconv, plain_var = 0.0, 0, 0, None
     pkw = dict(kw, rayKernelVariant=0, raysPerThread=0, nearFieldSampling=False)
     for s_ in range(steps):
         flush.zero_()
@@ -606,30 +623,38 @@ def measure_media(args, local, steps, warmup):
         plain_ms += sum(r.totalMilliseconds for r in pr)
         plain_rays += sum(r.raysTraced for r in pr)
         plain_unconv += sum(r.unconvergedSamples for r in pr)
+        plain_var = np.concatenate([LP.per_ray_variance(r) for r in pr])
     # e2e: beta of every medium uploaded from host and every result read back, each step
     betas = [c.mesh.betaVolume for c in ctxs]
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    te = time.perf_counter()
     for s_ in range(steps):
         for c, b in zip(ctxs, betas):
             c.update_beta(b)
-        batch.solve(items, rngSeed=1000 + 64 * s_, **kw)
-    e2e_s = time.perf_counter() - t0
-    ms = sum(st.totalMilliseconds for st in st_all)
-    ray_ms = sum(st.rayMilliseconds for st in st_all)
-    rays = sum(st.raysTraced for st in st_all)
-    cross = sum(st.crossings for st in st_all)
+        batch.solve(items, rngSeed=1000 + 64 * s_, net=net, **kw)
+    e2e_s = time.perf_counter() - te
+
+    def agg(st_all):
+        return {"ms": sum(st.totalMilliseconds for st in st_all), "ray_ms": sum(st.rayMilliseconds for st in st_all),
+                "imp_ms": sum(st.importanceMilliseconds for st in st_all),
+                "rays": sum(st.raysTraced for st in st_all), "cross": sum(st.crossings for st in st_all),
+                "unconverged": sum(st.unconvergedSamples for st in st_all),
+                "capture_ms": sum(st.captureMilliseconds for st in st_all)}
+
+    L, B = agg(lst), agg(bst)
+    lv = np.concatenate([LP.per_ray_variance(r) for r in lt[-1]])
+    nv = np.concatenate([LP.per_ray_variance(r) for r in bt[-1]])
     peaks, peak_kind = measured_peaks()
     f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
     r_fp32 = SMS * LANES_PER_SM * f_clk / FP32_INSTR_PER_CROSSING
     l2 = _native.l2_bandwidth(local)
     r_l2 = l2 * 1e9 / BYTES_PER_CROSSING
     roof = min(r_fp32, r_l2)
-    per_ray = np.concatenate([r.totalRays.astype(np.int64) for r in bt[-1]])
+    per_ray = np.concatenate([r.totalRays.astype(np.int64) for r in lt[-1]])
     out = {
-        "value": steps * rows / (ms * 1e-3), "unit": "samples/s", "ms_per_step": ms / steps,
-        "rays_per_s": rays / (ms * 1e-3), "crossings_per_s": cross / (ray_ms * 1e-3),
-        "config": {"workload": "media64 (config 3): 64 seeded gain media in one batched solve",
+        "value": steps * rows / (L["ms"] * 1e-3), "unit": "samples/s", "ms_per_step": L["ms"] / steps,
+        "rays_per_s": L["rays"] / (L["ms"] * 1e-3), "crossings_per_s": L["cross"] / (L["ray_ms"] * 1e-3),
+        "config": {"workload": "media64 (config 3): 64 seeded gain media in one batched solve, learned proposal",
                    "media": len(ctxs), "samples_per_medium": K, "samples_per_step": rows,
                    "triangles": [min(c.mesh.numberOfTriangles for c in ctxs),
                                  max(c.mesh.numberOfTriangles for c in ctxs)],
@@ -640,35 +665,48 @@ def measure_media(args, local, steps, warmup):
                    "l2": "flushed (256 MiB write) before every timed step",
                    "ray_kernel": {"variant": tune.name, "rays_per_lane": tune.raysPerThread,
                                   "autotuned_over": len(tune.table)}},
-        "breakdown_ms_per_step": {"importance": sum(st.importanceMilliseconds for st in st_all) / steps,
-                                  "map_ray_finalise_passes": ray_ms / steps,
-                                  "graph_capture_host": sum(st.captureMilliseconds for st in st_all) / steps},
+        "breakdown_ms_per_step": {"proposal_and_mixture": L["imp_ms"] / steps,
+                                  "map_ray_finalise_passes": L["ray_ms"] / steps,
+                                  "graph_capture_host": L["capture_ms"] / steps},
         "rays_per_sample": {"min": int(per_ray.min()), "median": float(np.median(per_ray)), "max": int(per_ray.max())},
-        "passes": max(st.passes for st in st_all),
-        "unconverged_samples": sum(st.unconvergedSamples for st in st_all),
-        "graph": {"kernels": st_all[-1].kernelLaunches, "nodes": st_all[-1].graphNodes, "chunks": st_all[-1].chunks},
-        "sequential": {"value": steps * rows / (seq_ms * 1e-3), "unit": "samples/s", "ms_per_step": seq_ms / steps,
-                       "wall_ms_per_step": wall_s * 1e3 / steps, "identical_results": bool(same),
-                       "note": "the same media, one calc_phi_ase per medium (host-synchronised passes)"},
-        "speedup_vs_sequential": seq_ms / ms,
+        "unconverged_samples": L["unconverged"],
+        "per_ray_variance": {"learned_median": float(np.median(lv)), "learned_max": float(lv.max()),
+                             "importance_nearfield_median": float(np.median(nv)),
+                             "importance_nearfield_max": float(nv.max()),
+                             "plain_is_median": float(np.median(plain_var)), "plain_is_max": float(plain_var.max())},
+        "training": {"media": 24, "samples_per_medium": 16, "groups": data.groups, "rows": int(data.offsets[-1]),
+                     "rays_logged": data.groups * data.rays, "log_s": t1 - t0, "train_s": t2 - t1,
+                     "loss_first_50": float(hist[:50].mean()), "loss_last_200": float(hist[-200:].mean()),
+                     "note": "24 media of the same generator on another seed (<= 3,000 triangles); the timed media "
+                             "are unseen"},
+        "importance_batched": {"value": steps * rows / (B["ms"] * 1e-3), "unit": "samples/s",
+                               "ms_per_step": B["ms"] / steps, "rays": B["rays"],
+                               "unconverged_samples": B["unconverged"],
+                               "note": "importance weights with near-field start points, the same batched graph"},
+        "importance_sequential": {"ms_per_step": seq_ms / steps, "wall_ms_per_step": wall_s * 1e3 / steps,
+                                  "identical_to_batched": bool(same),
+                                  "note": "the same media, one calc_phi_ase per medium (host-synchronised passes)"},
         "plain_is_sequential": {"value": steps * rows / (plain_ms * 1e-3), "unit": "samples/s",
                                 "ms_per_step": plain_ms / steps, "rays": plain_rays,
                                 "unconverged_samples": plain_unconv,
                                 "note": "the reference's importance weights with uniform start points, one medium "
                                         "after another"},
-        "speedup_vs_plain_is_sequential": plain_ms / ms,
-        "wall_ms_per_step": wall_b * 1e3 / steps,
+        "speedup_vs_plain_is_sequential": plain_ms / L["ms"],
+        "speedup_vs_importance_batched": B["ms"] / L["ms"],
+        "speedup_batched_vs_sequential": seq_ms / B["ms"],
         "e2e": {"value": steps * rows / e2e_s, "unit": "samples/s",
                 "h2d_bytes_per_step": sum(c.mesh.numberOfPrisms * 8 for c in ctxs),
                 "d2h_bytes_per_step": rows * (4 + 8 + 8 + 4 + 8 + 4)},
-        "gpu_launches": sum(st.kernelLaunches for st in st_all),
+        "gpu_launches": sum(st.kernelLaunches for st in lst),
+        "graph": {"kernels": lst[-1].kernelLaunches, "nodes": lst[-1].graphNodes, "chunks": lst[-1].chunks},
         "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel (pooled)",
-                     "achieved": cross / (ray_ms * 1e-3), "peak": roof, "unit": "crossings/s",
-                     "frac": cross / (ray_ms * 1e-3) / roof, "traffic": None, "peak_source": peak_kind,
+                     "achieved": L["cross"] / (L["ray_ms"] * 1e-3), "peak": roof, "unit": "crossings/s",
+                     "frac": L["cross"] / (L["ray_ms"] * 1e-3) / roof, "traffic": None, "peak_source": peak_kind,
                      "note": "ray time includes the map and finalise launches of every pass"},
         "clocks": clocks,
     }
     batch.close()
+    net.close()
     for c in ctxs:
         c.close()
     return out
@@ -877,8 +915,19 @@ def run_learned(args):
         if media is not None:
             line["batched_media"] = {k: media[k] for k in (
                 "value", "unit", "ms_per_step", "config", "rays_per_s", "crossings_per_s", "breakdown_ms_per_step",
-                "rays_per_sample", "unconverged_samples", "graph", "sequential", "speedup_vs_sequential",
-                "plain_is_sequential", "speedup_vs_plain_is_sequential", "e2e", "roofline")}
+                "rays_per_sample", "unconverged_samples", "per_ray_variance", "training", "importance_batched",
+                "importance_sequential", "plain_is_sequential", "speedup_vs_plain_is_sequential",
+                "speedup_vs_importance_batched", "speedup_batched_vs_sequential", "graph", "e2e", "roofline")}
+            line["north_star_target"] = {
+                "target": "learned proposal + persistent batching >= 5x less time to every sample's threshold than "
+                          "the plain importance-sampled GPU path",
+                "workload": "media64 (config 3), unseen media",
+                "learned_batched_ms": media["ms_per_step"],
+                "plain_is_sequential_ms": media["plain_is_sequential"]["ms_per_step"],
+                "plain_is_unconverged_samples": media["plain_is_sequential"]["unconverged_samples"],
+                "learned_batched_unconverged_samples": media["unconverged_samples"],
+                "ratio": media["speedup_vs_plain_is_sequential"],
+                "met": bool(media["speedup_vs_plain_is_sequential"] >= 5.0)}
         print(json.dumps(line), flush=True)
     net.close()
     ctx.close()

@@ -66,6 +66,7 @@ EXPORTED_SYMBOLS = (
     "hase_batch_create",
     "hase_batch_destroy",
     "hase_calc_phi_ase_batch",
+    "hase_calc_phi_ase_batch_learned",
 )
 PROPOSAL_FEATURES = 12
 PROPOSAL_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -304,6 +305,8 @@ class BatchStats(C.Structure):
         ("rayMilliseconds", C.c_double),
         ("totalMilliseconds", C.c_double),
         ("captureMilliseconds", C.c_double),
+        ("setupMilliseconds", C.c_double),
+        ("hostMilliseconds", C.c_double),
     ]
 
 
@@ -374,6 +377,9 @@ def lib():
         L.hase_batch_destroy.argtypes = [C.c_void_p]
         L.hase_calc_phi_ase_batch.argtypes = [C.c_void_p, C.POINTER(BatchInstance), C.c_uint32,
                                               C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), C.POINTER(BatchStats)]
+        L.hase_calc_phi_ase_batch_learned.argtypes = [C.c_void_p, C.POINTER(BatchInstance), C.c_uint32,
+                                                      C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), C.c_void_p,
+                                                      C.c_float, C.POINTER(BatchStats)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

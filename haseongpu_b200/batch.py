@@ -33,6 +33,8 @@ class BatchStats:
     rayMilliseconds: float
     totalMilliseconds: float
     captureMilliseconds: float
+    setupMilliseconds: float
+    hostMilliseconds: float
     status: int = 0
 
 
@@ -47,9 +49,12 @@ class MediaBatch:
 
     def solve(self, media, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
               nearFieldSampling=True, adaptiveSteps=0, rngSeed=5489, raysPerThread=0, workspaceBytes=0,
-              rayKernelVariant=0, importanceLayers=0):
+              rayKernelVariant=0, importanceLayers=0, net=None, mixture=0.0):
         """media: DeviceMesh objects, or (DeviceMesh, minSample, maxSample)
-        tuples (maxSample None = last).  Returns ([Result per medium], BatchStats)."""
+        tuples (maxSample None = last).  net: a ProposalNet whose learned
+        proposal replaces the importance weights of every medium (mixture:
+        weight of the beta V / d^2 prior, 0 = 0.1).  Returns
+        ([Result per medium], BatchStats)."""
         items = []
         for m in media:
             if isinstance(m, DeviceMesh):
@@ -73,8 +78,12 @@ class MediaBatch:
             descs[i].result = C.pointer(r)
             outs.append(out)
         st = N.BatchStats()
-        status = N.check(N.lib().hase_calc_phi_ase_batch(self.handle, descs, len(items), C.byref(ex), C.byref(cp),
-                                                          C.byref(st)), allow_warnings=True)
+        if net is None:
+            rc = N.lib().hase_calc_phi_ase_batch(self.handle, descs, len(items), C.byref(ex), C.byref(cp), C.byref(st))
+        else:
+            rc = N.lib().hase_calc_phi_ase_batch_learned(self.handle, descs, len(items), C.byref(ex), C.byref(cp),
+                                                         net.handle, float(mixture), C.byref(st))
+        status = N.check(rc, allow_warnings=True)
         for out, r in zip(outs, keep):
             DeviceMesh._fill(out, r, status)
         stats = BatchStats(*(getattr(st, f) for f, _ in N.BatchStats._fields_), status=status)

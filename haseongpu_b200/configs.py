@@ -136,4 +136,17 @@ def media64(count: int = 64) -> MediaWorkload:
     return MediaWorkload("media64", [batch_medium(rng, i) for i in range(count)], 10_000, 10_000_000, 0.001)
 
 
+def media_training(count: int = 24, max_triangles: int = 3000) -> list:
+    """Training media for a proposal network that serves the media64 family:
+    the same generator on its own seed, media above ``max_triangles``
+    skipped (the logged training rows grow with samples x prisms)."""
+    rng = _rng(3)
+    out = []
+    while len(out) < count:
+        m = batch_medium(rng, len(out))
+        if m.mesh.numberOfTriangles <= max_triangles:
+            out.append(m)
+    return out
+
+
 WORKLOADS = {"disc_small": disc_small, "disc_poly": disc_poly}

@@ -1140,6 +1140,9 @@ struct hase_context {
     std::vector<double> hBeta;  // betaVolume as given (FP64)
     // learned proposal: coarse gain grid, fallback rows, contribution log
     DevBuf<float> featGrid, logBuf, priorBuf;
+    uint64_t betaVersion = 1;       // bumped by every beta upload
+    uint64_t featVersion = 0;       // beta version the cached feature view was built for
+    double featA = 0.0, featB = 0.0;
     DevBuf<uint32_t> rowList;
 
     MeshView view() const {
@@ -1179,6 +1182,7 @@ hase_status uploadBeta(hase_context* c, const double* betaVolume) {
     }
     c->hGainBeta = gain;
     c->hBeta.assign(betaVolume, betaVolume + c->P);
+    ++c->betaVersion;
     HASE_CUDA(cudaMemcpyAsync(c->gainBeta.p, gain.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(c->srcBeta.p, src.data(), c->P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
@@ -1212,6 +1216,27 @@ constexpr uint32_t kGridCells = 48;  // feature grid cells along the longer side
 // Feature view of the context: the coarse gain grid (mean g = A beta - B of
 // the prisms whose centre falls in a cell, empty cells filled from their
 // neighbours), scales, and mean reflectivities.
+hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V);
+
+// The feature view, rebuilt only when beta or the averaged spectrum changed.
+hase_status cachedProposalView(hase_context* c, double A, double B, ProposalView& V) {
+    static thread_local std::unordered_map<const hase_context*, ProposalView> views;
+    if (c->featVersion == c->betaVersion && c->featA == A && c->featB == B) {
+        auto it = views.find(c);
+        if (it != views.end()) {
+            V = it->second;
+            return HASE_OK;
+        }
+    }
+    HASE_TRY(buildProposalView(c, A, B, V));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    views[c] = V;
+    c->featVersion = c->betaVersion;
+    c->featA = A;
+    c->featB = B;
+    return HASE_OK;
+}
+
 hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V) {
     float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY, R = 0.0f;
     for (const float2& q : c->hPoints) {
@@ -1489,7 +1514,7 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     if (la) {
         if (la->net->device != c->device)
             return fail(HASE_INVALID_ARGUMENT, "the proposal network and the context are on different devices");
-        HASE_TRY(buildProposalView(c, meanA, meanB, pv));
+        HASE_TRY(cachedProposalView(c, meanA, meanB, pv));
         HASE_CUDA(cudaFuncSetAttribute(proposalKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
         int sms = 0;
         HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -2216,7 +2241,7 @@ struct hase_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> ev;  // timing events recorded inside the graphs
-    DevBuf<float> lnw, phi;
+    DevBuf<float> lnw, phi, prior;
     DevBuf<uint32_t> q, offsets, activeA, activeB, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> counts;  // [0], [1]: active rows (alternating), [2]: item counter, [3 ..]: per pass
     DevBuf<unsigned long long> Q, accCross, pCross;
@@ -2343,12 +2368,18 @@ hase_status batchMedia(const hase_batch* b, const hase_batch_instance* in, uint3
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in, uint32_t count,
-                                    const hase_experiment_desc* ex, const hase_compute_desc* cp,
-                                    hase_batch_stats* stats) {
+// The batched solve; net != null: every medium's importance weights are
+// replaced by the learned proposal (network logits mixed with the
+// beta V R_j / d^2 prior, weight alpha), as hase_calc_phi_ase_learned does.
+hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t count, const hase_experiment_desc* ex,
+                      const hase_compute_desc* cp, hase_batch_stats* stats, hase_proposal* net, float alpha) {
     if (!b || !in || !ex || !cp || count == 0) return fail(HASE_INVALID_ARGUMENT, "null argument or no instances");
+    const auto hostStart = std::chrono::steady_clock::now();
+    auto sinceStart = [&] {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostStart).count();
+    };
     if (ex->minRays == 0) return fail(HASE_INVALID_ARGUMENT, "minRays must be positive");
     if (ex->maxRays != 0 && ex->maxRays < ex->minRays) return fail(HASE_INVALID_ARGUMENT, "maxRays < minRays");
     if (!(ex->mseThreshold >= 0.0)) return fail(HASE_INVALID_ARGUMENT, "mseThreshold must be >= 0");
@@ -2411,6 +2442,20 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
                               b->stream));
     HASE_CUDA(cudaMemcpyAsync(b->inst.p, views.data(), count * sizeof(InstanceView), cudaMemcpyHostToDevice,
                               b->stream));
+    // learned proposal: one feature view per medium (coarse gain grid on the medium's context)
+    std::vector<ProposalView> pviews;
+    uint32_t proposalGrid = 0;
+    if (net) {
+        if (net->device != b->device)
+            return fail(HASE_INVALID_ARGUMENT, "the proposal network and the batch are on different devices");
+        pviews.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            HASE_TRY(cachedProposalView(media[i].c, media[i].meanA, media[i].meanB, pviews[i]));
+            pviews[i].nW = media[i].nW;
+        }
+        HASE_CUDA(cudaFuncSetAttribute(proposalKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
+        proposalGrid = uint32_t(std::max(1, b->sms) * kMlpBlocksPerSM);
+    }
 
     // rows of every medium, cut into workspace chunks
     struct Chunk {
@@ -2450,6 +2495,7 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
     }
     if (maxRows > 0xffffffffull) return fail(HASE_INVALID_ARGUMENT, "too many sample points in one chunk");
     HASE_CUDA(b->lnw.ensure(maxWs));
+    if (net) HASE_CUDA(b->prior.ensure(maxWs));
     HASE_CUDA(b->q.ensure(maxWs));
     HASE_CUDA(b->offsets.ensure(maxWs + maxRows));
     HASE_CUDA(b->Q.ensure(maxRows));
@@ -2489,6 +2535,7 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
 
     for (const Chunk& ch : chunks) {
         const uint32_t nRows = uint32_t(ch.r1 - ch.r0);
+        if (&ch == &chunks.front()) st.setupMilliseconds = sinceStart();
         HASE_CUDA(cudaMemcpyAsync(b->rows.p, all.data() + ch.r0, nRows * sizeof(RowInfo), cudaMemcpyHostToDevice,
                                   b->stream));
         HASE_CUDA(cudaStreamSynchronize(b->stream));
@@ -2507,17 +2554,32 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
                 while (e < ch.r1 && all[e].inst == i && e - r < 65535) ++e;
                 const BatchMedium& md = media[i];
                 const hase_context* c = md.c;
-                ImportanceLaunch il{views[i].m, all[r].sample, slices, md.nW, float(md.meanA), float(md.meanB),
-                                    b->lnw.p + all[r].w, nullptr};
-                const uint32_t G = cp->importanceLayers == 4 ? 4u : uint32_t(kImportanceLayers);
-                const uint32_t threads = slices * ((c->layers + G - 1) / G) * c->T;
-                if (G == 4)
-                    importanceKernel<4><<<dim3((threads + 255) / 256, uint32_t(e - r)), 256, 0, b->stream>>>(il);
-                else
-                    importanceKernel<kImportanceLayers>
-                        <<<dim3((threads + 255) / 256, uint32_t(e - r)), 256, 0, b->stream>>>(il);
+                const uint32_t segRows = uint32_t(e - r);
+                if (net) {
+                    ProposalView pv = pviews[i];
+                    pv.firstSample = all[r].sample;
+                    ProposalLaunch pl{pv, net->wimg.p, net->vec.p, b->lnw.p + all[r].w, b->prior.p + all[r].w,
+                                      nullptr, segRows, net->error.p};
+                    const uint64_t tiles = (uint64_t(segRows) * md.nW + kTile - 1) / kTile;
+                    proposalKernel<<<uint32_t(std::min<uint64_t>(tiles, proposalGrid)), kTile, kSmemBytes,
+                                     b->stream>>>(pl);
+                    HASE_CUDA(cudaGetLastError());
+                    mixtureKernel<<<segRows, 1024, 0, b->stream>>>(md.nW, b->lnw.p + all[r].w, b->prior.p + all[r].w,
+                                                                  alpha);
+                    kernels += 2;
+                } else {
+                    ImportanceLaunch il{views[i].m, all[r].sample, slices, md.nW, float(md.meanA), float(md.meanB),
+                                        b->lnw.p + all[r].w, nullptr};
+                    const uint32_t G = cp->importanceLayers == 4 ? 4u : uint32_t(kImportanceLayers);
+                    const uint32_t threads = slices * ((c->layers + G - 1) / G) * c->T;
+                    if (G == 4)
+                        importanceKernel<4><<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
+                    else
+                        importanceKernel<kImportanceLayers>
+                            <<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
+                    ++kernels;
+                }
                 HASE_CUDA(cudaGetLastError());
-                ++kernels;
                 r = e;
             }
             HASE_CUDA(cudaEventRecordWithFlags(b->ev[1], b->stream, cudaEventRecordExternal));
@@ -2659,7 +2721,13 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
         res->totalMilliseconds = st.totalMilliseconds;
         res->kernelLaunches = st.kernelLaunches;
     }
+    st.hostMilliseconds = sinceStart();
     if (stats) *stats = st;
+    if (net) {
+        int err = 0;
+        HASE_CUDA(cudaMemcpy(&err, net->error.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return fail(HASE_DEVICE_TIMEOUT, "a tensor-core wait of the proposal network timed out");
+    }
     if (droppedTotal) {
         fail(HASE_DROPPED_RAYS, "%llu rays could not be walked", (unsigned long long)droppedTotal);
         return HASE_DROPPED_RAYS;
@@ -2669,6 +2737,24 @@ hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in
         return HASE_NOT_CONVERGED;
     }
     return HASE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in, uint32_t count,
+                                    const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                                    hase_batch_stats* stats) {
+    return batchCore(b, in, count, ex, cp, stats, nullptr, 0.0f);
+}
+
+hase_status hase_calc_phi_ase_batch_learned(hase_batch* b, const hase_batch_instance* in, uint32_t count,
+                                            const hase_experiment_desc* ex, const hase_compute_desc* cp,
+                                            hase_proposal* net, float mixture, hase_batch_stats* stats) {
+    if (!net) return fail(HASE_INVALID_ARGUMENT, "null network");
+    if (!(mixture >= 0.0f) || mixture >= 1.0f) return fail(HASE_INVALID_ARGUMENT, "mixture must be in [0, 1)");
+    return batchCore(b, in, count, ex, cp, stats, net, mixture > 0.0f ? mixture : 0.1f);
 }
 
 }  // extern "C"

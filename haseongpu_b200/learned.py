@@ -72,6 +72,30 @@ def training_set(ctx, fields, *, samples_per_field=32, rays=100_000, monochromat
                        rays)
 
 
+def training_set_media(ctxs, *, samples_per_medium=16, rays=100_000, monochromatic=False, useReflections=False,
+                       seed=TRAIN_SEED) -> TrainingSet:
+    """The training set of a family of media: per medium (a DeviceMesh with
+    its own mesh, beta and spectrum) a seeded block of consecutive sample
+    points solved with the importance weights, contributions logged per
+    (slice, prism) as the targets, and the features of the same pairs."""
+    rng = np.random.default_rng(seed)
+    feats, targs, offs = [], [], [0]
+    for k, ctx in enumerate(ctxs):
+        S = ctx.mesh.numberOfSamples
+        n = min(samples_per_medium, S)
+        first = int(rng.integers(0, max(1, S - n)))
+        _, con = ctx.log_contributions(minRays=rays, monochromatic=monochromatic, useReflections=useReflections,
+                                       rngSeed=seed + k, minSample=first, maxSample=first + n - 1)
+        f = ctx.proposal_features(first, n, useReflections=useReflections, monochromatic=monochromatic)
+        for i in range(n):
+            keep = f[i, :, 7] > 0
+            feats.append(f[i][keep])
+            targs.append(np.maximum(con[i][keep], 0.0))
+            offs.append(offs[-1] + int(keep.sum()))
+    return TrainingSet(np.asarray(offs, np.uint32), np.concatenate(feats), np.concatenate(targs).astype(np.float32),
+                       rays)
+
+
 def train_proposal(data: TrainingSet, *, steps=3000, groups_per_step=16, learning_rate=2e-3, device=0, seed=1):
     """A proposal network trained on `data` (Adam on the device); returns
     (net, loss history)."""

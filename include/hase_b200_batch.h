@@ -62,6 +62,8 @@ typedef struct {
     double rayMilliseconds;             /* map + ray + finalise launches of all passes */
     double totalMilliseconds;           /* graph launch to completion, all chunks */
     double captureMilliseconds;         /* host time spent capturing and instantiating graphs */
+    double setupMilliseconds;           /* host time before the first graph launch (tables, views, uploads) */
+    double hostMilliseconds;            /* host time of the whole call */
 } hase_batch_stats;
 
 hase_status hase_batch_create(int device, hase_batch** out);
@@ -77,6 +79,19 @@ hase_status hase_batch_destroy(hase_batch* batch);
 hase_status hase_calc_phi_ase_batch(hase_batch* batch, const hase_batch_instance* instances, uint32_t count,
                                     const hase_experiment_desc* experiment, const hase_compute_desc* compute,
                                     hase_batch_stats* stats);
+
+struct hase_proposal; /* include/hase_b200_proposal.h */
+
+/* The same batched solve with the learned proposal of `net` (on the batch's
+ * device) in place of every medium's importance weights:
+ * q = (1 - mixture) softmax(network logits) + mixture (beta V R_j / d^2
+ * prior), mixture 0 = 0.1, one network for all media (its features are
+ * normalised by each medium's radius and height).  Medium i equals
+ * hase_calc_phi_ase_learned on its context with seed rngSeed + i and no
+ * fallback; samples do not fall back to the importance weights here. */
+hase_status hase_calc_phi_ase_batch_learned(hase_batch* batch, const hase_batch_instance* instances, uint32_t count,
+                                            const hase_experiment_desc* experiment, const hase_compute_desc* compute,
+                                            struct hase_proposal* net, float mixture, hase_batch_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -133,3 +133,56 @@ def test_batch_rejects_bad_ranges(media):
             b.solve([], minRays=100)
         res, st = b.solve([(c, 5, 5)], minRays=100)
         assert res[0].phiAse.shape == (1,) and st.rows == 1
+
+
+def test_learned_batch_equals_single_medium_learned_solves(media):
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.proposal import ProposalNet
+
+    items = _ranges(media, n=48)
+    kw = dict(KW, maxRays=16000, adaptiveSteps=2)
+    with ProposalNet(seed=5) as net, MediaBatch(0) as b:
+        res, st = b.solve(items, net=net, **kw)
+        for i, (ctx, lo, hi) in enumerate(items):
+            solo = ctx.calc_phi_ase_learned(net, minRays=kw["minRays"], maxRays=kw["maxRays"],
+                                            mseThreshold=kw["mseThreshold"], adaptiveSteps=kw["adaptiveSteps"],
+                                            monochromatic=False, rngSeed=kw["rngSeed"] + i, minSample=lo,
+                                            maxSample=hi)
+            assert solo.fallbackSamples == 0
+            _same(res[i], solo)
+    assert st.kernelLaunches > 0
+
+
+def test_network_trained_on_the_media_family_lowers_the_variance_on_unseen_media():
+    """A proposal network trained on 24 seeded media of the config-3 family
+    (other seed) lowers the per-ray variance on unseen media64 media below
+    the importance weights with near-field start points, and bounds the tail."""
+    from haseongpu_b200 import DeviceMesh, MediaBatch
+    from haseongpu_b200 import learned as LP
+    from haseongpu_b200.configs import media64, media_training
+
+    trainers = [DeviceMesh(m.mesh, *m.spectra.resampled(False), device=0) for m in media_training()]
+    data = LP.training_set_media(trainers, samples_per_medium=16, rays=100_000)
+    for c in trainers:
+        c.close()
+    net, hist = LP.train_proposal(data, steps=3000)
+    assert hist[-200:].mean() < hist[:50].mean()
+    w = media64(16)
+    ctxs = [DeviceMesh(m.mesh, *m.spectra.resampled(False), device=0) for m in w.media]
+    rng = np.random.default_rng(5)
+    items = []
+    for c in ctxs:
+        S = c.mesh.numberOfSamples
+        lo = int(rng.integers(0, max(1, S - 64)))
+        items.append((c, lo, min(S - 1, lo + 63)))
+    kw = dict(minRays=20000, maxRays=20000, monochromatic=False, rngSeed=11, workspaceBytes=16 << 30)
+    with MediaBatch(0) as b:
+        near, _ = b.solve(items, **kw)
+        learned, _ = b.solve(items, net=net, **kw)
+    vn = np.concatenate([LP.per_ray_variance(r) for r in near])
+    vl = np.concatenate([LP.per_ray_variance(r) for r in learned])
+    assert np.median(vl) < 0.85 * np.median(vn), (np.median(vl), np.median(vn))
+    assert np.percentile(vl, 99) < np.percentile(vn, 99)
+    net.close()
+    for c in ctxs:
+        c.close()
