@@ -924,8 +924,9 @@ def run_learned(args):
                 "workload": "media64 (config 3), unseen media",
                 "learned_batched_ms": media["ms_per_step"],
                 "plain_is_sequential_ms": media["plain_is_sequential"]["ms_per_step"],
-                "plain_is_unconverged_samples": media["plain_is_sequential"]["unconverged_samples"],
-                "learned_batched_unconverged_samples": media["unconverged_samples"],
+                "plain_is_unconverged_samples_per_step": media["plain_is_sequential"]["unconverged_samples"] / 2,
+                "learned_batched_unconverged_samples_per_step": media["unconverged_samples"] / 2,
+                "samples_per_step": media["config"]["samples_per_step"],
                 "ratio": media["speedup_vs_plain_is_sequential"],
                 "met": bool(media["speedup_vs_plain_is_sequential"] >= 5.0)}
         print(json.dumps(line), flush=True)
