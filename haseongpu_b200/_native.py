@@ -47,6 +47,8 @@ EXPORTED_SYMBOLS = (
     # include/hase_b200_forward.h
     "hase_tet_context_create",
     "hase_tet_context_update_beta",
+    "hase_tet_context_info",
+    "hase_simulate_forward",
     "hase_tet_calc_phi_ase",
     "hase_tet_context_destroy",
     "hase_tet_tables",
@@ -354,6 +356,9 @@ def lib():
         L.hase_tet_context_create.argtypes = [C.POINTER(TetMeshDesc), C.POINTER(SpectrumDesc), C.c_int,
                                               C.POINTER(C.c_void_p)]
         L.hase_tet_context_update_beta.argtypes = [C.c_void_p, _f64p]
+        L.hase_tet_context_info.argtypes = [C.c_void_p, _u32p, _u32p]
+        L.hase_simulate_forward.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(ForwardDesc), C.POINTER(PumpDesc),
+                                            C.POINTER(TimeDesc), C.POINTER(TimeResultDesc)]
         L.hase_tet_calc_phi_ase.argtypes = [C.c_void_p, C.POINTER(ForwardDesc), C.POINTER(ForwardResultDesc)]
         L.hase_tet_context_destroy.argtypes = [C.c_void_p]
         L.hase_tet_tables.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _f64p]

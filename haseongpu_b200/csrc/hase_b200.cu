@@ -21,6 +21,7 @@
 // entry point include/core/simulation.hpp:42-47.
 #include "hase_b200.h"
 #include "hase_b200_batch.h"
+#include "hase_b200_forward.h"
 #include "hase_b200_proposal.h"
 #include "hase_device.cuh"
 #include "hase_host.cuh"
@@ -1774,24 +1775,39 @@ hase_status hase_calc_phi_ase(hase_context* c, const hase_experiment_desc* ex, c
     return calcCore(c, ex, cp, res, nullptr, nullptr);
 }
 
-hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVariance,
-                          const hase_experiment_desc* ex, const hase_compute_desc* cp, const hase_pump_desc* pd,
-                          const hase_time_desc* td, hase_time_result* res) {
-    if (!c || !ex || !cp || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+}  // extern "C"
+
+namespace {
+
+// The phi-ASE source of one step of the time loop: fills phiPrism (device,
+// [P] FP32, the ASE flux per prism), adds its device time, rays and the mean
+// phi it reports; returns the solve's status (warnings allowed).
+struct AseSource {
+    virtual ~AseSource() = default;
+    virtual hase_status solve(uint32_t step, float* phiPrism, double& ms, uint64_t& rays, double& meanPhi) = 0;
+};
+
+// Time-stepped rate equations (include/core/timeSteppedSimulation.hpp:132-617,
+// include/kernels/derivativeComposition.hpp:27-93): per step the ASE source,
+// then the pump by exact column Beer-Lambert and the frozen-ASE RK4 / Euler
+// update of beta on the device.  sA / sE are the ASE cross sections of the
+// depletion term.
+hase_status simulateCore(hase_context* c, double sA, double sE, AseSource& source, const hase_pump_desc* pd,
+                         const hase_time_desc* td, hase_time_result* res, std::vector<double>& betaHost) {
+    if (!c || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
     if (!(td->timeStep > 0.0) || td->steps == 0) return fail(HASE_INVALID_ARGUMENT, "timeStep and steps must be positive");
     if (td->integrator > 1) return fail(HASE_INVALID_ARGUMENT, "integrator must be 0 (frozen-ASE RK4) or 1 (Euler)");
     if (td->aseSteps > td->steps) return fail(HASE_INVALID_ARGUMENT, "aseSteps > steps");
     if (!(pd->radius > 0.0) || !(pd->exponent > 0.0) || !(pd->wavelength > 0.0) || !(pd->peakIntensity >= 0.0) ||
         !(pd->sigmaA >= 0.0) || !(pd->sigmaE >= 0.0))
         return fail(HASE_INVALID_ARGUMENT, "pump parameters must be positive (intensity and cross sections >= 0)");
-    if (!(fallbackVariance >= 0.0f)) return fail(HASE_INVALID_ARGUMENT, "fallbackVariance must be >= 0");
     HASE_TRY(setDevice(c));
-    const uint32_t P = c->P, T = c->T, S = c->Np * c->L;
+    const uint32_t P = c->P, T = c->T;
     std::vector<uint8_t> clad(P, 0);
     if (!c->cladTypes.empty())
         for (uint32_t p = 0; p < P; ++p) clad[p] = c->cladTypes[p % T] == c->cladNumber ? 1 : 0;
     DevBuf<double> beta0, stage, nextB, acc, rate, absorbed;
-    DevBuf<float> phiS, phiP, area;
+    DevBuf<float> phiP, area;
     DevBuf<uint8_t> dclad;
     HASE_CUDA(beta0.ensure(P));
     HASE_CUDA(stage.ensure(P));
@@ -1799,20 +1815,12 @@ hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVar
     HASE_CUDA(acc.ensure(P));
     HASE_CUDA(rate.ensure(P));
     HASE_CUDA(absorbed.ensure(1));
-    HASE_CUDA(phiS.ensure(S));
     HASE_CUDA(phiP.ensure(P));
     HASE_CUDA(area.ensure(T));
     HASE_CUDA(dclad.ensure(P));
     HASE_CUDA(cudaMemcpyAsync(beta0.p, c->hBeta.data(), P * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(area.p, c->hArea.data(), T * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     HASE_CUDA(cudaMemcpyAsync(dclad.p, clad.data(), P, cudaMemcpyHostToDevice, c->stream));
-    const uint32_t nL = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
-    double sA = c->sigmaA[0], sE = c->sigmaE[0];
-    if (nL > 1)
-        for (uint32_t l = 1; l < nL; ++l) {
-            sA = std::max(sA, c->sigmaA[l]);
-            sE = std::max(sE, c->sigmaE[l]);
-        }
     const double photon = 6.62607015e-34 * 2.99792458e8 / pd->wavelength;  // J
     PumpLaunch pl{};
     pl.centroid = c->centroid.p;
@@ -1838,12 +1846,7 @@ hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVar
         incident += pl.flux0 * std::exp(-std::pow(std::sqrt(dx * dx + dy * dy) / pd->radius, pd->exponent)) *
                     c->hArea[t];
     }
-    hase_compute_desc all = *cp;
-    all.minSample = 0;
-    all.maxSample = UINT32_MAX;
-    std::vector<float> phiHost(S);
-    std::vector<double> betaHost(P);
-    LearnedArgs la{net, 0.1f, fallbackVariance, 0u};
+    betaHost = c->hBeta;
     res->aseMilliseconds = res->pumpMilliseconds = res->totalMilliseconds = 0.0;
     res->raysTraced = 0;
     res->fallbackSamples = 0;
@@ -1877,21 +1880,15 @@ hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVar
     for (uint32_t step = 0; step < td->steps; ++step) {
         const bool ase = step < td->aseSteps, pumpOn = step < td->pumpSteps;
         if (ase) {
-            hase_result r{};
-            r.phiAse = phiHost.data();
-            const hase_status st = calcCore(c, ex, &all, &r, net ? &la : nullptr, nullptr);
+            double ms = 0.0, mp = 0.0;
+            uint64_t rays = 0;
+            const hase_status st = source.solve(step, phiP.p, ms, rays, mp);
             if (st != HASE_OK && st != HASE_NOT_CONVERGED && st != HASE_DROPPED_RAYS) return st;
             if (st != HASE_OK && worst == HASE_OK) worst = st;
-            res->aseMilliseconds += r.totalMilliseconds;
-            res->totalMilliseconds += r.totalMilliseconds;
-            res->raysTraced += r.raysTraced;
-            if (net) res->fallbackSamples += la.fallbackSamples;
-            double mp = 0.0;
-            for (uint32_t k = 0; k < S; ++k) mp += phiHost[k];
-            if (res->meanPhi) res->meanPhi[step] = mp / S;
-            if (res->phiHistory) std::copy(phiHost.begin(), phiHost.end(), res->phiHistory + size_t(step) * S);
-            HASE_CUDA(cudaMemcpyAsync(phiS.p, phiHost.data(), S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-            phiPrismKernel<<<blocksP, 256, 0, c->stream>>>(c->verts.p, phiS.p, phiP.p, T, c->layers, c->Np);
+            res->aseMilliseconds += ms;
+            res->totalMilliseconds += ms;
+            res->raysTraced += rays;
+            if (res->meanPhi) res->meanPhi[step] = mp;
         } else if (res->meanPhi) {
             res->meanPhi[step] = 0.0;
         }
@@ -1930,11 +1927,156 @@ hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVar
         // host copies the next solve's features read
         c->hBeta = betaHost;
         for (uint32_t p = 0; p < P; ++p) c->hGainBeta[p] = clad[p] ? NAN : float(betaHost[p]);
+        ++c->betaVersion;  // the learned proposal's feature grid follows the new beta
         if (res->meanBeta) res->meanBeta[step + 1] = meanGain(betaHost);
     }
     if (res->betaVolume) std::copy(betaHost.begin(), betaHost.end(), res->betaVolume);
     if (worst != HASE_OK) return fail(worst, "a phi-ASE solve of the time loop ended with a warning");
     return HASE_OK;
+}
+
+// ASE from the backward solve over every sample point (importance weights or
+// the learned proposal); a prism's phi is the mean of its six vertices.
+struct BackwardAse final : AseSource {
+    hase_context* c;
+    const hase_experiment_desc* ex;
+    hase_compute_desc all;
+    LearnedArgs la;
+    bool learned;
+    float* phiHistory;
+    uint32_t fallbackSamples = 0;
+    std::vector<float> phiHost;
+    DevBuf<float> phiS;
+    hase_status solve(uint32_t step, float* phiPrism, double& ms, uint64_t& rays, double& meanPhi) override {
+        const uint32_t S = c->Np * c->L;
+        phiHost.resize(S);
+        HASE_CUDA(phiS.ensure(S));
+        hase_result r{};
+        r.phiAse = phiHost.data();
+        const hase_status st = calcCore(c, ex, &all, &r, learned ? &la : nullptr, nullptr);
+        if (st != HASE_OK && st != HASE_NOT_CONVERGED && st != HASE_DROPPED_RAYS) return st;
+        ms = r.totalMilliseconds;
+        rays = r.raysTraced;
+        if (learned) fallbackSamples += la.fallbackSamples;
+        double mp = 0.0;
+        for (uint32_t k = 0; k < S; ++k) mp += phiHost[k];
+        meanPhi = mp / S;
+        if (phiHistory) std::copy(phiHost.begin(), phiHost.end(), phiHistory + size_t(step) * S);
+        HASE_CUDA(cudaMemcpyAsync(phiS.p, phiHost.data(), S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        phiPrismKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->verts.p, phiS.p, phiPrism, c->T, c->layers,
+                                                                 c->Np);
+        HASE_CUDA(cudaGetLastError());
+        return st;
+    }
+};
+
+// ASE from the forward method on the Tet4 twin (cell 3p + k belongs to prism
+// p): the prisms' beta go to their cells, one forward solve, a prism's phi is
+// the volume-weighted mean of its three cells.
+struct ForwardAse final : AseSource {
+    hase_context* c;
+    hase_tet_context* twin;
+    const hase_forward_desc* fw;
+    float* phiHistory;
+    const std::vector<double>* beta;  // the loop's current prism beta (host)
+    std::vector<double> vol, betaCells, rseCells;
+    std::vector<float> phiCells, phiHost;
+    std::vector<uint8_t> clad;
+    uint32_t srmStatus = 0;
+    hase_status solve(uint32_t step, float* phiPrism, double& ms, uint64_t& rays, double& meanPhi) override {
+        const uint32_t P = c->P;
+        betaCells.resize(3 * size_t(P));
+        for (uint32_t p = 0; p < P; ++p)
+            for (int k = 0; k < 3; ++k) betaCells[3 * size_t(p) + k] = (*beta)[p];
+        HASE_TRY(hase_tet_context_update_beta(twin, betaCells.data()));
+        phiCells.resize(3 * size_t(P));
+        hase_forward_result r{};
+        r.phiAse = phiCells.data();
+        const hase_status st = hase_tet_calc_phi_ase(twin, fw, &r);
+        if (st != HASE_OK && st != HASE_NOT_CONVERGED && st != HASE_DROPPED_RAYS) return st;
+        ms = r.totalMilliseconds;
+        rays = r.raysTraced;
+        srmStatus = std::max(srmStatus, r.srmStatus == 3 ? 4u : r.srmStatus == 4 ? 3u : r.srmStatus);
+        phiHost.resize(P);
+        double mp = 0.0;
+        uint32_t n = 0;
+        for (uint32_t p = 0; p < P; ++p) {
+            double num = 0.0, den = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                num += vol[3 * size_t(p) + k] * double(phiCells[3 * size_t(p) + k]);
+                den += vol[3 * size_t(p) + k];
+            }
+            phiHost[p] = float(den > 0.0 ? num / den : 0.0);
+            if (!clad[p]) {
+                mp += phiHost[p];
+                ++n;
+            }
+        }
+        meanPhi = n ? mp / n : 0.0;
+        if (phiHistory) std::copy(phiHost.begin(), phiHost.end(), phiHistory + size_t(step) * P);
+        HASE_CUDA(cudaMemcpyAsync(phiPrism, phiHost.data(), P * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        return st;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+hase_status hase_simulate(hase_context* c, hase_proposal* net, float fallbackVariance,
+                          const hase_experiment_desc* ex, const hase_compute_desc* cp, const hase_pump_desc* pd,
+                          const hase_time_desc* td, hase_time_result* res) {
+    if (!c || !ex || !cp || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    if (!(fallbackVariance >= 0.0f)) return fail(HASE_INVALID_ARGUMENT, "fallbackVariance must be >= 0");
+    const uint32_t nL = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double sA = c->sigmaA[0], sE = c->sigmaE[0];
+    for (uint32_t l = 1; l < nL; ++l) {
+        sA = std::max(sA, c->sigmaA[l]);
+        sE = std::max(sE, c->sigmaE[l]);
+    }
+    BackwardAse src;
+    src.c = c;
+    src.ex = ex;
+    src.all = *cp;
+    src.all.minSample = 0;
+    src.all.maxSample = UINT32_MAX;
+    src.la = LearnedArgs{net, 0.1f, fallbackVariance, 0u};
+    src.learned = net != nullptr;
+    src.phiHistory = res->phiHistory;
+    std::vector<double> betaHost;
+    const hase_status st = simulateCore(c, sA, sE, src, pd, td, res, betaHost);
+    res->fallbackSamples = src.fallbackSamples;
+    return st;
+}
+
+hase_status hase_simulate_forward(hase_context* c, hase_tet_context* twin, const hase_forward_desc* fw,
+                                  const hase_pump_desc* pd, const hase_time_desc* td, hase_time_result* res) {
+    if (!c || !twin || !fw || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
+    const size_t C = 3 * size_t(c->P);
+    ForwardAse src;
+    uint32_t cells = 0, points = 0;
+    HASE_TRY(hase_tet_context_info(twin, &cells, &points));
+    if (cells != C)
+        return fail(HASE_INVALID_ARGUMENT, "the Tet4 twin has %u cells, the prism mesh needs 3 x %u", cells, c->P);
+    src.vol.resize(C);
+    HASE_TRY(hase_tet_tables(twin, nullptr, nullptr, nullptr, src.vol.data()));
+    const uint32_t nL = fw->monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double sA = c->sigmaA[0], sE = c->sigmaE[0];
+    for (uint32_t l = 1; l < nL; ++l) {
+        sA = std::max(sA, c->sigmaA[l]);
+        sE = std::max(sE, c->sigmaE[l]);
+    }
+    src.c = c;
+    src.twin = twin;
+    src.fw = fw;
+    src.phiHistory = res->phiHistory;
+    src.clad.assign(c->P, 0);
+    if (!c->cladTypes.empty())
+        for (uint32_t p = 0; p < c->P; ++p) src.clad[p] = c->cladTypes[p % c->T] == c->cladNumber ? 1 : 0;
+    std::vector<double> betaHost;
+    src.beta = &betaHost;
+    res->fallbackSamples = 0;
+    return simulateCore(c, sA, sE, src, pd, td, res, betaHost);
 }
 
 hase_status hase_calc_phi_ase_learned(hase_context* c, hase_proposal* net, const hase_experiment_desc* ex,

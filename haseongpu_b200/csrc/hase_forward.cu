@@ -1120,6 +1120,13 @@ hase_status hase_tet_context_create(const hase_tet_mesh_desc* d, const hase_spec
     return HASE_OK;
 }
 
+hase_status hase_tet_context_info(hase_tet_context* c, uint32_t* numberOfCells, uint32_t* numberOfPoints) {
+    if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
+    if (numberOfCells) *numberOfCells = c->C;
+    if (numberOfPoints) *numberOfPoints = c->Np;
+    return HASE_OK;
+}
+
 hase_status hase_tet_context_update_beta(hase_tet_context* c, const double* betaVolume) {
     if (!c || !betaVolume) return fail(HASE_INVALID_ARGUMENT, "null argument");
     HASE_CUDA(cudaSetDevice(c->device));

@@ -166,6 +166,30 @@ class DeviceMesh:
                                                         N.ptr(contrib, N._f32p), C.byref(r)), allow_warnings=True)
         return self._fill(out, r, status), contrib
 
+    @staticmethod
+    def _time_descs(pump, time, width, keepPhi, P):
+        pd = N.PumpDesc(float(pump["peakIntensity"]), float(pump["radius"]), float(pump["exponent"]),
+                        float(pump.get("centerX", 0.0)), float(pump.get("centerY", 0.0)), float(pump["wavelength"]),
+                        float(pump["sigmaA"]), float(pump["sigmaE"]), 1 if pump.get("retroreflect", True) else 0)
+        steps = int(time["steps"])
+        td = N.TimeDesc(float(time["timeStep"]), steps, int(time.get("pumpSteps", steps)),
+                        int(time.get("aseSteps", steps)), int(time.get("integrator", 0)))
+        out = {"betaVolume": np.empty(P), "meanBeta": np.empty(steps + 1), "meanPhi": np.empty(steps),
+               "pumpAbsorbed": np.empty(steps)}
+        if keepPhi:
+            out["phiHistory"] = np.empty((td.aseSteps, width), np.float32)
+        r = N.TimeResultDesc(N.ptr(out["betaVolume"], N._f64p), N.ptr(out["meanBeta"], N._f64p),
+                             N.ptr(out["meanPhi"], N._f64p), N.ptr(out["pumpAbsorbed"], N._f64p),
+                             N.ptr(out.get("phiHistory"), N._f32p))
+        return pd, td, r, out
+
+    @staticmethod
+    def _time_out(out, r):
+        out.update(aseMilliseconds=r.aseMilliseconds, pumpMilliseconds=r.pumpMilliseconds,
+                   totalMilliseconds=r.totalMilliseconds, raysTraced=int(r.raysTraced),
+                   fallbackSamples=int(r.fallbackSamples))
+        return out
+
     def simulate(self, *, pump, time, net=None, fallbackVariance=0.0, minRays, maxRays=None, mseThreshold=0.0,
                  useReflections=False, monochromatic=False, nearFieldSampling=True, adaptiveSteps=0, rngSeed=5489,
                  keepPhi=False) -> dict:
@@ -174,27 +198,29 @@ class DeviceMesh:
         context's beta is advanced in place."""
         _, ex, cp, _, _ = self._descs(minRays, maxRays, mseThreshold, useReflections, monochromatic, nearFieldSampling,
                                       adaptiveSteps, 1, rngSeed, 0, None, 0, 0, 0, 0, 0)
-        pd = N.PumpDesc(float(pump["peakIntensity"]), float(pump["radius"]), float(pump["exponent"]),
-                        float(pump.get("centerX", 0.0)), float(pump.get("centerY", 0.0)), float(pump["wavelength"]),
-                        float(pump["sigmaA"]), float(pump["sigmaE"]), 1 if pump.get("retroreflect", True) else 0)
-        steps = int(time["steps"])
-        td = N.TimeDesc(float(time["timeStep"]), steps, int(time.get("pumpSteps", steps)),
-                        int(time.get("aseSteps", steps)), int(time.get("integrator", 0)))
-        P, S = self.mesh.numberOfPrisms, self.mesh.numberOfSamples
-        out = {"betaVolume": np.empty(P), "meanBeta": np.empty(steps + 1), "meanPhi": np.empty(steps),
-               "pumpAbsorbed": np.empty(steps)}
-        if keepPhi:
-            out["phiHistory"] = np.empty((td.aseSteps, S), np.float32)
-        r = N.TimeResultDesc(N.ptr(out["betaVolume"], N._f64p), N.ptr(out["meanBeta"], N._f64p),
-                             N.ptr(out["meanPhi"], N._f64p), N.ptr(out["pumpAbsorbed"], N._f64p),
-                             N.ptr(out.get("phiHistory"), N._f32p))
+        pd, td, r, out = self._time_descs(pump, time, self.mesh.numberOfSamples, keepPhi, self.mesh.numberOfPrisms)
         out["status"] = N.check(N.lib().hase_simulate(self.handle, net.handle if net is not None else None,
                                                       float(fallbackVariance), C.byref(ex), C.byref(cp), C.byref(pd),
                                                       C.byref(td), C.byref(r)), allow_warnings=True)
-        out.update(aseMilliseconds=r.aseMilliseconds, pumpMilliseconds=r.pumpMilliseconds,
-                   totalMilliseconds=r.totalMilliseconds, raysTraced=int(r.raysTraced),
-                   fallbackSamples=int(r.fallbackSamples))
-        return out
+        return self._time_out(out, r)
+
+    def simulate_forward(self, twin, *, pump, time, forwardRayCount, maxRays=None, adaptiveSteps=0,
+                         relativeStandardErrorThreshold=0.0, monochromatic=False, rngSeed=5489, batches=8,
+                         useReflections=False, reflectionMaxIterations=40, reflectionTolerance=1.0e-4,
+                         surfaceReservoirSize=32, keepPhi=False) -> dict:
+        """Time-stepped rate equations with the ASE term from the forward
+        method (hase_simulate_forward) on ``twin``, a TetDeviceMesh of
+        ``TetMesh.fromPrismMesh(self.mesh)``.  ``phiHistory`` (keepPhi) is
+        per prism.  The context's beta is advanced in place."""
+        fw = N.ForwardDesc(int(forwardRayCount), int(maxRays if maxRays is not None else forwardRayCount),
+                           int(adaptiveSteps), float(relativeStandardErrorThreshold), 1 if monochromatic else 0,
+                           int(rngSeed) & 0xFFFFFFFF, int(batches), 0, 0, 1 if useReflections else 0,
+                           int(reflectionMaxIterations), float(reflectionTolerance), int(surfaceReservoirSize), 0)
+        P = self.mesh.numberOfPrisms
+        pd, td, r, out = self._time_descs(pump, time, P, keepPhi, P)
+        out["status"] = N.check(N.lib().hase_simulate_forward(self.handle, twin.handle, C.byref(fw), C.byref(pd),
+                                                              C.byref(td), C.byref(r)), allow_warnings=True)
+        return self._time_out(out, r)
 
     def proposal_features(self, firstSample, count, useReflections=False, monochromatic=False) -> np.ndarray:
         slices = 5 if useReflections else 1

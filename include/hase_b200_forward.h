@@ -136,6 +136,8 @@ typedef struct {
 hase_status hase_tet_context_create(const hase_tet_mesh_desc* mesh, const hase_spectrum_desc* spectrum, int device,
                                     hase_tet_context** out);
 hase_status hase_tet_context_update_beta(hase_tet_context* ctx, const double* betaVolume);
+/* Sizes of the context's mesh (either pointer may be NULL). */
+hase_status hase_tet_context_info(hase_tet_context* ctx, uint32_t* numberOfCells, uint32_t* numberOfPoints);
 hase_status hase_tet_calc_phi_ase(hase_tet_context* ctx, const hase_forward_desc* forward,
                                   hase_forward_result* result);
 hase_status hase_tet_context_destroy(hase_tet_context* ctx);
@@ -157,6 +159,18 @@ hase_status hase_tet_tables(hase_tet_context* ctx, int32_t* neighbors, int32_t* 
 hase_status hase_tet_trace(hase_tet_context* ctx, uint32_t n, const uint32_t* startCell, const double* origin,
                            const double* direction, uint32_t wavelength, uint32_t maxSegments, uint32_t* segments,
                            uint32_t* cells, double* lengths, double* lnGain, double* endPoint, int32_t* status);
+
+/* hase_simulate (include/hase_b200.h) with the ASE term from the forward
+ * method instead of the backward solve: `twin` is the Tet4 twin of the prism
+ * mesh of `prism` (cell 3p + k, k < 3, belongs to prism p, the split of
+ * TetMesh.fromPrismMesh).  Every ASE step copies the prisms' beta to their
+ * cells, runs one forward solve with `forward` (surface-reservoir reflections
+ * when forward->useReflections), and takes a prism's phi as the
+ * volume-weighted mean of its three cells' phi; pump and rate equations are
+ * those of hase_simulate.  result->phiHistory (may be NULL) is
+ * [aseSteps][prisms]; result->meanPhi is the mean over the gain prisms. */
+hase_status hase_simulate_forward(hase_context* prism, hase_tet_context* twin, const hase_forward_desc* forward,
+                                  const hase_pump_desc* pump, const hase_time_desc* time, hase_time_result* result);
 
 #ifdef __cplusplus
 }

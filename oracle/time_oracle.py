@@ -61,8 +61,11 @@ def prism_phi(mesh, phi_samples):
     return out.ravel()
 
 
-def simulate(mesh, beta0, *, pump, time, sigma_ase, phi_history=None):
-    """beta after every step ([steps + 1][P]) and the absorbed pump fraction per step."""
+def simulate(mesh, beta0, *, pump, time, sigma_ase, phi_history=None, phi_prism_history=None):
+    """beta after every step ([steps + 1][P]) and the absorbed pump fraction per step.
+    phi_history: per-sample phi of every ASE step (a prism's phi is the mean of
+    its six vertices); phi_prism_history: per-prism phi of every ASE step (the
+    forward method's volume-weighted cell means) used as given."""
     sA, sE = sigma_ase
     P = mesh.numberOfPrisms
     clad = np.zeros(P, bool)
@@ -75,7 +78,12 @@ def simulate(mesh, beta0, *, pump, time, sigma_ase, phi_history=None):
     for step in range(time["steps"]):
         ase = step < time["aseSteps"]
         pump_on = step < time["pumpSteps"]
-        phi_p = prism_phi(mesh, phi_history[step]).astype(np.float64) if ase else np.zeros(P)
+        if not ase:
+            phi_p = np.zeros(P)
+        elif phi_prism_history is not None:
+            phi_p = np.asarray(phi_prism_history[step], np.float32).astype(np.float64)
+        else:
+            phi_p = prism_phi(mesh, phi_history[step]).astype(np.float64)
 
         def deriv(b, first=False):
             rate = np.zeros(P)

@@ -85,3 +85,56 @@ def test_learned_proposal_in_the_time_loop():
         out = ctx.simulate(pump=PUMP, time=time, net=net, fallbackVariance=1e9, minRays=4000, monochromatic=True)
     assert np.all(np.isfinite(out["betaVolume"])) and out["fallbackSamples"] == 0
     assert out["meanPhi"][0] > 0 and out["meanBeta"][2] > out["meanBeta"][0]
+
+
+def _twin(mesh, sa, se):
+    from haseongpu_b200 import TetDeviceMesh, TetMesh
+
+    return TetDeviceMesh(TetMesh.fromPrismMesh(mesh), sa, se, device=0)
+
+
+def test_forward_driver_without_ase_equals_the_backward_driver():
+    mesh, sa, se = _cladding_mesh()
+    time = dict(timeStep=2e-5, steps=6, pumpSteps=4, aseSteps=0, integrator=0)
+    with _ctx(mesh, sa, se) as a, _ctx(mesh, sa, se) as b, _twin(mesh, sa, se) as twin:
+        back = a.simulate(pump=PUMP, time=time, minRays=1000, monochromatic=True)
+        fwd = b.simulate_forward(twin, pump=PUMP, time=time, forwardRayCount=10000, monochromatic=True)
+    np.testing.assert_array_equal(fwd["betaVolume"], back["betaVolume"])
+    np.testing.assert_allclose(fwd["pumpAbsorbed"], back["pumpAbsorbed"], rtol=1e-12)  # FP64 atomic sums
+
+
+@pytest.mark.parametrize("integrator", [0, 1])
+def test_forward_ase_steps_replay_the_oracle(integrator):
+    """The oracle replays the forward driver's per-prism phi (volume-weighted
+    means of the twin's cells) through the same rate equations."""
+    from oracle import time_oracle as to
+
+    mesh, sa, se = _cladding_mesh()
+    beta0 = mesh.betaVolume.copy()
+    time = dict(timeStep=2e-5, steps=3, pumpSteps=3, aseSteps=2, integrator=integrator)
+    with _ctx(mesh, sa, se) as ctx, _twin(mesh, sa, se) as twin:
+        out = ctx.simulate_forward(twin, pump=PUMP, time=time, forwardRayCount=400_000, monochromatic=True,
+                                   keepPhi=True)
+    assert out["phiHistory"].shape == (2, mesh.numberOfPrisms)
+    assert out["raysTraced"] == 2 * 400_000 and out["meanPhi"][0] > 0 and out["meanPhi"][2] == 0.0
+    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=time, sigma_ase=(sa[0], se[0]),
+                          phi_prism_history=out["phiHistory"])
+    np.testing.assert_allclose(out["betaVolume"], hist[-1], rtol=1e-9, atol=1e-14)
+
+
+def test_forward_and_backward_ase_agree_on_the_mean_flux():
+    """The two methods estimate the same ASE flux: the gain-prism mean of phi
+    of the first step agrees to a few percent."""
+    mesh, sa, se = _cladding_mesh()
+    time = dict(timeStep=2e-5, steps=1, pumpSteps=1, aseSteps=1, integrator=0)
+    with _ctx(mesh, sa, se) as a, _ctx(mesh, sa, se) as b, _twin(mesh, sa, se) as twin:
+        back = a.simulate(pump=PUMP, time=time, minRays=20000, monochromatic=True, keepPhi=True)
+        fwd = b.simulate_forward(twin, pump=PUMP, time=time, forwardRayCount=4_000_000, monochromatic=True,
+                                 keepPhi=True)
+    from oracle import time_oracle as to
+
+    gain = ~np.tile(mesh.claddingCellTypes == mesh.claddingNumber, mesh.numberOfLevels - 1)
+    pb = to.prism_phi(mesh, back["phiHistory"][0])
+    pf = fwd["phiHistory"][0]
+    assert pf[gain].mean() == pytest.approx(pb[gain].mean(), rel=0.05)
+    np.testing.assert_allclose(fwd["betaVolume"][gain].mean(), back["betaVolume"][gain].mean(), rtol=1e-3)
