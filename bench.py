@@ -70,6 +70,8 @@ def parse():
                          "disc_small (importance-sampled solve)")
     ap.add_argument("--no-nested", action="store_true", help="learned workload only: skip the disc_poly and forward lines")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
+    ap.add_argument("--pulse-rays", type=int, default=2_000_000,
+                    help="pulse workload: forward source rays per time step")
     ap.add_argument("--media-samples", type=int, default=64,
                     help="media64 workload: sample points per medium (64 media) per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
@@ -735,6 +737,74 @@ def run_media(args):
     teardown_ranks(world)
 
 
+PULSE_METRIC = ("pump-pulse time series (config 5): 50 rate-equation steps of a 1 ms pump with a forward phi-ASE "
+                "solve (surface-reservoir reflections) per step on 1 B200, as time steps per second")
+
+
+def measure_pulse(args, local):
+    """Config 5 at its stated size: the ~20,000-triangle x 30-level disc (its
+    Tet4 twin: 1.64 M cells), 8 wavelengths, reflectivity 0.3 / 0.9 with
+    total internal reflection, beta from 0 through a 1 ms pump in 50 steps;
+    every step one forward solve of ``--pulse-rays`` source rays with the
+    surface-reservoir passes, then the pump and the RK4 rate-equation update
+    on the device.  Timed: the whole series (device time of the solves and of
+    the pump/update kernels).  After it, one more forward solve at the final
+    beta reports the per-cell relative error that budget reaches."""
+    import numpy as np
+    import torch
+
+    from haseongpu_b200 import DeviceMesh, TetDeviceMesh, TetMesh
+    from haseongpu_b200.configs import pulse
+
+    w = pulse()
+    sa, se = w.spectra.resampled(False)
+    tet = TetMesh.fromPrismMesh(w.mesh)
+    rays = int(args.pulse_rays)
+    kw = dict(forwardRayCount=rays, monochromatic=False, useReflections=True)
+    with DeviceMesh(w.mesh, sa, se, device=local) as ctx, TetDeviceMesh(tet, sa, se, device=local) as twin:
+        warm = dict(w.time, steps=3, pumpSteps=3, aseSteps=3)
+        ctx.simulate_forward(twin, pump=w.pump, time=warm, rngSeed=7, **kw)
+        ctx.update_beta(w.mesh.betaVolume)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = ctx.simulate_forward(twin, pump=w.pump, time=w.time, rngSeed=11, **kw)
+        wall = time.perf_counter() - t0
+        final = twin.calc_phi_ase(forwardRayCount=rays, rngSeed=13, monochromatic=False, useReflections=True)
+    gain = out["betaVolume"] > 0
+    rse = np.repeat(final.relativeStandardError.reshape(-1, 3).max(axis=1), 1)[gain]
+    return {
+        "value": w.time["steps"] / (out["totalMilliseconds"] * 1e-3), "unit": "time steps/s",
+        "ms_per_series": out["totalMilliseconds"], "wall_ms_per_series": wall * 1e3,
+        "ase_ms": out["aseMilliseconds"], "pump_and_update_ms": out["pumpMilliseconds"],
+        "rays_per_s": out["raysTraced"] / (out["aseMilliseconds"] * 1e-3),
+        "source_rays": out["raysTraced"],
+        "config": {"workload": "pulse (config 5): disc of 18,816 triangles x 30 levels, Tet4 twin 1,636,992 cells",
+                   "wavelengths": int(len(sa)), "reflectivity": [0.3, 0.9], "steps": w.time["steps"],
+                   "time_step_s": w.time["timeStep"], "pump_s": w.time["timeStep"] * w.time["pumpSteps"],
+                   "forward_rays_per_step": rays, "phi_method": "forward Tet4 with surface-reservoir reflections"},
+        "mean_beta": {"start": float(out["meanBeta"][0]), "mid": float(out["meanBeta"][25]),
+                      "end": float(out["meanBeta"][-1])},
+        "mean_phi_end": float(out["meanPhi"][-1]),
+        "pump_absorbed_fraction_end": float(out["pumpAbsorbed"][-1]),
+        "final_solve": {"srm_status": final.srmStatus, "srm_passes": final.srmPasses,
+                        "median_cell_rse_gain": float(np.median(rse)) if rse.size else None,
+                        "ms": final.totalMilliseconds, "crossings_per_s": final.crossings / (final.rayMilliseconds * 1e-3)},
+    }
+
+
+def run_pulse(args):
+    rank, world, local = setup_ranks()
+    m = measure_pulse(args, local)
+    if rank == 0:
+        line = {"metric": PULSE_METRIC, "value": m["value"], "unit": m["unit"], "n_gpus": world,
+                "steps": 1, "warmup": 1, "ms_per_step": m["ms_per_series"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 walk and sums",
+                "data": "synthetic (seeded gain medium and pump, no dataset)"}
+        line.update({k: v for k, v in m.items() if k not in ("value", "unit")})
+        print(json.dumps(line), flush=True)
+    teardown_ranks(world)
+
+
 LEARNED_METRIC = ("phi-ASE time to per-sample relative error <= threshold with the learned proposal, as sample points "
                   "solved per second (plain importance sampling on the same fields beside it; rays/s alongside)")
 
@@ -823,7 +893,7 @@ def run_learned(args):
     else:
         ms_l, ms_p, ms_n, e2e_max = a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s
         rays_all, solved_all = float(a["learned"]["rays"]), float(args.steps * S)
-    disc_poly = fwd = media = None
+    disc_poly = fwd = media = pulse_line = None
     if world == 1 and not args.no_nested:
         import argparse as _ap
 
@@ -832,6 +902,7 @@ def run_learned(args):
         nargs.steps, nargs.warmup = max(2, min(args.steps, 3)), max(args.warmup, 3)
         disc_poly = measure_importance(nargs, local, rank, world, nested=True)
         media = measure_media(nargs, local, steps=2, warmup=3)
+        pulse_line = measure_pulse(nargs, local)
         fwd = measure_forward(nargs, local, cpu_seconds=min(args.cpu_seconds, 6.0))
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -912,6 +983,8 @@ def run_learned(args):
                 "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline")}
         if fwd is not None:
             line["forward_tet4"] = fwd
+        if pulse_line is not None:
+            line["pulse_time_series"] = pulse_line
         if media is not None:
             line["batched_media"] = {k: media[k] for k in (
                 "value", "unit", "ms_per_step", "config", "rays_per_s", "crossings_per_s", "breakdown_ms_per_step",
@@ -974,6 +1047,8 @@ def main():
         run_learned(args)
     elif args.workload == "media64":
         run_media(args)
+    elif args.workload == "pulse":
+        run_pulse(args)
     else:
         run_ours(args)
 

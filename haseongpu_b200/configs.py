@@ -25,6 +25,14 @@ media64      64 independent gain media (config 3): per medium a seeded
              U(0.15, 0.35), 1..8 wavelengths (one pair: the disc_small pair;
              more: the two-Lorentzian spectrum); rays 1e4 -> 1e7 per sample,
              threshold 0.001.
+pulse        the pump-pulse time series (config 5): ~10,000 points on 56
+             jittered rings of a 1 cm disc (~20,000 triangles) x 30 levels
+             over 0.7 cm, 8 wavelength pairs of the two-Lorentzian spectrum,
+             reflectivity 0.3 bottom / 0.9 top with refractive index 1.83
+             inside / 1.0 outside; beta starts at 0 and a 1 ms rectangular
+             pump (super-Gaussian, radius 0.6 cm, order 40, 16 kW/cm^2 at
+             940 nm, sigma_a 0.8e-20 / sigma_e 0.16e-20 cm^2, retro-reflected)
+             drives it over 50 steps of 20 us.
 The fluorescence lifetime is 9.41e-4 s (the reference example media,
 example/laserPumpCladdingApi.py:241); it only scales phi.
 """
@@ -147,6 +155,32 @@ def media_training(count: int = 24, max_triangles: int = 3000) -> list:
         if m.mesh.numberOfTriangles <= max_triangles:
             out.append(m)
     return out
+
+
+@dataclass
+class PulseWorkload:
+    name: str
+    mesh: PrismMesh
+    spectra: CrossSectionData
+    pump: dict
+    time: dict
+
+
+def pulse() -> PulseWorkload:
+    rng = _rng(4)
+    pts = disc_points(1.0, 56, rng)
+    tri = delaunay_triangles(pts)
+    levels, thickness = 30, 0.7 / 29
+    T = tri.shape[0]
+    P = T * (levels - 1)
+    mesh = PrismMesh(points=pts, triangles=tri, numberOfLevels=levels, thickness=thickness, betaVolume=np.zeros(P),
+                     nTot=1.38e20, crystalTFluo=TAU, betaCells=np.zeros(pts.shape[0] * levels),
+                     reflectivities=np.tile([0.3, 0.9], (T, 1)), refractiveIndices=[1.83, 1.0, 1.83, 1.0],
+                     name="pulse")
+    pump = dict(peakIntensity=16e3, radius=0.6, exponent=40.0, centerX=0.0, centerY=0.0, wavelength=940e-9,
+                sigmaA=0.8e-20, sigmaE=0.16e-20, retroreflect=True)
+    time = dict(timeStep=20e-6, steps=50, pumpSteps=50, aseSteps=50, integrator=0)
+    return PulseWorkload("pulse", mesh, two_lorentzian_spectrum(8), pump, time)
 
 
 WORKLOADS = {"disc_small": disc_small, "disc_poly": disc_poly}

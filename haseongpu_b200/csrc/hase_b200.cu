@@ -1022,9 +1022,12 @@ __global__ void rateStageKernel(const double* beta0, const double* betaStage, co
     acc[p] = first ? wStage * k : acc[p] + wStage * k;
 }
 
+// beta += dt * (weighted stage derivatives), clipped to [0, 1] as the
+// reference clips after every update (include/kernels/timeIntegrationUpdateKernels.hpp:93-105,
+// include/core/timeSteppedSimulation.hpp:579-586).
 __global__ void rateFinishKernel(double* beta, const double* acc, uint32_t P, double dt) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < P) beta[p] += dt * acc[p];
+    if (p < P) beta[p] = fmin(1.0, fmax(0.0, beta[p] + dt * acc[p]));
 }
 
 // The context's walk / source beta from the FP64 state (NaN marks cladding in the walk table).

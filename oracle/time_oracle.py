@@ -10,7 +10,8 @@ per triangle column Beer-Lambert with g_p = N_tot [beta (sA_p + sE_p) - sA_p]
 per layer, absorbed photons / (N_tot h) (cladding prisms attenuate with
 claddingAbsorption and gain nothing).  Integration: RK4 with the step's
 phi-ASE frozen (the reference's FrozenPhiAseRungeKutta4,
-include/kernels/timeIntegrationUpdateKernels.hpp:21-127) or explicit Euler.
+include/kernels/timeIntegrationUpdateKernels.hpp:21-127) or explicit Euler,
+beta clipped to [0, 1] after every update as the reference's ClipBeta.
 The phi-ASE of each solve comes from the caller (the device's phiHistory),
 so both integrate the same ASE term.
 """
@@ -104,5 +105,7 @@ def simulate(mesh, beta0, *, pump, time, sigma_ase, phi_history=None, phi_prism_
             beta = beta + dt * (k1 / 6 + k2 / 3 + k3 / 3 + k4 / 6)
         else:
             beta = beta + dt * deriv(beta, True)
+        # clipped to [0, 1] after every update (include/kernels/timeIntegrationUpdateKernels.hpp:93-105)
+        beta = np.clip(beta, 0.0, 1.0)
         hist.append(beta.copy())
     return np.array(hist), np.array(absorbed)
