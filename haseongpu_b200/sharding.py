@@ -49,3 +49,44 @@ def gather_results(local: dict, first: int, last: int, group=None, device=None) 
         assert full.size == n
         out[name] = full.astype(a.dtype)
     return out
+
+
+def shard_media(costs, world: int, rank: int | None = None):
+    """Media of a batched solve spread over `world` ranks: longest-first greedy
+    assignment by cost (e.g. sample points x prisms x expected rays), ties to
+    the lowest rank, deterministic on every rank.  Returns the owner rank of
+    every medium, or the indices of `rank`'s media (in increasing order)."""
+    if world <= 0 or (rank is not None and not 0 <= rank < world):
+        raise ValueError("need world > 0 and 0 <= rank < world")
+    costs = np.asarray(costs, np.float64)
+    if np.any(costs < 0) or not np.all(np.isfinite(costs)):
+        raise ValueError("costs must be finite and non-negative")
+    order = np.argsort(-costs, kind="stable")
+    load = np.zeros(world)
+    owner = np.empty(costs.size, np.int64)
+    for i in order:
+        r = int(np.argmin(load))
+        owner[i] = r
+        load[r] += costs[i]
+    return owner if rank is None else np.nonzero(owner == rank)[0]
+
+
+def gather_media_results(local: dict, count: int, group=None) -> list:
+    """All-gather per-medium results ({medium index: result dict of arrays})
+    from every rank into one list of `count` entries on every rank."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    parts = [None] * world
+    dist.all_gather_object(parts, {int(k): {f: np.asarray(v) for f, v in r.items()} for k, r in local.items()},
+                           group=group)
+    out = [None] * count
+    for p in parts:
+        for k, r in p.items():
+            if out[k] is not None:
+                raise ValueError(f"medium {k} was solved on two ranks")
+            out[k] = r
+    missing = [k for k, r in enumerate(out) if r is None]
+    if missing:
+        raise ValueError(f"media {missing} were solved on no rank")
+    return out
