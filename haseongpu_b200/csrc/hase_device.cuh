@@ -160,6 +160,9 @@ template <typename Loader>
 __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
     float4 a, b, c;
     load(r.t, a, b, c);
+    // beta of the current prism, issued with the record so that its latency
+    // overlaps the edge tests
+    float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
     float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
     int bw = -1;
     const auto edge = [&](float nx, float ny, float cc, int nbw, int e) {
@@ -183,7 +186,6 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
     const int dl = r.uz > 0.0f ? -1 : 1;
     while (true) {
         const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
-        const float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
         const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
         const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
         if (next <= m.tolEnd) {
@@ -205,6 +207,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             r.phys = cand;
         }
         r.lu += dl;
+        gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
     }
     r.t = uint32_t(bw) >> 2;
     r.forb = bw & 3;
