@@ -195,15 +195,19 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
             sOut = 0.0f;
             done = true;
         }
+        // beta of every line's current prism in this triangle, issued together
+        float gbv[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) gbv[g] = ok[g] ? __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk) : 0.0f;
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             if (!ok[g]) continue;
             const int dl = kImg > l0 + g ? 1 : -1;  // layer step toward the image level
             float s = sc;
+            float gb = gbv[g];
             while (true) {
                 const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg) * invc[g];
                 if (!(sb > sOut)) break;
-                const float gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
                 J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sb, J[g]);
                 s = sb;
                 const int cand = phys[g] + pdir[g] * dl;
@@ -219,11 +223,11 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                     pdir[g] = -pdir[g];
                 } else {
                     phys[g] = cand;
+                    gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
                 }
                 ka[g] += dl;
             }
             if (!ok[g]) continue;
-            const float gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
             J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sOut, J[g]);
         }
         if (!done) {
