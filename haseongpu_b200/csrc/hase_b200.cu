@@ -67,6 +67,10 @@ constexpr int kRefill = 8;  // idle lanes that trigger a batched refill
 constexpr uint32_t kMaxItems = 1024;  // work items per sample and pass
 constexpr uint32_t kMinItemRays = 1024;
 constexpr uint32_t kMapBlock = 1024;
+#ifndef HASE_WALK_COLUMNS
+#define HASE_WALK_COLUMNS 32
+#endif
+constexpr int kWalkColumns = HASE_WALK_COLUMNS;  // triangle columns per stepRay call of the ray kernel
 constexpr double kPi = 3.14159265358979323846;
 
 // ------------------------------------------------------------ reductions ----
@@ -561,7 +565,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 fetch += uint32_t(nIdle);
             }
             if (active) {
-                const int st = stepRay(m, S.x, S.y, ray, load);
+                const int st = stepRay<kWalkColumns>(m, S.x, S.y, ray, load);
                 if (st != kContinue) {
                     crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {

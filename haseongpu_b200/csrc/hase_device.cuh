@@ -156,61 +156,70 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
 // compared as fractions num/den by cross multiplication; one approximate
 // division gives the chosen exit parameter), then every level plane crossed
 // before it.
-template <typename Loader>
+// Walks up to K triangle columns per call.  Once a column's exit edge is
+// known, the next triangle's walk record is loaded (into the registers the
+// current record no longer needs) while the current column's level planes are
+// worked through, so its latency is hidden behind them.
+template <int K = 1, typename Loader>
 __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
     float4 a, b, c;
     load(r.t, a, b, c);
     // beta of the current prism, issued with the record so that its latency
     // overlaps the edge tests
     float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
-    float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
-    int bw = -1;
-    const auto edge = [&](float nx, float ny, float cc, int nbw, int e) {
-        const float dd = -fmaf(nx, r.ux, ny * r.uy);       // > 0: moving out through e
-        const float nm = fmaf(nx, Sx, fmaf(ny, Sy, -cc));  // signed distance of the sample from the edge line
-        // Boundary edges are never exits: the 2-D mesh is convex and the
-        // target lies in it, so only rounding could route a ray across one.
-        const bool ok = (e != r.forb) & (dd > 0.0f) & (nbw >= 0);
-        if (ok && nm * bd > bn * dd) {
-            bn = nm;
-            bd = dd;
-            bw = nbw;
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+        float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
+        int bw = -1;
+        const auto edge = [&](float nx, float ny, float cc, int nbw, int e) {
+            const float dd = -fmaf(nx, r.ux, ny * r.uy);       // > 0: moving out through e
+            const float nm = fmaf(nx, Sx, fmaf(ny, Sy, -cc));  // signed distance of the sample from the edge line
+            // Boundary edges are never exits: the 2-D mesh is convex and the
+            // target lies in it, so only rounding could route a ray across one.
+            const bool ok = (e != r.forb) & (dd > 0.0f) & (nbw >= 0);
+            if (ok && nm * bd > bn * dd) {
+                bn = nm;
+                bd = dd;
+                bw = nbw;
+            }
+        };
+        edge(a.x, a.y, a.z, __float_as_int(c.y), 0);
+        edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
+        edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
+        const float sEdge = fminf(__fdividef(bn, bd), r.s);
+        if (K > 1 && k + 1 < K && bw >= 0) load(uint32_t(bw) >> 2, a, b, c);
+        // Level planes crossed before the edge exit: the triangle, and with it
+        // sEdge, stays the same, so they cost no edge test.
+        const int dl = r.uz > 0.0f ? -1 : 1;
+        while (true) {
+            const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
+            const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
+            const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
+            if (next <= m.tolEnd) {
+                r.G = fmaf(g, r.s, r.G);
+                r.s = 0.0f;
+                return kDone;
+            }
+            r.G = fmaf(g, r.s - next, r.G);
+            r.s = next;
+            if (++r.steps >= kMaxSteps) return kDropped;
+            if (sz < sEdge) break;
+            const int cand = r.phys + r.pdir * dl;
+            if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+                if (r.reflLeft <= 0) return kDropped;
+                r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
+                --r.reflLeft;
+                r.pdir = -r.pdir;
+            } else {
+                r.phys = cand;
+            }
+            r.lu += dl;
+            gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
         }
-    };
-    edge(a.x, a.y, a.z, __float_as_int(c.y), 0);
-    edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
-    edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
-    const float sEdge = fminf(__fdividef(bn, bd), r.s);
-    // Level planes crossed before the edge exit: the triangle, and with it
-    // sEdge, stays the same, so they cost no edge test.
-    const int dl = r.uz > 0.0f ? -1 : 1;
-    while (true) {
-        const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
-        const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
-        const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
-        if (next <= m.tolEnd) {
-            r.G = fmaf(g, r.s, r.G);
-            r.s = 0.0f;
-            return kDone;
-        }
-        r.G = fmaf(g, r.s - next, r.G);
-        r.s = next;
-        if (++r.steps >= kMaxSteps) return kDropped;
-        if (sz < sEdge) break;
-        const int cand = r.phys + r.pdir * dl;
-        if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
-            if (r.reflLeft <= 0) return kDropped;
-            r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
-            --r.reflLeft;
-            r.pdir = -r.pdir;
-        } else {
-            r.phys = cand;
-        }
-        r.lu += dl;
-        gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
+        r.t = uint32_t(bw) >> 2;
+        r.forb = bw & 3;
+        if (K > 1 && k + 1 < K) gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
     }
-    r.t = uint32_t(bw) >> 2;
-    r.forb = bw & 3;
     return kContinue;
 }
 
