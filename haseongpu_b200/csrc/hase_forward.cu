@@ -58,6 +58,7 @@ constexpr uint32_t kFwdBlock = 256u;
 constexpr int kFwdRefill = 8;          // idle lanes that trigger a batched start of new rays
 constexpr int kFwdMinBlocks = 3;       // resident ray-kernel blocks per SM the register budget is cut for
 constexpr int kFwdMaxSteps = 10000;    // bounded walk: a ray still inside after this many cells is dropped
+constexpr int kFwdSteps = 32;         // cells a lane walks between the warp's ray-claim checks
 constexpr size_t kMaxHistogramBytes = 200u * 1024u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
@@ -481,34 +482,37 @@ __global__ void __launch_bounds__(kFwdBlock, kFwdMinBlocks) fwdRayKernel(const F
                 }
             }
         }
-        if (!live) continue;
-        double lam[4], dl[4], len;
-        const int bf = exitFace(m.cell[r.c].plane, r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
-        bool drop = bf < 0 || ++r.steps > kFwdMaxSteps;
-        if (!drop) {
-            drop = !tallySegment(m, r, len, lam, dl);
-            if (!drop) atomicAdd(L.visits + r.c, 1u);
-        }
-        if (drop) {
-            atomicAdd(L.dropped + r.c, 1u);
-            flushPending(r, add);
-            live = false;
-            continue;
-        }
-        r.x = fma(r.ux, len, r.x);
-        r.y = fma(r.uy, len, r.y);
-        r.z = fma(r.uz, len, r.z);
-        const int n = bf == 0 ? r.nbr.x : bf == 1 ? r.nbr.y : bf == 2 ? r.nbr.z : r.nbr.w;
-        if (n < 0) {
-            flushPending(r, add);
-            if (MODE != 0 && n <= -2) depositReflection(L, b, uint32_t(-2 - n), r);
-            live = false;  // left the mesh
-        } else {
-            r.c = uint32_t(n) >> 2;
-            r.ff = n & 3;
-            const CellLinks lk = ldLinks(&m.cell[r.c].nbr);
-            r.nbr = lk.nbr;
-            carryPending(r, bf, r.ff, lk.matv, m.Np, add);
+        // up to kFwdSteps cells per lane before the warp meets again to claim rays
+#pragma unroll 1
+        for (int k = 0; k < kFwdSteps && live; ++k) {
+            double lam[4], dl[4], len;
+            const int bf = exitFace(m.cell[r.c].plane, r.x, r.y, r.z, r.ux, r.uy, r.uz, r.ff, lam, dl, len);
+            bool drop = bf < 0 || ++r.steps > kFwdMaxSteps;
+            const int n = bf == 0 ? r.nbr.x : bf == 1 ? r.nbr.y : bf == 2 ? r.nbr.z : r.nbr.w;
+            if (!drop) {
+                drop = !tallySegment(m, r, len, lam, dl);
+                if (!drop) atomicAdd(L.visits + r.c, 1u);
+            }
+            if (drop) {
+                atomicAdd(L.dropped + r.c, 1u);
+                flushPending(r, add);
+                live = false;
+                break;
+            }
+            r.x = fma(r.ux, len, r.x);
+            r.y = fma(r.uy, len, r.y);
+            r.z = fma(r.uz, len, r.z);
+            if (n < 0) {
+                flushPending(r, add);
+                if (MODE != 0 && n <= -2) depositReflection(L, b, uint32_t(-2 - n), r);
+                live = false;  // left the mesh
+            } else {
+                r.c = uint32_t(n) >> 2;
+                r.ff = n & 3;
+                const CellLinks lk = ldLinks(&m.cell[r.c].nbr);
+                r.nbr = lk.nbr;
+                carryPending(r, bf, r.ff, lk.matv, m.Np, add);
+            }
         }
     }
     if (SMEM) {
