@@ -889,7 +889,7 @@ __global__ void __launch_bounds__(kTile, kMlpBlocksPerSM) proposalKernel(const P
             for (int k = 0; k < kFeat; ++k) f[k] = 0.0f;
         }
         storeFeatures(T, SmemMap::a0, f);
-        const float logit = mlpTile(T);
+        const float logit = mlpTile<true>(T);
         if (gr < total) P.out[gr] = logit;
         if (!__syncthreads_and(T.ok)) break;
     }

@@ -161,6 +161,24 @@ __device__ __forceinline__ void tmemLd16(uint32_t taddr, uint32_t (&r)[16]) {
 // rounding that follows); v -> -inf gives -0.
 __device__ __forceinline__ float silu(float v) { return __fdividef(v, 1.0f + __expf(-v)); }
 
+// SiLU from one special-function instruction, for the proposal inside the
+// phi-ASE solve: v sigmoid(v) = h + h tanh(h), h = v / 2, with the hardware
+// tanh approximation (tanh.approx.f32).  Against the exact form it differs by
+// the approximation's relative error (about 2^-11), below the BF16 rounding
+// that follows on the hidden layers; the solve weights every ray by the
+// proposal it was actually drawn from, so the estimate stays unbiased.
+__device__ __forceinline__ float siluTanh(float v) {
+    const float h = 0.5f * v;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+    return fmaf(h, t, h);
+}
+
+template <bool FAST>
+__device__ __forceinline__ float act(float v) {
+    return FAST ? siluTanh(v) : silu(v);
+}
+
 __device__ __forceinline__ uint32_t packBf16(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&h);
@@ -217,6 +235,7 @@ __device__ __forceinline__ void runLayer(Tile& T, uint32_t aOff, uint32_t wOff, 
 
 // Bias + SiLU of the accumulator row, stored as bf16 row `threadIdx.x` of the
 // next layer's A operand (K = 64).
+template <bool FAST = false>
 __device__ __forceinline__ void epilogueToSmem(Tile& T, uint32_t col, const float* bias, uint32_t outOff) {
     float acc[kHid];
     loadRow(T, col, acc);
@@ -225,10 +244,10 @@ __device__ __forceinline__ void epilogueToSmem(Tile& T, uint32_t col, const floa
 #pragma unroll
     for (int c = 0; c < kHid / 8; ++c) {
         uint4 v;
-        v.x = packBf16(silu(acc[8 * c + 0] + bias[8 * c + 0]), silu(acc[8 * c + 1] + bias[8 * c + 1]));
-        v.y = packBf16(silu(acc[8 * c + 2] + bias[8 * c + 2]), silu(acc[8 * c + 3] + bias[8 * c + 3]));
-        v.z = packBf16(silu(acc[8 * c + 4] + bias[8 * c + 4]), silu(acc[8 * c + 5] + bias[8 * c + 5]));
-        v.w = packBf16(silu(acc[8 * c + 6] + bias[8 * c + 6]), silu(acc[8 * c + 7] + bias[8 * c + 7]));
+        v.x = packBf16(act<FAST>(acc[8 * c + 0] + bias[8 * c + 0]), act<FAST>(acc[8 * c + 1] + bias[8 * c + 1]));
+        v.y = packBf16(act<FAST>(acc[8 * c + 2] + bias[8 * c + 2]), act<FAST>(acc[8 * c + 3] + bias[8 * c + 3]));
+        v.z = packBf16(act<FAST>(acc[8 * c + 4] + bias[8 * c + 4]), act<FAST>(acc[8 * c + 5] + bias[8 * c + 5]));
+        v.w = packBf16(act<FAST>(acc[8 * c + 6] + bias[8 * c + 6]), act<FAST>(acc[8 * c + 7] + bias[8 * c + 7]));
         *reinterpret_cast<uint4*>(out + c * 128u) = v;
     }
     fenceBeforeSync();
@@ -255,13 +274,15 @@ __device__ __forceinline__ void storeFeatures(Tile& T, uint32_t a0Off, const flo
     __syncthreads();
 }
 
-// The three tensor-core layers and the output layer for the rows in A0.
+// The three tensor-core layers and the output layer for the rows in A0
+// (FAST: the single-instruction SiLU of the in-solve proposal).
+template <bool FAST = false>
 __device__ __forceinline__ float mlpTile(Tile& T) {
     const float* vec = reinterpret_cast<const float*>(T.base + SmemMap::vec);
     runLayer(T, SmemMap::a0, SmemMap::w1, kIn, 0, SmemMap::bar);
-    epilogueToSmem(T, 0, vec, SmemMap::a1);
+    epilogueToSmem<FAST>(T, 0, vec, SmemMap::a1);
     runLayer(T, SmemMap::a1, SmemMap::w2, kHid, 0, SmemMap::bar);
-    epilogueToSmem(T, 0, vec + kHid, SmemMap::a2);
+    epilogueToSmem<FAST>(T, 0, vec + kHid, SmemMap::a2);
     runLayer(T, SmemMap::a2, SmemMap::w3, kHid, 0, SmemMap::bar);
     float acc[kHid];
     loadRow(T, 0, acc);
@@ -269,7 +290,7 @@ __device__ __forceinline__ float mlpTile(Tile& T) {
     const float* w4 = vec + 3 * kHid;
     float logit = vec[4 * kHid];
 #pragma unroll
-    for (int n = 0; n < kHid; ++n) logit = fmaf(silu(acc[n] + b3[n]), w4[n], logit);
+    for (int n = 0; n < kHid; ++n) logit = fmaf(act<FAST>(acc[n] + b3[n]), w4[n], logit);
     fenceBeforeSync();
     __syncthreads();  // TMEM reads done before the next tile's MMA overwrites D
     return logit;
