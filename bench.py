@@ -597,12 +597,15 @@ def measure_media(args, local, steps, warmup):
             st_all.append(st)
         return out, st_all
 
+    # the plain method judges the learned proposal: the largest per-ray variance
+    # the importance weights reached on the logged training samples
+    fallback = data.fallback_limit(1.0)
     for k in range(warmup):
-        batch.solve(items, rngSeed=100 + 64 * k, net=net, **kw)
+        batch.solve(items, rngSeed=100 + 64 * k, net=net, fallbackVariance=fallback, **kw)
         batch.solve(items, rngSeed=100 + 64 * k, **kw)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        lt, lst = timed(lambda seed: batch.solve(items, rngSeed=seed, net=net, **kw))
+        lt, lst = timed(lambda seed: batch.solve(items, rngSeed=seed, net=net, fallbackVariance=fallback, **kw))
         bt, bst = timed(lambda seed: batch.solve(items, rngSeed=seed, **kw))
     clocks = clk.summary()
     seq_ms, wall_s, same = 0.0, 0.0, True
@@ -634,7 +637,7 @@ def measure_media(args, local, steps, warmup):
     for s_ in range(steps):
         for c, b in zip(ctxs, betas):
             c.update_beta(b)
-        batch.solve(items, rngSeed=1000 + 64 * s_, net=net, **kw)
+        batch.solve(items, rngSeed=1000 + 64 * s_, net=net, fallbackVariance=fallback, **kw)
     e2e_s = time.perf_counter() - te
 
     def agg(st_all):
@@ -673,6 +676,9 @@ def measure_media(args, local, steps, warmup):
                                   "graph_capture_host": L["capture_ms"] / steps},
         "rays_per_sample": {"min": int(per_ray.min()), "median": float(np.median(per_ray)), "max": int(per_ray.max())},
         "unconverged_samples": L["unconverged"],
+        "fallback": {"per_ray_variance_limit": fallback, "samples": sum(st.fallbackSamples for st in lst),
+                     "rule": "first-pass per-ray variance above the largest the importance weights reached on "
+                             "the logged training samples"},
         "per_ray_variance": {"learned_median": float(np.median(lv)), "learned_max": float(lv.max()),
                              "importance_nearfield_median": float(np.median(nv)),
                              "importance_nearfield_max": float(nv.max()),
@@ -844,10 +850,15 @@ def run_learned(args):
     kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
               monochromatic=True, minSample=0, maxSample=S - 1)
 
+    # the plain method judges the learned proposal: a sample whose first-pass
+    # per-ray variance exceeds the worst the importance weights reached on the
+    # logged training samples restarts with the importance weights
+    fallback = data.fallback_limit(1.0)
+
     def solve(kind, k):
         ctx.update_beta(fields[k])
         if kind == "learned":
-            return ctx.calc_phi_ase_learned(net, rngSeed=3000 + k, **kw)
+            return ctx.calc_phi_ase_learned(net, rngSeed=3000 + k, fallbackVariance=fallback, **kw)
         return ctx.calc_phi_ase(rngSeed=3000 + k, nearFieldSampling=(kind == "nearfield"), **kw)
 
     def barrier():
@@ -957,7 +968,11 @@ def run_learned(args):
                                      "rays_logged": data.groups * data.rays, "log_s": t1 - t0, "train_s": t2 - t1,
                                      "adam_steps": 3000, "loss_first_50": float(hist[:50].mean()),
                                      "loss_last_200": float(hist[-200:].mean())},
-                        "speedup_vs_plain_is": ms_p / ms_l, "speedup_vs_importance_nearfield": ms_n / ms_l},
+                        "speedup_vs_plain_is": ms_p / ms_l, "speedup_vs_importance_nearfield": ms_n / ms_l,
+                        "fallback": {"per_ray_variance_limit": fallback,
+                                     "samples": sum(r.fallbackSamples for r in acc["learned"]),
+                                     "rule": "first-pass per-ray variance above the largest the importance weights "
+                                             "reached on the logged training samples"}},
             "rays_per_s": rays_all / (ms_l * 1e-3),
             "e2e": {"value": solved_all / e2e_max, "unit": "samples/s", "h2d_bytes_per_step": mesh.numberOfPrisms * 8,
                     "d2h_bytes_per_step": S * (4 + 8 + 8 + 4 + 8 + 4)},
@@ -989,7 +1004,7 @@ def run_learned(args):
         if media is not None:
             line["batched_media"] = {k: media[k] for k in (
                 "value", "unit", "ms_per_step", "config", "rays_per_s", "crossings_per_s", "breakdown_ms_per_step",
-                "rays_per_sample", "unconverged_samples", "per_ray_variance", "training", "importance_batched",
+                "rays_per_sample", "unconverged_samples", "fallback", "per_ray_variance", "training", "importance_batched",
                 "importance_sequential", "plain_is_sequential", "speedup_vs_plain_is_sequential",
                 "speedup_vs_importance_batched", "speedup_batched_vs_sequential", "graph", "e2e", "roofline")}
             line["north_star_target"] = {

@@ -309,6 +309,7 @@ class BatchStats(C.Structure):
         ("captureMilliseconds", C.c_double),
         ("setupMilliseconds", C.c_double),
         ("hostMilliseconds", C.c_double),
+        ("fallbackSamples", C.c_uint32),
     ]
 
 
@@ -384,7 +385,7 @@ def lib():
                                               C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), C.POINTER(BatchStats)]
         L.hase_calc_phi_ase_batch_learned.argtypes = [C.c_void_p, C.POINTER(BatchInstance), C.c_uint32,
                                                       C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), C.c_void_p,
-                                                      C.c_float, C.POINTER(BatchStats)]
+                                                      C.c_float, C.c_float, C.POINTER(BatchStats)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("hase_last_error_message", "hase_status_string", "hase_abi_version",
                             "hase_ray_kernel_variant_count", "hase_ray_kernel_variant_name"):

@@ -35,6 +35,7 @@ class BatchStats:
     captureMilliseconds: float
     setupMilliseconds: float
     hostMilliseconds: float
+    fallbackSamples: int
     status: int = 0
 
 
@@ -49,11 +50,13 @@ class MediaBatch:
 
     def solve(self, media, *, minRays, maxRays=None, mseThreshold=0.0, useReflections=False, monochromatic=False,
               nearFieldSampling=True, adaptiveSteps=0, rngSeed=5489, raysPerThread=0, workspaceBytes=0,
-              rayKernelVariant=0, importanceLayers=0, net=None, mixture=0.0):
+              rayKernelVariant=0, importanceLayers=0, net=None, mixture=0.0, fallbackVariance=0.0):
         """media: DeviceMesh objects, or (DeviceMesh, minSample, maxSample)
         tuples (maxSample None = last).  net: a ProposalNet whose learned
         proposal replaces the importance weights of every medium (mixture:
-        weight of the beta V / d^2 prior, 0 = 0.1).  Returns
+        weight of the beta V / d^2 prior, 0 = 0.1; fallbackVariance: per-ray
+        variance above which a sample restarts with the importance weights
+        after the first pass, 0 = never).  Returns
         ([Result per medium], BatchStats)."""
         items = []
         for m in media:
@@ -82,7 +85,8 @@ class MediaBatch:
             rc = N.lib().hase_calc_phi_ase_batch(self.handle, descs, len(items), C.byref(ex), C.byref(cp), C.byref(st))
         else:
             rc = N.lib().hase_calc_phi_ase_batch_learned(self.handle, descs, len(items), C.byref(ex), C.byref(cp),
-                                                         net.handle, float(mixture), C.byref(st))
+                                                         net.handle, float(mixture), float(fallbackVariance),
+                                                         C.byref(st))
         status = N.check(rc, allow_warnings=True)
         for out, r in zip(outs, keep):
             DeviceMesh._fill(out, r, status)

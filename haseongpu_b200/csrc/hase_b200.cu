@@ -122,6 +122,8 @@ struct ImportanceLaunch {
     float A, B;   // spectrally averaged gain coefficients
     float* lnw;   // [rows][nW]
     const uint32_t* rowList;  // rows to compute (blockIdx.y indexes it), or null: rows 0 .. gridDim.y - 1
+    const uint8_t* rowFlag;   // batched media: only rows with rowFlag[flagBase + row] set are computed (or null)
+    uint32_t flagBase;
 };
 
 // One thread per (sample, reflection slice, triangle, group of G layers): the
@@ -140,6 +142,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= L.slices * perSlice) return;
     const uint32_t row = L.rowList ? L.rowList[blockIdx.y] : blockIdx.y;
+    if (L.rowFlag && !L.rowFlag[L.flagBase + row]) return;
     const uint32_t j = idx / perSlice;
     const uint32_t rem = idx - j * perSlice;
     const uint32_t grp = rem / m.T, t = rem - grp * m.T;
@@ -294,6 +297,7 @@ struct MapLaunch {
     uint32_t* offsets;          // [rows][nW+1]
     const RowInfo* rows;        // batched media: ragged rows (nW, workspace offset, sample, seed per row)
     const unsigned int* count;  // batched media: rows of rowList to map (device), blocks stride over them
+    const uint8_t* rowFlag;     // batched media: only rows with rowFlag[row] set are mapped (or null)
 };
 
 __device__ void mapRow(const MapLaunch& L, uint32_t row) {
@@ -390,7 +394,9 @@ __device__ void mapRow(const MapLaunch& L, uint32_t row) {
 __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
     const uint32_t n = L.count ? *L.count : gridDim.x;
     for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-        mapRow(L, L.rowList ? L.rowList[i] : i);
+        const uint32_t row = L.rowList ? L.rowList[i] : i;
+        if (L.rowFlag && !L.rowFlag[row]) continue;  // uniform over the block
+        mapRow(L, row);
         __syncthreads();  // shared scratch is reused by the next row
     }
 }
@@ -698,6 +704,38 @@ __device__ void finalizeRow(const FinalizeLaunch& L, uint32_t row, int lane) {
 __global__ void iotaKernel(uint32_t* a, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = i;
+}
+
+// Batched learned solve, after the first pass: the still-active rows whose
+// per-ray relative variance (rays x relative error^2) exceeds the limit are
+// flagged to restart with the importance weights (counted in *flagged).
+__global__ void fallbackMarkKernel(const uint32_t* active, const unsigned int* count, const uint32_t* total,
+                                   const double* rse, double limit, uint8_t* flag, unsigned int* flagged) {
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t row = active[i];
+        const double v = double(total[row]) * rse[row] * rse[row];
+        if (!(v <= limit)) {
+            flag[row] = 1;
+            atomicAdd(flagged, 1u);
+        }
+    }
+}
+
+// Zeroes the accumulators of the flagged active rows.
+__global__ void resetFlaggedKernel(const uint32_t* active, const unsigned int* count, const uint8_t* flag,
+                                   double* sum, double* sum2, uint32_t* total, uint32_t* drop,
+                                   unsigned long long* cross) {
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t row = active[i];
+        if (!flag[row]) continue;
+        sum[row] = 0.0;
+        sum2[row] = 0.0;
+        total[row] = 0u;
+        drop[row] = 0u;
+        cross[row] = 0ull;
+    }
 }
 
 // iota plus the device-held row count of a batched solve's first pass.
@@ -2395,6 +2433,7 @@ struct hase_batch {
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> ev;  // timing events recorded inside the graphs
     DevBuf<float> lnw, phi, prior;
+    DevBuf<uint8_t> rowFlag;      // rows restarting with the importance weights (learned solve)
     DevBuf<uint32_t> q, offsets, activeA, activeB, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> counts;  // [0], [1]: active rows (alternating), [2]: item counter, [3 ..]: per pass
     DevBuf<unsigned long long> Q, accCross, pCross;
@@ -2527,7 +2566,8 @@ namespace {
 // replaced by the learned proposal (network logits mixed with the
 // beta V R_j / d^2 prior, weight alpha), as hase_calc_phi_ase_learned does.
 hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t count, const hase_experiment_desc* ex,
-                      const hase_compute_desc* cp, hase_batch_stats* stats, hase_proposal* net, float alpha) {
+                      const hase_compute_desc* cp, hase_batch_stats* stats, hase_proposal* net, float alpha,
+                      float fallbackVariance) {
     if (!b || !in || !ex || !cp || count == 0) return fail(HASE_INVALID_ARGUMENT, "null argument or no instances");
     const auto hostStart = std::chrono::steady_clock::now();
     auto sinceStart = [&] {
@@ -2655,7 +2695,9 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
     HASE_CUDA(b->rows.ensure(maxRows));
     HASE_CUDA(b->activeA.ensure(maxRows));
     HASE_CUDA(b->activeB.ensure(maxRows));
-    HASE_CUDA(b->counts.ensure(3 + nPasses));
+    HASE_CUDA(b->counts.ensure(4 + nPasses));
+    const bool fallback = net && fallbackVariance > 0.0f && nPasses > 1;
+    if (fallback) HASE_CUDA(b->rowFlag.ensure(maxRows));
     HASE_CUDA(b->accSum.ensure(maxRows));
     HASE_CUDA(b->accSum2.ensure(maxRows));
     HASE_CUDA(b->accTotal.ensure(maxRows));
@@ -2682,7 +2724,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
     uint64_t droppedTotal = 0;
     std::vector<float> hPhi(maxRows);
     std::vector<double> hMse(maxRows);
-    std::vector<uint32_t> hTotal(maxRows), hDrop(maxRows), hCounts(3 + nPasses);
+    std::vector<uint32_t> hTotal(maxRows), hDrop(maxRows), hCounts(4 + nPasses);
     std::vector<unsigned long long> hCross(maxRows);
     const double thr = ex->mseThreshold;
 
@@ -2700,13 +2742,38 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
             HASE_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
             guard.active = true;
             HASE_CUDA(cudaEventRecordWithFlags(b->ev[0], b->stream, cudaEventRecordExternal));
-            // (a1) importance weights, one launch per run of rows of one medium
-            for (size_t r = ch.r0; r < ch.r1;) {
+            // importance weights of the rows [r, e) of one medium (only the flagged ones with a flag array)
+            auto importanceSegment = [&](size_t r, size_t e, const uint8_t* flag) -> hase_status {
                 const uint32_t i = all[r].inst;
-                size_t e = r;
-                while (e < ch.r1 && all[e].inst == i && e - r < 65535) ++e;
                 const BatchMedium& md = media[i];
                 const hase_context* c = md.c;
+                const uint32_t segRows = uint32_t(e - r);
+                ImportanceLaunch il{views[i].m, all[r].sample, slices, md.nW, float(md.meanA), float(md.meanB),
+                                    b->lnw.p + all[r].w, nullptr, flag, uint32_t(r - ch.r0)};
+                const uint32_t G = cp->importanceLayers == 4 ? 4u : uint32_t(kImportanceLayers);
+                const uint32_t threads = slices * ((c->layers + G - 1) / G) * c->T;
+                if (G == 4)
+                    importanceKernel<4><<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
+                else
+                    importanceKernel<kImportanceLayers>
+                        <<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
+                HASE_CUDA(cudaGetLastError());
+                ++kernels;
+                return HASE_OK;
+            };
+            // runs of rows of one medium (at most 65,535 rows each: the grid's y extent)
+            std::vector<std::pair<size_t, size_t>> segments;
+            for (size_t r = ch.r0; r < ch.r1;) {
+                size_t e = r;
+                while (e < ch.r1 && all[e].inst == all[r].inst && e - r < 65535) ++e;
+                segments.emplace_back(r, e);
+                r = e;
+            }
+            // (a1) importance weights or the learned proposal, one launch per run of rows of one medium
+            for (const auto& seg : segments) {
+                const size_t r = seg.first, e = seg.second;
+                const uint32_t i = all[r].inst;
+                const BatchMedium& md = media[i];
                 const uint32_t segRows = uint32_t(e - r);
                 if (net) {
                     ProposalView pv = pviews[i];
@@ -2721,19 +2788,9 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                                                                   alpha);
                     kernels += 2;
                 } else {
-                    ImportanceLaunch il{views[i].m, all[r].sample, slices, md.nW, float(md.meanA), float(md.meanB),
-                                        b->lnw.p + all[r].w, nullptr};
-                    const uint32_t G = cp->importanceLayers == 4 ? 4u : uint32_t(kImportanceLayers);
-                    const uint32_t threads = slices * ((c->layers + G - 1) / G) * c->T;
-                    if (G == 4)
-                        importanceKernel<4><<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
-                    else
-                        importanceKernel<kImportanceLayers>
-                            <<<dim3((threads + 255) / 256, segRows), 256, 0, b->stream>>>(il);
-                    ++kernels;
+                    HASE_TRY(importanceSegment(r, e, nullptr));
                 }
                 HASE_CUDA(cudaGetLastError());
-                r = e;
             }
             HASE_CUDA(cudaEventRecordWithFlags(b->ev[1], b->stream, cudaEventRecordExternal));
             HASE_CUDA(cudaMemsetAsync(b->accSum.p, 0, nRows * sizeof(double), b->stream));
@@ -2741,7 +2798,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
             HASE_CUDA(cudaMemsetAsync(b->accTotal.p, 0, nRows * sizeof(uint32_t), b->stream));
             HASE_CUDA(cudaMemsetAsync(b->accDrop.p, 0, nRows * sizeof(uint32_t), b->stream));
             HASE_CUDA(cudaMemsetAsync(b->accCross.p, 0, nRows * sizeof(unsigned long long), b->stream));
-            HASE_CUDA(cudaMemsetAsync(b->counts.p, 0, (3 + nPasses) * sizeof(unsigned int), b->stream));
+            HASE_CUDA(cudaMemsetAsync(b->counts.p, 0, (4 + nPasses) * sizeof(unsigned int), b->stream));
             iotaCountKernel<<<(nRows + 255) / 256, 256, 0, b->stream>>>(b->activeA.p, nRows, b->counts.p);
             HASE_CUDA(cudaGetLastError());
             ++kernels;
@@ -2795,6 +2852,25 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                 kernels += 3;
                 std::swap(cur, nxt);
                 std::swap(cntCur, cntNxt);
+                if (fallback && k == 0) {
+                    // the plain method judges: rows still active after the first pass whose per-ray
+                    // variance under the learned proposal exceeds the limit restart with the
+                    // importance weights (as hase_calc_phi_ase_learned does, on the device)
+                    const uint32_t g = std::min<uint32_t>((nRows + 255) / 256, uint32_t(8 * b->sms));
+                    HASE_CUDA(cudaMemsetAsync(b->rowFlag.p, 0, nRows, b->stream));
+                    fallbackMarkKernel<<<g, 256, 0, b->stream>>>(cur, cntCur, b->accTotal.p, b->mse.p,
+                                                                 double(fallbackVariance), b->rowFlag.p,
+                                                                 b->counts.p + 3 + nPasses);
+                    HASE_CUDA(cudaGetLastError());
+                    for (const auto& seg : segments) HASE_TRY(importanceSegment(seg.first, seg.second, b->rowFlag.p));
+                    MapLaunch rq{b->lnw.p, 1, 1, cur, 0u, 1u, nullptr, 0u, 0u, 0u, 0u, nullptr, b->q.p, b->Q.p,
+                                 b->offsets.p, b->rows.p, cntCur, b->rowFlag.p};
+                    mapKernel<<<mapGrid, kMapBlock, 0, b->stream>>>(rq);
+                    resetFlaggedKernel<<<g, 256, 0, b->stream>>>(cur, cntCur, b->rowFlag.p, b->accSum.p, b->accSum2.p,
+                                                                 b->accTotal.p, b->accDrop.p, b->accCross.p);
+                    HASE_CUDA(cudaGetLastError());
+                    kernels += 3;
+                }
             }
             // after the last pass cntCur holds the samples above the threshold at maxRays
             if (cntCur != b->counts.p)
@@ -2818,7 +2894,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                                   b->stream));
         HASE_CUDA(cudaMemcpyAsync(hCross.data(), b->accCross.p, nRows * sizeof(unsigned long long),
                                   cudaMemcpyDeviceToHost, b->stream));
-        HASE_CUDA(cudaMemcpyAsync(hCounts.data(), b->counts.p, (3 + nPasses) * sizeof(unsigned int),
+        HASE_CUDA(cudaMemcpyAsync(hCounts.data(), b->counts.p, (4 + nPasses) * sizeof(unsigned int),
                                   cudaMemcpyDeviceToHost, b->stream));
         HASE_CUDA(cudaStreamSynchronize(b->stream));
         float ms = 0.0f;
@@ -2832,6 +2908,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
             if (hCounts[3 + k] > 0) st.passes = std::max(st.passes, k + 1);
         }
         st.unconvergedSamples += hCounts[0];
+        st.fallbackSamples += fallback ? hCounts[3 + nPasses] : 0u;
         st.kernelLaunches += kernels;
         st.graphNodes += uint32_t(nodes);
         // scatter the chunk's rows into the media's results
@@ -2899,15 +2976,17 @@ extern "C" {
 hase_status hase_calc_phi_ase_batch(hase_batch* b, const hase_batch_instance* in, uint32_t count,
                                     const hase_experiment_desc* ex, const hase_compute_desc* cp,
                                     hase_batch_stats* stats) {
-    return batchCore(b, in, count, ex, cp, stats, nullptr, 0.0f);
+    return batchCore(b, in, count, ex, cp, stats, nullptr, 0.0f, 0.0f);
 }
 
 hase_status hase_calc_phi_ase_batch_learned(hase_batch* b, const hase_batch_instance* in, uint32_t count,
                                             const hase_experiment_desc* ex, const hase_compute_desc* cp,
-                                            hase_proposal* net, float mixture, hase_batch_stats* stats) {
+                                            hase_proposal* net, float mixture, float fallbackVariance,
+                                            hase_batch_stats* stats) {
     if (!net) return fail(HASE_INVALID_ARGUMENT, "null network");
     if (!(mixture >= 0.0f) || mixture >= 1.0f) return fail(HASE_INVALID_ARGUMENT, "mixture must be in [0, 1)");
-    return batchCore(b, in, count, ex, cp, stats, net, mixture > 0.0f ? mixture : 0.1f);
+    if (!(fallbackVariance >= 0.0f)) return fail(HASE_INVALID_ARGUMENT, "fallbackVariance must be >= 0");
+    return batchCore(b, in, count, ex, cp, stats, net, mixture > 0.0f ? mixture : 0.1f, fallbackVariance);
 }
 
 }  // extern "C"

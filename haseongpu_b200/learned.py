@@ -41,10 +41,19 @@ class TrainingSet:
     features: np.ndarray  # [rows, 12]
     targets: np.ndarray   # [rows]
     rays: int             # rays logged per group
+    importanceVariance: np.ndarray | None = None  # [groups] per-ray variance of the importance-weighted solves
 
     @property
     def groups(self) -> int:
         return self.offsets.size - 1
+
+    def fallback_limit(self, quantile: float = 1.0) -> float:
+        """The plain method as the judge: a per-ray relative variance limit
+        (``fallbackVariance`` of the learned solve) at the given quantile of
+        what the importance weights reached on the logged samples."""
+        if self.importanceVariance is None or self.importanceVariance.size == 0:
+            return 0.0
+        return float(np.quantile(self.importanceVariance, quantile))
 
 
 def training_set(ctx, fields, *, samples_per_field=32, rays=100_000, monochromatic=True, useReflections=False,
@@ -55,12 +64,13 @@ def training_set(ctx, fields, *, samples_per_field=32, rays=100_000, monochromat
     source (beta = 0) are left out: the proposal gives them no rays."""
     rng = np.random.default_rng(seed)
     S = ctx.mesh.numberOfSamples
-    feats, targs, offs = [], [], [0]
+    feats, targs, offs, var = [], [], [0], []
     for k, beta in enumerate(fields):
         ctx.update_beta(beta)
         first = int(rng.integers(0, max(1, S - samples_per_field)))
-        _, con = ctx.log_contributions(minRays=rays, monochromatic=monochromatic, useReflections=useReflections,
-                                       rngSeed=seed + k, minSample=first, maxSample=first + samples_per_field - 1)
+        res, con = ctx.log_contributions(minRays=rays, monochromatic=monochromatic, useReflections=useReflections,
+                                         rngSeed=seed + k, minSample=first, maxSample=first + samples_per_field - 1)
+        var.append(per_ray_variance(res))
         f = ctx.proposal_features(first, samples_per_field, useReflections=useReflections,
                                   monochromatic=monochromatic)
         for i in range(samples_per_field):
@@ -69,7 +79,7 @@ def training_set(ctx, fields, *, samples_per_field=32, rays=100_000, monochromat
             targs.append(np.maximum(con[i][keep], 0.0))
             offs.append(offs[-1] + int(keep.sum()))
     return TrainingSet(np.asarray(offs, np.uint32), np.concatenate(feats), np.concatenate(targs).astype(np.float32),
-                       rays)
+                       rays, np.concatenate(var))
 
 
 def training_set_media(ctxs, *, samples_per_medium=16, rays=100_000, monochromatic=False, useReflections=False,
@@ -79,13 +89,14 @@ def training_set_media(ctxs, *, samples_per_medium=16, rays=100_000, monochromat
     points solved with the importance weights, contributions logged per
     (slice, prism) as the targets, and the features of the same pairs."""
     rng = np.random.default_rng(seed)
-    feats, targs, offs = [], [], [0]
+    feats, targs, offs, var = [], [], [0], []
     for k, ctx in enumerate(ctxs):
         S = ctx.mesh.numberOfSamples
         n = min(samples_per_medium, S)
         first = int(rng.integers(0, max(1, S - n)))
-        _, con = ctx.log_contributions(minRays=rays, monochromatic=monochromatic, useReflections=useReflections,
-                                       rngSeed=seed + k, minSample=first, maxSample=first + n - 1)
+        res, con = ctx.log_contributions(minRays=rays, monochromatic=monochromatic, useReflections=useReflections,
+                                         rngSeed=seed + k, minSample=first, maxSample=first + n - 1)
+        var.append(per_ray_variance(res))
         f = ctx.proposal_features(first, n, useReflections=useReflections, monochromatic=monochromatic)
         for i in range(n):
             keep = f[i, :, 7] > 0
@@ -93,7 +104,7 @@ def training_set_media(ctxs, *, samples_per_medium=16, rays=100_000, monochromat
             targs.append(np.maximum(con[i][keep], 0.0))
             offs.append(offs[-1] + int(keep.sum()))
     return TrainingSet(np.asarray(offs, np.uint32), np.concatenate(feats), np.concatenate(targs).astype(np.float32),
-                       rays)
+                       rays, np.concatenate(var))
 
 
 def train_proposal(data: TrainingSet, *, steps=3000, groups_per_step=16, learning_rate=2e-3, device=0, seed=1):
@@ -107,7 +118,8 @@ def train_proposal(data: TrainingSet, *, steps=3000, groups_per_step=16, learnin
 
 
 def reorder(data: TrainingSet, order):
-    """The groups of `data` in `order` (training steps take consecutive groups)."""
+    """The groups of `data` in `order` (training steps take consecutive groups);
+    returns (offsets, features, targets)."""
     sizes = np.diff(data.offsets.astype(np.int64))
     idx = np.concatenate([np.arange(data.offsets[g], data.offsets[g + 1]) for g in order])
     off = np.concatenate([[0], np.cumsum(sizes[order])]).astype(np.uint32)

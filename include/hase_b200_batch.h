@@ -64,6 +64,7 @@ typedef struct {
     double captureMilliseconds;         /* host time spent capturing and instantiating graphs */
     double setupMilliseconds;           /* host time before the first graph launch (tables, views, uploads) */
     double hostMilliseconds;            /* host time of the whole call */
+    uint32_t fallbackSamples;           /* learned solve: samples that restarted with the importance weights */
 } hase_batch_stats;
 
 hase_status hase_batch_create(int device, hase_batch** out);
@@ -86,12 +87,16 @@ struct hase_proposal; /* include/hase_b200_proposal.h */
  * device) in place of every medium's importance weights:
  * q = (1 - mixture) softmax(network logits) + mixture (beta V R_j / d^2
  * prior), mixture 0 = 0.1, one network for all media (its features are
- * normalised by each medium's radius and height).  Medium i equals
- * hase_calc_phi_ase_learned on its context with seed rngSeed + i and no
- * fallback; samples do not fall back to the importance weights here. */
+ * normalised by each medium's radius and height).  fallbackVariance > 0:
+ * after the first pass, every sample still above the threshold whose per-ray
+ * relative variance (rays x relative error^2) exceeds it restarts with the
+ * importance weights, on the device (hase_learned_desc.fallbackVariance).
+ * Medium i equals hase_calc_phi_ase_learned on its context with seed
+ * rngSeed + i. */
 hase_status hase_calc_phi_ase_batch_learned(hase_batch* batch, const hase_batch_instance* instances, uint32_t count,
                                             const hase_experiment_desc* experiment, const hase_compute_desc* compute,
-                                            struct hase_proposal* net, float mixture, hase_batch_stats* stats);
+                                            struct hase_proposal* net, float mixture, float fallbackVariance,
+                                            hase_batch_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -142,14 +142,21 @@ def test_learned_batch_equals_single_medium_learned_solves(media):
     items = _ranges(media, n=48)
     kw = dict(KW, maxRays=16000, adaptiveSteps=2)
     with ProposalNet(seed=5) as net, MediaBatch(0) as b:
-        res, st = b.solve(items, net=net, **kw)
-        for i, (ctx, lo, hi) in enumerate(items):
-            solo = ctx.calc_phi_ase_learned(net, minRays=kw["minRays"], maxRays=kw["maxRays"],
-                                            mseThreshold=kw["mseThreshold"], adaptiveSteps=kw["adaptiveSteps"],
-                                            monochromatic=False, rngSeed=kw["rngSeed"] + i, minSample=lo,
-                                            maxSample=hi)
-            assert solo.fallbackSamples == 0
-            _same(res[i], solo)
+        for limit in (0.0, 0.5):  # no fallback; a limit that sends part of the samples back (untrained network)
+            res, st = b.solve(items, net=net, fallbackVariance=limit, **kw)
+            fb = 0
+            for i, (ctx, lo, hi) in enumerate(items):
+                solo = ctx.calc_phi_ase_learned(net, minRays=kw["minRays"], maxRays=kw["maxRays"],
+                                                mseThreshold=kw["mseThreshold"], adaptiveSteps=kw["adaptiveSteps"],
+                                                monochromatic=False, rngSeed=kw["rngSeed"] + i, minSample=lo,
+                                                maxSample=hi, fallbackVariance=limit)
+                fb += solo.fallbackSamples
+                _same(res[i], solo)
+            assert st.fallbackSamples == fb
+            if limit == 0.0:
+                assert fb == 0
+            else:
+                assert 0 < fb <= st.rows
     assert st.kernelLaunches > 0
 
 
