@@ -1193,6 +1193,7 @@ struct hase_context {
     uint64_t betaVersion = 1;       // bumped by every beta upload
     uint64_t featVersion = 0;       // beta version the cached feature view was built for
     double featA = 0.0, featB = 0.0;
+    ProposalView featView{};        // the cached feature view
     DevBuf<uint32_t> rowList;
 
     MeshView view() const {
@@ -1270,17 +1271,13 @@ hase_status buildProposalView(hase_context* c, double A, double B, ProposalView&
 
 // The feature view, rebuilt only when beta or the averaged spectrum changed.
 hase_status cachedProposalView(hase_context* c, double A, double B, ProposalView& V) {
-    static thread_local std::unordered_map<const hase_context*, ProposalView> views;
     if (c->featVersion == c->betaVersion && c->featA == A && c->featB == B) {
-        auto it = views.find(c);
-        if (it != views.end()) {
-            V = it->second;
-            return HASE_OK;
-        }
+        V = c->featView;
+        return HASE_OK;
     }
     HASE_TRY(buildProposalView(c, A, B, V));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
-    views[c] = V;
+    c->featView = V;
     c->featVersion = c->betaVersion;
     c->featA = A;
     c->featB = B;
