@@ -60,7 +60,7 @@ def autotune(ctx, *, firstSample: int, samples: int, rays: int, useReflections: 
             if best is None or t < best[2]:
                 best = (v, rpt, t)
     imp = []
-    for layers in (4, 8):
+    for layers in (2, 4, 8):
         t = min(ctx.calc_phi_ase(minRays=1, maxRays=1, useReflections=useReflections, monochromatic=monochromatic,
                                  nearFieldSampling=nearFieldSampling, rngSeed=3, minSample=firstSample,
                                  maxSample=firstSample + samples - 1, importanceLayers=layers).importanceMilliseconds

@@ -102,7 +102,7 @@ typedef struct {
     uint64_t workspaceBytes;            /* 0 = default device workspace budget */
     uint32_t rayKernelVariant;          /* launch shape of the ray kernel, 0 = default; see
                                            hase_ray_kernel_variant_name (chosen by the autotuner) */
-    uint32_t importanceLayers;          /* prism layers per importance-kernel thread: 0 (= 8), 4 or 8 */
+    uint32_t importanceLayers;          /* prism layers per importance-kernel thread: 0 (= 4), 2, 4 or 8 */
 } hase_compute_desc;
 
 /* Caller-allocated host arrays of (maxSample - minSample + 1) entries; any
