@@ -193,3 +193,26 @@ def test_network_trained_on_the_media_family_lowers_the_variance_on_unseen_media
     net.close()
     for c in ctxs:
         c.close()
+
+
+def test_medium_without_excitation_in_a_batch(media):
+    """A medium with beta = 0 everywhere (no source prism: every ray
+    contributes 0) solves to phi = 0 beside the others, which are unchanged."""
+    from haseongpu_b200 import DeviceMesh, MediaBatch
+    from haseongpu_b200.batch import solve_sequential
+
+    m0 = media[0]
+    dark = DeviceMesh(m0.mesh, np.array([1e-21]), np.array([2e-20]), device=0)
+    dark.update_beta(np.zeros(m0.mesh.numberOfPrisms))
+    try:
+        items = _ranges(media[1:3], n=24) + [(dark, 0, 23)]
+        kw = dict(KW, monochromatic=True, maxRays=8000, adaptiveSteps=1)
+        with MediaBatch(0) as b:
+            res, st = b.solve(items, **kw)
+        seq = solve_sequential(items, **kw)
+        for r, s in zip(res, seq):
+            _same(r, s)
+        assert np.all(res[-1].phiAse == 0) and res[-1].unconvergedSamples == 0
+        assert np.all(res[0].phiAse > 0)
+    finally:
+        dark.close()

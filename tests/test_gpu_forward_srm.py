@@ -102,3 +102,12 @@ def test_phiase_forward_with_prism_reflectivities():
     assert plain.srmStatus == "disabled" and refl.srmStatus in ("converged", "stable")
     assert refl.reflectingFaces == 2 * w.mesh.numberOfTriangles
     assert refl.phiAse.sum() > plain.phiAse.sum()
+
+
+def test_reflections_on_a_mesh_without_reflecting_surfaces():
+    mesh = _ball(0.3)
+    with _ctx(mesh) as ctx:
+        plain = ctx.calc_phi_ase(forwardRayCount=100_000, rngSeed=6)
+        r = ctx.calc_phi_ase(forwardRayCount=100_000, rngSeed=6, useReflections=True)
+    assert r.reflectingFaces == 0 and r.srmStatus == "converged" and r.srmPasses == 0
+    np.testing.assert_array_equal(r.phiAse, plain.phiAse)
