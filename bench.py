@@ -857,8 +857,17 @@ def run_learned(args):
     net, hist = LP.train_proposal(data, steps=3000, device=local)
     t2 = time.perf_counter()
     fields = LP.pump_fields(mesh, args.warmup + args.steps, LP.EVAL_SEED + 7919 * rank)
+    # launch shape of the ray kernel and importance layers: the project's
+    # autotuner on this geometry (untimed), shared by every arm
+    from haseongpu_b200.autotune import autotune
+
+    ctx.update_beta(fields[0])
+    tuned = autotune(ctx, firstSample=0, samples=min(S, 1024), rays=w.minRays, useReflections=False,
+                     monochromatic=True, device=local)
     kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
-              monochromatic=True, minSample=0, maxSample=S - 1)
+              monochromatic=True, minSample=0, maxSample=S - 1, rayKernelVariant=tuned.rayKernelVariant,
+              raysPerThread=tuned.raysPerThread)
+    ikw = dict(importanceLayers=tuned.importanceLayers)
 
     # the plain method judges the learned proposal: a sample whose first-pass
     # per-ray variance exceeds the worst the importance weights reached on the
@@ -869,7 +878,7 @@ def run_learned(args):
         ctx.update_beta(fields[k])
         if kind == "learned":
             return ctx.calc_phi_ase_learned(net, rngSeed=3000 + k, fallbackVariance=fallback, **kw)
-        return ctx.calc_phi_ase(rngSeed=3000 + k, nearFieldSampling=(kind == "nearfield"), **kw)
+        return ctx.calc_phi_ase(rngSeed=3000 + k, nearFieldSampling=(kind == "nearfield"), **kw, **ikw)
 
     def barrier():
         torch.cuda.synchronize()
@@ -960,6 +969,9 @@ def run_learned(args):
                        "levels": mesh.numberOfLevels, "prisms": mesh.numberOfPrisms, "wavelengths": 1,
                        "rays_per_sample": [w.minRays, w.maxRays], "threshold": w.threshold,
                        "adaptive_steps": w.adaptiveSteps, "parallelism": f"independent fields x{world}",
+                       "ray_kernel": {"variant": tuned.name, "rays_per_lane": tuned.raysPerThread,
+                                      "importance_layers": tuned.importanceLayers,
+                                      "autotuned_over": len(tuned.table)},
                        "l2": "flushed (256 MiB write) before every timed step"},
             "time_to_threshold_ms": ms_l / args.steps,
             "plain_is": {"value": solved_all / (ms_p * 1e-3), "unit": "samples/s", "ms_per_step": ms_p / args.steps,

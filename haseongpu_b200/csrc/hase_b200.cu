@@ -469,7 +469,7 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 // POOL: the rows belong to many gain media; the warp copies the view of its
 // item's medium into its shared-memory slot (when the medium changes) and
 // walks from there, and the number of active rows is read on the device.
-template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false>
+template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
     const int lane = threadIdx.x & 31;
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 fetch += uint32_t(nIdle);
             }
             if (active) {
-                const int st = stepRay<kWalkColumns>(m, S.x, S.y, ray, load);
+                const int st = stepRay<COLS>(m, S.x, S.y, ray, load);
                 if (st != kContinue) {
                     crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {
@@ -624,8 +624,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
 }
 
 // Launch shapes of rayKernel the autotuner chooses from: block size, idle
-// lanes that trigger a refill, and the occupancy target (blocks per SM the
-// register budget is fitted to).  Entry 0 is the default.
+// lanes that trigger a refill, the occupancy target (blocks per SM the
+// register budget is fitted to) and the triangle columns a lane walks per
+// step call (32 unless named).  Entry 0 is the default.
 struct RayVariant {
     void (*kernel)(RayLaunch);
     int block;
@@ -640,8 +641,11 @@ const RayVariant kRayVariants[] = {
     {rayKernel<128, 8, 10>, 128, "block128_refill8_occ10"},
     {rayKernel<128, 8, 12>, 128, "block128_refill8_occ12"},
     {rayKernel<512, 8, 2>, 512, "block512_refill8_occ2"},
+    {rayKernel<256, 16, 5, false, false, 64>, 256, "block256_refill16_occ5_cols64"},
+    {rayKernel<512, 8, 2, false, false, 64>, 512, "block512_refill8_occ2_cols64"},
 };
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
+static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
 // The same launch shapes for batched media (same order and names).
 const RayVariant kPoolVariants[] = {
     {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5"},
@@ -652,6 +656,8 @@ const RayVariant kPoolVariants[] = {
     {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10"},
     {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12"},
     {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2"},
+    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64"},
+    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64"},
 };
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
@@ -1200,7 +1206,7 @@ struct hase_context {
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> itemCounter;
     uint32_t persistentBlocks = 0;  // resident rayKernel blocks on the device
-    uint32_t variantBlocks[16] = {};  // the same for every launch shape of kRayVariants
+    uint32_t variantBlocks[16] = {};  // the same for every launch shape of kRayVariants (at most 16)
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
