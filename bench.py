@@ -1029,7 +1029,7 @@ def run_learned(args):
                 "rays_per_sample", "unconverged_samples", "fallback", "per_ray_variance", "training", "importance_batched",
                 "importance_sequential", "plain_is_sequential", "speedup_vs_plain_is_sequential",
                 "speedup_vs_importance_batched", "speedup_batched_vs_sequential", "graph", "e2e", "roofline")}
-            line["north_star_target"] = {
+            line["learned_batched_target"] = {
                 "target": "learned proposal + persistent batching >= 5x less time to every sample's threshold than "
                           "the plain importance-sampled GPU path",
                 "workload": "media64 (config 3), unseen media",
