@@ -293,13 +293,4 @@ struct GlobalLoader {
     }
 };
 
-struct SharedLoader {
-    const float4* tri;  // shared-memory copy
-    __device__ __forceinline__ void operator()(uint32_t t, float4& a, float4& b, float4& c) const {
-        a = tri[3 * t];
-        b = tri[3 * t + 1];
-        c = tri[3 * t + 2];
-    }
-};
-
 }  // namespace hase
