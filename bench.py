@@ -81,6 +81,10 @@ def parse():
     ap.add_argument("--forward-rays", type=int, default=16_000_000, help="source rays per forward step")
     ap.add_argument("--tally", default="auto", choices=["auto", "global", "shared"],
                     help="vertex tallies of the forward kernel")
+    ap.add_argument("--ray-variant", default=None,
+                    help="learned and importance workloads: this ray-kernel launch shape (by name) instead of the "
+                         "autotuner's choice, e.g. to profile one exact kernel")
+    ap.add_argument("--rays-per-lane", type=int, default=16, help="work-item size with --ray-variant")
     return ap.parse_args()
 
 
@@ -220,10 +224,13 @@ def measure_importance(args, local, rank=0, world=1, nested=False):
     flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MiB > 126 MB L2
 
     # launch shape of the ray kernel: the project's autotuner, on this workload (untimed)
-    from haseongpu_b200.autotune import autotune
+    from haseongpu_b200.autotune import autotune, pinned
 
-    tuned = autotune(ctx, firstSample=0, samples=min(B, 128), rays=w.minRays, useReflections=w.useReflections,
-                     monochromatic=w.monochromatic, device=local)
+    if args.ray_variant:
+        tuned = pinned(args.ray_variant, args.rays_per_lane)
+    else:
+        tuned = autotune(ctx, firstSample=0, samples=min(B, 128), rays=w.minRays, useReflections=w.useReflections,
+                         monochromatic=w.monochromatic, device=local)
 
     def run_step(step, beta=None):
         first = ((step * world + rank) * B) % (S - B + 1)
@@ -859,11 +866,14 @@ def run_learned(args):
     fields = LP.pump_fields(mesh, args.warmup + args.steps, LP.EVAL_SEED + 7919 * rank)
     # launch shape of the ray kernel and importance layers: the project's
     # autotuner on this geometry (untimed), shared by every arm
-    from haseongpu_b200.autotune import autotune
+    from haseongpu_b200.autotune import autotune, pinned
 
     ctx.update_beta(fields[0])
-    tuned = autotune(ctx, firstSample=0, samples=min(S, 1024), rays=w.minRays, useReflections=False,
-                     monochromatic=True, device=local)
+    if args.ray_variant:
+        tuned = pinned(args.ray_variant, args.rays_per_lane)
+    else:
+        tuned = autotune(ctx, firstSample=0, samples=min(S, 1024), rays=w.minRays, useReflections=False,
+                         monochromatic=True, device=local)
     kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
               monochromatic=True, minSample=0, maxSample=S - 1, rayKernelVariant=tuned.rayKernelVariant,
               raysPerThread=tuned.raysPerThread)

@@ -39,6 +39,15 @@ def variant_names() -> list[str]:
     return [lib.hase_ray_kernel_variant_name(i).decode() for i in range(lib.hase_ray_kernel_variant_count())]
 
 
+def pinned(name: str, raysPerThread: int = 16, importanceLayers: int = 2) -> TuneResult:
+    """A launch shape chosen by name instead of by a sweep (to time or profile
+    one exact kernel); raises ValueError for a name the library does not have."""
+    names = variant_names()
+    if name not in names:
+        raise ValueError(f"unknown ray-kernel launch shape {name!r}; known: {', '.join(names)}")
+    return TuneResult(names.index(name), raysPerThread, name, 0.0, [], importanceLayers, 0.0)
+
+
 def autotune(ctx, *, firstSample: int, samples: int, rays: int, useReflections: bool, monochromatic: bool,
              nearFieldSampling: bool = True, repeats: int = 2, device: int = 0) -> TuneResult:
     mesh = ctx.mesh

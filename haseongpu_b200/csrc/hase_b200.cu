@@ -469,7 +469,9 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 // POOL: the rows belong to many gain media; the warp copies the view of its
 // item's medium into its shared-memory slot (when the medium changes) and
 // walks from there, and the number of active rows is read on the device.
-template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns>
+// MONO: a monochromatic solve; the walk reads each prism's g from m.gTab.
+template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns,
+          bool MONO = false>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
     const int lane = threadIdx.x & 31;
@@ -591,7 +593,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 fetch += uint32_t(nIdle);
             }
             if (active) {
-                const int st = stepRay<COLS>(m, S.x, S.y, ray, load);
+                const int st = stepRay<COLS, MONO>(m, S.x, S.y, ray, load);
                 if (st != kContinue) {
                     crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {
@@ -626,38 +628,43 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
 // Launch shapes of rayKernel the autotuner chooses from: block size, idle
 // lanes that trigger a refill, the occupancy target (blocks per SM the
 // register budget is fitted to) and the triangle columns a lane walks per
-// step call (32 unless named).  Entry 0 is the default.
+// step call (32 unless named).  Entry 0 is the default.  Single-medium shapes
+// also carry the kernel for monochromatic solves.
 struct RayVariant {
     void (*kernel)(RayLaunch);
     int block;
     const char* name;
+    void (*mono)(RayLaunch);  // the same shape walking the g table (single-medium solves), or null
 };
+#define HASE_RAY_SHAPE(B, R, M, C, NAME) \
+    {rayKernel<B, R, M, false, false, C>, B, NAME, rayKernel<B, R, M, false, false, C, true>}
 const RayVariant kRayVariants[] = {
-    {rayKernel<256, 8, 5>, 256, "block256_refill8_occ5"},
-    {rayKernel<256, 4, 5>, 256, "block256_refill4_occ5"},
-    {rayKernel<256, 16, 5>, 256, "block256_refill16_occ5"},
-    {rayKernel<256, 8, 4>, 256, "block256_refill8_occ4"},
-    {rayKernel<256, 8, 6>, 256, "block256_refill8_occ6"},
-    {rayKernel<128, 8, 10>, 128, "block128_refill8_occ10"},
-    {rayKernel<128, 8, 12>, 128, "block128_refill8_occ12"},
-    {rayKernel<512, 8, 2>, 512, "block512_refill8_occ2"},
-    {rayKernel<256, 16, 5, false, false, 64>, 256, "block256_refill16_occ5_cols64"},
-    {rayKernel<512, 8, 2, false, false, 64>, 512, "block512_refill8_occ2_cols64"},
+    HASE_RAY_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
+    HASE_RAY_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
+    HASE_RAY_SHAPE(256, 16, 5, kWalkColumns, "block256_refill16_occ5"),
+    HASE_RAY_SHAPE(256, 8, 4, kWalkColumns, "block256_refill8_occ4"),
+    HASE_RAY_SHAPE(256, 8, 6, kWalkColumns, "block256_refill8_occ6"),
+    HASE_RAY_SHAPE(128, 8, 10, kWalkColumns, "block128_refill8_occ10"),
+    HASE_RAY_SHAPE(128, 8, 12, kWalkColumns, "block128_refill8_occ12"),
+    HASE_RAY_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
+    HASE_RAY_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
+    HASE_RAY_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
 };
+#undef HASE_RAY_SHAPE
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
 static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
 // The same launch shapes for batched media (same order and names).
 const RayVariant kPoolVariants[] = {
-    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5"},
-    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5"},
-    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5"},
-    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4"},
-    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6"},
-    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10"},
-    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12"},
-    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2"},
-    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64"},
-    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64"},
+    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5", nullptr},
+    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5", nullptr},
+    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5", nullptr},
+    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4", nullptr},
+    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6", nullptr},
+    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10", nullptr},
+    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12", nullptr},
+    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2", nullptr},
+    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64", nullptr},
+    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64", nullptr},
 };
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
@@ -1112,6 +1119,18 @@ __global__ void betaToTablesKernel(const double* beta, const uint8_t* clad, floa
     gainBeta[p] = (clad && clad[p]) ? __int_as_float(0x7fc00000) : b;
 }
 
+// Gain coefficient of every prism for the one wavelength of a monochromatic
+// solve: g = beta A - B (-claddingAbsorption in cladding), evaluated exactly as
+// the general walk evaluates it, so that the monochromatic walk reads g where
+// the general one reads beta.
+__global__ void gainTableKernel(const float* gainBeta, const float2* spec, float cladAbs, uint32_t P, float* g) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const float b = gainBeta[p];
+    const float2 ab = spec[0];
+    g[p] = (b == b) ? fmaf(b, ab.x, -ab.y) : -cladAbs;
+}
+
 // -------------------------------------------------------- host side ----
 struct HostTables {
     std::vector<int4> verts;
@@ -1201,12 +1220,14 @@ struct hase_context {
     DevBuf<int4> verts;
     DevBuf<float2> centroid, points, spec;
     DevBuf<float> gainBeta, srcBeta, reflect;
+    DevBuf<float> gTab;  // g of every prism for a monochromatic solve (rebuilt by each such solve)
     // workspace
     DevBuf<float> lnw;
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> itemCounter;
     uint32_t persistentBlocks = 0;  // resident rayKernel blocks on the device
     uint32_t variantBlocks[16] = {};  // the same for every launch shape of kRayVariants (at most 16)
+    uint32_t variantBlocksMono[16] = {};  // ... and for their monochromatic kernels
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
@@ -1229,6 +1250,7 @@ struct hase_context {
         v.verts = verts.p;
         v.centroid = centroid.p;
         v.gainBeta = gainBeta.p;
+        v.gTab = gTab.p;
         v.srcBeta = srcBeta.p;
         v.points = points.p;
         v.reflect = hasReflect ? reflect.p : nullptr;
@@ -1613,11 +1635,14 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         return fail(HASE_INVALID_ARGUMENT, "rayKernelVariant %u >= %u", cp->rayKernelVariant, kNumRayVariants);
     const uint32_t variant = cp->rayKernelVariant;
     if (c->variantBlocks[variant] == 0) {
-        int perSM = 0, sms = 0;
+        int perSM = 0, perSMMono = 0, sms = 0;
         HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kRayVariants[variant].kernel,
+                                                                kRayVariants[variant].block, 0));
+        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSMMono, kRayVariants[variant].mono,
                                                                 kRayVariants[variant].block, 0));
         HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
         c->variantBlocks[variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
+        c->variantBlocksMono[variant] = uint32_t(std::max(1, perSMMono) * std::max(1, sms));
     }
     if (c->persistentBlocks == 0) {
         int perSM = 0, sms = 0;
@@ -1645,6 +1670,16 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     std::vector<double> hRse;
     std::vector<uint32_t> hTot;
 
+    // a monochromatic solve walks the table of each prism's g (rebuilt here:
+    // beta may have changed since the last solve)
+    const bool monoWalk = nLambda == 1 && !logOut;
+    if (monoWalk) {
+        HASE_CUDA(c->gTab.ensure(c->P));
+        gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, c->spec.p, float(c->cladAbs), c->P,
+                                                                   c->gTab.p);
+        HASE_CUDA(cudaGetLastError());
+        res->kernelLaunches += 1;
+    }
     const MeshView mv = c->view();
     const double C = c->nTot / (4.0 * kPi * c->tau);
     std::vector<float> hPhi(rows);
@@ -1717,11 +1752,12 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             const RayVariant logVariant{rayKernel<kRayBlock, kRefill, kRayMinBlocks, true>, int(kRayBlock), "log"};
             const RayVariant& rv = logOut ? logVariant : kRayVariants[variant];
             const uint64_t totalItems = uint64_t(nActive) * items;
-            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1,
-                                                               uint64_t(c->variantBlocks[variant])));
+            const uint32_t grid = uint32_t(std::min<uint64_t>(
+                totalItems / (rv.block / 32) + 1,
+                uint64_t(monoWalk ? c->variantBlocksMono[variant] : c->variantBlocks[variant])));
             void* rayArgs[] = {&rl};
-            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(rv.kernel), dim3(grid), dim3(rv.block), rayArgs,
-                                       0, c->stream));
+            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(monoWalk ? rv.mono : rv.kernel), dim3(grid),
+                                       dim3(rv.block), rayArgs, 0, c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
             FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,

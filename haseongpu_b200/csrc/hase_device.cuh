@@ -71,6 +71,7 @@ struct MeshView {
     const int4* verts;       // [T] point ids of the triangle's vertices (w unused)
     const float2* centroid;  // [T]
     const float* gainBeta;   // [P] beta, NaN in cladding prisms (walk)
+    const float* gTab;       // [P] g of each prism for the one wavelength of a monochromatic solve, or null
     const float* srcBeta;    // [P] beta (source weight)
     const float2* points;    // [Np]
     const float* reflect;    // [T][2] or nullptr
@@ -107,17 +108,17 @@ __device__ __forceinline__ float reflectFactor(const MeshView& m, uint32_t t, in
 // reflection), so no division or modulo is needed per crossing.
 struct Ray {
     uint32_t t;     // triangle
-    int lu;         // unfolded layer index
-    int phys;       // physical layer of `lu`
+    int phys;       // physical layer of the current unfolded layer
     int pdir;       // +1 / -1
     int forb;       // entry edge (excluded exit), -1 none
     int reflLeft;   // reflections the slice still implies
-    int zoff;       // level-plane offset: exit plane of layer lu is (lu + zoff) h above the image
     int steps;
     float s;        // remaining distance to the image point
     float G;        // accumulated ln(gain), including reflection factors
     float ux, uy, uz;
     float hOverUz;  // h / uz
+    float zl;       // unfolded layer index + level-plane offset: the current layer's exit plane lies zl h
+                    // from the image point along z (a small integer, exact in float)
     float A, B;     // g = beta*A - B
 };
 
@@ -133,7 +134,6 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     const float D = sqrtf(D2);
     const float inv = 1.0f / D;
     r.t = t;
-    r.lu = layer;
     r.phys = layer;
     r.pdir = 1;
     r.forb = -1;
@@ -146,7 +146,7 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.uz = dz * inv;
     r.hOverUz = h / r.uz;
     // moving toward the image: down (dl = -1) when uz > 0, up (dl = +1) otherwise
-    r.zoff = (r.uz > 0.0f ? 0 : 1) - kImg;
+    r.zl = float(layer + (r.uz > 0.0f ? 0 : 1) - kImg);
     r.A = A;
     r.B = B;
     return D2;
@@ -160,13 +160,19 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
 // known, the next triangle's walk record is loaded (into the registers the
 // current record no longer needs) while the current column's level planes are
 // worked through, so its latency is hidden behind them.
-template <int K = 1, typename Loader>
+// The walk is bound by instruction issue, so the level-plane loop is kept
+// short: the step bound is checked once per column (the loop itself ends
+// within 3 x layers crossings: every physical layer step reaches a surface and
+// at most two reflections are allowed), and MONO walks the table of g = beta A
+// - B (m.gTab) instead of evaluating it at every crossing.
+template <int K = 1, bool MONO = false, typename Loader>
 __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
+    const float* gcol = MONO ? m.gTab : m.gainBeta;
     float4 a, b, c;
     load(r.t, a, b, c);
-    // beta of the current prism, issued with the record so that its latency
-    // overlaps the edge tests
-    float gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
+    // beta (MONO: g) of the current prism, issued with the record so that its
+    // latency overlaps the edge tests
+    float gb = __ldg(gcol + r.phys * m.T + r.t);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
         float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
@@ -186,15 +192,17 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
         edge(a.x, a.y, a.z, __float_as_int(c.y), 0);
         edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
         edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
-        const float sEdge = fminf(__fdividef(bn, bd), r.s);
+        // clamped at 0: the comparison sz < sEdge below is reached only with
+        // sz > tolEnd >= 0, where the clamp does not change it
+        const float sEdge = fmaxf(fminf(__fdividef(bn, bd), r.s), 0.0f);
         if (K > 1 && k + 1 < K && bw >= 0) load(uint32_t(bw) >> 2, a, b, c);
         // Level planes crossed before the edge exit: the triangle, and with it
         // sEdge, stays the same, so they cost no edge test.
         const int dl = r.uz > 0.0f ? -1 : 1;
         while (true) {
-            const float sz = fminf(float(r.lu + r.zoff) * r.hOverUz, r.s);
-            const float g = (gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs;
-            const float next = fmaxf(fmaxf(sEdge, sz), 0.0f);
+            const float sz = fminf(r.zl * r.hOverUz, r.s);
+            const float g = MONO ? gb : ((gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs);
+            const float next = fmaxf(sEdge, sz);
             if (next <= m.tolEnd) {
                 r.G = fmaf(g, r.s, r.G);
                 r.s = 0.0f;
@@ -202,7 +210,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             }
             r.G = fmaf(g, r.s - next, r.G);
             r.s = next;
-            if (++r.steps >= kMaxSteps) return kDropped;
+            ++r.steps;
             if (sz < sEdge) break;
             const int cand = r.phys + r.pdir * dl;
             if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
@@ -213,12 +221,13 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             } else {
                 r.phys = cand;
             }
-            r.lu += dl;
-            gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
+            r.zl += float(dl);
+            gb = __ldg(gcol + r.phys * m.T + r.t);
         }
+        if (r.steps >= kMaxSteps) return kDropped;
         r.t = uint32_t(bw) >> 2;
         r.forb = bw & 3;
-        if (K > 1 && k + 1 < K) gb = __ldg(m.gainBeta + r.phys * m.T + r.t);
+        if (K > 1 && k + 1 < K) gb = __ldg(gcol + r.phys * m.T + r.t);
     }
     return kContinue;
 }

@@ -325,3 +325,31 @@ def test_every_ray_kernel_variant_gives_the_same_estimate():
                 r = ctx.calc_phi_ase(minRays=20000, rngSeed=4, maxSample=63, rayKernelVariant=v, raysPerThread=rpt)
                 np.testing.assert_allclose(r.phiAse, ref.phiAse, rtol=1e-6)
                 np.testing.assert_array_equal(r.totalRays, ref.totalRays)
+
+
+@pytest.mark.parametrize("case", ["true_cladding", "disc_poly_reflections"])
+def test_monochromatic_walk_matches_the_general_walk(case):
+    """A monochromatic solve walks a table of each prism's gain coefficient g
+    (built once per solve); the same medium given its wavelength pair twice
+    takes the general walk, which reads beta and evaluates g at every crossing,
+    and draws the same rays.  Both must agree bit for bit, cladding prisms and
+    reflections included."""
+    from haseongpu_b200 import configs
+
+    if case == "true_cladding":
+        mesh = legacy_mesh("true_cladding", claddingAbsorption=5.5)
+        sa, se = legacy_spectrum("true_cladding")
+        kw = dict(minRays=20000, rngSeed=5, maxSample=255)
+    else:
+        w = configs.disc_poly()
+        mesh = w.mesh
+        sa, se = (list(map(float, v[:1])) for v in w.spectra.resampled(True))
+        kw = dict(minRays=20000, rngSeed=5, minSample=1000, maxSample=1127, useReflections=True)
+    with _ctx(mesh, sa, se) as one, _ctx(mesh, sa * 2, se * 2) as two:
+        a = one.calc_phi_ase(monochromatic=True, **kw)
+        b = two.calc_phi_ase(monochromatic=False, **kw)
+    assert a.crossings > 0
+    np.testing.assert_array_equal(a.phiAse, b.phiAse)
+    np.testing.assert_array_equal(a.relativeStandardError, b.relativeStandardError)
+    np.testing.assert_array_equal(a.totalRays, b.totalRays)
+    assert a.crossings == b.crossings
