@@ -134,9 +134,12 @@ struct ImportanceLaunch {
 // and, per line, the level planes and top/bottom reflections inside each
 // triangle: plane k of line l lies at sigma = D2 (k - kImg) / (l + 1/2 - kImg).
 // ln w = ln(beta V / d^2) + Int g dl, Int g dl = (D3 / D2) Int g dsigma.
-template <int G>
+// TAB: g of every prism is read from m.gTab (built for L.A, L.B) instead of
+// being evaluated from beta at every crossing.
+template <int G, bool TAB = false>
 __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     const MeshView& m = L.m;
+    const float* gcol = TAB ? m.gTab : m.gainBeta;
     const uint32_t groups = (m.layers + G - 1) / G;
     const uint32_t perSlice = groups * m.T;
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         // beta of every line's current prism in this triangle, issued together
         float gbv[G];
 #pragma unroll
-        for (int g = 0; g < G; ++g) gbv[g] = ok[g] ? __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk) : 0.0f;
+        for (int g = 0; g < G; ++g) gbv[g] = ok[g] ? __ldg(gcol + size_t(phys[g]) * m.T + tk) : 0.0f;
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             if (!ok[g]) continue;
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
             while (true) {
                 const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg) * invc[g];
                 if (!(sb > sOut)) break;
-                J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sb, J[g]);
+                J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
                 s = sb;
                 const int cand = phys[g] + pdir[g] * dl;
                 if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
@@ -230,12 +233,12 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                     pdir[g] = -pdir[g];
                 } else {
                     phys[g] = cand;
-                    gb = __ldg(m.gainBeta + size_t(phys[g]) * m.T + tk);
+                    gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
                 }
                 ka[g] += dl;
             }
             if (!ok[g]) continue;
-            J[g] = fmaf((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs, s - sOut, J[g]);
+            J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);
         }
         if (!done) {
             tk = uint32_t(bw) >> 2;
@@ -269,15 +272,22 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
 constexpr int kImportanceLayers = 4;
 
 // importanceKernel with G = layers (2, 4 or 8; 0 = the default) prism layers
-// per thread, over `rows` sample rows.
+// per thread, over `rows` sample rows; tab: il.m.gTab holds g for il.A, il.B.
 cudaError_t launchImportance(uint32_t layers, const ImportanceLaunch& il, uint32_t meshLayers, uint32_t T,
-                             uint32_t rows, cudaStream_t stream) {
+                             uint32_t rows, cudaStream_t stream, bool tab = false) {
     const uint32_t G = layers ? layers : uint32_t(kImportanceLayers);
     const uint32_t threads = il.slices * ((meshLayers + G - 1) / G) * T;
     const dim3 grid((threads + 255) / 256, rows);
-    if (G == 2) importanceKernel<2><<<grid, 256, 0, stream>>>(il);
-    else if (G == 8) importanceKernel<8><<<grid, 256, 0, stream>>>(il);
-    else importanceKernel<4><<<grid, 256, 0, stream>>>(il);
+    if (G == 2) {
+        if (tab) importanceKernel<2, true><<<grid, 256, 0, stream>>>(il);
+        else importanceKernel<2><<<grid, 256, 0, stream>>>(il);
+    } else if (G == 8) {
+        if (tab) importanceKernel<8, true><<<grid, 256, 0, stream>>>(il);
+        else importanceKernel<8><<<grid, 256, 0, stream>>>(il);
+    } else {
+        if (tab) importanceKernel<4, true><<<grid, 256, 0, stream>>>(il);
+        else importanceKernel<4><<<grid, 256, 0, stream>>>(il);
+    }
     return cudaGetLastError();
 }
 
@@ -1119,16 +1129,16 @@ __global__ void betaToTablesKernel(const double* beta, const uint8_t* clad, floa
     gainBeta[p] = (clad && clad[p]) ? __int_as_float(0x7fc00000) : b;
 }
 
-// Gain coefficient of every prism for the one wavelength of a monochromatic
-// solve: g = beta A - B (-claddingAbsorption in cladding), evaluated exactly as
-// the general walk evaluates it, so that the monochromatic walk reads g where
-// the general one reads beta.
-__global__ void gainTableKernel(const float* gainBeta, const float2* spec, float cladAbs, uint32_t P, float* g) {
+// Gain coefficient of every prism for one (A, B): g = beta A - B
+// (-claddingAbsorption in cladding), evaluated exactly as the walks evaluate
+// it, so that a walk can read g where it would read beta.  A solve builds it
+// for its spectrally averaged (A, B): the importance walks use those, and so
+// does the ray walk of a monochromatic solve (the mean of one pair is that pair).
+__global__ void gainTableKernel(const float* gainBeta, float A, float B, float cladAbs, uint32_t P, float* g) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
     const float b = gainBeta[p];
-    const float2 ab = spec[0];
-    g[p] = (b == b) ? fmaf(b, ab.x, -ab.y) : -cladAbs;
+    g[p] = (b == b) ? fmaf(b, A, -B) : -cladAbs;
 }
 
 // -------------------------------------------------------- host side ----
@@ -1220,7 +1230,7 @@ struct hase_context {
     DevBuf<int4> verts;
     DevBuf<float2> centroid, points, spec;
     DevBuf<float> gainBeta, srcBeta, reflect;
-    DevBuf<float> gTab;  // g of every prism for a monochromatic solve (rebuilt by each such solve)
+    DevBuf<float> gTab;  // g of every prism for the spectrally averaged (A, B) of the last solve
     // workspace
     DevBuf<float> lnw;
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
@@ -1670,16 +1680,15 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     std::vector<double> hRse;
     std::vector<uint32_t> hTot;
 
-    // a monochromatic solve walks the table of each prism's g (rebuilt here:
-    // beta may have changed since the last solve)
+    // the importance walks, and the ray walk of a monochromatic solve, read
+    // each prism's g from a table (rebuilt here: beta may have changed since
+    // the last solve)
     const bool monoWalk = nLambda == 1 && !logOut;
-    if (monoWalk) {
-        HASE_CUDA(c->gTab.ensure(c->P));
-        gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, c->spec.p, float(c->cladAbs), c->P,
-                                                                   c->gTab.p);
-        HASE_CUDA(cudaGetLastError());
-        res->kernelLaunches += 1;
-    }
+    HASE_CUDA(c->gTab.ensure(c->P));
+    gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, float(meanA), float(meanB),
+                                                               float(c->cladAbs), c->P, c->gTab.p);
+    HASE_CUDA(cudaGetLastError());
+    res->kernelLaunches += 1;
     const MeshView mv = c->view();
     const double C = c->nTot / (4.0 * kPi * c->tau);
     std::vector<float> hPhi(rows);
@@ -1702,7 +1711,7 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
         ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p, nullptr};
         auto launchImportanceRows = [&](uint32_t nLaunchRows) {
-            launchImportance(cp->importanceLayers, il, c->layers, c->T, nLaunchRows, c->stream);
+            launchImportance(cp->importanceLayers, il, c->layers, c->T, nLaunchRows, c->stream, true);
         };
         if (la) {
             pv.firstSample = firstSample;

@@ -71,7 +71,7 @@ struct MeshView {
     const int4* verts;       // [T] point ids of the triangle's vertices (w unused)
     const float2* centroid;  // [T]
     const float* gainBeta;   // [P] beta, NaN in cladding prisms (walk)
-    const float* gTab;       // [P] g of each prism for the one wavelength of a monochromatic solve, or null
+    const float* gTab;       // [P] g of each prism for the solve's averaged (A, B) (a monochromatic solve: its pair)
     const float* srcBeta;    // [P] beta (source weight)
     const float2* points;    // [Np]
     const float* reflect;    // [T][2] or nullptr
