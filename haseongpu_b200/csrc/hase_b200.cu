@@ -569,8 +569,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 if (!active && r < r1) {
                     const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
                     if (LOG) bsel = b;
-                    const uint32_t j = b / m.P, p = b - j * m.P;
-                    const uint32_t t = p % m.T, l = p / m.T;
+                    // reflection slice by subtraction (at most 4), layer by
+                    // an exact multiply-shift: no integer divisions per ray
+                    uint32_t j = 0, p = b;
+                    while (p >= m.P) {
+                        p -= m.P;
+                        ++j;
+                    }
+                    const uint32_t l = prismLayer(m, p), t = p - l * m.T;
                     const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, HASE_SEED_LO, L.seedHi);
                     uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
                     if (k1 + k2 + 1u > (1u << 24)) {
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
                                        unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
                         D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
-                        wf = __ldg(m.srcBeta + p) * alphaL / float(__ldg(q + b));
+                        wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, float(__ldg(q + b)));
                     } else {
                         const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
                         const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
@@ -595,7 +601,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
                         D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j,
                                      ab.x, ab.y, m.h);
-                        wf = __ldg(m.srcBeta + p) * g1.z * m.h / (D2 * float(__ldg(q + b)));
+                        wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * float(__ldg(q + b)));
                     }
                     active = D2 > 0.0f;
                     if (!active) ++dropped;  // start point on the sample point itself
@@ -608,7 +614,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                     crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {
                         finishReflections(m, ray);
-                        const double X = CQ * double(wf) * exp(double(ray.G));
+                        // the ray's gain in FP32 (FP64 only where exp(G)
+                        // nears the FP32 range; the sums stay FP64)
+                        const double eg = ray.G < 80.0f ? double(expf(ray.G)) : exp(double(ray.G));
+                        const double X = CQ * double(wf) * eg;
                         sum += X;
                         sum2 += X * X;
                         if (LOG) atomicAdd(L.logBuf + wBase + bsel, float(X));
@@ -1142,6 +1151,17 @@ __global__ void gainTableKernel(const float* gainBeta, float A, float B, float c
 }
 
 // -------------------------------------------------------- host side ----
+// Multiplier and shift with floor(n / d) = (n * mul) >> shift for every
+// n < 2^31 and 1 <= d < 2^32 (Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, theorem 4.2 with N = 31):
+// l = ceil(log2 d), mul = ceil(2^(31 + l) / d) (< 2^32), shift = 31 + l.
+void invariantDivisor(uint32_t d, uint32_t& mul, uint32_t& shift) {
+    uint32_t l = 0;
+    while ((uint64_t(1) << l) < d) ++l;
+    shift = 31 + l;
+    mul = uint32_t(((uint64_t(1) << shift) + d - 1) / d);
+}
+
 struct HostTables {
     std::vector<int4> verts;
     std::vector<float4> tri, geo;
@@ -1255,6 +1275,7 @@ struct hase_context {
 
     MeshView view() const {
         MeshView v{};
+        invariantDivisor(T, v.divTm, v.divTs);
         v.tri = tri.p;
         v.geo = geo.p;
         v.verts = verts.p;

@@ -76,11 +76,18 @@ struct MeshView {
     const float2* points;    // [Np]
     const float* reflect;    // [T][2] or nullptr
     uint32_t T, layers, P, Np;
+    uint32_t divTm, divTs;   // floor(p / T) = (p * divTm) >> divTs for p < 2^31 (invariantDivisor)
     float h;                 // level spacing
     float cladAbs;           // claddingAbsorption
     float tolEnd;            // |s| below which the target is reached
     float tirCos2[2];        // total internal reflection when uz^2 <= tirCos2[surface]
 };
+
+// Layer of prism index p < 2^31 (p = t + layer T): an exact multiply-shift
+// instead of a 32-bit division by the runtime T.
+__device__ __forceinline__ uint32_t prismLayer(const MeshView& m, uint32_t p) {
+    return uint32_t((uint64_t(p) * m.divTm) >> m.divTs);
+}
 
 // Unfolded integer level of the image of sample level ls for reflection slice.
 __device__ __forceinline__ int imageLevel(int ls, int layers, uint32_t slice) {
@@ -144,7 +151,7 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.ux = dx * inv;
     r.uy = dy * inv;
     r.uz = dz * inv;
-    r.hOverUz = h / r.uz;
+    r.hOverUz = __fdividef(h, r.uz);
     // moving toward the image: down (dl = -1) when uz > 0, up (dl = +1) otherwise
     r.zl = float(layer + (r.uz > 0.0f ? 0 : 1) - kImg);
     r.A = A;
@@ -273,7 +280,10 @@ __device__ __forceinline__ bool nearFieldStart(const MeshView& m, uint32_t t, in
     const float cosA = fminf(fmaxf(fmaf(e1x, e2x, e1y * e2y), -1.0f), 1.0f);
     const float alpha = acosf(cosA);
     const float sinA = sinf(alpha);
-    const float w1 = sinf((1.0f - uAz) * alpha) / sinA, w2 = sinf(uAz * alpha) / sinA;
+    // slerp weights: sin(u a)/sin a and sin((1-u) a)/sin a = cos(u a) - cos a sin(u a)/sin a
+    float su, cu;
+    sincosf(uAz * alpha, &su, &cu);
+    const float w2 = __fdividef(su, sinA), w1 = fmaf(-cosA, w2, cu);
     const float cx = fmaf(w1, e1x, w2 * e2x), cy = fmaf(w1, e1y, w2 * e2y);
     const float se = uEl, ce = sqrtf(fmaxf(0.0f, 1.0f - se * se));
     // edge opposite the vertex: edge (iv + 1) % 3 of the walk record
@@ -282,8 +292,8 @@ __device__ __forceinline__ bool nearFieldStart(const MeshView& m, uint32_t t, in
     const float nx = eo == 0 ? r0.x : (eo == 1 ? r0.w : r1.z);
     const float ny = eo == 0 ? r0.y : (eo == 1 ? r1.x : r1.w);
     const float cc = eo == 0 ? r0.z : (eo == 1 ? r1.y : r2.x);
-    const float lxy = (cc - fmaf(nx, S.x, ny * S.y)) / fmaf(nx, cx, ny * cy);
-    const float L = fminf(lxy / ce, m.h / se);
+    const float lxy = __fdividef(cc - fmaf(nx, S.x, ny * S.y), fmaf(nx, cx, ny * cy));
+    const float L = fminf(__fdividef(lxy, ce), __fdividef(m.h, se));
     const float r = uR * L;
     const float zs = l == kImg ? 1.0f : -1.0f;
     dx = r * ce * cx;
