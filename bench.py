@@ -57,6 +57,9 @@ FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count 
 BYTES_PER_TET_CROSSING = 148       # cell record 128 B + beta 8 B + one vertex tally 8 B + one visit count 4 B
 FWD_TRAFFIC_DISC_POLY = 49128192   # DRAM bytes of one fwdRayKernel launch on the disc_poly Tet4 twin (ncu)
 FP64_LANES_PER_SM = 64
+# DRAM bytes of one learned-solve rayKernel launch on disc_small (5,470 samples x 1e5 rays; ncu): the per-sample
+# ray maps (q, offsets) read once and the per-item partial sums written; the walk tables stay in L1/L2
+RAY_TRAFFIC_LEARNED = 403811328 + 29646848
 
 
 def parse():
@@ -1011,7 +1014,10 @@ def run_learned(args):
             "gpu_launches": a["learned"]["launches"],
             "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel",
                          "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
-                         "traffic": None, "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
+                         "traffic": RAY_TRAFFIC_LEARNED,
+                         "traffic_note": "DRAM bytes per launch (ncu): the per-sample ray maps read once and the "
+                                         "per-item partial sums; the walk tables stay in L1 (99 % hits) and L2",
+                         "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
                          "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
             "proposal_roofline": {"bound": "xu", "kernel": "proposalKernel",
                                   "achieved": rows / (a["learned"]["proposal_ms"] * 1e-3),
