@@ -30,7 +30,7 @@ constexpr int kFeat = HASE_PROPOSAL_FEATURES;
 constexpr int kHid = HASE_PROPOSAL_HIDDEN;
 constexpr int kIn = 16;     // padded input width: one K = 16 MMA
 constexpr int kTile = 128;  // rows per tile (MMA M)
-constexpr int kMlpBlocksPerSM = 3;  // inference CTAs per SM (shared memory ~57 KB, 64 TMEM columns each)
+constexpr int kMlpBlocksPerSM = 4;  // inference CTAs per SM (shared memory ~41 KB, 64 TMEM columns, <= 128 registers)
 constexpr uint32_t kSpinLimit = 1u << 22;  // mbarrier polls before the kernel gives up
 
 // parameter offsets in the FP32 master vector
@@ -53,8 +53,10 @@ constexpr uint32_t kA0Bytes = kTile * kIn * 2;
 constexpr uint32_t kA1Bytes = kTile * kHid * 2;
 constexpr int kVecFloats = 4 * kHid + 1;          // b1 b2 b3 w4 b4
 
-// Inference: forward weight images, one activation buffer per layer input,
-// 64 TMEM columns (one accumulator reused by the three layers).
+// Inference: forward weight images, the feature rows and one activation buffer
+// shared by the inputs of layers 2 and 3 (the layer-2 epilogue writes it only
+// after the MMAs that read it have completed), 64 TMEM columns (one
+// accumulator reused by the three layers).
 struct SmemMap {
     static constexpr uint32_t wBytes = kWFwdBytes;
     static constexpr uint32_t tmemCols = 64;
@@ -63,8 +65,8 @@ struct SmemMap {
     static constexpr uint32_t w3 = w2 + kW2Bytes;
     static constexpr uint32_t a0 = w3 + kW2Bytes;
     static constexpr uint32_t a1 = a0 + kA0Bytes;
-    static constexpr uint32_t a2 = a1 + kA1Bytes;
-    static constexpr uint32_t vec = a2 + kA1Bytes;
+    static constexpr uint32_t a2 = a1;
+    static constexpr uint32_t vec = a1 + kA1Bytes;
     static constexpr uint32_t bar = (vec + kVecFloats * 4 + 15) & ~15u;
     static constexpr uint32_t tslot = bar + 8;
     static constexpr uint32_t bytes = tslot + 8;
