@@ -30,7 +30,7 @@ constexpr int kFeat = HASE_PROPOSAL_FEATURES;
 constexpr int kHid = HASE_PROPOSAL_HIDDEN;
 constexpr int kIn = 16;     // padded input width: one K = 16 MMA
 constexpr int kTile = 128;  // rows per tile (MMA M)
-constexpr int kMlpBlocksPerSM = 4;  // inference CTAs per SM (shared memory ~41 KB, 64 TMEM columns, <= 128 registers)
+constexpr int kMlpBlocksPerSM = 5;  // inference CTAs per SM (shared memory ~41 KB, 64 TMEM columns, <= 102 registers)
 constexpr uint32_t kSpinLimit = 1u << 22;  // mbarrier polls before the kernel gives up
 
 // parameter offsets in the FP32 master vector
@@ -207,6 +207,20 @@ __device__ __forceinline__ void loadRow(const Tile& T, uint32_t col, float (&acc
     }
 }
 
+// Reads N (a multiple of 16) accumulator columns of this thread's row from
+// TMEM column `col`.
+template <int N>
+__device__ __forceinline__ void loadCols(const Tile& T, uint32_t col, float (&acc)[N]) {
+    const uint32_t lane0 = (threadIdx.x & ~31u) << 16;
+#pragma unroll
+    for (int q = 0; q < N / 16; ++q) {
+        uint32_t r[16];
+        tmemLd16(T.tmem + lane0 + col + uint32_t(16 * q), r);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[16 * q + j] = __uint_as_float(r[j]);
+    }
+}
+
 // Issues the MMAs of one product [128 x K] x [64 x K]^T (K = kIn or kHid)
 // into TMEM column `col` from thread 0 and commits them to the mbarrier.
 __device__ __forceinline__ void issueLayer(Tile& T, uint32_t aOff, uint32_t wOff, uint32_t K, uint32_t col,
@@ -237,20 +251,27 @@ __device__ __forceinline__ void runLayer(Tile& T, uint32_t aOff, uint32_t wOff, 
 
 // Bias + SiLU of the accumulator row, stored as bf16 row `threadIdx.x` of the
 // next layer's A operand (K = 64).
+// The row is processed in two halves of 32 columns, which keeps the register
+// count low enough for the inference occupancy target.
 template <bool FAST = false>
 __device__ __forceinline__ void epilogueToSmem(Tile& T, uint32_t col, const float* bias, uint32_t outOff) {
-    float acc[kHid];
-    loadRow(T, col, acc);
     const uint32_t t = threadIdx.x;
     uint8_t* out = T.base + outOff + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
 #pragma unroll
-    for (int c = 0; c < kHid / 8; ++c) {
-        uint4 v;
-        v.x = packBf16(act<FAST>(acc[8 * c + 0] + bias[8 * c + 0]), act<FAST>(acc[8 * c + 1] + bias[8 * c + 1]));
-        v.y = packBf16(act<FAST>(acc[8 * c + 2] + bias[8 * c + 2]), act<FAST>(acc[8 * c + 3] + bias[8 * c + 3]));
-        v.z = packBf16(act<FAST>(acc[8 * c + 4] + bias[8 * c + 4]), act<FAST>(acc[8 * c + 5] + bias[8 * c + 5]));
-        v.w = packBf16(act<FAST>(acc[8 * c + 6] + bias[8 * c + 6]), act<FAST>(acc[8 * c + 7] + bias[8 * c + 7]));
-        *reinterpret_cast<uint4*>(out + c * 128u) = v;
+    for (int h = 0; h < 2; ++h) {
+        constexpr int kHalf = kHid / 2;
+        float acc[kHalf];
+        loadCols<kHalf>(T, col + uint32_t(h * kHalf), acc);
+        const float* b = bias + h * kHalf;
+#pragma unroll
+        for (int c = 0; c < kHalf / 8; ++c) {
+            uint4 v;
+            v.x = packBf16(act<FAST>(acc[8 * c + 0] + b[8 * c + 0]), act<FAST>(acc[8 * c + 1] + b[8 * c + 1]));
+            v.y = packBf16(act<FAST>(acc[8 * c + 2] + b[8 * c + 2]), act<FAST>(acc[8 * c + 3] + b[8 * c + 3]));
+            v.z = packBf16(act<FAST>(acc[8 * c + 4] + b[8 * c + 4]), act<FAST>(acc[8 * c + 5] + b[8 * c + 5]));
+            v.w = packBf16(act<FAST>(acc[8 * c + 6] + b[8 * c + 6]), act<FAST>(acc[8 * c + 7] + b[8 * c + 7]));
+            *reinterpret_cast<uint4*>(out + uint32_t(h * kHalf / 8 + c) * 128u) = v;
+        }
     }
     fenceBeforeSync();
     fenceProxyAsync();
@@ -286,13 +307,18 @@ __device__ __forceinline__ float mlpTile(Tile& T) {
     runLayer(T, SmemMap::a1, SmemMap::w2, kHid, 0, SmemMap::bar);
     epilogueToSmem<FAST>(T, 0, vec + kHid, SmemMap::a2);
     runLayer(T, SmemMap::a2, SmemMap::w3, kHid, 0, SmemMap::bar);
-    float acc[kHid];
-    loadRow(T, 0, acc);
     const float* b3 = vec + 2 * kHid;
     const float* w4 = vec + 3 * kHid;
     float logit = vec[4 * kHid];
 #pragma unroll
-    for (int n = 0; n < kHid; ++n) logit = fmaf(act<FAST>(acc[n] + b3[n]), w4[n], logit);
+    for (int h = 0; h < 2; ++h) {
+        constexpr int kHalf = kHid / 2;
+        float acc[kHalf];
+        loadCols<kHalf>(T, uint32_t(h * kHalf), acc);
+#pragma unroll
+        for (int n = 0; n < kHalf; ++n)
+            logit = fmaf(act<FAST>(acc[n] + b3[h * kHalf + n]), w4[h * kHalf + n], logit);
+    }
     fenceBeforeSync();
     __syncthreads();  // TMEM reads done before the next tile's MMA overwrites D
     return logit;
