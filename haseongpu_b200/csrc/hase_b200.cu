@@ -479,9 +479,9 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 // POOL: the rows belong to many gain media; the warp copies the view of its
 // item's medium into its shared-memory slot (when the medium changes) and
 // walks from there, and the number of active rows is read on the device.
-// MONO: a monochromatic solve; the walk reads each prism's g from m.gTab.
+// WALK: how the walk obtains each prism's g (WalkMode).
 template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns,
-          bool MONO = false>
+          int WALK = kWalkBeta>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
     const int lane = threadIdx.x & 31;
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 fetch += uint32_t(nIdle);
             }
             if (active) {
-                const int st = stepRay<COLS, MONO>(m, S.x, S.y, ray, load);
+                const int st = stepRay<COLS, WALK>(m, S.x, S.y, ray, load);
                 if (st != kContinue) {
                     crossings += uint32_t(ray.steps) + 1u;
                     if (st == kDone) {
@@ -648,15 +648,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
 // lanes that trigger a refill, the occupancy target (blocks per SM the
 // register budget is fitted to) and the triangle columns a lane walks per
 // step call (32 unless named).  Entry 0 is the default.  Single-medium shapes
-// also carry the kernel for monochromatic solves.
+// also carry the kernels of the other walk modes.
 struct RayVariant {
     void (*kernel)(RayLaunch);
     int block;
     const char* name;
-    void (*mono)(RayLaunch);  // the same shape walking the g table (single-medium solves), or null
+    void (*mono)(RayLaunch);     // the same shape walking the g table (monochromatic single-medium solves), or null
+    void (*noClad)(RayLaunch);   // the same shape for a medium without cladding prisms, or null
 };
-#define HASE_RAY_SHAPE(B, R, M, C, NAME) \
-    {rayKernel<B, R, M, false, false, C>, B, NAME, rayKernel<B, R, M, false, false, C, true>}
+#define HASE_RAY_SHAPE(B, R, M, C, NAME)                                                      \
+    {rayKernel<B, R, M, false, false, C>, B, NAME, rayKernel<B, R, M, false, false, C, kWalkTable>, \
+     rayKernel<B, R, M, false, false, C, kWalkBetaNoClad>}
 const RayVariant kRayVariants[] = {
     HASE_RAY_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
     HASE_RAY_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
@@ -674,16 +676,16 @@ constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[
 static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
 // The same launch shapes for batched media (same order and names).
 const RayVariant kPoolVariants[] = {
-    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5", nullptr},
-    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5", nullptr},
-    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5", nullptr},
-    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4", nullptr},
-    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6", nullptr},
-    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10", nullptr},
-    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12", nullptr},
-    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2", nullptr},
-    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64", nullptr},
-    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64", nullptr},
+    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5", nullptr, nullptr},
+    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5", nullptr, nullptr},
+    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5", nullptr, nullptr},
+    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4", nullptr, nullptr},
+    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6", nullptr, nullptr},
+    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10", nullptr, nullptr},
+    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12", nullptr, nullptr},
+    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2", nullptr, nullptr},
+    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64", nullptr, nullptr},
+    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64", nullptr, nullptr},
 };
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
@@ -1243,6 +1245,7 @@ struct hase_context {
     double h = 0, nTot = 0, tau = 0, cladAbs = 0, extent = 0;
     uint32_t cladNumber = 0;
     std::vector<uint32_t> cladTypes;
+    bool hasClad = false;  // some prism is cladding
     std::vector<double> betaCells, sigmaA, sigmaE;
     bool hasReflect = false;
     float tirCos2[2] = {-1.0f, -1.0f};
@@ -1256,8 +1259,7 @@ struct hase_context {
     DevBuf<uint32_t> q, offsets, activeA, activeB, counter, accTotal, accDrop, pDrop;
     DevBuf<unsigned int> itemCounter;
     uint32_t persistentBlocks = 0;  // resident rayKernel blocks on the device
-    uint32_t variantBlocks[16] = {};  // the same for every launch shape of kRayVariants (at most 16)
-    uint32_t variantBlocksMono[16] = {};  // ... and for their monochromatic kernels
+    uint32_t variantBlocks[3][16] = {};  // the same for every walk mode x launch shape of kRayVariants (at most 16)
     DevBuf<unsigned long long> Q, accCross, pCross;
     DevBuf<double> accSum, accSum2, pSum, pSum2, mse;
     DevBuf<float> phi;
@@ -1510,6 +1512,7 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
     c->cladAbs = d->claddingAbsorption;
     c->cladNumber = d->claddingNumber;
     if (d->claddingCellTypes) c->cladTypes.assign(d->claddingCellTypes, d->claddingCellTypes + c->T);
+    c->hasClad = std::find(c->cladTypes.begin(), c->cladTypes.end(), c->cladNumber) != c->cladTypes.end();
     if (d->betaCells) c->betaCells.assign(d->betaCells, d->betaCells + size_t(c->Np) * c->L);
     c->sigmaA.assign(sp->sigmaA, sp->sigmaA + sp->numberOfWavelengths);
     c->sigmaE.assign(sp->sigmaE, sp->sigmaE + sp->numberOfWavelengths);
@@ -1665,15 +1668,16 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     if (cp->rayKernelVariant >= kNumRayVariants)
         return fail(HASE_INVALID_ARGUMENT, "rayKernelVariant %u >= %u", cp->rayKernelVariant, kNumRayVariants);
     const uint32_t variant = cp->rayKernelVariant;
-    if (c->variantBlocks[variant] == 0) {
-        int perSM = 0, perSMMono = 0, sms = 0;
-        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kRayVariants[variant].kernel,
-                                                                kRayVariants[variant].block, 0));
-        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSMMono, kRayVariants[variant].mono,
-                                                                kRayVariants[variant].block, 0));
+    if (c->variantBlocks[0][variant] == 0) {
+        const RayVariant& v = kRayVariants[variant];
+        int sms = 0;
         HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-        c->variantBlocks[variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
-        c->variantBlocksMono[variant] = uint32_t(std::max(1, perSMMono) * std::max(1, sms));
+        void (*const modes[3])(RayLaunch) = {v.kernel, v.mono, v.noClad};
+        for (int w = 0; w < 3; ++w) {
+            int perSM = 0;
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, modes[w], v.block, 0));
+            c->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
+        }
     }
     if (c->persistentBlocks == 0) {
         int perSM = 0, sms = 0;
@@ -1704,7 +1708,8 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     // the importance walks, and the ray walk of a monochromatic solve, read
     // each prism's g from a table (rebuilt here: beta may have changed since
     // the last solve)
-    const bool monoWalk = nLambda == 1 && !logOut;
+    // walk mode of the ray launches (the logging launches keep the general walk)
+    const int walk = logOut ? kWalkBeta : (nLambda == 1 ? kWalkTable : (c->hasClad ? kWalkBeta : kWalkBetaNoClad));
     HASE_CUDA(c->gTab.ensure(c->P));
     gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, float(meanA), float(meanB),
                                                                float(c->cladAbs), c->P, c->gTab.p);
@@ -1782,12 +1787,12 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             const RayVariant logVariant{rayKernel<kRayBlock, kRefill, kRayMinBlocks, true>, int(kRayBlock), "log"};
             const RayVariant& rv = logOut ? logVariant : kRayVariants[variant];
             const uint64_t totalItems = uint64_t(nActive) * items;
-            const uint32_t grid = uint32_t(std::min<uint64_t>(
-                totalItems / (rv.block / 32) + 1,
-                uint64_t(monoWalk ? c->variantBlocksMono[variant] : c->variantBlocks[variant])));
+            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1,
+                                                               uint64_t(c->variantBlocks[walk][variant])));
+            void (*const kern)(RayLaunch) = walk == kWalkTable ? rv.mono : (walk == kWalkBetaNoClad ? rv.noClad : rv.kernel);
             void* rayArgs[] = {&rl};
-            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(monoWalk ? rv.mono : rv.kernel), dim3(grid),
-                                       dim3(rv.block), rayArgs, 0, c->stream));
+            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs, 0,
+                                       c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
             FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,

@@ -131,6 +131,13 @@ struct Ray {
 
 enum StepResult { kContinue = 0, kDone = 1, kDropped = 2 };
 
+// How a walk obtains the gain coefficient g of the current prism.
+enum WalkMode {
+    kWalkBeta = 0,         // beta from m.gainBeta, g = beta A - B, cladding (NaN beta): g = -claddingAbsorption
+    kWalkTable = 1,        // g from m.gTab (a monochromatic solve: the table is built for its pair)
+    kWalkBetaNoClad = 2,   // as kWalkBeta for a medium without cladding prisms (beta is never NaN)
+};
+
 // Initialise a ray from the start point, given as its offset (dx, dy, dz)
 // from the image point (Sx, Sy, kImg*h), in physical layer `layer`.
 // Returns |start - image|^2.
@@ -170,15 +177,15 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
 // The walk is bound by instruction issue, so the level-plane loop is kept
 // short: the step bound is checked once per column (the loop itself ends
 // within 3 x layers crossings: every physical layer step reaches a surface and
-// at most two reflections are allowed), and MONO walks the table of g = beta A
-// - B (m.gTab) instead of evaluating it at every crossing.
-template <int K = 1, bool MONO = false, typename Loader>
+// at most two reflections are allowed), and kWalkTable walks the table of g = beta A
+// - B (m.gTab) instead of evaluating it at every crossing (WalkMode).
+template <int K = 1, int WALK = kWalkBeta, typename Loader>
 __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ray& r, Loader&& load) {
-    const float* gcol = MONO ? m.gTab : m.gainBeta;
+    const float* gcol = WALK == kWalkTable ? m.gTab : m.gainBeta;
     float4 a, b, c;
     load(r.t, a, b, c);
-    // beta (MONO: g) of the current prism, issued with the record so that its
-    // latency overlaps the edge tests
+    // beta (kWalkTable: g) of the current prism, issued with the record so
+    // that its latency overlaps the edge tests
     float gb = __ldg(gcol + r.phys * m.T + r.t);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
@@ -208,7 +215,9 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
         const int dl = r.uz > 0.0f ? -1 : 1;
         while (true) {
             const float sz = fminf(r.zl * r.hOverUz, r.s);
-            const float g = MONO ? gb : ((gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs);
+            const float g = WALK == kWalkTable        ? gb
+                            : WALK == kWalkBetaNoClad ? fmaf(gb, r.A, -r.B)
+                                                      : ((gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs);
             const float next = fmaxf(sEdge, sz);
             if (next <= m.tolEnd) {
                 r.G = fmaf(g, r.s, r.G);
