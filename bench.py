@@ -592,7 +592,7 @@ def measure_media(args, local, steps, warmup):
     for c in trainers:
         c.close()
     batch = MediaBatch(local)
-    tune = autotune_batch(batch, items, rays=20_000, workspaceBytes=ws)
+    tune = autotune_batch(batch, items, rays=100_000, repeats=3, workspaceBytes=ws)
     kw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, adaptiveSteps=w.adaptiveSteps,
               monochromatic=False, workspaceBytes=ws, rayKernelVariant=tune.rayKernelVariant,
               raysPerThread=tune.raysPerThread)

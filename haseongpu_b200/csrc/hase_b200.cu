@@ -674,19 +674,23 @@ const RayVariant kRayVariants[] = {
 #undef HASE_RAY_SHAPE
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
 static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
-// The same launch shapes for batched media (same order and names).
+// The same launch shapes for batched media (same order and names): the
+// general walk, and the walk for batches without cladding prisms.
+#define HASE_POOL_SHAPE(B, R, M, C, NAME) \
+    {rayKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayKernel<B, R, M, false, true, C, kWalkBetaNoClad>}
 const RayVariant kPoolVariants[] = {
-    {rayKernel<256, 8, 5, false, true>, 256, "block256_refill8_occ5", nullptr, nullptr},
-    {rayKernel<256, 4, 5, false, true>, 256, "block256_refill4_occ5", nullptr, nullptr},
-    {rayKernel<256, 16, 5, false, true>, 256, "block256_refill16_occ5", nullptr, nullptr},
-    {rayKernel<256, 8, 4, false, true>, 256, "block256_refill8_occ4", nullptr, nullptr},
-    {rayKernel<256, 8, 6, false, true>, 256, "block256_refill8_occ6", nullptr, nullptr},
-    {rayKernel<128, 8, 10, false, true>, 128, "block128_refill8_occ10", nullptr, nullptr},
-    {rayKernel<128, 8, 12, false, true>, 128, "block128_refill8_occ12", nullptr, nullptr},
-    {rayKernel<512, 8, 2, false, true>, 512, "block512_refill8_occ2", nullptr, nullptr},
-    {rayKernel<256, 16, 5, false, true, 64>, 256, "block256_refill16_occ5_cols64", nullptr, nullptr},
-    {rayKernel<512, 8, 2, false, true, 64>, 512, "block512_refill8_occ2_cols64", nullptr, nullptr},
+    HASE_POOL_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
+    HASE_POOL_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
+    HASE_POOL_SHAPE(256, 16, 5, kWalkColumns, "block256_refill16_occ5"),
+    HASE_POOL_SHAPE(256, 8, 4, kWalkColumns, "block256_refill8_occ4"),
+    HASE_POOL_SHAPE(256, 8, 6, kWalkColumns, "block256_refill8_occ6"),
+    HASE_POOL_SHAPE(128, 8, 10, kWalkColumns, "block128_refill8_occ10"),
+    HASE_POOL_SHAPE(128, 8, 12, kWalkColumns, "block128_refill8_occ12"),
+    HASE_POOL_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
+    HASE_POOL_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
+    HASE_POOL_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
 };
+#undef HASE_POOL_SHAPE
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
 // ------------------------------------------------ (c)+(d) finalise ----
@@ -2528,7 +2532,7 @@ struct hase_batch {
     DevBuf<float2> spec;
     DevBuf<InstanceView> inst;
     DevBuf<RowInfo> rows;
-    uint32_t variantBlocks[16] = {};
+    uint32_t variantBlocks[2][16] = {};  // general and no-cladding walks x launch shapes
     int sms = 0;
 };
 
@@ -2676,11 +2680,17 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
     const uint32_t slices = ex->useReflections ? 5u : 1u;
     const uint32_t variant = cp->rayKernelVariant;
     const RayVariant& rv = kPoolVariants[variant];
-    if (b->variantBlocks[variant] == 0) {
-        int perSM = 0;
-        HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, rv.kernel, rv.block, 0));
-        b->variantBlocks[variant] = uint32_t(std::max(1, perSM) * std::max(1, b->sms));
+    if (b->variantBlocks[0][variant] == 0) {
+        for (int w = 0; w < 2; ++w) {
+            int perSM = 0;
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, w ? rv.noClad : rv.kernel, rv.block, 0));
+            b->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, b->sms));
+        }
     }
+    // a batch without cladding prisms walks without the per-crossing cladding test
+    bool anyClad = false;
+    for (const BatchMedium& md : media) anyClad = anyClad || md.c->hasClad;
+    const int noClad = anyClad ? 0 : 1;
 
     // the pass schedule (shared by all media)
     struct Pass {
@@ -2918,10 +2928,10 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                 rl.rows = b->rows.p;
                 rl.count = cntCur;
                 const uint32_t grid = uint32_t(std::min<uint64_t>(uint64_t(nRows) * ps.items / (rv.block / 32) + 1,
-                                                                   uint64_t(b->variantBlocks[variant])));
+                                                                   uint64_t(b->variantBlocks[noClad][variant])));
                 void* rayArgs[] = {&rl};
-                HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(rv.kernel), dim3(grid), dim3(rv.block),
-                                           rayArgs, 0, b->stream));
+                HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(noClad ? rv.noClad : rv.kernel), dim3(grid),
+                                           dim3(rv.block), rayArgs, 0, b->stream));
                 HASE_CUDA(cudaEventRecordWithFlags(b->ev[4 + 2 * k], b->stream, cudaEventRecordExternal));
                 HASE_CUDA(cudaMemsetAsync(cntNxt, 0, sizeof(unsigned int), b->stream));
                 FinalizeLaunch fl{cur, 0u, ps.items, ps.M, ps.last ? 1 : 0, thr, b->pSum.p, b->pSum2.p, b->pDrop.p,
