@@ -900,6 +900,7 @@ struct ProposalView {
     float x0, y0, invCell;  // grid origin and 1 / cell size
     float lnRb, lnRt;       // mean ln reflectivity of the bottom and top surfaces
     float R, H;             // mesh radius and height
+    float invR, invH, invTwoH, invh;  // 1/R, 1/H, 1/(2H), 1/(level spacing)
     float lnVref;           // ln(mean prism volume / R^2)
     float lnSigmaRatio;     // ln(sigma_e / sigma_a) of the averaged spectrum
     uint32_t firstSample, nW;
@@ -912,10 +913,17 @@ __device__ __forceinline__ float sliceLnReflect(const ProposalView& V, uint32_t 
 // Returns the prior beta V R_j / d^2 (0 without a source) and fills f.
 __device__ __forceinline__ float pairFeatures(const ProposalView& V, uint32_t sample, uint32_t jp, float (&f)[kFeat]) {
     const MeshView& m = V.m;
-    const uint32_t j = jp / m.P, p = jp - j * m.P;
-    const uint32_t t = p % m.T, l = p / m.T;
-    const float2 S = __ldg(m.points + sample % m.Np);
-    const int ls = int(sample / m.Np);
+    // (slice, prism) and (triangle, layer), sample point and level: no
+    // integer divisions (slices by subtraction, the rest by multiply-shift)
+    uint32_t j = 0, p = jp;
+    while (p >= m.P) {
+        p -= m.P;
+        ++j;
+    }
+    const uint32_t l = prismLayer(m, p), t = p - l * m.T;
+    const uint32_t lsU = sampleLevel(m, sample);
+    const float2 S = __ldg(m.points + (sample - lsU * m.Np));
+    const int ls = int(lsU);
     const float zs = float(ls) * m.h;
     const float zi = float(imageLevel(ls, int(m.layers), j)) * m.h;
     const float2 c = __ldg(m.centroid + t);
@@ -933,22 +941,22 @@ __device__ __forceinline__ float pairFeatures(const ProposalView& V, uint32_t sa
         const float x = S.x + a * dx, y = S.y + a * dy;
         // fold the unfolded height into [0, H]: period 2H, mirrored halves
         float z = zi + a * dz;
-        z -= twoH * floorf(z / twoH);
+        z -= twoH * floorf(z * V.invTwoH);
         if (z > V.H) z = twoH - z;
-        const int ly = min(max(int(z / m.h), 0), int(m.layers) - 1);
+        const int ly = min(max(int(z * V.invh), 0), int(m.layers) - 1);
         const int ix = min(max(int((x - V.x0) * V.invCell), 0), int(V.gx) - 1);
         const int iy = min(max(int((y - V.y0) * V.invCell), 0), int(V.gy) - 1);
         lng += __ldg(V.grid + (size_t(ly) * V.gy + iy) * V.gx + ix);
     }
     const float lnR = sliceLnReflect(V, j);
     lng = lng * 0.125f * d + lnR;
-    f[0] = S.x / V.R;
-    f[1] = S.y / V.R;
-    f[2] = zs / V.H;
-    f[3] = dx / V.R;
-    f[4] = dy / V.R;
-    f[5] = dz / V.H;
-    f[6] = logf(d / V.R);
+    f[0] = S.x * V.invR;
+    f[1] = S.y * V.invR;
+    f[2] = zs * V.invH;
+    f[3] = dx * V.invR;
+    f[4] = dy * V.invR;
+    f[5] = dz * V.invH;
+    f[6] = logf(d * V.invR);
     f[7] = beta;
     f[8] = lng;
     f[9] = beta > 0.0f ? logf(beta * vol / (d * d)) - V.lnVref : 0.0f;
@@ -975,11 +983,17 @@ __global__ void __launch_bounds__(kTile, kMlpBlocksPerSM) proposalKernel(const P
     tileBegin<SmemMap>(T, dynSmem, P.wimg, P.vec);
     const uint64_t total = uint64_t(P.rows) * P.V.nW;
     const uint64_t tiles = (total + kTile - 1) / kTile;
+    // (row, column) of this thread's pair, advanced by the grid stride without
+    // a division per tile
+    const uint64_t gr0 = uint64_t(blockIdx.x) * kTile + threadIdx.x;
+    const uint64_t stride = uint64_t(gridDim.x) * kTile;
+    uint32_t row = uint32_t(gr0 / P.V.nW), col = uint32_t(gr0 % P.V.nW);
+    const uint32_t dRow = uint32_t(stride / P.V.nW), dCol = uint32_t(stride % P.V.nW);
     for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint64_t gr = tile * kTile + threadIdx.x;
         float f[kFeat];
         if (gr < total) {
-            P.prior[gr] = pairFeatures(P.V, P.V.firstSample + uint32_t(gr / P.V.nW), uint32_t(gr % P.V.nW), f);
+            P.prior[gr] = pairFeatures(P.V, P.V.firstSample + row, col, f);
         } else {
 #pragma unroll
             for (int k = 0; k < kFeat; ++k) f[k] = 0.0f;
@@ -987,6 +1001,12 @@ __global__ void __launch_bounds__(kTile, kMlpBlocksPerSM) proposalKernel(const P
         storeFeatures(T, SmemMap::a0, f);
         const float logit = mlpTile<true>(T);
         if (gr < total) P.out[gr] = logit;
+        col += dCol;
+        row += dRow;
+        if (col >= P.V.nW) {
+            col -= P.V.nW;
+            ++row;
+        }
         if (!__syncthreads_and(T.ok)) break;
     }
     tileEnd<SmemMap>(T, P.error);
@@ -1282,6 +1302,7 @@ struct hase_context {
     MeshView view() const {
         MeshView v{};
         invariantDivisor(T, v.divTm, v.divTs);
+        invariantDivisor(Np, v.divNpm, v.divNps);
         v.tri = tri.p;
         v.geo = geo.p;
         v.verts = verts.p;
@@ -1445,6 +1466,10 @@ hase_status buildProposalView(hase_context* c, double A, double B, ProposalView&
     V.lnRt = float(lnRt);
     V.R = std::max(R, 1e-6f);
     V.H = float(c->h * L);
+    V.invR = 1.0f / V.R;
+    V.invH = 1.0f / V.H;
+    V.invTwoH = 0.5f / V.H;
+    V.invh = float(1.0 / c->h);
     V.lnVref = float(std::log(std::max(vmean, 1e-30) / (double(V.R) * V.R)));
     const double se = (A - B), sa = B;
     V.lnSigmaRatio = float(std::log(std::max(se, 1e-30) / std::max(sa, 1e-30)));

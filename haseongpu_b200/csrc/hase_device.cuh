@@ -77,6 +77,7 @@ struct MeshView {
     const float* reflect;    // [T][2] or nullptr
     uint32_t T, layers, P, Np;
     uint32_t divTm, divTs;   // floor(p / T) = (p * divTm) >> divTs for p < 2^31 (invariantDivisor)
+    uint32_t divNpm, divNps; // the same for division by Np
     float h;                 // level spacing
     float cladAbs;           // claddingAbsorption
     float tolEnd;            // |s| below which the target is reached
@@ -87,6 +88,11 @@ struct MeshView {
 // instead of a 32-bit division by the runtime T.
 __device__ __forceinline__ uint32_t prismLayer(const MeshView& m, uint32_t p) {
     return uint32_t((uint64_t(p) * m.divTm) >> m.divTs);
+}
+
+// Level of sample index s < 2^31 (s = point + level Np), by multiply-shift.
+__device__ __forceinline__ uint32_t sampleLevel(const MeshView& m, uint32_t s) {
+    return uint32_t((uint64_t(s) * m.divNpm) >> m.divNps);
 }
 
 // Unfolded integer level of the image of sample level ls for reflection slice.
