@@ -584,9 +584,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         k2 = (1u << 24) - 1u - k2;
                     }
                     const int kImg = imageLevel(ls, int(m.layers), j);
-                    const uint32_t lam =
-                        HASE_N_LAMBDA > 1 ? uint32_t((uint64_t(r) * HASE_N_LAMBDA / L.M + lambdaPhase) % HASE_N_LAMBDA)
-                                        : 0u;
+                    // stratified wavelength bin (floor(r nL / M) + phase) mod nL
+                    // without a 64-bit division: an FP32 estimate of the quotient
+                    // (off by at most 1 for nL < 2^22) and one exact correction
+                    // on the 64-bit products; the quotient is below nL (r < M)
+                    uint32_t lam = 0u;
+                    if (HASE_N_LAMBDA > 1) {
+                        const uint64_t num = uint64_t(r) * HASE_N_LAMBDA;
+                        uint32_t qb = uint32_t(float(r) * (float(HASE_N_LAMBDA) / float(L.M)));
+                        if (uint64_t(qb) * L.M > num) --qb;
+                        else if (uint64_t(qb + 1u) * L.M <= num) ++qb;
+                        lam = qb + lambdaPhase;
+                        if (lam >= HASE_N_LAMBDA) lam -= HASE_N_LAMBDA;
+                    }
                     const float2 ab = __ldg(HASE_SPEC + lam);
                     float dx, dy, dz, alphaL, D2;
                     if (L.nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
