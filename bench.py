@@ -50,7 +50,10 @@ BYTES_PER_CROSSING = 52        # triangle record 48 B + prism beta 4 B
 SMS = 148
 LANES_PER_SM = 128
 MLP_FLOP_PER_PAIR = 2 * (12 * 64 + 64 * 64 + 64 * 64 + 64 * 1)  # 18,048 FLOP per (sample, prism) inference
-XU_INSTR_PER_PAIR = 238  # special-function (MUFU + conversion) instructions per pair: 192 SiLUs x 1 (tanh) + features
+# special-function (XU) instructions per pair, from ncu (XU pipe 65.2 % active over 7.44e6 cycles x 148 SMs x 16
+# lanes = 1.15e10 for 4.99e7 pairs): 192 SiLUs x 1 (tanh) + ~38 in the features (the float-to-int conversions and
+# floors of the 8-point gain-grid lookup, two logarithms, a square root, an exponential, reciprocals)
+XU_INSTR_PER_PAIR = 230
 XU_LANES_PER_SM = 16
 FWD_METRIC = "forward Tet4 phi-ASE source rays traced and tallied per second on 1 B200 (crossings/s alongside)"
 FP64_INSTR_PER_TET_CROSSING = 100  # stated per-crossing FP64 instruction count of the forward walk
