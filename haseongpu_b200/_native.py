@@ -64,6 +64,7 @@ EXPORTED_SYMBOLS = (
     "hase_calc_phi_ase_learned",
     "hase_log_contributions",
     "hase_proposal_features",
+    "hase_learned_weights",
     # include/hase_b200_batch.h
     "hase_batch_create",
     "hase_batch_destroy",
@@ -377,6 +378,8 @@ def lib():
         L.hase_log_contributions.argtypes = [C.c_void_p, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc), _f32p,
                                              C.POINTER(ResultDesc)]
         L.hase_proposal_features.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
+        L.hase_learned_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                           C.c_float, _f32p]
         L.hase_simulate.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc),
                                     C.POINTER(PumpDesc), C.POINTER(TimeDesc), C.POINTER(TimeResultDesc)]
         L.hase_batch_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]

@@ -2338,6 +2338,56 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     return HASE_OK;
 }
 
+hase_status hase_learned_weights(hase_context* c, hase_proposal* net, uint32_t firstSample, uint32_t count,
+                                uint32_t useReflections, uint32_t monochromatic, float mixture, float* weights) {
+    if (!c || !net || !weights || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
+    if (!(mixture >= 0.0f) || mixture >= 1.0f) return fail(HASE_INVALID_ARGUMENT, "mixture must be in [0, 1)");
+    if (net->device != c->device)
+        return fail(HASE_INVALID_ARGUMENT, "the proposal network and the context are on different devices");
+    HASE_TRY(setDevice(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    // the spectral average of calcCore: over the solve's wavelengths
+    const uint32_t nL = monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double meanA = 0, meanB = 0;
+    for (uint32_t l = 0; l < nL; ++l) {
+        meanA += c->nTot * (c->sigmaE[l] + c->sigmaA[l]) / nL;
+        meanB += c->nTot * c->sigmaA[l] / nL;
+    }
+    ProposalView pv{};
+    HASE_TRY(cachedProposalView(c, meanA, meanB, pv));
+    pv.firstSample = firstSample;
+    pv.nW = nW;
+    DevBuf<float> lnw, prior, w;
+    DevBuf<uint32_t> q, off;
+    DevBuf<unsigned long long> Q;
+    HASE_CUDA(lnw.ensure(size_t(count) * nW));
+    HASE_CUDA(prior.ensure(size_t(count) * nW));
+    HASE_CUDA(w.ensure(size_t(count) * nW));
+    HASE_CUDA(q.ensure(size_t(count) * nW));
+    HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
+    HASE_CUDA(Q.ensure(count));
+    HASE_CUDA(cudaFuncSetAttribute(proposalKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
+    int sms = 0;
+    HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    ProposalLaunch pl{pv, net->wimg.p, net->vec.p, lnw.p, prior.p, nullptr, count, net->error.p};
+    const uint64_t tiles = (uint64_t(count) * nW + kTile - 1) / kTile;
+    proposalKernel<<<uint32_t(std::min<uint64_t>(tiles, uint64_t(std::max(1, sms)) * kMlpBlocksPerSM)), kTile,
+                     kSmemBytes, c->stream>>>(pl);
+    HASE_CUDA(cudaGetLastError());
+    mixtureKernel<<<count, 1024, 0, c->stream>>>(nW, lnw.p, prior.p, mixture > 0.0f ? mixture : 0.1f);
+    HASE_CUDA(cudaGetLastError());
+    MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
+    mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(weights, w.p, size_t(count) * nW * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    int err = 0;
+    HASE_CUDA(cudaMemcpy(&err, net->error.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(HASE_DEVICE_TIMEOUT, "a tensor-core wait of the proposal network timed out");
+    return HASE_OK;
+}
+
 hase_status hase_ray_map(uint32_t rows, uint32_t n, const float* weights, uint32_t rays, const uint32_t* phases,
                          uint32_t* q, uint32_t* offsets, uint64_t* Qout) {
     if (!weights || !phases || !q || !offsets || !Qout || rows == 0 || n == 0)

@@ -56,10 +56,14 @@ class Result:
     tallyMode: int = 0
     fallbackSamples: int = 0
     status: int = 0
+    # backward solves: the legacy archives' ``mse``, the standard error of the
+    # unnormalised estimator phi tau / N_tot (a length): RSE * phi * tau / N_tot
+    legacyMse: np.ndarray = field(default_factory=lambda: np.empty(0))
 
     @property
     def mse(self) -> np.ndarray:
-        """Legacy name of the per-sample relative standard error."""
+        """Legacy name of the per-sample relative standard error (the quantity
+        every threshold applies to; ``legacyMse`` is the legacy archives' value)."""
         return self.relativeStandardError
 
 
@@ -79,6 +83,7 @@ class DeviceMesh:
         N.check(N.lib().hase_context_create(C.byref(desc), C.byref(spec), int(device), C.byref(handle)))
         self.handle = handle
         self.numberOfWavelengths = sa.size
+        self.sigmaA, self.sigmaE = sa, se
 
     def _hold(self, a):
         a = np.ascontiguousarray(a)
@@ -151,7 +156,7 @@ class DeviceMesh:
                                                            C.byref(ld), C.byref(r)), allow_warnings=True)
         self._fill(out, r, status)
         out.fallbackSamples = int(ld.fallbackSamples)
-        return out
+        return self._legacy_mse(out)
 
     def log_contributions(self, *, minRays, useReflections=False, monochromatic=False, nearFieldSampling=True,
                           rngSeed=5489, minSample=0, maxSample=None):
@@ -246,6 +251,11 @@ class DeviceMesh:
         out.passes = int(r.passes)
         out.unconvergedSamples = int(r.unconvergedSamples)
         out.kernelLaunches = int(r.kernelLaunches)
+        return self._legacy_mse(out)
+
+    def _legacy_mse(self, out: Result) -> Result:
+        out.legacyMse = out.relativeStandardError * out.phiAse.astype(np.float64) * (
+            float(self.mesh.crystalTFluo) / float(self.mesh.nTot))
         return out
 
     def importance_weights(self, firstSample, count, useReflections=False) -> np.ndarray:
@@ -253,6 +263,16 @@ class DeviceMesh:
         w = np.empty((count, slices * self.mesh.numberOfPrisms), np.float32)
         N.check(N.lib().hase_importance_weights(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
                                                 N.ptr(w, N._f32p)))
+        return w
+
+    def learned_weights(self, net, firstSample, count, useReflections=False, monochromatic=False,
+                        mixture=0.0) -> np.ndarray:
+        """The learned proposal's normalised first-pass weights (hase_learned_weights)."""
+        slices = 5 if useReflections else 1
+        w = np.empty((count, slices * self.mesh.numberOfPrisms), np.float32)
+        N.check(N.lib().hase_learned_weights(self.handle, net.handle, int(firstSample), int(count),
+                                             1 if useReflections else 0, 1 if monochromatic else 0, float(mixture),
+                                             N.ptr(w, N._f32p)))
         return w
 
     def trace(self, start, tri, level, sample, slice_=None, wavelength=0):

@@ -161,11 +161,11 @@ hase_status hase_trace_rays(hase_context* ctx, uint32_t n, const float* start, c
                             uint32_t wavelength, float* lnGain, float* distance, uint32_t* dropped);
 
 /* Allocation-free estimate of one sample point (no counterpart in the
- * reference).  For callers that must not allocate device memory -- code that
- * runs while a CUDA stream is being captured into a graph, real-time loops
- * whose memory is fixed up front, or hosts that hand out device memory through
- * their own pool -- this entry point calls no cudaMalloc/cudaFree and no
- * allocating library routine.  The caller passes device pointers:
+ * reference).  For callers that must not allocate device memory -- real-time
+ * loops whose memory is fixed up front (a cudaMalloc can block and
+ * synchronise the device mid-loop), or hosts that reserve the device's memory
+ * and hand it out only through their own pool -- this entry point calls no
+ * cudaMalloc/cudaFree and no allocating library routine.  The caller passes device pointers:
  * `deviceWeights` [slices * prisms] non-negative importance weights (slices =
  * 5 with reflections, else 1; e.g. from hase_importance_weights) and
  * `deviceResult` [4] doubles receiving phiAse, relative standard error, rays
@@ -177,7 +177,8 @@ hase_status hase_trace_rays(hase_context* ctx, uint32_t n, const float* start, c
  * the array's device address; make that first call before any stream
  * capture.  All calls on one device share the array: calls that overlap on
  * the GPU (other host threads, other contexts on the same device) race and
- * must be serialised by the caller.  Returns after the result is written. */
+ * must be serialised by the caller.  It synchronises the context's stream
+ * and returns once the result is written. */
 hase_status hase_estimate_sample_noalloc(hase_context* ctx, uint32_t sample, const float* deviceWeights, uint32_t rays,
                                          uint32_t rngSeed, uint32_t useReflections, uint32_t nearFieldSampling,
                                          double* deviceResult);

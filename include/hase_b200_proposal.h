@@ -114,6 +114,16 @@ hase_status hase_calc_phi_ase_learned(hase_context* ctx, hase_proposal* net, con
 hase_status hase_log_contributions(hase_context* ctx, const hase_experiment_desc* experiment,
                                    const hase_compute_desc* compute, float* contributions, hase_result* result);
 
+/* The normalised ray->prism proposal hase_calc_phi_ase_learned draws its
+ * first pass from for samples [firstSample, firstSample + count): the
+ * mixture (1 - mixture) softmax(logits) + mixture beta V R_j / d^2 prior
+ * (mixture 0 = the default 0.1), divided by its maximum, as FP32
+ * weights [count][slices * P] -- the learned counterpart of
+ * hase_importance_weights, for replaying a learned solve with the CPU
+ * oracle. */
+hase_status hase_learned_weights(hase_context* ctx, hase_proposal* net, uint32_t firstSample, uint32_t count,
+                                 uint32_t useReflections, uint32_t monochromatic, float mixture, float* weights);
+
 /* Network features of every (slice, prism) pair of samples
  * [firstSample, firstSample + count): features [count][slices * P][12]. */
 hase_status hase_proposal_features(hase_context* ctx, uint32_t firstSample, uint32_t count, uint32_t useReflections,

@@ -216,3 +216,54 @@ def test_medium_without_excitation_in_a_batch(media):
         assert np.all(res[0].phiAse > 0)
     finally:
         dark.close()
+
+
+def _oracle_replay(oracle, ctx, lo, hi, seed, W, kw):
+    """The oracle's adaptive solve of samples [lo, hi] of ctx with the device's
+    first-pass weights W, at threshold * (1 -+ 2e-3) (the device compares FP32
+    /FP64 errors with the threshold, the oracle FP64 ones)."""
+    okw = dict(minRays=kw["minRays"], maxRays=kw["maxRays"], adaptiveSteps=kw["adaptiveSteps"],
+               useReflections=kw.get("useReflections", False), seed=seed, minSample=lo, maxSample=hi, weights=W)
+    spec = (ctx.sigmaA[:1], ctx.sigmaE[:1]) if kw.get("monochromatic") else (ctx.sigmaA, ctx.sigmaE)
+    return [oracle.phi_ase(ctx.mesh, spec, mseThreshold=kw["mseThreshold"] * f, **okw) for f in (1 - 2e-3, 1 + 2e-3)]
+
+
+def _matches_replay(res, lo_hi):
+    lo, hi = lo_hi
+    same_lo, same_hi = res.totalRays == lo["totalRays"], res.totalRays == hi["totalRays"]
+    assert np.all(same_lo | same_hi), np.flatnonzero(~(same_lo | same_hi))
+    assert np.mean(same_lo & same_hi) >= 0.95
+    np.testing.assert_allclose(res.phiAse, np.where(same_lo, lo["phiAse"], hi["phiAse"]), rtol=1e-4)
+    assert int(res.droppedRays.sum()) == int(lo["droppedRays"].sum()) == 0
+
+
+def test_batched_media_replayed_by_the_oracle(media, oracle):
+    """Medium i of a batch (seed rngSeed + i, adaptive passes, polychromatic
+    spectra) against the FP64 oracle directly: the oracle walks the same rays
+    from the medium's importance weights, so ray counts agree exactly and phi
+    to 1e-4."""
+    from haseongpu_b200 import MediaBatch
+
+    items = _ranges(media, n=48)
+    with MediaBatch(0) as b:
+        res, st = b.solve(items, **KW)
+    assert st.passes >= 2
+    for i, (ctx, lo, hi) in enumerate(items):
+        W = ctx.importance_weights(lo, hi - lo + 1)
+        _matches_replay(res[i], _oracle_replay(oracle, ctx, lo, hi, KW["rngSeed"] + i, W, KW))
+
+
+def test_learned_batch_replayed_by_the_oracle(media, oracle):
+    """The learned batch (no fallback) against the oracle directly: medium i
+    replayed from the proposal's own first-pass weights (hase_learned_weights)
+    with seed rngSeed + i."""
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.proposal import ProposalNet
+
+    items = _ranges(media, n=32)
+    kw = dict(KW, maxRays=16000, adaptiveSteps=2)
+    with ProposalNet(seed=5) as net, MediaBatch(0) as b:
+        res, _ = b.solve(items, net=net, **kw)
+        for i, (ctx, lo, hi) in enumerate(items):
+            W = ctx.learned_weights(net, lo, hi - lo + 1)
+            _matches_replay(res[i], _oracle_replay(oracle, ctx, lo, hi, kw["rngSeed"] + i, W, kw))

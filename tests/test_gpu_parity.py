@@ -173,16 +173,51 @@ def test_estimator_replay_matches_oracle(oracle, workload):
     np.testing.assert_allclose(dev.relativeStandardError, ref["mse"], rtol=1e-3, atol=1e-7)
 
 
+@pytest.mark.parametrize("workload", ["disc_small", "disc_poly"])
+def test_adaptive_multipass_replay_matches_oracle(oracle, workload):
+    """Kernel (d): the multi-pass adaptive solve (geometric ray targets, only
+    the samples above the threshold topped up on each pass) replayed by the
+    oracle with the device's weights.  The threshold is set inside the
+    first-pass error distribution so that samples stop on different passes.
+    The device and the oracle compare slightly different FP32/FP64 errors
+    with the threshold, so the oracle is run at threshold * (1 -+ 2e-3):
+    every device sample must stop exactly where one of the two stops (and
+    almost all where both do), with phi within 1e-4 of that oracle run."""
+    from haseongpu_b200 import configs
+
+    w = configs.WORKLOADS[workload]()
+    mesh = w.mesh
+    sa, se = w.spectra.resampled(w.monochromatic)
+    first, count = 211, 48
+    kw = dict(minRays=4096, maxRays=65536, adaptiveSteps=4, useReflections=w.useReflections)
+    rng = dict(minSample=first, maxSample=first + count - 1)
+    with _ctx(mesh, sa, se) as ctx:
+        W = ctx.importance_weights(first, count, w.useReflections)
+        one = ctx.calc_phi_ase(minRays=4096, useReflections=w.useReflections, monochromatic=w.monochromatic,
+                               rngSeed=77, **rng)
+        thr = float(np.percentile(one.relativeStandardError, 70)) * 0.45
+        dev = ctx.calc_phi_ase(mseThreshold=thr, monochromatic=w.monochromatic, rngSeed=77, **kw, **rng)
+    lo, hi = (oracle.phi_ase(mesh, (sa, se), mseThreshold=thr * f, seed=77, weights=W, **kw, **rng)
+              for f in (1.0 - 2e-3, 1.0 + 2e-3))
+    assert len(np.unique(dev.totalRays)) >= 3, np.unique(dev.totalRays)  # several passes end somewhere
+    assert set(np.unique(dev.totalRays)) <= {4096, 8192, 16384, 32768, 65536}
+    same_lo, same_hi = dev.totalRays == lo["totalRays"], dev.totalRays == hi["totalRays"]
+    assert np.all(same_lo | same_hi), np.flatnonzero(~(same_lo | same_hi))
+    assert np.mean(same_lo & same_hi) >= 0.95
+    ref = np.where(same_lo, lo["phiAse"], hi["phiAse"])
+    np.testing.assert_allclose(dev.phiAse, ref, rtol=1e-4)
+    ref_rse = np.where(same_lo, lo["mse"], hi["mse"])
+    np.testing.assert_allclose(dev.relativeStandardError, ref_rse, rtol=1e-3, atol=1e-7)
+    assert dev.raysTraced == int(dev.totalRays.astype(np.int64).sum())
+    assert dev.unconvergedSamples == int(np.sum(dev.relativeStandardError > thr))
+
+
 @pytest.mark.parametrize("name", ["cuboid", "cylindrical"])
 def test_gpu_matches_legacy_serial_reference(name):
-    """Per-sample agreement with the legacy serial buffers (1e6 rays/sample).
-
-    With uniform start points (nearFieldSampling off) the estimator is the
-    legacy one: ratios within 0.3 % (mean) / 0.5 % (median) and >= 90 % of
-    samples within 3 sigma -- the 1/d^2 weight of the prisms touching the
-    sample is heavy-tailed, so the sample RSE understates some errors.
-    Near-field sampling (bounded weights, pinned to 1e-4 by the analytic
-    known answer) must agree on the mean and the volume integral."""
+    """Per-sample agreement with the legacy serial buffers (1e6 rays/sample,
+    uniform start points): ratios within 0.3 % (mean) / 0.5 % (median) for
+    both samplers, dndt exact, and the near-field estimator's volume integral
+    within 0.3 %."""
     d = np.load(GOLDEN / f"legacy_{name}.npz")
     mesh = legacy_mesh(name)
     sa, se = legacy_spectrum(name)
@@ -197,15 +232,61 @@ def test_gpu_matches_legacy_serial_reference(name):
         assert abs(np.median(ratio) - 1.0) < 0.005, np.median(ratio)
         np.testing.assert_allclose(r.dndtAse,
                                    (d["betaCells"] * (se[0] + sa[0]) - sa[0]) * r.phiAse.astype(np.float64), rtol=1e-12)
-    sigma = plain.relativeStandardError * plain.phiAse * np.sqrt(1.0 + 200000 / 1e6)
-    z = (plain.phiAse - legacy) / sigma
-    assert np.mean(np.abs(z) < 3) > 0.9, np.mean(np.abs(z) < 3)
-    # a few legacy values carry a rare large contribution of their heavy tail
-    # (both of our samplers agree with each other there)
-    dev = np.abs(near.phiAse / legacy - 1.0)
-    assert np.mean(dev < 0.03) > 0.99 and dev.max() < 0.12, (np.mean(dev < 0.03), dev.max())
     assert abs(near.phiAse.astype(np.float64).sum() / legacy.sum() - 1.0) < 0.003
     assert np.median(near.relativeStandardError) < 0.5 * np.median(plain.relativeStandardError)
+
+
+@pytest.mark.parametrize("name", ["cuboid", "cylindrical"])
+def test_gpu_within_3_sigma_of_the_oracle(oracle, name):
+    """The statistical level at its stated tolerance: per-sample phi of the
+    device (near-field start points, bounded weights, seed 11) against the
+    FP64 oracle's independent estimate (seed 12), every sample of the legacy
+    meshes, within 3 sigma of the combined Monte Carlo standard error
+    sigma = sqrt(sigma_gpu^2 + sigma_oracle^2).  The i.i.d. error formula
+    overstates the error of the systematic (stratified) ray->prism split, so
+    z is narrower than N(0, 1): at most 0.5 % of samples beyond 3 sigma
+    (0.27 % for N(0, 1)), a centred mean and a spread below 1.05."""
+    mesh = legacy_mesh(name)
+    sa, se = legacy_spectrum(name)
+    with _ctx(mesh, sa, se) as ctx:
+        dev = ctx.calc_phi_ase(minRays=20000, rngSeed=11)
+    ref = oracle.phi_ase(mesh, (sa, se), minRays=20000, seed=12)
+    sig = np.hypot(dev.relativeStandardError * dev.phiAse, ref["mse"] * ref["phiAse"])
+    z = (dev.phiAse - ref["phiAse"]) / sig
+    assert np.mean(np.abs(z) < 3.0) >= 0.995, np.mean(np.abs(z) < 3.0)
+    assert abs(z.mean()) < 4.0 / np.sqrt(z.size), z.mean()
+    assert z.std() < 1.05, z.std()
+
+
+@pytest.mark.parametrize("name", ["cuboid", "cylindrical"])
+def test_legacy_buffers_scatter_like_the_uniform_estimator(name):
+    """Why the legacy buffers are not held to 3 sigma per sample: with uniform
+    start points the 1/d^2 weight of the prisms touching a sample has an
+    infinite variance (P(X > x) ~ x^-3/2), so a 1e6-ray estimate is skewed
+    below its mean and its sample error is not a standard deviation.  Against
+    the bounded near-field estimate at 4e6 rays (relative error ~5e-4), the
+    legacy buffers' standardised deviations z = (legacy - near) / sigma_1e6
+    must be distributed like those of this build's own uniform-start
+    estimator at the same 1e6 rays: deciles within 0.3 and the fractions
+    within 3 sigma within 3 points (two-sample Kolmogorov-Smirnov distance
+    below 0.06)."""
+    d = np.load(GOLDEN / f"legacy_{name}.npz")
+    mesh = legacy_mesh(name)
+    sa, se = legacy_spectrum(name)
+    with _ctx(mesh, sa, se) as ctx:
+        near = ctx.calc_phi_ase(minRays=4_000_000, rngSeed=21)
+        plain = ctx.calc_phi_ase(minRays=1_000_000, rngSeed=22, nearFieldSampling=False)
+    assert np.median(near.relativeStandardError) < 1.5e-3
+    sig = plain.relativeStandardError * plain.phiAse
+    z_legacy = (d["phiASE"] - near.phiAse) / sig
+    z_ours = (plain.phiAse - near.phiAse) / sig
+    dec = np.arange(10, 100, 10)
+    np.testing.assert_allclose(np.percentile(z_legacy, dec), np.percentile(z_ours, dec), atol=0.3)
+    assert abs(np.mean(np.abs(z_legacy) < 3) - np.mean(np.abs(z_ours) < 3)) < 0.03
+    grid = np.sort(np.concatenate([z_legacy, z_ours]))
+    cdf = lambda v: np.searchsorted(np.sort(v), grid, side="right") / v.size  # noqa: E731
+    assert np.max(np.abs(cdf(z_legacy) - cdf(z_ours))) < 0.06
+    assert np.median(z_ours) > 0.2  # the skew itself: the typical 1e6-ray value lies below the mean
 
 
 def test_gpu_matches_legacy_true_cladding_run():
