@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "hase_calc_phi_ase",
     "hase_context_destroy",
     "hase_importance_weights",
+    "hase_importance_crossings",
     "hase_ray_map",
     "hase_trace_rays",
     "hase_philox",
@@ -347,6 +348,7 @@ def lib():
                                         C.POINTER(ResultDesc)]
         L.hase_context_destroy.argtypes = [C.c_void_p]
         L.hase_importance_weights.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
+        L.hase_importance_crossings.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
         L.hase_ray_map.argtypes = [C.c_uint32, C.c_uint32, _f32p, C.c_uint32, _u32p, _u32p, _u32p, _u64p]
         L.hase_trace_rays.argtypes = [C.c_void_p, C.c_uint32, _f32p, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                       _f32p, _f32p, _u32p]

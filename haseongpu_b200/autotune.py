@@ -39,7 +39,7 @@ def variant_names() -> list[str]:
     return [lib.hase_ray_kernel_variant_name(i).decode() for i in range(lib.hase_ray_kernel_variant_count())]
 
 
-def pinned(name: str, raysPerThread: int = 16, importanceLayers: int = 2) -> TuneResult:
+def pinned(name: str, raysPerThread: int = 16, importanceLayers: int = 0) -> TuneResult:
     """A launch shape chosen by name instead of by a sweep (to time or profile
     one exact kernel); raises ValueError for a name the library does not have."""
     names = variant_names()
@@ -69,7 +69,7 @@ def autotune(ctx, *, firstSample: int, samples: int, rays: int, useReflections: 
             if best is None or t < best[2]:
                 best = (v, rpt, t)
     imp = []
-    for layers in (2, 4, 8):
+    for layers in (0, 2, 4, 8):  # 0: the line-team kernel
         t = min(ctx.calc_phi_ase(minRays=1, maxRays=1, useReflections=useReflections, monochromatic=monochromatic,
                                  nearFieldSampling=nearFieldSampling, rngSeed=3, minSample=firstSample,
                                  maxSample=firstSample + samples - 1, importanceLayers=layers).importanceMilliseconds

@@ -124,6 +124,7 @@ struct ImportanceLaunch {
     const uint32_t* rowList;  // rows to compute (blockIdx.y indexes it), or null: rows 0 .. gridDim.y - 1
     const uint8_t* rowFlag;   // batched media: only rows with rowFlag[flagBase + row] set are computed (or null)
     uint32_t flagBase;
+    unsigned long long* crossings;  // counting launches only: total walk crossings
 };
 
 // One thread per (sample, reflection slice, triangle, group of G layers): the
@@ -266,16 +267,191 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     }
 }
 
-// Prism layers per importance thread when the caller leaves it to the library
-// (4: 74 registers, 3 blocks per SM; on disc_poly 28 ms per 256 samples
-// against 35 ms with 8 layers and 27 ms with 2).
-constexpr int kImportanceLayers = 4;
+// Line-team importance kernel: a team of TL lanes per (sample row,
+// triangle t).  Every line from the centre of a prism (t, l) to an image
+// s_j of the sample point projects onto the same 2-D segment, centroid ->
+// sample point, so the team walks that segment in lock step (no divergence
+// in the number of triangles crossed) and each lane carries LPL of the
+// triangle's slices x layers lines through the level planes and
+// reflections of every triangle on it (teams of TL lanes, lines in chunks
+// of TL x LPL).  The 2-D edge tests are thus shared by up to TL x LPL lines
+// instead of the G of importanceKernel; the per-line arithmetic is
+// importanceKernel's, operation for operation, so the weights are the same
+// bits.  COUNT: also add the walk's crossings (triangle segments plus level
+// planes and reflections, per line) to *L.crossings.
+template <int TL, int LPL, bool TAB = false, bool COUNT = false>
+__global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) {
+    static_assert(TL >= 1 && TL <= 32 && (32 % TL) == 0, "a team is a power-of-two part of a warp");
+    const MeshView& m = L.m;
+    const float* gcol = TAB ? m.gTab : m.gainBeta;
+    constexpr uint32_t kTeams = 256 / TL;
+    const uint32_t t = blockIdx.x * kTeams + threadIdx.x / TL;
+    const uint32_t li = threadIdx.x % TL;
+    const uint32_t row = L.rowList ? L.rowList[blockIdx.y] : blockIdx.y;
+    unsigned long long counted = 0;
+    if (t < m.T && !(L.rowFlag && !L.rowFlag[L.flagBase + row])) {
+        const uint32_t sample = L.firstSample + row;
+        const float2 S = __ldg(m.points + sample % m.Np);
+        const int ls = int(sample / m.Np);
+        const float2 c = __ldg(m.centroid + t);
+        const float area = __ldg(&m.geo[2 * t + 1].z);
+        const float dx = c.x - S.x, dy = c.y - S.y;
+        const float D2 = sqrtf(fmaf(dx, dx, dy * dy));
+        const float inv2 = 1.0f / D2;
+        const float ux = dx * inv2, uy = dy * inv2;
+        float* outRow = L.lnw + size_t(row) * L.nW + t;
+        const uint32_t nLines = L.slices * m.layers;
+        for (uint32_t c0 = 0; c0 < nLines; c0 += TL * LPL) {
+            float J[LPL], lnR[LPL], invc[LPL];
+            int ka[LPL], phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
+            uint32_t sl[LPL];
+            bool ok[LPL];
+#pragma unroll
+            for (int g = 0; g < LPL; ++g) {
+                const uint32_t q = c0 + li + uint32_t(TL * g);
+                const bool valid = q < nLines;
+                const uint32_t l = valid ? q / L.slices : 0u;
+                const uint32_t j = valid ? q - l * L.slices : 0u;
+                sl[g] = valid ? j : 0xffffffffu;
+                lay[g] = int(l);
+                kImg[g] = imageLevel(ls, int(m.layers), j);
+                ok[g] = valid && __ldg(m.srcBeta + size_t(l) * m.T + t) > 0.0f;
+                J[g] = 0.0f;
+                lnR[g] = 0.0f;
+                ka[g] = int(l);
+                phys[g] = int(l);
+                pdir[g] = 1;
+                left[g] = expectedReflections(j);
+                invc[g] = D2 / (float(int(l) - kImg[g]) + 0.5f);
+            }
+            GlobalLoader load{m.tri};
+            uint32_t tk = t;
+            int forb = -1;
+            float sc = D2;
+            bool done = false;
+            for (int step = 0; step < kMaxSteps && !done; ++step) {
+                float4 a, b, cc;
+                load(tk, a, b, cc);
+                float bn = -1.0f, bd = 0.0f;
+                int bw = -1;
+                const auto edge = [&](float nx, float ny, float ce, int nbw, int e) {
+                    const float dd = -fmaf(nx, ux, ny * uy);
+                    const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
+                    const bool okE = (e != forb) & (dd > 0.0f) & (nbw >= 0);
+                    if (okE && nm * bd > bn * dd) {
+                        bn = nm;
+                        bd = dd;
+                        bw = nbw;
+                    }
+                };
+                edge(a.x, a.y, a.z, __float_as_int(cc.y), 0);
+                edge(a.w, b.x, b.y, __float_as_int(cc.z), 1);
+                edge(b.z, b.w, cc.x, __float_as_int(cc.w), 2);
+                float sOut = fmaxf(fminf(__fdividef(bn, bd), sc), 0.0f);
+                if (sOut <= m.tolEnd) {
+                    sOut = 0.0f;
+                    done = true;
+                }
+                float gbv[LPL];
+#pragma unroll
+                for (int g = 0; g < LPL; ++g) gbv[g] = ok[g] ? __ldg(gcol + size_t(phys[g]) * m.T + tk) : 0.0f;
+#pragma unroll
+                for (int g = 0; g < LPL; ++g) {
+                    if (!ok[g]) continue;
+                    if (COUNT) ++counted;
+                    const int dl = kImg[g] > lay[g] ? 1 : -1;  // layer step toward the image level
+                    float s = sc;
+                    float gb = gbv[g];
+                    while (true) {
+                        const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg[g]) * invc[g];
+                        if (!(sb > sOut)) break;
+                        if (COUNT) ++counted;
+                        J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
+                        s = sb;
+                        const int cand = phys[g] + pdir[g] * dl;
+                        if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+                            if (left[g] <= 0) {
+                                ok[g] = false;
+                                break;
+                            }
+                            const float dz = (float(lay[g] - kImg[g]) + 0.5f) * m.h;
+                            const float uz = dz * rsqrtf(fmaf(D2, D2, dz * dz));
+                            lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, uz));
+                            --left[g];
+                            pdir[g] = -pdir[g];
+                        } else {
+                            phys[g] = cand;
+                            gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
+                        }
+                        ka[g] += dl;
+                    }
+                    if (!ok[g]) continue;
+                    J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);
+                }
+                if (!done) {
+                    tk = uint32_t(bw) >> 2;
+                    forb = bw & 3;
+                    sc = sOut;
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < LPL; ++g) {
+                if (sl[g] == 0xffffffffu) continue;
+                const int l = lay[g];
+                float v = -INFINITY;
+                if (ok[g] && done) {
+                    const float dz = (float(l - kImg[g]) + 0.5f) * m.h;
+                    const float D3sq = fmaf(D2, D2, dz * dz);
+                    if (left[g] > 0) {  // the bounce happens at the target itself, in the final triangle
+                        const int dl = kImg[g] > l ? 1 : -1;
+                        const int cand = phys[g] + pdir[g] * dl;
+                        lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
+                    }
+                    const float beta = __ldg(m.srcBeta + size_t(l) * m.T + t);
+                    v = __logf(beta * area * m.h / D3sq) + J[g] * (sqrtf(D3sq) * inv2) + lnR[g];
+                }
+                outRow[size_t(sl[g]) * m.P + size_t(l) * m.T] = v;
+            }
+        }
+    }
+    if (COUNT) {
+        counted = warpSum(counted);
+        if ((threadIdx.x & 31) == 0 && counted) atomicAdd(L.crossings, counted);
+    }
+}
 
-// importanceKernel with G = layers (2, 4 or 8; 0 = the default) prism layers
-// per thread, over `rows` sample rows; tab: il.m.gTab holds g for il.A, il.B.
+// Team width of the line-team kernel: the narrowest team whose lanes hold a
+// sample's slices x layers lines of one triangle in one chunk of 3 per lane
+// (32 lanes: chunks of 96 lines).
+uint32_t importanceTeamWidth(uint32_t lines) {
+    return lines <= 12 ? 4u : lines <= 24 ? 8u : lines <= 48 ? 16u : 32u;
+}
+
+// The importance walks of `rows` sample rows: layers = 0 (the library's
+// choice): importanceTeamKernel; 2, 4 or 8: importanceKernel with that many
+// prism layers per thread.  tab: il.m.gTab holds g for il.A, il.B.  count:
+// the counting team kernel (il.crossings accumulates the walk's crossings).
 cudaError_t launchImportance(uint32_t layers, const ImportanceLaunch& il, uint32_t meshLayers, uint32_t T,
-                             uint32_t rows, cudaStream_t stream, bool tab = false) {
-    const uint32_t G = layers ? layers : uint32_t(kImportanceLayers);
+                             uint32_t rows, cudaStream_t stream, bool tab = false, bool count = false) {
+    if (layers == 0 || count) {
+        const uint32_t tl = importanceTeamWidth(il.slices * meshLayers);
+#define HASE_TEAM(TL)                                                                         \
+    {                                                                                         \
+        const dim3 grid((T + 256 / TL - 1) / (256 / TL), rows);                               \
+        if (count) importanceTeamKernel<TL, 3, false, true><<<grid, 256, 0, stream>>>(il);   \
+        else if (tab) importanceTeamKernel<TL, 3, true><<<grid, 256, 0, stream>>>(il);       \
+        else importanceTeamKernel<TL, 3><<<grid, 256, 0, stream>>>(il);                      \
+    }
+        switch (tl) {
+            case 4: HASE_TEAM(4) break;
+            case 8: HASE_TEAM(8) break;
+            case 16: HASE_TEAM(16) break;
+            default: HASE_TEAM(32) break;
+        }
+#undef HASE_TEAM
+        return cudaGetLastError();
+    }
+    const uint32_t G = layers;
     const uint32_t threads = il.slices * ((meshLayers + G - 1) / G) * T;
     const dim3 grid((threads + 255) / 256, rows);
     if (G == 2) {
@@ -470,6 +646,63 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
     return lo;
 }
 
+// Start state of ray r of sample `sample`, drawn in entry b = slice * P +
+// prism of the sample's ray map: Philox4x32-10 counter (r, sample, pass,
+// kTagRay); a uniform point in the prism, or (nearField) the solid-angle
+// start in a prism touching the image point; the stratified wavelength bin
+// (floor(r nL / M) + phase) mod nL.  wf: the ray's weight without C Q,
+// beta V / (d^2 q) (uniform start) or beta alpha L / q (near field).
+// Returns |start - image|^2 (0: the start point is the sample point itself).
+__device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_t b, uint32_t sample, float2 S, int ls,
+                                          uint32_t pass, uint32_t seedLo, uint32_t seedHi, uint32_t nLambda,
+                                          uint32_t lambdaPhase, uint32_t M, const float2* spec, const uint32_t* q,
+                                          uint32_t nearField, Ray& ray, float& wf) {
+    // reflection slice by subtraction (at most 4), layer by an exact
+    // multiply-shift: no integer divisions per ray
+    uint32_t j = 0, p = b;
+    while (p >= m.P) {
+        p -= m.P;
+        ++j;
+    }
+    const uint32_t l = prismLayer(m, p), t = p - l * m.T;
+    const Philox4 rnd = philox4x32_10(r, sample, pass, kTagRay, seedLo, seedHi);
+    uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
+    if (k1 + k2 + 1u > (1u << 24)) {
+        k1 = (1u << 24) - 1u - k1;
+        k2 = (1u << 24) - 1u - k2;
+    }
+    const int kImg = imageLevel(ls, int(m.layers), j);
+    // stratified wavelength bin without a 64-bit division: an FP32 estimate
+    // of the quotient (off by at most 1 for nL < 2^22) and one exact
+    // correction on the 64-bit products; the quotient is below nL (r < M)
+    uint32_t lam = 0u;
+    if (nLambda > 1) {
+        const uint64_t num = uint64_t(r) * nLambda;
+        uint32_t qb = uint32_t(float(r) * (float(nLambda) / float(M)));
+        if (uint64_t(qb) * M > num) --qb;
+        else if (uint64_t(qb + 1u) * M <= num) ++qb;
+        lam = qb + lambdaPhase;
+        if (lam >= nLambda) lam -= nLambda;
+    }
+    const float2 ab = __ldg(spec + lam);
+    float dx, dy, dz, alphaL, D2;
+    if (nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
+        nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
+                       unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
+        D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
+        wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, float(__ldg(q + b)));
+    } else {
+        const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
+        const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
+        const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
+        const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
+        D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j, ab.x, ab.y,
+                     m.h);
+        wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * float(__ldg(q + b)));
+    }
+    return D2;
+}
+
 // Persistent ray kernel: every warp repeatedly takes a work item -- itemRays
 // consecutive rays of one active sample -- from a global counter, walks them
 // (lanes whose ray ends take the next ray of the item, in groups of at least
@@ -569,50 +802,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                 if (!active && r < r1) {
                     const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
                     if (LOG) bsel = b;
-                    // reflection slice by subtraction (at most 4), layer by
-                    // an exact multiply-shift: no integer divisions per ray
-                    uint32_t j = 0, p = b;
-                    while (p >= m.P) {
-                        p -= m.P;
-                        ++j;
-                    }
-                    const uint32_t l = prismLayer(m, p), t = p - l * m.T;
-                    const Philox4 rnd = philox4x32_10(r, sample, L.pass, kTagRay, HASE_SEED_LO, L.seedHi);
-                    uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
-                    if (k1 + k2 + 1u > (1u << 24)) {
-                        k1 = (1u << 24) - 1u - k1;
-                        k2 = (1u << 24) - 1u - k2;
-                    }
-                    const int kImg = imageLevel(ls, int(m.layers), j);
-                    // stratified wavelength bin (floor(r nL / M) + phase) mod nL
-                    // without a 64-bit division: an FP32 estimate of the quotient
-                    // (off by at most 1 for nL < 2^22) and one exact correction
-                    // on the 64-bit products; the quotient is below nL (r < M)
-                    uint32_t lam = 0u;
-                    if (HASE_N_LAMBDA > 1) {
-                        const uint64_t num = uint64_t(r) * HASE_N_LAMBDA;
-                        uint32_t qb = uint32_t(float(r) * (float(HASE_N_LAMBDA) / float(L.M)));
-                        if (uint64_t(qb) * L.M > num) --qb;
-                        else if (uint64_t(qb + 1u) * L.M <= num) ++qb;
-                        lam = qb + lambdaPhase;
-                        if (lam >= HASE_N_LAMBDA) lam -= HASE_N_LAMBDA;
-                    }
-                    const float2 ab = __ldg(HASE_SPEC + lam);
-                    float dx, dy, dz, alphaL, D2;
-                    if (L.nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
-                        nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
-                                       unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
-                        D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
-                        wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, float(__ldg(q + b)));
-                    } else {
-                        const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
-                        const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
-                        const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
-                        const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
-                        D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j,
-                                     ab.x, ab.y, m.h);
-                        wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * float(__ldg(q + b)));
-                    }
+                    const float D2 = startRay(m, r, b, sample, S, ls, L.pass, HASE_SEED_LO, L.seedHi, HASE_N_LAMBDA,
+                                              lambdaPhase, L.M, HASE_SPEC, q, L.nearField, ray, wf);
                     active = D2 > 0.0f;
                     if (!active) ++dropped;  // start point on the sample point itself
                 }
@@ -654,6 +845,238 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     }
 }
 
+// Prepared start states per warp in the ring kernel (a power of two of at
+// least 63: the ring holds at most 31 unconsumed rays when a batch of 32 is
+// produced).
+constexpr uint32_t kRing = 64;
+constexpr uint32_t kRingBytesPerWarp = kRing * 3 * sizeof(float4);
+
+// Ray kernel with start states produced a warp at a time.  The persistent
+// work queue and the walk are those of rayKernel; what differs is how idle
+// lanes get their next ray.  Whenever the warp's ring in shared memory holds
+// fewer prepared rays than there are idle lanes, all 32 lanes prepare the
+// next 32 consecutive rays of the item together -- the ray->prism search as
+// one warp-wide step (32 offsets of the map per load, a 5-step shuffle
+// search per lane), Philox, the start point, the initial walk state -- and
+// append the valid ones to the ring; idle lanes then take prepared rays with
+// three 16-byte shared loads.  Every start-state instruction thereby runs on
+// 32 lanes, where rayKernel runs it on the idle lanes only (REFILL or more of
+// 32), and a refill is cheap enough to happen whenever REFILL lanes are idle
+// after COLS columns.  The rays, their start states and their walks are
+// rayKernel's, so the per-item sums agree with it to FP64 rounding.
+template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns,
+          int WALK = kWalkBeta>
+__global__ void __launch_bounds__(BLOCK, MINB) rayRingKernel(RayLaunch L) {
+    extern __shared__ float4 ringSmem[];  // [BLOCK / 32][kRing][3]
+    __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
+    // the current item's constants that only the batch preparation and the
+    // finish of a ray read: kept in shared memory, not in registers across the walk
+    struct ItemConsts {
+        const uint32_t* off;
+        const uint32_t* q;
+        double CQ;
+        unsigned long long wBase;
+        uint32_t sample, lambdaPhase, nLambda, ls, seedLo, entry0;
+    };
+    __shared__ ItemConsts sItem[BLOCK / 32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned laneLt = (1u << lane) - 1u;
+    float4* ring = ringSmem + size_t(threadIdx.x >> 5) * kRing * 3;
+    volatile ItemConsts& ic = sItem[threadIdx.x >> 5];
+    const uint32_t nItems = (POOL ? *L.count : L.nActive) * L.itemsPerRow;
+    uint32_t curInst = 0xffffffffu;
+    while (true) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(L.itemCounter, 1u);
+        item = __shfl_sync(full, item, 0);
+        if (item >= nItems) break;
+        const uint32_t row = L.active[item / L.itemsPerRow];
+        const uint32_t k = item % L.itemsPerRow;
+        const size_t slot = size_t(row) * kMaxItems + k;
+        const unsigned long long Qrow = L.Q[row];
+        if (Qrow == 0ull) {  // no source prism: every ray contributes 0
+            if (lane == 0) {
+                L.pSum[slot] = 0.0;
+                L.pSum2[slot] = 0.0;
+                L.pDrop[slot] = 0u;
+                L.pCross[slot] = 0ull;
+            }
+            continue;
+        }
+        uint32_t sample, nW;
+        size_t wBase, oBase;
+        if constexpr (POOL) {
+            const RowInfo ri = L.rows[row];
+            if (ri.inst != curInst) {
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(L.inst + ri.inst);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(sInst + (threadIdx.x >> 5));
+                for (uint32_t w = uint32_t(lane); w < sizeof(InstanceView) / 4; w += 32) dst[w] = __ldg(src + w);
+                __syncwarp();
+                curInst = ri.inst;
+            }
+            sample = ri.sample;
+            nW = ri.nW;
+            wBase = ri.w;
+            oBase = ri.w + row;
+        } else {
+            sample = L.firstSample + row;
+            nW = L.nW;
+            wBase = size_t(row) * nW;
+            oBase = size_t(row) * (nW + 1);
+        }
+        const volatile InstanceView& iv = sInst[threadIdx.x >> 5];
+        const MeshView& m = POOL ? sInst[threadIdx.x >> 5].m : L.m;
+        const GlobalLoader load{m.tri};
+        const uint32_t r0 = k * L.itemRays;
+        const uint32_t r1 = min(r0 + L.itemRays, L.M);
+        const float2 S = __ldg(m.points + sample % m.Np);
+        {
+            const uint32_t seedLo = POOL ? uint32_t(iv.seedLo) : L.seedLo;
+            const uint32_t nLam = POOL ? uint32_t(iv.nLambda) : L.nLambda;
+            const uint32_t* off = L.offsets + oBase;
+            // entry of the map holding ray r0 (then carried: the entry of the
+            // last ray prepared so far)
+            uint32_t c0 = 0;
+            if (lane == 0) {
+                c0 = upperBound(off, nW + 1, r0) - 1u;
+                ic.off = off;
+                ic.q = L.q + wBase;
+                ic.CQ = (POOL ? double(iv.C) : double(L.C)) * double(Qrow);
+                ic.wBase = wBase;
+                ic.sample = sample;
+                ic.lambdaPhase =
+                    nLam > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, seedLo, L.seedHi).y % nLam : 0u;
+                ic.nLambda = nLam;
+                ic.ls = uint32_t(sample / m.Np);
+                ic.seedLo = seedLo;
+                ic.entry0 = c0;
+            }
+            __syncwarp();
+        }
+        uint32_t cur = ic.entry0;
+
+        double sum = 0.0, sum2 = 0.0;
+        uint32_t dropped = 0, crossings = 0;
+        uint32_t fetch = r0, head = 0, tail = 0;  // warp-uniform: next ray to prepare, ring read / write counts
+        bool active = false;
+        Ray ray;
+        float wf = 0.0f;
+        uint32_t bsel = 0;
+        while (true) {
+            const unsigned idle = __ballot_sync(full, !active);
+            const uint32_t nIdle = uint32_t(__popc(idle));
+            if (nIdle == 32 && head == tail && fetch >= r1) break;
+            if (nIdle >= uint32_t(REFILL) || nIdle == 32) {
+                if (tail - head < nIdle && fetch < r1) {
+                    // prepare rays fetch .. fetch + nb - 1, one per lane
+                    const uint32_t nb = min(32u, r1 - fetch);
+                    const uint32_t r = fetch + uint32_t(lane);
+                    const bool valid = uint32_t(lane) < nb;
+                    const uint32_t* off = ic.off;
+                    // map entry b of ray r: off[b] <= r < off[b + 1], searched
+                    // in windows of 32 offsets starting after `cur`
+                    uint32_t b = 0, bLo = cur;
+                    bool pending = valid;
+                    while (__any_sync(full, pending)) {
+                        const uint32_t o = __ldg(off + min(bLo + 1u + uint32_t(lane), nW));
+                        uint32_t cnt = 0;
+#pragma unroll
+                        for (int st = 16; st >= 1; st >>= 1) {
+                            const uint32_t v = __shfl_sync(full, o, int(cnt) + st - 1);
+                            if (v <= r) cnt += uint32_t(st);
+                        }
+                        const uint32_t oLast = __shfl_sync(full, o, 31);
+                        if (pending && r < oLast) {
+                            b = bLo + cnt;
+                            pending = false;
+                        }
+                        bLo += 32u;
+                    }
+                    cur = __shfl_sync(full, b, int(nb) - 1);
+                    Ray nr;
+                    float nwf = 0.0f;
+                    bool ok = false;
+                    if (valid) {
+                        const float D2 = startRay(m, r, b, ic.sample, S, int(ic.ls), L.pass, ic.seedLo, L.seedHi,
+                                                  ic.nLambda, ic.lambdaPhase, L.M,
+                                                  POOL ? (const float2*)iv.spec : L.spec, ic.q, L.nearField, nr, nwf);
+                        ok = D2 > 0.0f;
+                        if (!ok) ++dropped;  // start point on the sample point itself
+                    }
+                    const unsigned okMask = __ballot_sync(full, ok);
+                    __syncwarp();  // every lane's earlier reads of the slots about to be overwritten are done
+                    if (ok) {
+                        float4* e = ring + ((tail + uint32_t(__popc(okMask & laneLt))) & (kRing - 1)) * 3;
+                        e[0] = make_float4(nr.s, nr.ux, nr.uy, nr.uz);
+                        e[1] = make_float4(nr.hOverUz, nr.zl, nr.A, nr.B);
+                        e[2] = make_float4(__uint_as_float(nr.t),
+                                           __uint_as_float(uint32_t(nr.phys) | (uint32_t(nr.reflLeft) << 16)), nwf,
+                                           __uint_as_float(b));
+                    }
+                    __syncwarp();
+                    tail += uint32_t(__popc(okMask));
+                    fetch += nb;
+                }
+                const uint32_t avail = tail - head;
+                const uint32_t rank = uint32_t(__popc(idle & laneLt));
+                if (!active && rank < avail) {
+                    const float4* e = ring + ((head + rank) & (kRing - 1)) * 3;
+                    const float4 a = e[0], c = e[1], d = e[2];
+                    ray.s = a.x;
+                    ray.ux = a.y;
+                    ray.uy = a.z;
+                    ray.uz = a.w;
+                    ray.hOverUz = c.x;
+                    ray.zl = c.y;
+                    ray.A = c.z;
+                    ray.B = c.w;
+                    ray.t = __float_as_uint(d.x);
+                    const uint32_t pr = __float_as_uint(d.y);
+                    ray.phys = int(pr & 0xffffu);
+                    ray.reflLeft = int(pr >> 16);
+                    ray.pdir = 1;
+                    ray.forb = -1;
+                    ray.steps = 0;
+                    ray.G = 0.0f;
+                    wf = d.z;
+                    if (LOG) bsel = __float_as_uint(d.w);
+                    active = true;
+                }
+                head += min(nIdle, avail);
+            }
+            if (active) {
+                const int st = stepRay<COLS, WALK>(m, S.x, S.y, ray, load);
+                if (st != kContinue) {
+                    crossings += uint32_t(ray.steps) + 1u;
+                    if (st == kDone) {
+                        finishReflections(m, ray);
+                        const double eg = ray.G < 80.0f ? double(expf(ray.G)) : exp(double(ray.G));
+                        const double X = ic.CQ * double(wf) * eg;
+                        sum += X;
+                        sum2 += X * X;
+                        if (LOG) atomicAdd(L.logBuf + size_t(ic.wBase) + bsel, float(X));
+                    } else {
+                        ++dropped;
+                    }
+                    active = false;
+                }
+            }
+        }
+        sum = warpSum(sum);
+        sum2 = warpSum(sum2);
+        dropped = warpSum(dropped);
+        crossings = warpSum(crossings);
+        if (lane == 0) {
+            L.pSum[slot] = sum;
+            L.pSum2[slot] = sum2;
+            L.pDrop[slot] = dropped;
+            L.pCross[slot] = crossings;
+        }
+        __syncwarp();  // the item's constants are read before the next item overwrites them
+    }
+}
+
 // Launch shapes of rayKernel the autotuner chooses from: block size, idle
 // lanes that trigger a refill, the occupancy target (blocks per SM the
 // register budget is fitted to) and the triangle columns a lane walks per
@@ -665,10 +1088,14 @@ struct RayVariant {
     const char* name;
     void (*mono)(RayLaunch);     // the same shape walking the g table (monochromatic single-medium solves), or null
     void (*noClad)(RayLaunch);   // the same shape for a medium without cladding prisms, or null
+    uint32_t smem;               // dynamic shared memory per block (the ring kernel's prepared rays), bytes
 };
 #define HASE_RAY_SHAPE(B, R, M, C, NAME)                                                      \
     {rayKernel<B, R, M, false, false, C>, B, NAME, rayKernel<B, R, M, false, false, C, kWalkTable>, \
-     rayKernel<B, R, M, false, false, C, kWalkBetaNoClad>}
+     rayKernel<B, R, M, false, false, C, kWalkBetaNoClad>, 0u}
+#define HASE_RING_SHAPE(B, R, M, C, NAME)                                                             \
+    {rayRingKernel<B, R, M, false, false, C>, B, NAME, rayRingKernel<B, R, M, false, false, C, kWalkTable>, \
+     rayRingKernel<B, R, M, false, false, C, kWalkBetaNoClad>, uint32_t(B / 32) * kRingBytesPerWarp}
 const RayVariant kRayVariants[] = {
     HASE_RAY_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
     HASE_RAY_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
@@ -680,14 +1107,24 @@ const RayVariant kRayVariants[] = {
     HASE_RAY_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
     HASE_RAY_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
     HASE_RAY_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
+    HASE_RING_SHAPE(256, 4, 4, 16, "ring256_refill4_occ4_cols16"),
+    HASE_RING_SHAPE(256, 8, 4, 32, "ring256_refill8_occ4_cols32"),
+    HASE_RING_SHAPE(256, 2, 4, 8, "ring256_refill2_occ4_cols8"),
+    HASE_RING_SHAPE(512, 4, 2, 16, "ring512_refill4_occ2_cols16"),
+    HASE_RING_SHAPE(512, 8, 2, 32, "ring512_refill8_occ2_cols32"),
+    HASE_RING_SHAPE(128, 4, 8, 16, "ring128_refill4_occ8_cols16"),
 };
 #undef HASE_RAY_SHAPE
+#undef HASE_RING_SHAPE
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
 static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
 // The same launch shapes for batched media (same order and names): the
 // general walk, and the walk for batches without cladding prisms.
 #define HASE_POOL_SHAPE(B, R, M, C, NAME) \
-    {rayKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayKernel<B, R, M, false, true, C, kWalkBetaNoClad>}
+    {rayKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayKernel<B, R, M, false, true, C, kWalkBetaNoClad>, 0u}
+#define HASE_POOL_RING_SHAPE(B, R, M, C, NAME)                                                              \
+    {rayRingKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayRingKernel<B, R, M, false, true, C, kWalkBetaNoClad>, \
+     uint32_t(B / 32) * kRingBytesPerWarp}
 const RayVariant kPoolVariants[] = {
     HASE_POOL_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
     HASE_POOL_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
@@ -699,8 +1136,28 @@ const RayVariant kPoolVariants[] = {
     HASE_POOL_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
     HASE_POOL_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
     HASE_POOL_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
+    HASE_POOL_RING_SHAPE(256, 4, 4, 16, "ring256_refill4_occ4_cols16"),
+    HASE_POOL_RING_SHAPE(256, 8, 4, 32, "ring256_refill8_occ4_cols32"),
+    HASE_POOL_RING_SHAPE(256, 2, 4, 8, "ring256_refill2_occ4_cols8"),
+    HASE_POOL_RING_SHAPE(512, 4, 2, 16, "ring512_refill4_occ2_cols16"),
+    HASE_POOL_RING_SHAPE(512, 8, 2, 32, "ring512_refill8_occ2_cols32"),
+    HASE_POOL_RING_SHAPE(128, 4, 8, 16, "ring128_refill4_occ8_cols16"),
 };
 #undef HASE_POOL_SHAPE
+#undef HASE_POOL_RING_SHAPE
+
+// Lets a launch shape use its dynamic shared memory (above the default
+// 48 KB per block) in every walk mode it has.
+cudaError_t allowRayVariantSmem(const RayVariant& v) {
+    if (v.smem == 0) return cudaSuccess;
+    for (void (*k)(RayLaunch) : {v.kernel, v.mono, v.noClad}) {
+        if (!k) continue;
+        const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(v.smem));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
 // ------------------------------------------------ (c)+(d) finalise ----
@@ -1711,10 +2168,11 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         const RayVariant& v = kRayVariants[variant];
         int sms = 0;
         HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        HASE_CUDA(allowRayVariantSmem(v));
         void (*const modes[3])(RayLaunch) = {v.kernel, v.mono, v.noClad};
         for (int w = 0; w < 3; ++w) {
             int perSM = 0;
-            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, modes[w], v.block, 0));
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, modes[w], v.block, v.smem));
             c->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
         }
     }
@@ -1830,8 +2288,8 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
                                                                uint64_t(c->variantBlocks[walk][variant])));
             void (*const kern)(RayLaunch) = walk == kWalkTable ? rv.mono : (walk == kWalkBetaNoClad ? rv.noClad : rv.kernel);
             void* rayArgs[] = {&rl};
-            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs, 0,
-                                       c->stream));
+            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs,
+                                       rv.smem, c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
             FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,
@@ -2327,14 +2785,33 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
     HASE_CUDA(Q.ensure(count));
     ImportanceLaunch il{c->view(), firstSample, slices, nW, float(meanA), float(meanB), lnw.p};
-    const uint32_t impThreads = slices * ((c->layers + kImportanceLayers - 1) / kImportanceLayers) * c->T;
-    importanceKernel<kImportanceLayers><<<dim3((impThreads + 255) / 256, count), 256, 0, c->stream>>>(il);
-    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(launchImportance(0, il, c->layers, c->T, count, c->stream));
     MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
     mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
     HASE_CUDA(cudaGetLastError());
     HASE_CUDA(cudaMemcpyAsync(weights, w.p, size_t(count) * nW * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+hase_status hase_importance_crossings(hase_context* c, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                                      uint64_t* crossings) {
+    if (!c || !crossings || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
+    HASE_TRY(setDevice(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    DevBuf<float> lnw;
+    DevBuf<unsigned long long> n;
+    HASE_CUDA(lnw.ensure(size_t(count) * nW));
+    HASE_CUDA(n.ensure(1));
+    HASE_CUDA(cudaMemsetAsync(n.p, 0, sizeof(unsigned long long), c->stream));
+    ImportanceLaunch il{c->view(), firstSample, slices, nW, 0.0f, 0.0f, lnw.p};
+    il.crossings = n.p;
+    HASE_CUDA(launchImportance(0, il, c->layers, c->T, count, c->stream, false, true));
+    unsigned long long h = 0;
+    HASE_CUDA(cudaMemcpyAsync(&h, n.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    *crossings = h;
     return HASE_OK;
 }
 
@@ -2766,9 +3243,11 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
     const uint32_t variant = cp->rayKernelVariant;
     const RayVariant& rv = kPoolVariants[variant];
     if (b->variantBlocks[0][variant] == 0) {
+        HASE_CUDA(allowRayVariantSmem(rv));
         for (int w = 0; w < 2; ++w) {
             int perSM = 0;
-            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, w ? rv.noClad : rv.kernel, rv.block, 0));
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, w ? rv.noClad : rv.kernel, rv.block,
+                                                                    rv.smem));
             b->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, b->sms));
         }
     }
@@ -3016,7 +3495,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                                                                    uint64_t(b->variantBlocks[noClad][variant])));
                 void* rayArgs[] = {&rl};
                 HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(noClad ? rv.noClad : rv.kernel), dim3(grid),
-                                           dim3(rv.block), rayArgs, 0, b->stream));
+                                           dim3(rv.block), rayArgs, rv.smem, b->stream));
                 HASE_CUDA(cudaEventRecordWithFlags(b->ev[4 + 2 * k], b->stream, cudaEventRecordExternal));
                 HASE_CUDA(cudaMemsetAsync(cntNxt, 0, sizeof(unsigned int), b->stream));
                 FinalizeLaunch fl{cur, 0u, ps.items, ps.M, ps.last ? 1 : 0, thr, b->pSum.p, b->pSum2.p, b->pDrop.p,

@@ -265,6 +265,13 @@ class DeviceMesh:
                                                 N.ptr(w, N._f32p)))
         return w
 
+    def importance_crossings(self, firstSample, count, useReflections=False) -> int:
+        """Crossings of the importance walks of the samples (hase_importance_crossings)."""
+        n = np.zeros(1, np.uint64)
+        N.check(N.lib().hase_importance_crossings(self.handle, int(firstSample), int(count),
+                                                  1 if useReflections else 0, N.ptr(n, N._u64p)))
+        return int(n[0])
+
     def learned_weights(self, net, firstSample, count, useReflections=False, monochromatic=False,
                         mixture=0.0) -> np.ndarray:
         """The learned proposal's normalised first-pass weights (hase_learned_weights)."""

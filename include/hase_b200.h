@@ -102,7 +102,9 @@ typedef struct {
     uint64_t workspaceBytes;            /* 0 = default device workspace budget */
     uint32_t rayKernelVariant;          /* launch shape of the ray kernel, 0 = default; see
                                            hase_ray_kernel_variant_name (chosen by the autotuner) */
-    uint32_t importanceLayers;          /* prism layers per importance-kernel thread: 0 (= 4), 2, 4 or 8 */
+    uint32_t importanceLayers;          /* importance kernel: 0 = line teams (a team of lanes per (sample,
+                                           triangle) shares the 2-D walk); 2, 4, 8 = that many prism layers
+                                           per thread; the same weights either way */
 } hase_compute_desc;
 
 /* Caller-allocated host arrays of (maxSample - minSample + 1) entries; any
@@ -147,6 +149,14 @@ hase_status hase_context_destroy(hase_context* ctx);
  * weights[i][j*P + p] for reflection slice j (slices = 5 with reflections, else 1). */
 hase_status hase_importance_weights(hase_context* ctx, uint32_t firstSample, uint32_t count,
                                     uint32_t useReflections, float* weights);
+
+/* Crossings of the importance walks of samples [firstSample, firstSample +
+ * count): per (sample, reflection slice, prism) line, the triangles its 2-D
+ * projection crosses plus the level planes and reflections on the way -- the
+ * work unit of the importance kernel's roofline (counted by an instrumented
+ * copy of the kernel; the walks are those of hase_calc_phi_ase). */
+hase_status hase_importance_crossings(hase_context* ctx, uint32_t firstSample, uint32_t count,
+                                      uint32_t useReflections, uint64_t* crossings);
 
 /* Ray->prism map of `rows` weight rows of length n: q[row][n] (quantised
  * weights), offsets[row][n+1] (exclusive ray offsets), Q[row]. */
