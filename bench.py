@@ -63,6 +63,10 @@ FP64_LANES_PER_SM = 64
 # DRAM bytes of one learned-solve rayKernel launch on disc_small (5,470 samples x 1e5 rays; ncu): the per-sample
 # ray maps (q, offsets) read once and the per-item partial sums written; the walk tables stay in L1/L2
 RAY_TRAFFIC_LEARNED = 403811328 + 29646848
+# what binds the same launch (ncu --set full, profiles/rayKernel_learned_disc_small.md): instruction issue, with
+# the walk tables in L1 -- thread instructions per crossing and per ray of that capture
+RAY_BINDING_LEARNED = "instruction issue (ncu: issue active 86.5 %, top stall 'not selected'; L1 hits 99.2 %)"
+RAY_INSTR_LEARNED = {"per_crossing": 112, "per_ray": 1590, "crossings_per_ray": 14.2}
 
 
 def parse():
@@ -101,10 +105,13 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def cpu_baseline(workload, seconds):
-    """Oracle (FP64 port of the method) on all host threads: the same adaptive
-    solve to the threshold, one sample per thread at a time, bounded in time
-    (at least one round of `cores` samples)."""
+def cpu_baseline(workload, seconds, fields=None, nearField=False):
+    """The reference's method on the host cores: the oracle (FP64 restatement
+    of the importance-sampled method; uniform start points unless nearField)
+    runs the same adaptive solve to the threshold on all host threads,
+    `cores` consecutive samples from a random position at a time -- each
+    chunk on the next of `fields` (beta per prism) when given -- bounded in
+    time (at least one chunk)."""
     import numpy as np
 
     from oracle import oracle
@@ -116,18 +123,36 @@ def cpu_baseline(workload, seconds):
     rng = np.random.default_rng(1)
     rays = 0
     n_samples = 0
+    chunks = 0
     t0 = time.perf_counter()
     while n_samples == 0 or time.perf_counter() - t0 < seconds:
         first = int(rng.integers(0, S - cores))
-        r = oracle.phi_ase(w.mesh, (sa, se), minRays=w.minRays, maxRays=w.maxRays, adaptiveSteps=w.adaptiveSteps,
+        mesh = w.mesh if fields is None else w.mesh.withBeta(fields[chunks % len(fields)])
+        r = oracle.phi_ase(mesh, (sa, se), minRays=w.minRays, maxRays=w.maxRays, adaptiveSteps=w.adaptiveSteps,
                            mseThreshold=w.threshold, useReflections=w.useReflections, seed=7, minSample=first,
-                           maxSample=first + cores - 1, threads=cores)
+                           maxSample=first + cores - 1, threads=cores, nearField=nearField)
         rays += int(r["totalRays"].astype(np.int64).sum())
         n_samples += cores
+        chunks += 1
     dt = time.perf_counter() - t0
+    estimator = ("importance weights, near-field start points" if nearField else
+                 "the reference's estimator: importance weights, uniform start points")
+    where = f"{min(chunks, len(fields))} of the unseen pump fields" if fields is not None else f"{w.name}"
     return {"value": n_samples / dt, "unit": "samples/s", "rays_per_s": rays / dt, "cores": cores, "kind": "port",
-            "sample": f"{n_samples} samples solved to relative error <= {w.threshold} "
-                      f"({rays} rays, importance included), {dt:.1f} s on {cores} threads"}
+            "sample": f"{n_samples} samples of {where} solved to relative error <= {w.threshold} "
+                      f"(rays {w.minRays}-{w.maxRays}, {rays} rays, {estimator}, importance walks included), "
+                      f"{dt:.1f} s on {cores} threads"}
+
+
+def learned_config(w, mesh, n_gpus):
+    """The learned workload's config (both arms): what is solved, not how."""
+    return {"workload": "learned proposal (config 4): disc_small geometry, 32 training pump fields, "
+                        "unseen evaluation pump fields",
+            "samples_per_step_per_gpu": mesh.numberOfSamples, "triangles": mesh.numberOfTriangles,
+            "levels": mesh.numberOfLevels, "prisms": mesh.numberOfPrisms, "wavelengths": 1,
+            "rays_per_sample": [w.minRays, w.maxRays], "threshold": w.threshold,
+            "adaptive_steps": w.adaptiveSteps, "parallelism": f"independent fields x{n_gpus}",
+            "l2": "flushed (256 MiB write) before every timed step"}
 
 
 class ClockSampler:
@@ -290,6 +315,9 @@ def measure_importance(args, local, rank=0, world=1, nested=False):
     e2e_s = time.perf_counter() - t1
     ctx.update_beta(mesh.betaVolume)
 
+    # crossings of the timed steps' importance walks (an instrumented copy of the kernel, untimed)
+    imp_crossings = sum(ctx.importance_crossings(((args.warmup + s) * world + rank) * B % (S - B + 1), B,
+                                                 w.useReflections) for s in range(args.steps))
     # the plain method (uniform start points, as the legacy code) on one batch, for comparison
     plain = ctx.calc_phi_ase(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold,
                              useReflections=w.useReflections, monochromatic=w.monochromatic,
@@ -369,6 +397,17 @@ def measure_importance(args, local, rank=0, world=1, nested=False):
                          "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
                          "traffic": None, "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
                          "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
+            "importance_roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather",
+                                    "kernel": "importanceTeamKernel" if tuned.importanceLayers == 0
+                                    else f"importanceKernel<{tuned.importanceLayers}>",
+                                    "achieved": imp_crossings / (imp_ms * 1e-3), "peak": roof, "unit": "crossings/s",
+                                    "frac": imp_crossings / (imp_ms * 1e-3) / roof,
+                                    "fp32_issue_frac": imp_crossings / (imp_ms * 1e-3) / r_fp32,
+                                    "crossings_per_step": imp_crossings / args.steps,
+                                    "ms_per_step": imp_ms / args.steps,
+                                    "walks_per_step": B * mesh.numberOfPrisms * (5 if w.useReflections else 1),
+                                    "note": "crossings: per (sample, slice, prism) line, triangles crossed by its "
+                                            "2-D projection plus level planes and reflections (in-kernel counter)"},
             "clocks": clocks,
             "wall_s": wall,
         }
@@ -965,7 +1004,10 @@ def run_learned(args):
         lv = np.concatenate([LP.per_ray_variance(r) for r in acc["learned"]])
         pv = np.concatenate([LP.per_ray_variance(r) for r in acc["plain"]])
         nv = np.concatenate([LP.per_ray_variance(r) for r in acc["nearfield"]])
-        cpu = cpu_baseline(w, args.cpu_seconds) if world == 1 else None
+        cpu = cpu_baseline(w, args.cpu_seconds, fields=fields[args.warmup:]) if world == 1 else None
+        l1 = _native.l1_bandwidth(local)
+        smem = _native.l1_bandwidth(local, shared=True)
+        r_l1 = l1 * 1e9 / BYTES_PER_CROSSING
         line = {
             "metric": LEARNED_METRIC,
             "value": solved_all / (ms_l * 1e-3),
@@ -979,16 +1021,9 @@ def run_learned(args):
             "vs_baseline": None,
             "dtype": "f32 geometry, f64 sums, bf16 proposal network (f32 accumulation)",
             "data": "synthetic (seeded gain media and pump fields, no dataset)",
-            "config": {"workload": "learned proposal (config 4): disc_small geometry, 32 training pump fields, "
-                                   "unseen evaluation pump fields",
-                       "samples_per_step_per_gpu": S, "triangles": mesh.numberOfTriangles,
-                       "levels": mesh.numberOfLevels, "prisms": mesh.numberOfPrisms, "wavelengths": 1,
-                       "rays_per_sample": [w.minRays, w.maxRays], "threshold": w.threshold,
-                       "adaptive_steps": w.adaptiveSteps, "parallelism": f"independent fields x{world}",
-                       "ray_kernel": {"variant": tuned.name, "rays_per_lane": tuned.raysPerThread,
-                                      "importance_layers": tuned.importanceLayers,
-                                      "autotuned_over": len(tuned.table)},
-                       "l2": "flushed (256 MiB write) before every timed step"},
+            "config": learned_config(w, mesh, world),
+            "ray_kernel": {"variant": tuned.name, "rays_per_lane": tuned.raysPerThread,
+                           "importance_layers": tuned.importanceLayers, "autotuned_over": len(tuned.table)},
             "time_to_threshold_ms": ms_l / args.steps,
             "plain_is": {"value": solved_all / (ms_p * 1e-3), "unit": "samples/s", "ms_per_step": ms_p / args.steps,
                          "rays": a["plain"]["rays"], "unconverged_samples": a["plain"]["unconverged"],
@@ -1015,13 +1050,16 @@ def run_learned(args):
             "e2e": {"value": solved_all / e2e_max, "unit": "samples/s", "h2d_bytes_per_step": mesh.numberOfPrisms * 8,
                     "d2h_bytes_per_step": S * (4 + 8 + 8 + 4 + 8 + 4)},
             "gpu_launches": a["learned"]["launches"],
-            "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": "rayKernel",
+            "roofline": {"bound": "fp32_issue" if r_fp32 <= r_l2 else "l2_gather", "kernel": tuned.name,
                          "achieved": achieved, "peak": roof, "unit": "crossings/s", "frac": achieved / roof,
                          "traffic": RAY_TRAFFIC_LEARNED,
                          "traffic_note": "DRAM bytes per launch (ncu): the per-sample ray maps read once and the "
                                          "per-item partial sums; the walk tables stay in L1 (99 % hits) and L2",
-                         "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2,
-                         "l2_read_gbs_live": l2, "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
+                         "fp32_issue_peak": r_fp32, "l2_gather_peak": r_l2, "l1_gather_peak": r_l1,
+                         "fp32_issue_frac": achieved / r_fp32, "l1_gather_frac": achieved / r_l1,
+                         "l2_read_gbs_live": l2, "l1_read_gbs_live": l1, "smem_read_gbs_live": smem,
+                         "binding": RAY_BINDING_LEARNED, "ncu_thread_instructions": RAY_INSTR_LEARNED,
+                         "clock_mhz": f_clk / 1e6, "peak_source": peak_kind},
             "proposal_roofline": {"bound": "xu", "kernel": "proposalKernel",
                                   "achieved": rows / (a["learned"]["proposal_ms"] * 1e-3),
                                   "peak": SMS * XU_LANES_PER_SM * f_clk / XU_INSTR_PER_PAIR, "unit": "pairs/s",
@@ -1037,7 +1075,8 @@ def run_learned(args):
         if disc_poly is not None:
             line["importance_disc_poly"] = {k: disc_poly[k] for k in (
                 "value", "unit", "ms_per_step", "config", "time_to_threshold_ms", "breakdown_ms_per_step",
-                "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline")}
+                "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline",
+                "importance_roofline")}
         if fwd is not None:
             line["forward_tet4"] = fwd
         if pulse_line is not None:
@@ -1066,26 +1105,42 @@ def run_learned(args):
 
 
 def run_reference(args):
+    """The reference arm: the reference's method (importance weights, uniform
+    start points) in its CPU restatement, the oracle, on all host threads
+    (rank 0 only), on the same workload as this build's arm.  For the learned
+    workload each step solves a bounded sample of the sample points of the
+    same unseen evaluation pump field this build's rank 0 solves in that
+    step, with the same rays and threshold, and the line carries this build's
+    config."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    from haseongpu_b200.configs import WORKLOADS
+    from haseongpu_b200.configs import WORKLOADS, disc_small
 
-    # the learned workload's reference: the reference's method (importance
-    # weights, uniform start points) on its geometry
-    w = WORKLOADS["disc_small" if args.workload == "learned" else args.workload]()
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
-    for _ in range(args.warmup):
-        cpu_baseline(w, 0.0)
-    vals = [cpu_baseline(w, per_step) for _ in range(args.steps)]
+    if args.workload == "learned":
+        from haseongpu_b200 import learned as LP
+
+        w = disc_small()
+        fields = LP.pump_fields(w.mesh, args.warmup + args.steps, LP.EVAL_SEED)
+        for k in range(args.warmup):
+            cpu_baseline(w, 0.0, fields=[fields[k]])
+        vals = [cpu_baseline(w, per_step, fields=[fields[args.warmup + k]]) for k in range(args.steps)]
+        config, metric = learned_config(w, w.mesh, args.gpus), LEARNED_METRIC
+    else:
+        w = WORKLOADS[args.workload]()
+        for _ in range(args.warmup):
+            cpu_baseline(w, 0.0)
+        vals = [cpu_baseline(w, per_step) for _ in range(args.steps)]
+        config, metric = {"workload": w.name, "threshold": w.threshold, "reflections": w.useReflections}, METRIC
     value = statistics.median(v["value"] for v in vals)
     cores = vals[0]["cores"]
     line = {
-        "metric": LEARNED_METRIC if args.workload == "learned" else METRIC, "value": value, "unit": "samples/s",
+        "metric": metric, "value": value, "unit": "samples/s",
         "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded gain medium, no dataset)", "impl": "reference",
-        "config": {"workload": w.name, "threshold": w.threshold, "reflections": w.useReflections},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded gain medium and pump fields, no dataset)",
+        "impl": "reference", "config": config,
         "rays_per_s": statistics.median(v["rays_per_s"] for v in vals),
         "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port",
                          "sample": vals[0]["sample"]},

@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "hase_trace_rays",
     "hase_philox",
     "hase_probe_l2_bandwidth",
+    "hase_probe_l1_bandwidth",
     "hase_estimate_sample_noalloc",
     "hase_simulate",
     # include/hase_b200_forward.h
@@ -268,6 +269,7 @@ class TimeDesc(C.Structure):
         ("pumpSteps", C.c_uint32),
         ("aseSteps", C.c_uint32),
         ("integrator", C.c_uint32),
+        ("implicitIterations", C.c_uint32),
     ]
 
 
@@ -354,6 +356,7 @@ def lib():
                                       _f32p, _f32p, _u32p]
         L.hase_philox.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
         L.hase_probe_l2_bandwidth.argtypes = [C.c_int, C.c_uint64, C.c_uint32, _f64p]
+        L.hase_probe_l1_bandwidth.argtypes = [C.c_int, C.c_uint32, C.c_uint32, _f64p]
         L.hase_estimate_sample_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                                    C.c_uint32, C.c_uint32, C.c_void_p]
         _i32p = C.POINTER(C.c_int32)
@@ -424,6 +427,13 @@ def l2_bandwidth(device=0, bytes_=48 << 20, reps=40) -> float:
     """Measured L2 read bandwidth (GB/s) of `device`."""
     out = C.c_double(0.0)
     check(lib().hase_probe_l2_bandwidth(int(device), int(bytes_), int(reps), C.byref(out)))
+    return out.value
+
+
+def l1_bandwidth(device=0, shared=False, reps=2000) -> float:
+    """Measured L1 (or shared-memory) read bandwidth (GB/s) of `device`."""
+    out = C.c_double(0.0)
+    check(lib().hase_probe_l1_bandwidth(int(device), 1 if shared else 0, int(reps), C.byref(out)))
     return out.value
 
 

@@ -1334,6 +1334,47 @@ __global__ void __launch_bounds__(512) l2ProbeKernel(const float4* __restrict__ 
     if (acc == 1234.5f) *sink = acc;  // keeps the loads; never true for a zeroed buffer
 }
 
+// L1 and shared-memory read bandwidth probes: every block reads the same
+// 32 KB (which stays resident in each SM's L1, or in the block's shared
+// memory) `reps` times with 16-byte loads.  The loads are volatile inline
+// PTX, so none is hoisted out of the repeat loop.
+constexpr uint32_t kProbeVec = 2048;  // float4 elements: 32 KB
+__global__ void __launch_bounds__(1024) l1ProbeKernel(const float4* __restrict__ buf, uint32_t reps, float* sink) {
+    float a = 0.0f, b = 0.0f, c = 0.0f, d = 0.0f;
+    for (uint32_t r = 0; r < reps; ++r)
+        for (uint32_t i = threadIdx.x; i < kProbeVec; i += blockDim.x) {
+            float x, y, z, w;
+            asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(x), "=f"(y), "=f"(z), "=f"(w)
+                         : "l"(buf + i));
+            a += x;
+            b += y;
+            c += z;
+            d += w;
+        }
+    if (a + b + c + d == 1234.5f) *sink = a;  // never true for a zeroed buffer
+}
+
+__global__ void __launch_bounds__(1024) smemProbeKernel(uint32_t reps, float* sink) {
+    __shared__ float4 buf[kProbeVec];
+    for (uint32_t i = threadIdx.x; i < kProbeVec; i += blockDim.x) buf[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    __syncthreads();
+    float a = 0.0f, b = 0.0f, c = 0.0f, d = 0.0f;
+    for (uint32_t r = 0; r < reps; ++r)
+        for (uint32_t i = threadIdx.x; i < kProbeVec; i += blockDim.x) {
+            float x, y, z, w;
+            const uint32_t addr = uint32_t(__cvta_generic_to_shared(buf + i));
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(x), "=f"(y), "=f"(z), "=f"(w)
+                         : "r"(addr));
+            a += x;
+            b += y;
+            c += z;
+            d += w;
+        }
+    if (a + b + c + d == 1234.5f) *sink = a;
+}
+
 // ------------------------------------------- allocation-free estimate ----
 // Scratch of hase_estimate_sample_noalloc: a file-scope device array, so that
 // entry point never allocates.  Every GPU that loads this library holds it
@@ -1596,29 +1637,73 @@ __global__ void phiPrismKernel(const int4* verts, const float* phiSample, float*
     phiPrism[p] = (a[v.x] + a[v.y] + a[v.z] + b[v.x] + b[v.y] + b[v.z]) * (1.0f / 6.0f);
 }
 
-// k = pump - [beta (sE + sA) - sA] Phi - beta / tau (0 in cladding); then the
-// stage update: next = beta0 + cStage dt k, acc += wStage k.
-__global__ void rateStageKernel(const double* beta0, const double* betaStage, const double* pumpRate,
-                                const float* phiPrism, const uint8_t* clad, double* next, double* acc, uint32_t P,
-                                double sA, double sE, double tau, double dt, double cStage, double wStage,
-                                int first) {
+// Time integrators of hase_simulate (include/core/timeSteppedSimulation.hpp:321-415).
+enum TimeIntegrator : uint32_t {
+    kFrozenRk4 = 0,      // frozen-phi-ase-runge-kutta-4: phi-ASE solved at the step start only
+    kExplicitEuler = 1,  // explicit-euler
+    kHeun = 2,           // heun: phi-ASE re-solved at the predictor
+    kMidpoint = 3,       // midpoint: phi-ASE re-solved at the midpoint
+    kRk4 = 4,            // runge-kutta-4: phi-ASE re-solved at every stage
+    kImplicitEuler = 5,  // implicit-euler: fixed-point iterations, phi-ASE re-solved on each
+    kExpEuler = 6,       // exponential-euler
+    kNumIntegrators = 7,
+};
+
+// Derivative of beta at state b (include/kernels/derivativeComposition.hpp:27-63):
+// k = pump - [b (sE + sA) - sA] Phi - b / tau, 0 in cladding prisms.
+__global__ void rateDerivativeKernel(const double* b, const double* pumpRate, const float* phiPrism,
+                                     const uint8_t* clad, double* k, uint32_t P, double sA, double sE, double tau) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
-    double k = 0.0;
+    double v = 0.0;
     if (!(clad && clad[p])) {
-        const double b = betaStage[p];
-        k = pumpRate[p] - (b * (sE + sA) - sA) * double(phiPrism ? phiPrism[p] : 0.0f) - b / tau;
+        const double bp = b[p];
+        v = pumpRate[p] - (bp * (sE + sA) - sA) * double(phiPrism ? phiPrism[p] : 0.0f) - bp / tau;
     }
-    next[p] = beta0[p] + cStage * dt * k;
-    acc[p] = first ? wStage * k : acc[p] + wStage * k;
+    k[p] = v;
 }
 
-// beta += dt * (weighted stage derivatives), clipped to [0, 1] as the
-// reference clips after every update (include/kernels/timeIntegrationUpdateKernels.hpp:93-105,
-// include/core/timeSteppedSimulation.hpp:579-586).
-__global__ void rateFinishKernel(double* beta, const double* acc, uint32_t P, double dt) {
+// out = base + a k (a stage state, not clipped; AddScaled).
+__global__ void rateAxpyKernel(const double* base, const double* k, double a, double* out, uint32_t P) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < P) beta[p] = fmin(1.0, fmax(0.0, beta[p] + dt * acc[p]));
+    if (p < P) out[p] = base[p] + a * k[p];
+}
+
+// The step's update from its stage derivatives k[0 .. 3] ([4][P]) in the
+// reference's forms (AddScaled, CombineHeun, CombineRungeKutta4), clipped to
+// [0, 1] (ClipBeta): include/kernels/timeIntegrationUpdateKernels.hpp:21-105.
+__global__ void rateCombineKernel(const double* base, const double* k, uint32_t mode, double dt, double* out,
+                                  uint32_t P) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const double* k1 = k;
+    const double* k2 = k + P;
+    const double* k3 = k + 2 * size_t(P);
+    const double* k4 = k + 3 * size_t(P);
+    double v;
+    switch (mode) {
+        case kHeun: v = base[p] + 0.5 * dt * (k1[p] + k2[p]); break;
+        case kMidpoint: v = base[p] + dt * k2[p]; break;
+        case kFrozenRk4:
+        case kRk4: v = base[p] + (dt / 6.0) * (k1[p] + 2.0 * k2[p] + 2.0 * k3[p] + k4[p]); break;
+        default: v = base[p] + dt * k1[p]; break;  // explicit and implicit Euler
+    }
+    out[p] = fmin(1.0, fmax(0.0, v));
+}
+
+// Exponential Euler (ExponentialEulerUpdate, include/kernels/timeIntegrationUpdateKernels.hpp:67-90):
+// out = tau (pump - ASE term) (1 - e^{-dt/tau}) + b e^{-dt/tau}, the pump and
+// ASE terms 0 in cladding prisms, clipped to [0, 1].
+__global__ void rateExpEulerKernel(const double* b, const double* pumpRate, const float* phiPrism,
+                                   const uint8_t* clad, double* out, uint32_t P, double sA, double sE, double tau,
+                                   double dt) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const double decay = exp(-dt / tau);
+    const double bp = b[p];
+    double source = 0.0;
+    if (!(clad && clad[p])) source = pumpRate[p] - (bp * (sE + sA) - sA) * double(phiPrism ? phiPrism[p] : 0.0f);
+    out[p] = fmin(1.0, fmax(0.0, tau * source * (1.0 - decay) + bp * decay));
 }
 
 // The context's walk / source beta from the FP64 state (NaN marks cladding in the walk table).
@@ -2429,7 +2514,7 @@ hase_status simulateCore(hase_context* c, double sA, double sE, AseSource& sourc
                          const hase_time_desc* td, hase_time_result* res, std::vector<double>& betaHost) {
     if (!c || !pd || !td || !res) return fail(HASE_INVALID_ARGUMENT, "null argument");
     if (!(td->timeStep > 0.0) || td->steps == 0) return fail(HASE_INVALID_ARGUMENT, "timeStep and steps must be positive");
-    if (td->integrator > 1) return fail(HASE_INVALID_ARGUMENT, "integrator must be 0 (frozen-ASE RK4) or 1 (Euler)");
+    if (td->integrator >= kNumIntegrators) return fail(HASE_INVALID_ARGUMENT, "integrator must be 0 .. 6");
     if (td->aseSteps > td->steps) return fail(HASE_INVALID_ARGUMENT, "aseSteps > steps");
     if (!(pd->radius > 0.0) || !(pd->exponent > 0.0) || !(pd->wavelength > 0.0) || !(pd->peakIntensity >= 0.0) ||
         !(pd->sigmaA >= 0.0) || !(pd->sigmaE >= 0.0))
@@ -2439,13 +2524,13 @@ hase_status simulateCore(hase_context* c, double sA, double sE, AseSource& sourc
     std::vector<uint8_t> clad(P, 0);
     if (!c->cladTypes.empty())
         for (uint32_t p = 0; p < P; ++p) clad[p] = c->cladTypes[p % T] == c->cladNumber ? 1 : 0;
-    DevBuf<double> beta0, stage, nextB, acc, rate, absorbed;
+    DevBuf<double> beta0, stage, nextB, kb, rate, absorbed;
     DevBuf<float> phiP, area;
     DevBuf<uint8_t> dclad;
     HASE_CUDA(beta0.ensure(P));
     HASE_CUDA(stage.ensure(P));
     HASE_CUDA(nextB.ensure(P));
-    HASE_CUDA(acc.ensure(P));
+    HASE_CUDA(kb.ensure(4 * size_t(P)));
     HASE_CUDA(rate.ensure(P));
     HASE_CUDA(absorbed.ensure(1));
     HASE_CUDA(phiP.ensure(P));
@@ -2494,68 +2579,166 @@ hase_status simulateCore(hase_context* c, double sA, double sE, AseSource& sourc
         return n ? sum / n : 0.0;
     };
     if (res->meanBeta) res->meanBeta[0] = meanGain(c->hBeta);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    HASE_CUDA(cudaEventCreate(&e0));
-    if (cudaEventCreate(&e1) != cudaSuccess) {
-        cudaEventDestroy(e0);
-        return fail(HASE_CUDA_ERROR, "event creation failed");
-    }
-    struct Ev {
-        cudaEvent_t a, b;
-        ~Ev() {
-            cudaEventDestroy(a);
-            cudaEventDestroy(b);
-        }
-    } evs{e0, e1};
+    uint32_t solveIndex = 0;  // phi-ASE solves so far (the index of phiHistory)
     const uint32_t blocksP = (P + 255) / 256, blocksT = (T + 255) / 256;
     const double dt = td->timeStep;
+    const uint32_t method = td->integrator;
+    const uint32_t implicitIterations = std::max(1u, td->implicitIterations ? td->implicitIterations : 8u);
     hase_status worst = HASE_OK;
+    // device timing of the pump / derivative / update kernels: one event pair
+    // per group of launches between phi-ASE solves, read after each step
+    std::vector<cudaEvent_t> evPool;
+    struct EvPool {
+        std::vector<cudaEvent_t>& v;
+        ~EvPool() {
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
+        }
+    } evPoolOwner{evPool};
+    size_t evUsed = 0;
+    auto nextEvent = [&](cudaEvent_t& e) -> hase_status {
+        if (evUsed == evPool.size()) {
+            cudaEvent_t n = nullptr;
+            HASE_CUDA(cudaEventCreate(&n));
+            evPool.push_back(n);
+        }
+        e = evPool[evUsed++];
+        return HASE_OK;
+    };
+    // tables of the walks (device) and host copies of beta (the learned
+    // proposal's features, the forward twin) set to the state `b`
+    auto setState = [&](const double* b) -> hase_status {
+        betaToTablesKernel<<<blocksP, 256, 0, c->stream>>>(b, dclad.p, c->gainBeta.p, c->srcBeta.p, P);
+        HASE_CUDA(cudaGetLastError());
+        HASE_CUDA(cudaMemcpyAsync(betaHost.data(), b, P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        HASE_CUDA(cudaStreamSynchronize(c->stream));
+        c->hBeta = betaHost;
+        for (uint32_t p = 0; p < P; ++p) c->hGainBeta[p] = clad[p] ? NAN : float(betaHost[p]);
+        ++c->betaVersion;  // the learned proposal's feature grid follows the new beta
+        return HASE_OK;
+    };
     for (uint32_t step = 0; step < td->steps; ++step) {
         const bool ase = step < td->aseSteps, pumpOn = step < td->pumpSteps;
-        if (ase) {
+        bool firstSolve = true, firstPump = true, tablesAtStart = true;
+        evUsed = 0;
+        if (res->meanPhi) res->meanPhi[step] = 0.0;
+        HASE_CUDA(cudaMemsetAsync(absorbed.p, 0, sizeof(double), c->stream));
+        // phi-ASE of the state `b` (phiP), solved when `refresh` (otherwise the
+        // step's last solve stays in use, the frozen-ASE stages)
+        auto solveAt = [&](const double* b, bool refresh) -> hase_status {
+            if (!ase || !refresh) return HASE_OK;
+            if (b != beta0.p || !tablesAtStart) {
+                HASE_TRY(setState(b));
+                tablesAtStart = b == beta0.p;
+            }
             double ms = 0.0, mp = 0.0;
             uint64_t rays = 0;
-            const hase_status st = source.solve(step, phiP.p, ms, rays, mp);
+            const hase_status st = source.solve(solveIndex, phiP.p, ms, rays, mp);
             if (st != HASE_OK && st != HASE_NOT_CONVERGED && st != HASE_DROPPED_RAYS) return st;
             if (st != HASE_OK && worst == HASE_OK) worst = st;
+            ++solveIndex;
             res->aseMilliseconds += ms;
             res->totalMilliseconds += ms;
             res->raysTraced += rays;
-            if (res->meanPhi) res->meanPhi[step] = mp;
-        } else if (res->meanPhi) {
-            res->meanPhi[step] = 0.0;
-        }
-        HASE_CUDA(cudaEventRecord(e0, c->stream));
-        HASE_CUDA(cudaMemsetAsync(absorbed.p, 0, sizeof(double), c->stream));
-        const int stages = td->integrator == 0 ? 4 : 1;
-        const double cNext[4] = {0.5, 0.5, 1.0, 0.0};
-        const double wStage[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
-        const double* cur = beta0.p;
-        for (int sIdx = 0; sIdx < stages; ++sIdx) {
+            if (firstSolve && res->meanPhi) res->meanPhi[step] = mp;
+            firstSolve = false;
+            return HASE_OK;
+        };
+        // pump rate of the state `b` (the absorbed power of the step's first evaluation)
+        auto pumpAt = [&](const double* b) -> hase_status {
             HASE_CUDA(cudaMemsetAsync(rate.p, 0, P * sizeof(double), c->stream));
             if (pumpOn) {
-                pl.beta = cur;
-                pl.absorbed = sIdx == 0 ? absorbed.p : nullptr;
+                pl.beta = b;
+                pl.absorbed = firstPump ? absorbed.p : nullptr;
                 pumpColumnKernel<<<blocksT, 256, 0, c->stream>>>(pl);
             }
-            double* out = (sIdx % 2 == 0) ? stage.p : nextB.p;
-            rateStageKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, cur, rate.p, ase ? phiP.p : nullptr, dclad.p, out,
-                                                         acc.p, P, sA, sE, c->tau, dt, cNext[sIdx],
-                                                         stages == 1 ? 1.0 : wStage[sIdx], sIdx == 0 ? 1 : 0);
-            cur = out;
+            firstPump = false;
+            return HASE_OK;
+        };
+        // k[idx] = derivative at `b`, phi-ASE re-solved there when `refresh`
+        auto evaluate = [&](const double* b, uint32_t idx, bool refresh) -> hase_status {
+            HASE_TRY(solveAt(b, refresh));
+            cudaEvent_t ea, eb;
+            HASE_TRY(nextEvent(ea));
+            HASE_TRY(nextEvent(eb));
+            HASE_CUDA(cudaEventRecord(ea, c->stream));
+            HASE_TRY(pumpAt(b));
+            rateDerivativeKernel<<<blocksP, 256, 0, c->stream>>>(b, rate.p, ase ? phiP.p : nullptr, dclad.p,
+                                                                kb.p + size_t(idx) * P, P, sA, sE, c->tau);
+            HASE_CUDA(cudaGetLastError());
+            HASE_CUDA(cudaEventRecord(eb, c->stream));
+            return HASE_OK;
+        };
+        auto axpy = [&](const double* base, uint32_t idx, double a, double* out) -> hase_status {
+            rateAxpyKernel<<<blocksP, 256, 0, c->stream>>>(base, kb.p + size_t(idx) * P, a, out, P);
+            return cudaGetLastError() == cudaSuccess ? HASE_OK : fail(HASE_CUDA_ERROR, "stage update failed");
+        };
+        // the step, in the reference's stage order (include/core/timeSteppedSimulation.hpp:321-415)
+        switch (method) {
+            case kExplicitEuler:
+                HASE_TRY(evaluate(beta0.p, 0, true));
+                break;
+            case kHeun:
+                HASE_TRY(evaluate(beta0.p, 0, true));
+                HASE_TRY(axpy(beta0.p, 0, dt, stage.p));
+                HASE_TRY(evaluate(stage.p, 1, true));
+                break;
+            case kMidpoint:
+                HASE_TRY(evaluate(beta0.p, 0, true));
+                HASE_TRY(axpy(beta0.p, 0, 0.5 * dt, stage.p));
+                HASE_TRY(evaluate(stage.p, 1, true));
+                break;
+            case kFrozenRk4:
+            case kRk4: {
+                const bool re = method == kRk4;
+                HASE_TRY(evaluate(beta0.p, 0, true));
+                HASE_TRY(axpy(beta0.p, 0, 0.5 * dt, stage.p));
+                HASE_TRY(evaluate(stage.p, 1, re));
+                HASE_TRY(axpy(beta0.p, 1, 0.5 * dt, nextB.p));
+                HASE_TRY(evaluate(nextB.p, 2, re));
+                HASE_TRY(axpy(beta0.p, 2, dt, stage.p));
+                HASE_TRY(evaluate(stage.p, 3, re));
+                break;
+            }
+            case kImplicitEuler: {
+                // stage = beta; repeat: stage = beta + dt k(stage), phi-ASE re-solved each time
+                const double* cur = beta0.p;
+                for (uint32_t it = 0; it < implicitIterations; ++it) {
+                    HASE_TRY(evaluate(cur, 0, true));
+                    double* out = (it % 2 == 0) ? stage.p : nextB.p;
+                    HASE_TRY(axpy(beta0.p, 0, dt, out));
+                    cur = out;
+                }
+                break;
+            }
+            default:  // kExpEuler
+                HASE_TRY(solveAt(beta0.p, true));
+                break;
         }
-        rateFinishKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, acc.p, P, dt);
+        cudaEvent_t ea, eb;
+        HASE_TRY(nextEvent(ea));
+        HASE_TRY(nextEvent(eb));
+        HASE_CUDA(cudaEventRecord(ea, c->stream));
+        if (method == kExpEuler) {
+            HASE_TRY(pumpAt(beta0.p));
+            rateExpEulerKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, rate.p, ase ? phiP.p : nullptr, dclad.p,
+                                                              nextB.p, P, sA, sE, c->tau, dt);
+        } else {
+            rateCombineKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, kb.p, method, dt, nextB.p, P);
+        }
+        HASE_CUDA(cudaMemcpyAsync(beta0.p, nextB.p, P * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         betaToTablesKernel<<<blocksP, 256, 0, c->stream>>>(beta0.p, dclad.p, c->gainBeta.p, c->srcBeta.p, P);
         HASE_CUDA(cudaGetLastError());
-        HASE_CUDA(cudaEventRecord(e1, c->stream));
+        HASE_CUDA(cudaEventRecord(eb, c->stream));
         double abs = 0.0;
         HASE_CUDA(cudaMemcpyAsync(&abs, absorbed.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         HASE_CUDA(cudaMemcpyAsync(betaHost.data(), beta0.p, P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         HASE_CUDA(cudaStreamSynchronize(c->stream));
-        float ms = 0.0f;
-        HASE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        res->pumpMilliseconds += ms;
-        res->totalMilliseconds += ms;
+        for (size_t e = 0; e + 1 < evUsed; e += 2) {
+            float ms = 0.0f;
+            HASE_CUDA(cudaEventElapsedTime(&ms, evPool[e], evPool[e + 1]));
+            res->pumpMilliseconds += ms;
+            res->totalMilliseconds += ms;
+        }
         if (res->pumpAbsorbed) res->pumpAbsorbed[step] = pumpOn && incident > 0.0 ? abs / incident : 0.0;
         // host copies the next solve's features read
         c->hBeta = betaHost;
@@ -2988,6 +3171,43 @@ hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, d
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *gbPerSecond = double(n) * 16.0 * reps / (double(ms) * 1e-3) / 1e9;
+    return HASE_OK;
+}
+
+hase_status hase_probe_l1_bandwidth(int device, uint32_t sharedMemory, uint32_t reps, double* gbPerSecond) {
+    if (!gbPerSecond || reps == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(HASE_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return fail(HASE_INVALID_ARGUMENT, "device out of range");
+    HASE_CUDA(cudaSetDevice(device));
+    DevBuf<float4> buf;
+    DevBuf<float> sink;
+    HASE_CUDA(buf.ensure(kProbeVec));
+    HASE_CUDA(sink.ensure(1));
+    HASE_CUDA(cudaMemset(buf.p, 0, kProbeVec * sizeof(float4)));
+    int sms = 0;
+    HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const uint32_t blocks = uint32_t(sms) * 2;  // two 1024-thread blocks per SM
+    cudaEvent_t e0, e1;
+    HASE_CUDA(cudaEventCreate(&e0));
+    HASE_CUDA(cudaEventCreate(&e1));
+    for (int pass = 0; pass < 2; ++pass) {  // the first pass warms the caches and the clocks
+        const uint32_t r = pass == 0 ? 1u : reps;
+        HASE_CUDA(cudaEventRecord(e0));
+        if (sharedMemory) smemProbeKernel<<<blocks, 1024>>>(r, sink.p);
+        else l1ProbeKernel<<<blocks, 1024>>>(buf.p, r, sink.p);
+        HASE_CUDA(cudaEventRecord(e1));
+        HASE_CUDA(cudaGetLastError());
+    }
+    HASE_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    HASE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *gbPerSecond = double(blocks) * kProbeVec * 16.0 * reps / (double(ms) * 1e-3) / 1e9;
     return HASE_OK;
 }
 

@@ -67,6 +67,30 @@ class Result:
         return self.relativeStandardError
 
 
+# The reference's time integrators (pyInclude/openpmd/transport.py:1719-1727) and their
+# hase_time_desc.integrator codes.
+TIME_INTEGRATORS = {"frozen-phi-ase-runge-kutta-4": 0, "explicit-euler": 1, "heun": 2, "midpoint": 3,
+                    "runge-kutta-4": 4, "implicit-euler": 5, "exponential-euler": 6}
+
+
+def time_integrator(name) -> int:
+    """The integrator code of a reference integrator name (or a code)."""
+    if isinstance(name, str):
+        if name not in TIME_INTEGRATORS:
+            raise ValueError(f"unknown time integrator {name!r}; known: {', '.join(TIME_INTEGRATORS)}")
+        return TIME_INTEGRATORS[name]
+    code = int(name)
+    if not 0 <= code < len(TIME_INTEGRATORS):
+        raise ValueError(f"integrator code {code} outside 0 .. {len(TIME_INTEGRATORS) - 1}")
+    return code
+
+
+def solves_per_step(integrator, implicitIterations=0) -> int:
+    """phi-ASE solves of one time step with phi-ASE on: the stages that re-solve it."""
+    code = time_integrator(integrator)
+    return {2: 2, 3: 2, 4: 4, 5: max(1, int(implicitIterations) or 8)}.get(code, 1)
+
+
 class DeviceMesh:
     """A libhase_b200 context: the mesh tables resident on one device."""
 
@@ -177,12 +201,14 @@ class DeviceMesh:
                         float(pump.get("centerX", 0.0)), float(pump.get("centerY", 0.0)), float(pump["wavelength"]),
                         float(pump["sigmaA"]), float(pump["sigmaE"]), 1 if pump.get("retroreflect", True) else 0)
         steps = int(time["steps"])
+        integrator = time_integrator(time.get("integrator", 0))
+        iterations = int(time.get("implicitIterations", 0))
         td = N.TimeDesc(float(time["timeStep"]), steps, int(time.get("pumpSteps", steps)),
-                        int(time.get("aseSteps", steps)), int(time.get("integrator", 0)))
+                        int(time.get("aseSteps", steps)), integrator, iterations)
         out = {"betaVolume": np.empty(P), "meanBeta": np.empty(steps + 1), "meanPhi": np.empty(steps),
                "pumpAbsorbed": np.empty(steps)}
         if keepPhi:
-            out["phiHistory"] = np.empty((td.aseSteps, width), np.float32)
+            out["phiHistory"] = np.empty((td.aseSteps * solves_per_step(integrator, iterations), width), np.float32)
         r = N.TimeResultDesc(N.ptr(out["betaVolume"], N._f64p), N.ptr(out["meanBeta"], N._f64p),
                              N.ptr(out["meanPhi"], N._f64p), N.ptr(out["pumpAbsorbed"], N._f64p),
                              N.ptr(out.get("phiHistory"), N._f32p))

@@ -225,7 +225,12 @@ typedef struct {
     uint32_t steps;             /* simulation steps */
     uint32_t pumpSteps;         /* steps with the pump on, from the first */
     uint32_t aseSteps;          /* steps with a phi-ASE solve, from the first (0: pump and fluorescence only) */
-    uint32_t integrator;        /* 0: RK4 with the step's phi-ASE frozen (FrozenPhiAseRungeKutta4), 1: explicit Euler */
+    uint32_t integrator;        /* the reference's time integrators (include/core/timeSteppedSimulation.hpp:321-415):
+                                   0 frozen-phi-ase-runge-kutta-4 (phi-ASE solved at the step start only),
+                                   1 explicit-euler, 2 heun, 3 midpoint, 4 runge-kutta-4,
+                                   5 implicit-euler (fixed-point iterations), 6 exponential-euler;
+                                   2, 3, 4 and 5 re-solve phi-ASE at every stage they evaluate */
+    uint32_t implicitIterations; /* implicit-euler iterations (0: the reference's default, 8) */
 } hase_time_desc;
 
 typedef struct {
@@ -233,7 +238,9 @@ typedef struct {
     double* meanBeta;           /* out [steps + 1] mean beta of the gain prisms, or NULL */
     double* meanPhi;            /* out [steps] mean phi-ASE of the samples (0 without a solve), or NULL */
     double* pumpAbsorbed;       /* out [steps] absorbed fraction of the pump power (first stage), or NULL */
-    float* phiHistory;          /* out [aseSteps][samples] phi-ASE of every solve, or NULL */
+    float* phiHistory;          /* out [aseSteps x solves per step][samples] phi-ASE of every solve, in order,
+                                   or NULL; solves per step: 1 (integrators 0, 1, 6), 2 (2, 3), 4 (4),
+                                   implicitIterations (5) */
     double aseMilliseconds;     /* device time of the phi-ASE solves */
     double pumpMilliseconds;    /* device time of pump, derivative and stage kernels */
     double totalMilliseconds;
@@ -252,6 +259,12 @@ hase_status hase_simulate(hase_context* ctx, struct hase_proposal* proposal, flo
 /* Measurement support (no reference counterpart): L2 read bandwidth of
  * `device` in GB/s, from `reps` passes over an L2-resident buffer of `bytes`. */
 hase_status hase_probe_l2_bandwidth(int device, uint64_t bytes, uint32_t reps, double* gbPerSecond);
+
+/* Measured L1 (sharedMemory = 0) or shared-memory (1) read bandwidth of the
+ * whole device in GB/s: two 1024-thread blocks per SM read a resident 32 KB
+ * `reps` times with 16-byte loads (the on-chip bound of a walk whose tables
+ * stay in L1 or shared memory). */
+hase_status hase_probe_l1_bandwidth(int device, uint32_t sharedMemory, uint32_t reps, double* gbPerSecond);
 
 /* Philox4x32-10 on the device: out[i] = philox(ctr[i], key). */
 hase_status hase_philox(uint32_t n, const uint32_t* ctr, const uint32_t key[2], uint32_t* out);

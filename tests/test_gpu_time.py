@@ -59,21 +59,55 @@ def test_decay_without_pump_is_exponential():
     np.testing.assert_allclose(ratio, np.exp(-2e-5 / mesh.crystalTFluo), rtol=1e-10)
 
 
-@pytest.mark.parametrize("integrator", [0, 1])
+INTEGRATORS = ["frozen-phi-ase-runge-kutta-4", "explicit-euler", "heun", "midpoint", "runge-kutta-4",
+               "implicit-euler", "exponential-euler"]
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
 def test_ase_steps_replay_the_oracle(integrator):
+    """Every integrator of the reference, with phi-ASE re-solved at the stages
+    that re-solve it: the oracle integrates the device's own phi of every
+    solve (phiHistory, in order) and reaches the same beta."""
+    from haseongpu_b200.simulation import solves_per_step, time_integrator
     from oracle import time_oracle as to
 
     mesh, sa, se = _cladding_mesh()
     beta0 = mesh.betaVolume.copy()
-    time = dict(timeStep=2e-5, steps=3, pumpSteps=3, aseSteps=2, integrator=integrator)
+    time = dict(timeStep=2e-5, steps=3, pumpSteps=3, aseSteps=2, integrator=integrator, implicitIterations=3)
+    k = solves_per_step(integrator, 3)
     with _ctx(mesh, sa, se) as ctx:
         out = ctx.simulate(pump=PUMP, time=time, minRays=4000, monochromatic=True, keepPhi=True)
-    assert out["phiHistory"].shape == (2, mesh.numberOfSamples) and np.all(out["phiHistory"] > 0)
-    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=time, sigma_ase=(sa[0], se[0]),
+    assert out["phiHistory"].shape == (2 * k, mesh.numberOfSamples) and np.all(out["phiHistory"] > 0)
+    otime = dict(time, integrator=time_integrator(integrator))
+    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=otime, sigma_ase=(sa[0], se[0]),
                           phi_history=out["phiHistory"])
     np.testing.assert_allclose(out["betaVolume"], hist[-1], rtol=1e-9, atol=1e-14)
-    assert out["raysTraced"] == 2 * 4000 * mesh.numberOfSamples
+    assert out["raysTraced"] == 2 * k * 4000 * mesh.numberOfSamples
     assert out["meanPhi"][2] == 0.0 and out["meanPhi"][0] > 0
+    if k > 1:  # the stage solves saw the stage states: their phi differs from the step-start solve
+        assert np.any(out["phiHistory"][1] != out["phiHistory"][0])
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+def test_fluorescence_decay_known_answer(integrator):
+    """Pump and ASE off: d beta/dt = -beta/tau in every gain prism, so one
+    step of size h = dt/tau multiplies beta by the integrator's own
+    amplification factor -- 1 - h (explicit Euler), 1 - h + h^2/2 (Heun,
+    midpoint), the 4-term Taylor sum of e^-h (RK4), sum_{k<=N} (-h)^k (N
+    fixed-point iterations of implicit Euler), e^-h (exponential Euler)."""
+    from haseongpu_b200.simulation import time_integrator
+
+    mesh, sa, se = _cladding_mesh()
+    dt = 2e-4
+    h = dt / mesh.crystalTFluo
+    code = time_integrator(integrator)
+    factor = {0: 1 - h + h**2 / 2 - h**3 / 6 + h**4 / 24, 1: 1 - h, 2: 1 - h + h**2 / 2, 3: 1 - h + h**2 / 2,
+              4: 1 - h + h**2 / 2 - h**3 / 6 + h**4 / 24, 5: sum((-h) ** k for k in range(4)), 6: np.exp(-h)}[code]
+    time = dict(timeStep=dt, steps=3, pumpSteps=0, aseSteps=0, integrator=integrator, implicitIterations=3)
+    with _ctx(mesh, sa, se) as ctx:
+        out = ctx.simulate(pump=PUMP, time=time, minRays=1000, monochromatic=True)
+    gain = mesh.betaVolume > 0
+    np.testing.assert_allclose(out["betaVolume"][gain], mesh.betaVolume[gain] * factor**3, rtol=1e-12)
 
 
 def test_learned_proposal_in_the_time_loop():
@@ -103,22 +137,25 @@ def test_forward_driver_without_ase_equals_the_backward_driver():
     np.testing.assert_allclose(fwd["pumpAbsorbed"], back["pumpAbsorbed"], rtol=1e-12)  # FP64 atomic sums
 
 
-@pytest.mark.parametrize("integrator", [0, 1])
+@pytest.mark.parametrize("integrator", ["frozen-phi-ase-runge-kutta-4", "explicit-euler", "heun",
+                                        "runge-kutta-4", "exponential-euler"])
 def test_forward_ase_steps_replay_the_oracle(integrator):
     """The oracle replays the forward driver's per-prism phi (volume-weighted
-    means of the twin's cells) through the same rate equations."""
+    means of the twin's cells, every solve) through the same rate equations."""
+    from haseongpu_b200.simulation import solves_per_step, time_integrator
     from oracle import time_oracle as to
 
     mesh, sa, se = _cladding_mesh()
     beta0 = mesh.betaVolume.copy()
     time = dict(timeStep=2e-5, steps=3, pumpSteps=3, aseSteps=2, integrator=integrator)
+    k = solves_per_step(integrator)
     with _ctx(mesh, sa, se) as ctx, _twin(mesh, sa, se) as twin:
         out = ctx.simulate_forward(twin, pump=PUMP, time=time, forwardRayCount=400_000, monochromatic=True,
                                    keepPhi=True)
-    assert out["phiHistory"].shape == (2, mesh.numberOfPrisms)
-    assert out["raysTraced"] == 2 * 400_000 and out["meanPhi"][0] > 0 and out["meanPhi"][2] == 0.0
-    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=time, sigma_ase=(sa[0], se[0]),
-                          phi_prism_history=out["phiHistory"])
+    assert out["phiHistory"].shape == (2 * k, mesh.numberOfPrisms)
+    assert out["raysTraced"] == 2 * k * 400_000 and out["meanPhi"][0] > 0 and out["meanPhi"][2] == 0.0
+    hist, _ = to.simulate(mesh, beta0, pump=PUMP, time=dict(time, integrator=time_integrator(integrator)),
+                          sigma_ase=(sa[0], se[0]), phi_prism_history=out["phiHistory"])
     np.testing.assert_allclose(out["betaVolume"], hist[-1], rtol=1e-9, atol=1e-14)
 
 

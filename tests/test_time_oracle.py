@@ -6,6 +6,7 @@ exp(-t / tau)."""
 from __future__ import annotations
 
 import numpy as np
+import pytest
 
 from conftest import legacy_mesh
 
@@ -36,3 +37,22 @@ def test_decay_is_exponential():
                           time=dict(timeStep=2e-5, steps=4, pumpSteps=0, aseSteps=0, integrator=0),
                           sigma_ase=(1.1e-21, 2.2e-20))
     np.testing.assert_allclose(hist[1:] / hist[:-1], np.exp(-2e-5 / mesh.crystalTFluo), rtol=1e-9)
+
+
+@pytest.mark.parametrize("code", range(7))
+def test_oracle_integrators_fluorescence_known_answer(code):
+    """Pump and ASE off, d beta/dt = -beta/tau: one step multiplies beta by
+    each integrator's amplification factor (h = dt/tau)."""
+    from haseongpu_b200.configs import disc_small
+    from oracle import time_oracle as to
+
+    mesh = disc_small().mesh
+    dt = 2e-4
+    h = dt / mesh.crystalTFluo
+    factor = {0: 1 - h + h**2 / 2 - h**3 / 6 + h**4 / 24, 1: 1 - h, 2: 1 - h + h**2 / 2, 3: 1 - h + h**2 / 2,
+              4: 1 - h + h**2 / 2 - h**3 / 6 + h**4 / 24, 5: sum((-h) ** k for k in range(4)), 6: np.exp(-h)}[code]
+    pump = dict(peakIntensity=0.0, radius=0.3, exponent=2.0, centerX=0.0, centerY=0.0, wavelength=940e-9,
+                sigmaA=7.6e-21, sigmaE=1e-22, retroreflect=True)
+    time = dict(timeStep=dt, steps=2, pumpSteps=0, aseSteps=0, integrator=code, implicitIterations=3)
+    hist, _ = to.simulate(mesh, mesh.betaVolume, pump=pump, time=time, sigma_ase=(1.1e-21, 2.2e-20))
+    np.testing.assert_allclose(hist[-1], mesh.betaVolume * factor**2, rtol=1e-13)
