@@ -1845,6 +1845,14 @@ struct hase_context {
     std::vector<double> hBeta;  // betaVolume as given (FP64)
     // learned proposal: coarse gain grid, fallback rows, contribution log
     DevBuf<float> featGrid, logBuf, priorBuf;
+    // the feature grid's layout (beta-independent, built on first use): grid
+    // extents, the triangles (ascending) whose centre lies in each cell, and
+    // the fill order of the empty cells, sweep by sweep
+    bool featLayout = false;
+    uint32_t featGx = 0, featGy = 0, featSweeps = 0;
+    float featX0 = 0.0f, featY0 = 0.0f, featCellSize = 0.0f, featR = 0.0f;
+    double featLnRb = 0.0, featLnRt = 0.0, featVmean = 0.0;
+    DevBuf<uint32_t> featCellStart, featCellTris, featFill, featSweepStart;
     uint64_t betaVersion = 1;       // bumped by every beta upload
     uint64_t featVersion = 0;       // beta version the cached feature view was built for
     double featA = 0.0, featB = 0.0;
@@ -1922,27 +1930,41 @@ struct LearnedArgs {
 
 constexpr uint32_t kGridCells = 48;  // feature grid cells along the longer side
 
-// Feature view of the context: the coarse gain grid (mean g = A beta - B of
-// the prisms whose centre falls in a cell, empty cells filled from their
-// neighbours), scales, and mean reflectivities.
-hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V);
-
-// The feature view, rebuilt only when beta or the averaged spectrum changed.
-hase_status cachedProposalView(hase_context* c, double A, double B, ProposalView& V) {
-    if (c->featVersion == c->betaVersion && c->featA == A && c->featB == B) {
-        V = c->featView;
-        return HASE_OK;
+// Mean gain coefficient g = A beta - B (-claddingAbsorption in cladding) of
+// the prisms of one layer (block) whose centre falls in each grid cell, then
+// the empty cells filled from their filled 4-neighbours, sweep by sweep (a
+// cell filled in a sweep is read from the next sweep on).  The sums run in
+// ascending triangle order and in the neighbour order of the layout.
+__global__ void featureGridKernel(const float* gainBeta, uint32_t T, double A, double B, float cladAbs,
+                                  const uint32_t* cellStart, const uint32_t* cellTris, uint32_t cells,
+                                  const uint32_t* fill, const uint32_t* sweepStart, uint32_t sweeps, float* grid) {
+    const uint32_t l = blockIdx.x;
+    float* gl = grid + size_t(l) * cells;
+    const float* bl = gainBeta + size_t(l) * T;
+    for (uint32_t k = threadIdx.x; k < cells; k += blockDim.x) {
+        const uint32_t a = cellStart[k], e = cellStart[k + 1];
+        if (a == e) continue;  // empty: filled below
+        float sum = 0.0f;
+        for (uint32_t i = a; i < e; ++i) {
+            const float bt = bl[cellTris[i]];
+            sum += bt != bt ? -cladAbs : float(A * double(bt) - B);
+        }
+        gl[k] = sum / float(e - a);
     }
-    HASE_TRY(buildProposalView(c, A, B, V));
-    HASE_CUDA(cudaStreamSynchronize(c->stream));
-    c->featView = V;
-    c->featVersion = c->betaVersion;
-    c->featA = A;
-    c->featB = B;
-    return HASE_OK;
+    __syncthreads();
+    for (uint32_t sw = 0; sw < sweeps; ++sw) {
+        for (uint32_t e = sweepStart[sw] + threadIdx.x; e < sweepStart[sw + 1]; e += blockDim.x) {
+            const uint32_t* f = fill + 6 * size_t(e);  // cell, neighbours n, up to 4 neighbour cells
+            float add = 0.0f;
+            for (uint32_t i = 0; i < f[1]; ++i) add += gl[f[2 + i]];
+            gl[f[0]] = add / float(f[1]);
+        }
+        __syncthreads();
+    }
 }
 
-hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V) {
+// The feature grid's layout, once per mesh (host; it does not depend on beta).
+hase_status buildFeatureLayout(hase_context* c) {
     float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY, R = 0.0f;
     for (const float2& q : c->hPoints) {
         x0 = std::min(x0, q.x);
@@ -1953,51 +1975,52 @@ hase_status buildProposalView(hase_context* c, double A, double B, ProposalView&
     }
     const float cell = std::max(x1 - x0, y1 - y0) / float(kGridCells) * 1.0001f;
     const uint32_t gx = uint32_t(std::ceil((x1 - x0) / cell)) + 1, gy = uint32_t(std::ceil((y1 - y0) / cell)) + 1;
-    const uint32_t L = c->layers;
-    std::vector<float> sum(size_t(L) * gx * gy, 0.0f), cnt(sum.size(), 0.0f);
-    for (uint32_t l = 0; l < L; ++l)
-        for (uint32_t t = 0; t < c->T; ++t) {
-            const float b = c->hGainBeta[t + size_t(l) * c->T];
-            const float g = std::isnan(b) ? -float(c->cladAbs) : float(A * b - B);
-            const uint32_t ix = std::min(gx - 1, uint32_t((c->hCentroid[t].x - x0) / cell));
-            const uint32_t iy = std::min(gy - 1, uint32_t((c->hCentroid[t].y - y0) / cell));
-            const size_t k = (size_t(l) * gy + iy) * gx + ix;
-            sum[k] += g;
-            cnt[k] += 1.0f;
-        }
-    for (size_t k = 0; k < sum.size(); ++k)
-        if (cnt[k] > 0.0f) sum[k] /= cnt[k];
-    for (uint32_t l = 0; l < L; ++l)  // fill empty cells from filled 4-neighbours
-        for (uint32_t sweep = 0; sweep < gx + gy; ++sweep) {
-            bool changed = false;
-            std::vector<float> add(size_t(gx) * gy, 0.0f), n(size_t(gx) * gy, 0.0f);
-            for (uint32_t iy = 0; iy < gy; ++iy)
-                for (uint32_t ix = 0; ix < gx; ++ix) {
-                    const size_t k = (size_t(l) * gy + iy) * gx + ix;
-                    if (cnt[k] > 0.0f) continue;
-                    const int dxy[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
-                    for (auto& o : dxy) {
-                        const int jx = int(ix) + o[0], jy = int(iy) + o[1];
-                        if (jx < 0 || jy < 0 || jx >= int(gx) || jy >= int(gy)) continue;
-                        const size_t kk = (size_t(l) * gy + jy) * gx + jx;
-                        if (cnt[kk] > 0.0f) {
-                            add[iy * gx + ix] += sum[kk];
-                            n[iy * gx + ix] += 1.0f;
-                        }
-                    }
+    const uint32_t cells = gx * gy;
+    std::vector<uint32_t> cellOf(c->T), start(cells + 1, 0), tris(c->T);
+    for (uint32_t t = 0; t < c->T; ++t) {
+        const uint32_t ix = std::min(gx - 1, uint32_t((c->hCentroid[t].x - x0) / cell));
+        const uint32_t iy = std::min(gy - 1, uint32_t((c->hCentroid[t].y - y0) / cell));
+        cellOf[t] = iy * gx + ix;
+        ++start[cellOf[t] + 1];
+    }
+    for (uint32_t k = 0; k < cells; ++k) start[k + 1] += start[k];
+    std::vector<uint32_t> pos(start.begin(), start.end() - 1);
+    for (uint32_t t = 0; t < c->T; ++t) tris[pos[cellOf[t]]++] = t;  // ascending t within each cell
+    // fill order: every sweep fills the empty cells with a filled 4-neighbour
+    // (+x, -x, +y, -y), from the cells filled before the sweep
+    std::vector<uint8_t> filled(cells);
+    for (uint32_t k = 0; k < cells; ++k) filled[k] = start[k + 1] > start[k];
+    std::vector<uint32_t> fill, sweepStart{0};
+    for (uint32_t sweep = 0; sweep < gx + gy; ++sweep) {
+        std::vector<uint32_t> now;
+        for (uint32_t iy = 0; iy < gy; ++iy)
+            for (uint32_t ix = 0; ix < gx; ++ix) {
+                const uint32_t k = iy * gx + ix;
+                if (filled[k]) continue;
+                uint32_t e[6] = {k, 0, 0, 0, 0, 0};
+                const int dxy[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+                for (auto& o : dxy) {
+                    const int jx = int(ix) + o[0], jy = int(iy) + o[1];
+                    if (jx < 0 || jy < 0 || jx >= int(gx) || jy >= int(gy)) continue;
+                    const uint32_t kk = uint32_t(jy) * gx + uint32_t(jx);
+                    if (filled[kk]) e[2 + e[1]++] = kk;
                 }
-            for (uint32_t i = 0; i < gx * gy; ++i)
-                if (n[i] > 0.0f) {
-                    const size_t k = size_t(l) * gx * gy + i;
-                    sum[k] = add[i] / n[i];
-                    cnt[k] = 1.0f;
-                    changed = true;
-                }
-            if (!changed) break;
-        }
-    HASE_CUDA(c->featGrid.ensure(sum.size()));
-    HASE_CUDA(cudaMemcpyAsync(c->featGrid.p, sum.data(), sum.size() * sizeof(float), cudaMemcpyHostToDevice,
-                              c->stream));
+                if (e[1] == 0) continue;
+                fill.insert(fill.end(), e, e + 6);
+                now.push_back(k);
+            }
+        if (now.empty()) break;
+        for (uint32_t k : now) filled[k] = 1;
+        sweepStart.push_back(uint32_t(fill.size() / 6));
+    }
+    HASE_CUDA(c->featCellStart.ensure(cells + 1));
+    HASE_CUDA(c->featCellTris.ensure(std::max<uint32_t>(c->T, 1)));
+    HASE_CUDA(c->featFill.ensure(std::max<size_t>(fill.size(), 6)));
+    HASE_CUDA(c->featSweepStart.ensure(sweepStart.size()));
+    HASE_CUDA(cudaMemcpy(c->featCellStart.p, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
+    HASE_CUDA(cudaMemcpy(c->featCellTris.p, tris.data(), tris.size() * 4, cudaMemcpyHostToDevice));
+    if (!fill.empty()) HASE_CUDA(cudaMemcpy(c->featFill.p, fill.data(), fill.size() * 4, cudaMemcpyHostToDevice));
+    HASE_CUDA(cudaMemcpy(c->featSweepStart.p, sweepStart.data(), sweepStart.size() * 4, cudaMemcpyHostToDevice));
     double lnRb = 0.0, lnRt = 0.0, vmean = 0.0;
     if (!c->hReflect.empty()) {
         for (uint32_t t = 0; t < c->T; ++t) {
@@ -2006,25 +2029,66 @@ hase_status buildProposalView(hase_context* c, double A, double B, ProposalView&
         }
     }
     for (float a : c->hArea) vmean += double(a) * c->h / c->T;
+    c->featGx = gx;
+    c->featGy = gy;
+    c->featSweeps = uint32_t(sweepStart.size() - 1);
+    c->featX0 = x0;
+    c->featY0 = y0;
+    c->featCellSize = cell;
+    c->featR = R;
+    c->featLnRb = lnRb;
+    c->featLnRt = lnRt;
+    c->featVmean = vmean;
+    c->featLayout = true;
+    return HASE_OK;
+}
+
+// Feature view of the context: the coarse gain grid (mean g = A beta - B of
+// the prisms whose centre falls in a cell, empty cells filled from their
+// neighbours; built on the device from the resident beta), scales, and mean
+// reflectivities.
+hase_status buildProposalView(hase_context* c, double A, double B, ProposalView& V) {
+    if (!c->featLayout) HASE_TRY(buildFeatureLayout(c));
+    const uint32_t cells = c->featGx * c->featGy, L = c->layers;
+    HASE_CUDA(c->featGrid.ensure(size_t(L) * cells));
+    featureGridKernel<<<L, 256, 0, c->stream>>>(c->gainBeta.p, c->T, A, B, float(c->cladAbs), c->featCellStart.p,
+                                                 c->featCellTris.p, cells, c->featFill.p, c->featSweepStart.p,
+                                                 c->featSweeps, c->featGrid.p);
+    HASE_CUDA(cudaGetLastError());
     V = ProposalView{};
     V.m = c->view();
     V.grid = c->featGrid.p;
-    V.gx = gx;
-    V.gy = gy;
-    V.x0 = x0;
-    V.y0 = y0;
-    V.invCell = 1.0f / cell;
-    V.lnRb = float(lnRb);
-    V.lnRt = float(lnRt);
-    V.R = std::max(R, 1e-6f);
+    V.gx = c->featGx;
+    V.gy = c->featGy;
+    V.x0 = c->featX0;
+    V.y0 = c->featY0;
+    V.invCell = 1.0f / c->featCellSize;
+    V.lnRb = float(c->featLnRb);
+    V.lnRt = float(c->featLnRt);
+    V.R = std::max(c->featR, 1e-6f);
     V.H = float(c->h * L);
     V.invR = 1.0f / V.R;
     V.invH = 1.0f / V.H;
     V.invTwoH = 0.5f / V.H;
     V.invh = float(1.0 / c->h);
-    V.lnVref = float(std::log(std::max(vmean, 1e-30) / (double(V.R) * V.R)));
+    V.lnVref = float(std::log(std::max(c->featVmean, 1e-30) / (double(V.R) * V.R)));
     const double se = (A - B), sa = B;
     V.lnSigmaRatio = float(std::log(std::max(se, 1e-30) / std::max(sa, 1e-30)));
+    return HASE_OK;
+}
+
+// The feature view, rebuilt (one kernel on the context's stream) only when
+// beta or the averaged spectrum changed.
+hase_status cachedProposalView(hase_context* c, double A, double B, ProposalView& V) {
+    if (c->featVersion == c->betaVersion && c->featA == A && c->featB == B) {
+        V = c->featView;
+        return HASE_OK;
+    }
+    HASE_TRY(buildProposalView(c, A, B, V));
+    c->featView = V;
+    c->featVersion = c->betaVersion;
+    c->featA = A;
+    c->featB = B;
     return HASE_OK;
 }
 
