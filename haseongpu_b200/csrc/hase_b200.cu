@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
         float* outRow = L.lnw + size_t(row) * L.nW + t;
         const uint32_t nLines = L.slices * m.layers;
         for (uint32_t c0 = 0; c0 < nLines; c0 += TL * LPL) {
-            float J[LPL], lnR[LPL], invc[LPL];
+            float J[LPL], lnR[LPL], invc[LPL], nextPlane[LPL];
             int ka[LPL], phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
             uint32_t sl[LPL];
             bool ok[LPL];
@@ -323,6 +323,9 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 pdir[g] = 1;
                 left[g] = expectedReflections(j);
                 invc[g] = D2 / (float(int(l) - kImg[g]) + 0.5f);
+                // sigma of the next level plane toward the image level (carried,
+                // recomputed only when the line crosses it)
+                nextPlane[g] = float(int(l) + (kImg[g] > int(l) ? 1 : 0) - kImg[g]) * invc[g];
             }
             GlobalLoader load{m.tri};
             uint32_t tk = t;
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                     float s = sc;
                     float gb = gbv[g];
                     while (true) {
-                        const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg[g]) * invc[g];
+                        const float sb = nextPlane[g];
                         if (!(sb > sOut)) break;
                         if (COUNT) ++counted;
                         J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
@@ -384,6 +387,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                             gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
                         }
                         ka[g] += dl;
+                        nextPlane[g] = float(ka[g] + (dl > 0 ? 1 : 0) - kImg[g]) * invc[g];
                     }
                     if (!ok[g]) continue;
                     J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);
@@ -845,238 +849,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     }
 }
 
-// Prepared start states per warp in the ring kernel (a power of two of at
-// least 63: the ring holds at most 31 unconsumed rays when a batch of 32 is
-// produced).
-constexpr uint32_t kRing = 64;
-constexpr uint32_t kRingBytesPerWarp = kRing * 3 * sizeof(float4);
-
-// Ray kernel with start states produced a warp at a time.  The persistent
-// work queue and the walk are those of rayKernel; what differs is how idle
-// lanes get their next ray.  Whenever the warp's ring in shared memory holds
-// fewer prepared rays than there are idle lanes, all 32 lanes prepare the
-// next 32 consecutive rays of the item together -- the ray->prism search as
-// one warp-wide step (32 offsets of the map per load, a 5-step shuffle
-// search per lane), Philox, the start point, the initial walk state -- and
-// append the valid ones to the ring; idle lanes then take prepared rays with
-// three 16-byte shared loads.  Every start-state instruction thereby runs on
-// 32 lanes, where rayKernel runs it on the idle lanes only (REFILL or more of
-// 32), and a refill is cheap enough to happen whenever REFILL lanes are idle
-// after COLS columns.  The rays, their start states and their walks are
-// rayKernel's, so the per-item sums agree with it to FP64 rounding.
-template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns,
-          int WALK = kWalkBeta>
-__global__ void __launch_bounds__(BLOCK, MINB) rayRingKernel(RayLaunch L) {
-    extern __shared__ float4 ringSmem[];  // [BLOCK / 32][kRing][3]
-    __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
-    // the current item's constants that only the batch preparation and the
-    // finish of a ray read: kept in shared memory, not in registers across the walk
-    struct ItemConsts {
-        const uint32_t* off;
-        const uint32_t* q;
-        double CQ;
-        unsigned long long wBase;
-        uint32_t sample, lambdaPhase, nLambda, ls, seedLo, entry0;
-    };
-    __shared__ ItemConsts sItem[BLOCK / 32];
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const unsigned laneLt = (1u << lane) - 1u;
-    float4* ring = ringSmem + size_t(threadIdx.x >> 5) * kRing * 3;
-    volatile ItemConsts& ic = sItem[threadIdx.x >> 5];
-    const uint32_t nItems = (POOL ? *L.count : L.nActive) * L.itemsPerRow;
-    uint32_t curInst = 0xffffffffu;
-    while (true) {
-        uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(L.itemCounter, 1u);
-        item = __shfl_sync(full, item, 0);
-        if (item >= nItems) break;
-        const uint32_t row = L.active[item / L.itemsPerRow];
-        const uint32_t k = item % L.itemsPerRow;
-        const size_t slot = size_t(row) * kMaxItems + k;
-        const unsigned long long Qrow = L.Q[row];
-        if (Qrow == 0ull) {  // no source prism: every ray contributes 0
-            if (lane == 0) {
-                L.pSum[slot] = 0.0;
-                L.pSum2[slot] = 0.0;
-                L.pDrop[slot] = 0u;
-                L.pCross[slot] = 0ull;
-            }
-            continue;
-        }
-        uint32_t sample, nW;
-        size_t wBase, oBase;
-        if constexpr (POOL) {
-            const RowInfo ri = L.rows[row];
-            if (ri.inst != curInst) {
-                const uint32_t* src = reinterpret_cast<const uint32_t*>(L.inst + ri.inst);
-                uint32_t* dst = reinterpret_cast<uint32_t*>(sInst + (threadIdx.x >> 5));
-                for (uint32_t w = uint32_t(lane); w < sizeof(InstanceView) / 4; w += 32) dst[w] = __ldg(src + w);
-                __syncwarp();
-                curInst = ri.inst;
-            }
-            sample = ri.sample;
-            nW = ri.nW;
-            wBase = ri.w;
-            oBase = ri.w + row;
-        } else {
-            sample = L.firstSample + row;
-            nW = L.nW;
-            wBase = size_t(row) * nW;
-            oBase = size_t(row) * (nW + 1);
-        }
-        const volatile InstanceView& iv = sInst[threadIdx.x >> 5];
-        const MeshView& m = POOL ? sInst[threadIdx.x >> 5].m : L.m;
-        const GlobalLoader load{m.tri};
-        const uint32_t r0 = k * L.itemRays;
-        const uint32_t r1 = min(r0 + L.itemRays, L.M);
-        const float2 S = __ldg(m.points + sample % m.Np);
-        {
-            const uint32_t seedLo = POOL ? uint32_t(iv.seedLo) : L.seedLo;
-            const uint32_t nLam = POOL ? uint32_t(iv.nLambda) : L.nLambda;
-            const uint32_t* off = L.offsets + oBase;
-            // entry of the map holding ray r0 (then carried: the entry of the
-            // last ray prepared so far)
-            uint32_t c0 = 0;
-            if (lane == 0) {
-                c0 = upperBound(off, nW + 1, r0) - 1u;
-                ic.off = off;
-                ic.q = L.q + wBase;
-                ic.CQ = (POOL ? double(iv.C) : double(L.C)) * double(Qrow);
-                ic.wBase = wBase;
-                ic.sample = sample;
-                ic.lambdaPhase =
-                    nLam > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, seedLo, L.seedHi).y % nLam : 0u;
-                ic.nLambda = nLam;
-                ic.ls = uint32_t(sample / m.Np);
-                ic.seedLo = seedLo;
-                ic.entry0 = c0;
-            }
-            __syncwarp();
-        }
-        uint32_t cur = ic.entry0;
-
-        double sum = 0.0, sum2 = 0.0;
-        uint32_t dropped = 0, crossings = 0;
-        uint32_t fetch = r0, head = 0, tail = 0;  // warp-uniform: next ray to prepare, ring read / write counts
-        bool active = false;
-        Ray ray;
-        float wf = 0.0f;
-        uint32_t bsel = 0;
-        while (true) {
-            const unsigned idle = __ballot_sync(full, !active);
-            const uint32_t nIdle = uint32_t(__popc(idle));
-            if (nIdle == 32 && head == tail && fetch >= r1) break;
-            if (nIdle >= uint32_t(REFILL) || nIdle == 32) {
-                if (tail - head < nIdle && fetch < r1) {
-                    // prepare rays fetch .. fetch + nb - 1, one per lane
-                    const uint32_t nb = min(32u, r1 - fetch);
-                    const uint32_t r = fetch + uint32_t(lane);
-                    const bool valid = uint32_t(lane) < nb;
-                    const uint32_t* off = ic.off;
-                    // map entry b of ray r: off[b] <= r < off[b + 1], searched
-                    // in windows of 32 offsets starting after `cur`
-                    uint32_t b = 0, bLo = cur;
-                    bool pending = valid;
-                    while (__any_sync(full, pending)) {
-                        const uint32_t o = __ldg(off + min(bLo + 1u + uint32_t(lane), nW));
-                        uint32_t cnt = 0;
-#pragma unroll
-                        for (int st = 16; st >= 1; st >>= 1) {
-                            const uint32_t v = __shfl_sync(full, o, int(cnt) + st - 1);
-                            if (v <= r) cnt += uint32_t(st);
-                        }
-                        const uint32_t oLast = __shfl_sync(full, o, 31);
-                        if (pending && r < oLast) {
-                            b = bLo + cnt;
-                            pending = false;
-                        }
-                        bLo += 32u;
-                    }
-                    cur = __shfl_sync(full, b, int(nb) - 1);
-                    Ray nr;
-                    float nwf = 0.0f;
-                    bool ok = false;
-                    if (valid) {
-                        const float D2 = startRay(m, r, b, ic.sample, S, int(ic.ls), L.pass, ic.seedLo, L.seedHi,
-                                                  ic.nLambda, ic.lambdaPhase, L.M,
-                                                  POOL ? (const float2*)iv.spec : L.spec, ic.q, L.nearField, nr, nwf);
-                        ok = D2 > 0.0f;
-                        if (!ok) ++dropped;  // start point on the sample point itself
-                    }
-                    const unsigned okMask = __ballot_sync(full, ok);
-                    __syncwarp();  // every lane's earlier reads of the slots about to be overwritten are done
-                    if (ok) {
-                        float4* e = ring + ((tail + uint32_t(__popc(okMask & laneLt))) & (kRing - 1)) * 3;
-                        e[0] = make_float4(nr.s, nr.ux, nr.uy, nr.uz);
-                        e[1] = make_float4(nr.hOverUz, nr.zl, nr.A, nr.B);
-                        e[2] = make_float4(__uint_as_float(nr.t),
-                                           __uint_as_float(uint32_t(nr.phys) | (uint32_t(nr.reflLeft) << 16)), nwf,
-                                           __uint_as_float(b));
-                    }
-                    __syncwarp();
-                    tail += uint32_t(__popc(okMask));
-                    fetch += nb;
-                }
-                const uint32_t avail = tail - head;
-                const uint32_t rank = uint32_t(__popc(idle & laneLt));
-                if (!active && rank < avail) {
-                    const float4* e = ring + ((head + rank) & (kRing - 1)) * 3;
-                    const float4 a = e[0], c = e[1], d = e[2];
-                    ray.s = a.x;
-                    ray.ux = a.y;
-                    ray.uy = a.z;
-                    ray.uz = a.w;
-                    ray.hOverUz = c.x;
-                    ray.zl = c.y;
-                    ray.A = c.z;
-                    ray.B = c.w;
-                    ray.t = __float_as_uint(d.x);
-                    const uint32_t pr = __float_as_uint(d.y);
-                    ray.phys = int(pr & 0xffffu);
-                    ray.reflLeft = int(pr >> 16);
-                    ray.pdir = 1;
-                    ray.forb = -1;
-                    ray.steps = 0;
-                    ray.G = 0.0f;
-                    wf = d.z;
-                    if (LOG) bsel = __float_as_uint(d.w);
-                    active = true;
-                }
-                head += min(nIdle, avail);
-            }
-            if (active) {
-                const int st = stepRay<COLS, WALK>(m, S.x, S.y, ray, load);
-                if (st != kContinue) {
-                    crossings += uint32_t(ray.steps) + 1u;
-                    if (st == kDone) {
-                        finishReflections(m, ray);
-                        const double eg = ray.G < 80.0f ? double(expf(ray.G)) : exp(double(ray.G));
-                        const double X = ic.CQ * double(wf) * eg;
-                        sum += X;
-                        sum2 += X * X;
-                        if (LOG) atomicAdd(L.logBuf + size_t(ic.wBase) + bsel, float(X));
-                    } else {
-                        ++dropped;
-                    }
-                    active = false;
-                }
-            }
-        }
-        sum = warpSum(sum);
-        sum2 = warpSum(sum2);
-        dropped = warpSum(dropped);
-        crossings = warpSum(crossings);
-        if (lane == 0) {
-            L.pSum[slot] = sum;
-            L.pSum2[slot] = sum2;
-            L.pDrop[slot] = dropped;
-            L.pCross[slot] = crossings;
-        }
-        __syncwarp();  // the item's constants are read before the next item overwrites them
-    }
-}
-
 // Launch shapes of rayKernel the autotuner chooses from: block size, idle
 // lanes that trigger a refill, the occupancy target (blocks per SM the
 // register budget is fitted to) and the triangle columns a lane walks per
@@ -1088,14 +860,10 @@ struct RayVariant {
     const char* name;
     void (*mono)(RayLaunch);     // the same shape walking the g table (monochromatic single-medium solves), or null
     void (*noClad)(RayLaunch);   // the same shape for a medium without cladding prisms, or null
-    uint32_t smem;               // dynamic shared memory per block (the ring kernel's prepared rays), bytes
 };
 #define HASE_RAY_SHAPE(B, R, M, C, NAME)                                                      \
     {rayKernel<B, R, M, false, false, C>, B, NAME, rayKernel<B, R, M, false, false, C, kWalkTable>, \
-     rayKernel<B, R, M, false, false, C, kWalkBetaNoClad>, 0u}
-#define HASE_RING_SHAPE(B, R, M, C, NAME)                                                             \
-    {rayRingKernel<B, R, M, false, false, C>, B, NAME, rayRingKernel<B, R, M, false, false, C, kWalkTable>, \
-     rayRingKernel<B, R, M, false, false, C, kWalkBetaNoClad>, uint32_t(B / 32) * kRingBytesPerWarp}
+     rayKernel<B, R, M, false, false, C, kWalkBetaNoClad>}
 const RayVariant kRayVariants[] = {
     HASE_RAY_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
     HASE_RAY_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
@@ -1107,24 +875,14 @@ const RayVariant kRayVariants[] = {
     HASE_RAY_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
     HASE_RAY_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
     HASE_RAY_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
-    HASE_RING_SHAPE(256, 4, 4, 16, "ring256_refill4_occ4_cols16"),
-    HASE_RING_SHAPE(256, 8, 4, 32, "ring256_refill8_occ4_cols32"),
-    HASE_RING_SHAPE(256, 2, 4, 8, "ring256_refill2_occ4_cols8"),
-    HASE_RING_SHAPE(512, 4, 2, 16, "ring512_refill4_occ2_cols16"),
-    HASE_RING_SHAPE(512, 8, 2, 32, "ring512_refill8_occ2_cols32"),
-    HASE_RING_SHAPE(128, 4, 8, 16, "ring128_refill4_occ8_cols16"),
 };
 #undef HASE_RAY_SHAPE
-#undef HASE_RING_SHAPE
 constexpr uint32_t kNumRayVariants = sizeof(kRayVariants) / sizeof(kRayVariants[0]);
 static_assert(kNumRayVariants <= 16, "variantBlocks holds 16 launch shapes");
 // The same launch shapes for batched media (same order and names): the
 // general walk, and the walk for batches without cladding prisms.
 #define HASE_POOL_SHAPE(B, R, M, C, NAME) \
-    {rayKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayKernel<B, R, M, false, true, C, kWalkBetaNoClad>, 0u}
-#define HASE_POOL_RING_SHAPE(B, R, M, C, NAME)                                                              \
-    {rayRingKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayRingKernel<B, R, M, false, true, C, kWalkBetaNoClad>, \
-     uint32_t(B / 32) * kRingBytesPerWarp}
+    {rayKernel<B, R, M, false, true, C>, B, NAME, nullptr, rayKernel<B, R, M, false, true, C, kWalkBetaNoClad>}
 const RayVariant kPoolVariants[] = {
     HASE_POOL_SHAPE(256, 8, 5, kWalkColumns, "block256_refill8_occ5"),
     HASE_POOL_SHAPE(256, 4, 5, kWalkColumns, "block256_refill4_occ5"),
@@ -1136,28 +894,8 @@ const RayVariant kPoolVariants[] = {
     HASE_POOL_SHAPE(512, 8, 2, kWalkColumns, "block512_refill8_occ2"),
     HASE_POOL_SHAPE(256, 16, 5, 64, "block256_refill16_occ5_cols64"),
     HASE_POOL_SHAPE(512, 8, 2, 64, "block512_refill8_occ2_cols64"),
-    HASE_POOL_RING_SHAPE(256, 4, 4, 16, "ring256_refill4_occ4_cols16"),
-    HASE_POOL_RING_SHAPE(256, 8, 4, 32, "ring256_refill8_occ4_cols32"),
-    HASE_POOL_RING_SHAPE(256, 2, 4, 8, "ring256_refill2_occ4_cols8"),
-    HASE_POOL_RING_SHAPE(512, 4, 2, 16, "ring512_refill4_occ2_cols16"),
-    HASE_POOL_RING_SHAPE(512, 8, 2, 32, "ring512_refill8_occ2_cols32"),
-    HASE_POOL_RING_SHAPE(128, 4, 8, 16, "ring128_refill4_occ8_cols16"),
 };
 #undef HASE_POOL_SHAPE
-#undef HASE_POOL_RING_SHAPE
-
-// Lets a launch shape use its dynamic shared memory (above the default
-// 48 KB per block) in every walk mode it has.
-cudaError_t allowRayVariantSmem(const RayVariant& v) {
-    if (v.smem == 0) return cudaSuccess;
-    for (void (*k)(RayLaunch) : {v.kernel, v.mono, v.noClad}) {
-        if (!k) continue;
-        const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k),
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(v.smem));
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
 
 // ------------------------------------------------ (c)+(d) finalise ----
@@ -2317,11 +2055,10 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         const RayVariant& v = kRayVariants[variant];
         int sms = 0;
         HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-        HASE_CUDA(allowRayVariantSmem(v));
         void (*const modes[3])(RayLaunch) = {v.kernel, v.mono, v.noClad};
         for (int w = 0; w < 3; ++w) {
             int perSM = 0;
-            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, modes[w], v.block, v.smem));
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, modes[w], v.block, 0));
             c->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, sms));
         }
     }
@@ -2437,8 +2174,8 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
                                                                uint64_t(c->variantBlocks[walk][variant])));
             void (*const kern)(RayLaunch) = walk == kWalkTable ? rv.mono : (walk == kWalkBetaNoClad ? rv.noClad : rv.kernel);
             void* rayArgs[] = {&rl};
-            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs,
-                                       rv.smem, c->stream));
+            HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs, 0,
+                                       c->stream));
             HASE_CUDA(cudaEventRecord(c->ev[3], c->stream));
             HASE_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream));
             FinalizeLaunch fl{cur, nActive, items, M, lastPass ? 1 : 0, ex->mseThreshold, c->pSum.p, c->pSum2.p,
@@ -3527,11 +3264,9 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
     const uint32_t variant = cp->rayKernelVariant;
     const RayVariant& rv = kPoolVariants[variant];
     if (b->variantBlocks[0][variant] == 0) {
-        HASE_CUDA(allowRayVariantSmem(rv));
         for (int w = 0; w < 2; ++w) {
             int perSM = 0;
-            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, w ? rv.noClad : rv.kernel, rv.block,
-                                                                    rv.smem));
+            HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, w ? rv.noClad : rv.kernel, rv.block, 0));
             b->variantBlocks[w][variant] = uint32_t(std::max(1, perSM) * std::max(1, b->sms));
         }
     }
@@ -3779,7 +3514,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                                                                    uint64_t(b->variantBlocks[noClad][variant])));
                 void* rayArgs[] = {&rl};
                 HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(noClad ? rv.noClad : rv.kernel), dim3(grid),
-                                           dim3(rv.block), rayArgs, rv.smem, b->stream));
+                                           dim3(rv.block), rayArgs, 0, b->stream));
                 HASE_CUDA(cudaEventRecordWithFlags(b->ev[4 + 2 * k], b->stream, cudaEventRecordExternal));
                 HASE_CUDA(cudaMemsetAsync(cntNxt, 0, sizeof(unsigned int), b->stream));
                 FinalizeLaunch fl{cur, 0u, ps.items, ps.M, ps.last ? 1 : 0, thr, b->pSum.p, b->pSum2.p, b->pDrop.p,
