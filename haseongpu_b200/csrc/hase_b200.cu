@@ -306,10 +306,12 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
             int ka[LPL], phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
             uint32_t sl[LPL];
             bool ok[LPL];
+            const uint16_t* order = m.lineOrder[L.slices == 5 ? 1 : 0];
 #pragma unroll
             for (int g = 0; g < LPL; ++g) {
-                const uint32_t q = c0 + li + uint32_t(TL * g);
-                const bool valid = q < nLines;
+                const uint32_t qq = c0 + li + uint32_t(TL * g);
+                const bool valid = qq < nLines;
+                const uint32_t q = valid && order ? uint32_t(__ldg(order + size_t(ls) * nLines + qq)) : qq;
                 const uint32_t l = valid ? q / L.slices : 0u;
                 const uint32_t j = valid ? q - l * L.slices : 0u;
                 sl[g] = valid ? j : 0xffffffffu;
@@ -1549,6 +1551,27 @@ hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& exte
     return HASE_OK;
 }
 
+// The importance kernel's line order: for every sample level ls, the lines
+// q = l * slices + j (layer l, reflection slice j) by increasing distance
+// |l + 1/2 - kImg| to the image level (ties by q).  A line crosses about that
+// many level planes along its 2-D path, so the lines of one lane slot of a
+// team cross similar numbers of planes per triangle.
+void buildLineOrder(uint32_t layers, uint32_t slices, std::vector<uint16_t>& ord) {
+    const uint32_t n = slices * layers;
+    ord.resize(size_t(layers + 1) * n);
+    std::vector<std::pair<double, uint32_t>> key(n);
+    for (uint32_t ls = 0; ls <= layers; ++ls) {
+        for (uint32_t q = 0; q < n; ++q) {
+            const uint32_t l = q / slices, j = q % slices;
+            const int L = int(layers), s = int(ls);
+            const int kImg = j == 1 ? -s : j == 2 ? 2 * L - s : j == 3 ? s - 2 * L : j == 4 ? s + 2 * L : s;
+            key[q] = {std::fabs(double(l) + 0.5 - double(kImg)), q};
+        }
+        std::sort(key.begin(), key.end());
+        for (uint32_t i = 0; i < n; ++i) ord[size_t(ls) * n + i] = uint16_t(key[i].second);
+    }
+}
+
 }  // namespace
 
 struct hase_context {
@@ -1565,6 +1588,7 @@ struct hase_context {
     float tirCos2[2] = {-1.0f, -1.0f};
     DevBuf<float4> tri, geo;
     DevBuf<int4> verts;
+    DevBuf<uint16_t> lineOrder[2];  // importance line order per sample level: 1 and 5 reflection slices
     DevBuf<float2> centroid, points, spec;
     DevBuf<float> gainBeta, srcBeta, reflect;
     DevBuf<float> gTab;  // g of every prism for the spectrally averaged (A, B) of the last solve
@@ -1610,6 +1634,8 @@ struct hase_context {
         v.srcBeta = srcBeta.p;
         v.points = points.p;
         v.reflect = hasReflect ? reflect.p : nullptr;
+        v.lineOrder[0] = lineOrder[0].p;
+        v.lineOrder[1] = lineOrder[1].p;
         v.T = T;
         v.layers = layers;
         v.P = P;
@@ -1936,6 +1962,13 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
     if ((st = up(c->tri, ht.tri)) != HASE_OK) return cleanup(st);
     if ((st = up(c->geo, ht.geo)) != HASE_OK) return cleanup(st);
     if ((st = up(c->verts, ht.verts)) != HASE_OK) return cleanup(st);
+    if (uint64_t(5) * c->layers < 65536) {  // importance line order (16-bit line indices)
+        for (int r = 0; r < 2; ++r) {
+            std::vector<uint16_t> ord;
+            buildLineOrder(c->layers, r ? 5u : 1u, ord);
+            if ((st = up(c->lineOrder[r], ord)) != HASE_OK) return cleanup(st);
+        }
+    }
     if ((st = up(c->centroid, ht.centroid)) != HASE_OK) return cleanup(st);
     if ((st = up(c->points, ht.points)) != HASE_OK) return cleanup(st);
     if (c->gainBeta.ensure(c->P) != cudaSuccess || c->srcBeta.ensure(c->P) != cudaSuccess)

@@ -75,6 +75,11 @@ struct MeshView {
     const float* srcBeta;    // [P] beta (source weight)
     const float2* points;    // [Np]
     const float* reflect;    // [T][2] or nullptr
+    // importance walks: per sample level, the slices x layers lines of a
+    // triangle ordered by their layer distance to the image level (without,
+    // with reflections), so that lines with similar numbers of level planes
+    // share a lane slot of the line teams
+    const uint16_t* lineOrder[2];
     uint32_t T, layers, P, Np;
     uint32_t divTm, divTs;   // floor(p / T) = (p * divTm) >> divTs for p < 2^31 (invariantDivisor)
     uint32_t divNpm, divNps; // the same for division by Np
