@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "hase_context_update_beta",
     "hase_calc_phi_ase",
     "hase_context_destroy",
+    "hase_context_set_local_proposal",
     "hase_importance_weights",
     "hase_importance_crossings",
     "hase_ray_map",
@@ -349,6 +350,7 @@ def lib():
         L.hase_calc_phi_ase.argtypes = [C.c_void_p, C.POINTER(ExperimentDesc), C.POINTER(ComputeDesc),
                                         C.POINTER(ResultDesc)]
         L.hase_context_destroy.argtypes = [C.c_void_p]
+        L.hase_context_set_local_proposal.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         L.hase_importance_weights.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
         L.hase_importance_crossings.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
         L.hase_ray_map.argtypes = [C.c_uint32, C.c_uint32, _f32p, C.c_uint32, _u32p, _u32p, _u32p, _u64p]

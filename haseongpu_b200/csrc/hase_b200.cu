@@ -125,6 +125,10 @@ struct ImportanceLaunch {
     const uint8_t* rowFlag;   // batched media: only rows with rowFlag[flagBase + row] set are computed (or null)
     uint32_t flagBase;
     unsigned long long* crossings;  // counting launches only: total walk crossings
+    // local proposal: the K candidate triangles of every point ([Np][K]); the
+    // row then holds slices x layers x K entries (j (layers K) + l K + k)
+    const uint32_t* cand;
+    uint32_t K;
 };
 
 // One thread per (sample, reflection slice, triangle, group of G layers): the
@@ -285,13 +289,16 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
     const MeshView& m = L.m;
     const float* gcol = TAB ? m.gTab : m.gainBeta;
     constexpr uint32_t kTeams = 256 / TL;
-    const uint32_t t = blockIdx.x * kTeams + threadIdx.x / TL;
+    const uint32_t tIdx = blockIdx.x * kTeams + threadIdx.x / TL;  // triangle (or candidate) of the team
     const uint32_t li = threadIdx.x % TL;
     const uint32_t row = L.rowList ? L.rowList[blockIdx.y] : blockIdx.y;
+    const uint32_t strideL = L.cand ? L.K : m.T;            // entries per layer of a slice
     unsigned long long counted = 0;
-    if (t < m.T && !(L.rowFlag && !L.rowFlag[L.flagBase + row])) {
+    if (tIdx < strideL && !(L.rowFlag && !L.rowFlag[L.flagBase + row])) {
         const uint32_t sample = L.firstSample + row;
-        const float2 S = __ldg(m.points + sample % m.Np);
+        const uint32_t pt = sample % m.Np;
+        const uint32_t t = L.cand ? __ldg(L.cand + size_t(pt) * L.K + tIdx) : tIdx;
+        const float2 S = __ldg(m.points + pt);
         const int ls = int(sample / m.Np);
         const float2 c = __ldg(m.centroid + t);
         const float area = __ldg(&m.geo[2 * t + 1].z);
@@ -299,7 +306,8 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
         const float D2 = sqrtf(fmaf(dx, dx, dy * dy));
         const float inv2 = 1.0f / D2;
         const float ux = dx * inv2, uy = dy * inv2;
-        float* outRow = L.lnw + size_t(row) * L.nW + t;
+        float* outRow = L.lnw + size_t(row) * L.nW + tIdx;
+        const size_t strideJ = size_t(strideL) * m.layers;
         const uint32_t nLines = L.slices * m.layers;
         for (uint32_t c0 = 0; c0 < nLines; c0 += TL * LPL) {
             float J[LPL], lnR[LPL], invc[LPL], nextPlane[LPL];
@@ -416,7 +424,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                     const float beta = __ldg(m.srcBeta + size_t(l) * m.T + t);
                     v = __logf(beta * area * m.h / D3sq) + J[g] * (sqrtf(D3sq) * inv2) + lnR[g];
                 }
-                outRow[size_t(sl[g]) * m.P + size_t(l) * m.T] = v;
+                outRow[size_t(sl[g]) * strideJ + size_t(l) * strideL] = v;
             }
         }
     }
@@ -439,11 +447,12 @@ uint32_t importanceTeamWidth(uint32_t lines) {
 // the counting team kernel (il.crossings accumulates the walk's crossings).
 cudaError_t launchImportance(uint32_t layers, const ImportanceLaunch& il, uint32_t meshLayers, uint32_t T,
                              uint32_t rows, cudaStream_t stream, bool tab = false, bool count = false) {
-    if (layers == 0 || count) {
+    if (layers == 0 || count || il.cand) {
         const uint32_t tl = importanceTeamWidth(il.slices * meshLayers);
+        const uint32_t nTri = il.cand ? il.K : T;
 #define HASE_TEAM(TL)                                                                         \
     {                                                                                         \
-        const dim3 grid((T + 256 / TL - 1) / (256 / TL), rows);                               \
+        const dim3 grid((nTri + 256 / TL - 1) / (256 / TL), rows);                            \
         if (count) importanceTeamKernel<TL, 3, false, true><<<grid, 256, 0, stream>>>(il);   \
         else if (tab) importanceTeamKernel<TL, 3, true><<<grid, 256, 0, stream>>>(il);       \
         else importanceTeamKernel<TL, 3><<<grid, 256, 0, stream>>>(il);                      \
@@ -614,6 +623,35 @@ __global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
 }
 
 // --------------------------------------------------------- (b) rays ----
+// The far prior of the local proposal: R_j beta V / d^2 over all (slice j,
+// prism) pairs, with d a softened distance from the image of the sample
+// point in slice j to the prism's cell of a 2-D grid of triangle cells at
+// the prism's layer, and R_j a reflectivity factor of the slice (1 for the
+// direct slice).  Drawn in three steps: a (cell, slice) pair from the row's
+// prefix of w_cj = sum_l R_j m_cl / d_clj^2, a layer by a scan of the same
+// terms, a triangle of the cell from the cell's beta V prefix of that
+// layer.  p_far(j, t, l) = R_j beta V / (d_clj^2 W), W = sum_cj w_cj, the
+// same expression wherever it is evaluated.
+struct FarView {
+    const uint32_t* cellOf;     // [T] cell of each triangle
+    const uint32_t* cellStart;  // [C + 1] cell segments of cellTris
+    const uint32_t* cellTris;   // [T] triangles grouped by cell, ascending within a cell
+    const float4* cell;         // [C] (x, y, softening^2, 0)
+    const float* cellMass;      // [C][layers] beta V of the cell's prisms of each layer
+    const float* triPrefix;     // [layers][T] in cellTris order: inclusive beta V prefix within the cell
+    const double* rowCdf;       // [rows][C][slices] inclusive prefix of the row's (cell, slice) weights
+    uint32_t C, slices;
+    float prior[5];             // R_j
+};
+
+__device__ __forceinline__ float farDistance2(float4 cell, float2 S, int l, int kImg, float h) {
+    const float dx = cell.x - S.x, dy = cell.y - S.y, dz = (float(l - kImg) + 0.5f) * h;
+    return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, cell.z)));
+}
+
+// One term of the far prior: R_j m / d^2.
+__device__ __forceinline__ float farTerm(float prior, float mass, float d2) { return __fdividef(prior * mass, d2); }
+
 struct RayLaunch {
     MeshView m;
     const uint32_t* active;       // active row ids
@@ -640,6 +678,20 @@ struct RayLaunch {
     const InstanceView* inst;
     const RowInfo* rows;
     const unsigned int* count;
+    // local proposal (LOCAL kernels): a mixture of two ray sources.  Rays
+    // [0, Mnear) follow the map over the K candidate triangles of the
+    // sample's point (entries j (layers K) + l K + k); rays [Mnear, M) are
+    // far rays, drawn from the prior beta V / d^2 over the whole medium (a
+    // slice uniformly).  Every ray is weighted by the mixture's probability
+    // of its (slice, prism), (Mnear q_b / Q + Mfar p_far) / M, so neither
+    // source has to exclude the other's prisms.
+    const uint32_t* cand;         // [Np][K] candidate triangles, nearest first
+    const uint32_t* candSorted;   // [Np][K] the same, ascending
+    const uint32_t* candRank;     // [Np][K] position in cand of each candSorted entry
+    uint32_t K, Mnear;
+    uint32_t slices, divKm, divKs;  // entries of a layer: floor(x / K) = (x * divKm) >> divKs
+    float nearShare, farShare;      // Mnear / M, (M - Mnear) / M
+    FarView far;
 };
 
 __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, uint32_t x) {
@@ -652,24 +704,23 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
     return lo;
 }
 
-// Start state of ray r of sample `sample`, drawn in entry b = slice * P +
-// prism of the sample's ray map: Philox4x32-10 counter (r, sample, pass,
-// kTagRay); a uniform point in the prism, or (nearField) the solid-angle
-// start in a prism touching the image point; the stratified wavelength bin
-// (floor(r nL / M) + phase) mod nL.  wf: the ray's weight without C Q,
-// beta V / (d^2 q) (uniform start) or beta alpha L / q (near field).
+// Start state of ray r of sample `sample`, drawn in reflection slice j and
+// prism p with probability qf / Q (qf: the map's integer weight q of the
+// entry, scaled for the local proposal's split): Philox4x32-10 counter (r,
+// sample, pass, kTagRay); a uniform point in the prism, or (nearField) the
+// solid-angle start in a prism touching the image point; the wavelength bin
+// floor((rs 0x9E3779B9 + phase mod 2^32) nL / 2^32), rs the ray's index in
+// its source (r itself, or for the local proposal's two sources the index
+// within its own range).  wf: the ray's weight
+// without C Q, beta V / (d^2 qf) (uniform start) or beta alpha L / qf (near
+// field).
 // Returns |start - image|^2 (0: the start point is the sample point itself).
-__device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_t b, uint32_t sample, float2 S, int ls,
-                                          uint32_t pass, uint32_t seedLo, uint32_t seedHi, uint32_t nLambda,
-                                          uint32_t lambdaPhase, uint32_t M, const float2* spec, const uint32_t* q,
-                                          uint32_t nearField, Ray& ray, float& wf) {
-    // reflection slice by subtraction (at most 4), layer by an exact
-    // multiply-shift: no integer divisions per ray
-    uint32_t j = 0, p = b;
-    while (p >= m.P) {
-        p -= m.P;
-        ++j;
-    }
+__device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_t rs, uint32_t j, uint32_t p,
+                                          uint32_t sample,
+                                          float2 S, int ls, uint32_t pass, uint32_t seedLo, uint32_t seedHi,
+                                          uint32_t nLambda, uint32_t lambdaPhase, const float2* spec,
+                                          float qf, uint32_t nearField, Ray& ray, float& wf) {
+    // layer by an exact multiply-shift: no integer division per ray
     const uint32_t l = prismLayer(m, p), t = p - l * m.T;
     const Philox4 rnd = philox4x32_10(r, sample, pass, kTagRay, seedLo, seedHi);
     uint32_t k1 = rnd.x >> 8, k2 = rnd.y >> 8;
@@ -678,25 +729,19 @@ __device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_
         k2 = (1u << 24) - 1u - k2;
     }
     const int kImg = imageLevel(ls, int(m.layers), j);
-    // stratified wavelength bin without a 64-bit division: an FP32 estimate
-    // of the quotient (off by at most 1 for nL < 2^22) and one exact
-    // correction on the 64-bit products; the quotient is below nL (r < M)
-    uint32_t lam = 0u;
-    if (nLambda > 1) {
-        const uint64_t num = uint64_t(r) * nLambda;
-        uint32_t qb = uint32_t(float(r) * (float(nLambda) / float(M)));
-        if (uint64_t(qb) * M > num) --qb;
-        else if (uint64_t(qb + 1u) * M <= num) ++qb;
-        lam = qb + lambdaPhase;
-        if (lam >= nLambda) lam -= nLambda;
-    }
+    // wavelength bin: a golden-ratio (Weyl) sequence over the ray's index in
+    // its source, offset by the row's 32-bit phase of this pass.  Every ray's
+    // bin is uniform and independent of its prism (the phase is), and the
+    // consecutive rays of one prism spread over the spectrum, so the rays'
+    // sample variance is the estimate's
+    const uint32_t lam = nLambda > 1 ? __umulhi(rs * kWeylStep + lambdaPhase, nLambda) : 0u;
     const float2 ab = __ldg(spec + lam);
     float dx, dy, dz, alphaL, D2;
     if (nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
         nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
                        unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
         D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
-        wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, float(__ldg(q + b)));
+        wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, qf);
     } else {
         const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
         const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
@@ -704,9 +749,106 @@ __device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_
         const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
         D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j, ab.x, ab.y,
                      m.h);
-        wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * float(__ldg(q + b)));
+        wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * qf);
     }
     return D2;
+}
+
+// The (slice j, prism p) of ray r of a local-proposal row and its mixture
+// weight qf, startRay's divisor: the ray contributes C Qn beta V e^G /
+// (d^2 qf), so qf = Qn P_mix = Mnear/M q_b + Mfar/M Qn p_far.  Near rays take
+// the map's entry b; far rays draw from the prior (one Philox block: the
+// (cell, slice) pair from 53 bits, the layer, the triangle) and look the
+// drawn triangle up among the point's candidates for its q_b.  bsel: the prism's
+// candidate entry (for the contribution log) or ~0u.  Returns false for a
+// ray without a source (qf = 0).
+__device__ __forceinline__ bool localSource(const RayLaunch& L, const MeshView& m, uint32_t row, uint32_t sample,
+                                            float2 S, uint32_t r, const uint32_t* q, const uint32_t* off,
+                                            uint32_t pb, uint32_t count, unsigned long long Qrow,
+                                            unsigned long long Qn, uint32_t seedLo, uint32_t& j, uint32_t& p,
+                                            float& qf, uint32_t& bsel) {
+    const uint32_t pt = sample % m.Np;
+    const int ls = int(sample / m.Np);
+    const uint32_t layerK = m.layers * L.K;
+    const FarView& F = L.far;
+    uint32_t t, l, b = 0xffffffffu, cellIdx = 0;
+    j = 0;
+    if (r < L.Mnear) {
+        if (Qrow == 0ull) return false;  // the map places no near ray in a row without candidate weight
+        b = pb + upperBound(off + pb, count, r) - 1u;
+        uint32_t rem = b;  // entry j (layers K) + l K + k
+        while (rem >= layerK) {
+            rem -= layerK;
+            ++j;
+        }
+        l = uint32_t((uint64_t(rem) * L.divKm) >> L.divKs);
+        t = __ldg(L.cand + size_t(pt) * L.K + (rem - l * L.K));
+        if (L.farShare > 0.0f) cellIdx = __ldg(F.cellOf + t);
+    } else {
+        const uint32_t nE = F.C * F.slices;
+        const double* cdf = F.rowCdf + size_t(row) * nE;
+        const double total = __ldg(cdf + nE - 1);
+        if (!(total > 0.0)) return false;
+        const Philox4 a = philox4x32_10(r, sample, L.pass, kTagFar, seedLo, L.seedHi);
+        const double target = double((uint64_t(a.x) << 21) | (a.y >> 11)) * (1.0 / 9007199254740992.0) * total;
+        uint32_t lo = 0, hi = nE - 1;  // first (cell, slice) whose inclusive prefix exceeds the target
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(cdf + mid) <= target) lo = mid + 1;
+            else hi = mid;
+        }
+        cellIdx = lo / F.slices;
+        j = lo - cellIdx * F.slices;
+        const int kImg = imageLevel(ls, int(m.layers), j);
+        const float4 cl = __ldg(F.cell + cellIdx);
+        const float wc = float(__ldg(cdf + lo) - (lo ? __ldg(cdf + lo - 1) : 0.0));
+        const float target2 = unit24(a.z >> 8) * wc;
+        const float prior = F.prior[j];
+        const float* mass = F.cellMass + size_t(cellIdx) * m.layers;
+        float acc = 0.0f;  // the layer terms of farRowKernel, in its order
+        l = 0xffffffffu;
+        for (uint32_t l2 = 0; l2 < m.layers; ++l2) {
+            const float mcl = __ldg(mass + l2);
+            if (!(mcl > 0.0f)) continue;
+            acc += farTerm(prior, mcl, farDistance2(cl, S, int(l2), kImg, m.h));
+            l = l2;
+            if (acc > target2) break;
+        }
+        if (l == 0xffffffffu) return false;
+        const uint32_t s0 = __ldg(F.cellStart + cellIdx), s1 = __ldg(F.cellStart + cellIdx + 1);
+        const float* pre = F.triPrefix + size_t(l) * m.T;
+        const float target3 = unit24(a.w >> 8) * __ldg(pre + s1 - 1);
+        uint32_t lo3 = s0, hi3 = s1 - 1;  // first triangle of the cell whose prefix exceeds the target
+        while (lo3 < hi3) {
+            const uint32_t mid = (lo3 + hi3) >> 1;
+            if (__ldg(pre + mid) <= target3) lo3 = mid + 1;
+            else hi3 = mid;
+        }
+        t = __ldg(F.cellTris + lo3);
+        if (Qrow != 0ull) {  // a candidate triangle: its entry b
+            const uint32_t* cs = L.candSorted + size_t(pt) * L.K;
+            uint32_t x = 0, e = L.K;
+            while (x < e) {
+                const uint32_t mid = (x + e) >> 1;
+                if (__ldg(cs + mid) < t) x = mid + 1;
+                else e = mid;
+            }
+            if (x < L.K && __ldg(cs + x) == t) b = j * layerK + l * L.K + __ldg(L.candRank + size_t(pt) * L.K + x);
+        }
+    }
+    p = t + l * m.T;
+    float pf = 0.0f;
+    if (L.farShare > 0.0f) {
+        const float bv = __ldg(m.srcBeta + p) * __ldg(&m.geo[2 * t + 1].z) * m.h;
+        const uint32_t nE = F.C * F.slices;
+        const float W = float(__ldg(F.rowCdf + size_t(row) * nE + nE - 1));
+        pf = farTerm(F.prior[j], bv, farDistance2(__ldg(F.cell + cellIdx), S, int(l), imageLevel(ls, int(m.layers), j),
+                                                  m.h)) / W;
+    }
+    const float qb = b != 0xffffffffu ? float(__ldg(q + b)) : 0.0f;
+    qf = fmaf(L.nearShare, qb, L.farShare * float(Qn) * pf);
+    bsel = b;
+    return qf > 0.0f;
 }
 
 // Persistent ray kernel: every warp repeatedly takes a work item -- itemRays
@@ -720,7 +862,7 @@ __device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_
 // walks from there, and the number of active rows is read on the device.
 // WALK: how the walk obtains each prism's g (WalkMode).
 template <int BLOCK, int REFILL, int MINB, bool LOG = false, bool POOL = false, int COLS = kWalkColumns,
-          int WALK = kWalkBeta>
+          int WALK = kWalkBeta, bool LOCAL = false>
 __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
     __shared__ InstanceView sInst[POOL ? BLOCK / 32 : 1];
     const int lane = threadIdx.x & 31;
@@ -736,7 +878,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
         const uint32_t k = item % L.itemsPerRow;
         const size_t slot = size_t(row) * kMaxItems + k;
         const unsigned long long Qrow = L.Q[row];
-        if (Qrow == 0ull) {  // no source prism: every ray contributes 0
+        if (!LOCAL && Qrow == 0ull) {  // no source prism: every ray contributes 0
             if (lane == 0) {
                 L.pSum[slot] = 0.0;
                 L.pSum2[slot] = 0.0;
@@ -780,17 +922,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
         const uint32_t r1 = min(r0 + L.itemRays, L.M);
         const uint32_t* off = L.offsets + oBase;
         const uint32_t* q = L.q + wBase;
-        const double CQ = Cm * double(Qrow);
+        // local proposal without candidate weight (Q = 0): only far rays, their
+        // mixture weight taken against Qn = 1
+        const unsigned long long Qn = LOCAL && Qrow == 0ull ? 1ull : Qrow;
+        const double CQ = Cm * double(Qn);
         const float2 S = __ldg(m.points + sample % m.Np);
         const int ls = int(sample / m.Np);
         const uint32_t lambdaPhase =
-            HASE_N_LAMBDA > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, HASE_SEED_LO, L.seedHi).y % HASE_N_LAMBDA : 0u;
-        // prisms holding the item's rays: [pb, pb + count - 1)
+            HASE_N_LAMBDA > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, HASE_SEED_LO, L.seedHi).y : 0u;
+        // prisms holding the item's mapped rays [r0, rn1): [pb, pb + count - 1)
+        // (the local proposal maps its near rays [0, Mnear) only)
+        const uint32_t rn1 = LOCAL ? min(r1, L.Mnear) : r1;
         uint32_t bound = 0;
-        if (lane == 0) bound = upperBound(off, nW + 1, r0) - 1u;
-        if (lane == 1) bound = upperBound(off, nW + 1, r1 - 1u) - 1u;
+        if (r0 < rn1) {
+            if (lane == 0) bound = upperBound(off, nW + 1, r0) - 1u;
+            if (lane == 1) bound = upperBound(off, nW + 1, rn1 - 1u) - 1u;
+        }
         const uint32_t pb = __shfl_sync(0xffffffffu, bound, 0);
-        const uint32_t count = __shfl_sync(0xffffffffu, bound, 1) - pb + 2u;
+        const uint32_t count = r0 < rn1 ? __shfl_sync(0xffffffffu, bound, 1) - pb + 2u : 0u;
 
         double sum = 0.0, sum2 = 0.0;
         uint32_t dropped = 0, crossings = 0;
@@ -806,12 +955,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
             if (fetch < r1 && (nIdle >= REFILL || nIdle == 32)) {
                 const uint32_t r = fetch + __popc(idle & laneLt);
                 if (!active && r < r1) {
-                    const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
-                    if (LOG) bsel = b;
-                    const float D2 = startRay(m, r, b, sample, S, ls, L.pass, HASE_SEED_LO, L.seedHi, HASE_N_LAMBDA,
-                                              lambdaPhase, L.M, HASE_SPEC, q, L.nearField, ray, wf);
-                    active = D2 > 0.0f;
-                    if (!active) ++dropped;  // start point on the sample point itself
+                    uint32_t j = 0, p = 0;
+                    float qf = 1.0f;
+                    bool go = true;
+                    if constexpr (LOCAL) {
+                        uint32_t bl = 0xffffffffu;
+                        go = localSource(L, m, row, sample, S, r, q, off, pb, count, Qrow, Qn, HASE_SEED_LO, j, p,
+                                         qf, bl);
+                        if (LOG) bsel = bl;
+                    } else {
+                        const uint32_t b = pb + upperBound(off + pb, count, r) - 1u;
+                        if (LOG) bsel = b;
+                        // reflection slice by subtraction (at most 4)
+                        p = b;
+                        while (p >= m.P) {
+                            p -= m.P;
+                            ++j;
+                        }
+                        qf = float(__ldg(q + b));
+                    }
+                    if (go) {
+                        // wavelength sequence: over the rays of the ray's source
+                        const bool farRay = LOCAL && r >= L.Mnear;
+                        const float D2 = startRay(m, r, farRay ? r - L.Mnear : r, j, p, sample, S, ls, L.pass,
+                                                  HASE_SEED_LO, L.seedHi, HASE_N_LAMBDA, lambdaPhase, HASE_SPEC, qf,
+                                                  L.nearField, ray, wf);
+                        active = D2 > 0.0f;
+                        if (!active) ++dropped;  // start point on the sample point itself
+                    }
                 }
                 fetch += uint32_t(nIdle);
             }
@@ -827,7 +998,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         const double X = CQ * double(wf) * eg;
                         sum += X;
                         sum2 += X * X;
-                        if (LOG) atomicAdd(L.logBuf + wBase + bsel, float(X));
+                        if (LOG && (!LOCAL || bsel != 0xffffffffu)) atomicAdd(L.logBuf + wBase + bsel, float(X));
                     } else {
                         ++dropped;
                     }
@@ -899,6 +1070,11 @@ const RayVariant kPoolVariants[] = {
 };
 #undef HASE_POOL_SHAPE
 static_assert(sizeof(kPoolVariants) == sizeof(kRayVariants), "one batched variant per launch shape");
+// Ray kernels of the local proposal: the default's persistent 512-thread,
+// 64-column shape in every walk mode, and the contribution-logging kernel.
+const RayVariant kLocalVariant{rayKernel<512, 8, 2, false, false, 64, kWalkBeta, true>, 512, "local",
+                               rayKernel<512, 8, 2, false, false, 64, kWalkTable, true>,
+                               rayKernel<512, 8, 2, false, false, 64, kWalkBetaNoClad, true>};
 
 // ------------------------------------------------ (c)+(d) finalise ----
 struct FinalizeLaunch {
@@ -1152,6 +1328,10 @@ struct ProposalView {
     float lnVref;           // ln(mean prism volume / R^2)
     float lnSigmaRatio;     // ln(sigma_e / sigma_a) of the averaged spectrum
     uint32_t firstSample, nW;
+    // local proposal: pair jp is candidate entry j (layers K) + l K + k of the
+    // sample's point (cand null: jp = j P + prism)
+    const uint32_t* cand;
+    uint32_t K, divKm, divKs;
 };
 
 __device__ __forceinline__ float sliceLnReflect(const ProposalView& V, uint32_t j) {
@@ -1163,14 +1343,27 @@ __device__ __forceinline__ float pairFeatures(const ProposalView& V, uint32_t sa
     const MeshView& m = V.m;
     // (slice, prism) and (triangle, layer), sample point and level: no
     // integer divisions (slices by subtraction, the rest by multiply-shift)
-    uint32_t j = 0, p = jp;
-    while (p >= m.P) {
-        p -= m.P;
-        ++j;
-    }
-    const uint32_t l = prismLayer(m, p), t = p - l * m.T;
     const uint32_t lsU = sampleLevel(m, sample);
-    const float2 S = __ldg(m.points + (sample - lsU * m.Np));
+    const uint32_t pt = sample - lsU * m.Np;
+    uint32_t j = 0, p = jp, l, t;
+    if (V.cand) {
+        const uint32_t layerK = m.layers * V.K;
+        while (p >= layerK) {
+            p -= layerK;
+            ++j;
+        }
+        l = uint32_t((uint64_t(p) * V.divKm) >> V.divKs);
+        t = __ldg(V.cand + size_t(pt) * V.K + (p - l * V.K));
+        p = t + l * m.T;
+    } else {
+        while (p >= m.P) {
+            p -= m.P;
+            ++j;
+        }
+        l = prismLayer(m, p);
+        t = p - l * m.T;
+    }
+    const float2 S = __ldg(m.points + pt);
     const int ls = int(lsU);
     const float zs = float(ls) * m.h;
     const float zi = float(imageLevel(ls, int(m.layers), j)) * m.h;
@@ -1551,6 +1744,164 @@ hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& exte
     return HASE_OK;
 }
 
+// The far prior's tables of the current beta: per (layer, cell) the cell's
+// beta V prefix over its triangles (cellTris order) and its total.  One
+// thread per (layer, cell).
+__global__ void farCellKernel(const uint32_t* cellStart, const uint32_t* cellTris, uint32_t C, const float* srcBeta,
+                              const float4* geo, uint32_t T, uint32_t layers, float h, float* cellMass,
+                              float* triPrefix) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= C * layers) return;
+    const uint32_t l = idx / C, c = idx - l * C;
+    const uint32_t s0 = cellStart[c], s1 = cellStart[c + 1];
+    float run = 0.0f;
+    for (uint32_t i = s0; i < s1; ++i) {
+        const uint32_t t = cellTris[i];
+        run += srcBeta[size_t(l) * T + t] * geo[2 * t + 1].z * h;
+        triPrefix[size_t(l) * T + i] = run;
+    }
+    cellMass[size_t(c) * layers + l] = run;
+}
+
+struct FarRowLaunch {
+    const float4* cell;
+    const float* cellMass;
+    uint32_t C, slices, layers, Np, firstSample;
+    const float2* points;
+    float h;
+    float prior[5];
+    double* rowCdf;  // [rows][C][slices]
+};
+
+// Per sample row of a chunk: the inclusive FP64 prefix over (cell, slice)
+// pairs of the far prior's weights w_cj = sum_l R_j m_cl / d_clj^2 (FP32,
+// layers in order, empty layers skipped: the terms localSource's layer scan
+// adds).  One block per row, 256 pairs per step, warp-shuffle scans.
+__global__ void __launch_bounds__(256) farRowKernel(FarRowLaunch L) {
+    __shared__ double wsum[8];
+    const uint32_t row = blockIdx.x, sample = L.firstSample + row;
+    const float2 S = L.points[sample % L.Np];
+    const int ls = int(sample / L.Np);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nE = L.C * L.slices;
+    double* out = L.rowCdf + size_t(row) * nE;
+    double carry = 0.0;
+    for (uint32_t e0 = 0; e0 < nE; e0 += 256) {
+        const uint32_t e = e0 + threadIdx.x;
+        float w = 0.0f;
+        if (e < nE) {
+            const uint32_t c = e / L.slices, j = e - c * L.slices;
+            const int kImg = imageLevel(ls, int(L.layers), j);
+            const float prior = L.prior[j];
+            const float4 cl = L.cell[c];
+            const float* mass = L.cellMass + size_t(c) * L.layers;
+            for (uint32_t l = 0; l < L.layers; ++l) {
+                const float mcl = mass[l];
+                if (!(mcl > 0.0f)) continue;
+                w += farTerm(prior, mcl, farDistance2(cl, S, int(l), kImg, L.h));
+            }
+        }
+        double x = double(w);
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        double base = carry, block = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            if (k < warp) base += wsum[k];
+            block += wsum[k];
+        }
+        if (e < nE) out[e] = base + x;
+        carry += block;
+        __syncthreads();
+    }
+}
+
+// The K triangles nearest to every point (by centroid distance, ties by
+// index): nearest first, and the same set by ascending index.
+void buildCandidates(const std::vector<float2>& points, const std::vector<float2>& centroid, uint32_t K,
+                     std::vector<uint32_t>& nearest, std::vector<uint32_t>& sorted, std::vector<uint32_t>& rank) {
+    const uint32_t Np = uint32_t(points.size()), T = uint32_t(centroid.size());
+    nearest.resize(size_t(Np) * K);
+    sorted.resize(size_t(Np) * K);
+    rank.resize(size_t(Np) * K);
+    std::vector<std::pair<double, uint32_t>> d(T);
+    std::vector<std::pair<uint32_t, uint32_t>> byTri(K);
+    for (uint32_t pt = 0; pt < Np; ++pt) {
+        for (uint32_t t = 0; t < T; ++t) {
+            const double dx = double(centroid[t].x) - points[pt].x, dy = double(centroid[t].y) - points[pt].y;
+            d[t] = {dx * dx + dy * dy, t};
+        }
+        std::partial_sort(d.begin(), d.begin() + K, d.end());
+        for (uint32_t k = 0; k < K; ++k) {
+            nearest[size_t(pt) * K + k] = d[k].second;
+            byTri[k] = {d[k].second, k};
+        }
+        std::sort(byTri.begin(), byTri.end());
+        for (uint32_t k = 0; k < K; ++k) {
+            sorted[size_t(pt) * K + k] = byTri[k].first;
+            rank[size_t(pt) * K + k] = byTri[k].second;
+        }
+    }
+}
+
+constexpr double kFarCellTriangles = 8.0;  // triangles per cell of the far prior's grid (bounding-box average)
+
+// The far prior's cells: a square grid of side a over the triangle
+// centroids' bounding box, a^2 = box area x kFarCellTriangles / T; the
+// non-empty cells in row-major order, each with the mean centroid of its
+// triangles and the softening (a/2)^2; the triangles of each cell ascending.
+void buildFarCells(const std::vector<float2>& centroid, std::vector<uint32_t>& cellOf, std::vector<uint32_t>& cellStart,
+                   std::vector<uint32_t>& cellTris, std::vector<float4>& cellXY) {
+    const uint32_t T = uint32_t(centroid.size());
+    double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+    for (const float2& c : centroid) {
+        x0 = std::min(x0, double(c.x));
+        x1 = std::max(x1, double(c.x));
+        y0 = std::min(y0, double(c.y));
+        y1 = std::max(y1, double(c.y));
+    }
+    const double w = std::max(x1 - x0, 1e-12), hgt = std::max(y1 - y0, 1e-12);
+    const double a = std::sqrt(w * hgt * kFarCellTriangles / double(std::max(T, 1u)));
+    const uint32_t gx = uint32_t(std::min(4096.0, std::max(1.0, std::ceil(w / a))));
+    const uint32_t gy = uint32_t(std::min(4096.0, std::max(1.0, std::ceil(hgt / a))));
+    std::vector<uint32_t> grid(T);
+    for (uint32_t t = 0; t < T; ++t) {
+        const uint32_t ix = std::min(gx - 1, uint32_t(std::max(0.0, (double(centroid[t].x) - x0) / a)));
+        const uint32_t iy = std::min(gy - 1, uint32_t(std::max(0.0, (double(centroid[t].y) - y0) / a)));
+        grid[t] = iy * gx + ix;
+    }
+    std::vector<uint32_t> compact(size_t(gx) * gy, 0xffffffffu), count;
+    std::vector<uint32_t> order(T);
+    for (uint32_t t = 0; t < T; ++t) order[t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t u, uint32_t v) { return grid[u] < grid[v]; });
+    cellOf.assign(T, 0);
+    cellStart.clear();
+    cellTris.assign(order.begin(), order.end());
+    cellXY.clear();
+    for (uint32_t i = 0; i < T; ++i) {
+        const uint32_t t = order[i];
+        if (compact[grid[t]] == 0xffffffffu) {
+            compact[grid[t]] = uint32_t(cellStart.size());
+            cellStart.push_back(i);
+        }
+        cellOf[t] = compact[grid[t]];
+    }
+    cellStart.push_back(T);
+    const uint32_t C = uint32_t(cellStart.size() - 1);
+    for (uint32_t c = 0; c < C; ++c) {
+        double sx = 0.0, sy = 0.0;
+        for (uint32_t i = cellStart[c]; i < cellStart[c + 1]; ++i) {
+            sx += centroid[cellTris[i]].x;
+            sy += centroid[cellTris[i]].y;
+        }
+        const double n = double(cellStart[c + 1] - cellStart[c]);
+        cellXY.push_back(make_float4(float(sx / n), float(sy / n), float(0.25 * a * a), 0.0f));
+    }
+}
+
 // The importance kernel's line order: for every sample level ls, the lines
 // q = l * slices + j (layer l, reflection slice j) by increasing distance
 // |l + 1/2 - kImg| to the image level (ties by q).  A line crosses about that
@@ -1589,6 +1940,21 @@ struct hase_context {
     DevBuf<float4> tri, geo;
     DevBuf<int4> verts;
     DevBuf<uint16_t> lineOrder[2];  // importance line order per sample level: 1 and 5 reflection slices
+    // local proposal (hase_context_set_local_proposal): per point the K
+    // triangles nearest to it (by centroid distance, nearest first) and the
+    // same set by ascending index; the far proposal's prefix of beta V over
+    // the prisms and each point's candidate share of it, per beta version
+    uint32_t localK = 0;
+    float farFraction = 0.0f;
+    DevBuf<uint32_t> candTri, candSorted, candRank;
+    // the far prior: triangle cells (once per mesh), their beta V tables
+    // (once per beta version), and the cell prefixes of a chunk's rows
+    uint32_t farCells = 0;
+    DevBuf<uint32_t> cellOf, cellStart, cellTris;
+    DevBuf<float4> cellXY;
+    DevBuf<float> cellMass, triPrefix;
+    DevBuf<double> farRow;
+    uint64_t farVersion = 0;
     DevBuf<float2> centroid, points, spec;
     DevBuf<float> gainBeta, srcBeta, reflect;
     DevBuf<float> gTab;  // g of every prism for the spectrally averaged (A, B) of the last solve
@@ -1683,6 +2049,102 @@ uint32_t adaptiveTarget(uint32_t minRays, uint32_t maxRays, uint32_t steps, uint
 hase_status setDevice(hase_context* c) {
     HASE_CUDA(cudaSetDevice(c->device));
     return HASE_OK;
+}
+
+// Local proposal: candidate lists for the set K (once), and the far tables
+// of the current beta (one prefix kernel and one per-point kernel on the
+// context's stream, once per beta version).
+hase_status prepareLocal(hase_context* c) {
+    if (c->candTri.n != size_t(c->Np) * c->localK) {
+        std::vector<uint32_t> nearest, sorted, rank;
+        buildCandidates(c->hPoints, c->hCentroid, c->localK, nearest, sorted, rank);
+        c->candTri.release();
+        c->candSorted.release();
+        c->candRank.release();
+        HASE_CUDA(c->candTri.ensure(nearest.size()));
+        HASE_CUDA(c->candSorted.ensure(sorted.size()));
+        HASE_CUDA(c->candRank.ensure(rank.size()));
+        HASE_CUDA(cudaMemcpy(c->candTri.p, nearest.data(), nearest.size() * 4, cudaMemcpyHostToDevice));
+        HASE_CUDA(cudaMemcpy(c->candSorted.p, sorted.data(), sorted.size() * 4, cudaMemcpyHostToDevice));
+        HASE_CUDA(cudaMemcpy(c->candRank.p, rank.data(), rank.size() * 4, cudaMemcpyHostToDevice));
+    }
+    if (c->localK >= c->T) return HASE_OK;  // every triangle is a candidate: no far rays
+    if (c->farCells == 0) {
+        std::vector<uint32_t> cellOf, cellStart, cellTris;
+        std::vector<float4> cellXY;
+        buildFarCells(c->hCentroid, cellOf, cellStart, cellTris, cellXY);
+        const uint32_t C = uint32_t(cellXY.size());
+        HASE_CUDA(c->cellOf.ensure(cellOf.size()));
+        HASE_CUDA(c->cellStart.ensure(cellStart.size()));
+        HASE_CUDA(c->cellTris.ensure(cellTris.size()));
+        HASE_CUDA(c->cellXY.ensure(C));
+        HASE_CUDA(c->cellMass.ensure(size_t(C) * c->layers));
+        HASE_CUDA(c->triPrefix.ensure(c->P));
+        HASE_CUDA(cudaMemcpy(c->cellOf.p, cellOf.data(), cellOf.size() * 4, cudaMemcpyHostToDevice));
+        HASE_CUDA(cudaMemcpy(c->cellStart.p, cellStart.data(), cellStart.size() * 4, cudaMemcpyHostToDevice));
+        HASE_CUDA(cudaMemcpy(c->cellTris.p, cellTris.data(), cellTris.size() * 4, cudaMemcpyHostToDevice));
+        HASE_CUDA(cudaMemcpy(c->cellXY.p, cellXY.data(), C * sizeof(float4), cudaMemcpyHostToDevice));
+        c->farCells = C;
+        c->farVersion = 0;
+    }
+    if (c->farVersion != c->betaVersion) {
+        const uint32_t n = c->farCells * c->layers;
+        farCellKernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->cellStart.p, c->cellTris.p, c->farCells, c->srcBeta.p,
+                                                              c->geo.p, c->T, c->layers, float(c->h), c->cellMass.p,
+                                                              c->triPrefix.p);
+        HASE_CUDA(cudaGetLastError());
+        c->farVersion = c->betaVersion;
+    }
+    return HASE_OK;
+}
+
+// The far prior's slice factors R_j: 1 for the direct slice; the mean
+// reflectivity of the surfaces of the slice's bounces otherwise, each at
+// least 1/4 (rays beyond the critical angle reflect totally).
+void farSlicePrior(const hase_context* c, uint32_t slices, float prior[5]) {
+    double R[2] = {0.0, 0.0};
+    if (c->hasReflect && !c->hReflect.empty())
+        for (uint32_t t = 0; t < c->T; ++t)
+            for (int s = 0; s < 2; ++s) R[s] += double(c->hReflect[2 * t + s]) / double(c->T);
+    const double Rb = std::max(R[0], 0.25), Rt = std::max(R[1], 0.25);
+    const double v[5] = {1.0, Rb, Rt, Rb * Rt, Rt * Rb};
+    for (uint32_t j = 0; j < 5; ++j) prior[j] = j < slices ? float(v[j]) : 0.0f;
+}
+
+// The far prior's view of a context for a solve of `slices` reflection
+// slices (rowCdf: the chunk's row prefixes).
+FarView farView(const hase_context* c, uint32_t slices) {
+    FarView f{};
+    f.slices = slices;
+    farSlicePrior(c, slices, f.prior);
+    f.cellOf = c->cellOf.p;
+    f.cellStart = c->cellStart.p;
+    f.cellTris = c->cellTris.p;
+    f.cell = c->cellXY.p;
+    f.cellMass = c->cellMass.p;
+    f.triPrefix = c->triPrefix.p;
+    f.rowCdf = c->farRow.p;
+    f.C = c->farCells;
+    return f;
+}
+
+// Entries of a sample's weight row: every (slice, prism), or with the local
+// proposal the (slice, layer, candidate) entries.
+uint32_t rowEntries(const hase_context* c, uint32_t slices) {
+    return c->localK ? slices * c->layers * c->localK : slices * c->P;
+}
+
+// The local proposal's candidate fields of a launch's views.
+void localFields(hase_context* c, ProposalView& pv) {
+    if (!c->localK) return;
+    pv.cand = c->candTri.p;
+    pv.K = c->localK;
+    invariantDivisor(c->localK, pv.divKm, pv.divKs);
+}
+void localFields(hase_context* c, ImportanceLaunch& il) {
+    if (!c->localK) return;
+    il.cand = c->candTri.p;
+    il.K = c->localK;
 }
 
 struct LearnedArgs {
@@ -2007,6 +2469,16 @@ hase_status hase_context_update_beta(hase_context* c, const double* betaVolume, 
     return HASE_OK;
 }
 
+hase_status hase_context_set_local_proposal(hase_context* c, uint32_t triangles, float farFraction) {
+    if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
+    if (!(farFraction >= 0.0f) || farFraction >= 1.0f) return fail(HASE_INVALID_ARGUMENT, "farFraction must be in [0, 1)");
+    if (uint64_t(triangles) * c->layers * 5u >= (1ull << 31))
+        return fail(HASE_INVALID_ARGUMENT, "too many local triangles for this mesh");
+    c->localK = std::min(triangles, c->T);
+    c->farFraction = farFraction > 0.0f ? farFraction : 0.125f;
+    return HASE_OK;
+}
+
 hase_status hase_context_destroy(hase_context* c) {
     if (!c) return HASE_OK;
     cudaSetDevice(c->device);
@@ -2038,7 +2510,14 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     const uint32_t maxRays = std::max(ex->maxRays, ex->minRays);
     const uint32_t nS = last - first + 1;
     const uint32_t slices = ex->useReflections ? 5u : 1u;
-    const uint32_t nW = slices * c->P;
+    // local proposal: a row holds the point's K candidate triangles x layers
+    // x slices; the rest of the medium is sampled by the far rays
+    const bool local = c->localK > 0;
+    const uint32_t K = c->localK;
+    const uint32_t nW = local ? slices * c->layers * K : slices * c->P;
+    if (local) HASE_TRY(prepareLocal(c));
+    uint32_t divKm = 0, divKs = 0;
+    if (local) invariantDivisor(K, divKm, divKs);
 
     // spectrum: (A, B) per wavelength, g = beta*A - B
     const uint32_t nLambda = ex->monochromatic ? 1u : uint32_t(c->sigmaA.size());
@@ -2069,12 +2548,14 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
 
     // batch rows by the workspace budget
     const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
-    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxItems * 28ull + 64;
+    const bool farPrior = local && K < c->T;
+    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxItems * 28ull + 64 + (farPrior ? uint64_t(c->farCells) * slices * 8ull : 0ull);
     uint32_t rows = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nS, budget / perRow)));
     HASE_CUDA(c->lnw.ensure(size_t(rows) * nW));
     HASE_CUDA(c->q.ensure(size_t(rows) * nW));
     HASE_CUDA(c->offsets.ensure(size_t(rows) * (nW + 1)));
     HASE_CUDA(c->Q.ensure(rows));
+    if (farPrior) HASE_CUDA(c->farRow.ensure(size_t(rows) * c->farCells * slices));
     HASE_CUDA(c->activeA.ensure(rows));
     HASE_CUDA(c->activeB.ensure(rows));
     HASE_CUDA(c->counter.ensure(1));
@@ -2130,7 +2611,6 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, float(meanA), float(meanB),
                                                                float(c->cladAbs), c->P, c->gTab.p);
     HASE_CUDA(cudaGetLastError());
-    res->kernelLaunches += 1;
     const MeshView mv = c->view();
     const double C = c->nTot / (4.0 * kPi * c->tau);
     std::vector<float> hPhi(rows);
@@ -2144,7 +2624,7 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     res->totalMilliseconds = 0;
     res->passes = 0;
     res->unconvergedSamples = 0;
-    res->kernelLaunches = 0;
+    res->kernelLaunches = 1;  // the gain table
     uint64_t droppedTotal = 0;
 
     for (uint32_t b0 = 0; b0 < nS; b0 += rows) {
@@ -2152,12 +2632,15 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         const uint32_t firstSample = first + b0;
         HASE_CUDA(cudaEventRecord(c->ev[0], c->stream));
         ImportanceLaunch il{mv, firstSample, slices, nW, float(meanA), float(meanB), c->lnw.p, nullptr};
+        il.cand = local ? c->candTri.p : nullptr;
+        il.K = K;
         auto launchImportanceRows = [&](uint32_t nLaunchRows) {
             launchImportance(cp->importanceLayers, il, c->layers, c->T, nLaunchRows, c->stream, true);
         };
         if (la) {
             pv.firstSample = firstSample;
             pv.nW = nW;
+            localFields(c, pv);
             ProposalLaunch pl{pv, la->net->wimg.p, la->net->vec.p, c->lnw.p, c->priorBuf.p, nullptr, nRows,
                               la->net->error.p};
             const uint64_t tiles = (uint64_t(nRows) * nW + kTile - 1) / kTile;
@@ -2167,6 +2650,13 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             res->kernelLaunches += 1;
         } else {
             launchImportanceRows(nRows);
+        }
+        if (farPrior) {  // the far prior's cell prefixes of the chunk's rows
+            FarRowLaunch fl{c->cellXY.p, c->cellMass.p, c->farCells, slices, c->layers, c->Np, firstSample,
+                            c->points.p, float(c->h), {}, c->farRow.p};
+            farSlicePrior(c, slices, fl.prior);
+            farRowKernel<<<nRows, 256, 0, c->stream>>>(fl);
+            res->kernelLaunches += 1;
         }
         HASE_CUDA(cudaGetLastError());
         if (logOut) HASE_CUDA(cudaMemsetAsync(c->logBuf.p, 0, size_t(nRows) * nW * sizeof(float), c->stream));
@@ -2188,7 +2678,14 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             const uint32_t target = adaptiveTarget(ex->minRays, maxRays, cp->adaptiveSteps, pass);
             const bool lastPass = target >= maxRays || pass >= cp->adaptiveSteps;
             const uint32_t M = target - prevTarget;
-            MapLaunch ml{c->lnw.p, 1, pass == 0 ? 1 : 0, cur, nW, M, nullptr, firstSample, pass, cp->rngSeed, 0u,
+            // local proposal: the map places the near rays, the rest are far
+            // rays; both parts get at least one ray (a one-ray pass is near only)
+            const uint32_t Mfar = farPrior && M >= 2u
+                                      ? uint32_t(std::min<long long>(M - 1u, std::max(1ll, std::llround(double(M) *
+                                                                                                       c->farFraction))))
+                                      : 0u;
+            const uint32_t Mnear = M - Mfar;
+            MapLaunch ml{c->lnw.p, 1, pass == 0 ? 1 : 0, cur, nW, Mnear, nullptr, firstSample, pass, cp->rngSeed, 0u,
                          nullptr, c->q.p, c->Q.p, c->offsets.p};
             mapKernel<<<nActive, kMapBlock, 0, c->stream>>>(ml);
             HASE_CUDA(cudaGetLastError());
@@ -2200,12 +2697,33 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             RayLaunch rl{mv, cur, nActive, firstSample, pass, M, nW, itemRays, items, c->itemCounter.p, c->q.p,
                          c->Q.p, c->offsets.p, cp->rngSeed, 0u, c->spec.p, nLambda, ex->nearFieldSampling, C, c->pSum.p, c->pSum2.p,
                          c->pDrop.p, c->pCross.p, logOut ? c->logBuf.p : nullptr};
+            if (local) {
+                rl.cand = c->candTri.p;
+                rl.candSorted = c->candSorted.p;
+                rl.candRank = c->candRank.p;
+                rl.K = K;
+                rl.Mnear = Mnear;
+                rl.slices = slices;
+                rl.divKm = divKm;
+                rl.divKs = divKs;
+                rl.nearShare = float(double(Mnear) / double(M));
+                rl.farShare = float(double(Mfar) / double(M));
+                if (farPrior) rl.far = farView(c, slices);
+            }
             const RayVariant logVariant{rayKernel<kRayBlock, kRefill, kRayMinBlocks, true>, int(kRayBlock), "log"};
-            const RayVariant& rv = logOut ? logVariant : kRayVariants[variant];
+            const RayVariant localLog{rayKernel<kRayBlock, kRefill, kRayMinBlocks, true, false, kWalkColumns, kWalkBeta, true>,
+                                      int(kRayBlock), "local log"};
+            const RayVariant& rv = local ? (logOut ? localLog : kLocalVariant) : (logOut ? logVariant : kRayVariants[variant]);
             const uint64_t totalItems = uint64_t(nActive) * items;
-            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1,
-                                                               uint64_t(c->variantBlocks[walk][variant])));
             void (*const kern)(RayLaunch) = walk == kWalkTable ? rv.mono : (walk == kWalkBetaNoClad ? rv.noClad : rv.kernel);
+            uint32_t resident = c->variantBlocks[walk][variant];
+            if (local) {  // occupancy of the local kernel itself
+                int perSM = 0, sms = 0;
+                HASE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, rv.block, 0));
+                HASE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+                resident = uint32_t(std::max(1, perSM) * std::max(1, sms));
+            }
+            const uint32_t grid = uint32_t(std::min<uint64_t>(totalItems / (rv.block / 32) + 1, uint64_t(resident)));
             void* rayArgs[] = {&rl};
             HASE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(kern), dim3(grid), dim3(rv.block), rayArgs, 0,
                                        c->stream));
@@ -2758,7 +3276,8 @@ hase_status hase_proposal_features(hase_context* c, uint32_t firstSample, uint32
     if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L)
         return fail(HASE_INVALID_ARGUMENT, "sample range outside the mesh");
     HASE_TRY(setDevice(c));
-    const uint32_t nW = (useReflections ? 5u : 1u) * c->P;
+    if (c->localK) HASE_TRY(prepareLocal(c));
+    const uint32_t nW = rowEntries(c, useReflections ? 5u : 1u);
     const uint32_t nL = monochromatic ? 1u : uint32_t(c->sigmaA.size());
     double A = 0.0, B = 0.0;
     for (uint32_t l = 0; l < nL; ++l) {
@@ -2769,6 +3288,7 @@ hase_status hase_proposal_features(hase_context* c, uint32_t firstSample, uint32
     HASE_TRY(buildProposalView(c, A, B, pv));
     pv.firstSample = firstSample;
     pv.nW = nW;
+    localFields(c, pv);
     const size_t n = size_t(count) * nW * kFeat;
     DevBuf<float> out;
     HASE_CUDA(out.ensure(n));
@@ -2786,7 +3306,8 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     if (!c || !weights || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
     if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
     HASE_TRY(setDevice(c));
-    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    if (c->localK) HASE_TRY(prepareLocal(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = rowEntries(c, slices);
     double meanA = 0, meanB = 0;
     const uint32_t n = uint32_t(c->sigmaA.size());
     for (uint32_t l = 0; l < n; ++l) {
@@ -2802,6 +3323,7 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
     HASE_CUDA(Q.ensure(count));
     ImportanceLaunch il{c->view(), firstSample, slices, nW, float(meanA), float(meanB), lnw.p};
+    localFields(c, il);
     HASE_CUDA(launchImportance(0, il, c->layers, c->T, count, c->stream));
     MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
     mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
@@ -2816,13 +3338,15 @@ hase_status hase_importance_crossings(hase_context* c, uint32_t firstSample, uin
     if (!c || !crossings || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
     if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
     HASE_TRY(setDevice(c));
-    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    if (c->localK) HASE_TRY(prepareLocal(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = rowEntries(c, slices);
     DevBuf<float> lnw;
     DevBuf<unsigned long long> n;
     HASE_CUDA(lnw.ensure(size_t(count) * nW));
     HASE_CUDA(n.ensure(1));
     HASE_CUDA(cudaMemsetAsync(n.p, 0, sizeof(unsigned long long), c->stream));
     ImportanceLaunch il{c->view(), firstSample, slices, nW, 0.0f, 0.0f, lnw.p};
+    localFields(c, il);
     il.crossings = n.p;
     HASE_CUDA(launchImportance(0, il, c->layers, c->T, count, c->stream, false, true));
     unsigned long long h = 0;
@@ -2840,7 +3364,8 @@ hase_status hase_learned_weights(hase_context* c, hase_proposal* net, uint32_t f
     if (net->device != c->device)
         return fail(HASE_INVALID_ARGUMENT, "the proposal network and the context are on different devices");
     HASE_TRY(setDevice(c));
-    const uint32_t slices = useReflections ? 5u : 1u, nW = slices * c->P;
+    if (c->localK) HASE_TRY(prepareLocal(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = rowEntries(c, slices);
     // the spectral average of calcCore: over the solve's wavelengths
     const uint32_t nL = monochromatic ? 1u : uint32_t(c->sigmaA.size());
     double meanA = 0, meanB = 0;
@@ -2852,6 +3377,7 @@ hase_status hase_learned_weights(hase_context* c, hase_proposal* net, uint32_t f
     HASE_TRY(cachedProposalView(c, meanA, meanB, pv));
     pv.firstSample = firstSample;
     pv.nW = nW;
+    localFields(c, pv);
     DevBuf<float> lnw, prior, w;
     DevBuf<uint32_t> q, off;
     DevBuf<unsigned long long> Q;
@@ -3233,6 +3759,7 @@ hase_status batchMedia(const hase_batch* b, const hase_batch_instance* in, uint3
         if (c->device != b->device)
             return fail(HASE_INVALID_ARGUMENT, "instance %u is on device %d, the batch on %d", i, c->device, b->device);
         if (!in[i].result) return fail(HASE_INVALID_ARGUMENT, "instance %u has no result", i);
+        if (c->localK) return fail(HASE_INVALID_ARGUMENT, "instance %u uses the local proposal, which batches do not", i);
         const uint32_t nTot = c->Np * c->L;
         const uint32_t first = in[i].minSample;
         const uint32_t last = in[i].maxSample == UINT32_MAX ? nTot - 1 : in[i].maxSample;

@@ -20,6 +20,8 @@ namespace hase {
 
 constexpr uint32_t kTagRay = 0u;
 constexpr uint32_t kTagMap = 1u;
+constexpr uint32_t kTagFar = 2u;  // far rays of the local proposal: Philox counter word 3
+constexpr uint32_t kWeylStep = 0x9E3779B9u;  // 2^32 / golden ratio: the rays' wavelength sequence step
 constexpr int kMaxSteps = 10000;  // bounded walk (include/kernels/forward/policyRay.hpp:386)
 
 // ---------------------------------------------------------------- Philox ----

@@ -10,7 +10,8 @@
 //                  binary search of the inclusive prefix, a uniform point in
 //                  the tet from four exponentials (paired with the corners in
 //                  ascending point index), an isotropic direction, a
-//                  stratified wavelength bin.  Walk: per cell the four
+//                  wavelength bin from a golden-ratio sequence over the
+//                  batch's rays.  Walk: per cell the four
 //                  barycentric face coordinates lambda_f = a.x + d and their
 //                  rates along the ray; the exit is the decreasing coordinate
 //                  that reaches zero first (cross-multiplied comparisons, one
@@ -310,7 +311,9 @@ __device__ __forceinline__ void initSourceRay(const FwdLaunch& L, uint32_t b, ui
     r.ux = rr * cphi;
     r.uy = rr * sphi;
     r.uz = z;
-    const uint32_t lamIdx = uint32_t((uint64_t(i) * L.nL / nb + L.phase[b]) % L.nL);
+    // wavelength bin: golden-ratio sequence over the batch's ray index, so the
+    // bin is independent of the source cell (the CDF strata run in cell order)
+    const uint32_t lamIdx = __umulhi(i * kWeylStep + L.phase[b], L.nL);
     r.sA = __ldg(L.sigmaA + lamIdx);
     r.sE = __ldg(L.sigmaE + lamIdx);
     r.G = 1.0;
@@ -1390,7 +1393,7 @@ extern "C" hase_status hase_tet_calc_phi_ase(hase_tet_context* c, const hase_for
         for (uint32_t b = 0; b < B; ++b) {
             const Philox4 o = philox4x32_10(b, launch, 0u, kTagFwdBatch, fw->rngSeed, kFwdKeyHi);
             L.shift[b] = double(o.x) / 4294967296.0;
-            L.phase[b] = o.y % nL;
+            L.phase[b] = o.y;  // the batch's 32-bit offset of the wavelength sequence
             L.nb[b] = b < M ? (M - b + B - 1) / B : 0u;
             F.raysInBatch[b] += double(L.nb[b]);
             maxNb = std::max(maxNb, L.nb[b]);

@@ -108,6 +108,22 @@ class DeviceMesh:
         self.handle = handle
         self.numberOfWavelengths = sa.size
         self.sigmaA, self.sigmaE = sa, se
+        self.localTriangles = 0
+
+    def set_local_proposal(self, triangles: int, farFraction: float = 0.0):
+        """Local proposal (hase_context_set_local_proposal): per sample point its
+        ``triangles`` nearest triangles x layers x slices as weighted candidates,
+        a ``farFraction`` of the rays (0: 1/8) drawn from beta V over the rest of
+        the medium; 0 restores the full proposal."""
+        N.check(N.lib().hase_context_set_local_proposal(self.handle, int(triangles), float(farFraction)))
+        self.localTriangles = min(int(triangles), self.mesh.numberOfTriangles)
+
+    def row_entries(self, slices: int) -> int:
+        """Entries of a sample's weight row: every (slice, prism), or the local
+        proposal's (slice, layer, candidate) entries."""
+        if self.localTriangles:
+            return slices * (self.mesh.numberOfLevels - 1) * self.localTriangles
+        return slices * self.mesh.numberOfPrisms
 
     def _hold(self, a):
         a = np.ascontiguousarray(a)
@@ -190,7 +206,7 @@ class DeviceMesh:
         out, ex, cp, r, n = self._descs(minRays, minRays, 0.0, useReflections, monochromatic, nearFieldSampling, 0, 1,
                                         rngSeed, minSample, maxSample, 0, 0, 0, 0, 0)
         slices = 5 if useReflections else 1
-        contrib = np.empty((n, slices * self.mesh.numberOfPrisms), np.float32)
+        contrib = np.empty((n, self.row_entries(slices)), np.float32)
         status = N.check(N.lib().hase_log_contributions(self.handle, C.byref(ex), C.byref(cp),
                                                         N.ptr(contrib, N._f32p), C.byref(r)), allow_warnings=True)
         return self._fill(out, r, status), contrib
@@ -255,7 +271,7 @@ class DeviceMesh:
 
     def proposal_features(self, firstSample, count, useReflections=False, monochromatic=False) -> np.ndarray:
         slices = 5 if useReflections else 1
-        f = np.empty((int(count), slices * self.mesh.numberOfPrisms, N.PROPOSAL_FEATURES), np.float32)
+        f = np.empty((int(count), self.row_entries(slices), N.PROPOSAL_FEATURES), np.float32)
         N.check(N.lib().hase_proposal_features(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
                                                1 if monochromatic else 0, N.ptr(f, N._f32p)))
         return f
@@ -286,7 +302,7 @@ class DeviceMesh:
 
     def importance_weights(self, firstSample, count, useReflections=False) -> np.ndarray:
         slices = 5 if useReflections else 1
-        w = np.empty((count, slices * self.mesh.numberOfPrisms), np.float32)
+        w = np.empty((count, self.row_entries(slices)), np.float32)
         N.check(N.lib().hase_importance_weights(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
                                                 N.ptr(w, N._f32p)))
         return w
@@ -302,7 +318,7 @@ class DeviceMesh:
                         mixture=0.0) -> np.ndarray:
         """The learned proposal's normalised first-pass weights (hase_learned_weights)."""
         slices = 5 if useReflections else 1
-        w = np.empty((count, slices * self.mesh.numberOfPrisms), np.float32)
+        w = np.empty((count, self.row_entries(slices)), np.float32)
         N.check(N.lib().hase_learned_weights(self.handle, net.handle, int(firstSample), int(count),
                                              1 if useReflections else 0, 1 if monochromatic else 0, float(mixture),
                                              N.ptr(w, N._f32p)))

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define HASE_B200_ABI_VERSION 1
+#define HASE_B200_ABI_VERSION 2
 
 typedef enum {
     HASE_OK = 0,
@@ -140,6 +140,21 @@ hase_status hase_context_update_beta(hase_context* ctx, const double* betaVolume
 hase_status hase_calc_phi_ase(hase_context* ctx, const hase_experiment_desc* experiment,
                               const hase_compute_desc* compute, hase_result* result);
 hase_status hase_context_destroy(hase_context* ctx);
+
+/* Local proposal for media too large for a weight per (sample, slice,
+ * prism) pair (no reference counterpart; the reference weights every prism).
+ * With triangles = K > 0, every backward solve of the context (plain or
+ * learned), hase_importance_weights, hase_learned_weights,
+ * hase_log_contributions and hase_proposal_features use per sample point its
+ * K nearest triangles (by centroid distance) x layers x slices as the
+ * candidate entries of the weight rows (entry j (layers K) + l K + k), and
+ * draw a fraction farFraction (0: 1/8) of each pass's rays from beta V over
+ * all prisms outside the candidates (the reflection slice uniformly), each
+ * ray weighted by the inverse probability of its part: an unbiased estimate
+ * with O(K) weights per sample instead of O(prisms).  triangles = 0 restores
+ * the full proposal.  Batched media (hase_calc_phi_ase_batch) reject a
+ * context in local mode. */
+hase_status hase_context_set_local_proposal(hase_context* ctx, uint32_t triangles, float farFraction);
 
 /* ---- kernel-level entry points (the four hot-path kernels, one at a time) ----
  * Used by the parity tests and the benchmark; no reference counterpart beyond

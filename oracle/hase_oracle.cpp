@@ -439,8 +439,9 @@ int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum, con
                         const uint32_t b = uint32_t(std::upper_bound(off.begin(), off.end(), r) - off.begin()) - 1u;
                         const uint32_t j = b / md.P, p = b % md.P;
                         const uint32_t t = p % md.T, l = p / md.T;
+                        // golden-ratio sequence over r, offset by the 32-bit phase po[1]
                         const uint32_t lambda =
-                            uint32_t((uint64_t(r) * nLambda / M + po[1] % nLambda) % nLambda);
+                            uint32_t((uint64_t(uint32_t(r * 0x9E3779B9u + po[1])) * nLambda) >> 32);
                         uint32_t rc4[4] = {r, s, pass, kTagRay}, ro[4];
                         philox(rc4, key, ro);
                         const uint32_t* v = mesh->triangles + 3 * t;

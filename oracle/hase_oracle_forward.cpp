@@ -7,8 +7,10 @@
 //                 include/kernels/forward/volumeSampling.hpp:19-161
 //                 (stratified beta*V CDF per statistical batch, uniform point
 //                 in the tet from four exponentials paired with the corners
-//                 in ascending point index, isotropic direction,
-//                 stratified wavelength bin)
+//                 in ascending point index, isotropic direction; the
+//                 wavelength bin from a golden-ratio sequence over the
+//                 batch's rays, this build's choice: the reference draws
+//                 it per ray)
 //   walk + tally  include/kernels/forward/rayWalk.hpp:106-208,
 //                 include/kernels/forward/accumulation.hpp:300-352
 //                 (barycentric face planes; per crossed cell the tally
@@ -611,7 +613,7 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
             uint32_t o[4];
             philoxFwd(b, launch, 0u, kTagFwdBatch, ex->seed, o);
             shift[b] = double(o[0]) / 4294967296.0;
-            phase[b] = o[1] % nL;
+            phase[b] = o[1];
             nb[b] = b < M ? (M - b + B - 1) / B : 0u;
             raysInBatch[b] += nb[b];
         }
@@ -646,7 +648,7 @@ int oracle_forward_phi_ase(const oracle_tet_mesh* m, const oracle_spectrum* sp, 
                     const double z = 2.0 * unit(o2[0]) - 1.0, phi = 2.0 * kPi * unit(o2[1]);
                     const double rr = std::sqrt(std::max(0.0, 1.0 - z * z));
                     const double u[3] = {rr * std::cos(phi), rr * std::sin(phi), z};
-                    const uint32_t lam = uint32_t((uint64_t(i) * nL / nb[b] + phase[b]) % nL);
+                    const uint32_t lam = uint32_t((uint64_t(uint32_t(i * 0x9E3779B9u + phase[b])) * nL) >> 32);
                     uint32_t ec = 0;
                     int ef = -1;
                     double eg = 0.0;

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol(native):
     lib = native.lib()
     for name in declared:
         assert hasattr(lib, name), name
-    assert lib.hase_abi_version() == 1
+    assert lib.hase_abi_version() == 2
     assert lib.hase_status_string(7) == b"no CUDA device"
 
 
