@@ -113,8 +113,9 @@ class DeviceMesh:
     def set_local_proposal(self, triangles: int, farFraction: float = 0.0):
         """Local proposal (hase_context_set_local_proposal): per sample point its
         ``triangles`` nearest triangles x layers x slices as weighted candidates,
-        a ``farFraction`` of the rays (0: 1/8) drawn from beta V over the rest of
-        the medium; 0 restores the full proposal."""
+        a ``farFraction`` of the rays (0: 0.9) drawn from a beta V gain / d^2
+        prior over the whole medium, every ray weighted by the mixture's
+        probability; 0 restores the full proposal."""
         N.check(N.lib().hase_context_set_local_proposal(self.handle, int(triangles), float(farFraction)))
         self.localTriangles = min(int(triangles), self.mesh.numberOfTriangles)
 

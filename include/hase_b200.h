@@ -147,13 +147,17 @@ hase_status hase_context_destroy(hase_context* ctx);
  * learned), hase_importance_weights, hase_learned_weights,
  * hase_log_contributions and hase_proposal_features use per sample point its
  * K nearest triangles (by centroid distance) x layers x slices as the
- * candidate entries of the weight rows (entry j (layers K) + l K + k), and
- * draw a fraction farFraction (0: 1/8) of each pass's rays from beta V over
- * all prisms outside the candidates (the reflection slice uniformly), each
- * ray weighted by the inverse probability of its part: an unbiased estimate
- * with O(K) weights per sample instead of O(prisms).  triangles = 0 restores
- * the full proposal.  Batched media (hase_calc_phi_ase_batch) reject a
- * context in local mode. */
+ * candidate entries of the weight rows (entry j (layers K) + l K + k).  A
+ * fraction farFraction (0: 0.9) of each pass's rays is drawn instead from a
+ * prior over every (slice, prism): beta V times a two-point gain estimate
+ * over the squared distance to the slice's image of the sample point, on a
+ * grid of about 8 triangles per cell.  Each ray is weighted by the mixture
+ * of both sources' probabilities, so the estimate is unbiased with O(K)
+ * weights per sample instead of O(prisms).  Logged contributions
+ * (hase_log_contributions) are those of every ray in a candidate prism.
+ * triangles = 0 restores the full proposal; triangles >= the mesh's
+ * triangles uses every triangle as a candidate and no far rays.  Batched
+ * media (hase_calc_phi_ase_batch) reject a context in local mode. */
 hase_status hase_context_set_local_proposal(hase_context* ctx, uint32_t triangles, float farFraction);
 
 /* ---- kernel-level entry points (the four hot-path kernels, one at a time) ----

@@ -445,3 +445,20 @@ def test_monochromatic_walk_matches_the_general_walk(case):
     np.testing.assert_array_equal(a.relativeStandardError, b.relativeStandardError)
     np.testing.assert_array_equal(a.totalRays, b.totalRays)
     assert a.crossings == b.crossings
+
+
+def test_gpu_polychromatic_seeds_agree_within_reported_error():
+    """Two seeds of a polychromatic solve with reflections (disc_poly, 16
+    wavelengths) agree within their reported errors: the wavelength bin of a
+    ray is independent of its prism, so the reported relative error holds."""
+    from haseongpu_b200.configs import disc_poly
+
+    w = disc_poly()
+    sa, se = w.spectra.resampled()
+    kw = dict(minRays=400_000, useReflections=True, minSample=3000, maxSample=3127)
+    with _ctx(w.mesh, sa, se) as ctx:
+        a = ctx.calc_phi_ase(rngSeed=3, **kw)
+        b = ctx.calc_phi_ase(rngSeed=5, **kw)
+    sig = np.hypot(a.relativeStandardError * a.phiAse, b.relativeStandardError * b.phiAse)
+    z = (a.phiAse.astype(np.float64) - b.phiAse) / sig
+    assert z.std() < 1.3 and np.abs(z).max() < 4.5, (z.std(), np.abs(z).max())
