@@ -81,6 +81,10 @@ def parse():
                          "disc_small (importance-sampled solve)")
     ap.add_argument("--no-nested", action="store_true", help="learned workload only: skip the disc_poly and forward lines")
     ap.add_argument("--samples", type=int, default=1024, help="sample points per step and rank")
+    ap.add_argument("--pulse-backward-rays", type=int, default=2000,
+                    help="pulse workload: backward rays per sample point and time step (local proposal)")
+    ap.add_argument("--pulse-local-triangles", type=int, default=16,
+                    help="pulse workload: candidate triangles per sample point of the local proposal")
     ap.add_argument("--pulse-rays", type=int, default=2_000_000,
                     help="pulse workload: forward source rays per time step")
     ap.add_argument("--media-samples", type=int, default=64,
@@ -851,6 +855,87 @@ def measure_pulse(args, local):
     }
 
 
+def _rse_summary(res, rays):
+    import numpy as np
+
+    g = res.phiAse > 0
+    r = res.relativeStandardError[g]
+    return {"rays_per_sample": rays, "median_sample_rse": float(np.median(r)), "p90_sample_rse": float(np.percentile(r, 90)),
+            "max_sample_rse": float(r.max()), "per_ray_variance_median": float(np.median(rays * r ** 2)),
+            "ms": res.totalMilliseconds}
+
+
+def measure_pulse_backward(args, local):
+    """Config 5 with the backward method: every time step solves all 287,310
+    sample points (9,577 points x 30 levels) with the local proposal (per
+    point its ``--pulse-local-triangles`` nearest triangles x 29 layers x 5
+    slices weighted by the importance walks, 90 % of the rays from the far
+    beta V gain / d^2 prior; unbiased mixture weights), ``--pulse-backward-rays``
+    rays per sample, 8 wavelengths, reflections.  Two series of 50 steps:
+    the plain local proposal (device time of hase_simulate) and the learned
+    proposal warm-started from step to step (fine-tuned before every step
+    on the contributions the importance-weighted method logs for a block of
+    32 sample points, plain importance weights as the fallback above the
+    per-ray variance the logged block reached).  Then at the plain series'
+    final beta: the per-sample error the budget reaches, and an adaptive
+    solve to relative error 1e-3 of 2,048 sample points (a block of the
+    middle level) whose device time, scaled to all sample points, is the
+    cost of one time step at the stated accuracy."""
+    import time as clock
+
+    import numpy as np
+
+    from haseongpu_b200 import DeviceMesh
+    from haseongpu_b200.configs import pulse
+    from haseongpu_b200.learned import warm_started_series
+    from haseongpu_b200.proposal import ProposalNet
+
+    w = pulse()
+    sa, se = w.spectra.resampled(False)
+    rays, K = int(args.pulse_backward_rays), int(args.pulse_local_triangles)
+    S = w.mesh.numberOfSamples
+    out = {"config": {"local_triangles": K, "far_fraction": 0.9, "rays_per_sample_and_step": rays, "samples": S,
+                      "steps": w.time["steps"], "wavelengths": int(len(sa)), "phi_method": "backward, local proposal"}}
+    with DeviceMesh(w.mesh, sa, se, device=local) as ctx:
+        ctx.set_local_proposal(K, 0.9)
+        ctx.calc_phi_ase(minRays=1000, useReflections=True, minSample=0, maxSample=63)  # candidate tables
+        t0 = clock.perf_counter()
+        ser = ctx.simulate(pump=w.pump, time=w.time, minRays=rays, useReflections=True, rngSeed=11)
+        wall = clock.perf_counter() - t0
+        fin = ctx.calc_phi_ase(minRays=rays, useReflections=True, rngSeed=13)
+        first = (w.mesh.numberOfLevels // 2) * w.mesh.numberOfPoints
+        thr = ctx.calc_phi_ase(minRays=16000, maxRays=4_000_000, mseThreshold=1e-3, adaptiveSteps=6,
+                               useReflections=True, rngSeed=17, minSample=first, maxSample=first + 2047)
+        out["plain_local"] = {
+            "ms_per_series": ser["totalMilliseconds"], "wall_ms_per_series": wall * 1e3,
+            "value": w.time["steps"] / (ser["totalMilliseconds"] * 1e-3), "unit": "time steps/s",
+            "ase_ms": ser["aseMilliseconds"], "rays_traced": ser["raysTraced"],
+            "mean_beta_end": float(ser["meanBeta"][-1]), "mean_phi_end": float(ser["meanPhi"][-1]),
+            "final_beta_solve": _rse_summary(fin, rays)}
+        out["to_rse_1e-3"] = {
+            "samples": 2048, "ms": thr.totalMilliseconds, "unconverged": thr.unconvergedSamples,
+            "mean_rays_per_sample": float(thr.totalRays.mean()),
+            "median_sample_rse": float(np.median(thr.relativeStandardError)),
+            "ms_per_time_step_all_samples": thr.totalMilliseconds * S / 2048.0,
+            "note": "adaptive 16,000 -> 4e6 rays (6 increases) at the series' final beta; scaled by samples"}
+    with DeviceMesh(w.mesh, sa, se, device=local) as ctx, ProposalNet(device=local, seed=3) as net:
+        ctx.set_local_proposal(K, 0.9)
+        ctx.calc_phi_ase(minRays=1000, useReflections=True, minSample=0, maxSample=63)
+        t0 = clock.perf_counter()
+        ws = warm_started_series(ctx, net, w.pump, w.time, rays=rays, rngSeed=11, fallback="logged")
+        wall = clock.perf_counter() - t0
+        fin = ctx.calc_phi_ase_learned(net, minRays=rays, useReflections=True, rngSeed=13)
+        out["learned_warm_started"] = {
+            "ms_per_series": ws["totalMilliseconds"], "wall_ms_per_series": wall * 1e3,
+            "value": w.time["steps"] / (ws["totalMilliseconds"] * 1e-3), "unit": "time steps/s",
+            "fine_tune_s": ws["trainSeconds"], "fallback_samples": ws["fallbackSamples"],
+            "mean_beta_end": ws["meanBeta"][-1], "mean_phi_end": ws["meanPhi"][-1],
+            "loss_last": ws["loss"][-1] if ws["loss"] else None,
+            "final_beta_solve": _rse_summary(fin, rays),
+            "note": "device time of the 50 hase_simulate steps; fine-tuning and logging are host-timed (fine_tune_s)"}
+    return out
+
+
 def run_pulse(args):
     """Config 5 on its own line; with N ranks every rank runs its own series
     (replicas), timed as the maximum over ranks."""
@@ -859,6 +944,7 @@ def run_pulse(args):
 
     rank, world, local = setup_ranks()
     m = measure_pulse(args, local)
+    m["backward"] = measure_pulse_backward(args, local)
     ms = torch.tensor([m["ms_per_series"]], dtype=torch.float64, device=torch.device("cuda", local))
     if world > 1:
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
@@ -989,6 +1075,11 @@ def run_learned(args):
         disc_poly = measure_importance(nargs, local, rank, world, nested=True)
         media = measure_media(nargs, local, steps=2, warmup=3)
         pulse_line = measure_pulse(nargs, local)
+        # the backward series at a quarter of the pulse workload's budget
+        # (--workload pulse runs --pulse-backward-rays)
+        bargs = _ap.Namespace(**vars(nargs))
+        bargs.pulse_backward_rays = max(1, args.pulse_backward_rays // 4)
+        pulse_line["backward"] = measure_pulse_backward(bargs, local)
         fwd = measure_forward(nargs, local, cpu_seconds=min(args.cpu_seconds, 6.0))
     if rank == 0:
         peaks, peak_kind = measured_peaks()

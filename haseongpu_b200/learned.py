@@ -131,3 +131,77 @@ def per_ray_variance(result) -> np.ndarray:
     contribution relative to the mean squared (ray budget for a target error
     eps is this / eps^2)."""
     return result.totalRays.astype(np.float64) * result.relativeStandardError ** 2
+
+
+def warm_started_series(ctx, net, pump, time, *, rays, useReflections=True, monochromatic=False, log_samples=32,
+                        log_rays=20_000, train_steps=20, groups_per_step=8, learning_rate=1e-3, fallback="logged",
+                        rngSeed=5489):
+    """The time-stepped rate equations with the learned proposal warm-started
+    from step to step (the time loop of include/core/timeSteppedSimulation.hpp:
+    132-617, one step per hase_simulate call): before the phi-ASE solve of
+    step k > 0 the network ``net`` is fine-tuned on the current beta --
+    ``train_steps`` Adam steps on the device over the contributions logged by
+    the importance-weighted method for a seeded block of ``log_samples``
+    consecutive sample points (``log_rays`` rays each) -- and the step then
+    solves every sample point with ``rays`` rays per sample and the network.
+    ``fallback``: the per-ray variance above which the plain importance
+    weights take over a sample after the first pass -- "logged" (the largest
+    the importance-weighted log solve of the step reached on its block: the
+    plain method as the judge), a number, or 0 (never).  The pump runs
+    for ``time["pumpSteps"]`` steps and phi-ASE for ``time["aseSteps"]``.
+    With the context's local proposal set, the network weights the candidate
+    entries and the far prior keeps its share.  Returns the per-step series
+    and the device and host times."""
+    import time as clock
+
+    steps = int(time["steps"])
+    pump_steps = int(time.get("pumpSteps", steps))
+    ase_steps = int(time.get("aseSteps", steps))
+    S = ctx.mesh.numberOfSamples
+    n = min(int(log_samples), S)
+    rng = np.random.default_rng(rngSeed)
+    out = {"meanBeta": [], "meanPhi": [], "pumpAbsorbed": [], "loss": [], "aseMilliseconds": 0.0,
+           "pumpMilliseconds": 0.0, "totalMilliseconds": 0.0, "raysTraced": 0, "fallbackSamples": 0,
+           "trainSeconds": 0.0, "stepSeconds": 0.0}
+    fallbackVariance = 0.0 if fallback == "logged" else float(fallback)
+    for k in range(steps):
+        t0 = clock.perf_counter()
+        if k > 0 and ase_steps > k:
+            first = int(rng.integers(0, max(1, S - n)))
+            res, con = ctx.log_contributions(minRays=log_rays, monochromatic=monochromatic,
+                                             useReflections=useReflections, rngSeed=rngSeed + 7919 * k,
+                                             minSample=first, maxSample=first + n - 1)
+            if fallback == "logged":
+                v = per_ray_variance(res)
+                fallbackVariance = float(v[np.isfinite(v)].max()) if np.isfinite(v).any() else 0.0
+            f = ctx.proposal_features(first, n, useReflections=useReflections, monochromatic=monochromatic)
+            feats, targs, offs = [], [], [0]
+            for i in range(n):
+                keep = (f[i, :, 7] > 0) & (con[i] > 0)
+                if keep.sum() < 2:
+                    continue
+                feats.append(f[i][keep])
+                targs.append(con[i][keep])
+                offs.append(offs[-1] + int(keep.sum()))
+            if len(offs) > 1:
+                hist = net.train(np.asarray(offs, np.uint32), np.concatenate(feats),
+                                 np.concatenate(targs).astype(np.float32), steps=train_steps,
+                                 groups_per_step=min(groups_per_step, len(offs) - 1), learning_rate=learning_rate)
+                out["loss"].append(float(hist[-1]))
+        t1 = clock.perf_counter()
+        step = dict(time, steps=1, pumpSteps=1 if k < pump_steps else 0, aseSteps=1 if k < ase_steps else 0)
+        r = ctx.simulate(pump=pump, time=step, net=net, fallbackVariance=fallbackVariance, minRays=rays,
+                         useReflections=useReflections, monochromatic=monochromatic, rngSeed=rngSeed + k)
+        t2 = clock.perf_counter()
+        if k == 0:
+            out["meanBeta"].append(float(r["meanBeta"][0]))
+        out["meanBeta"].append(float(r["meanBeta"][-1]))
+        out["meanPhi"].append(float(r["meanPhi"][-1]))
+        out["pumpAbsorbed"].append(float(r["pumpAbsorbed"][-1]))
+        for key in ("aseMilliseconds", "pumpMilliseconds", "totalMilliseconds"):
+            out[key] += float(r[key])
+        out["raysTraced"] += int(r["raysTraced"])
+        out["fallbackSamples"] += int(r["fallbackSamples"])
+        out["trainSeconds"] += t1 - t0
+        out["stepSeconds"] += t2 - t1
+    return out
