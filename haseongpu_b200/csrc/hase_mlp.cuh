@@ -74,12 +74,18 @@ struct SmemMap {
 constexpr uint32_t kSmemBytes = SmemMap::bytes + 1024;  // + alignment slack
 
 // Training: also the backward weight images (W2, W3 as [in][out]: the B
-// operands of dz2 W2^T and dz3 W3^T), dz as the bf16 A operand and in f32 for
-// the weight-gradient reductions, and 256 TMEM columns: the three layer
-// accumulators side by side (0, 64, 128) and the backward products (192).
+// operands of dz2 W2^T and dz3 W3^T), dz as the bf16 operand of the backward
+// and weight-gradient products and in f32 for the bias sums, and 512 TMEM
+// columns: the three layer accumulators side by side (0, 64, 128), the
+// backward products (192), and the weight gradients accumulated over all
+// tiles of the CTA (M = 64 accumulators: dW3 at 256, dW2 at 320, dW1^T at
+// 384).
 struct TrainSmem {
     static constexpr uint32_t wBytes = kWBlobBytes;
-    static constexpr uint32_t tmemCols = 256;
+    static constexpr uint32_t tmemCols = 512;
+    static constexpr uint32_t colGradW3 = 256;
+    static constexpr uint32_t colGradW2 = 320;
+    static constexpr uint32_t colGradW1 = 384;
     static constexpr uint32_t w1 = 0;
     static constexpr uint32_t w2 = w1 + kW1Bytes;
     static constexpr uint32_t w3 = w2 + kW2Bytes;
@@ -116,12 +122,18 @@ __device__ __forceinline__ uint64_t smemDesc(uint32_t addr, uint32_t lbo, uint32
 // Instruction descriptor of kind::f16: D f32 (bits 4-5 = 1), A and B bf16
 // (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 constexpr uint32_t kIdescM128N64 = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// The weight-gradient products: A and B MN-major (bits 15 and 16), M = 64.
+constexpr uint32_t kIdescGradN64 =
+    (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
+constexpr uint32_t kIdescGradN16 =
+    (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((16u >> 3) << 17) | ((64u >> 4) << 24);
 
-__device__ __forceinline__ void mmaBf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mmaBf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                        uint32_t idesc = kIdescM128N64) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-        "l"(a), "l"(b), "r"(kIdescM128N64), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void mmaCommit(uint32_t bar) {
@@ -234,6 +246,25 @@ __device__ __forceinline__ void issueLayer(Tile& T, uint32_t aOff, uint32_t wOff
             mmaBf16(T.tmem + col, a, b, kk > 0 ? 1u : 0u);
         }
         mmaCommit(T.sbase + barOff);
+    }
+}
+
+// Issues (from thread 0, without a commit) the weight-gradient product
+// D[m][n] (+)= sum_r A[r][m] B[r][n] over the tile's 128 rows into TMEM
+// column `col` (an M = 64 accumulator: row m in TMEM lane 32 (m / 16) +
+// m % 16, the first 16 lanes of warp m / 16's lane quarter).  A ([128 x 64]) and B ([128 x bWidth])
+// are row-major bf16 images in the canonical layout of the forward operands
+// (8-row x 16-byte core matrices, 8-row groups width x 16 bytes apart), which
+// are MN-major operands of the transposed product: SBO = 128 bytes (next 8
+// columns), LBO = width x 16 bytes (next 8 rows), 16 rows per MMA.
+// accumulate = false starts the accumulator with this tile.
+__device__ __forceinline__ void issueGradient(const Tile& T, uint32_t aOff, uint32_t bOff, uint32_t bWidth,
+                                              uint32_t col, uint32_t idesc, bool accumulate) {
+    const uint32_t aRows = kHid * 16u, bRows = bWidth * 16u;
+    for (uint32_t kk = 0; kk < uint32_t(kTile) / 16u; ++kk) {
+        const uint64_t a = smemDesc(T.sbase + aOff + kk * 2u * aRows, aRows, 128u);
+        const uint64_t b = smemDesc(T.sbase + bOff + kk * 2u * bRows, bRows, 128u);
+        mmaBf16(T.tmem + col, a, b, (accumulate || kk > 0) ? 1u : 0u, idesc);
     }
 }
 

@@ -57,26 +57,25 @@ __device__ __forceinline__ float dsilu(float z) {
 }
 
 // g[j] += sum over the tile's rows r of h[r][i0 + j] * dz[r][o] (j < 32) and
-// gb += sum_r dz[r][o]: h bf16 in the canonical layout (K = 64) at hOff, dz
-// f32 [128][64] at dzOff.  Every lane of a warp reads the same h (broadcast).
-__device__ __forceinline__ void accumulateGrad64(const Tile& T, uint32_t hOff, uint32_t dzOff, uint32_t o,
-                                                 uint32_t ih, float (&g)[32], float& gb) {
+// sum over the tile's rows of dz[r][o] (f32 [128][64] at dzOff): a bias gradient.
+__device__ __forceinline__ float columnSum(const Tile& T, uint32_t dzOff, uint32_t o) {
     const float* dz = reinterpret_cast<const float*>(T.base + dzOff);
-    for (uint32_t r = 0; r < uint32_t(kTile); ++r) {
-        const float d = dz[r * kHid + o];
-        const uint8_t* hp = T.base + hOff + (r >> 3) * (kHid * 16u) + (r & 7u) * 16u;
-#pragma unroll
-        for (uint32_t cc = 0; cc < 4; ++cc) {
-            const uint4 v = *reinterpret_cast<const uint4*>(hp + (4u * ih + cc) * 128u);
-            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                g[8 * cc + 2 * e] = fmaf(__uint_as_float(w[e] << 16), d, g[8 * cc + 2 * e]);
-                g[8 * cc + 2 * e + 1] = fmaf(__uint_as_float(w[e] & 0xFFFF0000u), d, g[8 * cc + 2 * e + 1]);
-            }
-        }
-        gb += d;
-    }
+    float s = 0.0f;
+    for (uint32_t r = 0; r < uint32_t(kTile); ++r) s += dz[r * kHid + o];
+    return s;
+}
+
+// Adds this thread's row of an M = 64 weight-gradient accumulator (TMEM
+// column `col`, `cols` columns; lanes 0-15 of each warp hold rows 16 warp +
+// lane) to grad[base + row * rowStride + n * colStride] for n < keep.
+template <int COLS>
+__device__ __forceinline__ void flushGradient(const Tile& T, uint32_t col, float* grad, uint32_t rowStride,
+                                              uint32_t colStride, int keep) {
+    float acc[COLS];
+    loadCols<COLS>(T, col, acc);
+    const uint32_t lane = threadIdx.x & 31u, row = 16u * (threadIdx.x >> 5) + lane;
+    if (lane < 16u)
+        for (int n = 0; n < keep; ++n) atomicAdd(grad + row * rowStride + uint32_t(n) * colStride, acc[n]);
 }
 
 struct TrainLaunch {
@@ -90,10 +89,12 @@ struct TrainLaunch {
 };
 
 // Recomputes the forward pass of each tile (layer accumulators kept in TMEM
-// columns 0 / 64 / 128) and back-propagates dL/dlogit: the products
-// dz3 W3^T and dz2 W2^T on the tensor cores (TMEM column 192), the weight
-// and bias gradients as FP32 reductions over the tile's rows on the CUDA
-// cores, per-thread across tiles, added to `grad` once per CTA.
+// columns 0 / 64 / 128) and back-propagates dL/dlogit on the tensor cores:
+// per layer one commit covers the backward product (dz3 W3^T or dz2 W2^T,
+// TMEM column 192) and the weight-gradient product (h2^T dz3, h1^T dz2,
+// dz1^T x: the activation and dz images read as MN-major operands) that
+// accumulates in TMEM over all tiles of the CTA; the bias sums run on the
+// CUDA cores meanwhile.  The CTA adds its gradients to `grad` once.
 __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch P) {
     extern __shared__ uint8_t dynSmem[];
     Tile T;
@@ -103,10 +104,8 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
     const float *b1 = vec, *b2 = vec + kHid, *b3 = vec + 2 * kHid, *w4 = vec + 3 * kHid;
     float* dzf = reinterpret_cast<float*>(T.base + TrainSmem::dzf);
     float* dls = reinterpret_cast<float*>(T.base + TrainSmem::dls);
-    float gW3[32], gW2[32], gW1[6];
-    for (int j = 0; j < 32; ++j) gW3[j] = gW2[j] = 0.0f;
-    for (int j = 0; j < 6; ++j) gW1[j] = 0.0f;
     float gb1 = 0.0f, gb2 = 0.0f, gb3 = 0.0f, gw4 = 0.0f, gb4 = 0.0f;
+    bool accumulate = false;  // the gradient accumulators hold a tile
     const uint32_t tiles = (P.rows + kTile - 1) / kTile;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t row = tile * kTile + t;
@@ -128,11 +127,7 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             dls[t] = dl;
         }
         __syncthreads();
-        if (ih == 0) {
-            float sum = 0.0f;
-            for (uint32_t r = 0; r < uint32_t(kTile); ++r) sum += dzf[r * kHid + o];
-            gw4 += sum;
-        }
+        if (ih == 0) gw4 += columnSum(T, TrainSmem::dzf, o);
         if (t == 0)
             for (uint32_t r = 0; r < uint32_t(kTile); ++r) gb4 += dls[r];
         __syncthreads();
@@ -161,13 +156,16 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
-        // dh2 = dz3 W3^T on the tensor cores while the CUDA cores reduce g_W3
-        issueLayer(T, TrainSmem::dzb, TrainSmem::w3b, kHid, 192, TrainSmem::bar);
-        {
-            float gb = 0.0f;
-            accumulateGrad64(T, TrainSmem::a2, TrainSmem::dzf, o, ih, gW3, gb);
-            if (ih == 0) gb3 += gb;
+        // dh2 = dz3 W3^T and g_W3 += h2^T dz3 on the tensor cores, g_b3 on the CUDA cores
+        if (t == 0) {
+            fenceAfterSync();
+            for (uint32_t kk = 0; kk < uint32_t(kHid) / 16u; ++kk)
+                mmaBf16(T.tmem + 192, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
+                        smemDesc(T.sbase + TrainSmem::w3b + kk * 256u, 128u, kHid * 16u), kk > 0 ? 1u : 0u);
+            issueGradient(T, TrainSmem::a2, TrainSmem::dzb, kHid, TrainSmem::colGradW3, kIdescGradN64, accumulate);
+            mmaCommit(T.sbase + TrainSmem::bar);
         }
+        if (ih == 0) gb3 += columnSum(T, TrainSmem::dzf, o);
         waitLayer(T, TrainSmem::bar);
         float dh[kHid];
         loadRow(T, 192, dh);
@@ -177,7 +175,7 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b2[n]);
         }
         fenceBeforeSync();
-        __syncthreads();  // g_W3 reads of dzf done; TMEM column 192 read
+        __syncthreads();  // bias reads of dzf done; TMEM column 192 read
         {
             uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
 #pragma unroll
@@ -191,15 +189,19 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             }
             for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
         }
+        fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
-        // dh1 = dz2 W2^T while the CUDA cores reduce g_W2
-        issueLayer(T, TrainSmem::dzb, TrainSmem::w2b, kHid, 192, TrainSmem::bar);
-        {
-            float gb = 0.0f;
-            accumulateGrad64(T, TrainSmem::a1, TrainSmem::dzf, o, ih, gW2, gb);
-            if (ih == 0) gb2 += gb;
+        // dh1 = dz2 W2^T and g_W2 += h1^T dz2, g_b2 meanwhile
+        if (t == 0) {
+            fenceAfterSync();
+            for (uint32_t kk = 0; kk < uint32_t(kHid) / 16u; ++kk)
+                mmaBf16(T.tmem + 192, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
+                        smemDesc(T.sbase + TrainSmem::w2b + kk * 256u, 128u, kHid * 16u), kk > 0 ? 1u : 0u);
+            issueGradient(T, TrainSmem::a1, TrainSmem::dzb, kHid, TrainSmem::colGradW2, kIdescGradN64, accumulate);
+            mmaCommit(T.sbase + TrainSmem::bar);
         }
+        if (ih == 0) gb2 += columnSum(T, TrainSmem::dzf, o);
         waitLayer(T, TrainSmem::bar);
         loadRow(T, 192, dh);
         {
@@ -208,32 +210,42 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b1[n]);
         }
         fenceBeforeSync();
-        __syncthreads();
-        for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
-        __syncthreads();
-        // g_W1 from the bf16 features in A0 (inputs 6 ih .. 6 ih + 5), g_b1
-        for (uint32_t r = 0; r < uint32_t(kTile); ++r) {
-            const float d = dzf[r * kHid + o];
-            const uint8_t* xp = T.base + TrainSmem::a0 + (r >> 3) * (kIn * 16u) + (r & 7u) * 16u;
-            const uint4 v0 = *reinterpret_cast<const uint4*>(xp);
-            const uint4 v1 = *reinterpret_cast<const uint4*>(xp + 128u);
-            const uint32_t w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+        __syncthreads();  // bias reads of dzf done
+        {
+            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
 #pragma unroll
-            for (int j = 0; j < 6; ++j) {
-                const int i = int(6 * ih) + j;
-                const uint32_t bits = (i & 1) ? (w[i >> 1] & 0xFFFF0000u) : (w[i >> 1] << 16);
-                gW1[j] = fmaf(__uint_as_float(bits), d, gW1[j]);
+            for (int c = 0; c < kHid / 8; ++c) {
+                uint4 v;
+                v.x = packBf16(dh[8 * c + 0], dh[8 * c + 1]);
+                v.y = packBf16(dh[8 * c + 2], dh[8 * c + 3]);
+                v.z = packBf16(dh[8 * c + 4], dh[8 * c + 5]);
+                v.w = packBf16(dh[8 * c + 6], dh[8 * c + 7]);
+                *reinterpret_cast<uint4*>(out + c * 128u) = v;
             }
-            if (ih == 0) gb1 += d;
+            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
         }
+        fenceBeforeSync();
+        fenceProxyAsync();
+        __syncthreads();
+        // g_W1^T += dz1^T x (the bf16 features in A0, 16 columns), g_b1 meanwhile;
+        // the wait keeps A0 and the dz image until the products have read them
+        if (t == 0) {
+            fenceAfterSync();
+            issueGradient(T, TrainSmem::dzb, TrainSmem::a0, kIn, TrainSmem::colGradW1, kIdescGradN16, accumulate);
+            mmaCommit(T.sbase + TrainSmem::bar);
+        }
+        if (ih == 0) gb1 += columnSum(T, TrainSmem::dzf, o);
+        waitLayer(T, TrainSmem::bar);
+        accumulate = true;
         fenceBeforeSync();
         if (!__syncthreads_and(T.ok)) break;
     }
-    for (int j = 0; j < 32; ++j) {
-        atomicAdd(P.grad + kOffW3 + (32 * ih + j) * kHid + o, gW3[j]);
-        atomicAdd(P.grad + kOffW2 + (32 * ih + j) * kHid + o, gW2[j]);
+    if (accumulate) {
+        // g_W3 and g_W2 as [in][out] rows (row = input); g_W1^T as [out][in] rows
+        flushGradient<kHid>(T, TrainSmem::colGradW3, P.grad + kOffW3, kHid, 1u, kHid);
+        flushGradient<kHid>(T, TrainSmem::colGradW2, P.grad + kOffW2, kHid, 1u, kHid);
+        flushGradient<kIn>(T, TrainSmem::colGradW1, P.grad + kOffW1, 1u, kHid, kFeat);
     }
-    for (int j = 0; j < 6; ++j) atomicAdd(P.grad + kOffW1 + (6 * ih + j) * kHid + o, gW1[j]);
     if (ih == 0) {
         atomicAdd(P.grad + kOffB1 + o, gb1);
         atomicAdd(P.grad + kOffB2 + o, gb2);

@@ -124,14 +124,16 @@ def loss_and_grad(params, features, offsets, targets, group_weights=None):
     def r(a):
         return np.asarray(bf16(np.asarray(a, np.float32)), np.float64)
 
+    # the weight gradients take dz as the BF16 operand of the tensor-core
+    # product h^T dz (hase_proposal.cu, mlpBackwardKernel); the bias sums keep it in FP32
     dz3 = np.outer(dl, w4r) * _dsilu(z3)
-    g_W3 = h2.T @ dz3
+    g_W3 = h2.T @ r(dz3)
     g_b3 = dz3.sum(0)
     dz2 = (r(dz3) @ W3r.T) * _dsilu(z2)
-    g_W2 = h1.T @ dz2
+    g_W2 = h1.T @ r(dz2)
     g_b2 = dz2.sum(0)
     dz1 = (r(dz2) @ W2r.T) * _dsilu(z1)
-    g_W1 = x.T @ dz1
+    g_W1 = x.T @ r(dz1)
     g_b1 = dz1.sum(0)
     grad = np.concatenate([g_W1.ravel(), g_b1, g_W2.ravel(), g_b2, g_W3.ravel(), g_b3, g_w4, [g_b4]])
     return float(loss), grad
