@@ -1353,16 +1353,6 @@ struct ProposalView {
     uint32_t K, divKm, divKs;
 };
 
-// floor(v) for |v| < 2^22 on the FMA pipe instead of the conversion unit:
-// adding and removing 1.5 x 2^23 rounds to the nearest integer (exact in
-// FP32), one step down where that rounded up.  floorIntFma reads the integer
-// from the biased value's mantissa.
-__device__ __forceinline__ float floorFma(float v) {
-    const float r = __fsub_rn(__fadd_rn(v, 12582912.0f), 12582912.0f);
-    return r > v ? r - 1.0f : r;
-}
-__device__ __forceinline__ int floorIntFma(float v) { return __float_as_int(__fadd_rn(floorFma(v), 12582912.0f)) - 0x4B400000; }
-
 __device__ __forceinline__ float sliceLnReflect(const ProposalView& V, uint32_t j) {
     return j == 0 ? 0.0f : j == 1 ? V.lnRb : j == 2 ? V.lnRt : V.lnRb + V.lnRt;
 }
@@ -1410,13 +1400,12 @@ __device__ __forceinline__ float pairFeatures(const ProposalView& V, uint32_t sa
         const float a = (float(k) + 0.5f) * 0.125f;
         const float x = S.x + a * dx, y = S.y + a * dy;
         // fold the unfolded height into [0, H]: period 2H, mirrored halves
-        // (floor and truncation agree after the clamp to 0; no conversion-unit op)
         float z = zi + a * dz;
-        z -= twoH * floorFma(z * V.invTwoH);
+        z -= twoH * floorf(z * V.invTwoH);
         if (z > V.H) z = twoH - z;
-        const int ly = min(max(floorIntFma(z * V.invh), 0), int(m.layers) - 1);
-        const int ix = min(max(floorIntFma((x - V.x0) * V.invCell), 0), int(V.gx) - 1);
-        const int iy = min(max(floorIntFma((y - V.y0) * V.invCell), 0), int(V.gy) - 1);
+        const int ly = min(max(int(z * V.invh), 0), int(m.layers) - 1);
+        const int ix = min(max(int((x - V.x0) * V.invCell), 0), int(V.gx) - 1);
+        const int iy = min(max(int((y - V.y0) * V.invCell), 0), int(V.gy) - 1);
         lng += __ldg(V.grid + (size_t(ly) * V.gy + iy) * V.gx + ix);
     }
     const float lnR = sliceLnReflect(V, j);

@@ -75,7 +75,7 @@ constexpr uint32_t kSmemBytes = SmemMap::bytes + 1024;  // + alignment slack
 
 // Training: also the backward weight images (W2, W3 as [in][out]: the B
 // operands of dz2 W2^T and dz3 W3^T), dz as the bf16 operand of the backward
-// and weight-gradient products and in f32 for the bias sums, and 512 TMEM
+// and weight-gradient products, the warps' partial bias sums, and 512 TMEM
 // columns: the three layer accumulators side by side (0, 64, 128), the
 // backward products (192), and the weight gradients accumulated over all
 // tiles of the CTA (M = 64 accumulators: dW3 at 256, dW2 at 320, dW1^T at
@@ -95,9 +95,8 @@ struct TrainSmem {
     static constexpr uint32_t a1 = a0 + kA0Bytes;
     static constexpr uint32_t a2 = a1 + kA1Bytes;
     static constexpr uint32_t dzb = a2 + kA1Bytes;
-    static constexpr uint32_t dzf = dzb + kA1Bytes;
-    static constexpr uint32_t dls = dzf + kTile * kHid * 4;
-    static constexpr uint32_t vec = dls + kTile * 4;
+    static constexpr uint32_t red = dzb + kA1Bytes;  // [4 warps][64] column partials, [4] row-sum partials
+    static constexpr uint32_t vec = red + (4 * kHid + 4) * 4;
     static constexpr uint32_t bar = (vec + kVecFloats * 4 + 15) & ~15u;
     static constexpr uint32_t tslot = bar + 8;
     static constexpr uint32_t bytes = tslot + 8;

@@ -57,12 +57,56 @@ __device__ __forceinline__ float dsilu(float z) {
 }
 
 // g[j] += sum over the tile's rows r of h[r][i0 + j] * dz[r][o] (j < 32) and
-// sum over the tile's rows of dz[r][o] (f32 [128][64] at dzOff): a bias gradient.
-__device__ __forceinline__ float columnSum(const Tile& T, uint32_t dzOff, uint32_t o) {
-    const float* dz = reinterpret_cast<const float*>(T.base + dzOff);
-    float s = 0.0f;
-    for (uint32_t r = 0; r < uint32_t(kTile); ++r) s += dz[r * kHid + o];
-    return s;
+// This thread's row of 64 values as bf16 row threadIdx.x of a canonical
+// K = 64 image at off (the A operand of the backward products).
+__device__ __forceinline__ void storeRowBf16(const Tile& T, uint32_t off, const float (&v)[kHid]) {
+    uint8_t* out = T.base + off + (threadIdx.x >> 3) * (kHid * 16u) + (threadIdx.x & 7u) * 16u;
+#pragma unroll
+    for (int c = 0; c < kHid / 8; ++c) {
+        uint4 w;
+        w.x = packBf16(v[8 * c + 0], v[8 * c + 1]);
+        w.y = packBf16(v[8 * c + 2], v[8 * c + 3]);
+        w.z = packBf16(v[8 * c + 4], v[8 * c + 5]);
+        w.w = packBf16(v[8 * c + 6], v[8 * c + 7]);
+        *reinterpret_cast<uint4*>(out + c * 128u) = w;
+    }
+}
+
+// Column sums over the tile's 128 rows of the 64-wide row v each thread holds
+// (its row): a warp reduce-scatter in registers (five butterfly steps; lane
+// L ends with columns 2L and 2L + 1 summed over the warp's rows), then the
+// four warps' partials through shared memory: thread t < 64 adds column t to
+// acc.  v is consumed.  All threads; ends with a barrier.
+__device__ __forceinline__ void tileColumnSums(const Tile& T, float (&v)[kHid], float& acc) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int step = 0; step < 5; ++step) {
+        const int half = 32 >> step;
+        const uint32_t off = 16u >> step;
+        const bool upper = (lane & off) != 0u;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const float a = v[i], b = v[i + half];
+            v[i] = (upper ? b : a) + __shfl_xor_sync(0xffffffffu, upper ? a : b, off);
+        }
+    }
+    float* red = reinterpret_cast<float*>(T.base + TrainSmem::red);
+    red[warp * kHid + 2 * lane] = v[0];
+    red[warp * kHid + 2 * lane + 1] = v[1];
+    __syncthreads();
+    if (threadIdx.x < uint32_t(kHid))
+        acc += (red[threadIdx.x] + red[kHid + threadIdx.x]) + (red[2 * kHid + threadIdx.x] + red[3 * kHid + threadIdx.x]);
+    __syncthreads();
+}
+
+// The sum over the tile's rows of one value per thread, added to acc by thread 0.
+__device__ __forceinline__ void tileRowSum(const Tile& T, float x, float& acc) {
+    for (uint32_t off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    float* red = reinterpret_cast<float*>(T.base + TrainSmem::red) + 4 * kHid;
+    if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) acc += (red[0] + red[1]) + (red[2] + red[3]);
+    __syncthreads();
 }
 
 // Adds this thread's row of an M = 64 weight-gradient accumulator (TMEM
@@ -102,8 +146,6 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
     const uint32_t t = threadIdx.x, o = t & 63u, ih = t >> 6;
     const float* vec = reinterpret_cast<const float*>(T.base + TrainSmem::vec);
     const float *b1 = vec, *b2 = vec + kHid, *b3 = vec + 2 * kHid, *w4 = vec + 3 * kHid;
-    float* dzf = reinterpret_cast<float*>(T.base + TrainSmem::dzf);
-    float* dls = reinterpret_cast<float*>(T.base + TrainSmem::dls);
     float gb1 = 0.0f, gb2 = 0.0f, gb3 = 0.0f, gw4 = 0.0f, gb4 = 0.0f;
     bool accumulate = false;  // the gradient accumulators hold a tile
     const uint32_t tiles = (P.rows + kTile - 1) / kTile;
@@ -120,38 +162,22 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         epilogueToSmem(T, 64, b2, TrainSmem::a2);
         runLayer(T, TrainSmem::a2, TrainSmem::w3, kHid, 128, TrainSmem::bar);
         // output layer: g_w4 = sum_r h3 dl, g_b4 = sum_r dl
+        float dz[kHid];
         {
             float z[kHid];
             loadRow(T, 128, z);
-            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = silu(z[n] + b3[n]) * dl;
-            dls[t] = dl;
+#pragma unroll
+            for (int n = 0; n < kHid; ++n) dz[n] = silu(z[n] + b3[n]) * dl;
         }
-        __syncthreads();
-        if (ih == 0) gw4 += columnSum(T, TrainSmem::dzf, o);
-        if (t == 0)
-            for (uint32_t r = 0; r < uint32_t(kTile); ++r) gb4 += dls[r];
-        __syncthreads();
+        tileColumnSums(T, dz, gw4);
+        tileRowSum(T, dl, gb4);
         // dz3 = dl w4 * silu'(z3)
         {
             float z[kHid];
             loadRow(T, 128, z);
-            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
 #pragma unroll
-            for (int c = 0; c < kHid / 8; ++c) {
-                float d[8];
-#pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    const int n = 8 * c + e;
-                    d[e] = dl * w4[n] * dsilu(z[n] + b3[n]);
-                    dzf[t * kHid + n] = d[e];
-                }
-                uint4 v;
-                v.x = packBf16(d[0], d[1]);
-                v.y = packBf16(d[2], d[3]);
-                v.z = packBf16(d[4], d[5]);
-                v.w = packBf16(d[6], d[7]);
-                *reinterpret_cast<uint4*>(out + c * 128u) = v;
-            }
+            for (int n = 0; n < kHid; ++n) dz[n] = dl * w4[n] * dsilu(z[n] + b3[n]);
+            storeRowBf16(T, TrainSmem::dzb, dz);
         }
         fenceBeforeSync();
         fenceProxyAsync();
@@ -165,30 +191,18 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             issueGradient(T, TrainSmem::a2, TrainSmem::dzb, kHid, TrainSmem::colGradW3, kIdescGradN64, accumulate);
             mmaCommit(T.sbase + TrainSmem::bar);
         }
-        if (ih == 0) gb3 += columnSum(T, TrainSmem::dzf, o);
+        tileColumnSums(T, dz, gb3);
         waitLayer(T, TrainSmem::bar);
-        float dh[kHid];
-        loadRow(T, 192, dh);
+        loadRow(T, 192, dz);
         {
             float z[kHid];
             loadRow(T, 64, z);
-            for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b2[n]);
+#pragma unroll
+            for (int n = 0; n < kHid; ++n) dz[n] *= dsilu(z[n] + b2[n]);
         }
         fenceBeforeSync();
-        __syncthreads();  // bias reads of dzf done; TMEM column 192 read
-        {
-            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
-#pragma unroll
-            for (int c = 0; c < kHid / 8; ++c) {
-                uint4 v;
-                v.x = packBf16(dh[8 * c + 0], dh[8 * c + 1]);
-                v.y = packBf16(dh[8 * c + 2], dh[8 * c + 3]);
-                v.z = packBf16(dh[8 * c + 4], dh[8 * c + 5]);
-                v.w = packBf16(dh[8 * c + 6], dh[8 * c + 7]);
-                *reinterpret_cast<uint4*>(out + c * 128u) = v;
-            }
-            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
-        }
+        __syncthreads();  // TMEM column 192 read by every warp
+        storeRowBf16(T, TrainSmem::dzb, dz);
         fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
@@ -201,29 +215,18 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             issueGradient(T, TrainSmem::a1, TrainSmem::dzb, kHid, TrainSmem::colGradW2, kIdescGradN64, accumulate);
             mmaCommit(T.sbase + TrainSmem::bar);
         }
-        if (ih == 0) gb2 += columnSum(T, TrainSmem::dzf, o);
+        tileColumnSums(T, dz, gb2);
         waitLayer(T, TrainSmem::bar);
-        loadRow(T, 192, dh);
+        loadRow(T, 192, dz);
         {
             float z[kHid];
             loadRow(T, 0, z);
-            for (int n = 0; n < kHid; ++n) dh[n] *= dsilu(z[n] + b1[n]);
+#pragma unroll
+            for (int n = 0; n < kHid; ++n) dz[n] *= dsilu(z[n] + b1[n]);
         }
         fenceBeforeSync();
-        __syncthreads();  // bias reads of dzf done
-        {
-            uint8_t* out = T.base + TrainSmem::dzb + (t >> 3) * (kHid * 16u) + (t & 7u) * 16u;
-#pragma unroll
-            for (int c = 0; c < kHid / 8; ++c) {
-                uint4 v;
-                v.x = packBf16(dh[8 * c + 0], dh[8 * c + 1]);
-                v.y = packBf16(dh[8 * c + 2], dh[8 * c + 3]);
-                v.z = packBf16(dh[8 * c + 4], dh[8 * c + 5]);
-                v.w = packBf16(dh[8 * c + 6], dh[8 * c + 7]);
-                *reinterpret_cast<uint4*>(out + c * 128u) = v;
-            }
-            for (int n = 0; n < kHid; ++n) dzf[t * kHid + n] = dh[n];
-        }
+        __syncthreads();  // TMEM column 192 read by every warp
+        storeRowBf16(T, TrainSmem::dzb, dz);
         fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             issueGradient(T, TrainSmem::dzb, TrainSmem::a0, kIn, TrainSmem::colGradW1, kIdescGradN16, accumulate);
             mmaCommit(T.sbase + TrainSmem::bar);
         }
-        if (ih == 0) gb1 += columnSum(T, TrainSmem::dzf, o);
+        tileColumnSums(T, dz, gb1);
         waitLayer(T, TrainSmem::bar);
         accumulate = true;
         fenceBeforeSync();
