@@ -153,3 +153,32 @@ def test_local_mode_is_rejected_by_batches(poly):
             b.solve([(ctx, 0, 3)], minRays=100)
     finally:
         ctx.set_local_proposal(0)
+
+
+def test_warm_started_series_runs_and_matches_the_plain_series():
+    """The warm-started learned series (learned.warm_started_series) on a
+    small pump series with the local proposal: every step fine-tunes the
+    network and solves all samples with it; beta follows the plain local
+    series within the Monte Carlo noise of phi-ASE, and the pump-only part
+    (mean beta after the first step, before any phi-ASE) is identical."""
+    from haseongpu_b200 import DeviceMesh
+    from haseongpu_b200.configs import disc_small
+    from haseongpu_b200.learned import warm_started_series
+    from haseongpu_b200.proposal import ProposalNet
+
+    w = disc_small()
+    sa, se = w.spectra.resampled(True)
+    mesh = w.mesh.withBeta(np.zeros(w.mesh.numberOfPrisms))
+    pump = dict(peakIntensity=16e3, radius=0.6, exponent=40.0, wavelength=940e-9, sigmaA=0.8e-20, sigmaE=0.16e-20)
+    tm = dict(timeStep=50e-6, steps=4)
+    with DeviceMesh(mesh, sa, se) as ctx:
+        ctx.set_local_proposal(12)
+        plain = ctx.simulate(pump=pump, time=tm, minRays=4000, rngSeed=3)
+    with DeviceMesh(mesh, sa, se) as ctx, ProposalNet(seed=2) as net:
+        ctx.set_local_proposal(12)
+        ws = warm_started_series(ctx, net, pump, tm, rays=4000, useReflections=False, monochromatic=True,
+                                 log_samples=16, log_rays=4000, train_steps=5, rngSeed=3)
+    assert len(ws["meanBeta"]) == 5 and len(ws["loss"]) == 3 and ws["raysTraced"] > 0
+    assert np.all(np.isfinite(ws["loss"]))
+    assert ws["meanBeta"][1] == pytest.approx(plain["meanBeta"][1], rel=1e-9)
+    np.testing.assert_allclose(ws["meanBeta"], plain["meanBeta"], rtol=2e-3)
