@@ -75,17 +75,18 @@ constexpr uint32_t kSmemBytes = SmemMap::bytes + 1024;  // + alignment slack
 
 // Training: also the backward weight images (W2, W3 as [in][out]: the B
 // operands of dz2 W2^T and dz3 W3^T), dz as the bf16 operand of the backward
-// and weight-gradient products, the warps' partial bias sums, and 512 TMEM
-// columns: the three layer accumulators side by side (0, 64, 128), the
-// backward products (192), and the weight gradients accumulated over all
-// tiles of the CTA (M = 64 accumulators: dW3 at 256, dW2 at 320, dW1^T at
-// 384).
+// and weight-gradient products, silu'(z1 + b1) as bf16 rows (z1's TMEM
+// columns are reused by layer 3), the warps' partial bias sums, and 256 TMEM
+// columns, so two CTAs share an SM: z1, then z3 and the backward products
+// (0); z2 (64); the weight gradients accumulated over all tiles of the CTA
+// as M = 64 accumulators, dW3 and dW2 interleaved in one 64-column block
+// (lanes 0-15 and 16-31 of each warp quarter, 128) and dW1^T (lanes 0-15,
+// 192).
 struct TrainSmem {
     static constexpr uint32_t wBytes = kWBlobBytes;
-    static constexpr uint32_t tmemCols = 512;
-    static constexpr uint32_t colGradW3 = 256;
-    static constexpr uint32_t colGradW2 = 320;
-    static constexpr uint32_t colGradW1 = 384;
+    static constexpr uint32_t tmemCols = 256;
+    static constexpr uint32_t colGradW32 = 128;  // dW3 in lanes 0-15, dW2 in lanes 16-31
+    static constexpr uint32_t colGradW1 = 192;
     static constexpr uint32_t w1 = 0;
     static constexpr uint32_t w2 = w1 + kW1Bytes;
     static constexpr uint32_t w3 = w2 + kW2Bytes;
@@ -95,13 +96,15 @@ struct TrainSmem {
     static constexpr uint32_t a1 = a0 + kA0Bytes;
     static constexpr uint32_t a2 = a1 + kA1Bytes;
     static constexpr uint32_t dzb = a2 + kA1Bytes;
-    static constexpr uint32_t red = dzb + kA1Bytes;  // [4 warps][64] column partials, [4] row-sum partials
+    static constexpr uint32_t ds1 = dzb + kA1Bytes;  // silu'(z1 + b1), bf16, the canonical row layout
+    static constexpr uint32_t red = ds1 + kA1Bytes;  // [4 warps][64] column partials, [4] row-sum partials
     static constexpr uint32_t vec = red + (4 * kHid + 4) * 4;
     static constexpr uint32_t bar = (vec + kVecFloats * 4 + 15) & ~15u;
     static constexpr uint32_t tslot = bar + 8;
     static constexpr uint32_t bytes = tslot + 8;
 };
 constexpr uint32_t kTrainSmemBytes = TrainSmem::bytes + 1024;
+static_assert(2 * (kTrainSmemBytes + 1024) <= 228u * 1024u, "two training CTAs per SM");
 static_assert(SmemMap::w3 == TrainSmem::w3, "the forward images lead the weight blob in both maps");
 
 __host__ __device__ constexpr uint32_t canonOffset(uint32_t r, uint32_t k, uint32_t K) {

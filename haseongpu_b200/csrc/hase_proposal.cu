@@ -72,6 +72,40 @@ __device__ __forceinline__ void storeRowBf16(const Tile& T, uint32_t off, const 
     }
 }
 
+// This thread's bf16 row of a canonical K = 64 image at off, as floats.
+__device__ __forceinline__ void loadRowBf16(const Tile& T, uint32_t off, float (&v)[kHid]) {
+    const uint8_t* in = T.base + off + (threadIdx.x >> 3) * (kHid * 16u) + (threadIdx.x & 7u) * 16u;
+#pragma unroll
+    for (int c = 0; c < kHid / 8; ++c) {
+        const uint4 w = *reinterpret_cast<const uint4*>(in + c * 128u);
+        const uint32_t x[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            v[8 * c + 2 * e] = __uint_as_float(x[e] << 16);
+            v[8 * c + 2 * e + 1] = __uint_as_float(x[e] & 0xFFFF0000u);
+        }
+    }
+}
+
+// The layer-1 epilogue of a training tile: h1 = silu(z1 + b1) into A1 and
+// silu'(z1 + b1) into the ds1 rows (bf16), so that layer 3 can reuse z1's
+// TMEM columns.
+__device__ __forceinline__ void epilogueLayer1Train(Tile& T, const float* b1) {
+    float z[kHid], h[kHid];
+    loadRow(T, 0, z);
+#pragma unroll
+    for (int n = 0; n < kHid; ++n) {
+        const float v = z[n] + b1[n];
+        h[n] = silu(v);
+        z[n] = dsilu(v);
+    }
+    storeRowBf16(T, TrainSmem::a1, h);
+    storeRowBf16(T, TrainSmem::ds1, z);
+    fenceBeforeSync();
+    fenceProxyAsync();
+    __syncthreads();
+}
+
 // Column sums over the tile's 128 rows of the 64-wide row v each thread holds
 // (its row): a warp reduce-scatter in registers (five butterfly steps; lane
 // L ends with columns 2L and 2L + 1 summed over the warp's rows), then the
@@ -132,14 +166,15 @@ struct TrainLaunch {
     int* error;
 };
 
-// Recomputes the forward pass of each tile (layer accumulators kept in TMEM
-// columns 0 / 64 / 128) and back-propagates dL/dlogit on the tensor cores:
-// per layer one commit covers the backward product (dz3 W3^T or dz2 W2^T,
-// TMEM column 192) and the weight-gradient product (h2^T dz3, h1^T dz2,
-// dz1^T x: the activation and dz images read as MN-major operands) that
-// accumulates in TMEM over all tiles of the CTA; the bias sums run on the
-// CUDA cores meanwhile.  The CTA adds its gradients to `grad` once.
-__global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch P) {
+// Recomputes the forward pass of each tile and back-propagates dL/dlogit on
+// the tensor cores: per layer one commit covers the backward product (dz3
+// W3^T or dz2 W2^T, over the consumed layer-3 accumulator) and the
+// weight-gradient product (h2^T dz3, h1^T dz2, dz1^T x: the activation and dz
+// images read as MN-major operands) that accumulates in TMEM over all tiles
+// of the CTA; the bias sums run on the CUDA cores meanwhile.  Two CTAs per SM
+// (256 TMEM columns each, TrainSmem).  The CTA adds its gradients to `grad`
+// once.
+__global__ void __launch_bounds__(kTile, 2) mlpBackwardKernel(const TrainLaunch P) {
     extern __shared__ uint8_t dynSmem[];
     Tile T;
     tileBegin<TrainSmem>(T, dynSmem, P.wimg, P.vec);
@@ -157,15 +192,15 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         const float dl = row < P.rows ? P.dl[row] : 0.0f;
         storeFeatures(T, TrainSmem::a0, f);
         runLayer(T, TrainSmem::a0, TrainSmem::w1, kIn, 0, TrainSmem::bar);
-        epilogueToSmem(T, 0, b1, TrainSmem::a1);
+        epilogueLayer1Train(T, b1);
         runLayer(T, TrainSmem::a1, TrainSmem::w2, kHid, 64, TrainSmem::bar);
         epilogueToSmem(T, 64, b2, TrainSmem::a2);
-        runLayer(T, TrainSmem::a2, TrainSmem::w3, kHid, 128, TrainSmem::bar);
+        runLayer(T, TrainSmem::a2, TrainSmem::w3, kHid, 0, TrainSmem::bar);  // z3 over z1
         // output layer: g_w4 = sum_r h3 dl, g_b4 = sum_r dl
         float dz[kHid];
         {
             float z[kHid];
-            loadRow(T, 128, z);
+            loadRow(T, 0, z);
 #pragma unroll
             for (int n = 0; n < kHid; ++n) dz[n] = silu(z[n] + b3[n]) * dl;
         }
@@ -174,7 +209,7 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         // dz3 = dl w4 * silu'(z3)
         {
             float z[kHid];
-            loadRow(T, 128, z);
+            loadRow(T, 0, z);
 #pragma unroll
             for (int n = 0; n < kHid; ++n) dz[n] = dl * w4[n] * dsilu(z[n] + b3[n]);
             storeRowBf16(T, TrainSmem::dzb, dz);
@@ -182,18 +217,19 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
-        // dh2 = dz3 W3^T and g_W3 += h2^T dz3 on the tensor cores, g_b3 on the CUDA cores
+        // dh2 = dz3 W3^T (over z3, read by every thread before the barrier above)
+        // and g_W3 += h2^T dz3 on the tensor cores, g_b3 on the CUDA cores
         if (t == 0) {
             fenceAfterSync();
             for (uint32_t kk = 0; kk < uint32_t(kHid) / 16u; ++kk)
-                mmaBf16(T.tmem + 192, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
+                mmaBf16(T.tmem, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
                         smemDesc(T.sbase + TrainSmem::w3b + kk * 256u, 128u, kHid * 16u), kk > 0 ? 1u : 0u);
-            issueGradient(T, TrainSmem::a2, TrainSmem::dzb, kHid, TrainSmem::colGradW3, kIdescGradN64, accumulate);
+            issueGradient(T, TrainSmem::a2, TrainSmem::dzb, kHid, TrainSmem::colGradW32, kIdescGradN64, accumulate);
             mmaCommit(T.sbase + TrainSmem::bar);
         }
         tileColumnSums(T, dz, gb3);
         waitLayer(T, TrainSmem::bar);
-        loadRow(T, 192, dz);
+        loadRow(T, 0, dz);
         {
             float z[kHid];
             loadRow(T, 64, z);
@@ -201,31 +237,33 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
             for (int n = 0; n < kHid; ++n) dz[n] *= dsilu(z[n] + b2[n]);
         }
         fenceBeforeSync();
-        __syncthreads();  // TMEM column 192 read by every warp
+        __syncthreads();  // TMEM columns 0 (dh2) and 64 (z2) read by every warp
         storeRowBf16(T, TrainSmem::dzb, dz);
         fenceBeforeSync();
         fenceProxyAsync();
         __syncthreads();
-        // dh1 = dz2 W2^T and g_W2 += h1^T dz2, g_b2 meanwhile
+        // dh1 = dz2 W2^T (over dh2) and g_W2 += h1^T dz2 (the lanes 16-31 half
+        // of the gradient block), g_b2 meanwhile
         if (t == 0) {
             fenceAfterSync();
             for (uint32_t kk = 0; kk < uint32_t(kHid) / 16u; ++kk)
-                mmaBf16(T.tmem + 192, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
+                mmaBf16(T.tmem, smemDesc(T.sbase + TrainSmem::dzb + kk * 256u, 128u, kHid * 16u),
                         smemDesc(T.sbase + TrainSmem::w2b + kk * 256u, 128u, kHid * 16u), kk > 0 ? 1u : 0u);
-            issueGradient(T, TrainSmem::a1, TrainSmem::dzb, kHid, TrainSmem::colGradW2, kIdescGradN64, accumulate);
+            issueGradient(T, TrainSmem::a1, TrainSmem::dzb, kHid, (16u << 16) + TrainSmem::colGradW32, kIdescGradN64,
+                          accumulate);
             mmaCommit(T.sbase + TrainSmem::bar);
         }
         tileColumnSums(T, dz, gb2);
         waitLayer(T, TrainSmem::bar);
-        loadRow(T, 192, dz);
+        loadRow(T, 0, dz);
         {
-            float z[kHid];
-            loadRow(T, 0, z);
+            float d1[kHid];
+            loadRowBf16(T, TrainSmem::ds1, d1);
 #pragma unroll
-            for (int n = 0; n < kHid; ++n) dz[n] *= dsilu(z[n] + b1[n]);
+            for (int n = 0; n < kHid; ++n) dz[n] *= d1[n];
         }
         fenceBeforeSync();
-        __syncthreads();  // TMEM column 192 read by every warp
+        __syncthreads();  // TMEM column 0 read by every warp
         storeRowBf16(T, TrainSmem::dzb, dz);
         fenceBeforeSync();
         fenceProxyAsync();
@@ -244,9 +282,15 @@ __global__ void __launch_bounds__(kTile, 1) mlpBackwardKernel(const TrainLaunch 
         if (!__syncthreads_and(T.ok)) break;
     }
     if (accumulate) {
-        // g_W3 and g_W2 as [in][out] rows (row = input); g_W1^T as [out][in] rows
-        flushGradient<kHid>(T, TrainSmem::colGradW3, P.grad + kOffW3, kHid, 1u, kHid);
-        flushGradient<kHid>(T, TrainSmem::colGradW2, P.grad + kOffW2, kHid, 1u, kHid);
+        // g_W3 (lanes 0-15) and g_W2 (lanes 16-31) as [in][out] rows (row =
+        // input) from the interleaved block; g_W1^T as [out][in] rows
+        {
+            float acc[kHid];
+            loadCols<kHid>(T, TrainSmem::colGradW32, acc);
+            const uint32_t lane = t & 31u, r = 16u * (t >> 5) + (lane & 15u);
+            float* g = P.grad + (lane < 16u ? kOffW3 : kOffW2) + r * kHid;
+            for (int n = 0; n < kHid; ++n) atomicAdd(g + n, acc[n]);
+        }
         flushGradient<kIn>(T, TrainSmem::colGradW1, P.grad + kOffW1, 1u, kHid, kFeat);
     }
     if (ih == 0) {
@@ -573,7 +617,7 @@ hase_status lossGrad(hase_proposal* net, DeviceBatch& d, uint32_t g0, uint32_t g
     const uint32_t rows = r1 - r0;
     if (rows == 0) return HASE_OK;
     const uint32_t tiles = (rows + kTile - 1) / kTile;
-    const uint32_t grid = std::min(tiles, net->numSMs);
+    const uint32_t grid = std::min(tiles, 2u * net->numSMs);  // two CTAs per SM
     const uint32_t fgrid = std::min(tiles, net->numSMs * kMlpBlocksPerSM);
     ForwardLaunch F{net->wimg.p, net->vec.p, d.features.p + size_t(r0) * kFeat, d.logits.p + r0, rows, net->error.p};
     mlpForwardKernel<<<fgrid, kTile, kSmemBytes, net->stream>>>(F);

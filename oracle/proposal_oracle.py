@@ -132,7 +132,7 @@ def loss_and_grad(params, features, offsets, targets, group_weights=None):
     dz2 = (r(dz3) @ W3r.T) * _dsilu(z2)
     g_W2 = h1.T @ r(dz2)
     g_b2 = dz2.sum(0)
-    dz1 = (r(dz2) @ W2r.T) * _dsilu(z1)
+    dz1 = (r(dz2) @ W2r.T) * r(_dsilu(z1))  # silu'(z1) kept as bf16 rows on the device
     g_W1 = x.T @ r(dz1)
     g_b1 = dz1.sum(0)
     grad = np.concatenate([g_W1.ravel(), g_b1, g_W2.ravel(), g_b2, g_W3.ravel(), g_b3, g_w4, [g_b4]])
