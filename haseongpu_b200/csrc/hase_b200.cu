@@ -721,20 +721,18 @@ __device__ __forceinline__ uint32_t upperBound(const uint32_t* a, uint32_t n, ui
 
 // Start state of ray r of sample `sample`, drawn in reflection slice j and
 // prism p with probability qf / Q (qf: the map's integer weight q of the
-// entry, scaled for the local proposal's split): Philox4x32-10 counter (r,
+// entry, or the local proposal's mixture weight): Philox4x32-10 counter (r,
 // sample, pass, kTagRay); a uniform point in the prism, or (nearField) the
-// solid-angle start in a prism touching the image point; the wavelength bin
-// floor((rs 0x9E3779B9 + phase mod 2^32) nL / 2^32), rs the ray's index in
-// its source (r itself, or for the local proposal's two sources the index
-// within its own range).  wf: the ray's weight
-// without C Q, beta V / (d^2 qf) (uniform start) or beta alpha L / qf (near
-// field).
+// solid-angle start in a prism touching the image point.  No wavelength is
+// drawn: the walk keeps the path integrals every wavelength's gain is linear
+// in, and the ray's contribution is its gain averaged over the spectrum
+// (rayMeanGain); ab is the walk's reference pair (the spectrum's first).
+// wf: the ray's weight without C Q, beta V / (d^2 qf)
+// (uniform start) or beta alpha L / qf (near field).
 // Returns |start - image|^2 (0: the start point is the sample point itself).
-__device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_t rs, uint32_t j, uint32_t p,
-                                          uint32_t sample,
+__device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_t j, uint32_t p, uint32_t sample,
                                           float2 S, int ls, uint32_t pass, uint32_t seedLo, uint32_t seedHi,
-                                          uint32_t nLambda, uint32_t lambdaPhase, const float2* spec,
-                                          float qf, uint32_t nearField, Ray& ray, float& wf) {
+                                          float2 ab, float qf, uint32_t nearField, Ray& ray, float& wf) {
     // layer by an exact multiply-shift: no integer division per ray
     const uint32_t l = prismLayer(m, p), t = p - l * m.T;
     const Philox4 rnd = philox4x32_10(r, sample, pass, kTagRay, seedLo, seedHi);
@@ -744,13 +742,6 @@ __device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_
         k2 = (1u << 24) - 1u - k2;
     }
     const int kImg = imageLevel(ls, int(m.layers), j);
-    // wavelength bin: a golden-ratio (Weyl) sequence over the ray's index in
-    // its source, offset by the row's 32-bit phase of this pass.  Every ray's
-    // bin is uniform and independent of its prism (the phase is), and the
-    // consecutive rays of one prism spread over the spectrum, so the rays'
-    // sample variance is the estimate's
-    const uint32_t lam = nLambda > 1 ? __umulhi(rs * kWeylStep + lambdaPhase, nLambda) : 0u;
-    const float2 ab = __ldg(spec + lam);
     float dx, dy, dz, alphaL, D2;
     if (nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
         nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
@@ -947,8 +938,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
         const double CQ = Cm * double(Qn);
         const float2 S = __ldg(m.points + sample % m.Np);
         const int ls = int(sample / m.Np);
-        const uint32_t lambdaPhase =
-            HASE_N_LAMBDA > 1 ? philox4x32_10(0u, sample, L.pass, kTagMap, HASE_SEED_LO, L.seedHi).y : 0u;
         // prisms holding the item's mapped rays [r0, rn1): [pb, pb + count - 1)
         // (the local proposal maps its near rays [0, Mnear) only)
         const uint32_t rn1 = LOCAL ? min(r1, L.Mnear) : r1;
@@ -994,11 +983,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                         qf = float(__ldg(q + b));
                     }
                     if (go) {
-                        // wavelength sequence: over the rays of the ray's source
-                        const bool farRay = LOCAL && r >= L.Mnear;
-                        const float D2 = startRay(m, r, farRay ? r - L.Mnear : r, j, p, sample, S, ls, L.pass,
-                                                  HASE_SEED_LO, L.seedHi, HASE_N_LAMBDA, lambdaPhase, HASE_SPEC, qf,
-                                                  L.nearField, ray, wf);
+                        const float D2 = startRay(m, r, j, p, sample, S, ls, L.pass, HASE_SEED_LO, L.seedHi,
+                                                  __ldg(HASE_SPEC), qf, L.nearField, ray, wf);
                         active = D2 > 0.0f;
                         if (!active) ++dropped;  // start point on the sample point itself
                     }
@@ -1012,8 +998,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
                     if (st == kDone) {
                         finishReflections(m, ray);
                         // the ray's gain in FP32 (FP64 only where exp(G)
-                        // nears the FP32 range; the sums stay FP64)
-                        const double eg = ray.G < 80.0f ? double(expf(ray.G)) : exp(double(ray.G));
+                        // nears the FP32 range; the sums stay FP64), averaged
+                        // over the spectrum by the beta walks
+                        double eg;
+                        if constexpr (WALK == kWalkTable)
+                            eg = ray.G < 80.0f ? double(expf(ray.G)) : exp(double(ray.G));
+                        else
+                            eg = rayMeanGain(ray, HASE_SPEC, HASE_N_LAMBDA);
                         const double X = CQ * double(wf) * eg;
                         sum += X;
                         sum2 += X * X;

@@ -134,19 +134,27 @@ struct Ray {
     int reflLeft;   // reflections the slice still implies
     int steps;
     float s;        // remaining distance to the image point
-    float G;        // accumulated ln(gain), including reflection factors
+    float G;        // accumulated ln(gain) for the pair (A, B), including reflection factors
+    float A, B;     // g = beta*A - B: the walk's reference pair
+    float Jb;       // integral of beta dl over gain prisms (beta walks)
+    float Lc;       // path length in cladding prisms (kWalkBeta)
+    float D;        // path length, start to image point
     float ux, uy, uz;
     float hOverUz;  // h / uz
     float zl;       // unfolded layer index + level-plane offset: the current layer's exit plane lies zl h
                     // from the image point along z (a small integer, exact in float)
-    float A, B;     // g = beta*A - B
 };
 
 enum StepResult { kContinue = 0, kDone = 1, kDropped = 2 };
 
-// How a walk obtains the gain coefficient g of the current prism.
+// How a walk obtains the gain coefficient g of the current prism.  The beta
+// walks also keep the path integrals that make the gain of every wavelength
+// (A_l, B_l) follow from the reference pair's: ln G_l = G + (A_l - A) Jb -
+// (B_l - B)(D - Lc), so a ray's gain is known for the whole spectrum
+// (rayMeanGain); for the reference pair it is G itself, bit for bit as the
+// table walk gives it.
 enum WalkMode {
-    kWalkBeta = 0,         // beta from m.gainBeta, g = beta A - B, cladding (NaN beta): g = -claddingAbsorption
+    kWalkBeta = 0,         // beta from m.gainBeta; cladding prisms (NaN beta) add to Lc
     kWalkTable = 1,        // g from m.gTab (a monochromatic solve: the table is built for its pair)
     kWalkBetaNoClad = 2,   // as kWalkBeta for a medium without cladding prisms (beta is never NaN)
 };
@@ -168,6 +176,9 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.steps = 0;
     r.s = D;
     r.G = 0.0f;
+    r.Jb = 0.0f;
+    r.Lc = 0.0f;
+    r.D = D;
     r.ux = dx * inv;
     r.uy = dy * inv;
     r.uz = dz * inv;
@@ -177,6 +188,49 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.A = A;
     r.B = B;
     return D2;
+}
+
+// One segment of length len in a prism whose table value (kWalkTable: g) or
+// beta (NaN: cladding) is gb.
+template <int WALK>
+__device__ __forceinline__ void addSegment(Ray& r, float gb, float len, float cladAbs) {
+    if constexpr (WALK == kWalkTable) {
+        r.G = fmaf(gb, len, r.G);
+    } else if constexpr (WALK == kWalkBetaNoClad) {
+        r.G = fmaf(fmaf(gb, r.A, -r.B), len, r.G);
+        r.Jb = fmaf(gb, len, r.Jb);
+    } else {
+        const bool gain = gb == gb;
+        r.G = fmaf(gain ? fmaf(gb, r.A, -r.B) : -cladAbs, len, r.G);
+        r.Jb = fmaf(gain ? gb : 0.0f, len, r.Jb);
+        r.Lc += gain ? 0.0f : len;
+    }
+}
+
+// ln gain of a finished ray (beta walks) for the pair (A_l, B_l): exact for
+// the reference pair.
+__device__ __forceinline__ float rayLnGain(const Ray& r, float Al, float Bl) {
+    return fmaf(Al - r.A, r.Jb, fmaf(r.B - Bl, r.D - r.Lc, r.G));
+}
+
+// The mean over the nL wavelengths (A_l, B_l) of a finished ray's gain
+// (beta walks): the exponents shifted by their maximum, FP32 exponentials of
+// the differences, the maximum's exponential in FP64 where FP32 nears its
+// range.  One wavelength: exp(G), as the table walk.
+__device__ __forceinline__ double rayMeanGain(const Ray& r, const float2* spec, uint32_t nL) {
+    if (nL == 1) return r.G < 80.0f ? double(expf(r.G)) : exp(double(r.G));
+    float xm = -INFINITY;
+    for (uint32_t l = 0; l < nL; ++l) {
+        const float2 ab = __ldg(spec + l);
+        xm = fmaxf(xm, rayLnGain(r, ab.x, ab.y));
+    }
+    float sum = 0.0f;
+    for (uint32_t l = 0; l < nL; ++l) {
+        const float2 ab = __ldg(spec + l);
+        sum += __expf(rayLnGain(r, ab.x, ab.y) - xm);
+    }
+    const double e = xm < 80.0f ? double(expf(xm)) : exp(double(xm));
+    return e * double(sum) / double(nL);
 }
 
 // One triangle column: the edge exit of the current triangle (edge exits are
@@ -228,16 +282,13 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
         const int dl = r.uz > 0.0f ? -1 : 1;
         while (true) {
             const float sz = fminf(r.zl * r.hOverUz, r.s);
-            const float g = WALK == kWalkTable        ? gb
-                            : WALK == kWalkBetaNoClad ? fmaf(gb, r.A, -r.B)
-                                                      : ((gb == gb) ? fmaf(gb, r.A, -r.B) : -m.cladAbs);
             const float next = fmaxf(sEdge, sz);
             if (next <= m.tolEnd) {
-                r.G = fmaf(g, r.s, r.G);
+                addSegment<WALK>(r, gb, r.s, m.cladAbs);
                 r.s = 0.0f;
                 return kDone;
             }
-            r.G = fmaf(g, r.s - next, r.G);
+            addSegment<WALK>(r, gb, r.s - next, m.cladAbs);
             r.s = next;
             ++r.steps;
             if (sz < sEdge) break;

@@ -196,9 +196,12 @@ inline double reflectFactor(const Model& md, uint32_t t, int surf, double cz) {
 }
 
 struct Walk {
-    double lnGain;
+    double lnGain;  // for the (A, B) passed to walk
     double dist;
     bool dropped;
+    // path integrals every wavelength's ln gain is linear in:
+    // ln G_l = A_l jb - B_l lg - claddingAbsorption lc + lnR
+    double jb, lg, lc, lnR;
 };
 
 // Walk from start (x0,y0,z0) in prism (t, level) to the (image) target.
@@ -207,7 +210,7 @@ Walk walk(const Model& md, double x0, double y0, double z0, uint32_t t, uint32_t
     const Tables& tb = md.tab;
     double ux = x0 - Sx, uy = y0 - Sy, uz = z0 - Sz;
     const double D = std::sqrt(ux * ux + uy * uy + uz * uz);
-    Walk w{0.0, D, false};
+    Walk w{0.0, D, false, 0.0, 0.0, 0.0, 0.0};
     if (D == 0.0) return w;
     ux /= D; uy /= D; uz /= D;
     const double tol = 1e-9 * md.extent;
@@ -236,13 +239,17 @@ Walk walk(const Model& md, double x0, double y0, double z0, uint32_t t, uint32_t
         if (sz > s) sz = s;
         const uint32_t phys = physicalLayer(lu, md.layers);
         const double g = gainCoeff(md, t, phys, A, B);
+        const bool clad = isCladding(md, t);
+        const double beta = clad ? 0.0 : md.m->betaVolume[size_t(phys) * md.T + t];
         const double next = std::max(std::max(best, sz), 0.0);
+        const double len = next <= tol ? s : s - next;
+        G += g * len;
+        if (clad) w.lc += len;
+        else { w.jb += beta * len; w.lg += len; }
         if (next <= tol) {  // the target lies in (or on the boundary of) this prism
-            G += g * s;
             s = 0.0;
             break;
         }
-        G += g * (s - next);
         s = next;
         if (sz >= best) {
             // level plane k = lu (down) or lu + 1 (up)
@@ -270,6 +277,7 @@ Walk walk(const Model& md, double x0, double y0, double z0, uint32_t t, uint32_t
         lnR += R > 0.0 ? std::log(R) : -std::numeric_limits<double>::infinity();
     }
     w.lnGain = G + lnR;
+    w.lnR = lnR;
     return w;
 }
 
@@ -439,9 +447,6 @@ int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum, con
                         const uint32_t b = uint32_t(std::upper_bound(off.begin(), off.end(), r) - off.begin()) - 1u;
                         const uint32_t j = b / md.P, p = b % md.P;
                         const uint32_t t = p % md.T, l = p / md.T;
-                        // golden-ratio sequence over r, offset by the 32-bit phase po[1]
-                        const uint32_t lambda =
-                            uint32_t((uint64_t(uint32_t(r * 0x9E3779B9u + po[1])) * nLambda) >> 32);
                         uint32_t rc4[4] = {r, s, pass, kTagRay}, ro[4];
                         philox(rc4, key, ro);
                         const uint32_t* v = mesh->triangles + 3 * t;
@@ -483,10 +488,16 @@ int oracle_phi_ase(const oracle_mesh* mesh, const oracle_spectrum* spectrum, con
                             z = (double(l) + unit(ro[2])) * md.h;
                             factor = -1.0;  // uniform in the prism: density 1/V
                         }
-                        const Walk wk = walk(md, x, y, z, t, l, Sx, Sy, Iz, j, md.gainA[lambda], md.gainB[lambda]);
+                        const Walk wk = walk(md, x, y, z, t, l, Sx, Sy, Iz, j, md.meanA, md.meanB);
                         if (wk.dropped || wk.dist == 0.0) { ++dropped; continue; }
                         const double vol = factor > 0.0 ? factor : md.tab.area[t] * md.h / (wk.dist * wk.dist);
-                        const double X = C * mesh->betaVolume[p] * vol * (double(Q) / double(q[b])) * std::exp(wk.lnGain);
+                        // the ray's gain averaged over the spectrum (no wavelength is drawn)
+                        double eg = 0.0;
+                        for (uint32_t lam = 0; lam < nLambda; ++lam)
+                            eg += std::exp(md.gainA[lam] * wk.jb - md.gainB[lam] * wk.lg -
+                                           mesh->claddingAbsorption * wk.lc + wk.lnR);
+                        eg /= double(nLambda);
+                        const double X = C * mesh->betaVolume[p] * vol * (double(Q) / double(q[b])) * eg;
                         sum += X;
                         sum2 += X * X;
                     }
