@@ -449,8 +449,9 @@ def test_monochromatic_walk_matches_the_general_walk(case):
 
 def test_gpu_polychromatic_seeds_agree_within_reported_error():
     """Two seeds of a polychromatic solve with reflections (disc_poly, 16
-    wavelengths) agree within their reported errors: the wavelength bin of a
-    ray is independent of its prism, so the reported relative error holds."""
+    wavelengths) agree within their reported errors: every ray averages its
+    gain over the spectrum, so the rays are independent and the reported
+    relative error holds."""
     from haseongpu_b200.configs import disc_poly
 
     w = disc_poly()
@@ -462,3 +463,27 @@ def test_gpu_polychromatic_seeds_agree_within_reported_error():
     sig = np.hypot(a.relativeStandardError * a.phiAse, b.relativeStandardError * b.phiAse)
     z = (a.phiAse.astype(np.float64) - b.phiAse) / sig
     assert z.std() < 1.3 and np.abs(z).max() < 4.5, (z.std(), np.abs(z).max())
+
+
+def test_gpu_spectral_mean_equals_the_mean_of_monochromatic_solves():
+    """A polychromatic solve averages every ray's gain over the spectrum (the
+    walk's path integrals give each wavelength's exponent); its estimate is
+    the mean of the monochromatic solves of the 16 wavelengths, within the
+    combined Monte Carlo error (disc_poly, reflections, independent seeds)."""
+    from haseongpu_b200.configs import disc_poly
+
+    w = disc_poly()
+    sa, se = w.spectra.resampled()
+    kw = dict(minRays=200_000, useReflections=True, minSample=3000, maxSample=3031)
+    with _ctx(w.mesh, sa, se) as ctx:
+        poly = ctx.calc_phi_ase(rngSeed=3, **kw)
+    phis, var = [], []
+    for lam in range(len(sa)):
+        with _ctx(w.mesh, [float(sa[lam])], [float(se[lam])]) as one:
+            r = one.calc_phi_ase(rngSeed=10 + lam, **kw)
+        phis.append(r.phiAse.astype(np.float64))
+        var.append((r.relativeStandardError * r.phiAse.astype(np.float64)) ** 2)
+    mean = np.mean(phis, axis=0)
+    sigma = np.hypot(poly.relativeStandardError * poly.phiAse, np.sqrt(np.sum(var, axis=0)) / len(sa))
+    z = (poly.phiAse.astype(np.float64) - mean) / sigma
+    assert np.abs(z).max() < 4.5 and abs(z.mean()) < 4.0 / np.sqrt(z.size), (np.abs(z).max(), z.mean())

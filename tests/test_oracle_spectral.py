@@ -1,12 +1,13 @@
 """CPU: the polychromatic estimate's reported error is its error.
 
 Rays are ordered by prism (the ray map is a prefix over the weight row), so a
-wavelength bin that follows the ray index in contiguous strata gives whole
-regions of the medium one wavelength per pass; the rays' sample variance then
-misses the between-wavelength part.  With the golden-ratio sequence each
-ray's bin is independent of its prism.  Check: over eight seeds, the spread
-of each sample's estimate stays within its reported relative error (16
-wavelengths, reflections, fixed importance weights, 40,000 rays)."""
+wavelength drawn from the ray index in contiguous strata gives whole regions
+of the medium one wavelength per pass, and the rays' sample variance misses
+the between-wavelength part.  Each ray now averages its gain over the whole
+spectrum (its walk's path integrals give every wavelength's exponent), so
+the rays are independent again.  Check: over eight seeds, the spread of each
+sample's estimate stays within its reported relative error (16 wavelengths,
+reflections, fixed importance weights, 40,000 rays)."""
 
 from __future__ import annotations
 
