@@ -214,22 +214,20 @@ __device__ __forceinline__ float rayLnGain(const Ray& r, float Al, float Bl) {
 }
 
 // The mean over the nL wavelengths (A_l, B_l) of a finished ray's gain
-// (beta walks): the exponents shifted by their maximum, FP32 exponentials of
-// the differences, the maximum's exponential in FP64 where FP32 nears its
-// range.  One wavelength: exp(G), as the table walk.
+// (beta walks), relative to the reference pair's exact exp(G) (FP64 above
+// G = 80): one FP32 exponential per wavelength of the difference of its
+// exponent from G, (A_l - A) Jb - (B_l - B)(D - Lc) (bounded by the spread
+// of the cross sections along one path; clamped at 80).  One wavelength:
+// exp(G), as the table walk.
 __device__ __forceinline__ double rayMeanGain(const Ray& r, const float2* spec, uint32_t nL) {
-    if (nL == 1) return r.G < 80.0f ? double(expf(r.G)) : exp(double(r.G));
-    float xm = -INFINITY;
-    for (uint32_t l = 0; l < nL; ++l) {
-        const float2 ab = __ldg(spec + l);
-        xm = fmaxf(xm, rayLnGain(r, ab.x, ab.y));
-    }
+    const double e = r.G < 80.0f ? double(expf(r.G)) : exp(double(r.G));
+    if (nL == 1) return e;
+    const float Lg = r.D - r.Lc;
     float sum = 0.0f;
     for (uint32_t l = 0; l < nL; ++l) {
         const float2 ab = __ldg(spec + l);
-        sum += __expf(rayLnGain(r, ab.x, ab.y) - xm);
+        sum += __expf(fminf(fmaf(ab.x - r.A, r.Jb, (r.B - ab.y) * Lg), 80.0f));
     }
-    const double e = xm < 80.0f ? double(expf(xm)) : exp(double(xm));
     return e * double(sum) / double(nL);
 }
 
