@@ -73,6 +73,10 @@ typedef struct {
     const double* refractiveIndices;    /* [4]: bottom inside, bottom outside, top inside, top outside; NULL = 1 */
 } hase_mesh_desc;
 
+/* Cross sections on a common wavelength grid.  phi-ASE is the mean over the
+ * wavelengths: every ray of a polychromatic solve contributes its gain
+ * averaged over all of them (its walk keeps the path integrals every
+ * wavelength's exponent is linear in), so no wavelength is drawn per ray. */
 typedef struct {
     uint32_t numberOfWavelengths;       /* >= 1 */
     const double* sigmaA;               /* absorption cross sections (cm^2) */
