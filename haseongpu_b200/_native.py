@@ -38,6 +38,8 @@ EXPORTED_SYMBOLS = (
     "hase_calc_phi_ase",
     "hase_context_destroy",
     "hase_context_set_local_proposal",
+    "hase_context_set_grid_proposal",
+    "hase_grid_weights",
     "hase_importance_weights",
     "hase_importance_crossings",
     "hase_ray_map",
@@ -351,6 +353,8 @@ def lib():
                                         C.POINTER(ResultDesc)]
         L.hase_context_destroy.argtypes = [C.c_void_p]
         L.hase_context_set_local_proposal.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.hase_context_set_grid_proposal.argtypes = [C.c_void_p, C.c_uint32]
+        L.hase_grid_weights.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
         L.hase_importance_weights.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
         L.hase_importance_crossings.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
         L.hase_ray_map.argtypes = [C.c_uint32, C.c_uint32, _f32p, C.c_uint32, _u32p, _u32p, _u32p, _u64p]

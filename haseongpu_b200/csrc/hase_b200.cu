@@ -1473,6 +1473,35 @@ __global__ void featureKernel(const ProposalLaunch P) {
     for (int k = 0; k < kFeat; ++k) P.features[gr * kFeat + k] = f[k];
 }
 
+// The coarse-grid proposal (hase_context_set_grid_proposal): the importance
+// function beta V R / d^2 e^G of a (slice, prism) pair with the straight-line
+// gain G taken from the coarse gain grid (the 8-point estimate of the
+// features) instead of a walk, and the slice's reflection factor R taken per
+// bounce from the pair's own direction: 1 beyond the critical angle of the
+// surface, the surface's mean reflectivity otherwise.  ln w; -inf without a
+// source.
+__device__ __forceinline__ float gridLnWeight(const ProposalView& V, uint32_t sample, uint32_t jp) {
+    float f[kFeat];
+    pairFeatures(V, sample, jp, f);
+    if (!(f[7] > 0.0f)) return -INFINITY;
+    const uint32_t j = uint32_t(fmaf(f[10], 4.0f, 0.5f));
+    float lnR = 0.0f;
+    if (j > 0) {
+        const float dx = f[3] * V.R, dy = f[4] * V.R, dz = f[5] * V.H;
+        const float uz2 = __fdividef(dz * dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        const float lb = uz2 <= V.m.tirCos2[0] ? 0.0f : V.lnRb, lt = uz2 <= V.m.tirCos2[1] ? 0.0f : V.lnRt;
+        lnR = j == 1 ? lb : (j == 2 ? lt : lb + lt);
+    }
+    return f[9] + V.lnVref + (f[8] - sliceLnReflect(V, j)) + lnR;
+}
+
+// ln w of every pair of `rows` sample rows from the coarse grid (P.out).
+__global__ void gridWeightKernel(const ProposalLaunch P) {
+    const uint64_t gr = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gr >= uint64_t(P.rows) * P.V.nW) return;
+    P.out[gr] = gridLnWeight(P.V, P.V.firstSample + uint32_t(gr / P.V.nW), uint32_t(gr % P.V.nW));
+}
+
 template <bool MAX>
 __device__ __forceinline__ float blockReduce1024(float v, float* red) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -1970,6 +1999,7 @@ struct hase_context {
     // triangles nearest to it (by centroid distance, nearest first) and the
     // same set by ascending index; the far proposal's prefix of beta V over
     // the prisms and each point's candidate share of it, per beta version
+    bool gridProposal = false;  // coarse-grid weights instead of the importance walks
     uint32_t localK = 0;
     float farFraction = 0.0f;
     DevBuf<uint32_t> candTri, candSorted, candRank;
@@ -2505,6 +2535,12 @@ hase_status hase_context_update_beta(hase_context* c, const double* betaVolume, 
 // the full proposal).
 constexpr float kDefaultFarFraction = 0.9f;
 
+hase_status hase_context_set_grid_proposal(hase_context* c, uint32_t enable) {
+    if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
+    c->gridProposal = enable != 0;
+    return HASE_OK;
+}
+
 hase_status hase_context_set_local_proposal(hase_context* c, uint32_t triangles, float farFraction) {
     if (!c) return fail(HASE_INVALID_ARGUMENT, "null context");
     if (!(farFraction >= 0.0f) || farFraction >= 1.0f) return fail(HASE_INVALID_ARGUMENT, "farFraction must be in [0, 1)");
@@ -2571,6 +2607,8 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     HASE_CUDA(cudaMemcpyAsync(c->spec.p, spec.data(), nLambda * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
     ProposalView pv{};
     uint32_t proposalGrid = 0;
+    const bool gridWeights = c->gridProposal && !la;
+    if (gridWeights) HASE_TRY(cachedProposalView(c, meanA, meanB, pv));
     if (la) {
         if (la->net->device != c->device)
             return fail(HASE_INVALID_ARGUMENT, "the proposal network and the context are on different devices");
@@ -2690,6 +2728,13 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             HASE_CUDA(cudaGetLastError());
             mixtureKernel<<<nRows, 1024, 0, c->stream>>>(nW, c->lnw.p, c->priorBuf.p, la->alpha);
             res->kernelLaunches += 1;
+        } else if (gridWeights) {
+            pv.firstSample = firstSample;
+            pv.nW = nW;
+            localFields(c, pv);
+            const ProposalLaunch gl{pv, nullptr, nullptr, c->lnw.p, nullptr, nullptr, nRows, nullptr};
+            const uint64_t pairs = uint64_t(nRows) * nW;
+            gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, c->stream>>>(gl);
         } else {
             launchImportanceRows(nRows);
         }
@@ -3367,6 +3412,43 @@ hase_status hase_importance_weights(hase_context* c, uint32_t firstSample, uint3
     ImportanceLaunch il{c->view(), firstSample, slices, nW, float(meanA), float(meanB), lnw.p};
     localFields(c, il);
     HASE_CUDA(launchImportance(0, il, c->layers, c->T, count, c->stream));
+    MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
+    mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
+    HASE_CUDA(cudaGetLastError());
+    HASE_CUDA(cudaMemcpyAsync(weights, w.p, size_t(count) * nW * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HASE_CUDA(cudaStreamSynchronize(c->stream));
+    return HASE_OK;
+}
+
+hase_status hase_grid_weights(hase_context* c, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                              uint32_t monochromatic, float* weights) {
+    if (!c || !weights || count == 0) return fail(HASE_INVALID_ARGUMENT, "bad argument");
+    if (uint64_t(firstSample) + count > uint64_t(c->Np) * c->L) return fail(HASE_INVALID_ARGUMENT, "sample range");
+    HASE_TRY(setDevice(c));
+    if (c->localK) HASE_TRY(prepareLocal(c));
+    const uint32_t slices = useReflections ? 5u : 1u, nW = rowEntries(c, slices);
+    const uint32_t nL = monochromatic ? 1u : uint32_t(c->sigmaA.size());
+    double meanA = 0, meanB = 0;
+    for (uint32_t l = 0; l < nL; ++l) {
+        meanA += c->nTot * (c->sigmaE[l] + c->sigmaA[l]) / nL;
+        meanB += c->nTot * c->sigmaA[l] / nL;
+    }
+    ProposalView pv{};
+    HASE_TRY(cachedProposalView(c, meanA, meanB, pv));
+    pv.firstSample = firstSample;
+    pv.nW = nW;
+    localFields(c, pv);
+    DevBuf<float> lnw, w;
+    DevBuf<uint32_t> q, off;
+    DevBuf<unsigned long long> Q;
+    HASE_CUDA(lnw.ensure(size_t(count) * nW));
+    HASE_CUDA(w.ensure(size_t(count) * nW));
+    HASE_CUDA(q.ensure(size_t(count) * nW));
+    HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
+    HASE_CUDA(Q.ensure(count));
+    const ProposalLaunch gl{pv, nullptr, nullptr, lnw.p, nullptr, nullptr, count, nullptr};
+    const uint64_t pairs = uint64_t(count) * nW;
+    gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, c->stream>>>(gl);
     MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
     mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
     HASE_CUDA(cudaGetLastError());

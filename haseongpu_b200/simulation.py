@@ -119,6 +119,20 @@ class DeviceMesh:
         N.check(N.lib().hase_context_set_local_proposal(self.handle, int(triangles), float(farFraction)))
         self.localTriangles = min(int(triangles), self.mesh.numberOfTriangles)
 
+    def set_grid_proposal(self, enable: bool = True):
+        """Coarse-grid proposal (hase_context_set_grid_proposal): plain solves
+        take their weights from the coarse gain grid instead of the importance
+        walks; False restores the walks."""
+        N.check(N.lib().hase_context_set_grid_proposal(self.handle, 1 if enable else 0))
+
+    def grid_weights(self, firstSample, count, useReflections=False, monochromatic=False) -> np.ndarray:
+        """The coarse-grid proposal's normalised weights (hase_grid_weights)."""
+        slices = 5 if useReflections else 1
+        w = np.empty((count, self.row_entries(slices)), np.float32)
+        N.check(N.lib().hase_grid_weights(self.handle, int(firstSample), int(count), 1 if useReflections else 0,
+                                          1 if monochromatic else 0, N.ptr(w, N._f32p)))
+        return w
+
     def row_entries(self, slices: int) -> int:
         """Entries of a sample's weight row: every (slice, prism), or the local
         proposal's (slice, layer, candidate) entries."""

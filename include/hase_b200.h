@@ -164,6 +164,20 @@ hase_status hase_context_destroy(hase_context* ctx);
  * media (hase_calc_phi_ase_batch) reject a context in local mode. */
 hase_status hase_context_set_local_proposal(hase_context* ctx, uint32_t triangles, float farFraction);
 
+/* Coarse-grid proposal (no reference counterpart; the reference walks every
+ * (sample, slice, prism) line for its importance weights).  With enable = 1
+ * the context's plain backward solves (hase_calc_phi_ase, hase_simulate)
+ * take their weights from the importance function beta V R / d^2 e^G with
+ * the straight-line gain G estimated on the coarse gain grid of the learned
+ * proposal's features (8 points along the line, reflections folded) instead
+ * of a walk, and the reflection factor R of a slice taken per bounce from the
+ * pair's own direction: 1 beyond the surface's critical angle, its mean
+ * reflectivity otherwise.  Any positive proposal leaves the estimate unbiased;
+ * this one costs a fraction of the walks.  With the local proposal set, it
+ * weights the candidate rows.  Learned solves and batched media keep their
+ * own weights.  enable = 0 restores the walks. */
+hase_status hase_context_set_grid_proposal(hase_context* ctx, uint32_t enable);
+
 /* ---- kernel-level entry points (the four hot-path kernels, one at a time) ----
  * Used by the parity tests and the benchmark; no reference counterpart beyond
  * the kernels they expose (importance weights, ray->prism map, ray walk). */
@@ -172,6 +186,13 @@ hase_status hase_context_set_local_proposal(hase_context* ctx, uint32_t triangle
  * weights[i][j*P + p] for reflection slice j (slices = 5 with reflections, else 1). */
 hase_status hase_importance_weights(hase_context* ctx, uint32_t firstSample, uint32_t count,
                                     uint32_t useReflections, float* weights);
+
+/* The coarse-grid proposal's normalised weights (max 1), laid out as those of
+ * hase_importance_weights (the local proposal's candidate rows when it is
+ * set); monochromatic: the grid of the first wavelength pair, else of the
+ * spectral mean. */
+hase_status hase_grid_weights(hase_context* ctx, uint32_t firstSample, uint32_t count, uint32_t useReflections,
+                              uint32_t monochromatic, float* weights);
 
 /* Crossings of the importance walks of samples [firstSample, firstSample +
  * count): per (sample, reflection slice, prism) line, the triangles its 2-D
