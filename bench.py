@@ -327,6 +327,15 @@ def measure_importance(args, local, rank=0, world=1, nested=False):
                              useReflections=w.useReflections, monochromatic=w.monochromatic,
                              adaptiveSteps=w.adaptiveSteps, rngSeed=1000, minSample=0, maxSample=B - 1,
                              nearFieldSampling=False, **tuned.kwargs())
+    # the coarse-grid proposal on the same batch: weights from the gain grid
+    # instead of the importance walks (hase_context_set_grid_proposal)
+    gkw = dict(minRays=w.minRays, maxRays=w.maxRays, mseThreshold=w.threshold, useReflections=w.useReflections,
+               monochromatic=w.monochromatic, adaptiveSteps=w.adaptiveSteps, minSample=0, maxSample=B - 1,
+               **tuned.kwargs())
+    ctx.set_grid_proposal(True)
+    ctx.calc_phi_ase(rngSeed=2000, **gkw)  # warm-up: the grid is built once per beta
+    grid_runs = [ctx.calc_phi_ase(rngSeed=2001 + k, **gkw) for k in range(3)]
+    ctx.set_grid_proposal(False)
     # the forward Tet4 path on the twin of the same medium (1 GPU runs only; fewer steps)
     fwd = None
     if world == 1 and not nested:
@@ -394,6 +403,14 @@ def measure_importance(args, local, rank=0, world=1, nested=False):
                              "unconverged_samples": plain.unconvergedSamples,
                              "note": "uniform start points in every prism (legacy estimator), same batch size"},
             "unconverged_samples": unconverged,
+            "grid_proposal": {
+                "time_to_threshold_ms": statistics.median(r.totalMilliseconds for r in grid_runs),
+                "weights_ms": statistics.median(r.importanceMilliseconds for r in grid_runs),
+                "ray_ms": statistics.median(r.rayMilliseconds for r in grid_runs),
+                "rays": grid_runs[-1].raysTraced, "unconverged_samples": grid_runs[-1].unconvergedSamples,
+                "speedup_vs_walks": statistics.median(steps_ms) / statistics.median(r.totalMilliseconds for r in grid_runs),
+                "note": "the same 1,024-sample batch with the coarse-grid proposal (gain-grid weights with per-bounce "
+                        "total reflection instead of the importance walks); device time of calc_phi_ase"},
             "e2e": {"value": e2e_solved_all / e2e_max, "unit": "samples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "rays_per_s": e2e_rays_all / e2e_max},
             "gpu_launches": launches,
@@ -1171,7 +1188,7 @@ def run_learned(args):
         if disc_poly is not None:
             line["importance_disc_poly"] = {k: disc_poly[k] for k in (
                 "value", "unit", "ms_per_step", "config", "time_to_threshold_ms", "breakdown_ms_per_step",
-                "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "e2e", "roofline",
+                "rays_per_s", "crossings_per_s", "plain_method", "unconverged_samples", "grid_proposal", "e2e", "roofline",
                 "importance_roofline")}
         if fwd is not None:
             line["forward_tet4"] = fwd
