@@ -1041,6 +1041,12 @@ def run_learned(args):
         ctx.update_beta(fields[k])
         if kind == "learned":
             return ctx.calc_phi_ase_learned(net, rngSeed=3000 + k, fallbackVariance=fallback, **kw)
+        if kind == "grid":  # the coarse-grid proposal: weights from the gain grid, no walks, no network
+            ctx.set_grid_proposal(True)
+            try:
+                return ctx.calc_phi_ase(rngSeed=3000 + k, **kw)
+            finally:
+                ctx.set_grid_proposal(False)
         return ctx.calc_phi_ase(rngSeed=3000 + k, nearFieldSampling=(kind == "nearfield"), **kw, **ikw)
 
     def barrier():
@@ -1051,9 +1057,9 @@ def run_learned(args):
     for k in range(args.warmup):
         solve("learned", k)
     barrier()
-    acc = {"learned": [], "plain": [], "nearfield": []}
+    acc = {"learned": [], "plain": [], "nearfield": [], "grid": []}
     with ClockSampler(local) as clk:
-        for kind in ("learned", "plain", "nearfield"):
+        for kind in ("learned", "plain", "nearfield", "grid"):
             for s_ in range(args.steps):
                 ctx.update_beta(fields[args.warmup + s_])
                 flush.zero_()
@@ -1077,15 +1083,18 @@ def run_learned(args):
 
     a = {k: agg(v) for k, v in acc.items()}
     stats = torch.tensor([a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s,
-                          float(a["learned"]["rays"]), float(args.steps * S)], dtype=torch.float64, device=dev)
+                          float(a["learned"]["rays"]), float(args.steps * S), a["grid"]["ms"]], dtype=torch.float64,
+                         device=dev)
     if world > 1:
         mx, sm = stats.clone(), stats.clone()
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
         ms_l, ms_p, ms_n, e2e_max = float(mx[0]), float(mx[1]), float(mx[2]), float(mx[3])
         rays_all, solved_all = float(sm[4]), float(sm[5])
+        ms_g = float(mx[6])
     else:
         ms_l, ms_p, ms_n, e2e_max = a["learned"]["ms"], a["plain"]["ms"], a["nearfield"]["ms"], e2e_s
+        ms_g = a["grid"]["ms"]
         rays_all, solved_all = float(a["learned"]["rays"]), float(args.steps * S)
     disc_poly = fwd = media = pulse_line = None
     if world == 1 and not args.no_nested:
@@ -1117,6 +1126,7 @@ def run_learned(args):
         lv = np.concatenate([LP.per_ray_variance(r) for r in acc["learned"]])
         pv = np.concatenate([LP.per_ray_variance(r) for r in acc["plain"]])
         nv = np.concatenate([LP.per_ray_variance(r) for r in acc["nearfield"]])
+        gv = np.concatenate([LP.per_ray_variance(r) for r in acc["grid"]])
         cpu = cpu_baseline(w, args.cpu_seconds, fields=fields[args.warmup:]) if world == 1 else None
         l1 = _native.l1_bandwidth(local)
         smem = _native.l1_bandwidth(local, shared=True)
@@ -1146,6 +1156,12 @@ def run_learned(args):
                                      "ms_per_step": ms_n / args.steps, "rays": a["nearfield"]["rays"],
                                      "unconverged_samples": a["nearfield"]["unconverged"],
                                      "median_per_ray_variance": float(np.median(nv))},
+            "grid_proposal": {"value": solved_all / (ms_g * 1e-3), "unit": "samples/s", "ms_per_step": ms_g / args.steps,
+                              "rays": a["grid"]["rays"], "unconverged_samples": a["grid"]["unconverged"],
+                              "weights_ms_per_step": a["grid"]["proposal_ms"] / args.steps,
+                              "median_per_ray_variance": float(np.median(gv)), "speedup_vs_learned": ms_l / ms_g,
+                              "note": "importance weights from the coarse gain grid (no walks, no network), "
+                                      "near-field start points; the same fields"},
             "learned": {"rays": a["learned"]["rays"], "unconverged_samples": a["learned"]["unconverged"],
                         "median_per_ray_variance": float(np.median(lv)), "max_per_ray_variance": float(lv.max()),
                         "proposal_ms_per_step": a["learned"]["proposal_ms"] / args.steps,
