@@ -4012,7 +4012,18 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
         }
         HASE_CUDA(cudaFuncSetAttribute(proposalKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
         proposalGrid = uint32_t(std::max(1, b->sms) * kMlpBlocksPerSM);
+    } else {
+        // media whose context takes the coarse-grid proposal: their views
+        pviews.resize(count);
+        for (uint32_t i = 0; i < count; ++i)
+            if (media[i].c->gridProposal) {
+                HASE_TRY(cachedProposalView(media[i].c, media[i].meanA, media[i].meanB, pviews[i]));
+                pviews[i].nW = media[i].nW;
+            }
     }
+    // the views' gain grids are built on each context's own stream: finished
+    // before the batch's stream reads them
+    for (uint32_t i = 0; i < count; ++i) HASE_CUDA(cudaStreamSynchronize(media[i].c->stream));
 
     // rows of every medium, cut into workspace chunks
     struct Chunk {
@@ -4144,6 +4155,14 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                     mixtureKernel<<<segRows, 1024, 0, b->stream>>>(md.nW, b->lnw.p + all[r].w, b->prior.p + all[r].w,
                                                                   alpha);
                     kernels += 2;
+                } else if (md.c->gridProposal) {
+                    ProposalView pv = pviews[i];
+                    pv.firstSample = all[r].sample;
+                    const ProposalLaunch gl{pv, nullptr, nullptr, b->lnw.p + all[r].w, nullptr, nullptr, segRows,
+                                            nullptr};
+                    const uint64_t pairs = uint64_t(segRows) * md.nW;
+                    gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, b->stream>>>(gl);
+                    ++kernels;
                 } else {
                     HASE_TRY(importanceSegment(r, e, nullptr));
                 }

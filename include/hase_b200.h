@@ -174,8 +174,9 @@ hase_status hase_context_set_local_proposal(hase_context* ctx, uint32_t triangle
  * pair's own direction: 1 beyond the surface's critical angle, its mean
  * reflectivity otherwise.  Any positive proposal leaves the estimate unbiased;
  * this one costs a fraction of the walks.  With the local proposal set, it
- * weights the candidate rows.  Learned solves and batched media keep their
- * own weights.  enable = 0 restores the walks. */
+ * weights the candidate rows; a batched solve without a network uses it for
+ * the media whose context has it set.  Learned solves keep the network's
+ * weights.  enable = 0 restores the walks. */
 hase_status hase_context_set_grid_proposal(hase_context* ctx, uint32_t enable);
 
 /* ---- kernel-level entry points (the four hot-path kernels, one at a time) ----

@@ -267,3 +267,26 @@ def test_learned_batch_replayed_by_the_oracle(media, oracle):
         for i, (ctx, lo, hi) in enumerate(items):
             W = ctx.learned_weights(net, lo, hi - lo + 1)
             _matches_replay(res[i], _oracle_replay(oracle, ctx, lo, hi, kw["rngSeed"] + i, W, kw))
+
+
+def test_batch_with_grid_proposal_media_equals_sequential(media):
+    """Media whose context takes the coarse-grid proposal are weighted by it
+    inside the batch (the others by the walks): every medium equals its own
+    calc_phi_ase with seed + i, bit for bit, reflections included."""
+    from haseongpu_b200 import MediaBatch
+    from haseongpu_b200.batch import solve_sequential
+
+    grid_media = media[::2] + media[-1:]
+    for c in grid_media:
+        c.set_grid_proposal(True)
+    try:
+        items = _ranges(media, n=48)
+        kw = dict(KW, useReflections=True)
+        with MediaBatch(0) as b:
+            res, st = b.solve(items, **kw)
+        seq = solve_sequential(items, **kw)
+        for r, s in zip(res, seq):
+            _same(r, s)
+    finally:
+        for c in grid_media:
+            c.set_grid_proposal(False)
