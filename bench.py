@@ -680,6 +680,14 @@ def measure_media(args, local, steps, warmup):
     with ClockSampler(local) as clk:
         lt, lst = timed(lambda seed: batch.solve(items, rngSeed=seed, net=net, fallbackVariance=fallback, **kw))
         bt, bst = timed(lambda seed: batch.solve(items, rngSeed=seed, **kw))
+        for c in ctxs:  # the coarse-grid proposal for every medium, same batched graph
+            c.set_grid_proposal(True)
+        try:
+            batch.solve(items, rngSeed=999, **kw)  # warm-up: each medium's gain grid is built once per beta
+            gt, gst = timed(lambda seed: batch.solve(items, rngSeed=seed, **kw))
+        finally:
+            for c in ctxs:
+                c.set_grid_proposal(False)
     clocks = clk.summary()
     seq_ms, wall_s, same = 0.0, 0.0, True
     for s_ in range(steps):
@@ -720,7 +728,8 @@ def measure_media(args, local, steps, warmup):
                 "unconverged": sum(st.unconvergedSamples for st in st_all),
                 "capture_ms": sum(st.captureMilliseconds for st in st_all)}
 
-    L, B = agg(lst), agg(bst)
+    L, B, G = agg(lst), agg(bst), agg(gst)
+    gv = np.concatenate([LP.per_ray_variance(r) for r in gt[-1]])
     lv = np.concatenate([LP.per_ray_variance(r) for r in lt[-1]])
     nv = np.concatenate([LP.per_ray_variance(r) for r in bt[-1]])
     peaks, peak_kind = measured_peaks()
@@ -761,6 +770,12 @@ def measure_media(args, local, steps, warmup):
                      "loss_first_50": float(hist[:50].mean()), "loss_last_200": float(hist[-200:].mean()),
                      "note": "24 media of the same generator on another seed (<= 3,000 triangles); the timed media "
                              "are unseen"},
+        "grid_batched": {"value": steps * rows / (G["ms"] * 1e-3), "unit": "samples/s", "ms_per_step": G["ms"] / steps,
+                         "weights_ms_per_step": G["imp_ms"] / steps, "rays": G["rays"],
+                         "unconverged_samples": G["unconverged"], "median_per_ray_variance": float(np.median(gv)),
+                         "speedup_vs_learned_batched": L["ms"] / G["ms"],
+                         "note": "the coarse-grid proposal for every medium (no walks, no network), near-field "
+                                 "start points, the same batched graph"},
         "importance_batched": {"value": steps * rows / (B["ms"] * 1e-3), "unit": "samples/s",
                                "ms_per_step": B["ms"] / steps, "rays": B["rays"],
                                "unconverged_samples": B["unconverged"],
@@ -1213,7 +1228,8 @@ def run_learned(args):
         if media is not None:
             line["batched_media"] = {k: media[k] for k in (
                 "value", "unit", "ms_per_step", "config", "rays_per_s", "crossings_per_s", "breakdown_ms_per_step",
-                "rays_per_sample", "unconverged_samples", "fallback", "per_ray_variance", "training", "importance_batched",
+                "rays_per_sample", "unconverged_samples", "fallback", "per_ray_variance", "training", "grid_batched",
+                "importance_batched",
                 "importance_sequential", "plain_is_sequential", "speedup_vs_plain_is_sequential",
                 "speedup_vs_importance_batched", "speedup_batched_vs_sequential", "graph", "e2e", "roofline")}
             line["learned_batched_target"] = {
