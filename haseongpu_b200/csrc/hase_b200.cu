@@ -6,8 +6,8 @@
 //        straight-line walk from the prism centre to the (image) sample point,
 //        ln w = ln(beta V / d^2) + Int g dl.
 //   (a2) mapKernel         one CTA per sample: w = exp(ln w - max), integer
-//        quantisation q = ceil(w 2^24 / max w), block-wide warp-shuffle scan of
-//        q and the systematic-sampling ray offsets
+//        quantisation q = ceil(w 2^24 / max w), warp-shuffle scans of q over
+//        one contiguous segment per warp and the systematic-sampling ray offsets
 //        offsets[b] = floor((C_b M + floor(phase Q / 2^32)) / Q).
 //   (b)  rayKernel         CTAs over (ray chunk, active sample): Philox4x32-10
 //        start points, prism walk (neighbour + level crossings, top/bottom
@@ -87,31 +87,15 @@ __device__ __forceinline__ float warpMax(float v) {
     return v;
 }
 
-// Block-wide inclusive scan of 64-bit values (warp shuffles + one shared pass).
-template <int BLOCK>
-__device__ __forceinline__ unsigned long long blockInclusiveScan(unsigned long long v, unsigned long long* warpTot,
-                                                                 unsigned long long& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Warp-wide inclusive scan.
+template <typename T>
+__device__ __forceinline__ T warpInclusiveScan(T v) {
+    const uint32_t lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long n = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += n;
+        const T n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= uint32_t(o)) v += n;
     }
-    if (lane == 31) warpTot[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        unsigned long long t = lane < BLOCK / 32 ? warpTot[lane] : 0ull;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long n = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += n;
-        }
-        if (lane < BLOCK / 32) warpTot[lane] = t;
-    }
-    __syncthreads();
-    if (warp > 0) v += warpTot[warp - 1];
-    total = warpTot[BLOCK / 32 - 1];
-    __syncthreads();
     return v;
 }
 
@@ -521,11 +505,19 @@ struct MapLaunch {
     const uint8_t* rowFlag;     // batched media: only rows with rowFlag[row] set are mapped (or null)
 };
 
+// Each warp owns one contiguous segment of the row (a multiple of 32 entries
+// long, the last one cut at nW): the passes read and write it coalesced, four
+// loads in flight per lane, and the offsets' prefix sums need one block-wide
+// step (the warps' exclusive prefixes) instead of a block scan per 1,024
+// entries.  q, Q and the offsets are integers, so they do not depend on the
+// order of the sums.
 __device__ void mapRow(const MapLaunch& L, uint32_t row) {
-    __shared__ unsigned long long sWarp[kMapBlock / 32];
+    constexpr uint32_t kWarps = kMapBlock / 32;
+    static_assert(kWarps == 32, "one warp prefix per lane");
+    __shared__ unsigned long long sWarp[kWarps];  // q sum of each warp's segment, then its exclusive prefix
     __shared__ float sMax;
     __shared__ unsigned long long sQ;
-    __shared__ float sRed[kMapBlock / 32];
+    __shared__ float sRed[kWarps];
     uint32_t nW = L.nW, sample = L.firstSample + row, seedLo = L.seedLo;
     size_t wBase = size_t(row) * nW, oBase = size_t(row) * (nW + 1);
     if (L.rows) {
@@ -539,17 +531,23 @@ __device__ void mapRow(const MapLaunch& L, uint32_t row) {
     const float* in = L.in + wBase;
     uint32_t* q = L.q + wBase;
     uint32_t* off = L.offsets + oBase;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long Q;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t segLen = ((nW + kWarps - 1) / kWarps + 31u) & ~31u;
+    const uint32_t s0 = min(nW, warp * segLen), s1 = min(nW, s0 + segLen);
+    unsigned long long part = 0;
     if (L.full) {
         float mx = -INFINITY;
-        for (uint32_t b = threadIdx.x; b < nW; b += kMapBlock) mx = fmaxf(mx, in[b]);
+        {
+            uint32_t b = s0 + lane;
+            for (; b + 96 < s1; b += 128)
+                mx = fmaxf(fmaxf(mx, fmaxf(in[b], in[b + 32])), fmaxf(in[b + 64], in[b + 96]));
+            for (; b < s1; b += 32) mx = fmaxf(mx, in[b]);
+        }
         mx = warpMax(mx);
         if (lane == 0) sRed[warp] = mx;
         __syncthreads();
         if (warp == 0) {
-            float v = lane < kMapBlock / 32 ? sRed[lane] : -INFINITY;
-            v = warpMax(v);
+            const float v = warpMax(sRed[lane]);
             if (lane == 0) sMax = v;
         }
         __syncthreads();
@@ -557,31 +555,41 @@ __device__ void mapRow(const MapLaunch& L, uint32_t row) {
         // Normalised weights: exp(ln w - max) has maximum exactly 1.
         const float wmax = L.isLog ? (mx == -INFINITY ? 0.0f : 1.0f) : mx;
         const double scale = wmax > 0.0f ? 16777216.0 / double(wmax) : 0.0;
-        unsigned long long part = 0;
-        for (uint32_t b = threadIdx.x; b < nW; b += kMapBlock) {
-            const float v = in[b];
+        const auto quantise = [&](uint32_t b, float v) {
             const float w = L.isLog ? (v == -INFINITY || wmax == 0.0f ? 0.0f : expf(v - mx)) : v;
             const uint32_t qi = (w > 0.0f && wmax > 0.0f) ? uint32_t(ceil(double(w) * scale)) : 0u;
             q[b] = qi;
             if (L.wOut) L.wOut[wBase + b] = w;
             part += qi;
+        };
+        uint32_t b = s0 + lane;
+        for (; b + 96 < s1; b += 128) {
+            const float v0 = in[b], v1 = in[b + 32], v2 = in[b + 64], v3 = in[b + 96];
+            quantise(b, v0);
+            quantise(b + 32, v1);
+            quantise(b + 64, v2);
+            quantise(b + 96, v3);
         }
-        part = warpSum(part);
-        if (lane == 0) sWarp[warp] = part;
-        __syncthreads();
-        if (warp == 0) {
-            unsigned long long v = lane < kMapBlock / 32 ? sWarp[lane] : 0ull;
-            v = warpSum(v);
-            if (lane == 0) {
-                sQ = v;
-                L.Q[row] = v;
-            }
-        }
-        __syncthreads();
-        Q = sQ;
+        for (; b < s1; b += 32) quantise(b, in[b]);
     } else {
-        Q = L.Q[row];
+        uint32_t b = s0 + lane;
+        for (; b + 96 < s1; b += 128) part += (unsigned long long)(q[b] + q[b + 32]) + q[b + 64] + q[b + 96];
+        for (; b < s1; b += 32) part += q[b];
     }
+    part = warpSum(part);
+    if (lane == 0) sWarp[warp] = part;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned long long v = sWarp[lane];
+        const unsigned long long incl = warpInclusiveScan(v);
+        sWarp[lane] = incl - v;
+        if (lane == 31) {
+            sQ = incl;
+            if (L.full) L.Q[row] = incl;
+        }
+    }
+    __syncthreads();
+    const unsigned long long Q = L.full ? sQ : L.Q[row];
     const uint32_t M = L.M;
     if (Q == 0) {
         for (uint32_t b = threadIdx.x; b <= nW; b += kMapBlock) off[b] = 0u;
@@ -595,24 +603,41 @@ __device__ void mapRow(const MapLaunch& L, uint32_t row) {
     }
     using u128 = unsigned __int128;
     const unsigned long long phiQ = (unsigned long long)((u128(phase) * Q) >> 32);
-    unsigned long long carry = 0;
-    for (uint32_t base = 0; base < nW; base += kMapBlock) {
-        const uint32_t b = base + threadIdx.x;
-        const unsigned long long v = b < nW ? q[b] : 0u;
-        unsigned long long total;
-        const unsigned long long incl = blockInclusiveScan<kMapBlock>(v, sWarp, total);
-        if (b < nW) {
-            const unsigned long long C = carry + incl - v;
-            off[b] = uint32_t((u128(C) * M + phiQ) / Q);
+    // floor(x / Q), x = C M + phiQ, without a 128-bit division: the FP64
+    // quotient carries a relative error of a few 2^-53, and the true quotient
+    // is at most M < 2^32, so the truncated estimate k is off by at most one.
+    // Then x - k Q lies in [-Q, 2Q) with Q < 2^56 (q <= 2^24 + 1, nW < 2^31),
+    // so its low 64 bits, from wrapping 64-bit products, decide the correction.
+    const double invQ = 1.0 / double(Q);
+    unsigned long long carry = sWarp[warp];
+    const auto offsetOf = [&](uint32_t b, uint32_t v) {
+        const uint32_t incl = warpInclusiveScan(v);  // q <= 2^24 + 1: 32 of them fit 32 bits
+        if (b < s1) {
+            const unsigned long long C = carry + (incl - v);
+            unsigned long long k = (unsigned long long)(fma(double(C), double(M), double(phiQ)) * invQ);
+            const long long r = (long long)(C * M + phiQ - k * Q);
+            if (r < 0) --k;
+            else if (r >= (long long)Q) ++k;
+            off[b] = uint32_t(k);
         }
-        carry += total;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    };
+    // warp-uniform trip counts: every lane takes part in the scans
+    for (uint32_t base = s0; base < s1; base += 128) {
+        const uint32_t b = base + lane;
+        const uint32_t v0 = b < s1 ? q[b] : 0u, v1 = b + 32 < s1 ? q[b + 32] : 0u;
+        const uint32_t v2 = b + 64 < s1 ? q[b + 64] : 0u, v3 = b + 96 < s1 ? q[b + 96] : 0u;
+        offsetOf(b, v0);
+        offsetOf(b + 32, v1);
+        offsetOf(b + 64, v2);
+        offsetOf(b + 96, v3);
     }
     if (threadIdx.x == 0) off[nW] = M;
 }
 
 // One CTA per row (grid = rows), or, with L.count, CTAs striding over the
 // device-held number of rows.
-__global__ void __launch_bounds__(kMapBlock) mapKernel(MapLaunch L) {
+__global__ void __launch_bounds__(kMapBlock, 2) mapKernel(MapLaunch L) {
     const uint32_t n = L.count ? *L.count : gridDim.x;
     for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
         const uint32_t row = L.rowList ? L.rowList[i] : i;
@@ -1476,30 +1501,116 @@ __global__ void featureKernel(const ProposalLaunch P) {
 // The coarse-grid proposal (hase_context_set_grid_proposal): the importance
 // function beta V R / d^2 e^G of a (slice, prism) pair with the straight-line
 // gain G taken from the coarse gain grid (the 8-point estimate of the
-// features) instead of a walk, and the slice's reflection factor R taken per
-// bounce from the pair's own direction: 1 beyond the critical angle of the
-// surface, the surface's mean reflectivity otherwise.  ln w; -inf without a
-// source.
-__device__ __forceinline__ float gridLnWeight(const ProposalView& V, uint32_t sample, uint32_t jp) {
-    float f[kFeat];
-    pairFeatures(V, sample, jp, f);
-    if (!(f[7] > 0.0f)) return -INFINITY;
-    const uint32_t j = uint32_t(fmaf(f[10], 4.0f, 0.5f));
-    float lnR = 0.0f;
-    if (j > 0) {
-        const float dx = f[3] * V.R, dy = f[4] * V.R, dz = f[5] * V.H;
-        const float uz2 = __fdividef(dz * dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-        const float lb = uz2 <= V.m.tirCos2[0] ? 0.0f : V.lnRb, lt = uz2 <= V.m.tirCos2[1] ? 0.0f : V.lnRt;
-        lnR = j == 1 ? lb : (j == 2 ? lt : lb + lt);
-    }
-    return f[9] + V.lnVref + (f[8] - sliceLnReflect(V, j)) + lnR;
+// features, pairFeatures) instead of a walk, and the slice's reflection
+// factor R taken per bounce from the pair's own direction: 1 beyond the
+// critical angle of the surface, the surface's mean reflectivity otherwise.
+// ln w; -inf without a source.
+//
+// Only what the weight uses is computed.  A thread takes one column (prism,
+// or candidate entry l K + k) of a sample row and every reflection slice of
+// it: the sample point, the prism's centroid, beta V and the in-plane cells
+// of the 8 gain points do not depend on the slice, so they are found once;
+// per slice only the folded height of the 8 points, d^2 and the bounce
+// factor remain.  Rows come from the grid's y dimension (no 64-bit division
+// per pair).
+
+// floor(v) of 0 <= v < 2^22 as an integer, on the FP32 pipe: adding 1.5 2^23
+// rounded toward -inf leaves floor(v) in the low mantissa bits.
+__device__ __forceinline__ int floorSmall(float v) {
+    return __float_as_int(__fadd_rd(v, 12582912.0f)) - 0x4B400000;
+}
+
+// min(max(int(v), 0), hi) for finite v (the cell index of pairFeatures).
+__device__ __forceinline__ int clampedCell(float v, int hi) {
+    return floorSmall(fminf(fmaxf(v, 0.0f), float(hi)));
 }
 
 // ln w of every pair of `rows` sample rows from the coarse grid (P.out).
-__global__ void gridWeightKernel(const ProposalLaunch P) {
-    const uint64_t gr = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (gr >= uint64_t(P.rows) * P.V.nW) return;
-    P.out[gr] = gridLnWeight(P.V, P.V.firstSample + uint32_t(gr / P.V.nW), uint32_t(gr % P.V.nW));
+// Launch: x covers the columns of one slice (P.V.cand ? layers K : P),
+// y the rows (strided past 65535).
+__global__ void __launch_bounds__(256) gridWeightKernel(const ProposalLaunch P) {
+    const ProposalView& V = P.V;
+    const MeshView& m = V.m;
+    const uint32_t width = V.cand ? m.layers * V.K : m.P;
+    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= width) return;
+    const uint32_t slices = V.nW / width;
+    // the column's layer and its triangle (full rows) or candidate rank
+    uint32_t l, k;
+    if (V.cand) {
+        l = uint32_t((uint64_t(col) * V.divKm) >> V.divKs);
+        k = col - l * V.K;
+    } else {
+        l = prismLayer(m, col);
+        k = col - l * m.T;
+    }
+    const float zc = (float(l) + 0.5f) * m.h;
+    const float twoH = 2.0f * V.H;
+    const uint32_t gxy = V.gx * V.gy;
+    for (uint32_t row = blockIdx.y; row < P.rows; row += gridDim.y) {
+        const uint32_t sample = V.firstSample + row;
+        const uint32_t lsU = sampleLevel(m, sample);
+        const uint32_t pt = sample - lsU * m.Np;
+        const uint32_t t = V.cand ? __ldg(V.cand + size_t(pt) * V.K + k) : k;
+        const uint32_t p = t + l * m.T;
+        float* out = P.out + size_t(row) * V.nW + col;
+        const float beta = __ldg(m.srcBeta + p);
+        if (!(beta > 0.0f)) {
+            for (uint32_t j = 0; j < slices; ++j) out[size_t(j) * width] = -INFINITY;
+            continue;
+        }
+        const float2 S = __ldg(m.points + pt);
+        const float2 c = __ldg(m.centroid + t);
+        const float dx = c.x - S.x, dy = c.y - S.y;
+        const float r2 = dx * dx + dy * dy;
+        const float lnBV = __logf(beta * (__ldg(m.geo + 2 * t + 1).z * m.h));
+        // in-plane cell of each gain point: the same for every slice
+        uint32_t cellXY[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float a = (float(q) + 0.5f) * 0.125f;
+            const float x = S.x + a * dx, y = S.y + a * dy;
+            const int ix = clampedCell((x - V.x0) * V.invCell, int(V.gx) - 1);
+            const int iy = clampedCell((y - V.y0) * V.invCell, int(V.gy) - 1);
+            cellXY[q] = uint32_t(iy) * V.gx + uint32_t(ix);
+        }
+        const int ls = int(lsU);
+        for (uint32_t j = 0; j < slices; ++j) {
+            const float zi = float(imageLevel(ls, int(m.layers), j)) * m.h;
+            const float dz = zc - zi;
+            const float d2 = fmaf(dz, dz, r2);
+            float lng = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float a = (float(q) + 0.5f) * 0.125f;
+                // fold the unfolded height into [0, H]: period 2H, mirrored halves
+                float z = zi + a * dz;
+                const float fl = __fadd_rd(z * V.invTwoH, 12582912.0f) - 12582912.0f;  // floor, |.| < 2^22
+                z -= twoH * fl;
+                if (z > V.H) z = twoH - z;
+                const uint32_t ly = uint32_t(clampedCell(z * V.invh, int(m.layers) - 1));
+                lng += __ldg(V.grid + ly * gxy + cellXY[q]);
+            }
+            float lnR = 0.0f;
+            if (j > 0) {
+                const float dz2 = dz * dz;
+                const float lb = dz2 <= m.tirCos2[0] * d2 ? 0.0f : V.lnRb;
+                const float lt = dz2 <= m.tirCos2[1] * d2 ? 0.0f : V.lnRt;
+                lnR = j == 1 ? lb : (j == 2 ? lt : lb + lt);
+            }
+            const float d = d2 * rsqrtf(d2);
+            out[size_t(j) * width] = fmaf(lng * 0.125f, d, lnBV - __logf(d2) + lnR);
+        }
+    }
+}
+
+// Launches gridWeightKernel over `gl.rows` rows of gl.V.nW pairs.
+static cudaError_t launchGridWeights(const ProposalLaunch& gl, cudaStream_t s) {
+    const uint32_t width = gl.V.cand ? gl.V.m.layers * gl.V.K : gl.V.m.P;
+    if (width == 0 || gl.rows == 0) return cudaSuccess;
+    const dim3 grid((width + 255) / 256, std::min<uint32_t>(gl.rows, 65535u));
+    gridWeightKernel<<<grid, 256, 0, s>>>(gl);
+    return cudaGetLastError();
 }
 
 template <bool MAX>
@@ -2733,8 +2844,7 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
             pv.nW = nW;
             localFields(c, pv);
             const ProposalLaunch gl{pv, nullptr, nullptr, c->lnw.p, nullptr, nullptr, nRows, nullptr};
-            const uint64_t pairs = uint64_t(nRows) * nW;
-            gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, c->stream>>>(gl);
+            HASE_CUDA(launchGridWeights(gl, c->stream));
         } else {
             launchImportanceRows(nRows);
         }
@@ -3447,8 +3557,7 @@ hase_status hase_grid_weights(hase_context* c, uint32_t firstSample, uint32_t co
     HASE_CUDA(off.ensure(size_t(count) * (nW + 1)));
     HASE_CUDA(Q.ensure(count));
     const ProposalLaunch gl{pv, nullptr, nullptr, lnw.p, nullptr, nullptr, count, nullptr};
-    const uint64_t pairs = uint64_t(count) * nW;
-    gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, c->stream>>>(gl);
+    HASE_CUDA(launchGridWeights(gl, c->stream));
     MapLaunch ml{lnw.p, 1, 1, nullptr, nW, 1u, nullptr, firstSample, 0u, 0u, 0u, w.p, q.p, Q.p, off.p};
     mapKernel<<<count, kMapBlock, 0, c->stream>>>(ml);
     HASE_CUDA(cudaGetLastError());
@@ -4160,8 +4269,7 @@ hase_status batchCore(hase_batch* b, const hase_batch_instance* in, uint32_t cou
                     pv.firstSample = all[r].sample;
                     const ProposalLaunch gl{pv, nullptr, nullptr, b->lnw.p + all[r].w, nullptr, nullptr, segRows,
                                             nullptr};
-                    const uint64_t pairs = uint64_t(segRows) * md.nW;
-                    gridWeightKernel<<<uint32_t((pairs + 255) / 256), 256, 0, b->stream>>>(gl);
+                    HASE_CUDA(launchGridWeights(gl, b->stream));
                     ++kernels;
                 } else {
                     HASE_TRY(importanceSegment(r, e, nullptr));
