@@ -651,15 +651,24 @@ __global__ void __launch_bounds__(kMapBlock, 2) mapKernel(MapLaunch L) {
 // The far prior of the local proposal: R_j beta V e^Ghat / d^2 over all
 // (slice j, prism) pairs, with d a softened distance from the image of the
 // sample point in slice j to the prism's cell of a 2-D grid of triangle
-// cells at the prism's layer, R_j a reflectivity factor of the slice (1 for
-// the direct slice), and Ghat = d (g_cl + g_s) / 2 a two-point estimate of
+// cells at the prism's layer, R_j the slice's reflection factor (1 for the
+// direct slice; per bounce, 1 where the line from the cell meets the surface
+// beyond its critical angle, else the surface's mean reflectivity), and Ghat = d (g_cl + g_s + 6 g_mid) / 8 an estimate of
 // the gain along the way (g_cl: mean g of the cell's prisms of the layer,
-// g_s: g of the prism next to the sample point; clamped to [-10, 30]).
+// g_s: g of the prism next to the sample point, g_mid: mean over 6 interior
+// points of the 2-D segment from the sample point to the cell of the
+// layer-averaged coarse gain grid, one value per (row, cell) kept in gMid;
+// clamped to [-10, 30]).
 // Drawn in three steps: a (cell, slice) pair from the row's prefix of w_cj
 // = sum_l term_clj, a layer by a scan of the same terms, a triangle of the
 // cell from the cell's beta V prefix of that layer.  p_far(j, t, l) =
 // term_clj(beta V) / W, W = sum_cj w_cj, the same expression wherever it is
 // evaluated.
+struct FarSlices {
+    float R[2];    // per surface (bottom, top): mean reflectivity, at least 1/4
+    float tir[2];  // per surface: total internal reflection when uz^2 <= tir (0: none)
+};
+
 struct FarView {
     const uint32_t* cellOf;     // [T] cell of each triangle
     const uint32_t* cellStart;  // [C + 1] cell segments of cellTris
@@ -669,8 +678,9 @@ struct FarView {
     const float* triPrefix;     // [layers][T] in cellTris order: inclusive beta V prefix within the cell
     const float* gCell;         // [C][layers] mean g of the cell's prisms of each layer (this solve)
     const double* rowCdf;       // [rows][C][slices] inclusive prefix of the row's (cell, slice) weights
+    const float* gMid;          // [rows][C] g_mid of the row's sample point and each cell
     uint32_t C, slices;
-    float prior[5];             // R_j
+    FarSlices refl;
 };
 
 __device__ __forceinline__ float farDistance2(float4 cell, float2 S, int l, int kImg, float h) {
@@ -678,10 +688,25 @@ __device__ __forceinline__ float farDistance2(float4 cell, float2 S, int l, int 
     return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, cell.z)));
 }
 
-// One term of the far prior: R_j m e^Ghat / d^2, gsum = g_cl + g_s.
-__device__ __forceinline__ float farTerm(float prior, float mass, float d2, float gsum) {
-    const float G = fminf(fmaxf(0.5f * gsum * sqrtf(d2), -10.0f), 30.0f);
+// R_j of a term of slice j whose cell lies dl + 1/2 layers above the image
+// level (d2: its squared distance; uz^2 = dz^2 / d2).
+__device__ __forceinline__ float farSliceFactor(const FarSlices& S, uint32_t j, int dl, float h, float d2) {
+    if (j == 0) return 1.0f;
+    const float dz = (float(dl) + 0.5f) * h, dz2 = dz * dz;
+    const float rb = dz2 <= S.tir[0] * d2 ? 1.0f : S.R[0];
+    const float rt = dz2 <= S.tir[1] * d2 ? 1.0f : S.R[1];
+    return j == 1 ? rb : (j == 2 ? rt : rb * rt);
+}
+
+// One term of the far prior: R_j m e^Ghat / d^2, Ghat = gmean d.
+__device__ __forceinline__ float farTerm(float prior, float mass, float d2, float gmean) {
+    const float G = fminf(fmaxf(gmean * sqrtf(d2), -10.0f), 30.0f);
     return __fdividef(prior * mass * __expf(G), d2);
+}
+
+// The far prior's mean g along the way, (g_cl + g_s + 6 g_mid) / 8.
+__device__ __forceinline__ float farMeanGain(float gcl, float gs, float gmid) {
+    return fmaf(0.75f, gmid, 0.125f * (gcl + gs));
 }
 
 // g_s of a sample row: g of the point's nearest candidate triangle at the
@@ -835,15 +860,17 @@ __device__ __forceinline__ bool localSource(const RayLaunch& L, const MeshView& 
         const float4 cl = __ldg(F.cell + cellIdx);
         const float wc = float(__ldg(cdf + lo) - (lo ? __ldg(cdf + lo - 1) : 0.0));
         const float target2 = unit24(a.z >> 8) * wc;
-        const float prior = F.prior[j];
         const float* mass = F.cellMass + size_t(cellIdx) * m.layers;
         const float* gc = F.gCell + size_t(cellIdx) * m.layers;
+        const float gmid = __ldg(F.gMid + size_t(row) * F.C + cellIdx);
         float acc = 0.0f;  // the layer terms of farRowKernel, in its order
         l = 0xffffffffu;
         for (uint32_t l2 = 0; l2 < m.layers; ++l2) {
             const float mcl = __ldg(mass + l2);
             if (!(mcl > 0.0f)) continue;
-            acc += farTerm(prior, mcl, farDistance2(cl, S, int(l2), kImg, m.h), __ldg(gc + l2) + gs);
+            const float d2 = farDistance2(cl, S, int(l2), kImg, m.h);
+            acc += farTerm(farSliceFactor(F.refl, j, int(l2) - kImg, m.h, d2), mcl, d2,
+                           farMeanGain(__ldg(gc + l2), gs, gmid));
             l = l2;
             if (acc > target2) break;
         }
@@ -875,9 +902,11 @@ __device__ __forceinline__ bool localSource(const RayLaunch& L, const MeshView& 
         const float bv = __ldg(m.srcBeta + p) * __ldg(&m.geo[2 * t + 1].z) * m.h;
         const uint32_t nE = F.C * F.slices;
         const float W = float(__ldg(F.rowCdf + size_t(row) * nE + nE - 1));
-        pf = farTerm(F.prior[j], bv,
-                     farDistance2(__ldg(F.cell + cellIdx), S, int(l), imageLevel(ls, int(m.layers), j), m.h),
-                     __ldg(F.gCell + size_t(cellIdx) * m.layers + l) + gs) /
+        const int kImg = imageLevel(ls, int(m.layers), j);
+        const float d2 = farDistance2(__ldg(F.cell + cellIdx), S, int(l), kImg, m.h);
+        pf = farTerm(farSliceFactor(F.refl, j, int(l) - kImg, m.h, d2), bv, d2,
+                     farMeanGain(__ldg(F.gCell + size_t(cellIdx) * m.layers + l), gs,
+                                 __ldg(F.gMid + size_t(row) * F.C + cellIdx))) /
              W;
     }
     const float qb = b != 0xffffffffu ? float(__ldg(q + b)) : 0.0f;
@@ -1922,9 +1951,38 @@ struct FarRowLaunch {
     uint32_t C, slices, layers, Np, firstSample, K, T;
     const float2* points;
     float h;
-    float prior[5];
+    FarSlices refl;
     double* rowCdf;  // [rows][C][slices]
+    float* gMid;     // [rows][C]
+    // the layer-averaged coarse gain grid ([gy][gx], origin, 1 / cell size)
+    const float* colGrid;
+    uint32_t gx, gy;
+    float x0, y0, invCell;
 };
+
+// The layer average of the coarse gain grid: one thread per (x, y) cell.
+__global__ void farColumnKernel(const float* grid, uint32_t cells, uint32_t layers, float* colGrid) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cells) return;
+    float sum = 0.0f;
+    for (uint32_t l = 0; l < layers; ++l) sum += grid[size_t(l) * cells + k];
+    colGrid[k] = sum / float(layers);
+}
+
+// g_mid: the mean of the layer-averaged gain grid at the points a = 1/7 ..
+// 6/7 of the 2-D segment from the sample point S to the cell centre.
+__device__ __forceinline__ float farMidGain(const FarRowLaunch& L, float2 S, float cx, float cy) {
+    const float dx = cx - S.x, dy = cy - S.y;
+    float sum = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= 6; ++k) {
+        const float a = float(k) * (1.0f / 7.0f);
+        const int ix = clampedCell((S.x + a * dx - L.x0) * L.invCell, int(L.gx) - 1);
+        const int iy = clampedCell((S.y + a * dy - L.y0) * L.invCell, int(L.gy) - 1);
+        sum += __ldg(L.colGrid + uint32_t(iy) * L.gx + uint32_t(ix));
+    }
+    return sum * (1.0f / 6.0f);
+}
 
 // The far prior's mean g of every (cell, layer) for this solve's gain table.
 __global__ void farGainKernel(const uint32_t* cellStart, const uint32_t* cellTris, uint32_t C, const float* gTab,
@@ -1957,14 +2015,16 @@ __global__ void __launch_bounds__(256) farRowKernel(FarRowLaunch L) {
         if (e < nE) {
             const uint32_t c = e / L.slices, j = e - c * L.slices;
             const int kImg = imageLevel(ls, int(L.layers), j);
-            const float prior = L.prior[j];
             const float4 cl = L.cell[c];
             const float* mass = L.cellMass + size_t(c) * L.layers;
             const float* gc = L.gCell + size_t(c) * L.layers;
+            const float gmid = farMidGain(L, S, cl.x, cl.y);
+            if (j == 0) L.gMid[size_t(row) * L.C + c] = gmid;
             for (uint32_t l = 0; l < L.layers; ++l) {
                 const float mcl = mass[l];
                 if (!(mcl > 0.0f)) continue;
-                w += farTerm(prior, mcl, farDistance2(cl, S, int(l), kImg, L.h), gc[l] + gs);
+                const float d2 = farDistance2(cl, S, int(l), kImg, L.h);
+                w += farTerm(farSliceFactor(L.refl, j, int(l) - kImg, L.h, d2), mcl, d2, farMeanGain(gc[l], gs, gmid));
             }
         }
         double x = double(w);
@@ -2119,7 +2179,7 @@ struct hase_context {
     uint32_t farCells = 0;
     DevBuf<uint32_t> cellOf, cellStart, cellTris;
     DevBuf<float4> cellXY;
-    DevBuf<float> cellMass, triPrefix, gCell;
+    DevBuf<float> cellMass, triPrefix, gCell, farMid, farColGrid;
     DevBuf<double> farRow;
     uint64_t farVersion = 0;
     DevBuf<float2> centroid, points, spec;
@@ -2266,19 +2326,17 @@ hase_status prepareLocal(hase_context* c) {
     return HASE_OK;
 }
 
-// The far prior's slice factors R_j: 1 for the direct slice; for a bounce
-// slice the product over its bounces of 1 at a surface with total internal
-// reflection (far rays are grazing: they reflect totally), else the
-// surface's mean reflectivity, at least 1/4.
-void farSlicePrior(const hase_context* c, uint32_t slices, float prior[5]) {
+// The far prior's surface factors: each surface's mean reflectivity (at
+// least 1/4) and its total-internal-reflection bound on uz^2.
+void farSlicePrior(const hase_context* c, FarSlices& f) {
     double R[2] = {0.0, 0.0};
     if (c->hasReflect && !c->hReflect.empty())
         for (uint32_t t = 0; t < c->T; ++t)
             for (int s = 0; s < 2; ++s) R[s] += double(c->hReflect[2 * t + s]) / double(c->T);
-    for (int s = 0; s < 2; ++s) R[s] = c->tirCos2[s] > 0.0f ? 1.0 : std::max(R[s], 0.25);
-    const double Rb = R[0], Rt = R[1];
-    const double v[5] = {1.0, Rb, Rt, Rb * Rt, Rt * Rb};
-    for (uint32_t j = 0; j < 5; ++j) prior[j] = j < slices ? float(v[j]) : 0.0f;
+    for (int s = 0; s < 2; ++s) {
+        f.R[s] = float(std::max(R[s], 0.25));
+        f.tir[s] = c->tirCos2[s];
+    }
 }
 
 // The far prior's view of a context for a solve of `slices` reflection
@@ -2286,7 +2344,7 @@ void farSlicePrior(const hase_context* c, uint32_t slices, float prior[5]) {
 FarView farView(const hase_context* c, uint32_t slices) {
     FarView f{};
     f.slices = slices;
-    farSlicePrior(c, slices, f.prior);
+    farSlicePrior(c, f.refl);
     f.cellOf = c->cellOf.p;
     f.cellStart = c->cellStart.p;
     f.cellTris = c->cellTris.p;
@@ -2295,6 +2353,7 @@ FarView farView(const hase_context* c, uint32_t slices) {
     f.triPrefix = c->triPrefix.p;
     f.gCell = c->gCell.p;
     f.rowCdf = c->farRow.p;
+    f.gMid = c->farMid.p;
     f.C = c->farCells;
     return f;
 }
@@ -2734,13 +2793,16 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     // batch rows by the workspace budget
     const uint64_t budget = cp->workspaceBytes ? cp->workspaceBytes : (uint64_t(4) << 30);
     const bool farPrior = local && K < c->T;
-    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxItems * 28ull + 64 + (farPrior ? uint64_t(c->farCells) * slices * 8ull : 0ull);
+    const uint64_t perRow = uint64_t(nW) * 12 + 16 + kMaxItems * 28ull + 64 + (farPrior ? uint64_t(c->farCells) * (slices * 8ull + 4ull) : 0ull);
     uint32_t rows = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nS, budget / perRow)));
     HASE_CUDA(c->lnw.ensure(size_t(rows) * nW));
     HASE_CUDA(c->q.ensure(size_t(rows) * nW));
     HASE_CUDA(c->offsets.ensure(size_t(rows) * (nW + 1)));
     HASE_CUDA(c->Q.ensure(rows));
-    if (farPrior) HASE_CUDA(c->farRow.ensure(size_t(rows) * c->farCells * slices));
+    if (farPrior) {
+        HASE_CUDA(c->farRow.ensure(size_t(rows) * c->farCells * slices));
+        HASE_CUDA(c->farMid.ensure(size_t(rows) * c->farCells));
+    }
     HASE_CUDA(c->activeA.ensure(rows));
     HASE_CUDA(c->activeB.ensure(rows));
     HASE_CUDA(c->counter.ensure(1));
@@ -2796,10 +2858,16 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     gainTableKernel<<<(c->P + 255) / 256, 256, 0, c->stream>>>(c->gainBeta.p, float(meanA), float(meanB),
                                                                float(c->cladAbs), c->P, c->gTab.p);
     HASE_CUDA(cudaGetLastError());
-    if (farPrior) {  // the far prior's cell gains for this solve's g
+    ProposalView fpv{};
+    if (farPrior) {  // the far prior's cell gains for this solve's g, and the layer-averaged coarse gain grid
         const uint32_t n = c->farCells * c->layers;
         farGainKernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->cellStart.p, c->cellTris.p, c->farCells, c->gTab.p, c->T,
                                                               c->layers, c->gCell.p);
+        HASE_CUDA(cudaGetLastError());
+        HASE_TRY(cachedProposalView(c, meanA, meanB, fpv));
+        const uint32_t cells = fpv.gx * fpv.gy;
+        HASE_CUDA(c->farColGrid.ensure(cells));
+        farColumnKernel<<<(cells + 255) / 256, 256, 0, c->stream>>>(fpv.grid, cells, c->layers, c->farColGrid.p);
         HASE_CUDA(cudaGetLastError());
     }
     const MeshView mv = c->view();
@@ -2815,7 +2883,7 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
     res->totalMilliseconds = 0;
     res->passes = 0;
     res->unconvergedSamples = 0;
-    res->kernelLaunches = farPrior ? 2 : 1;  // the gain table (and the far prior's cell gains)
+    res->kernelLaunches = farPrior ? 3 : 1;  // the gain table (and the far prior's cell gains and gain grid)
     uint64_t droppedTotal = 0;
 
     for (uint32_t b0 = 0; b0 < nS; b0 += rows) {
@@ -2851,7 +2919,14 @@ static hase_status calcCore(hase_context* c, const hase_experiment_desc* ex, con
         if (farPrior) {  // the far prior's cell prefixes of the chunk's rows
             FarRowLaunch fl{c->cellXY.p, c->cellMass.p, c->gCell.p, c->gTab.p, c->candTri.p, c->farCells, slices,
                             c->layers, c->Np, firstSample, K, c->T, c->points.p, float(c->h), {}, c->farRow.p};
-            farSlicePrior(c, slices, fl.prior);
+            fl.gMid = c->farMid.p;
+            fl.colGrid = c->farColGrid.p;
+            fl.gx = fpv.gx;
+            fl.gy = fpv.gy;
+            fl.x0 = fpv.x0;
+            fl.y0 = fpv.y0;
+            fl.invCell = fpv.invCell;
+            farSlicePrior(c, fl.refl);
             farRowKernel<<<nRows, 256, 0, c->stream>>>(fl);
             res->kernelLaunches += 1;
         }
