@@ -168,7 +168,6 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     }
     GlobalLoader load{m.tri};
     uint32_t tk = t;
-    int forb = -1;
     float sc = D2;
     bool done = false;
     for (int step = 0; step < kMaxSteps && !done; ++step) {
@@ -176,19 +175,19 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         load(tk, a, b, cc);
         float bn = -1.0f, bd = 0.0f;
         int bw = -1;
-        const auto edge = [&](float nx, float ny, float ce, int nbw, int e) {
+        const auto edge = [&](float nx, float ny, float ce, int nbw) {
             const float dd = -fmaf(nx, ux, ny * uy);
             const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
-            const bool okE = (e != forb) & (dd > 0.0f) & (nbw >= 0);
+            const bool okE = (dd > 0.0f) & (nbw >= 0);  // the entry edge has dd < 0 (see stepRay)
             if (okE && nm * bd > bn * dd) {
                 bn = nm;
                 bd = dd;
                 bw = nbw;
             }
         };
-        edge(a.x, a.y, a.z, __float_as_int(cc.y), 0);
-        edge(a.w, b.x, b.y, __float_as_int(cc.z), 1);
-        edge(b.z, b.w, cc.x, __float_as_int(cc.w), 2);
+        edge(a.x, a.y, a.z, __float_as_int(cc.y));
+        edge(a.w, b.x, b.y, __float_as_int(cc.z));
+        edge(b.z, b.w, cc.x, __float_as_int(cc.w));
         float sOut = fmaxf(fminf(__fdividef(bn, bd), sc), 0.0f);
         if (sOut <= m.tolEnd) {
             sOut = 0.0f;
@@ -231,7 +230,6 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         }
         if (!done) {
             tk = uint32_t(bw) >> 2;
-            forb = bw & 3;
             sc = sOut;
         }
     }
@@ -323,7 +321,6 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
             }
             GlobalLoader load{m.tri};
             uint32_t tk = t;
-            int forb = -1;
             float sc = D2;
             bool done = false;
             for (int step = 0; step < kMaxSteps && !done; ++step) {
@@ -331,19 +328,19 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 load(tk, a, b, cc);
                 float bn = -1.0f, bd = 0.0f;
                 int bw = -1;
-                const auto edge = [&](float nx, float ny, float ce, int nbw, int e) {
+                const auto edge = [&](float nx, float ny, float ce, int nbw) {
                     const float dd = -fmaf(nx, ux, ny * uy);
                     const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
-                    const bool okE = (e != forb) & (dd > 0.0f) & (nbw >= 0);
+                    const bool okE = (dd > 0.0f) & (nbw >= 0);  // the entry edge has dd < 0 (see stepRay)
                     if (okE && nm * bd > bn * dd) {
                         bn = nm;
                         bd = dd;
                         bw = nbw;
                     }
                 };
-                edge(a.x, a.y, a.z, __float_as_int(cc.y), 0);
-                edge(a.w, b.x, b.y, __float_as_int(cc.z), 1);
-                edge(b.z, b.w, cc.x, __float_as_int(cc.w), 2);
+                edge(a.x, a.y, a.z, __float_as_int(cc.y));
+                edge(a.w, b.x, b.y, __float_as_int(cc.z));
+                edge(b.z, b.w, cc.x, __float_as_int(cc.w));
                 float sOut = fmaxf(fminf(__fdividef(bn, bd), sc), 0.0f);
                 if (sOut <= m.tolEnd) {
                     sOut = 0.0f;
@@ -388,7 +385,6 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 }
                 if (!done) {
                     tk = uint32_t(bw) >> 2;
-                    forb = bw & 3;
                     sc = sOut;
                 }
             }

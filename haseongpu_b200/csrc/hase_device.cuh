@@ -130,7 +130,6 @@ struct Ray {
     uint32_t t;     // triangle
     int phys;       // physical layer of the current unfolded layer
     int pdir;       // +1 / -1
-    int forb;       // entry edge (excluded exit), -1 none
     int reflLeft;   // reflections the slice still implies
     int steps;
     float s;        // remaining distance to the image point
@@ -171,7 +170,6 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.t = t;
     r.phys = layer;
     r.pdir = 1;
-    r.forb = -1;
     r.reflLeft = expectedReflections(slice);
     r.steps = 0;
     r.s = D;
@@ -256,21 +254,25 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
     for (int k = 0; k < K; ++k) {
         float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
         int bw = -1;
-        const auto edge = [&](float nx, float ny, float cc, int nbw, int e) {
-            const float dd = -fmaf(nx, r.ux, ny * r.uy);       // > 0: moving out through e
+        const auto edge = [&](float nx, float ny, float cc, int nbw) {
+            const float dd = -fmaf(nx, r.ux, ny * r.uy);       // > 0: moving out through the edge
             const float nm = fmaf(nx, Sx, fmaf(ny, Sy, -cc));  // signed distance of the sample from the edge line
             // Boundary edges are never exits: the 2-D mesh is convex and the
             // target lies in it, so only rounding could route a ray across one.
-            const bool ok = (e != r.forb) & (dd > 0.0f) & (nbw >= 0);
+            // The entry edge needs no test: the two triangles of an edge store
+            // exactly negated normals (both are computed in FP64 from the same
+            // two points and rounded), so the entry edge's dd is exactly minus
+            // the dd > 0 it was chosen with in the previous triangle.
+            const bool ok = (dd > 0.0f) & (nbw >= 0);
             if (ok && nm * bd > bn * dd) {
                 bn = nm;
                 bd = dd;
                 bw = nbw;
             }
         };
-        edge(a.x, a.y, a.z, __float_as_int(c.y), 0);
-        edge(a.w, b.x, b.y, __float_as_int(c.z), 1);
-        edge(b.z, b.w, c.x, __float_as_int(c.w), 2);
+        edge(a.x, a.y, a.z, __float_as_int(c.y));
+        edge(a.w, b.x, b.y, __float_as_int(c.z));
+        edge(b.z, b.w, c.x, __float_as_int(c.w));
         // clamped at 0: the comparison sz < sEdge below is reached only with
         // sz > tolEnd >= 0, where the clamp does not change it
         const float sEdge = fmaxf(fminf(__fdividef(bn, bd), r.s), 0.0f);
@@ -304,7 +306,6 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
         }
         if (r.steps >= kMaxSteps) return kDropped;
         r.t = uint32_t(bw) >> 2;
-        r.forb = bw & 3;
         if (K > 1 && k + 1 < K) gb = __ldg(gcol + r.phys * m.T + r.t);
     }
     return kContinue;
