@@ -152,7 +152,10 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     float* out = L.lnw + size_t(row) * L.nW + size_t(j) * m.P + t;
 
     float J[G], lnR[G], invc[G];
-    int ka[G], phys[G], pdir[G], left[G];
+    // kf: the layer offset of the line's next level plane from the image level,
+    // an exact small-integer float (the plane lies at kf * invc)
+    float kf[G];
+    int phys[G], pdir[G], left[G];
     bool ok[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         ok[g] = l < int(m.layers) && __ldg(m.srcBeta + size_t(min(l, int(m.layers) - 1)) * m.T + t) > 0.0f;
         J[g] = 0.0f;
         lnR[g] = 0.0f;
-        ka[g] = l;
+        kf[g] = float(l + (kImg > l ? 1 : 0) - kImg);
         phys[g] = l;
         pdir[g] = 1;
         left[g] = expectedReflections(j);
@@ -204,12 +207,12 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
             float s = sc;
             float gb = gbv[g];
             while (true) {
-                const float sb = float(ka[g] + (dl > 0 ? 1 : 0) - kImg) * invc[g];
+                const float sb = kf[g] * invc[g];
                 if (!(sb > sOut)) break;
                 J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
                 s = sb;
                 const int cand = phys[g] + pdir[g] * dl;
-                if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+                if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
                     if (left[g] <= 0) {
                         ok[g] = false;
                         break;
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                     phys[g] = cand;
                     gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
                 }
-                ka[g] += dl;
+                kf[g] += float(dl);
             }
             if (!ok[g]) continue;
             J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);
@@ -293,7 +296,8 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
         const uint32_t nLines = L.slices * m.layers;
         for (uint32_t c0 = 0; c0 < nLines; c0 += TL * LPL) {
             float J[LPL], lnR[LPL], invc[LPL], nextPlane[LPL];
-            int ka[LPL], phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
+            float kf[LPL];  // as in importanceKernel
+            int phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
             uint32_t sl[LPL];
             bool ok[LPL];
             const uint16_t* order = m.lineOrder[L.slices == 5 ? 1 : 0];
@@ -310,14 +314,14 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 ok[g] = valid && __ldg(m.srcBeta + size_t(l) * m.T + t) > 0.0f;
                 J[g] = 0.0f;
                 lnR[g] = 0.0f;
-                ka[g] = int(l);
+                kf[g] = float(int(l) + (kImg[g] > int(l) ? 1 : 0) - kImg[g]);
                 phys[g] = int(l);
                 pdir[g] = 1;
                 left[g] = expectedReflections(j);
                 invc[g] = D2 / (float(int(l) - kImg[g]) + 0.5f);
                 // sigma of the next level plane toward the image level (carried,
                 // recomputed only when the line crosses it)
-                nextPlane[g] = float(int(l) + (kImg[g] > int(l) ? 1 : 0) - kImg[g]) * invc[g];
+                nextPlane[g] = kf[g] * invc[g];
             }
             GlobalLoader load{m.tri};
             uint32_t tk = t;
@@ -363,7 +367,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                         J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
                         s = sb;
                         const int cand = phys[g] + pdir[g] * dl;
-                        if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+                        if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
                             if (left[g] <= 0) {
                                 ok[g] = false;
                                 break;
@@ -377,8 +381,8 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                             phys[g] = cand;
                             gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
                         }
-                        ka[g] += dl;
-                        nextPlane[g] = float(ka[g] + (dl > 0 ? 1 : 0) - kImg[g]) * invc[g];
+                        kf[g] += float(dl);
+                        nextPlane[g] = kf[g] * invc[g];
                     }
                     if (!ok[g]) continue;
                     J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);

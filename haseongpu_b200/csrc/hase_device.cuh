@@ -293,7 +293,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             ++r.steps;
             if (sz < sEdge) break;
             const int cand = r.phys + r.pdir * dl;
-            if (cand < 0 || cand >= int(m.layers)) {  // a physical bottom/top surface: reflect
+            if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
                 if (r.reflLeft <= 0) return kDropped;
                 r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
                 --r.reflLeft;
