@@ -155,7 +155,9 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     // kf: the layer offset of the line's next level plane from the image level,
     // an exact small-integer float (the plane lies at kf * invc)
     float kf[G];
-    int phys[G], pdir[G], left[G];
+    // lrow: the line's physical layer x T; rstep: the row offset of the next
+    // physical layer toward the image level (+-T, flipped at a reflection)
+    int lrow[G], rstep[G], left[G];
     bool ok[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -164,8 +166,8 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         J[g] = 0.0f;
         lnR[g] = 0.0f;
         kf[g] = float(l + (kImg > l ? 1 : 0) - kImg);
-        phys[g] = l;
-        pdir[g] = 1;
+        lrow[g] = l * int(m.T);
+        rstep[g] = kImg > l ? int(m.T) : -int(m.T);
         left[g] = expectedReflections(j);
         invc[g] = D2 / (float(l - kImg) + 0.5f);
     }
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         // beta of every line's current prism in this triangle, issued together
         float gbv[G];
 #pragma unroll
-        for (int g = 0; g < G; ++g) gbv[g] = ok[g] ? __ldg(gcol + size_t(phys[g]) * m.T + tk) : 0.0f;
+        for (int g = 0; g < G; ++g) gbv[g] = ok[g] ? __ldg(gcol + uint32_t(lrow[g]) + tk) : 0.0f;
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             if (!ok[g]) continue;
@@ -211,8 +213,8 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                 if (!(sb > sOut)) break;
                 J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
                 s = sb;
-                const int cand = phys[g] + pdir[g] * dl;
-                if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
+                const int cand = lrow[g] + rstep[g];
+                if (uint32_t(cand) >= m.P) {  // a physical bottom/top surface: reflect
                     if (left[g] <= 0) {
                         ok[g] = false;
                         break;
@@ -221,10 +223,10 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                     const float uz = dz * rsqrtf(fmaf(D2, D2, dz * dz));
                     lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, uz));
                     --left[g];
-                    pdir[g] = -pdir[g];
+                    rstep[g] = -rstep[g];
                 } else {
-                    phys[g] = cand;
-                    gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
+                    lrow[g] = cand;
+                    gb = __ldg(gcol + uint32_t(cand) + tk);
                 }
                 kf[g] += float(dl);
             }
@@ -245,9 +247,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
             const float dz = (float(l - kImg) + 0.5f) * m.h;
             const float D3sq = fmaf(D2, D2, dz * dz);
             if (left[g] > 0) {  // the bounce happens at the target itself, in the final triangle
-                const int dl = kImg > l ? 1 : -1;
-                const int cand = phys[g] + pdir[g] * dl;
-                lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
+                lnR[g] += __logf(reflectFactor(m, tk, lrow[g] + rstep[g] < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
             }
             const float beta = __ldg(m.srcBeta + size_t(l) * m.T + t);
             v = __logf(beta * area * m.h / D3sq) + J[g] * (sqrtf(D3sq) * inv2) + lnR[g];
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
         for (uint32_t c0 = 0; c0 < nLines; c0 += TL * LPL) {
             float J[LPL], lnR[LPL], invc[LPL], nextPlane[LPL];
             float kf[LPL];  // as in importanceKernel
-            int phys[LPL], pdir[LPL], left[LPL], kImg[LPL], lay[LPL];
+            int lrow[LPL], rstep[LPL], left[LPL], kImg[LPL], lay[LPL];  // lrow, rstep: as in importanceKernel
             uint32_t sl[LPL];
             bool ok[LPL];
             const uint16_t* order = m.lineOrder[L.slices == 5 ? 1 : 0];
@@ -315,8 +315,8 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 J[g] = 0.0f;
                 lnR[g] = 0.0f;
                 kf[g] = float(int(l) + (kImg[g] > int(l) ? 1 : 0) - kImg[g]);
-                phys[g] = int(l);
-                pdir[g] = 1;
+                lrow[g] = int(l * m.T);
+                rstep[g] = kImg[g] > int(l) ? int(m.T) : -int(m.T);
                 left[g] = expectedReflections(j);
                 invc[g] = D2 / (float(int(l) - kImg[g]) + 0.5f);
                 // sigma of the next level plane toward the image level (carried,
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 }
                 float gbv[LPL];
 #pragma unroll
-                for (int g = 0; g < LPL; ++g) gbv[g] = ok[g] ? __ldg(gcol + size_t(phys[g]) * m.T + tk) : 0.0f;
+                for (int g = 0; g < LPL; ++g) gbv[g] = ok[g] ? __ldg(gcol + uint32_t(lrow[g]) + tk) : 0.0f;
 #pragma unroll
                 for (int g = 0; g < LPL; ++g) {
                     if (!ok[g]) continue;
@@ -366,8 +366,8 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                         if (COUNT) ++counted;
                         J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sb, J[g]);
                         s = sb;
-                        const int cand = phys[g] + pdir[g] * dl;
-                        if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
+                        const int cand = lrow[g] + rstep[g];
+                        if (uint32_t(cand) >= m.P) {  // a physical bottom/top surface: reflect
                             if (left[g] <= 0) {
                                 ok[g] = false;
                                 break;
@@ -376,10 +376,10 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                             const float uz = dz * rsqrtf(fmaf(D2, D2, dz * dz));
                             lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, uz));
                             --left[g];
-                            pdir[g] = -pdir[g];
+                            rstep[g] = -rstep[g];
                         } else {
-                            phys[g] = cand;
-                            gb = __ldg(gcol + size_t(phys[g]) * m.T + tk);
+                            lrow[g] = cand;
+                            gb = __ldg(gcol + uint32_t(cand) + tk);
                         }
                         kf[g] += float(dl);
                         nextPlane[g] = kf[g] * invc[g];
@@ -401,9 +401,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                     const float dz = (float(l - kImg[g]) + 0.5f) * m.h;
                     const float D3sq = fmaf(D2, D2, dz * dz);
                     if (left[g] > 0) {  // the bounce happens at the target itself, in the final triangle
-                        const int dl = kImg[g] > l ? 1 : -1;
-                        const int cand = phys[g] + pdir[g] * dl;
-                        lnR[g] += __logf(reflectFactor(m, tk, cand < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
+                        lnR[g] += __logf(reflectFactor(m, tk, lrow[g] + rstep[g] < 0 ? 0 : 1, dz * rsqrtf(D3sq)));
                     }
                     const float beta = __ldg(m.srcBeta + size_t(l) * m.T + t);
                     v = __logf(beta * area * m.h / D3sq) + J[g] * (sqrtf(D3sq) * inv2) + lnR[g];
@@ -796,15 +794,14 @@ __device__ __forceinline__ float startRay(const MeshView& m, uint32_t r, uint32_
     if (nearField && (int(l) == kImg || int(l) + 1 == kImg) &&
         nearFieldStart(m, t, int(l), kImg, sample % m.Np, S, unit24(rnd.x >> 8), unit24(rnd.z >> 8),
                        unit24(rnd.w >> 8), dx, dy, dz, alphaL)) {
-        D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m.h);
+        D2 = initRay(ray, t, int(l), dx, dy, dz, kImg, j, ab.x, ab.y, m);
         wf = __fdividef(__ldg(m.srcBeta + p) * alphaL, qf);
     } else {
         const float u1 = unit24(k1), u2 = unit24(k2), u3 = unit24(rnd.z >> 8);
         const float4 g0 = __ldg(m.geo + 2 * t), g1 = __ldg(m.geo + 2 * t + 1);
         const float x = fmaf(u2, g1.x, fmaf(u1, g0.z, g0.x));
         const float y = fmaf(u2, g1.y, fmaf(u1, g0.w, g0.y));
-        D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j, ab.x, ab.y,
-                     m.h);
+        D2 = initRay(ray, t, int(l), x - S.x, y - S.y, (float(int(l) - kImg) + u3) * m.h, kImg, j, ab.x, ab.y, m);
         wf = __fdividef(__ldg(m.srcBeta + p) * g1.z * m.h, D2 * qf);
     }
     return D2;
@@ -1277,7 +1274,7 @@ __global__ void traceKernel(TraceLaunch L) {
     const float zImgOffset = float(kImg) * m.h;
     Ray r;
     const float D2 = initRay(r, L.tri[i], int(L.level[i]), L.start[3 * i] - S.x, L.start[3 * i + 1] - S.y,
-                             L.start[3 * i + 2] - zImgOffset, kImg, j, L.A, L.B, m.h);
+                             L.start[3 * i + 2] - zImgOffset, kImg, j, L.A, L.B, m);
     GlobalLoader load{m.tri};
     int st;
     do {

@@ -123,13 +123,14 @@ __device__ __forceinline__ float reflectFactor(const MeshView& m, uint32_t t, in
 }
 
 // One ray in flight.  The walk runs in the unfolded z coordinate (reflection
-// images); `phys` is the physical layer of the current unfolded layer and
-// `pdir` the sign mapping unfolded to physical layer steps (it flips at every
-// reflection), so no division or modulo is needed per crossing.
+// images); `row` is the prism-index offset (physical layer x T) of the current
+// unfolded layer and `rstep` the offset of the next physical layer toward the
+// image point, +T or -T (it flips at every reflection), so no division, modulo
+// or multiplication is needed per crossing.
 struct Ray {
     uint32_t t;     // triangle
-    int phys;       // physical layer of the current unfolded layer
-    int pdir;       // +1 / -1
+    int row;        // physical layer of the current unfolded layer, times T
+    int rstep;      // +T / -T
     int reflLeft;   // reflections the slice still implies
     int steps;
     float s;        // remaining distance to the image point
@@ -162,14 +163,14 @@ enum WalkMode {
 // from the image point (Sx, Sy, kImg*h), in physical layer `layer`.
 // Returns |start - image|^2.
 __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx, float dy, float dz, int kImg,
-                                         uint32_t slice, float A, float B, float h) {
+                                         uint32_t slice, float A, float B, const MeshView& m) {
+    const float h = m.h;
     if (dz == 0.0f) dz = 1e-6f * h;  // a ray inside a level plane: nudge it off the plane
     const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const float D = sqrtf(D2);
     const float inv = 1.0f / D;
     r.t = t;
-    r.phys = layer;
-    r.pdir = 1;
+    r.row = layer * int(m.T);
     r.reflLeft = expectedReflections(slice);
     r.steps = 0;
     r.s = D;
@@ -181,6 +182,7 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.uy = dy * inv;
     r.uz = dz * inv;
     r.hOverUz = __fdividef(h, r.uz);
+    r.rstep = r.uz > 0.0f ? -int(m.T) : int(m.T);  // toward the image: down when uz > 0
     // moving toward the image: down (dl = -1) when uz > 0, up (dl = +1) otherwise
     r.zl = float(layer + (r.uz > 0.0f ? 0 : 1) - kImg);
     r.A = A;
@@ -249,7 +251,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
     load(r.t, a, b, c);
     // beta (kWalkTable: g) of the current prism, issued with the record so
     // that its latency overlaps the edge tests
-    float gb = __ldg(gcol + r.phys * m.T + r.t);
+    float gb = __ldg(gcol + r.row + r.t);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
         float bn = -1.0f, bd = 0.0f;  // best fraction so far (-1/0 = -inf)
@@ -292,21 +294,21 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             r.s = next;
             ++r.steps;
             if (sz < sEdge) break;
-            const int cand = r.phys + r.pdir * dl;
-            if (uint32_t(cand) >= m.layers) {  // a physical bottom/top surface: reflect
+            const int cand = r.row + r.rstep;
+            if (uint32_t(cand) >= m.P) {  // a physical bottom/top surface: reflect
                 if (r.reflLeft <= 0) return kDropped;
                 r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
                 --r.reflLeft;
-                r.pdir = -r.pdir;
+                r.rstep = -r.rstep;
             } else {
-                r.phys = cand;
+                r.row = cand;
             }
             r.zl += float(dl);
-            gb = __ldg(gcol + r.phys * m.T + r.t);
+            gb = __ldg(gcol + r.row + r.t);
         }
         if (r.steps >= kMaxSteps) return kDropped;
         r.t = uint32_t(bw) >> 2;
-        if (K > 1 && k + 1 < K) gb = __ldg(gcol + r.phys * m.T + r.t);
+        if (K > 1 && k + 1 < K) gb = __ldg(gcol + r.row + r.t);
     }
     return kContinue;
 }
@@ -315,8 +317,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
 // itself (a sample on the reflecting surface) is applied in the final triangle.
 __device__ __forceinline__ void finishReflections(const MeshView& m, Ray& r) {
     if (r.reflLeft > 0) {
-        const int cand = r.phys + r.pdir * (r.uz > 0.0f ? -1 : 1);
-        r.G += __logf(reflectFactor(m, r.t, cand < 0 ? 0 : 1, r.uz));
+        r.G += __logf(reflectFactor(m, r.t, r.row + r.rstep < 0 ? 0 : 1, r.uz));
         r.reflLeft = 0;
     }
 }
