@@ -152,8 +152,10 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
     float* out = L.lnw + size_t(row) * L.nW + size_t(j) * m.P + t;
 
     float J[G], lnR[G], invc[G];
-    // kf: the layer offset of the line's next level plane from the image level,
-    // an exact small-integer float (the plane lies at kf * invc)
+    // the line's next level plane lies at s = kf * invc: kf is the plane's
+    // level offset from the image level (an exact small-integer float) and
+    // invc the distance per level, both times the line's layer step toward the
+    // image level, so that kf grows by 1 per plane
     float kf[G];
     // lrow: the line's physical layer x T; rstep: the row offset of the next
     // physical layer toward the image level (+-T, flipped at a reflection)
@@ -165,11 +167,12 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         ok[g] = l < int(m.layers) && __ldg(m.srcBeta + size_t(min(l, int(m.layers) - 1)) * m.T + t) > 0.0f;
         J[g] = 0.0f;
         lnR[g] = 0.0f;
-        kf[g] = float(l + (kImg > l ? 1 : 0) - kImg);
+        kf[g] = kImg > l ? float(l + 1 - kImg) : float(kImg - l);
         lrow[g] = l * int(m.T);
         rstep[g] = kImg > l ? int(m.T) : -int(m.T);
         left[g] = expectedReflections(j);
-        invc[g] = D2 / (float(l - kImg) + 0.5f);
+        const float ic = D2 / (float(l - kImg) + 0.5f);
+        invc[g] = kImg > l ? ic : -ic;
     }
     GlobalLoader load{m.tri};
     uint32_t tk = t;
@@ -205,7 +208,6 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             if (!ok[g]) continue;
-            const int dl = kImg > l0 + g ? 1 : -1;  // layer step toward the image level
             float s = sc;
             float gb = gbv[g];
             while (true) {
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
                     lrow[g] = cand;
                     gb = __ldg(gcol + uint32_t(cand) + tk);
                 }
-                kf[g] += float(dl);
+                kf[g] += 1.0f;
             }
             if (!ok[g]) continue;
             J[g] = fmaf(TAB ? gb : ((gb == gb) ? fmaf(gb, L.A, -L.B) : -m.cladAbs), s - sOut, J[g]);
@@ -314,11 +316,12 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 ok[g] = valid && __ldg(m.srcBeta + size_t(l) * m.T + t) > 0.0f;
                 J[g] = 0.0f;
                 lnR[g] = 0.0f;
-                kf[g] = float(int(l) + (kImg[g] > int(l) ? 1 : 0) - kImg[g]);
+                kf[g] = kImg[g] > int(l) ? float(int(l) + 1 - kImg[g]) : float(kImg[g] - int(l));
                 lrow[g] = int(l * m.T);
                 rstep[g] = kImg[g] > int(l) ? int(m.T) : -int(m.T);
                 left[g] = expectedReflections(j);
-                invc[g] = D2 / (float(int(l) - kImg[g]) + 0.5f);
+                const float ic = D2 / (float(int(l) - kImg[g]) + 0.5f);
+                invc[g] = kImg[g] > int(l) ? ic : -ic;
                 // sigma of the next level plane toward the image level (carried,
                 // recomputed only when the line crosses it)
                 nextPlane[g] = kf[g] * invc[g];
@@ -357,7 +360,6 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 for (int g = 0; g < LPL; ++g) {
                     if (!ok[g]) continue;
                     if (COUNT) ++counted;
-                    const int dl = kImg[g] > lay[g] ? 1 : -1;  // layer step toward the image level
                     float s = sc;
                     float gb = gbv[g];
                     while (true) {
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                             lrow[g] = cand;
                             gb = __ldg(gcol + uint32_t(cand) + tk);
                         }
-                        kf[g] += float(dl);
+                        kf[g] += 1.0f;
                         nextPlane[g] = kf[g] * invc[g];
                     }
                     if (!ok[g]) continue;

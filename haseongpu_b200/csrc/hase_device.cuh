@@ -140,9 +140,12 @@ struct Ray {
     float Lc;       // path length in cladding prisms (kWalkBeta)
     float D;        // path length, start to image point
     float ux, uy, uz;
-    float hOverUz;  // h / uz
-    float zl;       // unfolded layer index + level-plane offset: the current layer's exit plane lies zl h
-                    // from the image point along z (a small integer, exact in float)
+    // the current layer's exit plane lies at s = zl hOverUz: zl is the plane's
+    // unfolded level offset from the image point (a small integer, exact in
+    // float) and hOverUz = h / uz, both times the layer step toward the image
+    // (-1 when uz > 0, else +1), so that zl grows by 1 per plane
+    float hOverUz;
+    float zl;
 };
 
 enum StepResult { kContinue = 0, kDone = 1, kDropped = 2 };
@@ -181,10 +184,11 @@ __device__ __forceinline__ float initRay(Ray& r, uint32_t t, int layer, float dx
     r.ux = dx * inv;
     r.uy = dy * inv;
     r.uz = dz * inv;
-    r.hOverUz = __fdividef(h, r.uz);
-    r.rstep = r.uz > 0.0f ? -int(m.T) : int(m.T);  // toward the image: down when uz > 0
-    // moving toward the image: down (dl = -1) when uz > 0, up (dl = +1) otherwise
-    r.zl = float(layer + (r.uz > 0.0f ? 0 : 1) - kImg);
+    // moving toward the image: down (layer step -1) when uz > 0, up (+1) otherwise
+    const float hu = __fdividef(h, r.uz);
+    r.hOverUz = r.uz > 0.0f ? -hu : hu;
+    r.zl = r.uz > 0.0f ? float(kImg - layer) : float(layer + 1 - kImg);
+    r.rstep = r.uz > 0.0f ? -int(m.T) : int(m.T);
     r.A = A;
     r.B = B;
     return D2;
@@ -281,7 +285,6 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
         if (K > 1 && k + 1 < K && bw >= 0) load(uint32_t(bw) >> 2, a, b, c);
         // Level planes crossed before the edge exit: the triangle, and with it
         // sEdge, stays the same, so they cost no edge test.
-        const int dl = r.uz > 0.0f ? -1 : 1;
         while (true) {
             const float sz = fminf(r.zl * r.hOverUz, r.s);
             const float next = fmaxf(sEdge, sz);
@@ -303,7 +306,7 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             } else {
                 r.row = cand;
             }
-            r.zl += float(dl);
+            r.zl += 1.0f;
             gb = __ldg(gcol + r.row + r.t);
         }
         if (r.steps >= kMaxSteps) return kDropped;
