@@ -62,11 +62,11 @@ FWD_TRAFFIC_DISC_POLY = 49128192   # DRAM bytes of one fwdRayKernel launch on th
 FP64_LANES_PER_SM = 64
 # DRAM bytes of one learned-solve rayKernel launch on disc_small (5,470 samples x 1e5 rays; ncu): the per-sample
 # ray maps (q, offsets) read once and the per-item partial sums written; the walk tables stay in L1/L2
-RAY_TRAFFIC_LEARNED = 403811328 + 29646848
-# what binds the same launch (ncu --set full, profiles/rayKernel_learned_disc_small.md): instruction issue, with
-# the walk tables in L1 -- thread instructions per crossing and per ray of that capture
-RAY_BINDING_LEARNED = "instruction issue (ncu: issue active 86.5 %, top stall 'not selected'; L1 hits 99.2 %)"
-RAY_INSTR_LEARNED = {"per_crossing": 112, "per_ray": 1590, "crossings_per_ray": 14.2}
+RAY_TRAFFIC_LEARNED = 402847744 + 29695232
+# what binds the same launch (ncu --set full of it): instruction issue, with the walk tables in L1 -- thread
+# instructions per crossing and per ray of that capture (3.09e10 warp instructions x 24.4 threads, 5.47e8 rays)
+RAY_BINDING_LEARNED = "instruction issue (ncu: issue active 85.6 %, top stall 'not selected'; L1 hits 99.2 %)"
+RAY_INSTR_LEARNED = {"per_crossing": 97, "per_ray": 1379, "crossings_per_ray": 14.2}
 
 
 def parse():
