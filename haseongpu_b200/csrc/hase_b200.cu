@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <limits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         const float ic = D2 / (float(l - kImg) + 0.5f);
         invc[g] = kImg > l ? ic : -ic;
     }
-    GlobalLoader load{m.tri};
+    GlobalLoader load{m.walk};
     uint32_t tk = t;
     float sc = D2;
     bool done = false;
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(256) importanceKernel(ImportanceLaunch L) {
         const auto edge = [&](float nx, float ny, float ce, int nbw) {
             const float dd = -fmaf(nx, ux, ny * uy);
             const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
-            const bool okE = (dd > 0.0f) & (nbw >= 0);  // the entry edge has dd < 0 (see stepRay)
+            const bool okE = dd > 0.0f;  // the entry edge has dd < 0, a boundary edge NaN (see stepRay)
             if (okE && nm * bd > bn * dd) {
                 bn = nm;
                 bd = dd;
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 // recomputed only when the line crosses it)
                 nextPlane[g] = kf[g] * invc[g];
             }
-            GlobalLoader load{m.tri};
+            GlobalLoader load{m.walk};
             uint32_t tk = t;
             float sc = D2;
             bool done = false;
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(256) importanceTeamKernel(ImportanceLaunch L) 
                 const auto edge = [&](float nx, float ny, float ce, int nbw) {
                     const float dd = -fmaf(nx, ux, ny * uy);
                     const float nm = fmaf(nx, S.x, fmaf(ny, S.y, -ce));
-                    const bool okE = (dd > 0.0f) & (nbw >= 0);  // the entry edge has dd < 0 (see stepRay)
+                    const bool okE = dd > 0.0f;  // the entry edge has dd < 0, a boundary edge NaN (see stepRay)
                     if (okE && nm * bd > bn * dd) {
                         bn = nm;
                         bd = dd;
@@ -980,7 +981,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) rayKernel(RayLaunch L) {
 #define HASE_SPEC (POOL ? (const float2*)iv.spec : L.spec)
         const double Cm = POOL ? double(iv.C) : double(L.C);
         const MeshView& m = POOL ? sInst[threadIdx.x >> 5].m : L.m;
-        const GlobalLoader load{m.tri};
+        const GlobalLoader load{m.walk};
         const uint32_t r0 = k * L.itemRays;
         const uint32_t r1 = min(r0 + L.itemRays, L.M);
         const uint32_t* off = L.offsets + oBase;
@@ -1277,7 +1278,7 @@ __global__ void traceKernel(TraceLaunch L) {
     Ray r;
     const float D2 = initRay(r, L.tri[i], int(L.level[i]), L.start[3 * i] - S.x, L.start[3 * i + 1] - S.y,
                              L.start[3 * i + 2] - zImgOffset, kImg, j, L.A, L.B, m);
-    GlobalLoader load{m.tri};
+    GlobalLoader load{m.walk};
     int st;
     do {
         st = stepRay(m, S.x, S.y, r, load);
@@ -1853,7 +1854,7 @@ void invariantDivisor(uint32_t d, uint32_t& mul, uint32_t& shift) {
 
 struct HostTables {
     std::vector<int4> verts;
-    std::vector<float4> tri, geo;
+    std::vector<float4> tri, walk, geo;
     std::vector<float2> centroid, points;
 };
 
@@ -1918,6 +1919,19 @@ hase_status buildHostTables(const hase_mesh_desc* d, HostTables& h, double& exte
         }
         float* rec = &h.tri[3 * t + 2].y;
         std::memcpy(rec, w, sizeof(w));
+    }
+    // the walks' copy: a boundary edge's normal is NaN, so its dd > 0 test fails
+    // and the walks need no separate boundary test
+    h.walk = h.tri;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    for (uint32_t t = 0; t < T; ++t) {
+        float* r = &h.walk[3 * size_t(t)].x;  // nx0 ny0 c0 nx1 | ny1 c1 nx2 ny2 | c2 nb0 nb1 nb2
+        static const int kNx[3] = {0, 3, 6}, kNy[3] = {1, 4, 7};
+        for (int e = 0; e < 3; ++e) {
+            int32_t nb;
+            std::memcpy(&nb, r + 9 + e, sizeof(nb));
+            if (nb < 0) r[kNx[e]] = r[kNy[e]] = nan;
+        }
     }
     return HASE_OK;
 }
@@ -2162,7 +2176,7 @@ struct hase_context {
     std::vector<double> betaCells, sigmaA, sigmaE;
     bool hasReflect = false;
     float tirCos2[2] = {-1.0f, -1.0f};
-    DevBuf<float4> tri, geo;
+    DevBuf<float4> tri, walk, geo;
     DevBuf<int4> verts;
     DevBuf<uint16_t> lineOrder[2];  // importance line order per sample level: 1 and 5 reflection slices
     // local proposal (hase_context_set_local_proposal): per point the K
@@ -2218,6 +2232,7 @@ struct hase_context {
         invariantDivisor(T, v.divTm, v.divTs);
         invariantDivisor(Np, v.divNpm, v.divNps);
         v.tri = tri.p;
+        v.walk = walk.p;
         v.geo = geo.p;
         v.verts = verts.p;
         v.centroid = centroid.p;
@@ -2651,6 +2666,7 @@ hase_status hase_context_create(const hase_mesh_desc* d, const hase_spectrum_des
         return HASE_OK;
     };
     if ((st = up(c->tri, ht.tri)) != HASE_OK) return cleanup(st);
+    if ((st = up(c->walk, ht.walk)) != HASE_OK) return cleanup(st);
     if ((st = up(c->geo, ht.geo)) != HASE_OK) return cleanup(st);
     if ((st = up(c->verts, ht.verts)) != HASE_OK) return cleanup(st);
     if (uint64_t(5) * c->layers < 65536) {  // importance line order (16-bit line indices)

@@ -69,6 +69,7 @@ __device__ __forceinline__ float unit24(uint32_t k24) { return (float(k24) + 0.5
 //   g0 = (ax, ay, bx-ax, by-ay), g1 = (cx-ax, cy-ay, area, 0); centroid separate.
 struct MeshView {
     const float4* tri;       // [T][3]
+    const float4* walk;      // [T][3]: tri with NaN normals on mesh-boundary edges (the walks' records)
     const float4* geo;       // [T][2]
     const int4* verts;       // [T] point ids of the triangle's vertices (w unused)
     const float2* centroid;  // [T]
@@ -265,11 +266,13 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             const float nm = fmaf(nx, Sx, fmaf(ny, Sy, -cc));  // signed distance of the sample from the edge line
             // Boundary edges are never exits: the 2-D mesh is convex and the
             // target lies in it, so only rounding could route a ray across one.
-            // The entry edge needs no test: the two triangles of an edge store
-            // exactly negated normals (both are computed in FP64 from the same
-            // two points and rounded), so the entry edge's dd is exactly minus
-            // the dd > 0 it was chosen with in the previous triangle.
-            const bool ok = (dd > 0.0f) & (nbw >= 0);
+            // The walk records (MeshView::walk) give them NaN normals, so
+            // their dd > 0 test fails.  The entry edge needs no test either:
+            // the two triangles of an edge store exactly negated normals (both
+            // are computed in FP64 from the same two points and rounded), so
+            // the entry edge's dd is exactly minus the dd > 0 it was chosen
+            // with in the previous triangle.
+            const bool ok = dd > 0.0f;
             if (ok && nm * bd > bn * dd) {
                 bn = nm;
                 bd = dd;
