@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "hase_importance_weights",
     "hase_importance_crossings",
     "hase_ray_map",
+    "hase_mesh_tables",
     "hase_trace_rays",
     "hase_philox",
     "hase_probe_l2_bandwidth",

@@ -3765,6 +3765,19 @@ hase_status hase_ray_map(uint32_t rows, uint32_t n, const float* weights, uint32
     return HASE_OK;
 }
 
+hase_status hase_mesh_tables(const hase_mesh_desc* d, float* tri, float* walk) {
+    if (!d || !d->points || !d->triangles || d->numberOfTriangles == 0)
+        return fail(HASE_INVALID_ARGUMENT, "mesh points and triangles are required");
+    HostTables ht;
+    double extent = 0.0;
+    const hase_status st = buildHostTables(d, ht, extent);
+    if (st != HASE_OK) return st;
+    const size_t bytes = ht.tri.size() * sizeof(float4);
+    if (tri) std::memcpy(tri, ht.tri.data(), bytes);
+    if (walk) std::memcpy(walk, ht.walk.data(), bytes);
+    return HASE_OK;
+}
+
 hase_status hase_trace_rays(hase_context* c, uint32_t n, const float* start, const uint32_t* tri,
                             const uint32_t* level, const uint32_t* sample, const uint32_t* slice, uint32_t wavelength,
                             float* lnGain, float* distance, uint32_t* dropped) {

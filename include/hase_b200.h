@@ -203,6 +203,16 @@ hase_status hase_grid_weights(hase_context* ctx, uint32_t firstSample, uint32_t 
 hase_status hase_importance_crossings(hase_context* ctx, uint32_t firstSample, uint32_t count,
                                       uint32_t useReflections, uint64_t* crossings);
 
+/* The prism walk records hase_context_create builds on the host (no device
+ * needed; the reference derives the same neighbour table in
+ * pyInclude/geometry/core.py:733 _derived_topology): per triangle 12 floats, the outward
+ * unit normal and line constant (nx, ny, c) of its three edges followed by
+ * the three neighbour codes as int bits (neighbour << 2 | the edge's index in
+ * the neighbour, -1 at the mesh boundary), edge e joining the triangle's
+ * points e and e + 1.  `tri` receives the records as given, `walk` the walks'
+ * copy with NaN normals on the boundary edges; either may be NULL. */
+hase_status hase_mesh_tables(const hase_mesh_desc* mesh, float* tri, float* walk);
+
 /* Ray->prism map of `rows` weight rows of length n: q[row][n] (quantised
  * weights), offsets[row][n+1] (exclusive ray offsets), Q[row]. */
 hase_status hase_ray_map(uint32_t rows, uint32_t n, const float* weights, uint32_t rays, const uint32_t* phases,
