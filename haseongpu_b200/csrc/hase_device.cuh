@@ -245,7 +245,7 @@ __device__ __forceinline__ double rayMeanGain(const Ray& r, const float2* spec, 
 // current record no longer needs) while the current column's level planes are
 // worked through, so its latency is hidden behind them.
 // The walk is bound by instruction issue, so the level-plane loop is kept
-// short: the step bound is checked once per column (the loop itself ends
+// short: the step bound is checked once per call (the loop itself ends
 // within 3 x layers crossings: every physical layer step reaches a surface and
 // at most two reflections are allowed), and kWalkTable walks the table of g = beta A
 // - B (m.gTab) instead of evaluating it at every crossing (WalkMode).
@@ -312,11 +312,12 @@ __device__ __forceinline__ int stepRay(const MeshView& m, float Sx, float Sy, Ra
             r.zl += 1.0f;
             gb = __ldg(gcol + r.row + r.t);
         }
-        if (r.steps >= kMaxSteps) return kDropped;
         r.t = uint32_t(bw) >> 2;
         if (K > 1 && k + 1 < K) gb = __ldg(gcol + r.row + r.t);
     }
-    return kContinue;
+    // the step bound, once per call: a call walks at most K columns of at most
+    // 1 + 3 x layers segments each
+    return r.steps >= kMaxSteps ? kDropped : kContinue;
 }
 
 // After kDone: a reflection the slice implies but which happens at the target
